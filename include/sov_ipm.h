@@ -1,0 +1,239 @@
+/*
+ * sov_ipm.h -- C ABI of the B200 Mehrotra predictor-corrector interior-point engine.
+ *
+ * Plain C types only (fixed-width integers, doubles, raw pointers), so any host language that
+ * can call C can bind it. Every entry point returns 0 on success or a negative SOV_E* code on an
+ * argument / device error; the solve status itself is reported in sov_result.status.
+ *
+ * Reference interfaces replaced (paths inside the Abhishekmishra2808/sovereign tree):
+ *   sov_lp_solve        <- sovereign::InteriorPointSolver::solve
+ *                          solver/lp/include/sovereign/interior_point.hpp:26-36,
+ *                          solver/lp/src/interior_point.cpp:747-757 (reached from
+ *                          LpSolver::solve, solver/lp/src/lp_solver.cpp:59-62,70-72)
+ *   sov_qp_solve        <- sovereign::QpInteriorPointSolver::solve
+ *                          solver/qp/include/sovereign/qp_interior_point.hpp:21-31,
+ *                          solver/qp/src/qp_interior_point.cpp:3123-3186 (generic path)
+ *   sov_lp_solve_batch  <- no batched entry in the reference; replaces N independent
+ *                          InteriorPointSolver::solve calls (e.g. MILP node LPs,
+ *                          solver/milp/src/branch_and_bound.cpp:497)
+ *   sov_device_info     <- sovereign::cuda::device_info / gpu_available
+ *                          solver/gpu/include/sovereign/cuda_driver.hpp:14-40,
+ *                          solver/gpu/include/sovereign/gpu_spmv.hpp:16-49
+ *   sov_spmv_csc        <- sovereign::spmv_csc_auto (solver/gpu/src/gpu_spmv.cpp:70-102)
+ *   sov_normal_factor_solve <- NormalEquations::factor + ::solve
+ *                          (solver/lp/src/interior_point.cpp:163-182)
+ *
+ * Models cross the boundary in index form: variable j and row i of a sovereign::OptimizationModel
+ * (solver/core/include/sovereign/types.hpp:53-59) become column j and row i here; the adapter in
+ * sov_ipm_adapter.hpp maps names to indices and results back to name-keyed maps.
+ */
+#ifndef SOV_IPM_H
+#define SOV_IPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* sovereign::SolverStatus, same order (types.hpp:20-30). */
+enum {
+  SOV_OPTIMAL = 0,
+  SOV_FEASIBLE = 1,
+  SOV_INFEASIBLE = 2,
+  SOV_UNBOUNDED = 3,
+  SOV_TIME_LIMIT = 4,
+  SOV_ITERATION_LIMIT = 5,
+  SOV_NUMERICAL_ERROR = 6,
+  SOV_ERROR = 7,
+  SOV_NOT_IMPLEMENTED = 8
+};
+
+/* sovereign::ConstraintSense (types.hpp:12). */
+enum { SOV_LE = 0, SOV_GE = 1, SOV_EQ = 2 };
+
+/* Return codes of the entry points (the solve outcome is in sov_result.status). */
+enum {
+  SOV_OK = 0,
+  SOV_E_ARGUMENT = -1,   /* null pointer, negative size, inconsistent CSC */
+  SOV_E_NO_DEVICE = -2,  /* no CUDA device or the sm_100a kernels cannot load */
+  SOV_E_CUDA = -3,       /* a CUDA call failed; the message names it */
+  SOV_E_TOO_LARGE = -4,  /* model exceeds the engine's size limits */
+  SOV_E_UNSUPPORTED = -5 /* model shape this engine does not solve (message says why) */
+};
+
+/* Arithmetic of the Newton solves. */
+enum {
+  SOV_PRECISION_FP64 = 0,  /* FP64 normal matrix, FP64 Cholesky, FP64 solves */
+  SOV_PRECISION_MIXED = 1  /* FP32 normal matrix + FP32 (3xTF32 tensor-core) Cholesky as the
+                              preconditioner of FP64 PCG; FP64 residuals, mu, sigma, ratio test */
+};
+
+/* Normal-equation factorization (the reference's SOVEREIGN_IPM_NORMAL_EQUATIONS knob). */
+enum {
+  SOV_FACTOR_AUTO = 0,   /* banded when the bandwidth is small, else dense */
+  SOV_FACTOR_DENSE = 1,  /* dense m x m Cholesky (dense-Schur) */
+  SOV_FACTOR_BANDED = 2  /* banded LDL^T in the natural row order */
+};
+
+/* One LP or convex QP in index form.
+ *   min/max  obj'x + 1/2 x'Qx + obj_constant
+ *   s.t.     sum_j A[i][j] x_j  (<=, >=, =)  rhs[i]      (sense[i])
+ *            lb[j] <= x_j <= ub[j]
+ * A is column-compressed (CSC), m x n; duplicate (row, col) entries are summed.
+ * lb <= -1e29 means no lower bound (QP only; the LP path shifts every column by lb);
+ * ub >= 1e29 means no upper bound (interior_point.cpp:239, qp_interior_point.cpp:135-138).
+ * Q (QP only, else NULL) holds the stored quadratic terms q_ij of Objective::quadratic
+ * (types.hpp:43) column-compressed, each stored term once: the objective term is
+ * 1/2 * sum over stored terms of q_ij x_i x_j (qp_interior_point.cpp:65-67). */
+typedef struct sov_model {
+  int32_t n;
+  int32_t m;
+  int32_t maximize;
+  int32_t reserved;
+  const int32_t* col_ptr;  /* n + 1 */
+  const int32_t* row_idx;  /* nnz */
+  const double* values;    /* nnz */
+  const double* obj;       /* n */
+  double obj_constant;
+  const double* lb;        /* n */
+  const double* ub;        /* n */
+  const int8_t* sense;     /* m: SOV_LE / SOV_GE / SOV_EQ */
+  const double* rhs;       /* m */
+  const int32_t* q_col_ptr; /* n + 1, or NULL */
+  const int32_t* q_row_idx;
+  const double* q_values;
+} sov_model;
+
+/* Solver options; sov_default_lp_options / sov_default_qp_options give the reference defaults
+ * (InteriorPointOptions, interior_point.hpp:7-24; QpInteriorPointOptions,
+ * qp_interior_point.hpp:7-18). */
+typedef struct sov_options {
+  int32_t max_iterations;
+  int32_t enable_scaling;
+  double feasibility_tol;
+  double optimality_tol;
+  double fraction_to_boundary;
+  int32_t precision;      /* SOV_PRECISION_* */
+  int32_t factorization;  /* SOV_FACTOR_* */
+  /* Optional warm start in the engine's internal standard form (scaled, shifted, slack columns
+   * appended; sizes from sov_ipm_dims). NULL = Mehrotra-style start (interior_point.cpp:488-506).
+   * A warm start that is worse than the default start is discarded. */
+  const double* warm_x;   /* n_ipm */
+  const double* warm_y;   /* m_ipm */
+  const double* warm_s;   /* n_ipm */
+  /* Mixed precision: cap on FP64 PCG iterations per Newton solve before the engine refactors in
+   * FP64 for that iteration. */
+  int32_t pcg_max_iterations;
+  int32_t reserved;
+} sov_options;
+
+/* Per-solve diagnostics (the fields of sovereign::LpDiagnostics, types.hpp:64-89, that the IPM
+ * fills at interior_point.cpp:366-407,616-631,700-707). Optional: pass NULL to skip. */
+#define SOV_HISTORY_MAX 128
+typedef struct sov_diagnostics {
+  int32_t scaling_applied;
+  int32_t history_len;
+  int32_t step_history_len;
+  int32_t refactorizations;
+  double coefficient_min_abs_before, coefficient_max_abs_before;
+  double coefficient_min_abs_after, coefficient_max_abs_after;
+  int64_t stall_iteration;
+  double stall_gap, stall_mu, stall_primal_step, stall_dual_step;
+  int64_t history_iterations[SOV_HISTORY_MAX];
+  double objective_history[SOV_HISTORY_MAX];
+  double gap_history[SOV_HISTORY_MAX];
+  double mu_history[SOV_HISTORY_MAX];
+  double primal_step_history[SOV_HISTORY_MAX];
+  double dual_step_history[SOV_HISTORY_MAX];
+  /* engine counters (no reference counterpart) */
+  int32_t fp64_fallbacks;      /* mixed precision: iterations refactored in FP64 */
+  int32_t pcg_iterations;      /* mixed precision: total PCG iterations */
+  int32_t warm_start_used;     /* 1 when the supplied warm start was kept */
+  int32_t reserved;
+} sov_diagnostics;
+
+/* Result of one solve (sovereign::SolverResult, types.hpp:117-155, in index form).
+ * primal / dual_col / dual_row / ipm_x / ipm_y / ipm_s are caller-allocated and may be NULL. */
+typedef struct sov_result {
+  int32_t status;              /* SOV_OPTIMAL ... */
+  int32_t iterations;
+  int32_t has_objective_value;
+  int32_t n_ipm, m_ipm;        /* internal standard-form sizes */
+  double objective_value;      /* on the original model, constant included */
+  double duality_gap;          /* |x's| / (1 + |c'x|) on the scaled problem */
+  double primal_residual;      /* ||b - Ax||_inf / max(1, ||b||_inf) */
+  double dual_residual;        /* ||c - A'y - s||_inf / max(1, ||c||_inf) */
+  double* primal;              /* n: x_j (= shift + col_scale * x_ipm) */
+  double* dual_col;            /* n: dual slack s_j / col_scale_j, key = variable name */
+  double* dual_row;            /* m: row_scale_i * y_i, key = "row_<i>" */
+  double* ipm_x;               /* n_ipm: final internal iterate (training data for warm starts) */
+  double* ipm_y;               /* m_ipm */
+  double* ipm_s;               /* n_ipm */
+  sov_diagnostics* diagnostics;
+  double solve_seconds;        /* device time of the iteration loop */
+  char message[512];
+} sov_result;
+
+void sov_default_lp_options(sov_options* opt);
+void sov_default_qp_options(sov_options* opt);
+
+/* Internal standard-form sizes of a model (LP: interior_point.cpp:250,312-314;
+ * QP: qp_interior_point.cpp:155,195-197). */
+int sov_ipm_dims(const sov_model* model, int32_t qp, int32_t* n_ipm, int32_t* m_ipm);
+
+/* One LP through the GPU IPM. Synchronous; host pointers are borrowed for the call. */
+int sov_lp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
+
+/* One convex QP through the GPU IPM (diagonal-plus-low-rank Hessians take the normal-equation
+ * path; general Hessians the dense quasi-definite KKT path). */
+int sov_qp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
+
+/* count independent LPs in one persistent batched launch (one CTA per LP, the whole IPM loop
+ * on the device). opt may be one shared option block (opt_stride 0) or an array. LPs whose
+ * normal matrix does not fit the batched kernel are solved one by one through sov_lp_solve. */
+int sov_lp_solve_batch(int32_t count, const sov_model* models, const sov_options* opt,
+                       int32_t opt_stride, sov_result* results);
+
+/* Device-resident batch: prepare once (host standard form + upload), solve many times (device
+ * only, stream-ordered), read back. Used to time the solver with inputs already in HBM. */
+typedef struct sov_batch sov_batch;
+int sov_batch_create(int32_t count, const sov_model* models, const sov_options* opt,
+                     sov_batch** out);
+int sov_batch_solve(sov_batch* batch, void* cuda_stream);
+int sov_batch_results(sov_batch* batch, sov_result* results);
+/* Kernel launches issued by the last sov_batch_solve, and the device time of its kernels. */
+int sov_batch_stats(const sov_batch* batch, int32_t* launches, double* kernel_ms,
+                    double* algorithmic_bytes, double* algorithmic_flops);
+void sov_batch_destroy(sov_batch* batch);
+
+/* Batched-kernel schedule chosen by the autotuner for a size bucket (threads per CTA, normal
+ * matrix precision). tuning_file may be NULL (in-memory only). */
+int sov_autotune(int32_t count, const sov_model* models, const sov_options* opt,
+                 const char* tuning_file, char* report, int32_t report_len);
+
+/* y = A x (transpose = 0) or y = A' x (transpose = 1) for a CSC matrix, FP64, on the GPU.
+ * Host buffers in and out. Mirrors spmv_csc_auto (gpu_spmv.cpp:70-102). */
+int sov_spmv_csc(int32_t nrows, int32_t ncols, const int32_t* col_ptr, const int32_t* row_idx,
+                 const double* values, const double* x, double* y, int32_t transpose);
+
+/* Factor M = A diag(d) A' + 1e-12 I (interior_point.cpp:74-101,163-180) on the GPU and solve
+ * M z = rhs for nrhs right-hand sides (column-major m x nrhs, overwritten by z). Dependent rows
+ * are dropped as the reference's tiny-pivot rule does (sparse_ldlt.cpp:165-173). */
+int sov_normal_factor_solve(int32_t m, int32_t n, const int32_t* col_ptr, const int32_t* row_idx,
+                            const double* values, const double* d, int32_t precision,
+                            int32_t factorization, double* rhs, int32_t nrhs,
+                            int32_t* dropped_pivots);
+
+/* Device name, SM count, memory; returns SOV_E_NO_DEVICE when no usable sm_100 GPU exists. */
+int sov_device_info(char* buf, int32_t len);
+
+/* Last error message of this thread. */
+const char* sov_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOV_IPM_H */
