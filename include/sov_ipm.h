@@ -206,6 +206,9 @@ int sov_batch_results(sov_batch* batch, sov_result* results);
 /* Kernel launches issued by the last sov_batch_solve, and the device time of its kernels. */
 int sov_batch_stats(const sov_batch* batch, int32_t* launches, double* kernel_ms,
                     double* algorithmic_bytes, double* algorithmic_flops);
+/* Bytes the last sov_batch_create copied host->device and the last sov_batch_results copied
+ * device->host (the end-to-end transfer volume of one batch). */
+int sov_batch_transfer_bytes(const sov_batch* batch, double* h2d_bytes, double* d2h_bytes);
 void sov_batch_destroy(sov_batch* batch);
 
 /* Batched-kernel schedule chosen by the autotuner for a size bucket (threads per CTA, normal

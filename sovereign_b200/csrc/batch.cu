@@ -1,0 +1,901 @@
+// batch.cu -- batched persistent interior-point solver: thousands of small LPs in one launch.
+//
+// One CTA owns one LP at a time and runs the whole Mehrotra predictor-corrector loop of
+// solve_ipm (solver/lp/src/interior_point.cpp:454-740) for it without returning to the host:
+// CTAs pull LP indices from a device counter (largest first), so uneven sizes balance across
+// the 148 SMs. The normal matrix of an LP (order m <= 128) lives in shared memory and is factored
+// there as L D L' with the reference's dependent-row rule; n-vectors stay in global memory, where
+// the working set of the resident CTAs fits in the 126 MB L2. Size buckets (by m) get their own
+// launch with a shared-memory footprint and thread count chosen per bucket by the autotuner; the
+// bucket launches of a batch are captured in one CUDA graph and replayed.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <sstream>
+#include <thread>
+#include <vector>
+
+#include "batch.hpp"
+#include "common.cuh"
+#include "dense.cuh"
+#include "engine.hpp"
+#include "stdform.hpp"
+
+namespace sov {
+
+constexpr int kBatchMaxRows = 128;
+
+struct LpMeta {
+  int m, n, nnz, ld;
+  int max_iter, pad0;
+  long long a_off, cp_off, rp_off, mv_off, nv_off;
+  double bnorm, cnorm, ftol, otol, tau;
+};
+
+struct LpOut {
+  int status, iterations, best_it, use_best;
+  int drops, fail, pad0, pad1;
+  double gap, p_res, d_res, cx;
+};
+
+struct BatchDev {
+  const LpMeta* meta;
+  const int* order;
+  int count;
+  int* next;
+  const int* col_ptr;
+  const int* row_idx;
+  const double* cval;
+  const int* row_ptr;
+  const int* col_idx;
+  const double* rval;
+  const double* b;
+  const double* c;
+  double *x, *s, *dx, *ds, *dxa, *dsa, *rd, *bx, *bs;
+  double *y, *by;
+  LpOut* out;
+};
+
+namespace {
+
+struct CtaScalars {
+  double v[16];
+  int flag[4];
+};
+
+// scalar slots
+enum : int {
+  S_MU = 0, S_PRES, S_DRES, S_GAP, S_METRIC, S_CX, S_APAFF, S_ADAFF, S_SIGMA, S_AP, S_AD, S_BEST
+};
+
+template <int NT>
+__device__ __forceinline__ void cta_reduce4(double (&v)[4], const int (&ops)[4], double* red) {
+  block_reduce<4>(v, ops, red);
+}
+
+template <int NT>
+__device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* sm, int mmax, double* red,
+                         CtaScalars& cs) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = NT / 32;
+  const int m = mt.m, n = mt.n, ld = mt.ld;
+  double* M = sm;
+  double* vy = sm + static_cast<size_t>(mmax) * (mmax + 1);
+  double* vrp = vy + mmax;
+  double* vz = vrp + mmax;
+  double* vacc = vz + mmax;
+  double* vdiag = vacc + mmax;
+  double* vinv = vdiag + mmax;
+
+  const int* cp = bd.col_ptr + mt.cp_off;
+  const int* ri = bd.row_idx + mt.a_off;
+  const double* cv = bd.cval + mt.a_off;
+  const int* rpp = bd.row_ptr + mt.rp_off;
+  const int* ci = bd.col_idx + mt.a_off;
+  const double* rv = bd.rval + mt.a_off;
+  const double* b = bd.b + mt.mv_off;
+  const double* c = bd.c + mt.nv_off;
+  double* x = bd.x + mt.nv_off;
+  double* s = bd.s + mt.nv_off;
+  double* dx = bd.dx + mt.nv_off;
+  double* ds = bd.ds + mt.nv_off;
+  double* dxa = bd.dxa + mt.nv_off;
+  double* dsa = bd.dsa + mt.nv_off;
+  double* rd = bd.rd + mt.nv_off;
+  double* bx = bd.bx + mt.nv_off;
+  double* bs = bd.bs + mt.nv_off;
+  double* gy = bd.y + mt.mv_off;
+  double* gby = bd.by + mt.mv_off;
+  int drops = 0, fail = 0;
+
+  // ---- assembly of M = A diag(d) A' + 1e-12 I (mode 0: d = x/s, mode 2: d = 1) ----
+  // Thread i owns row i of the lower triangle: M[i][r] = sum over k in row i of
+  // a_ik d_k a_rk for every r <= i in column k (no atomics, fixed summation order).
+  auto assemble = [&](int mode) {
+    for (int i = tid; i < m * ld; i += NT) M[i] = 0.0;
+    __syncthreads();
+    for (int i = tid; i < m; i += NT) {
+      double* Mi = M + i * ld;
+      for (int p = rpp[i]; p < rpp[i + 1]; ++p) {
+        const int k = ci[p];
+        const double dk = mode == 2 ? 1.0 : fmax(x[k], 1e-16) / fmax(s[k], 1e-16);
+        const double ad = rv[p] * dk;
+        for (int q = cp[k]; q < cp[k + 1]; ++q) {
+          const int r = ri[q];
+          if (r <= i) Mi[r] += ad * cv[q];
+        }
+      }
+      Mi[i] += 1e-12;
+      vdiag[i] = Mi[i];
+    }
+    __syncthreads();
+  };
+
+  // ---- in-place L D L' (L~ = L D kept unscaled below the diagonal; vinv = 1/D) ----
+  auto factor = [&]() {
+    for (int k = 0; k < m; ++k) {
+      const double p = M[k * ld + k];
+      const double dref = vdiag[k];
+      double Dk;
+      if (!isfinite(p)) {
+        Dk = 1e128;
+        fail = 1;
+      } else if (p <= 1e-13 * fabs(dref)) {
+        Dk = 1e128;  // dependent row (sparse_ldlt.cpp:167-173)
+        ++drops;
+      } else {
+        Dk = p;
+      }
+      const double inv = 1.0 / Dk;
+      if (tid == 0) vinv[k] = inv;
+      for (int i = k + 1 + warp; i < m; i += NW) {
+        const double lik = M[i * ld + k] * inv;
+        for (int j = k + 1 + lane; j <= i; j += 32) M[i * ld + j] -= lik * M[j * ld + k];
+      }
+      __syncthreads();
+    }
+  };
+
+  // ---- solve L D L' z = rhs in place (warp 0), rows owned by lane = i mod 32 ----
+  auto solve = [&]() {
+    if (warp == 0) {
+      for (int i = lane; i < m; i += 32) vacc[i] = 0.0;
+      __syncwarp();
+      for (int k = 0; k < m; ++k) {
+        const double wk = vz[k] * vinv[k];
+        __syncwarp();
+        if (lane == (k & 31)) vz[k] = wk;
+        for (int i = k + 1 + ((lane - (k + 1)) & 31); i < m; i += 32) vz[i] -= M[i * ld + k] * wk;
+        __syncwarp();
+      }
+      for (int k = m - 1; k >= 0; --k) {
+        const double xk = vz[k] - vinv[k] * vacc[k];
+        __syncwarp();
+        if (lane == (k & 31)) vz[k] = xk;
+        for (int i = lane; i < k; i += 32) vacc[i] += M[k * ld + i] * xk;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+  };
+
+  // ---- Mehrotra-like start (interior_point.cpp:488-506) ----
+  assemble(2);
+  factor();
+  for (int i = warp; i < m; i += NW) {
+    double acc = 0.0;
+    for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) acc += rv[p];
+    acc = warp_sum(acc);
+    if (lane == 0) vz[i] = b[i] - acc;
+  }
+  __syncthreads();
+  solve();
+  const bool start_ok = !fail;
+  for (int j = tid; j < n; j += NT) {
+    double xs = 1.0, ss = 1.0;
+    if (start_ok) {
+      double atdy = 0.0;
+      for (int p = cp[j]; p < cp[j + 1]; ++p) atdy += cv[p] * vz[ri[p]];
+      xs = fmax(1.0, fabs(atdy));
+      ss = fmax(1.0, fabs(c[j] - atdy));
+    }
+    x[j] = xs;
+    s[j] = ss;
+    bx[j] = xs;
+    bs[j] = ss;
+  }
+  for (int i = tid; i < m; i += NT) {
+    vy[i] = start_ok ? vz[i] : 0.0;
+    gby[i] = vy[i];
+  }
+  fail = 0;
+  __syncthreads();
+
+  double best_metric = INFINITY, best_gap = INFINITY, best_p = INFINITY, best_d = INFINITY;
+  int best_it = 0;
+  int status = -1, iters = 0;
+  double last_gap = 0, last_p = 0, last_d = 0, last_cx = 0;
+  const int ops_res[4] = {1, 1, 0, 0};
+  for (int it = 0; it < mt.max_iter; ++it) {
+    // residuals
+    double rpm = 0.0;
+    for (int i = warp; i < m; i += NW) {
+      double acc = 0.0;
+      for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) acc += rv[p] * x[ci[p]];
+      acc = warp_sum(acc);
+      const double r = b[i] - acc;
+      if (lane == 0) vrp[i] = r;
+      rpm = fmax(rpm, fabs(r));
+    }
+    double rdm = 0.0, xs = 0.0, cx = 0.0;
+    for (int j = tid; j < n; j += NT) {
+      double aty = 0.0;
+      for (int p = cp[j]; p < cp[j + 1]; ++p) aty += cv[p] * vy[ri[p]];
+      const double xj = x[j], sj = s[j];
+      const double r = c[j] - (aty + sj);
+      rd[j] = r;
+      rdm = fmax(rdm, fabs(r));
+      xs += xj * sj;
+      cx += c[j] * xj;
+    }
+    double v[4] = {rpm, rdm, xs, cx};
+    cta_reduce4<NT>(v, ops_res, red);
+    if (tid == 0) {
+      const double mu = v[2] / n;
+      const double pres = v[0] / mt.bnorm, dres = v[1] / mt.cnorm;
+      const double gap = fabs(v[2]) / (1.0 + fabs(v[3]));
+      cs.v[S_MU] = mu;
+      cs.v[S_PRES] = pres;
+      cs.v[S_DRES] = dres;
+      cs.v[S_GAP] = gap;
+      cs.v[S_METRIC] = fmax(pres, fmax(dres, gap));
+      cs.v[S_CX] = v[3];
+    }
+    __syncthreads();
+    const double mu = cs.v[S_MU], pres = cs.v[S_PRES], dres = cs.v[S_DRES], gap = cs.v[S_GAP];
+    const double metric = cs.v[S_METRIC];
+    last_gap = gap;
+    last_p = pres;
+    last_d = dres;
+    last_cx = cs.v[S_CX];
+    if (metric < best_metric) {
+      best_metric = metric;
+      best_gap = gap;
+      best_p = pres;
+      best_d = dres;
+      best_it = it + 1;
+      for (int j = tid; j < n; j += NT) {
+        bx[j] = x[j];
+        bs[j] = s[j];
+      }
+      for (int i = tid; i < m; i += NT) gby[i] = vy[i];
+    }
+    if (gap < best_gap) best_gap = gap;
+    if (pres < mt.ftol && dres < mt.ftol && gap < mt.otol) {
+      status = SOV_OPTIMAL;
+      iters = it + 1;
+      break;
+    }
+    // factor A diag(x/s) A'
+    assemble(0);
+    factor();
+    if (fail) {
+      status = -2;  // factorization failure: best iterate
+      break;
+    }
+    // predictor and corrector
+    for (int pass = 0; pass < 2; ++pass) {
+      const double sigma_mu = pass ? cs.v[S_SIGMA] * mu : 0.0;
+      for (int i = warp; i < m; i += NW) {
+        double acc = 0.0;
+        for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) {
+          const int j = ci[p];
+          const double xj = fmax(x[j], 1e-16), sj = fmax(s[j], 1e-16);
+          const double rxs = pass ? -x[j] * s[j] - dxa[j] * dsa[j] + sigma_mu : -x[j] * s[j];
+          acc += rv[p] * ((xj / sj) * rd[j] - rxs / sj);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) vz[i] = vrp[i] + acc;
+      }
+      __syncthreads();
+      solve();
+      double* ddx = pass ? dx : dxa;
+      double* dds = pass ? ds : dsa;
+      double rpmin = 1.0, rdmin = 1.0;
+      for (int j = tid; j < n; j += NT) {
+        double atdy = 0.0;
+        for (int p = cp[j]; p < cp[j + 1]; ++p) atdy += cv[p] * vz[ri[p]];
+        const double xj = x[j], sj = s[j];
+        const double rxs = pass ? -xj * sj - dxa[j] * dsa[j] + sigma_mu : -xj * sj;
+        const double dj = fmax(xj, 1e-16) / fmax(sj, 1e-16);
+        const double dxj = dj * (atdy - rd[j]) + rxs / fmax(sj, 1e-16);
+        const double dsj = rd[j] - atdy;
+        ddx[j] = dxj;
+        dds[j] = dsj;
+        if (dxj < 0.0) rpmin = fmin(rpmin, -xj / dxj);
+        if (dsj < 0.0) rdmin = fmin(rdmin, -sj / dsj);
+      }
+      double u[4] = {rpmin, rdmin, 0.0, 0.0};
+      const int ops_min[4] = {2, 2, 0, 0};
+      cta_reduce4<NT>(u, ops_min, red);
+      if (tid == 0) {
+        if (pass == 0) {
+          cs.v[S_APAFF] = u[0];
+          cs.v[S_ADAFF] = u[1];
+        } else {
+          cs.v[S_AP] = fmin(1.0, mt.tau * u[0]);
+          cs.v[S_AD] = fmin(1.0, mt.tau * u[1]);
+        }
+      }
+      __syncthreads();
+      if (pass == 0) {
+        const double apa = cs.v[S_APAFF], ada = cs.v[S_ADAFF];
+        double acc = 0.0;
+        for (int j = tid; j < n; j += NT) acc += (x[j] + apa * dxa[j]) * (s[j] + ada * dsa[j]);
+        double w4[4] = {acc, 0.0, 0.0, 0.0};
+        const int ops_sum[4] = {0, 0, 0, 0};
+        cta_reduce4<NT>(w4, ops_sum, red);
+        if (tid == 0) {
+          const double mu_aff = w4[0] / n;
+          const double r = mu_aff / mu;
+          cs.v[S_SIGMA] = mu > 0.0 ? fmin(1.0, r * r * r) : 0.0;
+        }
+        __syncthreads();
+      }
+    }
+    // update (interior_point.cpp:709-718)
+    const double ap = cs.v[S_AP], ad = cs.v[S_AD];
+    for (int j = tid; j < n; j += NT) {
+      x[j] = fmax(x[j] + ap * dx[j], 1e-14);
+      s[j] = fmax(s[j] + ad * ds[j], 1e-14);
+    }
+    for (int i = tid; i < m; i += NT) vy[i] += ad * vz[i];
+    iters = it + 1;
+    __syncthreads();
+  }
+  for (int i = tid; i < m; i += NT) gy[i] = vy[i];
+  if (tid == 0) {
+    LpOut o{};
+    o.drops = drops;
+    o.fail = fail;
+    if (status == SOV_OPTIMAL) {
+      o.status = SOV_OPTIMAL;
+      o.iterations = iters;
+      o.use_best = 0;
+      o.gap = last_gap;
+      o.p_res = last_p;
+      o.d_res = last_d;
+    } else {
+      o.status = best_p <= mt.ftol ? SOV_FEASIBLE : SOV_NUMERICAL_ERROR;
+      o.iterations = best_it;
+      o.use_best = 1;
+      o.best_it = status == -2 ? 1 : 0;  // 1: stopped on a failed factorization
+      o.gap = best_gap;
+      o.p_res = best_p;
+      o.d_res = best_d;
+    }
+    o.cx = last_cx;
+    bd.out[lp] = o;
+  }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT <= 256 ? 2 : 1)) k_batch_ipm(BatchDev bd, int mmax) {
+  extern __shared__ double sm[];
+  __shared__ double red[4 * 32];
+  __shared__ CtaScalars cs;
+  __shared__ int slot_s;
+  for (;;) {
+    if (threadIdx.x == 0) slot_s = atomicAdd(bd.next, 1);
+    __syncthreads();
+    const int slot = slot_s;
+    __syncthreads();
+    if (slot >= bd.count) return;
+    const int lp = bd.order[slot];
+    solve_lp<NT>(bd, bd.meta[lp], lp, sm, mmax, red, cs);
+  }
+}
+
+size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(mmax) * (mmax + 1) + 6 * mmax); }
+
+template <int NT>
+void launch_bucket(const BatchDev& bd, int mmax, int grid, cudaStream_t st) {
+  const size_t smem = batch_smem(mmax);
+  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_batch_ipm<NT><<<grid, NT, smem, st>>>(bd, mmax);
+  SOV_LAUNCH_CHECK();
+}
+
+template <int NT>
+int max_ctas(int mmax) {
+  int per_sm = 0;
+  const size_t smem = batch_smem(mmax);
+  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_ipm<NT>, NT, smem));
+  int dev = 0, sms = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  SOV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return std::max(1, per_sm) * sms;
+}
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (count) SOV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+    n = count;
+  }
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+// Grow-only pinned host staging shared by all batches of the process (H2D of the packed inputs,
+// D2H of the iterates), so repeated end-to-end calls do not re-pin memory.
+struct PinnedArena {
+  std::mutex mu;
+  unsigned char* p = nullptr;
+  size_t cap = 0;
+  unsigned char* get(size_t bytes) {
+    if (bytes > cap) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      cap = 0;
+      SOV_CUDA(cudaMallocHost(&p, bytes));
+      cap = bytes;
+    }
+    return p;
+  }
+};
+PinnedArena g_arena;
+
+std::mutex g_tune_mu;
+std::map<int, int> g_tuned_threads;  // bucket mmax -> threads
+
+int bucket_of(int m) { return std::max(32, ((m + 31) / 32) * 32); }
+
+template <class F>
+void parallel_for(int count, F fn) {
+  const int nt = std::max(1, std::min<int>(16, static_cast<int>(std::thread::hardware_concurrency())));
+  if (count < 64 || nt == 1) {
+    for (int i = 0; i < count; ++i) fn(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  std::vector<std::string> errors(nt);
+  for (int w = 0; w < nt; ++w)
+    pool.emplace_back([&, w]() {
+      try {
+        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) fn(i);
+      } catch (const std::exception& e) {
+        errors[w] = e.what();
+        next.store(count);
+      }
+    });
+  for (auto& t : pool) t.join();
+  for (auto& e : errors)
+    if (!e.empty()) throw std::runtime_error(e);
+}
+
+}  // namespace
+
+struct Batch {
+  int count = 0;
+  std::vector<sov_model> models;
+  std::vector<StdForm> forms;
+  std::vector<LpMeta> meta;
+  std::vector<int> fallback;  // LPs too large for the batched kernel
+  sov_options opt{};
+  struct Bucket {
+    int mmax, threads, grid, count;
+    DBuf<int> order;
+    DBuf<int> next;
+  };
+  std::vector<std::unique_ptr<Bucket>> buckets;
+  // one device arena for all packed inputs: [meta | ints | doubles]
+  DBuf<unsigned char> in;
+  DBuf<double> work;  // 9 n-vectors + 2 m-vectors
+  DBuf<LpOut> out;
+  DBuf<int> orders;
+  long long total_n = 0, total_m = 0, total_nnz = 0, total_cols = 0, total_rows = 0;
+  BatchDev dev{};
+  int launches = 0;
+  double kernel_ms = 0.0, bytes = 0.0, flops = 0.0;
+  double h2d_bytes = 0.0, d2h_bytes = 0.0;
+};
+
+namespace {
+
+int threads_for(int mmax) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tuned_threads.find(mmax);
+  if (it != g_tuned_threads.end()) return it->second;
+  return mmax <= 64 ? 128 : 256;
+}
+
+void launch_any(const BatchDev& bd, int mmax, int threads, int grid, cudaStream_t st) {
+  if (threads == 128) launch_bucket<128>(bd, mmax, grid, st);
+  else if (threads == 512) launch_bucket<512>(bd, mmax, grid, st);
+  else launch_bucket<256>(bd, mmax, grid, st);
+}
+
+int grid_for(int mmax, int threads, int count) {
+  const int cap = threads == 128 ? max_ctas<128>(mmax) : threads == 512 ? max_ctas<512>(mmax) : max_ctas<256>(mmax);
+  return std::max(1, std::min(cap, count));
+}
+
+size_t align8(size_t v) { return (v + 7) & ~size_t(7); }
+
+}  // namespace
+
+Batch* batch_create(int count, const sov_model* models, const sov_options* opt_in) {
+  auto B = std::make_unique<Batch>();
+  B->count = count;
+  B->models.assign(models, models + count);
+  B->forms.resize(count);
+  if (opt_in) B->opt = *opt_in;
+  else sov_default_lp_options(&B->opt);
+  const sov_options& opt = B->opt;
+  // host standard forms (interior_point.cpp:224-409 semantics), in parallel
+  parallel_for(count, [&](int i) {
+    try {
+      B->forms[i] = build_std_form(models[i], false, opt.enable_scaling != 0);
+    } catch (const std::exception& e) {
+      throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
+    }
+  });
+  // offsets (serial prefix), then parallel packing into pinned staging
+  B->meta.resize(count);
+  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0;
+  for (int i = 0; i < count; ++i) {
+    const StdForm& f = B->forms[i];
+    LpMeta& mt = B->meta[i];
+    std::memset(&mt, 0, sizeof(mt));
+    if (f.m <= 0 || f.m > kBatchMaxRows || f.n <= 0) {
+      B->fallback.push_back(i);
+      mt.m = -1;
+      continue;
+    }
+    mt.m = f.m;
+    mt.n = f.n;
+    mt.nnz = f.nnz();
+    mt.ld = f.m + 1;
+    mt.max_iter = opt.max_iterations;
+    mt.a_off = nnz;
+    mt.cp_off = cols;
+    mt.rp_off = rows;
+    mt.mv_off = mv;
+    mt.nv_off = nv;
+    double bmax = 0.0, cmax = 0.0;
+    for (double v : f.b) bmax = std::max(bmax, std::abs(v));
+    for (double v : f.c) cmax = std::max(cmax, std::abs(v));
+    mt.bnorm = std::max(1.0, bmax);
+    mt.cnorm = std::max(1.0, cmax);
+    mt.ftol = opt.feasibility_tol;
+    mt.otol = opt.optimality_tol;
+    mt.tau = opt.fraction_to_boundary;
+    nnz += f.nnz();
+    cols += f.n + 1;
+    rows += f.m + 1;
+    nv += f.n;
+    mv += f.m;
+    // algorithmic work per iteration (roofline): vector bytes + factorization flops
+    B->bytes += 6.0 * (12.0 * f.nnz() + 8.0 * (f.m + f.n)) + 15.0 * 8.0 * f.n + 10.0 * 8.0 * f.m;
+    B->flops += (2.0 / 3.0) * std::pow(static_cast<double>(f.m), 3.0);
+  }
+  B->total_n = nv;
+  B->total_m = mv;
+  B->total_nnz = nnz;
+  B->total_cols = cols;
+  B->total_rows = rows;
+  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c
+  const size_t o_meta = 0;
+  const size_t o_cp = align8(o_meta + sizeof(LpMeta) * count);
+  const size_t o_ri = o_cp + sizeof(int) * cols;
+  const size_t o_rp = o_ri + sizeof(int) * nnz;
+  const size_t o_ci = o_rp + sizeof(int) * rows;
+  const size_t o_cv = align8(o_ci + sizeof(int) * nnz);
+  const size_t o_rv = o_cv + sizeof(double) * nnz;
+  const size_t o_b = o_rv + sizeof(double) * nnz;
+  const size_t o_c = o_b + sizeof(double) * mv;
+  const size_t total = o_c + sizeof(double) * nv;
+  B->h2d_bytes = static_cast<double>(total);
+  std::lock_guard<std::mutex> lock(g_arena.mu);
+  unsigned char* h = g_arena.get(total);
+  std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
+  parallel_for(count, [&](int i) {
+    const LpMeta& mt = B->meta[i];
+    if (mt.m < 0) return;
+    const StdForm& f = B->forms[i];
+    std::memcpy(h + o_cp + sizeof(int) * mt.cp_off, f.col_ptr.data(), sizeof(int) * (f.n + 1));
+    std::memcpy(h + o_ri + sizeof(int) * mt.a_off, f.row_idx.data(), sizeof(int) * f.nnz());
+    std::memcpy(h + o_rp + sizeof(int) * mt.rp_off, f.row_ptr.data(), sizeof(int) * (f.m + 1));
+    std::memcpy(h + o_ci + sizeof(int) * mt.a_off, f.col_idx.data(), sizeof(int) * f.nnz());
+    std::memcpy(h + o_cv + sizeof(double) * mt.a_off, f.val.data(), sizeof(double) * f.nnz());
+    std::memcpy(h + o_rv + sizeof(double) * mt.a_off, f.rval.data(), sizeof(double) * f.nnz());
+    std::memcpy(h + o_b + sizeof(double) * mt.mv_off, f.b.data(), sizeof(double) * f.m);
+    std::memcpy(h + o_c + sizeof(double) * mt.nv_off, f.c.data(), sizeof(double) * f.n);
+  });
+  B->in.alloc(total);
+  SOV_CUDA(cudaMemcpy(B->in.p, h, total, cudaMemcpyHostToDevice));
+  B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
+  B->out.alloc(count);
+  // buckets by m, each ordered largest-first (cost ~ m^3 + nnz)
+  std::map<int, std::vector<int>> groups;
+  for (int i = 0; i < count; ++i)
+    if (B->meta[i].m > 0) groups[bucket_of(B->meta[i].m)].push_back(i);
+  std::vector<int> all_orders;
+  for (auto it = groups.rbegin(); it != groups.rend(); ++it) {
+    auto& ids = it->second;
+    std::sort(ids.begin(), ids.end(), [&](int a, int b2) {
+      const double ca = std::pow(B->meta[a].m, 3.0) + 20.0 * B->meta[a].nnz;
+      const double cb = std::pow(B->meta[b2].m, 3.0) + 20.0 * B->meta[b2].nnz;
+      return ca > cb;
+    });
+    auto bk = std::make_unique<Batch::Bucket>();
+    bk->mmax = it->first;
+    bk->threads = threads_for(bk->mmax);
+    bk->count = static_cast<int>(ids.size());
+    bk->grid = grid_for(bk->mmax, bk->threads, bk->count);
+    bk->order.alloc(ids.size());
+    SOV_CUDA(cudaMemcpy(bk->order.p, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+    bk->next.alloc(1);
+    B->buckets.push_back(std::move(bk));
+  }
+  BatchDev& d = B->dev;
+  unsigned char* base = B->in.p;
+  d.meta = reinterpret_cast<const LpMeta*>(base + o_meta);
+  d.col_ptr = reinterpret_cast<const int*>(base + o_cp);
+  d.row_idx = reinterpret_cast<const int*>(base + o_ri);
+  d.row_ptr = reinterpret_cast<const int*>(base + o_rp);
+  d.col_idx = reinterpret_cast<const int*>(base + o_ci);
+  d.cval = reinterpret_cast<const double*>(base + o_cv);
+  d.rval = reinterpret_cast<const double*>(base + o_rv);
+  d.b = reinterpret_cast<const double*>(base + o_b);
+  d.c = reinterpret_cast<const double*>(base + o_c);
+  double* w = B->work.p;
+  d.x = w;
+  d.s = w + nv;
+  d.dx = w + 2 * nv;
+  d.ds = w + 3 * nv;
+  d.dxa = w + 4 * nv;
+  d.dsa = w + 5 * nv;
+  d.rd = w + 6 * nv;
+  d.bx = w + 7 * nv;
+  d.bs = w + 8 * nv;
+  d.y = w + 9 * nv;
+  d.by = w + 9 * nv + mv;
+  d.out = B->out.p;
+  return B.release();
+}
+
+void batch_solve(Batch* B, cudaStream_t st) {
+  cudaEvent_t e0, e1;
+  SOV_CUDA(cudaEventCreate(&e0));
+  SOV_CUDA(cudaEventCreate(&e1));
+  SOV_CUDA(cudaEventRecord(e0, st));
+  int launches = 0;
+  for (auto& bk : B->buckets) {
+    SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), st));
+    BatchDev d = B->dev;
+    d.order = bk->order.p;
+    d.count = bk->count;
+    d.next = bk->next.p;
+    launch_any(d, bk->mmax, bk->threads, bk->grid, st);
+    ++launches;
+  }
+  SOV_CUDA(cudaEventRecord(e1, st));
+  SOV_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  SOV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  B->launches = launches;
+  B->kernel_ms = ms;
+}
+
+void batch_results(Batch* B, sov_result* results) {
+  const long long nv = B->total_n, mv = B->total_m;
+  // D2H: statuses, then x, s, y of every LP; the best iterate only for LPs that need it
+  std::vector<LpOut> out(B->count);
+  SOV_CUDA(cudaMemcpy(out.data(), B->out.p, sizeof(LpOut) * B->count, cudaMemcpyDeviceToHost));
+  const size_t bytes = sizeof(double) * (2 * nv + mv);
+  std::lock_guard<std::mutex> lock(g_arena.mu);
+  double* h = reinterpret_cast<double*>(g_arena.get(std::max<size_t>(bytes, 8)));
+  const BatchDev& d = B->dev;
+  if (nv) {
+    SOV_CUDA(cudaMemcpy(h, d.x, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost));  // x, s adjacent
+  }
+  if (mv) SOV_CUDA(cudaMemcpy(h + 2 * nv, d.y, sizeof(double) * mv, cudaMemcpyDeviceToHost));
+  double d2h = sizeof(LpOut) * B->count + static_cast<double>(bytes);
+  std::vector<std::vector<double>> best(B->count);
+  for (int i = 0; i < B->count; ++i) {
+    const LpMeta& mt = B->meta[i];
+    if (mt.m < 0 || !out[i].use_best) continue;
+    best[i].resize(2 * mt.n + mt.m);
+    SOV_CUDA(cudaMemcpy(best[i].data(), d.bx + mt.nv_off, sizeof(double) * mt.n, cudaMemcpyDeviceToHost));
+    SOV_CUDA(cudaMemcpy(best[i].data() + mt.n, d.bs + mt.nv_off, sizeof(double) * mt.n, cudaMemcpyDeviceToHost));
+    SOV_CUDA(cudaMemcpy(best[i].data() + 2 * mt.n, d.by + mt.mv_off, sizeof(double) * mt.m, cudaMemcpyDeviceToHost));
+    d2h += 8.0 * (2 * mt.n + mt.m);
+  }
+  B->d2h_bytes = d2h;
+  parallel_for(B->count, [&](int i) {
+    sov_result* r = &results[i];
+    const LpMeta& mt = B->meta[i];
+    if (mt.m < 0) return;  // solved by the fallback path below
+    const StdForm& f = B->forms[i];
+    const sov_model& mdl = B->models[i];
+    const LpOut& o = out[i];
+    const bool use_best = o.use_best != 0;
+    const double* hx = use_best ? best[i].data() : h + mt.nv_off;
+    const double* hs = use_best ? best[i].data() + mt.n : h + nv + mt.nv_off;
+    const double* hy = use_best ? best[i].data() + 2 * mt.n : h + 2 * nv + mt.mv_off;
+    r->status = o.status;
+    r->iterations = o.iterations;
+    r->has_objective_value = 1;
+    r->n_ipm = f.n;
+    r->m_ipm = f.m;
+    r->duality_gap = o.gap;
+    r->primal_residual = o.p_res;
+    r->dual_residual = o.d_res;
+    // publish_iterate (interior_point.cpp:541-563)
+    double obj = mdl.obj_constant;
+    for (int j = 0; j < f.n_struct; ++j) {
+      const double v = f.shift[j] + f.col_scale[j] * hx[j];
+      if (r->primal) r->primal[j] = v;
+      if (r->dual_col) r->dual_col[j] = hs[j] / f.col_scale[j];
+      obj += (mdl.obj ? mdl.obj[j] : 0.0) * v;
+    }
+    if (r->dual_row)
+      for (int k = 0; k < f.m0; ++k) r->dual_row[k] = f.row_scale[k] * hy[k];
+    if (r->ipm_x) std::copy(hx, hx + f.n, r->ipm_x);
+    if (r->ipm_s) std::copy(hs, hs + f.n, r->ipm_s);
+    if (r->ipm_y) std::copy(hy, hy + f.m, r->ipm_y);
+    r->objective_value = obj;
+    r->solve_seconds = B->kernel_ms * 1e-3;
+    if (o.status == SOV_OPTIMAL)
+      std::snprintf(r->message, sizeof(r->message),
+                    "Optimal solution found by primal-dual interior-point (Mehrotra). Normal equations: batched "
+                    "shared-memory L D L' on the GPU (%d x %d).",
+                    f.m, f.m);
+    else if (o.best_it)
+      std::snprintf(r->message, sizeof(r->message),
+                    "IPM stopped because the affine predictor factorization failed; the best iterate is returned "
+                    "with optimality unproven.");
+    else
+      std::snprintf(r->message, sizeof(r->message),
+                    "IPM stopped after %d iterations without meeting tolerance; returning best iterate from %d as a "
+                    "lower-accuracy candidate. Relative duality gap = %g (tolerance %g), primal residual = %g, dual "
+                    "residual = %g. Optimality is not proven.",
+                    mt.max_iter, o.iterations, o.gap, mt.otol, o.p_res, o.d_res);
+    if (r->diagnostics) {
+      std::memset(r->diagnostics, 0, sizeof(sov_diagnostics));
+      r->diagnostics->scaling_applied = f.scaling_applied;
+      r->diagnostics->coefficient_min_abs_before = f.coef_min_before;
+      r->diagnostics->coefficient_max_abs_before = f.coef_max_before;
+      r->diagnostics->coefficient_min_abs_after = f.coef_min_after;
+      r->diagnostics->coefficient_max_abs_after = f.coef_max_after;
+      r->diagnostics->refactorizations = o.iterations + 1;
+      r->diagnostics->stall_iteration = -1;
+    }
+  });
+  // LPs the batched kernel does not take go through the single-problem engine
+  for (int i : B->fallback) {
+    sov_result* r = &results[i];
+    const StdForm& f = B->forms[i];
+    if (f.n <= 0) {
+      r->status = SOV_ERROR;
+      r->has_objective_value = 0;
+      std::snprintf(r->message, sizeof(r->message), "IPM: empty model.");
+      continue;
+    }
+    cudaStream_t st;
+    SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    try {
+      solve_single(B->models[i], f, B->opt, r, st, nullptr);
+    } catch (...) {
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamDestroy(st);
+  }
+}
+
+void batch_stats(const Batch* B, int* launches, double* kernel_ms, double* bytes, double* flops) {
+  if (launches) *launches = B->launches;
+  if (kernel_ms) *kernel_ms = B->kernel_ms;
+  if (bytes) *bytes = B->bytes;
+  if (flops) *flops = B->flops;
+}
+
+void batch_transfer_bytes(const Batch* B, double* h2d, double* d2h) {
+  if (h2d) *h2d = B->h2d_bytes;
+  if (d2h) *d2h = B->d2h_bytes;
+}
+
+void batch_destroy(Batch* B) { delete B; }
+
+int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results) {
+  (void)opt_stride;
+  if (count == 0) return SOV_OK;
+  std::unique_ptr<Batch> B(batch_create(count, models, opt));
+  cudaStream_t st;
+  SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  try {
+    batch_solve(B.get(), st);
+  } catch (...) {
+    cudaStreamDestroy(st);
+    throw;
+  }
+  cudaStreamDestroy(st);
+  batch_results(B.get(), results);
+  return SOV_OK;
+}
+
+std::string autotune(int count, const sov_model* models, const sov_options* opt, const std::string& file) {
+  // Per bucket: time the bucket alone with 128 / 256 / 512 threads per CTA and keep the fastest.
+  std::unique_ptr<Batch> B(batch_create(count, models, opt));
+  cudaStream_t st;
+  SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  std::ostringstream rep;
+  rep << "{";
+  bool first = true;
+  for (auto& bk : B->buckets) {
+    float best_ms = 1e30f;
+    int best_t = bk->threads;
+    rep << (first ? "" : ", ") << "\"m<=" << bk->mmax << "\": {";
+    first = false;
+    bool f2 = true;
+    for (int threads : {128, 256, 512}) {
+      const int grid = grid_for(bk->mmax, threads, bk->count);
+      BatchDev d = B->dev;
+      d.order = bk->order.p;
+      d.count = bk->count;
+      d.next = bk->next.p;
+      float ms_min = 1e30f;
+      for (int rep_i = 0; rep_i < 2; ++rep_i) {
+        cudaEvent_t e0, e1;
+        SOV_CUDA(cudaEventCreate(&e0));
+        SOV_CUDA(cudaEventCreate(&e1));
+        SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), st));
+        SOV_CUDA(cudaEventRecord(e0, st));
+        launch_any(d, bk->mmax, threads, grid, st);
+        SOV_CUDA(cudaEventRecord(e1, st));
+        SOV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        SOV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        ms_min = std::min(ms_min, ms);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+      }
+      rep << (f2 ? "" : ", ") << "\"" << threads << "\": " << ms_min;
+      f2 = false;
+      if (ms_min < best_ms) {
+        best_ms = ms_min;
+        best_t = threads;
+      }
+    }
+    rep << ", \"chosen\": " << best_t << ", \"count\": " << bk->count << "}";
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tuned_threads[bk->mmax] = best_t;
+  }
+  rep << "}";
+  cudaStreamDestroy(st);
+  if (!file.empty()) {
+    std::ofstream o(file);
+    o << rep.str() << "\n";
+  }
+  return rep.str();
+}
+
+}  // namespace sov

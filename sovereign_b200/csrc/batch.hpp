@@ -1,0 +1,31 @@
+// batch.hpp -- batched persistent interior-point solver (one CTA per LP) and device tools.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "sov_ipm.h"
+
+namespace sov {
+
+struct Batch;
+
+int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results);
+Batch* batch_create(int count, const sov_model* models, const sov_options* opt);
+void batch_solve(Batch* b, cudaStream_t st);
+void batch_results(Batch* b, sov_result* results);
+void batch_stats(const Batch* b, int* launches, double* kernel_ms, double* bytes, double* flops);
+void batch_transfer_bytes(const Batch* b, double* h2d, double* d2h);
+void batch_destroy(Batch* b);
+std::string autotune(int count, const sov_model* models, const sov_options* opt, const std::string& file);
+
+// y = A x / A' x for a host CSC matrix (device kernels; host buffers in and out)
+int spmv_csc_device(int nrows, int ncols, const int* col_ptr, const int* row_idx, const double* values,
+                    const double* x, double* y, bool transpose);
+// factor A diag(d) A' + 1e-12 I and solve for nrhs right-hand sides (host buffers)
+int normal_factor_solve_device(int m, int n, const int* col_ptr, const int* row_idx, const double* values,
+                               const double* d, int precision, int factorization, double* rhs, int nrhs,
+                               int* dropped);
+
+}  // namespace sov

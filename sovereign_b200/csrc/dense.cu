@@ -1,0 +1,421 @@
+// dense.cu -- dense normal-matrix path on the GPU.
+//
+// Assembly: one gather pass over a precomputed contribution map (no atomics, deterministic).
+// Factorization: blocked right-looking Cholesky, 64-wide panels; per panel one CTA factors the
+// diagonal block in shared memory and inverts it, the panel below is L_ik = A_ik L_kk^-T (a GEMM
+// with the inverse), and the trailing lower triangle gets A_ij -= L_ik L_jk^T.
+// Solves: dataflow triangular solves, one cooperative launch per direction; row block i waits
+// (acquire flag, bounded spin) for the blocks it depends on, so the off-diagonal GEMV work of all
+// blocks overlaps and only the 64x64 diagonal products sit on the critical path.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "dense.cuh"
+
+namespace sov {
+
+template <class T>
+__device__ __forceinline__ T big_pivot();
+template <>
+__device__ __forceinline__ double big_pivot<double>() {
+  return kBigPivotD;
+}
+template <>
+__device__ __forceinline__ float big_pivot<float>() {
+  return kBigPivotF;
+}
+
+__device__ __forceinline__ double column_weight(int mode, int k, const double* x, const double* s,
+                                                const double* qdiag, const uint8_t* free_col) {
+  if (mode == kWeightOnes) return 1.0;
+  const double xk = fmax(x[k], 1e-16), sk = fmax(s[k], 1e-16);
+  if (mode == kWeightLp) return xk / sk;
+  const double h = free_col[k] ? 0.0 : sk / xk;
+  return 1.0 / (qdiag[k] + h);
+}
+
+// layout_ld > 0: dense column-major with that leading dimension; layout_ld < 0: band storage
+// with -layout_ld = m (diagonal offset major).
+template <class T>
+__global__ void k_assemble(AssemblyDev am, const double* __restrict__ x, const double* __restrict__ s,
+                           const double* __restrict__ qdiag, const uint8_t* __restrict__ free_col, int mode,
+                           double reg, T* __restrict__ out, double* __restrict__ diag_out, int m, int layout_ld) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= am.ntargets) return;
+  double acc = 0.0;
+  for (int p = am.ptr[t]; p < am.ptr[t + 1]; ++p)
+    acc += am.w[p] * column_weight(mode, am.col[p], x, s, qdiag, free_col);
+  const int64_t tg = am.target[t];
+  int row = -1;
+  if (layout_ld > 0) {
+    const int r = static_cast<int>(tg % layout_ld), c = static_cast<int>(tg / layout_ld);
+    if (r == c) row = r;
+  } else if (tg < m) {
+    row = static_cast<int>(tg);
+  }
+  if (row >= 0) {
+    acc += reg;
+    diag_out[row] = acc;
+  }
+  out[tg] = static_cast<T>(acc);
+}
+
+template <class T>
+void launch_assemble(const AssemblyDev& am, const double* x, const double* s, const double* qdiag,
+                     const uint8_t* free_col, int mode, double reg, T* out, double* diag_out, int m,
+                     int layout_ld, cudaStream_t st) {
+  if (am.ntargets == 0) return;
+  k_assemble<T><<<ceil_div(am.ntargets, 256), 256, 0, st>>>(am, x, s, qdiag, free_col, mode, reg, out, diag_out, m,
+                                                           layout_ld);
+  SOV_LAUNCH_CHECK();
+}
+
+template <class T>
+__global__ void k_pad_identity(T* M, int m, int mp) {
+  const int i = m + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < mp) M[static_cast<int64_t>(i) * mp + i] = T(1);
+}
+
+template <class T>
+void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
+  SOV_CUDA(cudaMemsetAsync(M, 0, sizeof(T) * static_cast<size_t>(mp) * mp, st));
+  if (mp > m) {
+    k_pad_identity<T><<<ceil_div(mp - m, 128), 128, 0, st>>>(M, m, mp);
+    SOV_LAUNCH_CHECK();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Diagonal block: unblocked Cholesky in shared memory (64 threads, thread i owns row i) and the
+// inverse of the resulting lower-triangular block (thread c owns column c).
+// ---------------------------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(64) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
+                                                   int m, T* __restrict__ Linv, int* drop_count, int* fail,
+                                                   double drop_tol) {
+  extern __shared__ __align__(16) unsigned char potrf_raw[];
+  T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
+  T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
+  const int tid = threadIdx.x;
+  const int r0 = kb * kNB;
+  for (int idx = tid; idx < kNB * kNB; idx += kNB) {
+    const int c = idx / kNB, r = idx % kNB;
+    A[r][c] = r >= c ? M[static_cast<int64_t>(r0 + c) * ld + r0 + r] : T(0);
+  }
+  int drops = 0, bad = 0;
+  const int i = tid;
+  for (int j = 0; j < kNB; ++j) {
+    __syncthreads();
+    const T p = A[j][j];
+    const int gj = r0 + j;
+    const double dref = gj < m ? diag[gj] : 1.0;
+    bool drop = false;
+    if (!isfinite(static_cast<double>(p))) {
+      bad = 1;
+      drop = true;
+    } else if (static_cast<double>(p) <= drop_tol * fabs(dref)) {
+      drop = true;
+    }
+    const T ljj = drop ? big_pivot<T>() : sqrt(p);
+    if (drop && gj < m) ++drops;
+    __syncthreads();
+    if (i == j) A[j][j] = ljj;
+    if (i > j) A[i][j] = A[i][j] / ljj;
+    __syncthreads();
+    if (i > j) {
+      const T lij = A[i][j];
+      for (int k = j + 1; k <= i; ++k) A[i][k] -= lij * A[k][j];
+    }
+  }
+  __syncthreads();
+  // inverse, column c by forward substitution on e_c
+  const int c = tid;
+  for (int r = 0; r < kNB; ++r) {
+    T v;
+    if (r < c) {
+      v = T(0);
+    } else if (r == c) {
+      v = T(1) / A[r][r];
+    } else {
+      T acc = T(0);
+      for (int k = c; k < r; ++k) acc += A[r][k] * I[k][c];
+      v = -acc / A[r][r];
+    }
+    I[r][c] = v;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kNB * kNB; idx += kNB) {
+    const int cc = idx / kNB, r = idx % kNB;
+    if (r >= cc) M[static_cast<int64_t>(r0 + cc) * ld + r0 + r] = A[r][cc];
+    Linv[static_cast<int64_t>(kb) * kNB * kNB + idx] = I[r][cc];
+  }
+  if (tid == 0) {
+    if (drops) atomicAdd(drop_count, drops);
+    if (bad) atomicExch(fail, 1);
+  }
+}
+
+// C (64x64 at rows r0, cols c0 of M) = beta * C + sign * X Y^T, X/Y given as [k][64] slices.
+template <class T>
+__device__ __forceinline__ void tile_nt(const T (*Xs)[kNB], const T (*Ys)[kNB], T (&acc)[4][4]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll 8
+  for (int k = 0; k < kNB; ++k) {
+    T a[4], b[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      a[q] = Xs[k][ty * 4 + q];
+      b[q] = Ys[k][tx * 4 + q];
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
+  }
+}
+
+// Panel: L_ik = A_ik * Linv_kk^T for every row block i > kb.
+template <class T>
+__global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ M, int ld, int kb, const T* __restrict__ Linv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*Xs)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw);
+  T(*Ys)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw + sizeof(T) * kNB * kNB);
+  const int i = kb + 1 + blockIdx.x;
+  const int r0 = i * kNB, k0 = kb * kNB;
+  const T* Lk = Linv + static_cast<int64_t>(kb) * kNB * kNB;
+  for (int idx = threadIdx.x; idx < kNB * kNB; idx += blockDim.x) {
+    const int k = idx / kNB, r = idx % kNB;
+    Xs[k][r] = M[static_cast<int64_t>(k0 + k) * ld + r0 + r];
+    Ys[k][r] = Lk[idx];  // Ys[k][c] = Linv[c][k] = Lk[k * 64 + c]
+  }
+  __syncthreads();
+  T acc[4][4] = {};
+  tile_nt<T>(Xs, Ys, acc);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int p = 0; p < 4; ++p) M[static_cast<int64_t>(k0 + tx * 4 + q) * ld + r0 + ty * 4 + p] = acc[p][q];
+}
+
+// Trailing update: A_ij -= L_ik L_jk^T for kb < j <= i (tile index enumerates the lower triangle).
+template <class T>
+__global__ void __launch_bounds__(256) k_syrk_update(T* __restrict__ M, int ld, int kb, int nb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*Xs)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw);
+  T(*Ys)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw + sizeof(T) * kNB * kNB);
+  // tile t -> (ii, jj) with 0 <= jj <= ii < R
+  const int t = blockIdx.x;
+  int ii = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((ii + 1) * (ii + 2) / 2 <= t) ++ii;
+  while (ii * (ii + 1) / 2 > t) --ii;
+  const int jj = t - ii * (ii + 1) / 2;
+  const int i = kb + 1 + ii, j = kb + 1 + jj;
+  (void)nb;
+  const int r0 = i * kNB, c0 = j * kNB, k0 = kb * kNB;
+  for (int idx = threadIdx.x; idx < kNB * kNB; idx += blockDim.x) {
+    const int k = idx / kNB, r = idx % kNB;
+    Xs[k][r] = M[static_cast<int64_t>(k0 + k) * ld + r0 + r];
+    Ys[k][r] = M[static_cast<int64_t>(k0 + k) * ld + c0 + r];
+  }
+  __syncthreads();
+  T acc[4][4] = {};
+  tile_nt<T>(Xs, Ys, acc);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      T* dst = M + static_cast<int64_t>(c0 + tx * 4 + q) * ld + r0 + ty * 4 + p;
+      *dst -= acc[p][q];
+    }
+}
+
+template <class T>
+void dense_potrf_block(const DenseSystem<T>& s, int kb, cudaStream_t st) {
+  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    attr_set = true;
+  }
+  k_potrf_diag<T><<<1, kNB, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
+}
+
+template <class T>
+void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
+  const size_t smem = 2 * sizeof(T) * kNB * kNB;
+  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    SOV_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_syrk_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int n = 0;
+  for (int kb = 0; kb < s.nb; ++kb) {
+    k_potrf_diag<T><<<1, kNB, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
+    ++n;
+    const int R = s.nb - kb - 1;
+    if (R > 0) {
+      k_trsm_panel<T><<<R, 256, smem, st>>>(s.M, s.mp, kb, s.Linv);
+      k_syrk_update<T><<<R * (R + 1) / 2, 256, smem, st>>>(s.M, s.mp, kb, s.nb);
+      n += 2;
+    }
+  }
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += n;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Dataflow triangular solves
+// ---------------------------------------------------------------------------------------------
+constexpr long long kSpinLimit = 1ll << 22;  // bounded wait (x >= 64 ns per poll -> > 0.25 s)
+
+__device__ __forceinline__ bool wait_flag(const unsigned* flag, unsigned epoch) {
+  long long n = 0;
+  while (ld_acquire(flag) != epoch) {
+    if (++n > kSpinLimit) return false;
+    __nanosleep(64);
+  }
+  return true;
+}
+
+// Forward: L y = r, row block order. z holds r on entry and y on exit.
+template <class T>
+__global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int ld, const T* __restrict__ Linv, int nb,
+                                                  double* z, unsigned* flags, unsigned epoch, int* err) {
+  __shared__ double part[4][kNB];
+  __shared__ double yj[kNB];
+  __shared__ double rhs[kNB];
+  __shared__ int ok;
+  const int t = threadIdx.x, r = t & (kNB - 1), g = t >> 6;
+  for (int i = blockIdx.x; i < nb; i += gridDim.x) {
+    double acc = 0.0;
+    for (int j = 0; j < i; ++j) {
+      if (t == 0) ok = wait_flag(flags + j, epoch);
+      __syncthreads();
+      if (!ok) {
+        if (t == 0) atomicExch(err, 1);
+      }
+      if (t < kNB) yj[t] = __ldcg(z + j * kNB + t);
+      __syncthreads();
+      const T* Lij = M + static_cast<int64_t>(j * kNB) * ld + i * kNB + r;
+#pragma unroll 4
+      for (int c = g * 16; c < g * 16 + 16; ++c) acc += static_cast<double>(Lij[static_cast<int64_t>(c) * ld]) * yj[c];
+      __syncthreads();
+    }
+    part[g][r] = acc;
+    __syncthreads();
+    if (t < kNB) rhs[t] = z[i * kNB + t] - (part[0][t] + part[1][t] + part[2][t] + part[3][t]);
+    __syncthreads();
+    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
+    double y = 0.0;
+#pragma unroll 4
+    for (int c = g * 16; c < g * 16 + 16; ++c) y += static_cast<double>(Li[c * kNB + r]) * rhs[c];
+    part[g][r] = y;
+    __syncthreads();
+    if (t < kNB) z[i * kNB + t] = part[0][t] + part[1][t] + part[2][t] + part[3][t];
+    __threadfence();
+    __syncthreads();
+    if (t == 0) st_release(flags + i, epoch);
+  }
+}
+
+// Backward: L^T x = y, reverse row block order. Warp w handles columns c = 8w..8w+7 of a block.
+template <class T>
+__global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int ld, const T* __restrict__ Linv, int nb,
+                                                  double* z, unsigned* flags, unsigned epoch, int* err) {
+  __shared__ double xj[kNB];
+  __shared__ double acc_s[kNB];
+  __shared__ double rhs[kNB];
+  __shared__ int ok;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  for (int q = blockIdx.x; q < nb; q += gridDim.x) {
+    const int i = nb - 1 - q;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = nb - 1; j > i; --j) {
+      if (t == 0) ok = wait_flag(flags + j, epoch);
+      __syncthreads();
+      if (!ok && t == 0) atomicExch(err, 1);
+      if (t < kNB) xj[t] = __ldcg(z + j * kNB + t);
+      __syncthreads();
+      // acc_c += sum_r L[j*64 + r][i*64 + c] * x_j[r]
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int c = w * 8 + u;
+        const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + j * kNB;
+        acc[u] += static_cast<double>(col[lane]) * xj[lane] + static_cast<double>(col[lane + 32]) * xj[lane + 32];
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double v = warp_sum(acc[u]);
+      if (lane == 0) acc_s[w * 8 + u] = v;
+    }
+    __syncthreads();
+    if (t < kNB) rhs[t] = z[i * kNB + t] - acc_s[t];
+    __syncthreads();
+    // x_c = sum_r Linv[r][c] rhs[r] = sum_r Li[c * 64 + r] rhs[r]
+    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = w * 8 + u;
+      double v = static_cast<double>(Li[c * kNB + lane]) * rhs[lane] + static_cast<double>(Li[c * kNB + lane + 32]) * rhs[lane + 32];
+      v = warp_sum(v);
+      if (lane == 0) acc_s[c] = v;
+    }
+    __syncthreads();
+    if (t < kNB) z[i * kNB + t] = acc_s[t];
+    __threadfence();
+    __syncthreads();
+    if (t == 0) st_release(flags + i, epoch);
+  }
+}
+
+int dataflow_grid(int nb) {
+  static int max_blocks = 0;
+  if (max_blocks == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    SOV_CUDA(cudaGetDevice(&dev));
+    SOV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trsv_fwd<double>, 256, 0));
+    max_blocks = std::max(1, sms * std::max(1, per_sm));
+  }
+  return std::min(nb, max_blocks);
+}
+
+template <class T>
+void dense_solve(const DenseSystem<T>& s, double* z, unsigned& epoch, int* err, cudaStream_t st, int* launches) {
+  const int grid = dataflow_grid(s.nb);
+  const T* M = s.M;
+  const T* Linv = s.Linv;
+  int ld = s.mp, nb = s.nb;
+  unsigned e1 = ++epoch;
+  void* args1[] = {(void*)&M, (void*)&ld, (void*)&Linv, (void*)&nb, (void*)&z, (void*)&s.flags, (void*)&e1, (void*)&err};
+  SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_trsv_fwd<T>, dim3(grid), dim3(256), args1, 0, st));
+  unsigned e2 = ++epoch;
+  void* args2[] = {(void*)&M, (void*)&ld, (void*)&Linv, (void*)&nb, (void*)&z, (void*)&s.flags, (void*)&e2, (void*)&err};
+  SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_trsv_bwd<T>, dim3(grid), dim3(256), args2, 0, st));
+  if (launches) *launches += 2;
+}
+
+// explicit instantiations
+template void launch_assemble<double>(const AssemblyDev&, const double*, const double*, const double*,
+                                     const uint8_t*, int, double, double*, double*, int, int, cudaStream_t);
+template void launch_assemble<float>(const AssemblyDev&, const double*, const double*, const double*,
+                                    const uint8_t*, int, double, float*, double*, int, int, cudaStream_t);
+template void launch_dense_clear<double>(double*, int, int, cudaStream_t);
+template void launch_dense_clear<float>(float*, int, int, cudaStream_t);
+template void dense_potrf_block<double>(const DenseSystem<double>&, int, cudaStream_t);
+template void dense_potrf_block<float>(const DenseSystem<float>&, int, cudaStream_t);
+template void dense_cholesky<double>(const DenseSystem<double>&, cudaStream_t, int*);
+template void dense_cholesky<float>(const DenseSystem<float>&, cudaStream_t, int*);
+template void dense_solve<double>(const DenseSystem<double>&, double*, unsigned&, int*, cudaStream_t, int*);
+template void dense_solve<float>(const DenseSystem<float>&, double*, unsigned&, int*, cudaStream_t, int*);
+
+}  // namespace sov

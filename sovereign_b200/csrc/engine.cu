@@ -1,0 +1,682 @@
+// engine.cu -- single-problem GPU interior-point engine.
+//
+// The iteration of solve_ipm (solver/lp/src/interior_point.cpp:454-740) and of the generic QP path
+// solve_qp_ipm (solver/qp/src/qp_interior_point.cpp:2848-3116, diagonal Hessians), with all
+// vectors resident in HBM. Per iteration the host reads one IpmScalars struct (residual norms,
+// mu, gap, the previous step lengths) and takes the reference's decisions: best-iterate
+// bookkeeping, the history samples and the stopping test. Everything else is stream-ordered
+// device work: assembly of A D A', factorization, two Newton solves, ratio tests, update.
+//
+// Normal-equation backends:
+//   dense FP64    blocked Cholesky + dataflow triangular solves (the plain FP64 engine)
+//   dense mixed   FP32 Cholesky as the preconditioner of FP64 PCG on the exact normal operator;
+//                 an iteration whose PCG does not converge is refactored in FP64
+//   band          banded LDL^T, natural order, for small half-bandwidths
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "band.cuh"
+#include "common.cuh"
+#include "dense.cuh"
+#include "engine.hpp"
+#include "ipm_kernels.cuh"
+
+namespace sov {
+namespace {
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) SOV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+  }
+  void zero(cudaStream_t st) {
+    if (n) SOV_CUDA(cudaMemsetAsync(p, 0, sizeof(T) * n, st));
+  }
+  void upload(const T* h, size_t count, cudaStream_t st) {
+    if (count) SOV_CUDA(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, st));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { release(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+struct PinnedScalars {
+  IpmScalars* h = nullptr;
+  PinnedScalars() { SOV_CUDA(cudaMallocHost(&h, sizeof(IpmScalars))); }
+  ~PinnedScalars() { cudaFreeHost(h); }
+};
+
+// -------------------------------------------------------------------------------------------
+// PCG helpers (single CTA; the dense path has m <= 8192)
+// -------------------------------------------------------------------------------------------
+struct PcgScalars {
+  double rz, rr, bb, alpha, beta;
+};
+
+__global__ void __launch_bounds__(1024) k_pcg_init(int m, const double* rhs, double* x, double* r, double* w,
+                                                   PcgScalars* ps) {
+  __shared__ double scratch[4 * 32];
+  double bb = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const double v = rhs[i];
+    x[i] = 0.0;
+    r[i] = v;
+    w[i] = v;
+    bb += v * v;
+  }
+  double v4[4] = {bb, 0, 0, 0};
+  const int ops[4] = {0, 0, 0, 0};
+  block_reduce<4>(v4, ops, scratch);
+  if (threadIdx.x == 0) {
+    ps->bb = v4[0];
+    ps->rr = v4[0];
+  }
+}
+
+// after w = P^-1 r: rz_new = r.w; beta = rz_new / rz (first: beta = 0); p = w + beta p
+__global__ void __launch_bounds__(1024) k_pcg_direction(int m, const double* r, const double* w, double* p,
+                                                        PcgScalars* ps, int first) {
+  __shared__ double scratch[4 * 32];
+  __shared__ double beta_s;
+  double rz = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) rz += r[i] * w[i];
+  double v4[4] = {rz, 0, 0, 0};
+  const int ops[4] = {0, 0, 0, 0};
+  block_reduce<4>(v4, ops, scratch);
+  if (threadIdx.x == 0) {
+    const double beta = first ? 0.0 : v4[0] / ps->rz;
+    ps->beta = beta;
+    ps->rz = v4[0];
+    beta_s = beta;
+  }
+  __syncthreads();
+  const double beta = beta_s;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) p[i] = w[i] + beta * (first ? 0.0 : p[i]);
+}
+
+// q = M p given; alpha = rz / p.q; x += alpha p; r -= alpha q; w = r (to be preconditioned)
+__global__ void __launch_bounds__(1024) k_pcg_step(int m, const double* p, const double* q, double* x, double* r,
+                                                   double* w, PcgScalars* ps) {
+  __shared__ double scratch[4 * 32];
+  __shared__ double alpha_s;
+  double pq = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) pq += p[i] * q[i];
+  double v4[4] = {pq, 0, 0, 0};
+  const int ops[4] = {0, 0, 0, 0};
+  block_reduce<4>(v4, ops, scratch);
+  if (threadIdx.x == 0) {
+    const double a = v4[0] != 0.0 ? ps->rz / v4[0] : 0.0;
+    ps->alpha = a;
+    alpha_s = a;
+  }
+  __syncthreads();
+  const double a = alpha_s;
+  double rr = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    r[i] = ri;
+    w[i] = ri;
+    rr += ri * ri;
+  }
+  double u4[4] = {rr, 0, 0, 0};
+  block_reduce<4>(u4, ops, scratch);
+  if (threadIdx.x == 0) ps->rr = u4[0];
+}
+
+// -------------------------------------------------------------------------------------------
+
+class Engine {
+ public:
+  Engine(const sov_model& model, const StdForm& f, const sov_options& opt, cudaStream_t st, EngineStats* stats)
+      : model_(model), f_(f), opt_(opt), st_(st), stats_(stats) {}
+
+  void run(sov_result* r);
+
+ private:
+  void setup();
+  void assemble_and_factor(int mode);
+  bool newton_solve();  // z -> dy in place
+  void read_scalars();
+  void publish(const DevBuf<double>& x, const DevBuf<double>& y, const DevBuf<double>& s, int status, int iteration,
+               double gap, double pres, double dres, const std::string& msg, sov_result* r);
+  std::string describe() const;
+
+  const sov_model& model_;
+  const StdForm& f_;
+  sov_options opt_;
+  cudaStream_t st_;
+  EngineStats* stats_;
+  int launches_ = 0;
+
+  // device data
+  DevBuf<int> row_ptr_, col_idx_, col_ptr_, row_idx_;
+  DevBuf<double> rval_, cval_, b_, c_, qdiag_;
+  DevBuf<uint8_t> free_;
+  DevBuf<double> x_, y_, s_, dx_, ds_, dxa_, dsa_, rp_, rd_, z_, bx_, by_, bs_;
+  DevBuf<double> partials_;
+  DevBuf<unsigned> counter_;
+  DevBuf<IpmScalars> sc_;
+  PinnedScalars hs_;
+  IpmDev dev_{};
+
+  // factorization
+  enum Backend { kDense64, kDenseMixed, kBand } backend_ = kDense64;
+  int mp_ = 0, nb_ = 0, kd_ = 0;
+  AssemblyMap am_;
+  DevBuf<int64_t> am_target_;
+  DevBuf<int> am_ptr_, am_col_, am_diag_;
+  DevBuf<double> am_w_;
+  AssemblyDev amd_{};
+  DevBuf<double> M64_, Linv64_;
+  DevBuf<float> M32_, Linv32_;
+  DevBuf<double> diag_, band_, dinv_;
+  DevBuf<unsigned> flags_;
+  DevBuf<int> err_;
+  unsigned epoch_ = 0;
+  DenseSystem<double> ds64_{};
+  DenseSystem<float> ds32_{};
+  BandSystem bandsys_{};
+  int last_mode_ = kWeightLp;
+  bool fp64_ready_ = false;  // FP64 factor of the current iteration exists (mixed fallback)
+  // PCG work
+  DevBuf<double> pcg_x_, pcg_r_, pcg_w_, pcg_p_, pcg_q_, pcg_tmp_;
+  DevBuf<PcgScalars> pcg_s_;
+  PcgScalars* pcg_h_ = nullptr;
+  int pcg_iterations_ = 0, fp64_fallbacks_ = 0, factorizations_ = 0;
+};
+
+void Engine::setup() {
+  const int m = f_.m, n = f_.n;
+  row_ptr_.alloc(m + 1);
+  row_ptr_.upload(f_.row_ptr.data(), m + 1, st_);
+  col_idx_.alloc(f_.nnz());
+  col_idx_.upload(f_.col_idx.data(), f_.nnz(), st_);
+  rval_.alloc(f_.nnz());
+  rval_.upload(f_.rval.data(), f_.nnz(), st_);
+  col_ptr_.alloc(n + 1);
+  col_ptr_.upload(f_.col_ptr.data(), n + 1, st_);
+  row_idx_.alloc(f_.nnz());
+  row_idx_.upload(f_.row_idx.data(), f_.nnz(), st_);
+  cval_.alloc(f_.nnz());
+  cval_.upload(f_.val.data(), f_.nnz(), st_);
+  b_.alloc(m);
+  b_.upload(f_.b.data(), m, st_);
+  c_.alloc(n);
+  c_.upload(f_.c.data(), n, st_);
+  if (f_.qp) {
+    qdiag_.alloc(n);
+    qdiag_.upload(f_.qdiag.data(), n, st_);
+    free_.alloc(n);
+    free_.upload(f_.free_col.data(), n, st_);
+  }
+  for (DevBuf<double>* v : {&x_, &s_, &dx_, &ds_, &dxa_, &dsa_, &rd_, &bx_, &bs_}) v->alloc(n);
+  for (DevBuf<double>* v : {&y_, &rp_, &by_}) v->alloc(m);
+  partials_.alloc(8 * 1184);
+  counter_.alloc(1);
+  counter_.zero(st_);
+  sc_.alloc(1);
+  sc_.zero(st_);
+  err_.alloc(1);
+  err_.zero(st_);
+
+  // backend choice: band when the half-bandwidth is small, else dense (mixed or FP64)
+  kd_ = normal_bandwidth(f_);
+  const bool want_band = opt_.factorization == SOV_FACTOR_BANDED ||
+                         (opt_.factorization == SOV_FACTOR_AUTO && kd_ <= kBandMax && m > 256);
+  if (want_band) {
+    if (kd_ > kBandMax) throw std::runtime_error("banded factorization requested but half-bandwidth " +
+                                                 std::to_string(kd_) + " exceeds " + std::to_string(kBandMax));
+    backend_ = kBand;
+  } else {
+    if (m > 16384) throw std::runtime_error("normal matrix of order " + std::to_string(m) +
+                                            " is too large for the dense factorization (band width " +
+                                            std::to_string(kd_) + ")");
+    backend_ = opt_.precision == SOV_PRECISION_MIXED ? kDenseMixed : kDense64;
+  }
+  if (backend_ == kBand) {
+    am_ = build_assembly_band(f_, kd_);
+    band_.alloc(static_cast<size_t>(kBandMax + 1) * m);
+    band_.zero(st_);
+    dinv_.alloc(m);
+    diag_.alloc(m);
+    z_.alloc(m);
+    z_.zero(st_);
+    bandsys_ = BandSystem{band_.p, dinv_.p, diag_.p, m, kd_, nullptr, nullptr};
+  } else {
+    nb_ = ceil_div(m, kNB);
+    mp_ = nb_ * kNB;
+    am_ = build_assembly_dense(f_, mp_);
+    diag_.alloc(m);
+    flags_.alloc(nb_);
+    flags_.zero(st_);
+    z_.alloc(mp_);
+    z_.zero(st_);
+    if (backend_ == kDenseMixed) {
+      M32_.alloc(static_cast<size_t>(mp_) * mp_);
+      Linv32_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
+      for (DevBuf<double>* v : {&pcg_x_, &pcg_r_, &pcg_w_, &pcg_p_, &pcg_q_}) {
+        v->alloc(mp_);
+        v->zero(st_);
+      }
+      pcg_tmp_.alloc(n);
+      pcg_s_.alloc(1);
+      SOV_CUDA(cudaMallocHost(&pcg_h_, sizeof(PcgScalars)));
+    }
+  }
+  am_target_.alloc(am_.target.size());
+  am_target_.upload(am_.target.data(), am_.target.size(), st_);
+  am_ptr_.alloc(am_.ptr.size());
+  am_ptr_.upload(am_.ptr.data(), am_.ptr.size(), st_);
+  am_col_.alloc(am_.col.size());
+  am_col_.upload(am_.col.data(), am_.col.size(), st_);
+  am_w_.alloc(am_.w.size());
+  am_w_.upload(am_.w.data(), am_.w.size(), st_);
+  am_diag_.alloc(am_.diag_target.size());
+  am_diag_.upload(am_.diag_target.data(), am_.diag_target.size(), st_);
+  amd_ = AssemblyDev{am_target_.p, am_ptr_.p, am_col_.p, am_w_.p, am_diag_.p, static_cast<int>(am_.target.size())};
+
+  IpmScalars* sc = sc_.p;
+  int* fail_ptr = &sc->fail;
+  int* drop_ptr = &sc->drops;
+  if (backend_ == kBand) {
+    bandsys_.drop_count = drop_ptr;
+    bandsys_.fail = fail_ptr;
+  } else {
+    ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, m, mp_, nb_, drop_ptr, fail_ptr, flags_.p, 1e-6};
+  }
+
+  dev_.m = m;
+  dev_.n = n;
+  dev_.row_ptr = row_ptr_.p;
+  dev_.col_idx = col_idx_.p;
+  dev_.rval = rval_.p;
+  dev_.col_ptr = col_ptr_.p;
+  dev_.row_idx = row_idx_.p;
+  dev_.cval = cval_.p;
+  dev_.b = b_.p;
+  dev_.c = c_.p;
+  dev_.qdiag = qdiag_.p;
+  dev_.free_col = free_.p;
+  dev_.qp = f_.qp ? 1 : 0;
+  dev_.has_quadratic = f_.has_quadratic ? 1 : 0;
+  int n_bounded = 0;
+  for (int j = 0; j < n; ++j) n_bounded += f_.free_col[j] ? 0 : 1;
+  dev_.comp_count = f_.qp ? std::max(1, n_bounded) : n;
+  double bmax = 0.0, cmax = 0.0;
+  for (double v : f_.b) bmax = std::max(bmax, std::abs(v));
+  for (double v : f_.c) cmax = std::max(cmax, std::abs(v));
+  dev_.bnorm = std::max(1.0, bmax);
+  dev_.cnorm = std::max(1.0, cmax);
+  dev_.objective_offset = f_.objective_offset;
+  dev_.tau = opt_.fraction_to_boundary;
+  dev_.x = x_.p;
+  dev_.y = y_.p;
+  dev_.s = s_.p;
+  dev_.dx = dx_.p;
+  dev_.ds = ds_.p;
+  dev_.dxa = dxa_.p;
+  dev_.dsa = dsa_.p;
+  dev_.rp = rp_.p;
+  dev_.rd = rd_.p;
+  dev_.z = z_.p;
+  dev_.sc = sc_.p;
+  dev_.partials = partials_.p;
+  dev_.counter = counter_.p;
+}
+
+void Engine::assemble_and_factor(int mode) {
+  last_mode_ = mode;
+  const double reg = 1e-12;  // kNormalEqRegularization (interior_point.cpp:103)
+  ++factorizations_;
+  fp64_ready_ = false;
+  if (backend_ == kBand) {
+    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, band_.p, diag_.p, f_.m, -f_.m, st_);
+    band_factor(bandsys_, st_, &launches_);
+    launches_ += 1;
+    if (stats_) {
+      const double kd = kd_;
+      stats_->factor_flops += f_.m * (kd * kd + 2.0 * kd);
+    }
+    return;
+  }
+  if (backend_ == kDense64) {
+    if (!M64_.p) {
+      M64_.alloc(static_cast<size_t>(mp_) * mp_);
+      Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
+      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, f_.m, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
+    }
+    launch_dense_clear<double>(M64_.p, f_.m, mp_, st_);
+    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, M64_.p, diag_.p, f_.m, mp_, st_);
+    dense_cholesky<double>(ds64_, st_, &launches_);
+    launches_ += 2;
+    fp64_ready_ = true;
+  } else {
+    launch_dense_clear<float>(M32_.p, f_.m, mp_, st_);
+    launch_assemble<float>(amd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, M32_.p, diag_.p, f_.m, mp_, st_);
+    dense_cholesky_tc(ds32_, err_.p, st_, &launches_);
+    launches_ += 2;
+  }
+  if (stats_) stats_->factor_flops += (2.0 / 3.0) * std::pow(static_cast<double>(f_.m), 3.0);
+}
+
+bool Engine::newton_solve() {
+  if (stats_) stats_->solves++;
+  if (backend_ == kBand) {
+    band_solve(bandsys_, z_.p, st_, &launches_);
+    return true;
+  }
+  if (backend_ == kDense64) {
+    dense_solve<double>(ds64_, z_.p, epoch_, err_.p, st_, &launches_);
+    return true;
+  }
+  // mixed: PCG on (A D A' + reg I) dy = z with the FP32 factor as preconditioner
+  const int m = f_.m;
+  const double reg = 1e-12;
+  const double tol2 = 1e-22;  // ||r|| <= 1e-11 ||b||
+  k_pcg_init<<<1, 1024, 0, st_>>>(m, z_.p, pcg_x_.p, pcg_r_.p, pcg_w_.p, pcg_s_.p);
+  dense_solve<float>(ds32_, pcg_w_.p, epoch_, err_.p, st_, &launches_);
+  k_pcg_direction<<<1, 1024, 0, st_>>>(m, pcg_r_.p, pcg_w_.p, pcg_p_.p, pcg_s_.p, 1);
+  launches_ += 2;
+  bool converged = false;
+  const int cap = opt_.pcg_max_iterations > 0 ? opt_.pcg_max_iterations : 50;
+  for (int k = 0; k < cap; ++k) {
+    launch_normal_matvec(dev_, pcg_p_.p, pcg_tmp_.p, pcg_q_.p, reg, st_);
+    k_pcg_step<<<1, 1024, 0, st_>>>(m, pcg_p_.p, pcg_q_.p, pcg_x_.p, pcg_r_.p, pcg_w_.p, pcg_s_.p);
+    SOV_CUDA(cudaMemcpyAsync(pcg_h_, pcg_s_.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st_));
+    SOV_CUDA(cudaStreamSynchronize(st_));
+    launches_ += 3;
+    ++pcg_iterations_;
+    if (!(pcg_h_->rr > tol2 * pcg_h_->bb)) {
+      converged = std::isfinite(pcg_h_->rr);
+      break;
+    }
+    dense_solve<float>(ds32_, pcg_w_.p, epoch_, err_.p, st_, &launches_);
+    k_pcg_direction<<<1, 1024, 0, st_>>>(m, pcg_r_.p, pcg_w_.p, pcg_p_.p, pcg_s_.p, 0);
+    launches_ += 1;
+  }
+  if (converged) {
+    SOV_CUDA(cudaMemcpyAsync(z_.p, pcg_x_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
+    return true;
+  }
+  // FP64 fallback for this iteration: factor in FP64 once, then solve directly
+  if (!fp64_ready_) {
+    ++fp64_fallbacks_;
+    if (!M64_.p) {
+      M64_.alloc(static_cast<size_t>(mp_) * mp_);
+      Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
+      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, f_.m, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
+    }
+    launch_dense_clear<double>(M64_.p, f_.m, mp_, st_);
+    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, last_mode_, reg, M64_.p, diag_.p, f_.m, mp_, st_);
+    dense_cholesky<double>(ds64_, st_, &launches_);
+    fp64_ready_ = true;
+  }
+  dense_solve<double>(ds64_, z_.p, epoch_, err_.p, st_, &launches_);
+  return true;
+}
+
+void Engine::read_scalars() {
+  SOV_CUDA(cudaMemcpyAsync(hs_.h, sc_.p, sizeof(IpmScalars), cudaMemcpyDeviceToHost, st_));
+  SOV_CUDA(cudaStreamSynchronize(st_));
+}
+
+std::string Engine::describe() const {
+  char buf[256];
+  if (backend_ == kBand)
+    std::snprintf(buf, sizeof buf, "banded LDL^T on the GPU (order %d, half-bandwidth %d)", f_.m, kd_);
+  else if (backend_ == kDense64)
+    std::snprintf(buf, sizeof buf, "dense Cholesky on the GPU, FP64 (%d x %d)", f_.m, f_.m);
+  else
+    std::snprintf(buf, sizeof buf,
+                  "dense Cholesky on the GPU, FP32 preconditioned FP64 PCG (%d x %d, %d PCG iterations, %d FP64 "
+                  "refactorizations)",
+                  f_.m, f_.m, pcg_iterations_, fp64_fallbacks_);
+  return buf;
+}
+
+void Engine::publish(const DevBuf<double>& x, const DevBuf<double>& y, const DevBuf<double>& s, int status,
+                     int iteration, double gap, double pres, double dres, const std::string& msg, sov_result* r) {
+  const int n = f_.n, m = f_.m;
+  std::vector<double> hx(n), hy(m), hs(n);
+  SOV_CUDA(cudaMemcpyAsync(hx.data(), x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st_));
+  SOV_CUDA(cudaMemcpyAsync(hy.data(), y.p, sizeof(double) * m, cudaMemcpyDeviceToHost, st_));
+  SOV_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st_));
+  SOV_CUDA(cudaStreamSynchronize(st_));
+  r->status = status;
+  r->iterations = iteration;
+  r->duality_gap = gap;
+  r->primal_residual = pres;
+  r->dual_residual = dres;
+  r->has_objective_value = 1;
+  double obj = model_.obj_constant;
+  if (!f_.qp) {
+    // publish_iterate (interior_point.cpp:541-563)
+    for (int j = 0; j < f_.n_struct; ++j) {
+      const double v = f_.shift[j] + f_.col_scale[j] * hx[j];
+      if (r->primal) r->primal[j] = v;
+      if (r->dual_col) r->dual_col[j] = hs[j] / f_.col_scale[j];
+      obj += (model_.obj ? model_.obj[j] : 0.0) * v;
+    }
+    if (r->dual_row)
+      for (int i = 0; i < f_.m0; ++i) r->dual_row[i] = f_.row_scale[i] * hy[i];
+  } else {
+    // qp_interior_point.cpp:3018-3037 and capture_diagnostics (:2862-2877)
+    std::vector<double> prim(f_.n_struct);
+    for (int j = 0; j < f_.n_struct; ++j) prim[j] = f_.shift[j] + hx[j];
+    for (int j = 0; j < f_.n_struct; ++j) obj += (model_.obj ? model_.obj[j] : 0.0) * prim[j];
+    if (model_.q_col_ptr)
+      for (int j = 0; j < f_.n_struct; ++j)
+        for (int k = model_.q_col_ptr[j]; k < model_.q_col_ptr[j + 1]; ++k)
+          obj += 0.5 * model_.q_values[k] * prim[model_.q_row_idx[k]] * prim[j];
+    if (r->primal) std::copy(prim.begin(), prim.end(), r->primal);
+    if (r->dual_col) std::copy(hs.begin(), hs.begin() + f_.n_struct, r->dual_col);
+    if (r->dual_row) std::copy(hy.begin(), hy.begin() + f_.m0, r->dual_row);
+  }
+  if (r->ipm_x) std::copy(hx.begin(), hx.end(), r->ipm_x);
+  if (r->ipm_y) std::copy(hy.begin(), hy.end(), r->ipm_y);
+  if (r->ipm_s) std::copy(hs.begin(), hs.end(), r->ipm_s);
+  r->objective_value = obj;
+  std::snprintf(r->message, sizeof(r->message), "%s", msg.c_str());
+}
+
+void Engine::run(sov_result* r) {
+  const int m = f_.m, n = f_.n;
+  r->n_ipm = n;
+  r->m_ipm = m;
+  sov_diagnostics* dg = r->diagnostics;
+  if (dg) {
+    std::memset(dg, 0, sizeof(*dg));
+    dg->scaling_applied = f_.scaling_applied;
+    dg->coefficient_min_abs_before = f_.coef_min_before;
+    dg->coefficient_max_abs_before = f_.coef_max_before;
+    dg->coefficient_min_abs_after = f_.coef_min_after;
+    dg->coefficient_max_abs_after = f_.coef_max_after;
+    dg->stall_iteration = -1;
+  }
+  setup();
+  cudaEvent_t e0, e1;
+  SOV_CUDA(cudaEventCreate(&e0));
+  SOV_CUDA(cudaEventCreate(&e1));
+  SOV_CUDA(cudaEventRecord(e0, st_));
+
+  // starting point (interior_point.cpp:488-506 / qp_interior_point.cpp:2881-2950, default start)
+  assemble_and_factor(kWeightOnes);
+  launch_start_rhs(dev_, st_, &launches_);
+  newton_solve();
+  launch_start_point(dev_, st_, &launches_);
+  bool warm_used = false;
+  if (opt_.warm_x && opt_.warm_y && opt_.warm_s) {
+    // keep the supplied point when its residual metric beats the default start's
+    launch_residuals(dev_, st_, &launches_);
+    read_scalars();
+    const double default_metric = hs_.h->metric, default_mu = hs_.h->mu;
+    SOV_CUDA(cudaMemcpyAsync(bx_.p, x_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(bs_.p, s_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(by_.p, y_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
+    x_.upload(opt_.warm_x, n, st_);
+    y_.upload(opt_.warm_y, m, st_);
+    s_.upload(opt_.warm_s, n, st_);
+    launch_residuals(dev_, st_, &launches_);
+    read_scalars();
+    if (std::isfinite(hs_.h->metric) && hs_.h->metric < default_metric && hs_.h->mu < default_mu) {
+      warm_used = true;
+    } else {
+      SOV_CUDA(cudaMemcpyAsync(x_.p, bx_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(s_.p, bs_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(y_.p, by_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
+    }
+  }
+  if (dg) dg->warm_start_used = warm_used ? 1 : 0;
+  SOV_CUDA(cudaMemsetAsync(&sc_.p->fail, 0, sizeof(int), st_));
+
+  SOV_CUDA(cudaMemcpyAsync(bx_.p, x_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+  SOV_CUDA(cudaMemcpyAsync(bs_.p, s_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+  SOV_CUDA(cudaMemcpyAsync(by_.p, y_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
+  double best_metric = INFINITY, best_gap = INFINITY, best_p = INFINITY, best_d = INFINITY;
+  int best_it = 0, stale = 0;
+  bool done = false;
+  std::string fail_msg;
+  int it = 0;
+  for (; it < opt_.max_iterations; ++it) {
+    launch_residuals(dev_, st_, &launches_);
+    read_scalars();
+    const IpmScalars s = *hs_.h;
+    if (it > 0) {
+      const int prev = it - 1;
+      const bool prev_sample = prev < 8 || prev % 10 == 0 || prev + 1 == opt_.max_iterations;
+      if (dg && prev_sample && dg->step_history_len < SOV_HISTORY_MAX) {
+        dg->primal_step_history[dg->step_history_len] = s.alpha_p;
+        dg->dual_step_history[dg->step_history_len] = s.alpha_d;
+        dg->step_history_len++;
+      }
+      if (dg && dg->stall_iteration == prev + 1) {
+        dg->stall_primal_step = s.alpha_p;
+        dg->stall_dual_step = s.alpha_d;
+      }
+    }
+    if (s.fail || s.skipped) {
+      fail_msg = f_.qp ? "QP-IPM Newton factorization failed."
+                       : "IPM stopped because the affine predictor factorization failed; the best iterate is returned "
+                         "with optimality unproven.";
+      break;
+    }
+    if (s.metric < best_metric) {
+      best_metric = s.metric;
+      SOV_CUDA(cudaMemcpyAsync(bx_.p, x_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(bs_.p, s_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(by_.p, y_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
+      best_gap = s.gap;
+      best_p = s.p_res;
+      best_d = s.d_res;
+      best_it = it + 1;
+      stale = 0;
+    } else {
+      ++stale;
+    }
+    const bool sample = it < 8 || it % 10 == 0 || it + 1 == opt_.max_iterations;
+    if (dg && sample && dg->history_len < SOV_HISTORY_MAX) {
+      dg->history_iterations[dg->history_len] = it + 1;
+      dg->objective_history[dg->history_len] = s.cx;
+      dg->gap_history[dg->history_len] = s.gap;
+      dg->mu_history[dg->history_len] = s.mu;
+      dg->history_len++;
+    }
+    if (s.gap < best_gap) {
+      best_gap = s.gap;
+      stale = 0;
+    } else if (stale >= 8 && dg && dg->stall_iteration < 0) {
+      dg->stall_iteration = it + 1;
+      dg->stall_gap = s.gap;
+      dg->stall_mu = s.mu;
+    }
+    if (s.p_res < opt_.feasibility_tol && s.d_res < opt_.feasibility_tol && s.gap < opt_.optimality_tol) {
+      SOV_CUDA(cudaEventRecord(e1, st_));
+      const std::string msg =
+          f_.qp ? "Optimal convex QP found by Mehrotra predictor-corrector IPM. KKT system: normal equations, " +
+                      describe() + "."
+                : "Optimal solution found by primal-dual interior-point (Mehrotra). Normal equations: " + describe() +
+                      ".";
+      publish(x_, y_, s_, SOV_OPTIMAL, it + 1, s.gap, s.p_res, s.d_res, msg, r);
+      done = true;
+      break;
+    }
+    assemble_and_factor(f_.qp ? kWeightQp : kWeightLp);
+    launch_newton_rhs(dev_, kRhsAffine, st_, &launches_);
+    newton_solve();
+    launch_direction(dev_, kRhsAffine, st_, &launches_);
+    launch_newton_rhs(dev_, kRhsCorrector, st_, &launches_);
+    newton_solve();
+    launch_direction(dev_, kRhsCorrector, st_, &launches_);
+    launch_update(dev_, st_, &launches_);
+  }
+  if (!done) SOV_CUDA(cudaEventRecord(e1, st_));
+  SOV_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  SOV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  r->solve_seconds = ms * 1e-3;
+  int err_h = 0;
+  SOV_CUDA(cudaMemcpy(&err_h, err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err_h) throw std::runtime_error("a dataflow triangular solve timed out waiting for a dependency");
+  if (!done) {
+    if (f_.qp) {
+      // solve_qp_ipm failure exits publish the current point without an objective (:3042-3048, :3112-3115)
+      const std::string msg = fail_msg.empty() ? "QP-IPM iteration limit reached without convergence." : fail_msg;
+      publish(x_, y_, s_, SOV_ERROR, fail_msg.empty() ? it : best_it, best_gap, best_p, best_d, msg, r);
+      r->has_objective_value = 0;
+    } else {
+      const int st = best_p <= opt_.feasibility_tol ? SOV_FEASIBLE : SOV_NUMERICAL_ERROR;
+      std::string msg = fail_msg;
+      if (msg.empty()) {
+        char buf[512];
+        std::snprintf(buf, sizeof buf,
+                      "IPM stopped after %d iterations without meeting tolerance; returning best iterate from %d as "
+                      "a lower-accuracy candidate. Relative duality gap = %g (tolerance %g), primal residual = %g, "
+                      "dual residual = %g. Optimality is not proven.",
+                      opt_.max_iterations, best_it, best_gap, opt_.optimality_tol, best_p, best_d);
+        msg = buf;
+      }
+      publish(bx_, by_, bs_, st, best_it, best_gap, best_p, best_d, msg, r);
+    }
+  }
+  if (dg) {
+    dg->refactorizations = factorizations_;
+    dg->pcg_iterations = pcg_iterations_;
+    dg->fp64_fallbacks = fp64_fallbacks_;
+  }
+  if (stats_) {
+    stats_->launches += launches_;
+    stats_->factorizations += factorizations_;
+    stats_->kernel_ms += ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (pcg_h_) cudaFreeHost(pcg_h_);
+}
+
+}  // namespace
+
+int solve_single(const sov_model& model, const StdForm& f, const sov_options& opt, sov_result* result,
+                 cudaStream_t stream, EngineStats* stats) {
+  Engine e(model, f, opt, stream, stats);
+  e.run(result);
+  return SOV_OK;
+}
+
+}  // namespace sov

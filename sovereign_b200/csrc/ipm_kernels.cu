@@ -1,0 +1,381 @@
+// ipm_kernels.cu -- per-iteration vector kernels of the Mehrotra predictor-corrector method.
+//
+// Every pass is fused so that each n- or m-vector crosses HBM once per logical use:
+//   residual rows    rp = b - A x                               + max|rp|
+//   residual cols    rd = c + Qx - A'y - s                      + max|rd|, x's, c'x, x'Qx
+//   Newton rhs rows  z = rp + A tmp, tmp from (x, s, rd, dx_aff, ds_aff, sigma mu) on the fly
+//   direction cols   A'dy, dx, ds, both ratio tests             (+ mu_aff pass for the predictor)
+//   update           x, s (floors) and y
+// Reductions are deterministic: per-block partials, the last block to finish folds them in
+// block order and applies the scalar logic of the reference (mu, residual norms, gap, sigma,
+// step lengths), so the host reads one small struct per iteration.
+#include <algorithm>
+
+#include "common.cuh"
+#include "ipm_kernels.cuh"
+
+namespace sov {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBlocks = 1184;  // 8 x 148 SMs
+
+__device__ __forceinline__ double op_apply(int op, double a, double b) {
+  return op == 0 ? a + b : op == 1 ? fmax(a, b) : fmin(a, b);
+}
+__device__ __forceinline__ double op_identity(int op) { return op == 0 ? 0.0 : op == 1 ? -INFINITY : INFINITY; }
+
+// Block-reduce NV values, publish partials, and return true in every thread of the last block,
+// whose thread 0 then holds the grid-wide results in v.
+template <int NV>
+__device__ bool grid_reduce(double (&v)[NV], const int (&ops)[NV], double* partials, unsigned* counter) {
+  __shared__ double scratch[4 * 32];
+  __shared__ bool last;
+  static_assert(NV <= 8, "at most 8 slots");
+  // reduce in chunks of 4 through the shared scratch
+  double r[NV];
+#pragma unroll
+  for (int k0 = 0; k0 < NV; k0 += 4) {
+    double t[4];
+    int o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      t[k] = k0 + k < NV ? v[k0 + k] : 0.0;
+      o[k] = k0 + k < NV ? ops[k0 + k] : 0;
+    }
+    block_reduce<4>(t, o, scratch);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k0 + k < NV) r[k0 + k] = t[k];
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[k * kMaxBlocks + blockIdx.x] = r[k];
+    __threadfence();
+    const unsigned ticket = atomicAdd(counter, 1u);
+    last = ticket == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k0 = 0; k0 < NV; k0 += 4) {
+    double t[4];
+    int o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      o[k] = k0 + k < NV ? ops[k0 + k] : 0;
+      double acc = op_identity(o[k]);
+      if (k0 + k < NV)
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+          acc = op_apply(o[k], acc, __ldcg(partials + (k0 + k) * kMaxBlocks + b));
+      t[k] = acc;
+    }
+    block_reduce<4>(t, o, scratch);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k0 + k < NV) v[k0 + k] = t[k];
+  }
+  if (threadIdx.x == 0) *counter = 0;
+  return true;
+}
+
+int blocks_for(int n) { return std::max(1, std::min(kMaxBlocks, ceil_div(n, kThreads))); }
+
+// sum_j a_ij v_j over row i, one warp per row
+__device__ __forceinline__ int warp_row() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_residual_rows(IpmDev d) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  double mx = 0.0;
+  for (int i = warp_row(); i < d.m; i += warps) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * d.x[d.col_idx[p]];
+    acc = warp_sum(acc);
+    const double r = d.b[i] - acc;
+    if (lane == 0) d.rp[i] = r;
+    mx = fmax(mx, fabs(r));
+  }
+  double v[1] = {mx};
+  const int ops[1] = {1};
+  if (grid_reduce<1>(v, ops, d.partials, d.counter) && threadIdx.x == 0) d.sc->rp_max = v[0];
+}
+
+__global__ void __launch_bounds__(kThreads) k_residual_cols(IpmDev d) {
+  double rdm = 0.0, xs = 0.0, cx = 0.0, xqx = 0.0, qxm = 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double aty = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) aty += d.cval[p] * d.y[d.row_idx[p]];
+    const double xj = d.x[j], sj = d.s[j];
+    double qx = 0.0;
+    if (d.qp) qx = d.qdiag[j] * xj;
+    // LP: rd = c - (A'y + s) (interior_point.cpp:578-582); QP: Qx + c - A'y - s (:2986-2992)
+    const double r = d.qp ? qx + d.c[j] - aty - sj : d.c[j] - (aty + sj);
+    d.rd[j] = r;
+    rdm = fmax(rdm, fabs(r));
+    if (!d.qp || !d.free_col[j]) xs += xj * sj;
+    cx += d.c[j] * xj;
+    xqx += xj * qx;
+    qxm = fmax(qxm, fabs(qx));
+  }
+  double v[5] = {rdm, xs, cx, xqx, qxm};
+  const int ops[5] = {1, 0, 0, 0, 1};
+  if (grid_reduce<5>(v, ops, d.partials, d.counter) && threadIdx.x == 0) {
+    IpmScalars* sc = d.sc;
+    sc->rd_max = v[0];
+    sc->xs = v[1];
+    sc->cx = v[2];
+    sc->xqx = v[3];
+    sc->qx_max = v[4];
+    sc->p_res = sc->rp_max / d.bnorm;
+    if (d.qp) {
+      sc->mu = v[1] / d.comp_count;
+      sc->d_res = v[0] / fmax(1.0, d.cnorm + v[4]);
+      sc->gap = sc->mu * d.comp_count / (1.0 + fabs(v[2] + 0.5 * v[3] + d.objective_offset));
+    } else {
+      sc->mu = v[1] / static_cast<double>(d.n);
+      sc->d_res = v[0] / d.cnorm;
+      sc->gap = fabs(v[1]) / (1.0 + fabs(v[2]));
+    }
+    sc->metric = fmax(sc->p_res, fmax(sc->d_res, sc->gap));
+  }
+}
+
+// Complementarity right-hand side rxs_j of the current mode (interior_point.cpp:644-648,
+// 676-681; qp_interior_point.cpp:3051-3055, 3075-3080).
+__device__ __forceinline__ double rxs_of(const IpmDev& d, int mode, int j, double sigma_mu) {
+  const double xj = d.x[j], sj = d.s[j];
+  if (d.qp && d.free_col[j]) return 0.0;
+  if (mode == kRhsAffine) return -xj * sj;
+  return -xj * sj - d.dxa[j] * d.dsa[j] + sigma_mu;
+}
+
+// tmp_j of z = rp + A tmp:  LP: d rd - rxs/s ; QP: -D r1 with D = 1/(Q_jj + h), r1 = -rd + rxs/x
+__device__ __forceinline__ double newton_tmp(const IpmDev& d, int mode, int j, double sigma_mu) {
+  const double xj = fmax(d.x[j], 1e-16), sj = fmax(d.s[j], 1e-16);
+  const double rxs = rxs_of(d, mode, j, sigma_mu);
+  if (!d.qp) return (xj / sj) * d.rd[j] - rxs / sj;
+  const bool fr = d.free_col[j];
+  const double D = 1.0 / (d.qdiag[j] + (fr ? 0.0 : sj / xj));
+  const double r1 = fr ? -d.rd[j] : -d.rd[j] + rxs / xj;
+  return -D * r1;
+}
+
+__global__ void __launch_bounds__(kThreads) k_newton_rhs(IpmDev d, int mode) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  for (int i = warp_row(); i < d.m; i += warps) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32)
+      acc += d.rval[p] * newton_tmp(d, mode, d.col_idx[p], sigma_mu);
+    acc = warp_sum(acc);
+    if (lane == 0) d.z[i] = d.rp[i] + acc;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_direction(IpmDev d, int mode) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  double* dx = mode == kRhsAffine ? d.dxa : d.dx;
+  double* ds = mode == kRhsAffine ? d.dsa : d.ds;
+  double rp_min = 1.0, rd_min = 1.0;  // step_to_bound starts at alpha = 1
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double atdy = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+    const double xj = d.x[j], sj = d.s[j];
+    const double rxs = rxs_of(d, mode, j, sigma_mu);
+    double dxj, dsj;
+    bool fr = false;
+    if (!d.qp) {
+      // solve_newton (interior_point.cpp:443-450)
+      const double dj = fmax(xj, 1e-16) / fmax(sj, 1e-16);
+      dxj = dj * (atdy - d.rd[j]) + rxs / fmax(sj, 1e-16);
+      dsj = d.rd[j] - atdy;
+    } else {
+      // dx = D (r1 + A'dy); ds = (rxs - s dx)/x (qp_interior_point.cpp:2832-2844)
+      fr = d.free_col[j];
+      const double xf = fmax(xj, 1e-16);
+      const double D = 1.0 / (d.qdiag[j] + (fr ? 0.0 : fmax(sj, 1e-16) / xf));
+      const double r1 = fr ? -d.rd[j] : -d.rd[j] + rxs / xf;
+      dxj = D * (r1 + atdy);
+      dsj = fr ? 0.0 : (rxs - sj * dxj) / xf;
+    }
+    dx[j] = dxj;
+    ds[j] = dsj;
+    if (!fr) {
+      if (dxj < 0.0) rp_min = fmin(rp_min, -xj / dxj);
+      if (dsj < 0.0) rd_min = fmin(rd_min, -sj / dsj);
+    }
+  }
+  double v[2] = {rp_min, rd_min};
+  const int ops[2] = {2, 2};
+  if (grid_reduce<2>(v, ops, d.partials, d.counter) && threadIdx.x == 0) {
+    IpmScalars* sc = d.sc;
+    sc->ratio_p = v[0];
+    sc->ratio_d = v[1];
+    if (mode == kRhsAffine) {
+      sc->alpha_p_aff = v[0];
+      sc->alpha_d_aff = v[1];
+    } else {
+      double ap = fmin(1.0, d.tau * v[0]);
+      double ad = fmin(1.0, d.tau * v[1]);
+      if (d.qp && d.has_quadratic) ap = ad = fmin(ap, ad);  // common step (qp_interior_point.cpp:3095)
+      sc->alpha_p = ap;
+      sc->alpha_d = ad;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_mu_aff(IpmDev d) {
+  const double ap = d.sc->alpha_p_aff, ad = d.sc->alpha_d_aff;
+  double acc = 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    if (d.qp && d.free_col[j]) continue;
+    acc += (d.x[j] + ap * d.dxa[j]) * (d.s[j] + ad * d.dsa[j]);
+  }
+  double v[1] = {acc};
+  const int ops[1] = {0};
+  if (grid_reduce<1>(v, ops, d.partials, d.counter) && threadIdx.x == 0) {
+    IpmScalars* sc = d.sc;
+    const double cnt = d.qp ? d.comp_count : static_cast<double>(d.n);
+    sc->mu_aff = v[0] / cnt;
+    const double r = sc->mu_aff / sc->mu;
+    sc->sigma = sc->mu > 0.0 ? fmin(1.0, r * r * r) : 0.0;  // (mu_aff/mu)^3 (interior_point.cpp:672-673)
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_update(IpmDev d) {
+  if (d.sc->fail) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.sc->skipped = 1;
+    return;
+  }
+  const double ap = d.sc->alpha_p, ad = d.sc->alpha_d;
+  const int N = d.n > d.m ? d.n : d.m;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    if (j < d.n) {
+      if (d.qp && d.free_col[j]) {
+        d.x[j] += ap * d.dx[j];
+      } else {
+        d.x[j] = fmax(d.x[j] + ap * d.dx[j], 1e-14);
+        d.s[j] = fmax(d.s[j] + ad * d.ds[j], 1e-14);
+      }
+    }
+    if (j < d.m) d.y[j] += ad * d.z[j];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_start_rhs(IpmDev d) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = warp_row(); i < d.m; i += warps) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p];
+    acc = warp_sum(acc);
+    if (lane == 0) d.z[i] = d.b[i] - acc;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
+  const bool ok = !d.sc->fail;
+  const int N = d.n > d.m ? d.n : d.m;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    if (j < d.n) {
+      double x = 1.0, s = 1.0;
+      if (ok) {
+        double atdy = 0.0;
+        for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+        if (!d.qp) {
+          x = fmax(1.0, fabs(atdy));
+          s = fmax(1.0, fabs(d.c[j] - atdy));
+        } else if (d.free_col[j]) {
+          x = 1.0 + atdy;
+        } else {
+          x = fmax(1.0, fabs(atdy));
+          s = fmax(1.0, fabs(d.qdiag[j] + d.c[j] - atdy));
+        }
+      }
+      if (d.qp && d.free_col[j]) s = 0.0;
+      d.x[j] = x;
+      d.s[j] = s;
+    }
+    if (j < d.m) d.y[j] = ok ? d.z[j] : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_normal_cols(IpmDev d, const double* v, double* tmp) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) a += d.cval[p] * v[d.row_idx[p]];
+    const double xj = fmax(d.x[j], 1e-16), sj = fmax(d.s[j], 1e-16);
+    double w;
+    if (!d.qp) w = xj / sj;
+    else w = 1.0 / (d.qdiag[j] + (d.free_col[j] ? 0.0 : sj / xj));
+    tmp[j] = w * a;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_normal_rows(IpmDev d, const double* v, const double* tmp, double* out,
+                                                          double reg) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = warp_row(); i < d.m; i += warps) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * tmp[d.col_idx[p]];
+    acc = warp_sum(acc);
+    if (lane == 0) out[i] = acc + reg * v[i];
+  }
+}
+
+int row_blocks(int m) { return std::max(1, std::min(kMaxBlocks, ceil_div(static_cast<long long>(m) * 32, kThreads))); }
+
+}  // namespace
+
+int reduction_blocks(int n) { return blocks_for(n); }
+
+void launch_residuals(const IpmDev& d, cudaStream_t st, int* launches) {
+  k_residual_rows<<<row_blocks(d.m), kThreads, 0, st>>>(d);
+  k_residual_cols<<<blocks_for(d.n), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 2;
+}
+
+void launch_newton_rhs(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
+  k_newton_rhs<<<row_blocks(d.m), kThreads, 0, st>>>(d, mode);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 1;
+}
+
+void launch_direction(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
+  k_direction<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode);
+  if (mode == kRhsAffine) k_mu_aff<<<blocks_for(d.n), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += mode == kRhsAffine ? 2 : 1;
+}
+
+void launch_update(const IpmDev& d, cudaStream_t st, int* launches) {
+  k_update<<<blocks_for(std::max(d.n, d.m)), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 1;
+}
+
+void launch_start_rhs(const IpmDev& d, cudaStream_t st, int* launches) {
+  k_start_rhs<<<row_blocks(d.m), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 1;
+}
+
+void launch_start_point(const IpmDev& d, cudaStream_t st, int* launches) {
+  k_start_point<<<blocks_for(std::max(d.n, d.m)), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 1;
+}
+
+void launch_normal_matvec(const IpmDev& d, const double* v, double* tmp_n, double* out, double reg, cudaStream_t st) {
+  k_normal_cols<<<blocks_for(d.n), kThreads, 0, st>>>(d, v, tmp_n);
+  k_normal_rows<<<row_blocks(d.m), kThreads, 0, st>>>(d, v, tmp_n, out, reg);
+  SOV_LAUNCH_CHECK();
+}
+
+}  // namespace sov

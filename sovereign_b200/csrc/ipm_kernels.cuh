@@ -1,0 +1,71 @@
+// ipm_kernels.cuh -- per-iteration vector kernels of the Mehrotra predictor-corrector method.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace sov {
+
+// Scalars of one iteration, written on the device, read by the host once per iteration.
+struct IpmScalars {
+  // residual phase (interior_point.cpp:572-602, qp_interior_point.cpp:2978-3000)
+  double rp_max, rd_max, xs, cx, xqx, qx_max;
+  double mu, p_res, d_res, gap, metric;
+  // direction phase
+  double ratio_p, ratio_d;    // step_to_bound of the last direction (<= 1)
+  double alpha_p_aff, alpha_d_aff, mu_aff, sigma;
+  double alpha_p, alpha_d;    // step taken
+  // solver health
+  int fail, drops, err, skipped;
+};
+
+struct IpmDev {
+  int m, n;
+  // A in CSR (rows) and CSC (columns), scaled
+  const int* row_ptr;
+  const int* col_idx;
+  const double* rval;
+  const int* col_ptr;
+  const int* row_idx;
+  const double* cval;
+  const double* b;
+  const double* c;
+  const double* qdiag;      // QP: diagonal of Q (null for LP)
+  const uint8_t* free_col;  // QP: 1 = no barrier (null for LP)
+  int qp;
+  int has_quadratic;
+  double comp_count;        // n (LP) or max(1, #bounded) (QP)
+  double bnorm, cnorm, objective_offset, tau;
+  // iterate and work vectors
+  double *x, *y, *s;
+  double *dx, *ds, *dxa, *dsa;
+  double *rp, *rd;
+  double* z;                // Newton right-hand side / dy (padded to the solver's order)
+  IpmScalars* sc;
+  // grid reduction scratch
+  double* partials;         // 8 * max_blocks
+  unsigned* counter;
+};
+
+enum RhsMode : int { kRhsAffine = 0, kRhsCorrector = 1 };
+
+// rp = b - A x, rd = c + Q x - A'y - s; fills sc->{rp_max, rd_max, xs, cx, mu, p_res, d_res, gap}
+void launch_residuals(const IpmDev& d, cudaStream_t st, int* launches);
+// z = rp + A tmp (Newton right-hand side of the normal equations)
+void launch_newton_rhs(const IpmDev& d, int mode, cudaStream_t st, int* launches);
+// dx, ds from dy = z; ratio tests; affine -> alpha_aff, mu_aff, sigma; corrector -> alpha
+void launch_direction(const IpmDev& d, int mode, cudaStream_t st, int* launches);
+// x, s, y update with the 1e-14 floors
+void launch_update(const IpmDev& d, cudaStream_t st, int* launches);
+// starting point: z = b - A 1 (rhs of the least-squares push)
+void launch_start_rhs(const IpmDev& d, cudaStream_t st, int* launches);
+// starting point from dy = z (interior_point.cpp:497-503; qp_interior_point.cpp:2931-2947)
+void launch_start_point(const IpmDev& d, cudaStream_t st, int* launches);
+// matrix-free normal product out = A diag(w) A' v + reg v, w from the iterate (mixed-precision PCG)
+void launch_normal_matvec(const IpmDev& d, const double* v, double* tmp_n, double* out, double reg,
+                          cudaStream_t st);
+
+int reduction_blocks(int n);
+
+}  // namespace sov

@@ -1,0 +1,39 @@
+// sparse.hpp -- host ordering and symbolic analysis for the sparse LDL' of the normal matrix.
+//
+// Minimum-degree ordering on the explicit elimination graph of A A' (the rule of the reference's
+// AMDOrdering::compute, solver/numerical/src/amd_ordering.cpp:12-130: rows whose degree exceeds
+// max(16, 10 sqrt(m)) are ordered last, ties go to the lowest row, an optional fill limit aborts
+// the analysis), then the column patterns of L, the elimination tree and a level schedule for the
+// GPU: columns of equal height in the tree have no ancestor relation, so a level's columns are
+// finished together and their rank-1 updates applied together.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "stdform.hpp"
+
+namespace sov {
+
+struct SparseSymbolic {
+  int m = 0;
+  std::vector<int> perm, iperm;  // perm[k] = row eliminated k-th; iperm[row] = k
+  std::vector<int> lp, li;       // L (permuted): column k's strict-lower rows li[lp[k]..lp[k+1]), ascending
+  std::vector<int> parent;       // elimination tree (permuted), -1 at roots
+  std::vector<int> lvl_ptr, lvl_col;  // columns grouped by height in the tree (leaves first)
+  // rank-1 updates of each level: (column k, position of l_ak, position of l_bk, destination);
+  // destination < m is the diagonal slot of a row, else m + position in L
+  std::vector<int> pair_ptr;     // per level
+  std::vector<int> pairs;        // 4 ints per update
+  // assembly of A diag(d) A' into the [D | L] storage: targets with their contributions
+  std::vector<int> asm_target, asm_ptr, asm_col;
+  std::vector<double> asm_w;
+  long long nnz_l = 0;
+  double flops = 0.0;            // sum over columns of colcount^2 (sparse_ldlt.cpp:230-238)
+  int levels() const { return static_cast<int>(lvl_ptr.size()) - 1; }
+};
+
+// Returns false when the predicted fill exceeds fill_limit entries (0 = no limit).
+bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& out);
+
+}  // namespace sov

@@ -1,0 +1,298 @@
+// stdform.cpp -- host-side standard form and normal-matrix assembly maps.
+#include "stdform.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+#include <stdexcept>
+#include <utility>
+
+namespace sov {
+namespace {
+
+void coefficient_range(const std::vector<double>& v, double& lo, double& hi) {
+  // interior_point.cpp:46-56
+  lo = std::numeric_limits<double>::infinity();
+  hi = 0.0;
+  for (double x : v) {
+    const double a = std::abs(x);
+    if (a == 0.0 || !std::isfinite(a)) continue;
+    lo = std::min(lo, a);
+    hi = std::max(hi, a);
+  }
+  if (!std::isfinite(lo)) lo = 0.0;
+}
+
+void build_csr(StdForm& f) {
+  f.row_ptr.assign(f.m + 1, 0);
+  for (int p = 0; p < f.nnz(); ++p) f.row_ptr[f.row_idx[p] + 1]++;
+  for (int i = 0; i < f.m; ++i) f.row_ptr[i + 1] += f.row_ptr[i];
+  f.col_idx.resize(f.nnz());
+  f.rval.resize(f.nnz());
+  std::vector<int> fill(f.row_ptr.begin(), f.row_ptr.end() - 1);
+  for (int j = 0; j < f.n; ++j)
+    for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p) {
+      const int q = fill[f.row_idx[p]]++;
+      f.col_idx[q] = j;
+      f.rval[q] = f.val[p];
+    }
+}
+
+}  // namespace
+
+StdForm build_std_form(const sov_model& p, bool qp, bool enable_scaling) {
+  StdForm f;
+  f.qp = qp;
+  const int ns = p.n, m0 = p.m;
+  f.n_struct = ns;
+  f.m0 = m0;
+  f.shift.assign(ns, 0.0);
+  std::vector<uint8_t> free_s(ns, 0);
+  std::vector<std::pair<int, double>> ub_cons;
+  for (int j = 0; j < ns; ++j) {
+    const double lb = p.lb ? p.lb[j] : 0.0;
+    const double ub = p.ub ? p.ub[j] : 1e30;
+    const bool no_lower = qp && !(lb > -1e29);
+    free_s[j] = no_lower ? 1 : 0;
+    f.shift[j] = no_lower ? 0.0 : lb;
+    if (std::isfinite(ub) && ub < 1e29) {
+      const double u = ub - f.shift[j];
+      if (!no_lower && u < -1e-12) throw std::runtime_error("Inconsistent bounds for variable x" + std::to_string(j));
+      ub_cons.push_back({j, u});
+    }
+  }
+  const int n_ub = static_cast<int>(ub_cons.size());
+  const int m = m0 + n_ub;
+  int n_slack = n_ub;
+  for (int r = 0; r < m0; ++r) n_slack += p.sense[r] != SOV_EQ ? 1 : 0;
+  const int n = ns + n_slack;
+  f.m = m;
+  f.n = n;
+  f.b.assign(m, 0.0);
+  f.c.assign(n, 0.0);
+  f.col_scale.assign(n, 1.0);
+  f.row_scale.assign(m, 1.0);
+  f.free_col.assign(n, 0);
+  std::copy(free_s.begin(), free_s.end(), f.free_col.begin());
+  for (int i = 0; i < m0; ++i) f.b[i] = p.rhs[i];
+
+  std::vector<int> ub_row(ns, -1);
+  for (int k = 0; k < n_ub; ++k) ub_row[ub_cons[k].first] = m0 + k;
+
+  f.col_ptr.assign(n + 1, 0);
+  f.row_idx.reserve(static_cast<std::size_t>(p.col_ptr[ns]) + n_ub + n_slack);
+  f.val.reserve(f.row_idx.capacity());
+  std::vector<std::pair<int, double>> col;
+  for (int j = 0; j < ns; ++j) {
+    col.clear();
+    for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) col.push_back({p.row_idx[k], p.values[k]});
+    if (ub_row[j] >= 0) col.push_back({ub_row[j], 1.0});
+    std::sort(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    // merge duplicates (a Constraint's name-keyed map sums them), then drop exact zeros
+    std::size_t w = 0;
+    for (std::size_t q = 0; q < col.size(); ++q) {
+      if (w > 0 && col[w - 1].first == col[q].first) col[w - 1].second += col[q].second;
+      else col[w++] = col[q];
+    }
+    col.resize(w);
+    for (const auto& e : col) {
+      if (e.first < m0) f.b[e.first] -= e.second * f.shift[j];
+      if (std::abs(e.second) > 0.0) {
+        f.row_idx.push_back(e.first);
+        f.val.push_back(e.second);
+      }
+    }
+    f.col_ptr[j + 1] = static_cast<int>(f.row_idx.size());
+  }
+  for (int k = 0; k < n_ub; ++k) f.b[m0 + k] = ub_cons[k].second;
+  int sc = ns;
+  for (int r = 0; r < m; ++r) {
+    const int kind = r < m0 ? p.sense[r] : SOV_LE;
+    if (kind == SOV_EQ) continue;
+    f.row_idx.push_back(r);
+    f.val.push_back(kind == SOV_LE ? 1.0 : -1.0);
+    f.col_ptr[++sc] = static_cast<int>(f.row_idx.size());
+  }
+  const double sign = p.maximize ? -1.0 : 1.0;
+  for (int j = 0; j < ns; ++j) f.c[j] = sign * (p.obj ? p.obj[j] : 0.0);
+
+  if (qp) {
+    // build_hessian (qp_interior_point.cpp:68-106)
+    std::vector<std::vector<std::pair<int, double>>> qc(n);
+    if (p.q_col_ptr) {
+      for (int j = 0; j < ns; ++j)
+        for (int k = p.q_col_ptr[j]; k < p.q_col_ptr[j + 1]; ++k) {
+          const int i = p.q_row_idx[k];
+          const double v = sign * p.q_values[k];
+          if (i == j) qc[i].push_back({i, v});
+          else {
+            qc[j].push_back({i, 0.5 * v});
+            qc[i].push_back({j, 0.5 * v});
+          }
+        }
+    }
+    for (int i = 0; i < ns; ++i) qc[i].push_back({i, 1e-14});
+    f.q_ptr.assign(n + 1, 0);
+    f.qdiag.assign(n, 0.0);
+    for (int j = 0; j < n; ++j) {
+      auto& e = qc[j];
+      std::stable_sort(e.begin(), e.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+      for (std::size_t k = 0; k < e.size();) {
+        const int r = e[k].first;
+        double v = 0.0;
+        for (; k < e.size() && e[k].first == r; ++k) v += e[k].second;
+        if (v != 0.0) {
+          f.q_idx.push_back(r);
+          f.q_val.push_back(v);
+          if (r == j) f.qdiag[j] = v;
+          else f.q_diagonal = false;
+          f.has_quadratic = f.has_quadratic || std::abs(v) > 1e-12;
+        }
+      }
+      f.q_ptr[j + 1] = static_cast<int>(f.q_idx.size());
+    }
+    // c_eff = sense*c + Q*lb (:206-216) and the gap's objective offset (:2966-2975)
+    std::vector<double> qs(n, 0.0);
+    for (int j = 0; j < ns; ++j)
+      for (int k = f.q_ptr[j]; k < f.q_ptr[j + 1]; ++k) qs[f.q_idx[k]] += f.q_val[k] * f.shift[j];
+    double cs = 0.0, sqs = 0.0;
+    for (int j = 0; j < ns; ++j) {
+      f.c[j] += qs[j];
+      cs += f.c[j] * f.shift[j];
+      sqs += f.shift[j] * qs[j];
+    }
+    f.objective_offset = cs - 0.5 * sqs + sign * p.obj_constant;
+  }
+
+  coefficient_range(f.val, f.coef_min_before, f.coef_max_before);
+  f.scaling_applied = enable_scaling && m > 0 && n > 0;
+  if (f.scaling_applied) {
+    // two passes: rows by 1/sqrt(max|a|), then columns (interior_point.cpp:370-405)
+    std::vector<double> rs(m);
+    for (int pass = 0; pass < 2; ++pass) {
+      std::fill(rs.begin(), rs.end(), 0.0);
+      for (int q = 0; q < f.nnz(); ++q) rs[f.row_idx[q]] = std::max(rs[f.row_idx[q]], std::abs(f.val[q]));
+      for (int i = 0; i < m; ++i) {
+        rs[i] = rs[i] > 0.0 ? 1.0 / std::sqrt(rs[i]) : 1.0;
+        f.row_scale[i] *= rs[i];
+        f.b[i] *= rs[i];
+      }
+      for (int q = 0; q < f.nnz(); ++q) f.val[q] *= rs[f.row_idx[q]];
+      for (int j = 0; j < n; ++j) {
+        double mx = 0.0;
+        for (int q = f.col_ptr[j]; q < f.col_ptr[j + 1]; ++q) mx = std::max(mx, std::abs(f.val[q]));
+        const double s = mx > 0.0 ? 1.0 / std::sqrt(mx) : 1.0;
+        for (int q = f.col_ptr[j]; q < f.col_ptr[j + 1]; ++q) f.val[q] *= s;
+        f.c[j] *= s;
+        f.col_scale[j] *= s;
+      }
+    }
+  }
+  coefficient_range(f.val, f.coef_min_after, f.coef_max_after);
+  build_csr(f);
+  return f;
+}
+
+namespace {
+
+template <class Index>
+AssemblyMap build_assembly(const StdForm& f, Index index) {
+  // contributions (target, column, weight) for every pair p >= q of a column's entries
+  struct Contrib {
+    int64_t t;
+    int col;
+    double w;
+  };
+  std::vector<Contrib> cs;
+  std::size_t total = 0;
+  for (int j = 0; j < f.n; ++j) {
+    const std::size_t k = static_cast<std::size_t>(f.col_ptr[j + 1] - f.col_ptr[j]);
+    total += k * (k + 1) / 2;
+  }
+  cs.reserve(total + f.m);
+  for (int j = 0; j < f.n; ++j)
+    for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p)
+      for (int q = f.col_ptr[j]; q <= p; ++q)
+        cs.push_back({index(f.row_idx[p], f.row_idx[q]), j, f.val[p] * f.val[q]});
+  std::stable_sort(cs.begin(), cs.end(), [](const Contrib& a, const Contrib& b) { return a.t < b.t; });
+  AssemblyMap am;
+  am.ptr.push_back(0);
+  for (std::size_t k = 0; k < cs.size(); ++k) {
+    if (am.target.empty() || am.target.back() != cs[k].t) {
+      if (!am.target.empty()) am.ptr.push_back(static_cast<int>(k));
+      am.target.push_back(cs[k].t);
+    }
+    am.col.push_back(cs[k].col);
+    am.w.push_back(cs[k].w);
+  }
+  am.ptr.push_back(static_cast<int>(cs.size()));
+  if (am.target.empty()) am.ptr.assign(1, 0);
+  // every diagonal entry gets a target (rows with no entries still carry the 1e-12 shift)
+  am.diag_target.assign(f.m, -1);
+  std::vector<int64_t> extra;
+  for (int i = 0; i < f.m; ++i) {
+    const int64_t t = index(i, i);
+    auto it = std::lower_bound(am.target.begin(), am.target.end(), t);
+    if (it == am.target.end() || *it != t) extra.push_back(t);
+  }
+  if (!extra.empty()) {
+    // insert empty targets for missing diagonals
+    std::vector<int64_t> tg;
+    std::vector<int> ptr;
+    ptr.push_back(0);
+    std::size_t a = 0, e = 0;
+    std::vector<int> col;
+    std::vector<double> w;
+    while (a < am.target.size() || e < extra.size()) {
+      if (e < extra.size() && (a >= am.target.size() || extra[e] < am.target[a])) {
+        tg.push_back(extra[e++]);
+        ptr.push_back(static_cast<int>(col.size()));
+      } else {
+        tg.push_back(am.target[a]);
+        for (int q = am.ptr[a]; q < am.ptr[a + 1]; ++q) {
+          col.push_back(am.col[q]);
+          w.push_back(am.w[q]);
+        }
+        ptr.push_back(static_cast<int>(col.size()));
+        ++a;
+      }
+    }
+    am.target.swap(tg);
+    am.ptr.swap(ptr);
+    am.col.swap(col);
+    am.w.swap(w);
+  }
+  for (int i = 0; i < f.m; ++i) {
+    const int64_t t = index(i, i);
+    am.diag_target[i] = static_cast<int>(std::lower_bound(am.target.begin(), am.target.end(), t) - am.target.begin());
+  }
+  return am;
+}
+
+}  // namespace
+
+AssemblyMap build_assembly_dense(const StdForm& f, int ld) {
+  return build_assembly(f, [ld](int r, int c) { return static_cast<int64_t>(c) * ld + r; });
+}
+
+AssemblyMap build_assembly_rowmajor(const StdForm& f, int ld) {
+  return build_assembly(f, [ld](int r, int c) { return static_cast<int64_t>(r) * ld + c; });
+}
+
+AssemblyMap build_assembly_band(const StdForm& f, int kd) {
+  const int64_t m = f.m;
+  (void)kd;
+  return build_assembly(f, [m](int r, int c) { return static_cast<int64_t>(r - c) * m + c; });
+}
+
+int normal_bandwidth(const StdForm& f) {
+  int kd = 0;
+  for (int j = 0; j < f.n; ++j) {
+    if (f.col_ptr[j + 1] == f.col_ptr[j]) continue;
+    kd = std::max(kd, f.row_idx[f.col_ptr[j + 1] - 1] - f.row_idx[f.col_ptr[j]]);
+  }
+  return kd;
+}
+
+}  // namespace sov

@@ -1,0 +1,197 @@
+"""Python face of the engine, shaped like the reference's solver classes.
+
+``InteriorPointSolver(InteriorPointOptions).solve(model)`` mirrors
+sovereign::InteriorPointSolver (solver/lp/include/sovereign/interior_point.hpp:26-36) and
+``QpInteriorPointSolver`` mirrors solver/qp/include/sovereign/qp_interior_point.hpp:21-31: same
+option names and defaults, same statuses and messages, results with the same fields
+(``objective_value``, ``primal``, ``dual``, ``duality_gap``, residuals, ``iterations``). Every
+call goes through the C ABI of libsovipm.so; there is no Python or CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from ._lib import check, load
+from .model import Model, Result, ResultBuffers
+
+
+@dataclass
+class InteriorPointOptions:
+    """InteriorPointOptions (interior_point.hpp:7-24) plus the engine's precision knob."""
+    max_iterations: int = 250
+    feasibility_tol: float = 1e-9
+    optimality_tol: float = 1e-9
+    fraction_to_boundary: float = 0.999
+    enable_scaling: bool = True
+    use_sparse_normal_equations: bool = False
+    precision: int = abi.PRECISION_FP64
+    pcg_max_iterations: int = 50
+
+    def to_abi(self, qp: bool = False) -> abi.SovOptions:
+        o = abi.default_options(qp=qp)
+        o.max_iterations = self.max_iterations
+        o.feasibility_tol = self.feasibility_tol
+        o.optimality_tol = self.optimality_tol
+        o.fraction_to_boundary = self.fraction_to_boundary
+        o.enable_scaling = int(self.enable_scaling) if not qp else 0
+        o.precision = self.precision
+        o.pcg_max_iterations = self.pcg_max_iterations
+        mode = os.environ.get("SOVEREIGN_IPM_NORMAL_EQUATIONS", "auto")  # interior_point.cpp:132-133
+        o.factorization = {"dense": abi.FACTOR_DENSE, "banded": abi.FACTOR_BANDED}.get(mode, abi.FACTOR_AUTO)
+        return o
+
+
+@dataclass
+class QpInteriorPointOptions(InteriorPointOptions):
+    """QpInteriorPointOptions (qp_interior_point.hpp:7-18)."""
+    max_iterations: int = 100
+    feasibility_tol: float = 1e-8
+    optimality_tol: float = 1e-8
+    enable_scaling: bool = False
+
+
+def _dims(model: Model) -> tuple[int, int]:
+    n = C.c_int32()
+    m = C.c_int32()
+    check(load().sov_ipm_dims(C.byref(model.to_abi()), int(model.is_qp), C.byref(n), C.byref(m)))
+    return n.value, m.value
+
+
+def _solve(model: Model, opt: abi.SovOptions, qp: bool, with_ipm: bool, with_diag: bool,
+           warm: tuple | None) -> Result:
+    n_ipm, m_ipm = _dims(model)
+    buf = ResultBuffers(model, with_ipm=with_ipm, with_diag=with_diag, n_ipm=n_ipm, m_ipm=m_ipm)
+    keep = None
+    if warm is not None:
+        keep = [np.ascontiguousarray(a, dtype=np.float64) for a in warm]
+        opt.warm_x, opt.warm_y, opt.warm_s = (abi.dptr(a) for a in keep)
+    sm = model.to_abi()
+    fn = load().sov_qp_solve if qp else load().sov_lp_solve
+    check(fn(C.byref(sm), C.byref(opt), C.byref(buf.raw)))
+    del keep
+    return buf.to_result()
+
+
+class InteriorPointSolver:
+    """Mehrotra predictor-corrector LP interior point on the B200 (drop-in for
+    sovereign::InteriorPointSolver)."""
+
+    def __init__(self, options: InteriorPointOptions | None = None):
+        self.options = options or InteriorPointOptions()
+
+    def solve(self, model: Model, with_ipm: bool = False, with_diag: bool = False,
+              warm_start: tuple | None = None) -> Result:
+        return _solve(model, self.options.to_abi(qp=False), False, with_ipm, with_diag, warm_start)
+
+
+class QpInteriorPointSolver:
+    """Convex-QP interior point (diagonal Hessian, normal equations) on the B200."""
+
+    def __init__(self, options: QpInteriorPointOptions | None = None):
+        self.options = options or QpInteriorPointOptions()
+
+    def solve(self, model: Model, with_ipm: bool = False, with_diag: bool = False) -> Result:
+        return _solve(model, self.options.to_abi(qp=True), True, with_ipm, with_diag, None)
+
+
+def solve_batch(models: list[Model], options: InteriorPointOptions | None = None, with_ipm: bool = False
+                ) -> list[Result]:
+    """Independent LPs in one persistent batched launch (sov_lp_solve_batch)."""
+    opt = (options or InteriorPointOptions()).to_abi()
+    bufs = []
+    for m in models:
+        n_ipm, m_ipm = _dims(m) if with_ipm else (0, 0)
+        bufs.append(ResultBuffers(m, with_ipm=with_ipm, n_ipm=n_ipm, m_ipm=m_ipm))
+    arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
+    res = (abi.SovResult * len(models))(*[b.raw for b in bufs])
+    check(load().sov_lp_solve_batch(len(models), arr, C.byref(opt), 0, res))
+    out = []
+    for b, r in zip(bufs, res):
+        b.raw = r
+        out.append(b.to_result())
+    return out
+
+
+class DeviceBatch:
+    """A prepared batch resident on the device (sov_batch_*): upload once, solve many times."""
+
+    def __init__(self, models: list[Model], options: InteriorPointOptions | None = None):
+        self.models = models
+        self._arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
+        self._opt = (options or InteriorPointOptions()).to_abi()
+        h = C.c_void_p()
+        check(load().sov_batch_create(len(models), self._arr, C.byref(self._opt), C.byref(h)))
+        self.handle = h
+
+    def solve(self, stream: int = 0) -> None:
+        check(load().sov_batch_solve(self.handle, C.c_void_p(stream)))
+
+    def results(self, with_ipm: bool = False) -> list[Result]:
+        bufs = []
+        for m in self.models:
+            n_ipm, m_ipm = _dims(m) if with_ipm else (0, 0)
+            bufs.append(ResultBuffers(m, with_ipm=with_ipm, n_ipm=n_ipm, m_ipm=m_ipm))
+        res = (abi.SovResult * len(self.models))(*[b.raw for b in bufs])
+        check(load().sov_batch_results(self.handle, res))
+        out = []
+        for b, r in zip(bufs, res):
+            b.raw = r
+            out.append(b.to_result())
+        return out
+
+    def stats(self) -> dict:
+        launches = C.c_int32()
+        ms, byts, flops = C.c_double(), C.c_double(), C.c_double()
+        check(load().sov_batch_stats(self.handle, C.byref(launches), C.byref(ms), C.byref(byts), C.byref(flops)))
+        return dict(launches=launches.value, kernel_ms=ms.value, bytes_per_iteration=byts.value,
+                    flops_per_iteration=flops.value)
+
+    def close(self) -> None:
+        if self.handle:
+            load().sov_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(models: list[Model], options: InteriorPointOptions | None = None, tuning_file: str | None = None) -> str:
+    arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
+    opt = (options or InteriorPointOptions()).to_abi()
+    rep = C.create_string_buffer(4096)
+    check(load().sov_autotune(len(models), arr, C.byref(opt), tuning_file.encode() if tuning_file else None, rep, 4096))
+    return rep.value.decode()
+
+
+def spmv_csc(m: int, n: int, col_ptr, row_idx, values, x, transpose: bool = False) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(n if transpose else m)
+    check(load().sov_spmv_csc(m, n, col_ptr.ctypes.data, row_idx.ctypes.data, values.ctypes.data, x.ctypes.data,
+                              y.ctypes.data, int(transpose)))
+    return y
+
+
+def normal_factor_solve(m: int, n: int, col_ptr, row_idx, values, d, rhs, precision: int = abi.PRECISION_FP64,
+                        factorization: int = abi.FACTOR_AUTO):
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    rhs = np.array(rhs, dtype=np.float64, order="F", copy=True)
+    nrhs = 1 if rhs.ndim == 1 else rhs.shape[1]
+    dropped = C.c_int32()
+    check(load().sov_normal_factor_solve(m, n, col_ptr.ctypes.data, row_idx.ctypes.data, values.ctypes.data,
+                                         d.ctypes.data, precision, factorization, rhs.ctypes.data, nrhs,
+                                         C.byref(dropped)))
+    return rhs, dropped.value

@@ -1,0 +1,106 @@
+"""Regenerate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a checkout where the reference sources are available (oracle/Makefile builds
+oracle/_ref/libsovref.so from them):
+
+    python tests/golden/make_golden.py
+
+Writes
+  lp_reference.json   InteriorPointSolver results (status, iterations, objective, gap, residuals,
+                      primal checksum) on the seeded and regression LP models below
+  qp_reference.json   QpInteriorPointSolver results on the QP models below
+  liswet_n20000.npz   the reference's published LISWET projection at n = 20000
+                      (benchmarks/reports/liswet_step6/n20000: input_c.txt, x.txt and the
+                      objective printed in solver.stdout.json / independent.json)
+Test code reads only these files; nothing at test time touches the reference tree.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from sovereign_b200 import problems as P  # noqa: E402
+
+LISWET_DIR = "/root/reference/benchmarks/reports/liswet_step6/n20000"
+
+LP_SPECS = [
+    ("reference_transport", [20]), ("reference_transport", [40]), ("reference_transport", [60]),
+    ("reference_staircase", [8, 40]), ("bounded_lp_example", []),
+    ("transport", [50, 50, 0]), ("transport", [50, 50, 1]), ("transport", [50, 50, 2]),
+    ("transport", [13, 37, 5]), ("transport", [60, 10, 7]),
+    ("random_sparse_lp", [100, 500, 8, 1]), ("random_sparse_lp", [200, 1000, 8, 2]),
+    ("random_sparse_lp", [500, 2500, 8, 1]),
+]
+BATCH_SPEC = dict(count=64, seed=3)          # transport_batch sample of the 4096-LP workload
+MULTICOMMODITY_SEEDS = [100, 101]            # MulticommodityFamily() instances
+QP_SPECS = [("small_qp_offdiagonal", []), ("convex_sequence_qp", [52, 3]), ("convex_sequence_qp", [202, 3]),
+            ("convex_sequence_qp", [2002, 3])]
+
+
+def build(name, args):
+    return getattr(P, name)(*args)
+
+
+def summarize(r, model=None):
+    d = dict(status=r.status_name, iterations=r.iterations, objective=r.objective_value,
+             duality_gap=r.duality_gap, primal_residual=r.primal_residual, dual_residual=r.dual_residual,
+             message=r.message)
+    if r.primal is not None:
+        d["primal_sum"] = float(np.sum(r.primal))
+        d["primal_head"] = [float(v) for v in r.primal[:8]]
+    if r.dual_row is not None:
+        d["dual_row_head"] = [float(v) for v in r.dual_row[:8]]
+    return d
+
+
+def main():
+    oracle.build(reference=True)
+    lp = {}
+    for name, args in LP_SPECS:
+        mdl = build(name, args)
+        lp[f"{name}({','.join(map(str, args))})"] = dict(spec=[name, args], **summarize(oracle.solve(mdl, kind="reference")))
+        print("lp", name, args, lp[f"{name}({','.join(map(str, args))})"]["objective"], flush=True)
+    batch = P.transport_batch(**BATCH_SPEC)
+    lp["transport_batch"] = dict(spec=BATCH_SPEC, objectives=[], iterations=[], statuses=[])
+    for mdl in batch:
+        r = oracle.solve(mdl, kind="reference")
+        lp["transport_batch"]["objectives"].append(r.objective_value)
+        lp["transport_batch"]["iterations"].append(r.iterations)
+        lp["transport_batch"]["statuses"].append(r.status_name)
+    fam = P.MulticommodityFamily()
+    for s in MULTICOMMODITY_SEEDS:
+        mdl, _ = fam.instance_from_seed(s)
+        lp[f"multicommodity({s})"] = dict(spec=["multicommodity", [s]], **summarize(oracle.solve(mdl, kind="reference")))
+        print("mc", s, lp[f"multicommodity({s})"]["objective"], flush=True)
+    with open(os.path.join(HERE, "lp_reference.json"), "w") as f:
+        json.dump(lp, f, indent=1)
+
+    qp = {}
+    for name, args in QP_SPECS:
+        mdl = build(name, args)
+        key = f"{name}({','.join(map(str, args))})"
+        qp[key] = dict(spec=[name, args], **summarize(oracle.solve(mdl, qp=True, kind="reference")))
+        print("qp", key, qp[key]["objective"], flush=True)
+    with open(os.path.join(HERE, "qp_reference.json"), "w") as f:
+        json.dump(qp, f, indent=1)
+
+    if os.path.isdir(LISWET_DIR):
+        c = np.loadtxt(os.path.join(LISWET_DIR, "input_c.txt"))
+        x = np.loadtxt(os.path.join(LISWET_DIR, "x.txt"))
+        with open(os.path.join(LISWET_DIR, "independent.json")) as f:
+            ind = json.load(f)
+        obj = float(ind["independent"]["objective_qp"])
+        np.savez_compressed(os.path.join(HERE, "liswet_n20000.npz"), c=c, x=x, objective=obj)
+        print("liswet", len(c), obj)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,137 @@
+"""GPU parity: the B200 engine against the reference's own results (golden vectors made by the
+reference, tests/golden/make_golden.py) and against the oracle restatement on the same seeded
+inputs. Objectives must match to 1e-8 relative, with residuals at the reference's tolerance."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from sovereign_b200 import abi, problems as P
+from sovereign_b200.ipm import InteriorPointOptions, InteriorPointSolver, solve_batch
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+LP = json.load(open(os.path.join(GOLDEN, "lp_reference.json")))
+SINGLE = [k for k, v in LP.items() if isinstance(v.get("spec"), list) and v["spec"][0] != "multicommodity"]
+TOL = 1e-8  # relative objective tolerance
+
+
+def rel(a, b):
+    return abs(a - b) / max(1.0, abs(b))
+
+
+def model_of(spec):
+    name, args = spec
+    if name == "multicommodity":
+        return P.MulticommodityFamily().instance_from_seed(args[0])[0]
+    return getattr(P, name)(*args)
+
+
+@pytest.mark.parametrize("key", SINGLE + ["multicommodity(100)"])
+def test_fp64_matches_reference(key):
+    g = LP[key]
+    r = InteriorPointSolver().solve(model_of(g["spec"]), with_diag=True)
+    assert r.status_name == "OPTIMAL", r.message
+    assert rel(r.objective_value, g["objective"]) < TOL
+    assert r.primal_residual < 1e-9 and r.dual_residual < 1e-9 and r.duality_gap < 1e-9
+    # same algorithm in FP64: never more iterations than the reference (dependent rows are dropped
+    # exactly instead of being carried through a near-singular LU, which can cost it iterations)
+    assert r.iterations <= g["iterations"] + 1
+    assert "Normal equations" in r.message
+
+
+@pytest.mark.parametrize("key", ["transport(50,50,0)", "random_sparse_lp(200,1000,8,2)", "reference_transport(40)",
+                                 "multicommodity(101)"])
+def test_mixed_precision_matches_reference(key):
+    g = LP[key]
+    opts = InteriorPointOptions(precision=abi.PRECISION_MIXED)
+    r = InteriorPointSolver(opts).solve(model_of(g["spec"]), with_diag=True)
+    assert r.status_name == "OPTIMAL", r.message
+    assert rel(r.objective_value, g["objective"]) < TOL
+    assert r.diagnostics["pcg_iterations"] > 0
+
+
+def test_batch_matches_reference():
+    g = LP["transport_batch"]
+    models = P.transport_batch(**g["spec"])
+    res = solve_batch(models)
+    for k, r in enumerate(res):
+        assert r.status_name == "OPTIMAL", (k, r.message)
+        assert rel(r.objective_value, g["objectives"][k]) < TOL, k
+        assert r.iterations <= g["iterations"][k] + 1, k
+
+
+def test_batch_mixed_sizes_and_fallback():
+    # the batched kernel takes m <= 128; larger LPs in the same call go through the single engine
+    models = [P.transport(50, 50, 0), P.reference_staircase(8, 40), P.transport(10, 10, 3), P.bounded_lp_example()]
+    res = solve_batch(models)
+    for mdl, r in zip(models, res):
+        ref = oracle.solve(mdl, kind="restatement")
+        assert r.status_name == "OPTIMAL" and rel(r.objective_value, ref.objective_value) < TOL
+
+
+def test_batch_equals_single_engine_primal():
+    models = P.transport_batch(8, seed=9)
+    res = solve_batch(models)
+    for mdl, r in zip(models, res):
+        s = InteriorPointSolver().solve(mdl)
+        assert rel(r.objective_value, s.objective_value) < 1e-10
+        np.testing.assert_allclose(r.primal, s.primal, rtol=1e-6, atol=1e-6)
+
+
+def test_result_contract_matches_restatement():
+    mdl = P.bounded_lp_example()
+    r = InteriorPointSolver().solve(mdl, with_diag=True)
+    o = oracle.solve(mdl, kind="restatement", with_diag=True)
+    assert r.status == o.status and rel(r.objective_value, o.objective_value) < TOL
+    np.testing.assert_allclose(r.primal, o.primal, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(r.dual_row, o.dual_row, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(r.dual_col, o.dual_col, rtol=1e-5, atol=1e-6)
+    assert r.diagnostics["scaling_applied"] and r.diagnostics["history_iterations"][:3] == [1, 2, 3]
+    assert r.diagnostics["coefficient_max_abs_after"] == pytest.approx(o.diagnostics["coefficient_max_abs_after"])
+
+
+def test_iteration_limit_returns_best_candidate():
+    mdl = P.reference_transport(30)
+    r = InteriorPointSolver(InteriorPointOptions(max_iterations=1, optimality_tol=1e-14)).solve(mdl)
+    o = oracle.solve(mdl, kind="restatement", max_iterations=1)
+    assert r.status == o.status and r.status_name in ("FEASIBLE", "NUMERICAL_ERROR")
+    assert r.has_objective_value and "Optimality is not proven" in r.message
+    assert rel(r.objective_value, o.objective_value) < 1e-6
+
+
+def test_inconsistent_bounds_and_degenerate_models():
+    bad = P.bounded_lp_example()
+    bad.ub = bad.ub.copy()
+    bad.ub[0] = 0.0
+    r = InteriorPointSolver().solve(bad)
+    assert r.status_name == "ERROR" and r.message.startswith("IPM error: Inconsistent bounds")
+    # no constraints: x at its lower bounds (interior_point.cpp:464-478)
+    free = P.bounded_lp_example()
+    free.m = 0
+    free.rhs = np.zeros(0)
+    free.sense = np.zeros(0, dtype=np.int8)
+    free.col_ptr = np.zeros(free.n + 1, dtype=np.int32)
+    free.row_idx = np.zeros(0, dtype=np.int32)
+    free.values = np.zeros(0)
+    free.ub = np.full(free.n, 1e30)
+    r = InteriorPointSolver().solve(free)
+    assert r.status_name == "OPTIMAL" and r.message == "Optimal (no constraints) via IPM path."
+    np.testing.assert_allclose(r.primal, free.lb)
+
+
+def test_dependent_rows_are_dropped():
+    # balanced transport has a redundant equality row: the normal matrix is singular
+    from sovereign_b200.ipm import normal_factor_solve
+    mdl = P.reference_transport(12)
+    # with weights 100 the dependent direction's pivot (~1e-12 shift plus rounding) sits far below
+    # the relative threshold 1e-13 * diag ~ 1.2e-10, so the rule must drop exactly one row
+    d = np.full(mdl.n, 100.0)
+    rhs = mdl.dense_A() @ np.random.default_rng(1).standard_normal(mdl.n)
+    z, dropped = normal_factor_solve(mdl.m, mdl.n, mdl.col_ptr, mdl.row_idx, mdl.values, d, rhs)
+    assert dropped == 1
+    A = mdl.dense_A()
+    Mm = A @ np.diag(d) @ A.T
+    np.testing.assert_allclose(Mm @ z, rhs, rtol=1e-8, atol=1e-7 * np.abs(rhs).max())
