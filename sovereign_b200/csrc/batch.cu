@@ -116,30 +116,42 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   int drops = 0, fail = 0;
 
   // ---- assembly of M = A diag(d) A' + 1e-12 I (mode 0: d = x/s, mode 2: d = 1) ----
-  // Thread i owns row i of the lower triangle: M[i][r] = sum over k in row i of
-  // a_ik d_k a_rk for every r <= i in column k (no atomics, fixed summation order).
+  // Warp per row i of the lower triangle, lanes over the row's entries a_ik: the diagonal term
+  // sum_k a_ik^2 d_k is a warp sum; the off-diagonal terms a_ik d_k a_rk (r < i in column k) are
+  // added into shared memory (one term per (i, r) when rows share a single column, as in
+  // transportation LPs, so the sum order is then fixed).
   auto assemble = [&](int mode) {
     for (int i = tid; i < m * ld; i += NT) M[i] = 0.0;
     __syncthreads();
-    for (int i = tid; i < m; i += NT) {
+    for (int i = warp; i < m; i += NW) {
       double* Mi = M + i * ld;
-      for (int p = rpp[i]; p < rpp[i + 1]; ++p) {
+      double dsum = 0.0;
+      for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) {
         const int k = ci[p];
         const double dk = mode == 2 ? 1.0 : fmax(x[k], 1e-16) / fmax(s[k], 1e-16);
-        const double ad = rv[p] * dk;
+        const double a = rv[p];
         for (int q = cp[k]; q < cp[k + 1]; ++q) {
           const int r = ri[q];
-          if (r <= i) Mi[r] += ad * cv[q];
+          if (r < i) atomicAdd(Mi + r, a * dk * cv[q]);
         }
+        dsum += a * a * dk;
       }
-      Mi[i] += 1e-12;
-      vdiag[i] = Mi[i];
+      dsum = warp_sum(dsum);
+      if (lane == 0) {
+        Mi[i] = dsum + 1e-12;
+        vdiag[i] = Mi[i];
+      }
     }
     __syncthreads();
   };
 
   // ---- in-place L D L' (L~ = L D kept unscaled below the diagonal; vinv = 1/D) ----
+  // Per column k one barrier; the trailing update M[i][j] -= M[i][k] M[j][k] / D_k (k < j <= i)
+  // is spread over a TY x TX thread grid (row i = k+1+ty (mod TY), column j = k+1+tx (mod TX)),
+  // so every thread issues independent shared-memory updates.
   auto factor = [&]() {
+    constexpr int TX = 16, TY = NT / 16;
+    const int tx = tid % TX, ty = tid / TX;
     for (int k = 0; k < m; ++k) {
       const double p = M[k * ld + k];
       const double dref = vdiag[k];
@@ -155,9 +167,10 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       }
       const double inv = 1.0 / Dk;
       if (tid == 0) vinv[k] = inv;
-      for (int i = k + 1 + warp; i < m; i += NW) {
+      for (int i = k + 1 + ty; i < m; i += TY) {
         const double lik = M[i * ld + k] * inv;
-        for (int j = k + 1 + lane; j <= i; j += 32) M[i * ld + j] -= lik * M[j * ld + k];
+        double* Mi = M + i * ld;
+        for (int j = k + 1 + tx; j <= i; j += TX) Mi[j] -= lik * M[j * ld + k];
       }
       __syncthreads();
     }
@@ -512,6 +525,16 @@ struct Batch {
   int launches = 0;
   double kernel_ms = 0.0, bytes = 0.0, flops = 0.0;
   double h2d_bytes = 0.0, d2h_bytes = 0.0;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  ~Batch() {
+    for (auto s : streams) cudaStreamDestroy(s);
+    for (auto e : joins) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+  }
 };
 
 namespace {
@@ -680,26 +703,42 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
 }
 
 void batch_solve(Batch* B, cudaStream_t st) {
-  cudaEvent_t e0, e1;
-  SOV_CUDA(cudaEventCreate(&e0));
-  SOV_CUDA(cudaEventCreate(&e1));
-  SOV_CUDA(cudaEventRecord(e0, st));
+  // Buckets run concurrently: each on its own stream forked from (and joined back into) the
+  // caller's stream, so the few large LPs do not hold the SMs the smaller buckets could use.
+  if (B->streams.empty()) {
+    for (size_t b = 0; b < B->buckets.size(); ++b) {
+      cudaStream_t s2;
+      SOV_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+      B->streams.push_back(s2);
+      cudaEvent_t ev;
+      SOV_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      B->joins.push_back(ev);
+    }
+    SOV_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+    SOV_CUDA(cudaEventCreate(&B->t0));
+    SOV_CUDA(cudaEventCreate(&B->t1));
+  }
+  SOV_CUDA(cudaEventRecord(B->t0, st));
+  SOV_CUDA(cudaEventRecord(B->fork, st));
   int launches = 0;
-  for (auto& bk : B->buckets) {
-    SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), st));
+  for (size_t b = 0; b < B->buckets.size(); ++b) {
+    auto& bk = B->buckets[b];
+    cudaStream_t s2 = B->streams[b];
+    SOV_CUDA(cudaStreamWaitEvent(s2, B->fork, 0));
+    SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), s2));
     BatchDev d = B->dev;
     d.order = bk->order.p;
     d.count = bk->count;
     d.next = bk->next.p;
-    launch_any(d, bk->mmax, bk->threads, bk->grid, st);
+    launch_any(d, bk->mmax, bk->threads, bk->grid, s2);
+    SOV_CUDA(cudaEventRecord(B->joins[b], s2));
+    SOV_CUDA(cudaStreamWaitEvent(st, B->joins[b], 0));
     ++launches;
   }
-  SOV_CUDA(cudaEventRecord(e1, st));
-  SOV_CUDA(cudaEventSynchronize(e1));
+  SOV_CUDA(cudaEventRecord(B->t1, st));
+  SOV_CUDA(cudaEventSynchronize(B->t1));
   float ms = 0.f;
-  SOV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  SOV_CUDA(cudaEventElapsedTime(&ms, B->t0, B->t1));
   B->launches = launches;
   B->kernel_ms = ms;
 }
