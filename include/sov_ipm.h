@@ -229,6 +229,23 @@ int sov_normal_factor_solve(int32_t m, int32_t n, const int32_t* col_ptr, const 
                             int32_t factorization, double* rhs, int32_t nrhs,
                             int32_t* dropped_pivots);
 
+/* No counterpart in the reference. For callers that cannot let the library allocate device
+ * memory (applications that own all device memory through their own pool, or run close to the
+ * memory limit): the dense FP64 factor of A diag(d) A' + 1e-12 I and the solve for nrhs
+ * right-hand sides, like sov_normal_factor_solve, but col_ptr, row_idx, values, d and rhs
+ * (column-major m x nrhs, overwritten by the solution) are DEVICE pointers, rows within a column
+ * must be distinct, and the work runs on cuda_stream. It calls no cudaMalloc or cudaFree: its
+ * working storage is one fixed device array sized for m <= SOV_NOALLOC_MAX_ROWS (about 2.3 MB,
+ * held by every GPU that loads the library until the process exits); larger m returns
+ * SOV_E_TOO_LARGE. The first call on a device looks that array up (cudaGetSymbolAddress), so it
+ * should come before any stream capture on that device. Calls share the array: two calls whose
+ * work overlaps on the GPU race and must be ordered by the caller. The call returns after the
+ * stream has finished this work; dropped_pivots is a host pointer (or NULL). */
+#define SOV_NOALLOC_MAX_ROWS 512
+int sov_normal_factor_solve_noalloc(int32_t m, int32_t n, const int32_t* col_ptr, const int32_t* row_idx,
+                                    const double* values, const double* d, double* rhs, int32_t nrhs,
+                                    int32_t* dropped_pivots, void* cuda_stream);
+
 /* Device name, SM count, memory; returns SOV_E_NO_DEVICE when no usable sm_100 GPU exists. */
 int sov_device_info(char* buf, int32_t len);
 

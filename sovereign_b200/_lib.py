@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsovipm.s
 EXPORTS = [
     "sov_default_lp_options", "sov_default_qp_options", "sov_ipm_dims", "sov_lp_solve", "sov_qp_solve",
     "sov_lp_solve_batch", "sov_batch_create", "sov_batch_solve", "sov_batch_results", "sov_batch_stats",
-    "sov_batch_transfer_bytes", "sov_batch_destroy", "sov_autotune", "sov_spmv_csc", "sov_normal_factor_solve", "sov_device_info",
+    "sov_batch_transfer_bytes", "sov_batch_destroy", "sov_autotune", "sov_spmv_csc", "sov_normal_factor_solve", "sov_normal_factor_solve_noalloc", "sov_device_info",
     "sov_last_error",
 ]
 
@@ -60,6 +60,9 @@ def load(build_if_missing: bool = True):
                                  C.c_void_p, C.c_int32]
     lib.sov_normal_factor_solve.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+    lib.sov_normal_factor_solve_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                                    C.c_void_p]
     lib.sov_device_info.argtypes = [C.c_char_p, C.c_int32]
     lib.sov_last_error.restype = C.c_char_p
     _lib = lib
