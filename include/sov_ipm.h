@@ -74,7 +74,10 @@ enum {
 enum {
   SOV_FACTOR_AUTO = 0,   /* banded when the bandwidth is small, else dense */
   SOV_FACTOR_DENSE = 1,  /* dense m x m Cholesky (dense-Schur) */
-  SOV_FACTOR_BANDED = 2  /* banded LDL^T in the natural row order */
+  SOV_FACTOR_BANDED = 2, /* banded LDL^T in the natural row order */
+  SOV_FACTOR_XSPACE = 3  /* QP only: eliminate the slacks and factor Q + H + A'ZW^-1A over the structural
+                            columns (rows must all be inequalities, Q_jj > 0); exact Newton step, but
+                            with FP64 iterates it stalls once slack weights exceed ~1e12 */
 };
 
 /* One LP or convex QP in index form.
@@ -126,7 +129,10 @@ typedef struct sov_options {
   /* Mixed precision: cap on FP64 PCG iterations per Newton solve before the engine refactors in
    * FP64 for that iteration. */
   int32_t pcg_max_iterations;
-  int32_t reserved;
+  /* 0: sov_result.ipm_x/y/s receive the final iterate; k >= 1: the iterate at the start of
+   * iteration k (k = 1 is the starting point), or the final one if the solve ends earlier. A point
+   * on the central path's early stretch is the training target of the learned warm start. */
+  int32_t ipm_iterate_at;
 } sov_options;
 
 /* Per-solve diagnostics (the fields of sovereign::LpDiagnostics, types.hpp:64-89, that the IPM
@@ -245,6 +251,24 @@ int sov_normal_factor_solve(int32_t m, int32_t n, const int32_t* col_ptr, const 
 int sov_normal_factor_solve_noalloc(int32_t m, int32_t n, const int32_t* col_ptr, const int32_t* row_idx,
                                     const double* values, const double* d, double* rhs, int32_t nrhs,
                                     int32_t* dropped_pivots, void* cuda_stream);
+
+/* Warm-start network (no counterpart in the reference): an MLP n_in -> hidden x hidden_layers
+ * (ReLU) -> n_out with FP32 master weights and BF16 tensor-core products (FP32 accumulate),
+ * trained with Adam on mean-squared error. Parameters are laid out layer by layer as W (out x in,
+ * row-major) then b. Host buffers in and out; row-major batches. */
+typedef struct sov_mlp sov_mlp;
+int sov_mlp_create(int32_t n_in, int32_t hidden, int32_t hidden_layers, int32_t n_out, uint64_t seed,
+                   sov_mlp** out);
+int64_t sov_mlp_param_count(const sov_mlp* mlp);
+int sov_mlp_get_params(const sov_mlp* mlp, float* params, int64_t count);
+int sov_mlp_set_params(sov_mlp* mlp, const float* params, int64_t count);
+int sov_mlp_forward(sov_mlp* mlp, const float* x, int32_t batch, float* y);
+/* loss = mean((f(x) - t)^2); grad (param_count floats, or NULL) = its gradient */
+int sov_mlp_loss_grad(sov_mlp* mlp, const float* x, const float* t, int32_t batch, double* loss, float* grad);
+/* epochs of shuffled mini-batches over count samples; final_loss = mean loss of the last epoch */
+int sov_mlp_train(sov_mlp* mlp, const float* x, const float* t, int32_t count, int32_t epochs, int32_t batch,
+                  float lr, uint64_t seed, double* final_loss);
+void sov_mlp_destroy(sov_mlp* mlp);
 
 /* Device name, SM count, memory; returns SOV_E_NO_DEVICE when no usable sm_100 GPU exists. */
 int sov_device_info(char* buf, int32_t len);

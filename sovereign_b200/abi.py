@@ -17,7 +17,7 @@ STATUS_NAMES = ["OPTIMAL", "FEASIBLE", "INFEASIBLE", "UNBOUNDED", "TIME_LIMIT", 
 # sovereign::ConstraintSense (types.hpp:12)
 LE, GE, EQ = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-FACTOR_AUTO, FACTOR_DENSE, FACTOR_BANDED = 0, 1, 2
+FACTOR_AUTO, FACTOR_DENSE, FACTOR_BANDED, FACTOR_XSPACE = 0, 1, 2, 3
 HISTORY_MAX = 128
 
 _dp = C.POINTER(C.c_double)
@@ -41,7 +41,7 @@ class SovOptions(C.Structure):
         ("fraction_to_boundary", C.c_double),
         ("precision", C.c_int32), ("factorization", C.c_int32),
         ("warm_x", _dp), ("warm_y", _dp), ("warm_s", _dp),
-        ("pcg_max_iterations", C.c_int32), ("reserved", C.c_int32),
+        ("pcg_max_iterations", C.c_int32), ("ipm_iterate_at", C.c_int32),
     ]
 
 

@@ -32,6 +32,7 @@ __device__ __forceinline__ double column_weight(int mode, int k, const double* x
   if (mode == kWeightOnes) return 1.0;
   const double xk = fmax(x[k], 1e-16), sk = fmax(s[k], 1e-16);
   if (mode == kWeightLp) return xk / sk;
+  if (mode == kWeightTheta) return sk / xk;
   const double h = free_col[k] ? 0.0 : sk / xk;
   return 1.0 / (qdiag[k] + h);
 }
@@ -88,65 +89,98 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Diagonal block: unblocked Cholesky in shared memory (64 threads, thread i owns row i) and the
-// inverse of the resulting lower-triangular block (thread c owns column c).
+// Diagonal block (64 x 64) on 256 threads, in four 16-column sub-panels: warp 0 factors the 16 x 16
+// diagonal sub-block warp-synchronously (the pivot rule per column), each row below is solved
+// against it by one thread, and all threads update the trailing lower part. Then the inverse of the
+// 64 x 64 factor, four threads per column (shuffle-reduced dot products).
 // ---------------------------------------------------------------------------------------------
+constexpr int kSub = 16;
+
 template <class T>
-__global__ void __launch_bounds__(64) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
-                                                   int m, T* __restrict__ Linv, int* drop_count, int* fail,
-                                                   double drop_tol) {
+__global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
+                                                    int m, T* __restrict__ Linv, int* drop_count, int* fail,
+                                                    double drop_tol) {
   extern __shared__ __align__(16) unsigned char potrf_raw[];
   T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
   T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = kb * kNB;
-  for (int idx = tid; idx < kNB * kNB; idx += kNB) {
+  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
     const int c = idx / kNB, r = idx % kNB;
     A[r][c] = r >= c ? M[static_cast<int64_t>(r0 + c) * ld + r0 + r] : T(0);
   }
+  __syncthreads();
   int drops = 0, bad = 0;
-  const int i = tid;
-  for (int j = 0; j < kNB; ++j) {
-    __syncthreads();
-    const T p = A[j][j];
-    const int gj = r0 + j;
-    const double dref = gj < m ? diag[gj] : 1.0;
-    bool drop = false;
-    if (!isfinite(static_cast<double>(p))) {
-      bad = 1;
-      drop = true;
-    } else if (static_cast<double>(p) <= drop_tol * fabs(dref)) {
-      drop = true;
+  for (int k0 = 0; k0 < kNB; k0 += kSub) {
+    // 1. factor A[k0:k0+16, k0:k0+16] (warp 0; lane i owns row k0 + i)
+    if (warp == 0) {
+      for (int j = k0; j < k0 + kSub; ++j) {
+        __syncwarp();
+        const T p = A[j][j];
+        const int gj = r0 + j;
+        const double dref = gj < m ? diag[gj] : 1.0;
+        bool drop = false;
+        if (!isfinite(static_cast<double>(p))) {
+          bad = 1;
+          drop = true;
+        } else if (static_cast<double>(p) <= drop_tol * fabs(dref)) {
+          drop = true;  // dependent row (sparse_ldlt.cpp:165-173)
+        }
+        const T ljj = drop ? big_pivot<T>() : sqrt(p);
+        if (drop && gj < m) ++drops;
+        __syncwarp();
+        const int i = k0 + lane;
+        if (lane < kSub) {
+          if (i == j) A[j][j] = ljj;
+          if (i > j) A[i][j] = A[i][j] / ljj;
+        }
+        __syncwarp();
+        if (lane < kSub && i > j) {
+          const T lij = A[i][j];
+          for (int k = j + 1; k <= i; ++k) A[i][k] -= lij * A[k][j];
+        }
+      }
     }
-    const T ljj = drop ? big_pivot<T>() : sqrt(p);
-    if (drop && gj < m) ++drops;
     __syncthreads();
-    if (i == j) A[j][j] = ljj;
-    if (i > j) A[i][j] = A[i][j] / ljj;
-    __syncthreads();
-    if (i > j) {
-      const T lij = A[i][j];
-      for (int k = j + 1; k <= i; ++k) A[i][k] -= lij * A[k][j];
+    const int rest = kNB - (k0 + kSub);
+    if (rest <= 0) break;
+    // 2. rows below: L[i][k0:k0+16] = A[i][k0:k0+16] L_kk^-T (forward substitution, one row per thread)
+    if (tid < rest) {
+      const int i = k0 + kSub + tid;
+      for (int c = k0; c < k0 + kSub; ++c) {
+        T v = A[i][c];
+        for (int k = k0; k < c; ++k) v -= A[i][k] * A[c][k];
+        A[i][c] = v / A[c][c];
+      }
     }
-  }
-  __syncthreads();
-  // inverse, column c by forward substitution on e_c
-  const int c = tid;
-  for (int r = 0; r < kNB; ++r) {
-    T v;
-    if (r < c) {
-      v = T(0);
-    } else if (r == c) {
-      v = T(1) / A[r][r];
-    } else {
+    __syncthreads();
+    // 3. trailing update A[i][j] -= sum_k L[i][k] L[j][k] over the sub-panel, k0+16 <= j <= i
+    const int tot = rest * rest;
+    for (int t = tid; t < tot; t += blockDim.x) {
+      const int i = k0 + kSub + t / rest, j = k0 + kSub + t % rest;
+      if (j > i) continue;
       T acc = T(0);
-      for (int k = c; k < r; ++k) acc += A[r][k] * I[k][c];
-      v = -acc / A[r][r];
+#pragma unroll
+      for (int k = 0; k < kSub; ++k) acc += A[i][k0 + k] * A[j][k0 + k];
+      A[i][j] -= acc;
     }
-    I[r][c] = v;
+    __syncthreads();
+  }
+  // inverse, column c by forward substitution on e_c; 4 threads per column split each dot product
+  {
+    const int c = tid >> 2, part = tid & 3;
+    for (int r = 0; r < kNB; ++r) {
+      T acc = T(0);
+      if (r > c)
+        for (int k = c + part; k < r; k += 4) acc += A[r][k] * I[k][c];
+      acc += __shfl_xor_sync(kFull, acc, 1);
+      acc += __shfl_xor_sync(kFull, acc, 2);
+      if (part == 0) I[r][c] = r < c ? T(0) : (r == c ? T(1) / A[r][r] : -acc / A[r][r]);
+      __syncwarp();
+    }
   }
   __syncthreads();
-  for (int idx = tid; idx < kNB * kNB; idx += kNB) {
+  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
     const int cc = idx / kNB, r = idx % kNB;
     if (r >= cc) M[static_cast<int64_t>(r0 + cc) * ld + r0 + r] = A[r][cc];
     Linv[static_cast<int64_t>(kb) * kNB * kNB + idx] = I[r][cc];
@@ -241,7 +275,7 @@ void dense_potrf_block(const DenseSystem<T>& s, int kb, cudaStream_t st) {
     SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
     attr_set = true;
   }
-  k_potrf_diag<T><<<1, kNB, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
+  k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
 }
 
 template <class T>
@@ -257,7 +291,7 @@ void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
   }
   int n = 0;
   for (int kb = 0; kb < s.nb; ++kb) {
-    k_potrf_diag<T><<<1, kNB, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
+    k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
     ++n;
     const int R = s.nb - kb - 1;
     if (R > 0) {

@@ -170,6 +170,8 @@ class Engine {
   DevBuf<double> rval_, cval_, b_, c_, qdiag_;
   DevBuf<uint8_t> free_;
   DevBuf<double> x_, y_, s_, dx_, ds_, dxa_, dsa_, rp_, rd_, z_, bx_, by_, bs_;
+  DevBuf<double> cx_, cy_, cs_;  // iterate captured at the start of iteration opt_.ipm_iterate_at
+  bool captured_ = false;
   DevBuf<double> partials_;
   DevBuf<unsigned> counter_;
   DevBuf<IpmScalars> sc_;
@@ -200,6 +202,12 @@ class Engine {
   DevBuf<PcgScalars> pcg_s_;
   PcgScalars* pcg_h_ = nullptr;
   int pcg_iterations_ = 0, fp64_fallbacks_ = 0, factorizations_ = 0;
+  // x-space QP
+  XSpace xs_;
+  bool xspace_ = false;
+  int order_ = 0;  // order of the factored system: m (y-space) or structural columns (x-space)
+  DevBuf<int> slack_of_row_;
+  DevBuf<double> sigma_, tr_, dyv_;
 };
 
 void Engine::setup() {
@@ -236,34 +244,42 @@ void Engine::setup() {
   err_.alloc(1);
   err_.zero(st_);
 
+  // x-space for QPs whose rows all carry slacks and whose structural columns have Q_jj > 0
+  xs_ = analyze_xspace(f_);
+  if (opt_.factorization == SOV_FACTOR_XSPACE && !(f_.qp && xs_.eligible))
+    throw std::runtime_error("x-space factorization needs a QP whose rows are all inequalities and whose structural "
+                             "columns all have Q_jj > 0");
+  xspace_ = opt_.factorization == SOV_FACTOR_XSPACE;
+  order_ = xspace_ ? f_.n_struct : m;
   // backend choice: band when the half-bandwidth is small, else dense (mixed or FP64)
-  kd_ = normal_bandwidth(f_);
-  const bool want_band = opt_.factorization == SOV_FACTOR_BANDED ||
-                         (opt_.factorization == SOV_FACTOR_AUTO && kd_ <= kBandMax && m > 256);
+  kd_ = xspace_ ? xs_.kd : normal_bandwidth(f_);
+  const bool auto_pick = opt_.factorization == SOV_FACTOR_AUTO || opt_.factorization == SOV_FACTOR_XSPACE;
+  const bool want_band = opt_.factorization == SOV_FACTOR_BANDED || (auto_pick && kd_ <= kBandMax && order_ > 256);
   if (want_band) {
     if (kd_ > kBandMax) throw std::runtime_error("banded factorization requested but half-bandwidth " +
                                                  std::to_string(kd_) + " exceeds " + std::to_string(kBandMax));
     backend_ = kBand;
   } else {
-    if (m > 16384) throw std::runtime_error("normal matrix of order " + std::to_string(m) +
-                                            " is too large for the dense factorization (band width " +
-                                            std::to_string(kd_) + ")");
-    backend_ = opt_.precision == SOV_PRECISION_MIXED ? kDenseMixed : kDense64;
+    if (order_ > 16384) throw std::runtime_error("normal matrix of order " + std::to_string(order_) +
+                                                 " is too large for the dense factorization (band width " +
+                                                 std::to_string(kd_) + ")");
+    // the x-space system has no matrix-free PCG operator: it is factored in FP64
+    backend_ = (opt_.precision == SOV_PRECISION_MIXED && !xspace_) ? kDenseMixed : kDense64;
   }
   if (backend_ == kBand) {
-    am_ = build_assembly_band(f_, kd_);
-    band_.alloc(static_cast<size_t>(kBandMax + 1) * m);
+    am_ = xspace_ ? build_assembly_xspace_band(f_, xs_) : build_assembly_band(f_, kd_);
+    band_.alloc(static_cast<size_t>(kBandMax + 1) * order_);
     band_.zero(st_);
-    dinv_.alloc(m);
-    diag_.alloc(m);
-    z_.alloc(m);
+    dinv_.alloc(order_);
+    diag_.alloc(order_);
+    z_.alloc(order_);
     z_.zero(st_);
-    bandsys_ = BandSystem{band_.p, dinv_.p, diag_.p, m, kd_, nullptr, nullptr};
+    bandsys_ = BandSystem{band_.p, dinv_.p, diag_.p, order_, kd_, nullptr, nullptr};
   } else {
-    nb_ = ceil_div(m, kNB);
+    nb_ = ceil_div(order_, kNB);
     mp_ = nb_ * kNB;
-    am_ = build_assembly_dense(f_, mp_);
-    diag_.alloc(m);
+    am_ = xspace_ ? build_assembly_xspace(f_, xs_, mp_) : build_assembly_dense(f_, mp_);
+    diag_.alloc(order_);
     flags_.alloc(nb_);
     flags_.zero(st_);
     z_.alloc(mp_);
@@ -279,6 +295,14 @@ void Engine::setup() {
       pcg_s_.alloc(1);
       SOV_CUDA(cudaMallocHost(&pcg_h_, sizeof(PcgScalars)));
     }
+  }
+  if (xspace_) {
+    slack_of_row_.alloc(m);
+    slack_of_row_.upload(xs_.slack_of_row.data(), m, st_);
+    sigma_.alloc(m);
+    sigma_.upload(xs_.sigma.data(), m, st_);
+    tr_.alloc(m);
+    dyv_.alloc(m);
   }
   am_target_.alloc(am_.target.size());
   am_target_.upload(am_.target.data(), am_.target.size(), st_);
@@ -299,7 +323,7 @@ void Engine::setup() {
     bandsys_.drop_count = drop_ptr;
     bandsys_.fail = fail_ptr;
   } else {
-    ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, m, mp_, nb_, drop_ptr, fail_ptr, flags_.p, 1e-6};
+    ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, order_, mp_, nb_, drop_ptr, fail_ptr, flags_.p, 1e-6};
   }
 
   dev_.m = m;
@@ -336,6 +360,12 @@ void Engine::setup() {
   dev_.rp = rp_.p;
   dev_.rd = rd_.p;
   dev_.z = z_.p;
+  dev_.dy = xspace_ ? dyv_.p : z_.p;
+  dev_.xspace = xspace_ ? 1 : 0;
+  dev_.nx = f_.n_struct;
+  dev_.slack_of_row = slack_of_row_.p;
+  dev_.sigma = sigma_.p;
+  dev_.tr = tr_.p;
   dev_.sc = sc_.p;
   dev_.partials = partials_.p;
   dev_.counter = counter_.p;
@@ -346,13 +376,16 @@ void Engine::assemble_and_factor(int mode) {
   const double reg = 1e-12;  // kNormalEqRegularization (interior_point.cpp:103)
   ++factorizations_;
   fp64_ready_ = false;
+  // x-space: K = A_x' Theta A_x (+ diag Q + H after assembly); start system: Theta = 1, diag 1
+  const int amode = xspace_ ? (mode == kWeightOnes ? kWeightOnes : kWeightTheta) : mode;
   if (backend_ == kBand) {
-    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, band_.p, diag_.p, f_.m, -f_.m, st_);
+    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, amode, reg, band_.p, diag_.p, order_, -order_, st_);
+    if (xspace_) launch_xspace_diag(dev_, mode == kWeightOnes ? 0 : 1, band_.p, -1, diag_.p, st_);
     band_factor(bandsys_, st_, &launches_);
-    launches_ += 1;
+    launches_ += xspace_ ? 2 : 1;
     if (stats_) {
       const double kd = kd_;
-      stats_->factor_flops += f_.m * (kd * kd + 2.0 * kd);
+      stats_->factor_flops += order_ * (kd * kd + 2.0 * kd);
     }
     return;
   }
@@ -360,12 +393,13 @@ void Engine::assemble_and_factor(int mode) {
     if (!M64_.p) {
       M64_.alloc(static_cast<size_t>(mp_) * mp_);
       Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
-      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, f_.m, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
+      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
     }
-    launch_dense_clear<double>(M64_.p, f_.m, mp_, st_);
-    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, M64_.p, diag_.p, f_.m, mp_, st_);
+    launch_dense_clear<double>(M64_.p, order_, mp_, st_);
+    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, amode, reg, M64_.p, diag_.p, order_, mp_, st_);
+    if (xspace_) launch_xspace_diag(dev_, mode == kWeightOnes ? 0 : 1, M64_.p, mp_, diag_.p, st_);
     dense_cholesky<double>(ds64_, st_, &launches_);
-    launches_ += 2;
+    launches_ += xspace_ ? 3 : 2;
     fp64_ready_ = true;
   } else {
     launch_dense_clear<float>(M32_.p, f_.m, mp_, st_);
@@ -373,7 +407,7 @@ void Engine::assemble_and_factor(int mode) {
     dense_cholesky_tc(ds32_, err_.p, st_, &launches_);
     launches_ += 2;
   }
-  if (stats_) stats_->factor_flops += (2.0 / 3.0) * std::pow(static_cast<double>(f_.m), 3.0);
+  if (stats_) stats_->factor_flops += (2.0 / 3.0) * std::pow(static_cast<double>(order_), 3.0);
 }
 
 bool Engine::newton_solve() {
@@ -421,7 +455,7 @@ bool Engine::newton_solve() {
     if (!M64_.p) {
       M64_.alloc(static_cast<size_t>(mp_) * mp_);
       Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
-      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, f_.m, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
+      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
     }
     launch_dense_clear<double>(M64_.p, f_.m, mp_, st_);
     launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, last_mode_, reg, M64_.p, diag_.p, f_.m, mp_, st_);
@@ -439,10 +473,11 @@ void Engine::read_scalars() {
 
 std::string Engine::describe() const {
   char buf[256];
+  const char* space = xspace_ ? "x-space Q + A'ZW^-1A, " : "";
   if (backend_ == kBand)
-    std::snprintf(buf, sizeof buf, "banded LDL^T on the GPU (order %d, half-bandwidth %d)", f_.m, kd_);
+    std::snprintf(buf, sizeof buf, "%sbanded LDL^T on the GPU (order %d, half-bandwidth %d)", space, order_, kd_);
   else if (backend_ == kDense64)
-    std::snprintf(buf, sizeof buf, "dense Cholesky on the GPU, FP64 (%d x %d)", f_.m, f_.m);
+    std::snprintf(buf, sizeof buf, "%sdense Cholesky on the GPU, FP64 (%d x %d)", space, order_, order_);
   else
     std::snprintf(buf, sizeof buf,
                   "dense Cholesky on the GPU, FP32 preconditioned FP64 PCG (%d x %d, %d PCG iterations, %d FP64 "
@@ -489,9 +524,15 @@ void Engine::publish(const DevBuf<double>& x, const DevBuf<double>& y, const Dev
     if (r->dual_col) std::copy(hs.begin(), hs.begin() + f_.n_struct, r->dual_col);
     if (r->dual_row) std::copy(hy.begin(), hy.begin() + f_.m0, r->dual_row);
   }
-  if (r->ipm_x) std::copy(hx.begin(), hx.end(), r->ipm_x);
-  if (r->ipm_y) std::copy(hy.begin(), hy.end(), r->ipm_y);
-  if (r->ipm_s) std::copy(hs.begin(), hs.end(), r->ipm_s);
+  if (captured_) {
+    if (r->ipm_x) SOV_CUDA(cudaMemcpy(r->ipm_x, cx_.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (r->ipm_y) SOV_CUDA(cudaMemcpy(r->ipm_y, cy_.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
+    if (r->ipm_s) SOV_CUDA(cudaMemcpy(r->ipm_s, cs_.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  } else {
+    if (r->ipm_x) std::copy(hx.begin(), hx.end(), r->ipm_x);
+    if (r->ipm_y) std::copy(hy.begin(), hy.end(), r->ipm_y);
+    if (r->ipm_s) std::copy(hs.begin(), hs.end(), r->ipm_s);
+  }
   r->objective_value = obj;
   std::snprintf(r->message, sizeof(r->message), "%s", msg.c_str());
 }
@@ -518,8 +559,10 @@ void Engine::run(sov_result* r) {
 
   // starting point (interior_point.cpp:488-506 / qp_interior_point.cpp:2881-2950, default start)
   assemble_and_factor(kWeightOnes);
-  launch_start_rhs(dev_, st_, &launches_);
+  if (xspace_) launch_start_rhs_x(dev_, st_, &launches_);
+  else launch_start_rhs(dev_, st_, &launches_);
   newton_solve();
+  if (xspace_) launch_start_dy_x(dev_, st_, &launches_);
   launch_start_point(dev_, st_, &launches_);
   bool warm_used = false;
   if (opt_.warm_x && opt_.warm_y && opt_.warm_s) {
@@ -535,7 +578,10 @@ void Engine::run(sov_result* r) {
     s_.upload(opt_.warm_s, n, st_);
     launch_residuals(dev_, st_, &launches_);
     read_scalars();
-    if (std::isfinite(hs_.h->metric) && hs_.h->metric < default_metric && hs_.h->mu < default_mu) {
+    // safeguard against gross mispredictions: keep the supplied point unless its residual metric
+    // is more than 10x the default start's (its mu is normally far smaller)
+    if (std::isfinite(hs_.h->metric) && std::isfinite(hs_.h->mu) && hs_.h->metric <= 10.0 * default_metric &&
+        hs_.h->mu <= default_mu) {
       warm_used = true;
     } else {
       SOV_CUDA(cudaMemcpyAsync(x_.p, bx_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
@@ -555,6 +601,15 @@ void Engine::run(sov_result* r) {
   std::string fail_msg;
   int it = 0;
   for (; it < opt_.max_iterations; ++it) {
+    if (opt_.ipm_iterate_at == it + 1) {
+      cx_.alloc(n);
+      cy_.alloc(m);
+      cs_.alloc(n);
+      SOV_CUDA(cudaMemcpyAsync(cx_.p, x_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(cs_.p, s_.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(cy_.p, y_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
+      captured_ = true;
+    }
     launch_residuals(dev_, st_, &launches_);
     read_scalars();
     const IpmScalars s = *hs_.h;
@@ -618,12 +673,13 @@ void Engine::run(sov_result* r) {
       break;
     }
     assemble_and_factor(f_.qp ? kWeightQp : kWeightLp);
-    launch_newton_rhs(dev_, kRhsAffine, st_, &launches_);
-    newton_solve();
-    launch_direction(dev_, kRhsAffine, st_, &launches_);
-    launch_newton_rhs(dev_, kRhsCorrector, st_, &launches_);
-    newton_solve();
-    launch_direction(dev_, kRhsCorrector, st_, &launches_);
+    for (int pass : {kRhsAffine, kRhsCorrector}) {
+      if (xspace_) launch_newton_rhs_x(dev_, pass, st_, &launches_);
+      else launch_newton_rhs(dev_, pass, st_, &launches_);
+      newton_solve();
+      if (xspace_) launch_direction_x(dev_, pass, st_, &launches_);
+      else launch_direction(dev_, pass, st_, &launches_);
+    }
     launch_update(dev_, st_, &launches_);
   }
   if (!done) SOV_CUDA(cudaEventRecord(e1, st_));

@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kThreads) k_update(IpmDev d) {
         d.s[j] = fmax(d.s[j] + ad * d.ds[j], 1e-14);
       }
     }
-    if (j < d.m) d.y[j] += ad * d.z[j];
+    if (j < d.m) d.y[j] += ad * d.dy[j];
   }
 }
 
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
       double x = 1.0, s = 1.0;
       if (ok) {
         double atdy = 0.0;
-        for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+        for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.dy[d.row_idx[p]];
         if (!d.qp) {
           x = fmax(1.0, fabs(atdy));
           s = fmax(1.0, fabs(d.c[j] - atdy));
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
       d.x[j] = x;
       d.s[j] = s;
     }
-    if (j < d.m) d.y[j] = ok ? d.z[j] : 0.0;
+    if (j < d.m) d.y[j] = ok ? d.dy[j] : 0.0;
   }
 }
 
@@ -325,6 +325,124 @@ __global__ void __launch_bounds__(kThreads) k_normal_rows(IpmDev d, const double
     for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * tmp[d.col_idx[p]];
     acc = warp_sum(acc);
     if (lane == 0) out[i] = acc + reg * v[i];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// x-space QP: K dx_x = r1_x + A_x'(Theta rp - sigma r1_w), dy = Theta (rp - A_x dx_x) - sigma r1_w,
+// dw = (r1_w + sigma dy) / h_w  (the slack columns of the KKT system of solve_newton_qp,
+// qp_interior_point.cpp:2832-2844, eliminated row by row)
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double h_of(const IpmDev& d, int j) {
+  return fmax(d.s[j], 1e-16) / fmax(d.x[j], 1e-16);
+}
+__device__ __forceinline__ double r1_of(const IpmDev& d, int mode, int j, double sigma_mu) {
+  const double rxs = rxs_of(d, mode, j, sigma_mu);
+  if (d.free_col[j]) return -d.rd[j];
+  return -d.rd[j] + rxs / fmax(d.x[j], 1e-16);
+}
+
+__global__ void __launch_bounds__(kThreads) k_xrhs_rows(IpmDev d, int mode) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < d.m; r += gridDim.x * blockDim.x) {
+    const int w = d.slack_of_row[r];
+    d.tr[r] = h_of(d, w) * d.rp[r] - d.sigma[r] * r1_of(d, mode, w, sigma_mu);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_xrhs_cols(IpmDev d, int mode) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.nx; j += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) acc += d.cval[p] * d.tr[d.row_idx[p]];
+    d.z[j] = (mode < 0 ? 0.0 : r1_of(d, mode, j, sigma_mu)) + acc;
+  }
+}
+
+// rows: dy, dw and the slack's ds; structural columns: dx = z, ds; both ratio tests
+__global__ void __launch_bounds__(kThreads) k_xdirection(IpmDev d, int mode) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  double* dx = mode == kRhsAffine ? d.dxa : d.dx;
+  double* ds = mode == kRhsAffine ? d.dsa : d.ds;
+  double rp_min = 1.0, rd_min = 1.0;
+  const int N = d.m > d.nx ? d.m : d.nx;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+    if (t < d.m) {
+      const int r = t, w = d.slack_of_row[r];
+      double ax = 0.0;
+      for (int p = d.row_ptr[r]; p < d.row_ptr[r + 1]; ++p) {
+        const int j = d.col_idx[p];
+        if (j < d.nx) ax += d.rval[p] * d.z[j];
+      }
+      const double hw = h_of(d, w);
+      const double r1w = r1_of(d, mode, w, sigma_mu);
+      const double dyr = hw * (d.rp[r] - ax) - d.sigma[r] * r1w;
+      const double dw = (r1w + d.sigma[r] * dyr) / hw;
+      const double xw = d.x[w], sw = d.s[w];
+      const double dsw = (rxs_of(d, mode, w, sigma_mu) - sw * dw) / fmax(xw, 1e-16);
+      d.dy[r] = dyr;
+      dx[w] = dw;
+      ds[w] = dsw;
+      if (dw < 0.0) rp_min = fmin(rp_min, -xw / dw);
+      if (dsw < 0.0) rd_min = fmin(rd_min, -sw / dsw);
+    }
+    if (t < d.nx) {
+      const int j = t;
+      const double dxj = d.z[j];
+      const bool fr = d.free_col[j];
+      const double dsj = fr ? 0.0 : (rxs_of(d, mode, j, sigma_mu) - d.s[j] * dxj) / fmax(d.x[j], 1e-16);
+      dx[j] = dxj;
+      ds[j] = dsj;
+      if (!fr) {
+        if (dxj < 0.0) rp_min = fmin(rp_min, -d.x[j] / dxj);
+        if (dsj < 0.0) rd_min = fmin(rd_min, -d.s[j] / dsj);
+      }
+    }
+  }
+  double v[2] = {rp_min, rd_min};
+  const int ops[2] = {2, 2};
+  if (grid_reduce<2>(v, ops, d.partials, d.counter) && threadIdx.x == 0) {
+    IpmScalars* sc = d.sc;
+    sc->ratio_p = v[0];
+    sc->ratio_d = v[1];
+    if (mode == kRhsAffine) {
+      sc->alpha_p_aff = v[0];
+      sc->alpha_d_aff = v[1];
+    } else {
+      double ap = fmin(1.0, d.tau * v[0]);
+      double ad = fmin(1.0, d.tau * v[1]);
+      if (d.has_quadratic) ap = ad = fmin(ap, ad);  // common step (qp_interior_point.cpp:3095)
+      sc->alpha_p = ap;
+      sc->alpha_d = ad;
+    }
+  }
+}
+
+// start (qp_interior_point.cpp:2884-2891 with H = I): t = b - A 1, K = I + A_x'A_x, z = A_x' t
+__global__ void __launch_bounds__(kThreads) k_xstart_rows(IpmDev d) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < d.m; r += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[r]; p < d.row_ptr[r + 1]; ++p) acc += d.rval[p];
+    d.tr[r] = d.b[r] - acc;
+  }
+}
+__global__ void __launch_bounds__(kThreads) k_xstart_dy(IpmDev d) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < d.m; r += gridDim.x * blockDim.x) {
+    double ax = 0.0;
+    for (int p = d.row_ptr[r]; p < d.row_ptr[r + 1]; ++p) {
+      const int j = d.col_idx[p];
+      if (j < d.nx) ax += d.rval[p] * d.z[j];
+    }
+    d.dy[r] = d.tr[r] - ax;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_xdiag(IpmDev d, int mode, double* M, int layout_ld, double* diag) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.nx; j += gridDim.x * blockDim.x) {
+    const double add = mode == 0 ? 1.0 : d.qdiag[j] + (d.free_col[j] ? 0.0 : h_of(d, j));
+    const int64_t pos = layout_ld > 0 ? static_cast<int64_t>(j) * layout_ld + j : j;
+    M[pos] += add;
+    diag[j] += add;
   }
 }
 
@@ -370,6 +488,38 @@ void launch_start_point(const IpmDev& d, cudaStream_t st, int* launches) {
   k_start_point<<<blocks_for(std::max(d.n, d.m)), kThreads, 0, st>>>(d);
   SOV_LAUNCH_CHECK();
   if (launches) *launches += 1;
+}
+
+void launch_newton_rhs_x(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
+  k_xrhs_rows<<<blocks_for(d.m), kThreads, 0, st>>>(d, mode);
+  k_xrhs_cols<<<blocks_for(d.nx), kThreads, 0, st>>>(d, mode);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 2;
+}
+
+void launch_direction_x(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
+  k_xdirection<<<blocks_for(std::max(d.m, d.nx)), kThreads, 0, st>>>(d, mode);
+  if (mode == kRhsAffine) k_mu_aff<<<blocks_for(d.n), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += mode == kRhsAffine ? 2 : 1;
+}
+
+void launch_start_rhs_x(const IpmDev& d, cudaStream_t st, int* launches) {
+  k_xstart_rows<<<blocks_for(d.m), kThreads, 0, st>>>(d);
+  k_xrhs_cols<<<blocks_for(d.nx), kThreads, 0, st>>>(d, -1);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 2;
+}
+
+void launch_start_dy_x(const IpmDev& d, cudaStream_t st, int* launches) {
+  k_xstart_dy<<<blocks_for(d.m), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += 1;
+}
+
+void launch_xspace_diag(const IpmDev& d, int mode, double* M, int layout_ld, double* diag, cudaStream_t st) {
+  k_xdiag<<<blocks_for(d.nx), kThreads, 0, st>>>(d, mode, M, layout_ld, diag);
+  SOV_LAUNCH_CHECK();
 }
 
 void launch_normal_matvec(const IpmDev& d, const double* v, double* tmp_n, double* out, double reg, cudaStream_t st) {

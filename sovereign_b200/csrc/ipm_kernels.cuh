@@ -41,7 +41,14 @@ struct IpmDev {
   double *x, *y, *s;
   double *dx, *ds, *dxa, *dsa;
   double *rp, *rd;
-  double* z;                // Newton right-hand side / dy (padded to the solver's order)
+  double* z;                // Newton right-hand side / solution (padded to the solver's order)
+  double* dy;               // dy of the last direction (== z in y-space)
+  // x-space QP (every row has a slack, Q_jj > 0 on structural columns): K dx_x = rhs, then dy, dw
+  int xspace;
+  int nx;                   // structural columns
+  const int* slack_of_row;  // m
+  const double* sigma;      // m: slack coefficient of the row (+1 / -1)
+  double* tr;               // m scratch
   IpmScalars* sc;
   // grid reduction scratch
   double* partials;         // 8 * max_blocks
@@ -65,6 +72,14 @@ void launch_start_point(const IpmDev& d, cudaStream_t st, int* launches);
 // matrix-free normal product out = A diag(w) A' v + reg v, w from the iterate (mixed-precision PCG)
 void launch_normal_matvec(const IpmDev& d, const double* v, double* tmp_n, double* out, double reg,
                           cudaStream_t st);
+
+// x-space counterparts (xspace == 1)
+void launch_newton_rhs_x(const IpmDev& d, int mode, cudaStream_t st, int* launches);
+void launch_direction_x(const IpmDev& d, int mode, cudaStream_t st, int* launches);
+void launch_start_rhs_x(const IpmDev& d, cudaStream_t st, int* launches);
+void launch_start_dy_x(const IpmDev& d, cudaStream_t st, int* launches);
+// K_jj += Q_jj + h_j (mode 1) or += 1 (start, mode 0); same on the recorded diagonal
+void launch_xspace_diag(const IpmDev& d, int mode, double* M, int layout_ld, double* diag, cudaStream_t st);
 
 int reduction_blocks(int n);
 

@@ -286,6 +286,90 @@ AssemblyMap build_assembly_band(const StdForm& f, int kd) {
   return build_assembly(f, [m](int r, int c) { return static_cast<int64_t>(r - c) * m + c; });
 }
 
+XSpace analyze_xspace(const StdForm& f) {
+  XSpace xs;
+  if (!f.qp || !f.q_diagonal || f.m == 0) return xs;
+  for (int j = 0; j < f.n_struct; ++j)
+    if (!(f.qdiag[j] > 0.0)) return xs;
+  xs.slack_of_row.assign(f.m, -1);
+  xs.sigma.assign(f.m, 0.0);
+  for (int j = f.n_struct; j < f.n; ++j) {
+    if (f.col_ptr[j + 1] - f.col_ptr[j] != 1) return xs;
+    const int r = f.row_idx[f.col_ptr[j]];
+    xs.slack_of_row[r] = j;
+    xs.sigma[r] = f.val[f.col_ptr[j]];
+  }
+  for (int r = 0; r < f.m; ++r)
+    if (xs.slack_of_row[r] < 0) return xs;  // an equality row: stay in y-space
+  for (int r = 0; r < f.m; ++r) {
+    int lo = f.n_struct, hi = -1;
+    for (int p = f.row_ptr[r]; p < f.row_ptr[r + 1]; ++p) {
+      const int j = f.col_idx[p];
+      if (j >= f.n_struct) continue;
+      lo = std::min(lo, j);
+      hi = std::max(hi, j);
+    }
+    if (hi >= lo) xs.kd = std::max(xs.kd, hi - lo);
+  }
+  xs.eligible = true;
+  return xs;
+}
+
+namespace {
+
+template <class Index>
+AssemblyMap build_xspace_map(const StdForm& f, const XSpace& xs, Index index) {
+  struct Contrib {
+    int64_t t;
+    int col;
+    double w;
+  };
+  std::vector<Contrib> cs;
+  for (int r = 0; r < f.m; ++r) {
+    const int slack = xs.slack_of_row[r];
+    for (int p = f.row_ptr[r]; p < f.row_ptr[r + 1]; ++p) {
+      const int jp = f.col_idx[p];
+      if (jp >= f.n_struct) continue;
+      for (int q = f.row_ptr[r]; q < f.row_ptr[r + 1]; ++q) {
+        const int jq = f.col_idx[q];
+        if (jq >= f.n_struct || jq > jp) continue;
+        cs.push_back({index(jp, jq), slack, f.rval[p] * f.rval[q]});
+      }
+    }
+  }
+  for (int j = 0; j < f.n_struct; ++j) cs.push_back({index(j, j), -1, 0.0});  // every diagonal has a target
+  std::stable_sort(cs.begin(), cs.end(), [](const Contrib& a, const Contrib& b) { return a.t < b.t; });
+  AssemblyMap am;
+  am.ptr.push_back(0);
+  for (std::size_t k = 0; k < cs.size(); ++k) {
+    if (am.target.empty() || am.target.back() != cs[k].t) {
+      if (!am.target.empty()) am.ptr.push_back(static_cast<int>(am.col.size()));
+      am.target.push_back(cs[k].t);
+    }
+    if (cs[k].col >= 0) {
+      am.col.push_back(cs[k].col);
+      am.w.push_back(cs[k].w);
+    }
+  }
+  am.ptr.push_back(static_cast<int>(am.col.size()));
+  am.diag_target.assign(f.n_struct, 0);
+  for (int j = 0; j < f.n_struct; ++j)
+    am.diag_target[j] = static_cast<int>(std::lower_bound(am.target.begin(), am.target.end(), index(j, j)) -
+                                         am.target.begin());
+  return am;
+}
+
+}  // namespace
+
+AssemblyMap build_assembly_xspace(const StdForm& f, const XSpace& xs, int ld) {
+  return build_xspace_map(f, xs, [ld](int r, int c) { return static_cast<int64_t>(c) * ld + r; });
+}
+
+AssemblyMap build_assembly_xspace_band(const StdForm& f, const XSpace& xs) {
+  const int64_t nx = f.n_struct;
+  return build_xspace_map(f, xs, [nx](int r, int c) { return static_cast<int64_t>(r - c) * nx + c; });
+}
+
 int normal_bandwidth(const StdForm& f) {
   int kd = 0;
   for (int j = 0; j < f.n; ++j) {

@@ -64,4 +64,18 @@ AssemblyMap build_assembly_band(const StdForm& f, int kd);  // band storage: (kd
 // Half-bandwidth of A D A' in the natural row order.
 int normal_bandwidth(const StdForm& f);
 
+// x-space form of a QP whose every row carries a slack column and whose structural columns all
+// have Q_jj > 0: K = diag(Q_jj + h_j) + A_x' Theta A_x over the structural columns, Theta_r the
+// barrier weight s/x of row r's slack column.
+struct XSpace {
+  bool eligible = false;
+  std::vector<int> slack_of_row;  // m: IPM column of row r's slack
+  std::vector<double> sigma;      // m: that slack's coefficient (+1 slack, -1 surplus)
+  int kd = 0;                     // half-bandwidth of K in the natural column order
+};
+XSpace analyze_xspace(const StdForm& f);
+// Gather map of A_x' Theta A_x (contribution weight column = the row's slack column).
+AssemblyMap build_assembly_xspace(const StdForm& f, const XSpace& xs, int ld);   // dense, ld >= n_struct
+AssemblyMap build_assembly_xspace_band(const StdForm& f, const XSpace& xs);     // band, (kd+1) x n_struct
+
 }  // namespace sov

@@ -44,23 +44,39 @@ __device__ void tc3_tile(float* C, int ldc, const float* A, int lda, const float
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) tc::tmem_alloc(&tmem_base, N < 32 ? 32 : N);
   if (tid == 0) tc::mbar_init(&mbar, 1);
-  // stage A and B: coalesced along rows, split into hi / lo, K-major core-matrix layout
-  for (int idx = tid; idx < kTcM * kTcK; idx += kTcThreads) {
-    const int r = idx % kTcM, k = idx / kTcM;
-    const float v = r < rows_valid ? A[static_cast<int64_t>(k) * lda + r] : 0.0f;
-    const float hi = to_tf32(v);
-    const uint32_t off = tc::kmajor_offset(r, k, kTcK, 4);
-    *reinterpret_cast<float*>(a_hi + off) = hi;
-    *reinterpret_cast<float*>(a_lo + off) = to_tf32(v - hi);
-  }
-  for (int idx = tid; idx < N * kTcK; idx += kTcThreads) {
-    const int n = idx % N, k = idx / N;
-    const float v = n < cols_valid ? B[static_cast<int64_t>(k) * ldb + n] : 0.0f;
-    const float hi = to_tf32(v);
-    const uint32_t off = tc::kmajor_offset(n, k, kTcK, 4);
-    *reinterpret_cast<float*>(b_hi + off) = hi;
-    *reinterpret_cast<float*>(b_lo + off) = to_tf32(v - hi);
-  }
+  // stage A and B: float4 loads along the contiguous row dimension, all of a thread's loads issued
+  // before any use (operand origins and valid extents are multiples of 64 rows, so a float4 is
+  // either wholly inside or wholly outside), then split into hi / lo in the K-major layout
+  auto stage = [&](const float* src, int ld, int rows, int valid, unsigned char* hi_buf, unsigned char* lo_buf) {
+    const int per_col = rows / 4;
+    const int total = per_col * kTcK;
+    constexpr int kMaxPer = (kTcM / 4) * kTcK / kTcThreads;  // 16
+    float4 v[kMaxPer];
+#pragma unroll
+    for (int it = 0; it < kMaxPer; ++it) {
+      const int idx = it * kTcThreads + tid;
+      const int q = idx % per_col, k = idx / per_col;
+      v[it] = (idx < total && 4 * q < valid)
+                  ? __ldg(reinterpret_cast<const float4*>(src + static_cast<int64_t>(k) * ld + 4 * q))
+                  : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int it = 0; it < kMaxPer; ++it) {
+      const int idx = it * kTcThreads + tid;
+      if (idx >= total) continue;
+      const int q = idx % per_col, k = idx / per_col;
+      const float e[4] = {v[it].x, v[it].y, v[it].z, v[it].w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float h = to_tf32(e[u]);
+        const uint32_t off = tc::kmajor_offset(4 * q + u, k, kTcK, 4);
+        *reinterpret_cast<float*>(hi_buf + off) = h;
+        *reinterpret_cast<float*>(lo_buf + off) = to_tf32(e[u] - h);
+      }
+    }
+  };
+  stage(A, lda, kTcM, rows_valid, a_hi, a_lo);
+  stage(B, ldb, N, cols_valid, b_hi, b_lo);
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();

@@ -31,6 +31,7 @@ class InteriorPointOptions:
     use_sparse_normal_equations: bool = False
     precision: int = abi.PRECISION_FP64
     pcg_max_iterations: int = 50
+    ipm_iterate_at: int = 0   # iterate returned in ipm_x/y/s: 0 final, k >= 1 start of iteration k
 
     def to_abi(self, qp: bool = False) -> abi.SovOptions:
         o = abi.default_options(qp=qp)
@@ -41,6 +42,7 @@ class InteriorPointOptions:
         o.enable_scaling = int(self.enable_scaling) if not qp else 0
         o.precision = self.precision
         o.pcg_max_iterations = self.pcg_max_iterations
+        o.ipm_iterate_at = self.ipm_iterate_at
         mode = os.environ.get("SOVEREIGN_IPM_NORMAL_EQUATIONS", "auto")  # interior_point.cpp:132-133
         o.factorization = {"dense": abi.FACTOR_DENSE, "banded": abi.FACTOR_BANDED}.get(mode, abi.FACTOR_AUTO)
         return o

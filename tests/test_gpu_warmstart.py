@@ -1,0 +1,71 @@
+"""The warm-start network: its hand-written BF16 forward and backward kernels against the FP64
+restatement (oracle/mlp_oracle.py), its training, and what a trained network gains the IPM on a
+parametric LP family (fewer iterations, the same optimum)."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle
+from sovereign_b200 import problems as P
+from sovereign_b200.ipm import InteriorPointOptions
+from sovereign_b200.warmstart import Mlp, WarmStart, solve_many
+
+pytestmark = pytest.mark.gpu
+
+
+def test_forward_and_gradients_match_fp64_restatement():
+    rng = np.random.default_rng(0)
+    dims = (96, 64, 3, 80)  # n_in, hidden, layers, n_out: partial 128-tiles on every side
+    mlp = Mlp(dims[0], dims[3], dims[1], dims[2], seed=3)
+    x = rng.standard_normal((40, dims[0])).astype(np.float32)
+    t = rng.standard_normal((40, dims[3])).astype(np.float32)
+    loss, g = mlp.loss_grad(x, t)
+    ref_loss, ref_g, ref_y = mlp_oracle.loss_and_grad(mlp.params, mlp.dims, x, t)
+    y = mlp.forward(x)
+    # BF16 operands (8-bit mantissa), FP32 accumulation: ~1e-2 relative agreement
+    assert np.linalg.norm(y - ref_y) / np.linalg.norm(ref_y) < 2e-2
+    assert abs(loss - ref_loss) / ref_loss < 2e-2
+    cos = float(g @ ref_g / (np.linalg.norm(g) * np.linalg.norm(ref_g)))
+    assert cos > 0.999
+    assert abs(np.linalg.norm(g) / np.linalg.norm(ref_g) - 1.0) < 3e-2
+    # per layer, against the restatement with the kernels' BF16 operand rounding: only the
+    # accumulation order differs
+    _, bf_g, bf_y = mlp_oracle.loss_and_grad(mlp.params, mlp.dims, x, t, bf16_operands=True)
+    assert np.linalg.norm(y - bf_y) <= 1e-3 * np.linalg.norm(bf_y)
+    off = 0
+    for l in range(len(mlp.dims) - 1):
+        for size in (mlp.dims[l + 1] * mlp.dims[l], mlp.dims[l + 1]):
+            a, b = g[off:off + size], bf_g[off:off + size]
+            assert np.linalg.norm(a - b) <= 5e-3 * np.linalg.norm(b) + 1e-7, (l, size)
+            off += size
+
+
+def test_training_reduces_loss():
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((512, 32)).astype(np.float32)
+    w = rng.standard_normal((32, 16)).astype(np.float32) / 6
+    t = np.tanh(x @ w).astype(np.float32)
+    mlp = Mlp(32, 16, 64, 2, seed=0)
+    before, _ = mlp.loss_grad(x, t)
+    after = mlp.train(x, t, epochs=60, batch=64, lr=3e-3)
+    assert after < 0.2 * before
+
+
+def test_warm_start_saves_iterations_on_a_parametric_family():
+    fam = P.MulticommodityFamily(nodes=30, arcs=100, commodities=2, sinks=3, seed=11)
+    train = [fam.instance_from_seed(1000 + k) for k in range(192)]
+    test = [fam.instance_from_seed(5000 + k) for k in range(24)]
+    opts = InteriorPointOptions()
+    # targets: the iterate at the start of iteration 5, an early, well-centred point of the path
+    cold_train, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=5))
+    ws = WarmStart(fam.param_dim, cold_train[0].n_ipm, cold_train[0].m_ipm, hidden=128, layers=3, seed=0)
+    ws.fit(np.stack([p for _, p in train]), cold_train, epochs=150, batch=64, lr=2e-3)
+    cold, _ = solve_many([m for m, _ in test], opts)
+    warm, _ = solve_many([m for m, _ in test], opts, warm=ws.predict(np.stack([p for _, p in test])))
+    for c, w in zip(cold, warm):
+        assert c.status_name == "OPTIMAL" and w.status_name == "OPTIMAL"
+        assert abs(c.objective_value - w.objective_value) <= 1e-8 * max(1.0, abs(c.objective_value))
+    used = sum(w.diagnostics["warm_start_used"] for w in warm)
+    gain = np.mean([c.iterations for c in cold]) - np.mean([w.iterations for w in warm])
+    info = (gain, used, [c.iterations for c in cold], [w.iterations for w in warm])
+    assert gain > 0.5, info
+    assert used >= len(test) // 2, info

@@ -121,3 +121,21 @@ def test_ipm_form_scaling_and_slacks():
             A[f["row_idx"][k], j] = f["values"][k]
     assert np.all(np.abs(A).max(axis=1) > 0.5) and np.all(np.abs(A).max(axis=0) > 0.5)
     np.testing.assert_allclose(f["shift"], [1.0, 0.0, 0.5])
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle import mlp_oracle
+    dims = [5, 7, 7, 4]
+    rng = np.random.default_rng(0)
+    n = sum(dims[l + 1] * dims[l] + dims[l + 1] for l in range(3))
+    p = rng.standard_normal(n) * 0.5
+    x, t = rng.standard_normal((6, 5)), rng.standard_normal((6, 4))
+    _, g, _ = mlp_oracle.loss_and_grad(p, dims, x, t)
+    fd = np.zeros(n)
+    for i in range(n):
+        q = p.copy()
+        q[i] += 1e-6
+        a = mlp_oracle.loss_and_grad(q, dims, x, t)[0]
+        q[i] -= 2e-6
+        fd[i] = (a - mlp_oracle.loss_and_grad(q, dims, x, t)[0]) / 2e-6
+    np.testing.assert_allclose(g, fd, atol=1e-7)
