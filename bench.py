@@ -94,9 +94,8 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus: int):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from sovereign_b200.shard import world as world_env
+    rank, world, local = world_env()
     if world > 1:
         import torch
         import torch.distributed as dist
@@ -115,12 +114,8 @@ def barrier(dist, local):
 
 
 def max_over_ranks(dist, v: float, local: int) -> float:
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from sovereign_b200.shard import max_over_ranks as mor
+    return mor(v, dist, device=f"cuda:{local}")
 
 
 def per_lp_bytes(mdl) -> float:
@@ -179,15 +174,110 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line))
 
 
+def _line(metric, value, unit, args, ms, dtype, config, **extra):
+    d = dict(metric=metric, value=value, unit=unit, n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
+             higher_is_better=True, scaling="weak", vs_baseline=None, dtype=dtype, data="synthetic", config=config)
+    d.update(extra)
+    print(json.dumps(d))
+
+
+def run_single_workload(args):
+    """Single-problem workloads of the other configurations (one JSON line each)."""
+    import torch
+    from sovereign_b200 import abi, problems as P
+    from sovereign_b200.ipm import InteriorPointOptions, InteriorPointSolver, QpInteriorPointSolver
+    import oracle
+    torch.cuda.init()
+
+    def timed(solver, mdl, **kw):
+        for _ in range(args.warmup):
+            solver.solve(mdl, **kw)
+        rs, ts = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            r = solver.solve(mdl, with_diag=True, **kw)
+            ts.append(time.perf_counter() - t0)
+            rs.append(r)
+        return rs[-1], float(np.median(ts)), float(np.median([r.solve_seconds for r in rs]))
+
+    if args.workload in ("c0", "c1"):
+        mdl = P.transport(50, 50, 0) if args.workload == "c0" else P.random_sparse_lp(2000, 10000, 8, 1)
+        lines = {}
+        for name, prec in (("fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+            r, wall, dev = timed(InteriorPointSolver(InteriorPointOptions(precision=prec)), mdl)
+            lines[name] = dict(status=r.status_name, iterations=r.iterations, objective=r.objective_value,
+                               wall_s=wall, device_s=dev, pcg_iterations=r.diagnostics["pcg_iterations"],
+                               fp64_refactorizations=r.diagnostics["fp64_fallbacks"])
+        ref = {}
+        if args.workload == "c0":
+            rr = oracle.solve(mdl, kind="reference")
+            ref = dict(objective=rr.objective_value, seconds=rr.solve_seconds, iterations=rr.iterations)
+        best = min(lines.values(), key=lambda v: v["wall_s"])
+        _line(METRIC, 1.0 / best["wall_s"], UNIT, args, 1e3 * best["wall_s"], "f64",
+              dict(workload="transport 50x50 (single LP)" if args.workload == "c0" else
+                   "random sparse LP m=2000 n=10000, 8 nnz/column (single LP)"),
+              variants=lines, cpu_reference=ref or None,
+              max_rel_obj_err_vs_reference=(abs(best["objective"] - ref["objective"]) / max(1.0, abs(ref["objective"]))
+                                            if ref else None))
+        return
+    if args.workload == "c2":
+        mdl = P.convex_sequence_qp(20002, 2)
+        r, wall, dev = timed(QpInteriorPointSolver(), mdl)
+        _line(METRIC, 1.0 / wall, UNIT, args, 1e3 * wall, "f64",
+              dict(workload="convex-sequence QP n=20002, m=20000 (single QP)"),
+              status=r.status_name, iterations=r.iterations, objective=r.objective_value, device_s=dev,
+              duality_gap=r.duality_gap, message=r.message[:160])
+        return
+    # c4: learned warm start on the multicommodity family
+    from sovereign_b200.warmstart import WarmStart, solve_many
+    fam = P.MulticommodityFamily()
+    train = [fam.instance_from_seed(100000 + k) for k in range(args.train)]
+    test = [fam.instance_from_seed(900000 + k) for k in range(args.eval)]
+    opts = InteriorPointOptions()
+    t0 = time.perf_counter()
+    # training targets: the iterate at the start of iteration 6 (early central-path stretch)
+    cold_train, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=6))
+    t_gen = time.perf_counter() - t0
+    ws = WarmStart(fam.param_dim, cold_train[0].n_ipm, cold_train[0].m_ipm, hidden=512, layers=3, seed=0)
+    t0 = time.perf_counter()
+    loss = ws.fit(np.stack([p for _, p in train]), cold_train, epochs=40, batch=128, lr=1e-3)
+    t_train = time.perf_counter() - t0
+    cold, t_cold = solve_many([m for m, _ in test], opts)
+    t0 = time.perf_counter()
+    starts = ws.predict(np.stack([p for _, p in test]))
+    t_pred = time.perf_counter() - t0
+    warm, t_warm = solve_many([m for m, _ in test], opts, warm=starts)
+    ok = [k for k in range(len(test)) if cold[k].status_name == "OPTIMAL" and warm[k].status_name == "OPTIMAL"]
+    err = max(abs(cold[k].objective_value - warm[k].objective_value) / max(1.0, abs(cold[k].objective_value))
+              for k in ok) if ok else None
+    _line(METRIC, len(test) / (t_warm + t_pred), UNIT, args, 1e3 * (t_warm + t_pred) / len(test), "f64",
+          dict(workload=f"multicommodity 200 nodes / 1000 arcs / 4 commodities, {args.eval} eval instances, "
+                        f"MLP 4040-512x3-11800 trained on {args.train} IPM solutions"),
+          cold=dict(lps_per_s=len(test) / t_cold, mean_iterations=float(np.mean([r.iterations for r in cold]))),
+          warm=dict(lps_per_s=len(test) / (t_warm + t_pred), mean_iterations=float(np.mean([r.iterations for r in warm])),
+                    used=int(sum(r.diagnostics["warm_start_used"] for r in warm))),
+          optimal=f"{len(ok)}/{len(test)}", max_rel_obj_diff_warm_vs_cold=err, train_loss=loss,
+          seconds=dict(generate=t_gen, train=t_train, predict=t_pred))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sovereign_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=COUNT, help="LPs per step (profiling runs use fewer)")
+    ap.add_argument("--workload", default="batch", choices=["batch", "c0", "c1", "c2", "c4"],
+                    help="batch (default, headline): 4096 uneven transportation LPs; c0: one 50x50 transportation "
+                         "LP; c1: random LP m=2000 n=10000 (FP64 and mixed); c2: convex-sequence QP n=20002; "
+                         "c4: multicommodity family, learned warm start vs Mehrotra start")
+    ap.add_argument("--train", type=int, default=1024, help="c4: training instances")
+    ap.add_argument("--eval", type=int, default=128, help="c4: evaluation instances")
     args = ap.parse_args()
+    if args.workload != "batch":
+        run_single_workload(args)
+        return
     rank, world, local, dist = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -198,18 +288,30 @@ def main():
     import ctypes as C
 
     from sovereign_b200 import _lib, problems as P
-    from sovereign_b200.ipm import DeviceBatch, InteriorPointSolver, solve_batch
+    from sovereign_b200.ipm import DeviceBatch, InteriorPointSolver, autotune, solve_batch
 
     lib = _lib.load(build_if_missing=False)
     # weak scaling: every rank solves its own 4096 LPs (seed offset by rank)
     count = args.count
-    models = P.transport_batch(count, seed=2026 + rank)
+    from sovereign_b200.shard import shard_seed
+    models = P.transport_batch(count, seed=shard_seed(2026, rank))
     bytes_iter = np.array([per_lp_bytes(m) for m in models])
 
-    batch = DeviceBatch(models)
-    stream = C.c_void_p(0)
     import torch
     torch.cuda.set_device(local)
+    if rank == 0:
+        # plain FP64 single-problem engine on a bounded sample of the same LPs, measured first
+        # (after one untimed solve) so that it runs in a clean process state
+        sample = models[:48]
+        InteriorPointSolver().solve(sample[0])
+        t0 = time.perf_counter()
+        single = [InteriorPointSolver().solve(m) for m in sample]
+        t_plain = time.perf_counter() - t0
+        plain = dict(value=len(sample) / t_plain, unit=UNIT,
+                     sample=f"first {len(sample)} LPs one at a time through sov_lp_solve (FP64), wall clock")
+    # untimed: threads per CTA for each size bucket, picked by timing the bucket alone
+    tuning = json.loads(autotune(models))
+    batch = DeviceBatch(models)
     ts = torch.cuda.Stream()
     for _ in range(args.warmup):
         batch.solve(ts.cuda_stream)
@@ -242,18 +344,34 @@ def main():
                     note="algorithmic bytes = sum over LPs of (iterations + 1) x [6 SpMV x (12 nnz + 8(m+n)) + "
                          "15 x 8n + 10 x 8m]; kernel time from CUDA events of the last step")
 
-    # end to end through the public C ABI with host buffers (bounded: every step re-creates)
-    e2e_steps = max(1, min(args.steps, 3))
+    # end to end through the C ABI, sov_lp_solve_batch, with caller-owned host buffers (the models'
+    # CSC arrays in, primal/dual arrays out), as a C or C++ caller holds them: host standard form,
+    # H2D, solve, D2H and publishing are all inside the timed region
+    from sovereign_b200 import abi as A
+    from sovereign_b200.model import ResultBuffers
+    arr = (A.SovModel * count)(*[m.to_abi() for m in models])
+    bufs = [ResultBuffers(m) for m in models]
+    res_arr = (A.SovResult * count)(*[b.raw for b in bufs])
+    opt = A.default_options()
+    e2e_steps = max(1, min(args.steps, 5))
     barrier(dist, local)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        out = solve_batch(models)
+        _lib.check(lib.sov_lp_solve_batch(count, arr, C.byref(opt), 0, res_arr))
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(dist, e2e_s, local)
+    e2e_obj_diff = max(abs(r.objective_value - q.objective_value) / max(1.0, abs(q.objective_value))
+                       for r, q in zip(res_arr, res))
     h2d, d2h = C.c_double(), C.c_double()
     lib.sov_batch_transfer_bytes(batch.handle, C.byref(h2d), C.byref(d2h))
     e2e = dict(value=world * count * e2e_steps / e2e_s, unit=UNIT, h2d_bytes_per_step=int(h2d.value),
-               d2h_bytes_per_step=int(d2h.value), note="sov_lp_solve_batch: host standard form + H2D + solve + D2H")
+               d2h_bytes_per_step=int(d2h.value), max_rel_obj_diff_vs_device_batch=e2e_obj_diff,
+               note="sov_lp_solve_batch with caller-owned host buffers: host standard form + H2D + solve + "
+                    "D2H + publish, wall clock")
+    # the Python wrapper adds marshalling of the model and result objects on top
+    t0 = time.perf_counter()
+    solve_batch(models)
+    e2e["python_api_lps_per_s"] = world * count / max_over_ranks(dist, time.perf_counter() - t0, local)
 
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=dev_ms / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
@@ -261,19 +379,14 @@ def main():
                 config=dict(workload=WORKLOAD if count == COUNT else f"{count} uneven transportation LPs (profiling size)",
                             lps_per_gpu=count, precision="fp64 batched",
                             l2="per-step working set ~0.6 GB > 126 MB L2 (no flush needed)",
-                            parallelism=f"independent LPs sharded per rank (dp{world})"),
+                            parallelism=f"independent LPs sharded per rank (dp{world})",
+                            threads_per_bucket={k: v["chosen"] for k, v in tuning.items()}),
                 gpu_launches=int(stats["launches"] * args.steps), roofline=roofline, e2e=e2e,
                 optimal=f"{status_ok}/{count}", mean_iterations=float(iters.mean()))
     if rank == 0:
         line["clocks"] = clk.summary()
-        # plain FP64 single-problem engine on a bounded sample of the same LPs
-        sample = models[:48]
-        t0 = time.perf_counter()
-        single = [InteriorPointSolver().solve(m) for m in sample]
-        t_plain = time.perf_counter() - t0
-        line["plain_fp64_gpu"] = dict(value=len(sample) / t_plain, unit=UNIT,
-                                      sample=f"first {len(sample)} LPs one at a time through sov_lp_solve (FP64)")
-        line["speedup_vs_plain_fp64"] = value / line["plain_fp64_gpu"]["value"]
+        line["plain_fp64_gpu"] = plain
+        line["speedup_vs_plain_fp64"] = value / plain["value"]
         err = max(abs(a.objective_value - b.objective_value) / max(1.0, abs(b.objective_value))
                   for a, b in zip(res[:48], single))
         line["max_rel_obj_diff_batched_vs_plain"] = err

@@ -3,15 +3,17 @@
 // One CTA owns one LP at a time and runs the whole Mehrotra predictor-corrector loop of
 // solve_ipm (solver/lp/src/interior_point.cpp:454-740) for it without returning to the host:
 // CTAs pull LP indices from a device counter (largest first), so uneven sizes balance across
-// the 148 SMs. The normal matrix of an LP (order m <= 128) lives in shared memory and is factored
-// there as L D L' with the reference's dependent-row rule; n-vectors stay in global memory, where
+// the 148 SMs. The normal matrix of an LP (order m <= 128; lower triangle packed by rows, 66 KB at
+// m = 128, so up to three LPs share an SM) lives in shared memory and is factored there as L D L'
+// with the reference's dependent-row rule; n-vectors stay in global memory, where
 // the working set of the resident CTAs fits in the 126 MB L2. Size buckets (by m) get their own
 // launch with a shared-memory footprint and thread count chosen per bucket by the autotuner; the
-// bucket launches of a batch are captured in one CUDA graph and replayed.
+// bucket launches of a batch run concurrently on streams forked from the caller's stream.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -32,8 +34,11 @@ namespace sov {
 
 constexpr int kBatchMaxRows = 128;
 
+// offset of row i of a row-packed lower triangle
+__host__ __device__ constexpr int tri(int i) { return i * (i + 1) / 2; }
+
 struct LpMeta {
-  int m, n, nnz, ld;
+  int m, n, nnz, pad1;
   int max_iter, pad0;
   long long a_off, cp_off, rp_off, mv_off, nv_off;
   double bnorm, cnorm, ftol, otol, tau;
@@ -85,9 +90,10 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
                          CtaScalars& cs) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = NT / 32;
-  const int m = mt.m, n = mt.n, ld = mt.ld;
+  const int m = mt.m, n = mt.n;
+  // M: lower triangle, packed by rows (row i at tri(i)); then six m-vectors
   double* M = sm;
-  double* vy = sm + static_cast<size_t>(mmax) * (mmax + 1);
+  double* vy = sm + tri(mmax);
   double* vrp = vy + mmax;
   double* vz = vrp + mmax;
   double* vacc = vz + mmax;
@@ -115,100 +121,282 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   double* gby = bd.by + mt.mv_off;
   int drops = 0, fail = 0;
 
-  // ---- assembly of M = A diag(d) A' + 1e-12 I (mode 0: d = x/s, mode 2: d = 1) ----
-  // Warp per row i of the lower triangle, lanes over the row's entries a_ik: the diagonal term
-  // sum_k a_ik^2 d_k is a warp sum; the off-diagonal terms a_ik d_k a_rk (r < i in column k) are
-  // added into shared memory (one term per (i, r) when rows share a single column, as in
-  // transportation LPs, so the sum order is then fixed).
-  auto assemble = [&](int mode) {
-    for (int i = tid; i < m * ld; i += NT) M[i] = 0.0;
-    __syncthreads();
-    for (int i = warp; i < m; i += NW) {
-      double* Mi = M + i * ld;
-      double dsum = 0.0;
-      for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) {
-        const int k = ci[p];
-        const double dk = mode == 2 ? 1.0 : fmax(x[k], 1e-16) / fmax(s[k], 1e-16);
-        const double a = rv[p];
-        for (int q = cp[k]; q < cp[k + 1]; ++q) {
-          const int r = ri[q];
-          if (r < i) atomicAdd(Mi + r, a * dk * cv[q]);
-        }
-        dsum += a * a * dk;
-      }
-      dsum = warp_sum(dsum);
-      if (lane == 0) {
-        Mi[i] = dsum + 1e-12;
-        vdiag[i] = Mi[i];
+  // ---- normal matrix M = A diag(d) A' + 1e-12 I, assembled inside the residual passes ----
+  // Off-diagonal entries come from the column pass: thread per column j, one shared-memory atomic
+  // per pair of entries, (a_hj d_j) a_lj into M[h][l] (h > l). When no two rows share more than
+  // one column (transportation LPs) each entry receives one term, so the order does not matter.
+  // Diagonal entries come from the row pass as a warp sum of (a_ik a_ik) d_k over row i.
+  // M is cleared by the pass before (start-up, or the update of the previous iteration).
+  auto offdiag = [&](int pb, int pe, double dj) {
+    for (int qa = pb; qa < pe; ++qa) {
+      const int ra = ri[qa];
+      const double va = cv[qa] * dj;
+      for (int qb = pb; qb < pe; ++qb) {
+        const int rb = ri[qb];
+        if (rb < ra) atomicAdd(M + tri(ra) + rb, va * cv[qb]);
       }
     }
-    __syncthreads();
+  };
+
+  // Row pass, two rows per warp (both rows' gathers in flight), lanes over the row's entries:
+  //  mode 0 (start):     z = b - A 1,                diag M_ii = sum a_ik^2 + 1e-12
+  //  mode 1 (iteration): rp = b - A x, z = rp + A t,  diag M_ii = sum a_ik^2 d_k + 1e-12
+  //  mode 2 (corrector): z = rp + A t
+  // Returns this thread's share of max |rp_i| (mode 1).
+  auto row_pass = [&](const int mode, const double* dv, const double* tv) {
+    double rpm = 0.0;
+    for (int i0 = warp; i0 < m; i0 += 2 * NW) {
+      const int rows[2] = {i0, i0 + NW};
+      int pb[2], pe[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        pb[h] = rows[h] < m ? rpp[rows[h]] : 0;
+        pe[h] = rows[h] < m ? rpp[rows[h] + 1] : 0;
+      }
+      double g0[2] = {0.0, 0.0}, g1[2] = {0.0, 0.0}, g2[2] = {0.0, 0.0};
+      const int len = max(pe[0] - pb[0], pe[1] - pb[1]);
+      for (int o = lane; o < len; o += 32) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int p = pb[h] + o;
+          if (p < pe[h]) {
+            const double a = rv[p];
+            if (mode == 0) {
+              g0[h] += a;
+              g1[h] += a * a;
+            } else {
+              const int k = ci[p];
+              if (mode == 1) {
+                g0[h] += a * x[k];
+                g1[h] += a * a * dv[k];
+              }
+              g2[h] += a * tv[k];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double s0 = mode != 2 ? warp_sum(g0[h]) : 0.0;
+        const double s1 = mode != 2 ? warp_sum(g1[h]) : 0.0;
+        const double s2 = mode != 0 ? warp_sum(g2[h]) : 0.0;
+        const int i = rows[h];
+        if (i >= m) continue;
+        if (mode == 2) {
+          if (lane == 0) vz[i] = vrp[i] + s2;
+          continue;
+        }
+        const double r = b[i] - s0;
+        if (mode == 1) rpm = fmax(rpm, fabs(r));
+        if (lane == 0) {
+          M[tri(i) + i] = s1 + 1e-12;
+          vdiag[i] = s1 + 1e-12;
+          if (mode == 1) {
+            vrp[i] = r;
+            vz[i] = r + s2;
+          } else {
+            vz[i] = r;
+          }
+        }
+      }
+    }
+    return rpm;
   };
 
   // ---- in-place L D L' (L~ = L D kept unscaled below the diagonal; vinv = 1/D) ----
-  // Per column k one barrier; the trailing update M[i][j] -= M[i][k] M[j][k] / D_k (k < j <= i)
-  // is spread over a TY x TX thread grid (row i = k+1+ty (mod TY), column j = k+1+tx (mod TX)),
-  // so every thread issues independent shared-memory updates.
+  // Blocked right-looking over panels of KB columns, three barriers per panel:
+  //  (1) warp 0 factors the KB x KB diagonal block, lane = row, one column at a time;
+  //  (2) one thread per row below the block runs the same column recurrence on its KB panel
+  //      entries held in registers;
+  //  (3) the trailing lower triangle takes the panel's rank-KB update in 4 x 4 register tiles
+  //      (8 shared loads per 16 FMAs instead of 3 shared accesses per FMA).
+  // Every entry sees the same operations in the same order as the column-at-a-time algorithm
+  // (M[i][j] -= (M[i][k] / D_k) * M[j][k] for k = 0, 1, ...), so the factor is bit-identical to it.
+  // vdiag[k] (the assembled diagonal, the reference for the dependent-row test) is overwritten
+  // with the pivot outcome of column k once it has been used: 0 kept, 1 dropped, 2 not finite.
   auto factor = [&]() {
-    constexpr int TX = 16, TY = NT / 16;
-    const int tx = tid % TX, ty = tid / TX;
-    for (int k = 0; k < m; ++k) {
-      const double p = M[k * ld + k];
-      const double dref = vdiag[k];
-      double Dk;
-      if (!isfinite(p)) {
-        Dk = 1e128;
-        fail = 1;
-      } else if (p <= 1e-13 * fabs(dref)) {
-        Dk = 1e128;  // dependent row (sparse_ldlt.cpp:167-173)
-        ++drops;
-      } else {
-        Dk = p;
+    constexpr int KB = 8;
+    for (int k0 = 0; k0 < m; k0 += KB) {
+      const int k1 = min(k0 + KB, m);
+      if (warp == 0) {
+        for (int k = k0; k < k1; ++k) {
+          const double p = M[tri(k) + k];
+          const double dref = vdiag[k];
+          double Dk, code;
+          if (!isfinite(p)) {
+            Dk = 1e128;
+            code = 2.0;
+          } else if (p <= 1e-13 * fabs(dref)) {
+            Dk = 1e128;  // dependent row (sparse_ldlt.cpp:167-173)
+            code = 1.0;
+          } else {
+            Dk = p;
+            code = 0.0;
+          }
+          const double inv = 1.0 / Dk;
+          const int i = k + 1 + lane;
+          if (i < k1) {
+            const double lik = M[tri(i) + k] * inv;
+            double* Mi = M + tri(i);
+            for (int j = k + 1; j <= i; ++j) Mi[j] -= lik * M[tri(j) + k];
+          }
+          __syncwarp();
+          if (lane == 0) {
+            vinv[k] = inv;
+            vdiag[k] = code;
+          }
+        }
       }
-      const double inv = 1.0 / Dk;
-      if (tid == 0) vinv[k] = inv;
-      for (int i = k + 1 + ty; i < m; i += TY) {
-        const double lik = M[i * ld + k] * inv;
-        double* Mi = M + i * ld;
-        for (int j = k + 1 + tx; j <= i; j += TX) Mi[j] -= lik * M[j * ld + k];
+      __syncthreads();
+      for (int k = k0; k < k1; ++k) {
+        const double code = vdiag[k];
+        if (code == 1.0) ++drops;
+        if (code == 2.0) fail = 1;
+      }
+      for (int i = k1 + tid; i < m; i += NT) {
+        double r[KB];
+        double* Mi = M + tri(i) + k0;
+#pragma unroll
+        for (int a = 0; a < KB; ++a) r[a] = k0 + a < k1 ? Mi[a] : 0.0;
+#pragma unroll
+        for (int a = 0; a < KB; ++a) {
+          if (k0 + a < k1) {
+            const double l = r[a] * vinv[k0 + a];
+#pragma unroll
+            for (int c = a + 1; c < KB; ++c)
+              if (k0 + c < k1) r[c] -= l * M[tri(k0 + c) + k0 + a];
+          }
+        }
+#pragma unroll
+        for (int a = 0; a < KB; ++a)
+          if (k0 + a < k1) Mi[a] = r[a];
+      }
+      __syncthreads();
+      const int tt = (m - k1 + 3) >> 2;
+      const int ntiles = tt * (tt + 1) / 2;
+      for (int tile = tid; tile < ntiles; tile += NT) {
+        int ti = static_cast<int>((sqrtf(8.0f * tile + 1.0f) - 1.0f) * 0.5f);
+        while (ti * (ti + 1) / 2 > tile) --ti;
+        while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
+        const int tj = tile - ti * (ti + 1) / 2;
+        const int i0 = k1 + 4 * ti, j0 = k1 + 4 * tj;
+        // rows past m are clamped to m - 1 and columns to the row (in-bounds loads, stores masked)
+        int ri4[4], rj4[4], iq[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          iq[q] = min(i0 + q, m - 1);
+          ri4[q] = tri(iq[q]);
+          rj4[q] = tri(min(j0 + q, m - 1));
+        }
+        double acc[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) acc[q][r] = M[ri4[q] + min(j0 + r, iq[q])];
+        for (int k = k0; k < k1; ++k) {
+          const double inv = vinv[k];
+          double li[4], lj[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            li[q] = M[ri4[q] + k] * inv;
+            lj[q] = M[rj4[q] + k];
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[q][r] -= li[q] * lj[r];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if (i0 + q < m && j0 + r <= i0 + q) M[ri4[q] + j0 + r] = acc[q][r];
       }
       __syncthreads();
     }
   };
 
-  // ---- solve L D L' z = rhs in place (warp 0), rows owned by lane = i mod 32 ----
+  // ---- solve L D L' z = rhs in place (warp 0) ----
+  // Lane l holds rows l, l + 32, l + 64, l + 96 of z (and of 1/D) in registers; step k broadcasts
+  // the finished entry with a shuffle, so the serial chain per step is shuffle + FMA with the
+  // shared-memory loads of L~ off the chain. Same operations, in the same order, as the
+  // row-at-a-time substitution: forward w_k = z_k / D_k, z_i -= L~_ik w_k (L~ = L D); backward
+  // x_k = w_k - (1/D_k) sum_{j>k} L~_jk x_j.
   auto solve = [&]() {
     if (warp == 0) {
-      for (int i = lane; i < m; i += 32) vacc[i] = 0.0;
-      __syncwarp();
-      for (int k = 0; k < m; ++k) {
-        const double wk = vz[k] * vinv[k];
-        __syncwarp();
-        if (lane == (k & 31)) vz[k] = wk;
-        for (int i = k + 1 + ((lane - (k + 1)) & 31); i < m; i += 32) vz[i] -= M[i * ld + k] * wk;
-        __syncwarp();
+      double zr[4], ir[4], ar[4];
+      int ro[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = t * 32 + lane;
+        zr[t] = i < m ? vz[i] : 0.0;
+        ir[t] = i < m ? vinv[i] : 0.0;
+        ar[t] = 0.0;
+        ro[t] = tri(min(i, m - 1));
       }
-      for (int k = m - 1; k >= 0; --k) {
-        const double xk = vz[k] - vinv[k] * vacc[k];
-        __syncwarp();
-        if (lane == (k & 31)) vz[k] = xk;
-        for (int i = lane; i < k; i += 32) vacc[i] += M[k * ld + i] * xk;
-        __syncwarp();
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int kend = min(32, m - t * 32);
+        for (int kk = 0; kk < kend; ++kk) {
+          const int k = t * 32 + kk;
+          const double wk = __shfl_sync(0xffffffffu, zr[t], kk) * __shfl_sync(0xffffffffu, ir[t], kk);
+          if (lane == kk) zr[t] = wk;
+#pragma unroll
+          for (int u = t; u < 4; ++u) {
+            const int i = u * 32 + lane;
+            if (i > k && i < m) zr[u] -= M[ro[u] + k] * wk;
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 3; t >= 0; --t) {
+        const int kstart = min(31, m - 1 - t * 32);
+        for (int kk = kstart; kk >= 0; --kk) {
+          const int k = t * 32 + kk;
+          const double own = zr[t] - ir[t] * ar[t];
+          const double xk = __shfl_sync(0xffffffffu, own, kk);
+          if (lane == kk) zr[t] = xk;
+          const int rk = tri(k);
+#pragma unroll
+          for (int u = 0; u <= t; ++u) {
+            const int i = u * 32 + lane;
+            if (i < k) ar[u] += M[rk + i] * xk;
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = t * 32 + lane;
+        if (i < m) vz[i] = zr[t];
       }
     }
     __syncthreads();
   };
 
+  // sum_p a_pj v[row_p] over column j, the first two entries loaded unconditionally-predicated so
+  // the loads of several columns can be in flight together
+  auto col_dot = [&](int pb, int pe, const double* v) {
+    const bool h0 = pb < pe, h1 = pb + 1 < pe;
+    const int r0 = h0 ? ri[pb] : 0, r1 = h1 ? ri[pb + 1] : 0;
+    const double a0 = h0 ? cv[pb] : 0.0, a1 = h1 ? cv[pb + 1] : 0.0;
+    double acc = a0 * v[r0] + a1 * v[r1];
+    for (int p = pb + 2; p < pe; ++p) acc += cv[p] * v[ri[p]];
+    return acc;
+  };
+  constexpr int U = 4;  // columns per thread per pass, loads issued before use
+
   // ---- Mehrotra-like start (interior_point.cpp:488-506) ----
-  assemble(2);
-  factor();
-  for (int i = warp; i < m; i += NW) {
-    double acc = 0.0;
-    for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) acc += rv[p];
-    acc = warp_sum(acc);
-    if (lane == 0) vz[i] = b[i] - acc;
-  }
+  // per-column scratch of an iteration: d = x/s in ds, t = d rd - rxs/s in dx (both free between
+  // the update of one iteration and the direction pass that overwrites them)
+  double* dvec = ds;
+  double* tvec = dx;
+  for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
   __syncthreads();
+  for (int j = tid; j < n; j += NT) offdiag(cp[j], cp[j + 1], 1.0);
+  __syncthreads();
+  row_pass(0, nullptr, nullptr);
+  __syncthreads();
+  factor();
   solve();
   const bool start_ok = !fail;
   for (int j = tid; j < n; j += NT) {
@@ -228,6 +416,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     vy[i] = start_ok ? vz[i] : 0.0;
     gby[i] = vy[i];
   }
+  for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
   fail = 0;
   __syncthreads();
 
@@ -237,27 +426,42 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   double last_gap = 0, last_p = 0, last_d = 0, last_cx = 0;
   const int ops_res[4] = {1, 1, 0, 0};
   for (int it = 0; it < mt.max_iter; ++it) {
-    // residuals
-    double rpm = 0.0;
-    for (int i = warp; i < m; i += NW) {
-      double acc = 0.0;
-      for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) acc += rv[p] * x[ci[p]];
-      acc = warp_sum(acc);
-      const double r = b[i] - acc;
-      if (lane == 0) vrp[i] = r;
-      rpm = fmax(rpm, fabs(r));
-    }
+    // residuals, with the predictor's right-hand side and the normal matrix built in the same two
+    // passes (interior_point.cpp:572-582, :418-432, :74-101)
     double rdm = 0.0, xs = 0.0, cx = 0.0;
-    for (int j = tid; j < n; j += NT) {
-      double aty = 0.0;
-      for (int p = cp[j]; p < cp[j + 1]; ++p) aty += cv[p] * vy[ri[p]];
-      const double xj = x[j], sj = s[j];
-      const double r = c[j] - (aty + sj);
-      rd[j] = r;
-      rdm = fmax(rdm, fabs(r));
-      xs += xj * sj;
-      cx += c[j] * xj;
+    for (int j0 = tid; j0 < n; j0 += U * NT) {
+      int pb[U], pe[U];
+      double xv[U], sv[U], cvv[U], aty[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = min(j0 + u * NT, n - 1);
+        pb[u] = cp[j];
+        pe[u] = cp[j + 1];
+        xv[u] = x[j];
+        sv[u] = s[j];
+        cvv[u] = c[j];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) aty[u] = col_dot(pb[u], pe[u], vy);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = j0 + u * NT;
+        if (j >= n) continue;
+        const double r = cvv[u] - (aty[u] + sv[u]);
+        rd[j] = r;
+        rdm = fmax(rdm, fabs(r));
+        xs += xv[u] * sv[u];
+        cx += cvv[u] * xv[u];
+        const double xj = fmax(xv[u], 1e-16), sj = fmax(sv[u], 1e-16);
+        const double dj = xj / sj;
+        const double rxs = -xv[u] * sv[u];
+        dvec[j] = dj;
+        tvec[j] = dj * r - rxs / sj;
+        offdiag(pb[u], pe[u], dj);
+      }
     }
+    __syncthreads();
+    const double rpm = row_pass(1, dvec, tvec);
     double v[4] = {rpm, rdm, xs, cx};
     cta_reduce4<NT>(v, ops_res, red);
     if (tid == 0) {
@@ -296,8 +500,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       iters = it + 1;
       break;
     }
-    // factor A diag(x/s) A'
-    assemble(0);
+    // factor A diag(x/s) A' (assembled by the residual passes)
     factor();
     if (fail) {
       status = -2;  // factorization failure: best iterate
@@ -306,34 +509,67 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     // predictor and corrector
     for (int pass = 0; pass < 2; ++pass) {
       const double sigma_mu = pass ? cs.v[S_SIGMA] * mu : 0.0;
-      for (int i = warp; i < m; i += NW) {
-        double acc = 0.0;
-        for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) {
-          const int j = ci[p];
-          const double xj = fmax(x[j], 1e-16), sj = fmax(s[j], 1e-16);
-          const double rxs = pass ? -x[j] * s[j] - dxa[j] * dsa[j] + sigma_mu : -x[j] * s[j];
-          acc += rv[p] * ((xj / sj) * rd[j] - rxs / sj);
+      if (pass == 1) {
+        // corrector right-hand side: t = d rd - rxs/s with rxs = -x s - dx_aff ds_aff + sigma mu
+        // (interior_point.cpp:676-681), then z = rp + A t; the predictor's was built with the residuals
+        for (int j0 = tid; j0 < n; j0 += U * NT) {
+          double xv[U], sv[U], rdv[U], av[U], bv[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int j = min(j0 + u * NT, n - 1);
+            xv[u] = x[j];
+            sv[u] = s[j];
+            rdv[u] = rd[j];
+            av[u] = dxa[j];
+            bv[u] = dsa[j];
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int j = j0 + u * NT;
+            if (j >= n) continue;
+            const double xj = fmax(xv[u], 1e-16), sj = fmax(sv[u], 1e-16);
+            const double rxs = -xv[u] * sv[u] - av[u] * bv[u] + sigma_mu;
+            tvec[j] = (xj / sj) * rdv[u] - rxs / sj;
+          }
         }
-        acc = warp_sum(acc);
-        if (lane == 0) vz[i] = vrp[i] + acc;
+        __syncthreads();
+        row_pass(2, nullptr, tvec);
+        __syncthreads();
       }
-      __syncthreads();
       solve();
       double* ddx = pass ? dx : dxa;
       double* dds = pass ? ds : dsa;
       double rpmin = 1.0, rdmin = 1.0;
-      for (int j = tid; j < n; j += NT) {
-        double atdy = 0.0;
-        for (int p = cp[j]; p < cp[j + 1]; ++p) atdy += cv[p] * vz[ri[p]];
-        const double xj = x[j], sj = s[j];
-        const double rxs = pass ? -xj * sj - dxa[j] * dsa[j] + sigma_mu : -xj * sj;
-        const double dj = fmax(xj, 1e-16) / fmax(sj, 1e-16);
-        const double dxj = dj * (atdy - rd[j]) + rxs / fmax(sj, 1e-16);
-        const double dsj = rd[j] - atdy;
-        ddx[j] = dxj;
-        dds[j] = dsj;
-        if (dxj < 0.0) rpmin = fmin(rpmin, -xj / dxj);
-        if (dsj < 0.0) rdmin = fmin(rdmin, -sj / dsj);
+      for (int j0 = tid; j0 < n; j0 += U * NT) {
+        int pb[U], pe[U];
+        double xv[U], sv[U], rdv[U], av[U], bv[U], atdy[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = min(j0 + u * NT, n - 1);
+          pb[u] = cp[j];
+          pe[u] = cp[j + 1];
+          xv[u] = x[j];
+          sv[u] = s[j];
+          rdv[u] = rd[j];
+          av[u] = pass ? dxa[j] : 0.0;
+          bv[u] = pass ? dsa[j] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) atdy[u] = col_dot(pb[u], pe[u], vz);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = j0 + u * NT;
+          if (j >= n) continue;
+          const double xj = xv[u], sj = sv[u];
+          const double rxs = pass ? -xj * sj - av[u] * bv[u] + sigma_mu : -xj * sj;
+          const double dj = fmax(xj, 1e-16) / fmax(sj, 1e-16);
+          const double dxj = dj * (atdy[u] - rdv[u]) + rxs / fmax(sj, 1e-16);
+          const double dsj = rdv[u] - atdy[u];
+          ddx[j] = dxj;
+          dds[j] = dsj;
+          if (dxj < 0.0) rpmin = fmin(rpmin, -xj / dxj);
+          if (dsj < 0.0) rdmin = fmin(rdmin, -sj / dsj);
+        }
       }
       double u[4] = {rpmin, rdmin, 0.0, 0.0};
       const int ops_min[4] = {2, 2, 0, 0};
@@ -351,7 +587,20 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       if (pass == 0) {
         const double apa = cs.v[S_APAFF], ada = cs.v[S_ADAFF];
         double acc = 0.0;
-        for (int j = tid; j < n; j += NT) acc += (x[j] + apa * dxa[j]) * (s[j] + ada * dsa[j]);
+        for (int j0 = tid; j0 < n; j0 += U * NT) {
+          double xv[U], sv[U], av[U], bv[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int j = min(j0 + u * NT, n - 1);
+            xv[u] = x[j];
+            sv[u] = s[j];
+            av[u] = dxa[j];
+            bv[u] = dsa[j];
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (j0 + u * NT < n) acc += (xv[u] + apa * av[u]) * (sv[u] + ada * bv[u]);
+        }
         double w4[4] = {acc, 0.0, 0.0, 0.0};
         const int ops_sum[4] = {0, 0, 0, 0};
         cta_reduce4<NT>(w4, ops_sum, red);
@@ -365,11 +614,26 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     }
     // update (interior_point.cpp:709-718)
     const double ap = cs.v[S_AP], ad = cs.v[S_AD];
-    for (int j = tid; j < n; j += NT) {
-      x[j] = fmax(x[j] + ap * dx[j], 1e-14);
-      s[j] = fmax(s[j] + ad * ds[j], 1e-14);
+    for (int j0 = tid; j0 < n; j0 += U * NT) {
+      double xv[U], sv[U], av[U], bv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = min(j0 + u * NT, n - 1);
+        xv[u] = x[j];
+        sv[u] = s[j];
+        av[u] = dx[j];
+        bv[u] = ds[j];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = j0 + u * NT;
+        if (j >= n) continue;
+        x[j] = fmax(xv[u] + ap * av[u], 1e-14);
+        s[j] = fmax(sv[u] + ad * bv[u], 1e-14);
+      }
     }
     for (int i = tid; i < m; i += NT) vy[i] += ad * vz[i];
+    for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
     iters = it + 1;
     __syncthreads();
   }
@@ -417,7 +681,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT <= 256 ? 2 : 1)) k_bat
   }
 }
 
-size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(mmax) * (mmax + 1) + 6 * mmax); }
+size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(mmax)) + 6 * mmax); }
 
 template <int NT>
 void launch_bucket(const BatchDev& bd, int mmax, int grid, cudaStream_t st) {
@@ -540,6 +804,11 @@ struct Batch {
 namespace {
 
 int threads_for(int mmax) {
+  // SOVEREIGN_BATCH_THREADS=128|256|512 pins every bucket (tests run each width this way)
+  if (const char* e = std::getenv("SOVEREIGN_BATCH_THREADS")) {
+    const int t = std::atoi(e);
+    if (t == 128 || t == 256 || t == 512) return t;
+  }
   std::lock_guard<std::mutex> g(g_tune_mu);
   auto it = g_tuned_threads.find(mmax);
   if (it != g_tuned_threads.end()) return it->second;
@@ -592,7 +861,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     mt.m = f.m;
     mt.n = f.n;
     mt.nnz = f.nnz();
-    mt.ld = f.m + 1;
+    mt.pad1 = 0;
     mt.max_iter = opt.max_iterations;
     mt.a_off = nnz;
     mt.cp_off = cols;

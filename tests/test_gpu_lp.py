@@ -9,7 +9,7 @@ import pytest
 
 import oracle
 from sovereign_b200 import abi, problems as P
-from sovereign_b200.ipm import InteriorPointOptions, InteriorPointSolver, solve_batch
+from sovereign_b200.ipm import InteriorPointOptions, InteriorPointSolver, autotune, solve_batch
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -61,6 +61,26 @@ def test_batch_matches_reference():
         assert r.status_name == "OPTIMAL", (k, r.message)
         assert rel(r.objective_value, g["objectives"][k]) < TOL, k
         assert r.iterations <= g["iterations"][k] + 1, k
+
+
+@pytest.mark.parametrize("threads", ["128", "256", "512"])
+def test_batch_every_cta_width(threads, monkeypatch):
+    # the per-bucket thread count is a tuning choice only: every width gives the reference's answers
+    monkeypatch.setenv("SOVEREIGN_BATCH_THREADS", threads)
+    g = LP["transport_batch"]
+    res = solve_batch(P.transport_batch(**g["spec"]))
+    for k, r in enumerate(res):
+        assert r.status_name == "OPTIMAL", (k, r.message)
+        assert rel(r.objective_value, g["objectives"][k]) < TOL, k
+
+
+def test_autotune_reports_every_bucket():
+    models = P.transport_batch(64, seed=5)
+    rep = json.loads(autotune(models))
+    assert rep and all(set(v) >= {"128", "256", "512", "chosen", "count"} for v in rep.values())
+    assert sum(v["count"] for v in rep.values()) == len(models)
+    res = solve_batch(models)
+    assert all(r.status_name == "OPTIMAL" for r in res)
 
 
 def test_batch_mixed_sizes_and_fallback():
