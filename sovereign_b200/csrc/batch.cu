@@ -8,7 +8,7 @@
 // with the reference's dependent-row rule; n-vectors stay in global memory, where
 // the working set of the resident CTAs fits in the 126 MB L2. Size buckets (by m) get their own
 // launch with a shared-memory footprint and thread count chosen per bucket by the autotuner; the
-// bucket launches of a batch run concurrently on streams forked from the caller's stream.
+// bucket launches of a batch run concurrently on forked streams, captured once in a CUDA graph.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -683,11 +683,18 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT <= 256 ? 2 : 1)) k_bat
 
 size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(mmax)) + 6 * mmax); }
 
+// The dynamic shared-memory limit of every instantiation is raised once to the largest bucket's
+// footprint, so launches (and launches captured in a graph) need no per-launch attribute call.
+void ensure_smem_limits() {
+  const int smem = static_cast<int>(batch_smem(kBatchMaxRows));
+  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+}
+
 template <int NT>
 void launch_bucket(const BatchDev& bd, int mmax, int grid, cudaStream_t st) {
-  const size_t smem = batch_smem(mmax);
-  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_batch_ipm<NT><<<grid, NT, smem, st>>>(bd, mmax);
+  k_batch_ipm<NT><<<grid, NT, batch_smem(mmax), st>>>(bd, mmax);
   SOV_LAUNCH_CHECK();
 }
 
@@ -695,7 +702,6 @@ template <int NT>
 int max_ctas(int mmax) {
   int per_sm = 0;
   const size_t smem = batch_smem(mmax);
-  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_ipm<NT>, NT, smem));
   int dev = 0, sms = 0;
   SOV_CUDA(cudaGetDevice(&dev));
@@ -792,7 +798,11 @@ struct Batch {
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> joins;
   cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t graph = nullptr;  // the bucket launches of one solve
   ~Batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (cap) cudaStreamDestroy(cap);
     for (auto s : streams) cudaStreamDestroy(s);
     for (auto e : joins) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -838,6 +848,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   if (opt_in) B->opt = *opt_in;
   else sov_default_lp_options(&B->opt);
   const sov_options& opt = B->opt;
+  ensure_smem_limits();
   // host standard forms (interior_point.cpp:224-409 semantics), in parallel
   parallel_for(count, [&](int i) {
     try {
@@ -972,9 +983,12 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
 }
 
 void batch_solve(Batch* B, cudaStream_t st) {
-  // Buckets run concurrently: each on its own stream forked from (and joined back into) the
-  // caller's stream, so the few large LPs do not hold the SMs the smaller buckets could use.
-  if (B->streams.empty()) {
+  // Buckets run concurrently: each on its own stream forked from (and joined back into) one
+  // capture stream, so the few large LPs do not hold the SMs the smaller buckets could use. The
+  // fork / reset / launch / join sequence is captured once into a CUDA graph and replayed on the
+  // caller's stream by every solve.
+  if (!B->graph) {
+    SOV_CUDA(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
     for (size_t b = 0; b < B->buckets.size(); ++b) {
       cudaStream_t s2;
       SOV_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
@@ -986,29 +1000,34 @@ void batch_solve(Batch* B, cudaStream_t st) {
     SOV_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
     SOV_CUDA(cudaEventCreate(&B->t0));
     SOV_CUDA(cudaEventCreate(&B->t1));
+    SOV_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
+    SOV_CUDA(cudaEventRecord(B->fork, B->cap));
+    for (size_t b = 0; b < B->buckets.size(); ++b) {
+      auto& bk = B->buckets[b];
+      cudaStream_t s2 = B->streams[b];
+      SOV_CUDA(cudaStreamWaitEvent(s2, B->fork, 0));
+      SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), s2));
+      BatchDev d = B->dev;
+      d.order = bk->order.p;
+      d.count = bk->count;
+      d.next = bk->next.p;
+      launch_any(d, bk->mmax, bk->threads, bk->grid, s2);
+      SOV_CUDA(cudaEventRecord(B->joins[b], s2));
+      SOV_CUDA(cudaStreamWaitEvent(B->cap, B->joins[b], 0));
+    }
+    cudaGraph_t g = nullptr;
+    SOV_CUDA(cudaStreamEndCapture(B->cap, &g));
+    const cudaError_t e = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    SOV_CUDA(e);
   }
   SOV_CUDA(cudaEventRecord(B->t0, st));
-  SOV_CUDA(cudaEventRecord(B->fork, st));
-  int launches = 0;
-  for (size_t b = 0; b < B->buckets.size(); ++b) {
-    auto& bk = B->buckets[b];
-    cudaStream_t s2 = B->streams[b];
-    SOV_CUDA(cudaStreamWaitEvent(s2, B->fork, 0));
-    SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), s2));
-    BatchDev d = B->dev;
-    d.order = bk->order.p;
-    d.count = bk->count;
-    d.next = bk->next.p;
-    launch_any(d, bk->mmax, bk->threads, bk->grid, s2);
-    SOV_CUDA(cudaEventRecord(B->joins[b], s2));
-    SOV_CUDA(cudaStreamWaitEvent(st, B->joins[b], 0));
-    ++launches;
-  }
+  SOV_CUDA(cudaGraphLaunch(B->graph, st));
   SOV_CUDA(cudaEventRecord(B->t1, st));
   SOV_CUDA(cudaEventSynchronize(B->t1));
   float ms = 0.f;
   SOV_CUDA(cudaEventElapsedTime(&ms, B->t0, B->t1));
-  B->launches = launches;
+  B->launches = static_cast<int>(B->buckets.size());
   B->kernel_ms = ms;
 }
 

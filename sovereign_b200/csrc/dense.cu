@@ -89,12 +89,13 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Diagonal block (64 x 64) on 256 threads, in four 16-column sub-panels: warp 0 factors the 16 x 16
-// diagonal sub-block warp-synchronously (the pivot rule per column), each row below is solved
-// against it by one thread, and all threads update the trailing lower part. Then the inverse of the
-// 64 x 64 factor, four threads per column (shuffle-reduced dot products).
+// Diagonal block (64 x 64) on 256 threads, right-looking over 8-column panels, three barriers per
+// panel: warp 0 factors the 8 x 8 diagonal block (lane = row, the pivot rule per column), one
+// thread per row below solves its 8 panel entries against it in registers, and the trailing lower
+// triangle takes the panel's rank-8 update in 4 x 4 register tiles (one tile per thread). Then
+// the inverse of the 64 x 64 factor, four threads per column (shuffle-reduced dot products).
 // ---------------------------------------------------------------------------------------------
-constexpr int kSub = 16;
+constexpr int kPanel = 8;
 
 template <class T>
 __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
@@ -103,6 +104,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, i
   extern __shared__ __align__(16) unsigned char potrf_raw[];
   T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
   T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
+  __shared__ T rinv[kNB];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = kb * kNB;
   for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
@@ -111,11 +113,12 @@ __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, i
   }
   __syncthreads();
   int drops = 0, bad = 0;
-  for (int k0 = 0; k0 < kNB; k0 += kSub) {
-    // 1. factor A[k0:k0+16, k0:k0+16] (warp 0; lane i owns row k0 + i)
+  for (int k0 = 0; k0 < kNB; k0 += kPanel) {
+    const int k1 = k0 + kPanel;
+    // 1. the 8 x 8 diagonal block (warp 0, lane c = row k0 + c)
     if (warp == 0) {
-      for (int j = k0; j < k0 + kSub; ++j) {
-        __syncwarp();
+      const int i = k0 + lane;
+      for (int j = k0; j < k1; ++j) {
         const T p = A[j][j];
         const int gj = r0 + j;
         const double dref = gj < m ? diag[gj] : 1.0;
@@ -127,42 +130,75 @@ __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, i
           drop = true;  // dependent row (sparse_ldlt.cpp:165-173)
         }
         const T ljj = drop ? big_pivot<T>() : sqrt(p);
+        const T inv = T(1) / ljj;
         if (drop && gj < m) ++drops;
-        __syncwarp();
-        const int i = k0 + lane;
-        if (lane < kSub) {
-          if (i == j) A[j][j] = ljj;
-          if (i > j) A[i][j] = A[i][j] / ljj;
+        if (lane < kPanel && i > j) A[i][j] *= inv;
+        if (lane == 0) {
+          A[j][j] = ljj;
+          rinv[j] = inv;
         }
         __syncwarp();
-        if (lane < kSub && i > j) {
+        if (lane < kPanel && i > j) {
           const T lij = A[i][j];
-          for (int k = j + 1; k <= i; ++k) A[i][k] -= lij * A[k][j];
-        }
-      }
-    }
-    __syncthreads();
-    const int rest = kNB - (k0 + kSub);
-    if (rest <= 0) break;
-    // 2. rows below: L[i][k0:k0+16] = A[i][k0:k0+16] L_kk^-T (forward substitution, one row per thread)
-    if (tid < rest) {
-      const int i = k0 + kSub + tid;
-      for (int c = k0; c < k0 + kSub; ++c) {
-        T v = A[i][c];
-        for (int k = k0; k < c; ++k) v -= A[i][k] * A[c][k];
-        A[i][c] = v / A[c][c];
-      }
-    }
-    __syncthreads();
-    // 3. trailing update A[i][j] -= sum_k L[i][k] L[j][k] over the sub-panel, k0+16 <= j <= i
-    const int tot = rest * rest;
-    for (int t = tid; t < tot; t += blockDim.x) {
-      const int i = k0 + kSub + t / rest, j = k0 + kSub + t % rest;
-      if (j > i) continue;
-      T acc = T(0);
 #pragma unroll
-      for (int k = 0; k < kSub; ++k) acc += A[i][k0 + k] * A[j][k0 + k];
-      A[i][j] -= acc;
+          for (int k = 1; k < kPanel; ++k)
+            if (j + k <= i) A[i][j + k] -= lij * A[j + k][j];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    if (k1 >= kNB) break;
+    // 2. rows below: L[i][k0:k1] = A[i][k0:k1] L_kk^-T, one row per thread, in registers
+    if (tid < kNB - k1) {
+      const int i = k1 + tid;
+      T r[kPanel];
+#pragma unroll
+      for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
+#pragma unroll
+      for (int c = 0; c < kPanel; ++c) {
+        r[c] *= rinv[k0 + c];
+#pragma unroll
+        for (int d = c + 1; d < kPanel; ++d) r[d] -= r[c] * A[k0 + d][k0 + c];
+      }
+#pragma unroll
+      for (int c = 0; c < kPanel; ++c) A[i][k0 + c] = r[c];
+    }
+    __syncthreads();
+    // 3. trailing lower triangle: A[i][j] -= sum_k L[i][k] L[j][k], 4 x 4 tiles
+    {
+      const int nt = (kNB - k1) / 4;
+      const int ntiles = nt * (nt + 1) / 2;
+      if (tid < ntiles) {
+        int ti = static_cast<int>((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
+        while (ti * (ti + 1) / 2 > tid) --ti;
+        while ((ti + 1) * (ti + 2) / 2 <= tid) ++ti;
+        const int tj = tid - ti * (ti + 1) / 2;
+        const int i0 = k1 + 4 * ti, j0 = k1 + 4 * tj;
+        T acc[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int u = 0; u < 4; ++u) acc[q][u] = A[i0 + q][j0 + u];
+#pragma unroll
+        for (int k = k0; k < k1; ++k) {
+          T li[4], lj[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            li[q] = A[i0 + q][k];
+            lj[q] = A[j0 + q][k];
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[q][u] -= li[q] * lj[u];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (j0 + u <= i0 + q) A[i0 + q][j0 + u] = acc[q][u];
+      }
     }
     __syncthreads();
   }
