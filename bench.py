@@ -338,8 +338,16 @@ def main():
     kernel_s = stats["kernel_ms"] * 1e-3
     pk = peaks()
     achieved = alg_bytes / kernel_s / 1e9
+    traffic = None
+    try:  # DRAM bytes of one full-size step from the committed ncu capture (profiles/)
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")) as fh:
+            if count == COUNT:
+                traffic = json.load(fh)["k_batch_ipm"]["dram_bytes_per_step"]
+    except (OSError, KeyError, ValueError):
+        pass
     roofline = dict(bound="hbm", achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
-                    frac=achieved / pk["hbm_gbs"], traffic=None,
+                    frac=achieved / pk["hbm_gbs"], traffic=traffic,
+                    algorithmic_bytes_per_step=alg_bytes, traffic_unit="bytes per step (ncu, serialised buckets)",
                     kernel="k_batch_ipm", peak_source=pk["source"],
                     note="algorithmic bytes = sum over LPs of (iterations + 1) x [6 SpMV x (12 nnz + 8(m+n)) + "
                          "15 x 8n + 10 x 8m]; kernel time from CUDA events of the last step")

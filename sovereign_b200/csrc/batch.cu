@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <numeric>
 #include <sstream>
 #include <thread>
@@ -709,16 +710,133 @@ int max_ctas(int mmax) {
   return std::max(1, per_sm) * sms;
 }
 
+// Per-device cache of released device blocks: a batch created per end-to-end call (hundreds of MB
+// of inputs and work vectors) reuses the previous call's memory instead of paying cudaMalloc and
+// cudaFree each time. A block is reused for a request of at least half its size; at most
+// kMaxCached bytes stay cached, and a failed cudaMalloc first returns the cache to the device.
+// Blocks return to the cache only after the batch's work has finished (every batch operation is
+// synchronous with respect to its own device memory).
+class DevicePool {
+ public:
+  void* acquire(size_t bytes, size_t* got) {
+    int dev = 0;
+    SOV_CUDA(cudaGetDevice(&dev));
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      for (auto it = free_.lower_bound(bytes); it != free_.end() && it->first <= 2 * bytes + (1u << 20); ++it) {
+        if (it->second.first != dev) continue;
+        void* p = it->second.second;
+        *got = it->first;
+        cached_ -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      trim(0);
+      SOV_CUDA(cudaMalloc(&p, bytes));
+    }
+    *got = bytes;
+    return p;
+  }
+  void release(void* p, size_t bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      free_.emplace(bytes, std::make_pair(dev, p));
+      cached_ += bytes;
+    }
+    trim(kMaxCached);
+  }
+  // free cached blocks (largest first) until at most `keep` bytes stay cached
+  void trim(size_t keep) {
+    std::lock_guard<std::mutex> g(mu_);
+    while (cached_ > keep && !free_.empty()) {
+      auto it = std::prev(free_.end());
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(it->second.first);
+      cudaFree(it->second.second);
+      cudaSetDevice(cur);
+      cached_ -= it->first;
+      free_.erase(it);
+    }
+  }
+
+ private:
+  static constexpr size_t kMaxCached = size_t(4) << 30;
+  std::mutex mu_;
+  std::multimap<size_t, std::pair<int, void*>> free_;
+  size_t cached_ = 0;
+};
+DevicePool g_dpool;
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0, cap_bytes = 0;
   void alloc(size_t count) {
-    if (count) SOV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+    if (count) p = static_cast<T*>(g_dpool.acquire(sizeof(T) * count, &cap_bytes));
     n = count;
   }
   ~DBuf() {
-    if (p) cudaFree(p);
+    if (p) g_dpool.release(p, cap_bytes);
+  }
+};
+
+// Host counterpart for per-batch host arrays (the publishing data of every LP): released blocks
+// stay mapped and are reused, so building a batch does not page-fault fresh memory each call.
+class HostPool {
+ public:
+  void* acquire(size_t bytes, size_t* got) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      auto it = free_.lower_bound(bytes);
+      if (it != free_.end() && it->first <= 2 * bytes + (1u << 20)) {
+        void* p = it->second;
+        *got = it->first;
+        cached_ -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    void* p = std::malloc(bytes);
+    if (!p) throw std::bad_alloc();
+    *got = bytes;
+    return p;
+  }
+  void release(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    free_.emplace(bytes, p);
+    cached_ += bytes;
+    while (cached_ > kMaxCached && !free_.empty()) {
+      auto it = std::prev(free_.end());
+      std::free(it->second);
+      cached_ -= it->first;
+      free_.erase(it);
+    }
+  }
+
+ private:
+  static constexpr size_t kMaxCached = size_t(2) << 30;
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  size_t cached_ = 0;
+};
+HostPool g_hpool;
+
+template <class T>
+struct HBuf {
+  T* p = nullptr;
+  size_t cap_bytes = 0;
+  void alloc(size_t count) {
+    if (count) p = static_cast<T*>(g_hpool.acquire(sizeof(T) * count, &cap_bytes));
+  }
+  ~HBuf() {
+    if (p) g_hpool.release(p, cap_bytes);
   }
 };
 
@@ -775,8 +893,17 @@ void parallel_for(int count, F fn) {
 struct Batch {
   int count = 0;
   std::vector<sov_model> models;
-  std::vector<StdForm> forms;
+  std::vector<StdForm> forms;  // only for LPs not built in place (non-plain columns, or too large)
   std::vector<LpMeta> meta;
+  // publishing (interior_point.cpp:521-569): per LP its sizes and where its shift / column and
+  // row scales sit in `pubdata`
+  struct Pub {
+    int n_struct, m0, n, m;
+    long long shift_off, cs_off, rs_off;
+    LpFormInfo info;
+  };
+  std::vector<Pub> pub;
+  HBuf<double> pubdata;
   std::vector<int> fallback;  // LPs too large for the batched kernel
   sov_options opt{};
   struct Bucket {
@@ -848,59 +975,79 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   if (opt_in) B->opt = *opt_in;
   else sov_default_lp_options(&B->opt);
   const sov_options& opt = B->opt;
+  const bool scaling = opt.enable_scaling != 0;
   ensure_smem_limits();
-  // host standard forms (interior_point.cpp:224-409 semantics), in parallel
+  // 1. shapes, in parallel. LPs with plain columns are later built in place, straight into the
+  //    pinned staging; the others get a StdForm here (build_ipm_form semantics,
+  //    interior_point.cpp:224-409), batched if small enough, else solved by the single engine.
+  enum : uint8_t { kInPlace = 0, kFromForm = 1, kSingle = 2 };
+  std::vector<LpShape> shape(count);
+  std::vector<uint8_t> kind(count);
   parallel_for(count, [&](int i) {
+    LpShape sh{};
+    if (plain_lp_shape(models[i], &sh) && sh.m > 0 && sh.m <= kBatchMaxRows && sh.n > 0) {
+      shape[i] = sh;
+      kind[i] = kInPlace;
+      return;
+    }
     try {
-      B->forms[i] = build_std_form(models[i], false, opt.enable_scaling != 0);
+      B->forms[i] = build_std_form(models[i], false, scaling);
     } catch (const std::exception& e) {
       throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
     }
-  });
-  // offsets (serial prefix), then parallel packing into pinned staging
-  B->meta.resize(count);
-  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0;
-  for (int i = 0; i < count; ++i) {
     const StdForm& f = B->forms[i];
+    shape[i] = LpShape{f.n_struct, f.m0, f.m, f.n, f.nnz(), 0};
+    kind[i] = (f.m > 0 && f.m <= kBatchMaxRows && f.n > 0) ? kFromForm : kSingle;
+  });
+  // 2. offsets (serial prefix over the LPs)
+  B->meta.resize(count);
+  B->pub.resize(count);
+  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0, pubn = 0;
+  for (int i = 0; i < count; ++i) {
+    const LpShape& sh = shape[i];
     LpMeta& mt = B->meta[i];
     std::memset(&mt, 0, sizeof(mt));
-    if (f.m <= 0 || f.m > kBatchMaxRows || f.n <= 0) {
+    if (kind[i] == kSingle) {
       B->fallback.push_back(i);
       mt.m = -1;
       continue;
     }
-    mt.m = f.m;
-    mt.n = f.n;
-    mt.nnz = f.nnz();
-    mt.pad1 = 0;
+    mt.m = sh.m;
+    mt.n = sh.n;
+    mt.nnz = sh.nnz;
     mt.max_iter = opt.max_iterations;
     mt.a_off = nnz;
     mt.cp_off = cols;
     mt.rp_off = rows;
     mt.mv_off = mv;
     mt.nv_off = nv;
-    double bmax = 0.0, cmax = 0.0;
-    for (double v : f.b) bmax = std::max(bmax, std::abs(v));
-    for (double v : f.c) cmax = std::max(cmax, std::abs(v));
-    mt.bnorm = std::max(1.0, bmax);
-    mt.cnorm = std::max(1.0, cmax);
     mt.ftol = opt.feasibility_tol;
     mt.otol = opt.optimality_tol;
     mt.tau = opt.fraction_to_boundary;
-    nnz += f.nnz();
-    cols += f.n + 1;
-    rows += f.m + 1;
-    nv += f.n;
-    mv += f.m;
+    Batch::Pub& pb = B->pub[i];
+    pb.n_struct = sh.n_struct;
+    pb.m0 = sh.m0;
+    pb.n = sh.n;
+    pb.m = sh.m;
+    pb.shift_off = pubn;
+    pb.cs_off = pubn + sh.n_struct;
+    pb.rs_off = pubn + sh.n_struct + sh.n;
+    pubn += sh.n_struct + sh.n + sh.m;
+    nnz += sh.nnz;
+    cols += sh.n + 1;
+    rows += sh.m + 1;
+    nv += sh.n;
+    mv += sh.m;
     // algorithmic work per iteration (roofline): vector bytes + factorization flops
-    B->bytes += 6.0 * (12.0 * f.nnz() + 8.0 * (f.m + f.n)) + 15.0 * 8.0 * f.n + 10.0 * 8.0 * f.m;
-    B->flops += (2.0 / 3.0) * std::pow(static_cast<double>(f.m), 3.0);
+    B->bytes += 6.0 * (12.0 * sh.nnz + 8.0 * (sh.m + sh.n)) + 15.0 * 8.0 * sh.n + 10.0 * 8.0 * sh.m;
+    B->flops += (2.0 / 3.0) * std::pow(static_cast<double>(sh.m), 3.0);
   }
   B->total_n = nv;
   B->total_m = mv;
   B->total_nnz = nnz;
   B->total_cols = cols;
   B->total_rows = rows;
+  B->pubdata.alloc(static_cast<size_t>(std::max(1LL, pubn)));
   // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c
   const size_t o_meta = 0;
   const size_t o_cp = align8(o_meta + sizeof(LpMeta) * count);
@@ -913,22 +1060,52 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   const size_t o_c = o_b + sizeof(double) * mv;
   const size_t total = o_c + sizeof(double) * nv;
   B->h2d_bytes = static_cast<double>(total);
+  // 3. every LP's standard form written into its slots of the pinned staging, in parallel
   std::lock_guard<std::mutex> lock(g_arena.mu);
   unsigned char* h = g_arena.get(total);
-  std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
+  double* pubd = B->pubdata.p;
   parallel_for(count, [&](int i) {
-    const LpMeta& mt = B->meta[i];
+    LpMeta& mt = B->meta[i];
     if (mt.m < 0) return;
-    const StdForm& f = B->forms[i];
-    std::memcpy(h + o_cp + sizeof(int) * mt.cp_off, f.col_ptr.data(), sizeof(int) * (f.n + 1));
-    std::memcpy(h + o_ri + sizeof(int) * mt.a_off, f.row_idx.data(), sizeof(int) * f.nnz());
-    std::memcpy(h + o_rp + sizeof(int) * mt.rp_off, f.row_ptr.data(), sizeof(int) * (f.m + 1));
-    std::memcpy(h + o_ci + sizeof(int) * mt.a_off, f.col_idx.data(), sizeof(int) * f.nnz());
-    std::memcpy(h + o_cv + sizeof(double) * mt.a_off, f.val.data(), sizeof(double) * f.nnz());
-    std::memcpy(h + o_rv + sizeof(double) * mt.a_off, f.rval.data(), sizeof(double) * f.nnz());
-    std::memcpy(h + o_b + sizeof(double) * mt.mv_off, f.b.data(), sizeof(double) * f.m);
-    std::memcpy(h + o_c + sizeof(double) * mt.nv_off, f.c.data(), sizeof(double) * f.n);
+    Batch::Pub& pb = B->pub[i];
+    int* cp = reinterpret_cast<int*>(h + o_cp) + mt.cp_off;
+    int* ri = reinterpret_cast<int*>(h + o_ri) + mt.a_off;
+    int* rp = reinterpret_cast<int*>(h + o_rp) + mt.rp_off;
+    int* ci = reinterpret_cast<int*>(h + o_ci) + mt.a_off;
+    double* cv = reinterpret_cast<double*>(h + o_cv) + mt.a_off;
+    double* rv = reinterpret_cast<double*>(h + o_rv) + mt.a_off;
+    double* bb = reinterpret_cast<double*>(h + o_b) + mt.mv_off;
+    double* cc = reinterpret_cast<double*>(h + o_c) + mt.nv_off;
+    if (kind[i] == kInPlace) {
+      const LpFormOut out{cp, ri, cv, rp, ci, rv, bb, cc, pubd + pb.shift_off, pubd + pb.cs_off, pubd + pb.rs_off};
+      try {
+        build_plain_lp_into(models[i], shape[i], scaling, out, &pb.info);
+      } catch (const std::exception& e) {
+        throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
+      }
+    } else {
+      const StdForm& f = B->forms[i];
+      std::memcpy(cp, f.col_ptr.data(), sizeof(int) * (f.n + 1));
+      std::memcpy(ri, f.row_idx.data(), sizeof(int) * f.nnz());
+      std::memcpy(rp, f.row_ptr.data(), sizeof(int) * (f.m + 1));
+      std::memcpy(ci, f.col_idx.data(), sizeof(int) * f.nnz());
+      std::memcpy(cv, f.val.data(), sizeof(double) * f.nnz());
+      std::memcpy(rv, f.rval.data(), sizeof(double) * f.nnz());
+      std::memcpy(bb, f.b.data(), sizeof(double) * f.m);
+      std::memcpy(cc, f.c.data(), sizeof(double) * f.n);
+      std::copy(f.shift.begin(), f.shift.end(), pubd + pb.shift_off);
+      std::copy(f.col_scale.begin(), f.col_scale.end(), pubd + pb.cs_off);
+      std::copy(f.row_scale.begin(), f.row_scale.end(), pubd + pb.rs_off);
+      pb.info = LpFormInfo{f.scaling_applied, f.coef_min_before, f.coef_max_before, f.coef_min_after,
+                           f.coef_max_after};
+    }
+    double bmax = 0.0, cmax = 0.0;
+    for (int k = 0; k < mt.m; ++k) bmax = std::max(bmax, std::abs(bb[k]));
+    for (int k = 0; k < mt.n; ++k) cmax = std::max(cmax, std::abs(cc[k]));
+    mt.bnorm = std::max(1.0, bmax);
+    mt.cnorm = std::max(1.0, cmax);
   });
+  std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
   B->in.alloc(total);
   SOV_CUDA(cudaMemcpy(B->in.p, h, total, cudaMemcpyHostToDevice));
   B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
@@ -1060,7 +1237,10 @@ void batch_results(Batch* B, sov_result* results) {
     sov_result* r = &results[i];
     const LpMeta& mt = B->meta[i];
     if (mt.m < 0) return;  // solved by the fallback path below
-    const StdForm& f = B->forms[i];
+    const Batch::Pub& f = B->pub[i];
+    const double* shift = B->pubdata.p + f.shift_off;
+    const double* col_scale = B->pubdata.p + f.cs_off;
+    const double* row_scale = B->pubdata.p + f.rs_off;
     const sov_model& mdl = B->models[i];
     const LpOut& o = out[i];
     const bool use_best = o.use_best != 0;
@@ -1078,13 +1258,13 @@ void batch_results(Batch* B, sov_result* results) {
     // publish_iterate (interior_point.cpp:541-563)
     double obj = mdl.obj_constant;
     for (int j = 0; j < f.n_struct; ++j) {
-      const double v = f.shift[j] + f.col_scale[j] * hx[j];
+      const double v = shift[j] + col_scale[j] * hx[j];
       if (r->primal) r->primal[j] = v;
-      if (r->dual_col) r->dual_col[j] = hs[j] / f.col_scale[j];
+      if (r->dual_col) r->dual_col[j] = hs[j] / col_scale[j];
       obj += (mdl.obj ? mdl.obj[j] : 0.0) * v;
     }
     if (r->dual_row)
-      for (int k = 0; k < f.m0; ++k) r->dual_row[k] = f.row_scale[k] * hy[k];
+      for (int k = 0; k < f.m0; ++k) r->dual_row[k] = row_scale[k] * hy[k];
     if (r->ipm_x) std::copy(hx, hx + f.n, r->ipm_x);
     if (r->ipm_s) std::copy(hs, hs + f.n, r->ipm_s);
     if (r->ipm_y) std::copy(hy, hy + f.m, r->ipm_y);
@@ -1107,11 +1287,11 @@ void batch_results(Batch* B, sov_result* results) {
                     mt.max_iter, o.iterations, o.gap, mt.otol, o.p_res, o.d_res);
     if (r->diagnostics) {
       std::memset(r->diagnostics, 0, sizeof(sov_diagnostics));
-      r->diagnostics->scaling_applied = f.scaling_applied;
-      r->diagnostics->coefficient_min_abs_before = f.coef_min_before;
-      r->diagnostics->coefficient_max_abs_before = f.coef_max_before;
-      r->diagnostics->coefficient_min_abs_after = f.coef_min_after;
-      r->diagnostics->coefficient_max_abs_after = f.coef_max_after;
+      r->diagnostics->scaling_applied = f.info.scaling_applied;
+      r->diagnostics->coefficient_min_abs_before = f.info.coef_min_before;
+      r->diagnostics->coefficient_max_abs_before = f.info.coef_max_before;
+      r->diagnostics->coefficient_min_abs_after = f.info.coef_min_after;
+      r->diagnostics->coefficient_max_abs_after = f.info.coef_max_after;
       r->diagnostics->refactorizations = o.iterations + 1;
       r->diagnostics->stall_iteration = -1;
     }

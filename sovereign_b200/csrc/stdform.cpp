@@ -11,32 +11,77 @@
 namespace sov {
 namespace {
 
-void coefficient_range(const std::vector<double>& v, double& lo, double& hi) {
-  // interior_point.cpp:46-56
-  lo = std::numeric_limits<double>::infinity();
+void coefficient_range(const double* v, int count, double& lo, double& hi) {
+  // interior_point.cpp:46-56 (zeros and non-finite magnitudes are skipped)
+  constexpr double kInf = std::numeric_limits<double>::infinity();
+  lo = kInf;
   hi = 0.0;
-  for (double x : v) {
-    const double a = std::abs(x);
-    if (a == 0.0 || !std::isfinite(a)) continue;
-    lo = std::min(lo, a);
-    hi = std::max(hi, a);
+  for (int q = 0; q < count; ++q) {
+    const double a = std::abs(v[q]);
+    const bool use = a > 0.0 && a < kInf;
+    lo = std::min(lo, use ? a : kInf);
+    hi = std::max(hi, use ? a : 0.0);
   }
-  if (!std::isfinite(lo)) lo = 0.0;
+  if (!(lo < kInf)) lo = 0.0;
+}
+
+// CSR (row_ptr, col_idx, rval) of an m x n CSC matrix; within a row, columns ascending.
+void csr_from_csc(int m, int n, const int* col_ptr, const int* row_idx, const double* val, int* row_ptr,
+                  int* col_idx, double* rval, std::vector<int>& fill) {
+  std::fill(row_ptr, row_ptr + m + 1, 0);
+  for (int p = 0; p < col_ptr[n]; ++p) row_ptr[row_idx[p] + 1]++;
+  for (int i = 0; i < m; ++i) row_ptr[i + 1] += row_ptr[i];
+  fill.assign(row_ptr, row_ptr + m);
+  for (int j = 0; j < n; ++j)
+    for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p) {
+      const int q = fill[row_idx[p]]++;
+      col_idx[q] = j;
+      rval[q] = val[p];
+    }
+}
+
+// Two passes of row then column scaling by 1/sqrt(max|a|) (interior_point.cpp:370-405), in place.
+// Scale factors repeat (many rows / columns share their largest magnitude), so the last value's
+// factor is reused: the same arithmetic with fewer square roots and divisions.
+void scale_two_pass(int m, int n, const int* col_ptr, const int* row_idx, double* val, double* b, double* c,
+                    double* row_scale, double* col_scale, std::vector<double>& rs) {
+  double last_in = 1.0, last_out = 1.0;
+  auto inv_sqrt = [&](double v) {
+    if (v != last_in) {
+      last_in = v;
+      last_out = 1.0 / std::sqrt(v);
+    }
+    return last_out;
+  };
+  const int nnz = col_ptr[n];
+  rs.resize(m);
+  for (int pass = 0; pass < 2; ++pass) {
+    std::fill(rs.begin(), rs.end(), 0.0);
+    for (int q = 0; q < nnz; ++q) rs[row_idx[q]] = std::max(rs[row_idx[q]], std::abs(val[q]));
+    for (int i = 0; i < m; ++i) {
+      rs[i] = rs[i] > 0.0 ? inv_sqrt(rs[i]) : 1.0;
+      row_scale[i] *= rs[i];
+      b[i] *= rs[i];
+    }
+    for (int q = 0; q < nnz; ++q) val[q] *= rs[row_idx[q]];
+    for (int j = 0; j < n; ++j) {
+      double mx = 0.0;
+      for (int q = col_ptr[j]; q < col_ptr[j + 1]; ++q) mx = std::max(mx, std::abs(val[q]));
+      const double sc = mx > 0.0 ? inv_sqrt(mx) : 1.0;
+      for (int q = col_ptr[j]; q < col_ptr[j + 1]; ++q) val[q] *= sc;
+      c[j] *= sc;
+      col_scale[j] *= sc;
+    }
+  }
 }
 
 void build_csr(StdForm& f) {
-  f.row_ptr.assign(f.m + 1, 0);
-  for (int p = 0; p < f.nnz(); ++p) f.row_ptr[f.row_idx[p] + 1]++;
-  for (int i = 0; i < f.m; ++i) f.row_ptr[i + 1] += f.row_ptr[i];
+  f.row_ptr.resize(f.m + 1);
   f.col_idx.resize(f.nnz());
   f.rval.resize(f.nnz());
-  std::vector<int> fill(f.row_ptr.begin(), f.row_ptr.end() - 1);
-  for (int j = 0; j < f.n; ++j)
-    for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p) {
-      const int q = fill[f.row_idx[p]]++;
-      f.col_idx[q] = j;
-      f.rval[q] = f.val[p];
-    }
+  std::vector<int> fill;
+  csr_from_csc(f.m, f.n, f.col_ptr.data(), f.row_idx.data(), f.val.data(), f.row_ptr.data(), f.col_idx.data(),
+               f.rval.data(), fill);
 }
 
 }  // namespace
@@ -85,10 +130,29 @@ StdForm build_std_form(const sov_model& p, bool qp, bool enable_scaling) {
   f.val.reserve(f.row_idx.capacity());
   std::vector<std::pair<int, double>> col;
   for (int j = 0; j < ns; ++j) {
+    // fast path: no upper-bound row, rows strictly increasing, no zero or NaN -> copied as is
+    if (ub_row[j] < 0) {
+      bool plain = true;
+      for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k)
+        if (!(std::abs(p.values[k]) > 0.0) || (k > p.col_ptr[j] && p.row_idx[k] <= p.row_idx[k - 1])) {
+          plain = false;
+          break;
+        }
+      if (plain) {
+        for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) {
+          if (p.row_idx[k] < m0) f.b[p.row_idx[k]] -= p.values[k] * f.shift[j];
+          f.row_idx.push_back(p.row_idx[k]);
+          f.val.push_back(p.values[k]);
+        }
+        f.col_ptr[j + 1] = static_cast<int>(f.row_idx.size());
+        continue;
+      }
+    }
     col.clear();
     for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) col.push_back({p.row_idx[k], p.values[k]});
     if (ub_row[j] >= 0) col.push_back({ub_row[j], 1.0});
-    std::sort(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    if (!std::is_sorted(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; }))
+      std::sort(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
     // merge duplicates (a Constraint's name-keyed map sums them), then drop exact zeros
     std::size_t w = 0;
     for (std::size_t q = 0; q < col.size(); ++q) {
@@ -165,33 +229,91 @@ StdForm build_std_form(const sov_model& p, bool qp, bool enable_scaling) {
     f.objective_offset = cs - 0.5 * sqs + sign * p.obj_constant;
   }
 
-  coefficient_range(f.val, f.coef_min_before, f.coef_max_before);
+  coefficient_range(f.val.data(), f.nnz(), f.coef_min_before, f.coef_max_before);
   f.scaling_applied = enable_scaling && m > 0 && n > 0;
   if (f.scaling_applied) {
-    // two passes: rows by 1/sqrt(max|a|), then columns (interior_point.cpp:370-405)
-    std::vector<double> rs(m);
-    for (int pass = 0; pass < 2; ++pass) {
-      std::fill(rs.begin(), rs.end(), 0.0);
-      for (int q = 0; q < f.nnz(); ++q) rs[f.row_idx[q]] = std::max(rs[f.row_idx[q]], std::abs(f.val[q]));
-      for (int i = 0; i < m; ++i) {
-        rs[i] = rs[i] > 0.0 ? 1.0 / std::sqrt(rs[i]) : 1.0;
-        f.row_scale[i] *= rs[i];
-        f.b[i] *= rs[i];
-      }
-      for (int q = 0; q < f.nnz(); ++q) f.val[q] *= rs[f.row_idx[q]];
-      for (int j = 0; j < n; ++j) {
-        double mx = 0.0;
-        for (int q = f.col_ptr[j]; q < f.col_ptr[j + 1]; ++q) mx = std::max(mx, std::abs(f.val[q]));
-        const double s = mx > 0.0 ? 1.0 / std::sqrt(mx) : 1.0;
-        for (int q = f.col_ptr[j]; q < f.col_ptr[j + 1]; ++q) f.val[q] *= s;
-        f.c[j] *= s;
-        f.col_scale[j] *= s;
-      }
-    }
+    std::vector<double> rs;
+    scale_two_pass(m, n, f.col_ptr.data(), f.row_idx.data(), f.val.data(), f.b.data(), f.c.data(),
+                   f.row_scale.data(), f.col_scale.data(), rs);
   }
-  coefficient_range(f.val, f.coef_min_after, f.coef_max_after);
+  coefficient_range(f.val.data(), f.nnz(), f.coef_min_after, f.coef_max_after);
   build_csr(f);
   return f;
+}
+
+bool plain_lp_shape(const sov_model& p, LpShape* s) {
+  const int ns = p.n, m0 = p.m;
+  int n_ub = 0;
+  for (int j = 0; j < ns; ++j) {
+    const double ub = p.ub ? p.ub[j] : 1e30;
+    if (std::isfinite(ub) && ub < 1e29) ++n_ub;
+    for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k)
+      if (!(std::abs(p.values[k]) > 0.0) || (k > p.col_ptr[j] && p.row_idx[k] <= p.row_idx[k - 1])) return false;
+  }
+  int n_slack = n_ub;
+  for (int r = 0; r < m0; ++r) n_slack += p.sense[r] != SOV_EQ ? 1 : 0;
+  s->n_struct = ns;
+  s->m0 = m0;
+  s->n_ub = n_ub;
+  s->m = m0 + n_ub;
+  s->n = ns + n_slack;
+  s->nnz = (p.col_ptr[ns] - p.col_ptr[0]) + n_ub + n_slack;
+  return true;
+}
+
+void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scaling, const LpFormOut& o,
+                         LpFormInfo* info) {
+  thread_local std::vector<double> rs;
+  thread_local std::vector<int> fill;
+  const int ns = s.n_struct, m0 = s.m0, m = s.m, n = s.n;
+  for (int i = 0; i < m0; ++i) o.b[i] = p.rhs[i];
+  // structural columns: shift by lb, the column's entries, then its upper-bound row
+  // (interior_point.cpp:238-247, :289-293)
+  int q = 0, k_ub = 0;
+  o.col_ptr[0] = 0;
+  for (int j = 0; j < ns; ++j) {
+    const double lb = p.lb ? p.lb[j] : 0.0;
+    const double ub = p.ub ? p.ub[j] : 1e30;
+    o.shift[j] = lb;
+    for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) {
+      const int r = p.row_idx[k];
+      o.b[r] -= p.values[k] * lb;
+      o.row_idx[q] = r;
+      o.val[q] = p.values[k];
+      ++q;
+    }
+    if (std::isfinite(ub) && ub < 1e29) {
+      const double u = ub - lb;
+      if (u < -1e-12) throw std::runtime_error("Inconsistent bounds for variable x" + std::to_string(j));
+      const int r = m0 + k_ub++;
+      o.b[r] = u;
+      o.row_idx[q] = r;
+      o.val[q] = 1.0;
+      ++q;
+    }
+    o.col_ptr[j + 1] = q;
+  }
+  // slack (+1) / surplus (-1) columns (:339-350)
+  int col = ns;
+  for (int r = 0; r < m; ++r) {
+    const int kind = r < m0 ? p.sense[r] : SOV_LE;
+    if (kind == SOV_EQ) continue;
+    o.row_idx[q] = r;
+    o.val[q] = kind == SOV_LE ? 1.0 : -1.0;
+    ++q;
+    o.col_ptr[++col] = q;
+  }
+  const double sign = p.maximize ? -1.0 : 1.0;
+  for (int j = 0; j < n; ++j) {
+    o.c[j] = j < ns ? sign * (p.obj ? p.obj[j] : 0.0) : 0.0;
+    o.col_scale[j] = 1.0;
+  }
+  for (int i = 0; i < m; ++i) o.row_scale[i] = 1.0;
+  coefficient_range(o.val, q, info->coef_min_before, info->coef_max_before);
+  info->scaling_applied = enable_scaling && m > 0 && n > 0;
+  if (info->scaling_applied) scale_two_pass(m, n, o.col_ptr, o.row_idx, o.val, o.b, o.c, o.row_scale, o.col_scale, rs);
+  coefficient_range(o.val, q, info->coef_min_after, info->coef_max_after);
+  csr_from_csc(m, n, o.col_ptr, o.row_idx, o.val, o.row_ptr, o.col_idx, o.rval, fill);
 }
 
 namespace {

@@ -44,6 +44,34 @@ struct StdForm {
 // Throws std::runtime_error with the reference's message for inconsistent bounds.
 StdForm build_std_form(const sov_model& model, bool qp, bool enable_scaling);
 
+// LP standard form written straight into caller-provided arrays, for LPs whose structural columns
+// are "plain" (rows strictly increasing, no zero or NaN values: nothing to sort, merge or drop).
+// The arrays receive bit for bit what build_std_form(model, false, scaling) would hold.
+struct LpShape {
+  int n_struct, m0, m, n, nnz, n_ub;
+};
+// false when some column is not plain (the caller then uses build_std_form)
+bool plain_lp_shape(const sov_model& model, LpShape* shape);
+struct LpFormOut {
+  int* col_ptr;       // n + 1
+  int* row_idx;       // nnz
+  double* val;        // nnz
+  int* row_ptr;       // m + 1
+  int* col_idx;       // nnz
+  double* rval;       // nnz
+  double* b;          // m
+  double* c;          // n
+  double* shift;      // n_struct
+  double* col_scale;  // n
+  double* row_scale;  // m
+};
+struct LpFormInfo {
+  bool scaling_applied;
+  double coef_min_before, coef_max_before, coef_min_after, coef_max_after;
+};
+void build_plain_lp_into(const sov_model& model, const LpShape& shape, bool enable_scaling, const LpFormOut& out,
+                         LpFormInfo* info);
+
 // Lower-triangle pattern of M = A diag(d) A' as a gather map: target entry t (position in the
 // caller's matrix layout, from `index(row, col)`) receives sum over its contributions
 // w * d[col_of_w]. Built once per solve; each IPM iteration is then one pass over this map
