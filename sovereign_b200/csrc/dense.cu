@@ -97,11 +97,11 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 // ---------------------------------------------------------------------------------------------
 constexpr int kPanel = 8;
 
+// Runs on a CTA of 256 threads; `potrf_raw` is at least 2 * 64 * 65 elements of dynamic shared memory.
 template <class T>
-__global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
-                                                    int m, T* __restrict__ Linv, int* drop_count, int* fail,
-                                                    double drop_tol) {
-  extern __shared__ __align__(16) unsigned char potrf_raw[];
+__device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag, int m,
+                            T* __restrict__ Linv, int* drop_count, int* fail, double drop_tol,
+                            unsigned char* potrf_raw) {
   T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
   T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
   __shared__ T rinv[kNB];
@@ -227,6 +227,14 @@ __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, i
   }
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
+                                                    int m, T* __restrict__ Linv, int* drop_count, int* fail,
+                                                    double drop_tol) {
+  extern __shared__ __align__(16) unsigned char potrf_raw[];
+  potrf_block<T>(M, ld, kb, diag, m, Linv, drop_count, fail, drop_tol, potrf_raw);
+}
+
 // C (64x64 at rows r0, cols c0 of M) = beta * C + sign * X Y^T, X/Y given as [k][64] slices.
 template <class T>
 __device__ __forceinline__ void tile_nt(const T (*Xs)[kNB], const T (*Ys)[kNB], T (&acc)[4][4]) {
@@ -271,8 +279,13 @@ __global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ M, int ld, i
 }
 
 // Trailing update: A_ij -= L_ik L_jk^T for kb < j <= i (tile index enumerates the lower triangle).
+// Look-ahead: tile 0 is the next diagonal block (kb+1, kb+1); the CTA that updates it goes on to
+// factor and invert it (potrf_block), so the next panel's diagonal factor overlaps the rest of this
+// update instead of running alone on one SM afterwards.
 template <class T>
-__global__ void __launch_bounds__(256) k_syrk_update(T* __restrict__ M, int ld, int kb, int nb) {
+__global__ void __launch_bounds__(256) k_syrk_update(T* __restrict__ M, int ld, int kb, int nb, const double* __restrict__ diag,
+                                                     int m, T* __restrict__ Linv, int* drop_count, int* fail,
+                                                     double drop_tol) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T(*Xs)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw);
   T(*Ys)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw + sizeof(T) * kNB * kNB);
@@ -301,6 +314,10 @@ __global__ void __launch_bounds__(256) k_syrk_update(T* __restrict__ M, int ld, 
       T* dst = M + static_cast<int64_t>(c0 + tx * 4 + q) * ld + r0 + ty * 4 + p;
       *dst -= acc[p][q];
     }
+  if (t == 0) {
+    __syncthreads();
+    potrf_block<T>(M, ld, kb + 1, diag, m, Linv, drop_count, fail, drop_tol, smem_raw);
+  }
 }
 
 template <class T>
@@ -322,19 +339,19 @@ void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
   if (!attr_set) {
     SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
     SOV_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SOV_CUDA(cudaFuncSetAttribute(k_syrk_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_syrk_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
     attr_set = true;
   }
-  int n = 0;
-  for (int kb = 0; kb < s.nb; ++kb) {
-    k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
-    ++n;
+  // panel 0's diagonal block alone; every later one is factored by its look-ahead CTA inside the
+  // previous panel's trailing update
+  k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, 0, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
+  int n = 1;
+  for (int kb = 0; kb + 1 < s.nb; ++kb) {
     const int R = s.nb - kb - 1;
-    if (R > 0) {
-      k_trsm_panel<T><<<R, 256, smem, st>>>(s.M, s.mp, kb, s.Linv);
-      k_syrk_update<T><<<R * (R + 1) / 2, 256, smem, st>>>(s.M, s.mp, kb, s.nb);
-      n += 2;
-    }
+    k_trsm_panel<T><<<R, 256, smem, st>>>(s.M, s.mp, kb, s.Linv);
+    k_syrk_update<T><<<R * (R + 1) / 2, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.nb, s.diag, s.m, s.Linv,
+                                                                s.drop_count, s.fail, s.drop_tol);
+    n += 2;
   }
   SOV_LAUNCH_CHECK();
   if (launches) *launches += n;
