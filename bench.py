@@ -304,11 +304,14 @@ def main():
         # (after one untimed solve) so that it runs in a clean process state
         sample = models[:48]
         InteriorPointSolver().solve(sample[0])
-        t0 = time.perf_counter()
-        single = [InteriorPointSolver().solve(m) for m in sample]
-        t_plain = time.perf_counter() - t0
+        t_plain = float("inf")
+        for _ in range(2):  # the faster of two passes (single solves are sensitive to host load)
+            t0 = time.perf_counter()
+            single = [InteriorPointSolver().solve(m) for m in sample]
+            t_plain = min(t_plain, time.perf_counter() - t0)
         plain = dict(value=len(sample) / t_plain, unit=UNIT,
-                     sample=f"first {len(sample)} LPs one at a time through sov_lp_solve (FP64), wall clock")
+                     sample=f"first {len(sample)} LPs one at a time through sov_lp_solve (FP64), wall clock, "
+                            "faster of two passes")
     # untimed: threads per CTA for each size bucket, picked by timing the bucket alone
     tuning = json.loads(autotune(models))
     batch = DeviceBatch(models)

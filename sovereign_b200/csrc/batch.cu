@@ -908,15 +908,15 @@ struct Batch {
   sov_options opt{};
   struct Bucket {
     int mmax, threads, grid, count;
-    DBuf<int> order;
-    DBuf<int> next;
+    const int* order;  // device: this bucket's LP indices, largest first (inside `in`)
+    int* next;         // device: its work counter (inside `nexts`)
   };
   std::vector<std::unique_ptr<Bucket>> buckets;
-  // one device arena for all packed inputs: [meta | ints | doubles]
+  // one device arena for all packed inputs: [meta | ints | doubles | bucket orders]
   DBuf<unsigned char> in;
   DBuf<double> work;  // 9 n-vectors + 2 m-vectors
   DBuf<LpOut> out;
-  DBuf<int> orders;
+  DBuf<int> nexts;
   long long total_n = 0, total_m = 0, total_nnz = 0, total_cols = 0, total_rows = 0;
   BatchDev dev{};
   int launches = 0;
@@ -1003,7 +1003,12 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   B->meta.resize(count);
   B->pub.resize(count);
   long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0, pubn = 0;
+  struct Run {
+    long long nnz, cols, rows, mv, nv;
+  };
+  std::vector<Run> run(count + 1);  // running totals before LP i (chunk boundaries of the staging)
   for (int i = 0; i < count; ++i) {
+    run[i] = Run{nnz, cols, rows, mv, nv};
     const LpShape& sh = shape[i];
     LpMeta& mt = B->meta[i];
     std::memset(&mt, 0, sizeof(mt));
@@ -1042,13 +1047,38 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     B->bytes += 6.0 * (12.0 * sh.nnz + 8.0 * (sh.m + sh.n)) + 15.0 * 8.0 * sh.n + 10.0 * 8.0 * sh.m;
     B->flops += (2.0 / 3.0) * std::pow(static_cast<double>(sh.m), 3.0);
   }
+  run[count] = Run{nnz, cols, rows, mv, nv};
   B->total_n = nv;
   B->total_m = mv;
   B->total_nnz = nnz;
   B->total_cols = cols;
   B->total_rows = rows;
   B->pubdata.alloc(static_cast<size_t>(std::max(1LL, pubn)));
-  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c
+  // buckets by m, each ordered largest-first (cost ~ m^3 + nnz); their orders travel with the inputs
+  std::map<int, std::vector<int>> groups;
+  for (int i = 0; i < count; ++i)
+    if (B->meta[i].m > 0) groups[bucket_of(B->meta[i].m)].push_back(i);
+  std::vector<double> cost(count, 0.0);
+  for (int i = 0; i < count; ++i) {
+    const double mm = B->meta[i].m;
+    cost[i] = mm * mm * mm + 20.0 * B->meta[i].nnz;
+  }
+  std::vector<int> all_orders;
+  all_orders.reserve(count);
+  std::vector<size_t> order_at;
+  for (auto it = groups.rbegin(); it != groups.rend(); ++it) {
+    auto& ids = it->second;
+    std::sort(ids.begin(), ids.end(), [&](int a1, int a2) { return cost[a1] > cost[a2]; });
+    auto bk = std::make_unique<Batch::Bucket>();
+    bk->mmax = it->first;
+    bk->threads = threads_for(bk->mmax);
+    bk->count = static_cast<int>(ids.size());
+    bk->grid = grid_for(bk->mmax, bk->threads, bk->count);
+    order_at.push_back(all_orders.size());
+    all_orders.insert(all_orders.end(), ids.begin(), ids.end());
+    B->buckets.push_back(std::move(bk));
+  }
+  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c | orders
   const size_t o_meta = 0;
   const size_t o_cp = align8(o_meta + sizeof(LpMeta) * count);
   const size_t o_ri = o_cp + sizeof(int) * cols;
@@ -1058,79 +1088,96 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   const size_t o_rv = o_cv + sizeof(double) * nnz;
   const size_t o_b = o_rv + sizeof(double) * nnz;
   const size_t o_c = o_b + sizeof(double) * mv;
-  const size_t total = o_c + sizeof(double) * nv;
+  const size_t o_ord = o_c + sizeof(double) * nv;
+  const size_t total = o_ord + sizeof(int) * all_orders.size();
   B->h2d_bytes = static_cast<double>(total);
-  // 3. every LP's standard form written into its slots of the pinned staging, in parallel
+  B->in.alloc(total);
+  B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
+  B->out.alloc(count);
+  B->nexts.alloc(std::max<size_t>(1, B->buckets.size()));
+  // 3. every LP's standard form written into its slots of the pinned staging, chunk by chunk in
+  //    LP order; each finished chunk's slots are copied to the device (async) while the next
+  //    chunk is built
   std::lock_guard<std::mutex> lock(g_arena.mu);
   unsigned char* h = g_arena.get(total);
   double* pubd = B->pubdata.p;
-  parallel_for(count, [&](int i) {
-    LpMeta& mt = B->meta[i];
-    if (mt.m < 0) return;
-    Batch::Pub& pb = B->pub[i];
-    int* cp = reinterpret_cast<int*>(h + o_cp) + mt.cp_off;
-    int* ri = reinterpret_cast<int*>(h + o_ri) + mt.a_off;
-    int* rp = reinterpret_cast<int*>(h + o_rp) + mt.rp_off;
-    int* ci = reinterpret_cast<int*>(h + o_ci) + mt.a_off;
-    double* cv = reinterpret_cast<double*>(h + o_cv) + mt.a_off;
-    double* rv = reinterpret_cast<double*>(h + o_rv) + mt.a_off;
-    double* bb = reinterpret_cast<double*>(h + o_b) + mt.mv_off;
-    double* cc = reinterpret_cast<double*>(h + o_c) + mt.nv_off;
-    if (kind[i] == kInPlace) {
-      const LpFormOut out{cp, ri, cv, rp, ci, rv, bb, cc, pubd + pb.shift_off, pubd + pb.cs_off, pubd + pb.rs_off};
-      try {
-        build_plain_lp_into(models[i], shape[i], scaling, out, &pb.info);
-      } catch (const std::exception& e) {
-        throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
-      }
-    } else {
-      const StdForm& f = B->forms[i];
-      std::memcpy(cp, f.col_ptr.data(), sizeof(int) * (f.n + 1));
-      std::memcpy(ri, f.row_idx.data(), sizeof(int) * f.nnz());
-      std::memcpy(rp, f.row_ptr.data(), sizeof(int) * (f.m + 1));
-      std::memcpy(ci, f.col_idx.data(), sizeof(int) * f.nnz());
-      std::memcpy(cv, f.val.data(), sizeof(double) * f.nnz());
-      std::memcpy(rv, f.rval.data(), sizeof(double) * f.nnz());
-      std::memcpy(bb, f.b.data(), sizeof(double) * f.m);
-      std::memcpy(cc, f.c.data(), sizeof(double) * f.n);
-      std::copy(f.shift.begin(), f.shift.end(), pubd + pb.shift_off);
-      std::copy(f.col_scale.begin(), f.col_scale.end(), pubd + pb.cs_off);
-      std::copy(f.row_scale.begin(), f.row_scale.end(), pubd + pb.rs_off);
-      pb.info = LpFormInfo{f.scaling_applied, f.coef_min_before, f.coef_max_before, f.coef_min_after,
-                           f.coef_max_after};
+  cudaStream_t cs = nullptr;
+  SOV_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  auto copy_range = [&](size_t off, size_t bytes) {
+    if (bytes) SOV_CUDA(cudaMemcpyAsync(B->in.p + off, h + off, bytes, cudaMemcpyHostToDevice, cs));
+  };
+  const int chunks = count >= 512 ? 8 : 1;
+  try {
+    for (int ch = 0; ch < chunks; ++ch) {
+      const int lo = static_cast<int>(static_cast<long long>(count) * ch / chunks);
+      const int hi = static_cast<int>(static_cast<long long>(count) * (ch + 1) / chunks);
+      parallel_for(hi - lo, [&](int t) {
+        const int i = lo + t;
+        LpMeta& mt = B->meta[i];
+        if (mt.m < 0) return;
+        Batch::Pub& pb = B->pub[i];
+        int* cp = reinterpret_cast<int*>(h + o_cp) + mt.cp_off;
+        int* ri = reinterpret_cast<int*>(h + o_ri) + mt.a_off;
+        int* rp = reinterpret_cast<int*>(h + o_rp) + mt.rp_off;
+        int* ci = reinterpret_cast<int*>(h + o_ci) + mt.a_off;
+        double* cv = reinterpret_cast<double*>(h + o_cv) + mt.a_off;
+        double* rv = reinterpret_cast<double*>(h + o_rv) + mt.a_off;
+        double* bb = reinterpret_cast<double*>(h + o_b) + mt.mv_off;
+        double* cc = reinterpret_cast<double*>(h + o_c) + mt.nv_off;
+        if (kind[i] == kInPlace) {
+          const LpFormOut out{cp, ri, cv, rp, ci, rv, bb, cc, pubd + pb.shift_off, pubd + pb.cs_off, pubd + pb.rs_off};
+          try {
+            build_plain_lp_into(models[i], shape[i], scaling, out, &pb.info);
+          } catch (const std::exception& e) {
+            throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
+          }
+        } else {
+          const StdForm& f = B->forms[i];
+          std::memcpy(cp, f.col_ptr.data(), sizeof(int) * (f.n + 1));
+          std::memcpy(ri, f.row_idx.data(), sizeof(int) * f.nnz());
+          std::memcpy(rp, f.row_ptr.data(), sizeof(int) * (f.m + 1));
+          std::memcpy(ci, f.col_idx.data(), sizeof(int) * f.nnz());
+          std::memcpy(cv, f.val.data(), sizeof(double) * f.nnz());
+          std::memcpy(rv, f.rval.data(), sizeof(double) * f.nnz());
+          std::memcpy(bb, f.b.data(), sizeof(double) * f.m);
+          std::memcpy(cc, f.c.data(), sizeof(double) * f.n);
+          std::copy(f.shift.begin(), f.shift.end(), pubd + pb.shift_off);
+          std::copy(f.col_scale.begin(), f.col_scale.end(), pubd + pb.cs_off);
+          std::copy(f.row_scale.begin(), f.row_scale.end(), pubd + pb.rs_off);
+          pb.info = LpFormInfo{f.scaling_applied, f.coef_min_before, f.coef_max_before, f.coef_min_after,
+                               f.coef_max_after};
+        }
+        double bmax = 0.0, cmax = 0.0;
+        for (int k = 0; k < mt.m; ++k) bmax = std::max(bmax, std::abs(bb[k]));
+        for (int k = 0; k < mt.n; ++k) cmax = std::max(cmax, std::abs(cc[k]));
+        mt.bnorm = std::max(1.0, bmax);
+        mt.cnorm = std::max(1.0, cmax);
+      });
+      const Run& r0 = run[lo];
+      const Run& r1 = run[hi];
+      copy_range(o_cp + sizeof(int) * r0.cols, sizeof(int) * (r1.cols - r0.cols));
+      copy_range(o_ri + sizeof(int) * r0.nnz, sizeof(int) * (r1.nnz - r0.nnz));
+      copy_range(o_rp + sizeof(int) * r0.rows, sizeof(int) * (r1.rows - r0.rows));
+      copy_range(o_ci + sizeof(int) * r0.nnz, sizeof(int) * (r1.nnz - r0.nnz));
+      copy_range(o_cv + sizeof(double) * r0.nnz, sizeof(double) * (r1.nnz - r0.nnz));
+      copy_range(o_rv + sizeof(double) * r0.nnz, sizeof(double) * (r1.nnz - r0.nnz));
+      copy_range(o_b + sizeof(double) * r0.mv, sizeof(double) * (r1.mv - r0.mv));
+      copy_range(o_c + sizeof(double) * r0.nv, sizeof(double) * (r1.nv - r0.nv));
     }
-    double bmax = 0.0, cmax = 0.0;
-    for (int k = 0; k < mt.m; ++k) bmax = std::max(bmax, std::abs(bb[k]));
-    for (int k = 0; k < mt.n; ++k) cmax = std::max(cmax, std::abs(cc[k]));
-    mt.bnorm = std::max(1.0, bmax);
-    mt.cnorm = std::max(1.0, cmax);
-  });
-  std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
-  B->in.alloc(total);
-  SOV_CUDA(cudaMemcpy(B->in.p, h, total, cudaMemcpyHostToDevice));
-  B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
-  B->out.alloc(count);
-  // buckets by m, each ordered largest-first (cost ~ m^3 + nnz)
-  std::map<int, std::vector<int>> groups;
-  for (int i = 0; i < count; ++i)
-    if (B->meta[i].m > 0) groups[bucket_of(B->meta[i].m)].push_back(i);
-  std::vector<int> all_orders;
-  for (auto it = groups.rbegin(); it != groups.rend(); ++it) {
-    auto& ids = it->second;
-    std::sort(ids.begin(), ids.end(), [&](int a, int b2) {
-      const double ca = std::pow(B->meta[a].m, 3.0) + 20.0 * B->meta[a].nnz;
-      const double cb = std::pow(B->meta[b2].m, 3.0) + 20.0 * B->meta[b2].nnz;
-      return ca > cb;
-    });
-    auto bk = std::make_unique<Batch::Bucket>();
-    bk->mmax = it->first;
-    bk->threads = threads_for(bk->mmax);
-    bk->count = static_cast<int>(ids.size());
-    bk->grid = grid_for(bk->mmax, bk->threads, bk->count);
-    bk->order.alloc(ids.size());
-    SOV_CUDA(cudaMemcpy(bk->order.p, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
-    bk->next.alloc(1);
-    B->buckets.push_back(std::move(bk));
+    std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
+    if (!all_orders.empty()) std::memcpy(h + o_ord, all_orders.data(), sizeof(int) * all_orders.size());
+    copy_range(o_meta, sizeof(LpMeta) * count);
+    copy_range(o_ord, sizeof(int) * all_orders.size());
+    SOV_CUDA(cudaStreamSynchronize(cs));
+  } catch (...) {
+    cudaStreamSynchronize(cs);  // the staging is reused by the next batch: no copy may still read it
+    cudaStreamDestroy(cs);
+    throw;
+  }
+  SOV_CUDA(cudaStreamDestroy(cs));
+  for (size_t k = 0; k < B->buckets.size(); ++k) {
+    B->buckets[k]->order = reinterpret_cast<const int*>(B->in.p + o_ord) + order_at[k];
+    B->buckets[k]->next = B->nexts.p + k;
   }
   BatchDev& d = B->dev;
   unsigned char* base = B->in.p;
@@ -1183,11 +1230,11 @@ void batch_solve(Batch* B, cudaStream_t st) {
       auto& bk = B->buckets[b];
       cudaStream_t s2 = B->streams[b];
       SOV_CUDA(cudaStreamWaitEvent(s2, B->fork, 0));
-      SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), s2));
+      SOV_CUDA(cudaMemsetAsync(bk->next, 0, sizeof(int), s2));
       BatchDev d = B->dev;
-      d.order = bk->order.p;
+      d.order = bk->order;
       d.count = bk->count;
-      d.next = bk->next.p;
+      d.next = bk->next;
       launch_any(d, bk->mmax, bk->threads, bk->grid, s2);
       SOV_CUDA(cudaEventRecord(B->joins[b], s2));
       SOV_CUDA(cudaStreamWaitEvent(B->cap, B->joins[b], 0));
@@ -1366,15 +1413,15 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
     for (int threads : {128, 256, 512}) {
       const int grid = grid_for(bk->mmax, threads, bk->count);
       BatchDev d = B->dev;
-      d.order = bk->order.p;
+      d.order = bk->order;
       d.count = bk->count;
-      d.next = bk->next.p;
+      d.next = bk->next;
       float ms_min = 1e30f;
       for (int rep_i = 0; rep_i < 2; ++rep_i) {
         cudaEvent_t e0, e1;
         SOV_CUDA(cudaEventCreate(&e0));
         SOV_CUDA(cudaEventCreate(&e1));
-        SOV_CUDA(cudaMemsetAsync(bk->next.p, 0, sizeof(int), st));
+        SOV_CUDA(cudaMemsetAsync(bk->next, 0, sizeof(int), st));
         SOV_CUDA(cudaEventRecord(e0, st));
         launch_any(d, bk->mmax, threads, grid, st);
         SOV_CUDA(cudaEventRecord(e1, st));
