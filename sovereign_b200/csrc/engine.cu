@@ -202,6 +202,11 @@ class Engine {
   DevBuf<PcgScalars> pcg_s_;
   PcgScalars* pcg_h_ = nullptr;
   int pcg_iterations_ = 0, fp64_fallbacks_ = 0, factorizations_ = 0;
+  // mixed precision stops paying once the FP32 factor needs many PCG steps per solve (the normal
+  // matrix only gets worse conditioned as the iterates approach the boundary): from the next
+  // factorization on, the engine factors in FP64
+  static constexpr int kPcgSwitch = 12;
+  bool to_fp64_ = false;
   // x-space QP
   XSpace xs_;
   bool xspace_ = false;
@@ -376,6 +381,7 @@ void Engine::assemble_and_factor(int mode) {
   const double reg = 1e-12;  // kNormalEqRegularization (interior_point.cpp:103)
   ++factorizations_;
   fp64_ready_ = false;
+  if (to_fp64_ && backend_ == kDenseMixed) backend_ = kDense64;
   // x-space: K = A_x' Theta A_x (+ diag Q + H after assembly); start system: Theta = 1, diag 1
   const int amode = xspace_ ? (mode == kWeightOnes ? kWeightOnes : kWeightTheta) : mode;
   if (backend_ == kBand) {
@@ -430,6 +436,7 @@ bool Engine::newton_solve() {
   launches_ += 2;
   bool converged = false;
   const int cap = opt_.pcg_max_iterations > 0 ? opt_.pcg_max_iterations : 50;
+  const int used_before = pcg_iterations_;
   for (int k = 0; k < cap; ++k) {
     launch_normal_matvec(dev_, pcg_p_.p, pcg_tmp_.p, pcg_q_.p, reg, st_);
     k_pcg_step<<<1, 1024, 0, st_>>>(m, pcg_p_.p, pcg_q_.p, pcg_x_.p, pcg_r_.p, pcg_w_.p, pcg_s_.p);
@@ -445,6 +452,7 @@ bool Engine::newton_solve() {
     k_pcg_direction<<<1, 1024, 0, st_>>>(m, pcg_r_.p, pcg_w_.p, pcg_p_.p, pcg_s_.p, 0);
     launches_ += 1;
   }
+  if (!converged || pcg_iterations_ - used_before > kPcgSwitch) to_fp64_ = true;
   if (converged) {
     SOV_CUDA(cudaMemcpyAsync(z_.p, pcg_x_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st_));
     return true;
