@@ -228,6 +228,9 @@ def run_single_workload(args):
               status=r.status_name, iterations=r.iterations, objective=r.objective_value, device_s=dev,
               duality_gap=r.duality_gap, message=r.message[:160])
         return
+    if args.workload == "c3w":
+        run_batched_warm_start(args)
+        return
     # c4: learned warm start on the multicommodity family
     from sovereign_b200.warmstart import WarmStart, solve_many
     fam = P.MulticommodityFamily()
@@ -236,28 +239,93 @@ def run_single_workload(args):
     opts = InteriorPointOptions()
     t0 = time.perf_counter()
     # training targets: the iterate at the start of iteration 6 (early central-path stretch)
-    cold_train, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=6))
+    cold_train, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=6), workers=args.workers)
     t_gen = time.perf_counter() - t0
     ws = WarmStart(fam.param_dim, cold_train[0].n_ipm, cold_train[0].m_ipm, hidden=512, layers=3, seed=0)
     t0 = time.perf_counter()
     loss = ws.fit(np.stack([p for _, p in train]), cold_train, epochs=40, batch=128, lr=1e-3)
     t_train = time.perf_counter() - t0
-    cold, t_cold = solve_many([m for m, _ in test], opts)
+    cold, t_cold = solve_many([m for m, _ in test], opts, workers=args.workers)
     t0 = time.perf_counter()
     starts = ws.predict(np.stack([p for _, p in test]))
     t_pred = time.perf_counter() - t0
-    warm, t_warm = solve_many([m for m, _ in test], opts, warm=starts)
+    warm, t_warm = solve_many([m for m, _ in test], opts, warm=starts, workers=args.workers)
     ok = [k for k in range(len(test)) if cold[k].status_name == "OPTIMAL" and warm[k].status_name == "OPTIMAL"]
     err = max(abs(cold[k].objective_value - warm[k].objective_value) / max(1.0, abs(cold[k].objective_value))
               for k in ok) if ok else None
     _line(METRIC, len(test) / (t_warm + t_pred), UNIT, args, 1e3 * (t_warm + t_pred) / len(test), "f64",
           dict(workload=f"multicommodity 200 nodes / 1000 arcs / 4 commodities, {args.eval} eval instances, "
-                        f"MLP 4040-512x3-11800 trained on {args.train} IPM solutions"),
+                        f"MLP 4040-512x3-11800 trained on {args.train} IPM solutions, {args.workers} concurrent solves"),
           cold=dict(lps_per_s=len(test) / t_cold, mean_iterations=float(np.mean([r.iterations for r in cold]))),
           warm=dict(lps_per_s=len(test) / (t_warm + t_pred), mean_iterations=float(np.mean([r.iterations for r in warm])),
                     used=int(sum(r.diagnostics["warm_start_used"] for r in warm))),
           optimal=f"{len(ok)}/{len(test)}", max_rel_obj_diff_warm_vs_cold=err, train_loss=loss,
           seconds=dict(generate=t_gen, train=t_train, predict=t_pred))
+
+
+def run_batched_warm_start(args):
+    """Batched + learned warm start: a parametric 40 x 40 transportation family, `--eval` instances
+    solved in one sov_lp_solve_batch call cold (Mehrotra start in every CTA) and warm (one predicted
+    start per LP, passed as per-LP option blocks), both through the C ABI with caller-owned host
+    buffers, after training the MLP on `--train` instances' early iterates."""
+    import ctypes as C
+
+    from sovereign_b200 import _lib, abi as A, problems as P
+    from sovereign_b200.ipm import InteriorPointOptions
+    from sovereign_b200.model import ResultBuffers
+    from sovereign_b200.warmstart import WarmStart, solve_many
+    lib = _lib.load(build_if_missing=False)
+    fam = P.TransportFamily()
+    train = [fam.instance_from_seed(200000 + k) for k in range(args.train)]
+    count = args.count
+    test = [fam.instance_from_seed(700000 + k) for k in range(count)]
+    t0 = time.perf_counter()
+    early, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=5), workers=args.workers)
+    t_gen = time.perf_counter() - t0
+    ws = WarmStart(fam.param_dim, early[0].n_ipm, early[0].m_ipm, hidden=512, layers=3, seed=0)
+    t0 = time.perf_counter()
+    loss = ws.fit(np.stack([p for _, p in train]), early, epochs=60, batch=128, lr=1e-3)
+    t_train = time.perf_counter() - t0
+    models = [m for m, _ in test]
+    arr = (A.SovModel * count)(*[m.to_abi() for m in models])
+    bufs = [ResultBuffers(m, with_diag=True) for m in models]
+    res = (A.SovResult * count)(*[b.raw for b in bufs])
+    base = A.default_options()
+
+    def run(opts, stride, steps):
+        best = float("inf")
+        for _ in range(steps):
+            t = time.perf_counter()
+            _lib.check(lib.sov_lp_solve_batch(count, arr, opts, stride, res))
+            best = min(best, time.perf_counter() - t)
+        return best, [(r.status, r.iterations, r.objective_value, r.diagnostics.contents.warm_start_used) for r in res]
+
+    run(C.byref(base), 0, 1)  # warm-up
+    t_cold, cold = run(C.byref(base), 0, max(1, args.steps))
+    t0 = time.perf_counter()
+    starts = ws.predict(np.stack([p for _, p in test]))
+    t_pred = time.perf_counter() - t0
+    opts = (A.SovOptions * count)()
+    keep = []
+    for k, (x, y, s_) in enumerate(starts):
+        C.memmove(C.byref(opts[k]), C.byref(base), C.sizeof(A.SovOptions))
+        a = [np.ascontiguousarray(v) for v in (x, y, s_)]
+        keep.append(a)
+        opts[k].warm_x, opts[k].warm_y, opts[k].warm_s = (A.dptr(v) for v in a)
+    t_warm, warm = run(opts, C.sizeof(A.SovOptions), max(1, args.steps))
+    ok = [k for k in range(count) if cold[k][0] == A.OPTIMAL and warm[k][0] == A.OPTIMAL]
+    err = max(abs(cold[k][2] - warm[k][2]) / max(1.0, abs(cold[k][2])) for k in ok) if ok else None
+    value = count / (t_warm + t_pred)
+    _line(METRIC, value, UNIT, args, 1e3 * (t_warm + t_pred), "f64",
+          dict(workload=f"parametric transportation family 40x40 (m=80, n=1600), {count} LPs per batched call, "
+                        f"MLP 1680-512x3-3280 trained on {args.train} early IPM iterates",
+               parallelism="one sov_lp_solve_batch call (C ABI, caller-owned host buffers), best of steps"),
+          cold=dict(lps_per_s=count / t_cold, mean_iterations=float(np.mean([c[1] for c in cold]))),
+          warm=dict(lps_per_s=value, mean_iterations=float(np.mean([w[1] for w in warm])),
+                    used=int(sum(w[3] for w in warm)), predict_s=t_pred),
+          speedup_warm_vs_cold=t_cold / (t_warm + t_pred), optimal=f"{len(ok)}/{count}",
+          max_rel_obj_diff_warm_vs_cold=err, train_loss=loss, seconds=dict(generate=t_gen, train=t_train))
+    del keep
 
 
 def main():
@@ -268,11 +336,13 @@ def main():
     ap.add_argument("--impl", default="sovereign_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=COUNT, help="LPs per step (profiling runs use fewer)")
-    ap.add_argument("--workload", default="batch", choices=["batch", "c0", "c1", "c2", "c4"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "c0", "c1", "c2", "c3w", "c4"],
                     help="batch (default, headline): 4096 uneven transportation LPs; c0: one 50x50 transportation "
                          "LP; c1: random LP m=2000 n=10000 (FP64 and mixed); c2: convex-sequence QP n=20002; "
+                         "c3w: parametric 40x40 transportation family, batched, learned warm start vs cold; "
                          "c4: multicommodity family, learned warm start vs Mehrotra start")
     ap.add_argument("--train", type=int, default=1024, help="c4: training instances")
+    ap.add_argument("--workers", type=int, default=16, help="c4: concurrent single-LP solves (one stream each)")
     ap.add_argument("--eval", type=int, default=128, help="c4: evaluation instances")
     args = ap.parse_args()
     if args.workload != "batch":

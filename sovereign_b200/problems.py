@@ -126,6 +126,43 @@ def convex_sequence_qp(n: int, seed: int, target: np.ndarray | None = None,
     return mdl
 
 
+class TransportFamily:
+    """A fixed ns x nt transportation network whose data vary per instance: supplies x(1 + 0.2 N),
+    demands x(1 + 0.2 N) rebalanced to the total supply, costs x(1 + 0.1 N) around base values
+    drawn like `transport` (costs U[1,100], supplies and demand weights U{10..100}). Instance
+    parameters = the concatenated multiplicative factors (ns + nt + ns*nt). Small enough (m = ns + nt
+    <= 128) for the batched kernel."""
+
+    def __init__(self, ns: int = 40, nt: int = 40, seed: int = 8):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.ns, self.nt = ns, nt
+        self.base_cost = rng.uniform(1.0, 100.0, size=(ns, nt))
+        self.base_supply = rng.integers(10, 101, size=ns).astype(np.float64)
+        self.base_weight = rng.integers(10, 101, size=nt).astype(np.float64)
+
+    @property
+    def param_dim(self) -> int:
+        return self.ns + self.nt + self.ns * self.nt
+
+    def sample_params(self, seed: int) -> np.ndarray:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        return np.concatenate([1.0 + 0.2 * rng.standard_normal(self.ns + self.nt),
+                               1.0 + 0.1 * rng.standard_normal(self.ns * self.nt)])
+
+    def instance(self, params: np.ndarray, name: str = "") -> Model:
+        ns, nt = self.ns, self.nt
+        f = np.maximum(params, 0.05)
+        supply = self.base_supply * f[:ns]
+        weight = self.base_weight * f[ns:ns + nt]
+        demand = weight * supply.sum() / weight.sum()
+        cost = self.base_cost * f[ns + nt:].reshape(ns, nt)
+        return transport_structure(ns, nt, cost, supply, demand, name or f"transport_family_{ns}x{nt}")
+
+    def instance_from_seed(self, seed: int) -> tuple[Model, np.ndarray]:
+        p = self.sample_params(seed)
+        return self.instance(p, f"transport_family_s{seed}"), p
+
+
 class MulticommodityFamily:
     """A fixed network (nodes, arcs, capacities U[5,50], unit costs U[1,20]) with K commodities,
     each shipping from one source node to `sinks` sink nodes. Instance parameters are the
