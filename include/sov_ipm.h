@@ -192,21 +192,25 @@ int sov_ipm_dims(const sov_model* model, int32_t qp, int32_t* n_ipm, int32_t* m_
 /* One LP through the GPU IPM. Synchronous; host pointers are borrowed for the call. */
 int sov_lp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
 
-/* One convex QP through the GPU IPM (diagonal-plus-low-rank Hessians take the normal-equation
- * path; general Hessians the dense quasi-definite KKT path). */
+/* One convex QP through the GPU IPM, normal-equation path: separable (diagonal) Hessians; a model
+ * with off-diagonal Hessian entries returns SOV_ERROR with a message saying so. */
 int sov_qp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
 
 /* count independent LPs in one persistent batched launch (one CTA per LP, the whole IPM loop
- * on the device). opt may be one shared option block (opt_stride 0) or an array. LPs whose
- * normal matrix does not fit the batched kernel are solved one by one through sov_lp_solve. */
+ * on the device). opt is one shared option block (opt_stride 0; NULL = LP defaults) or an array
+ * of blocks opt_stride bytes apart, one per LP: per-LP tolerances, iteration limits, scaling and
+ * warm starts (warm_x / warm_y / warm_s in the engine's standard form, taken under the same
+ * safeguard as sov_lp_solve; diagnostics->warm_start_used reports it). LPs whose normal matrix
+ * does not fit the batched kernel are solved one by one through sov_lp_solve. */
 int sov_lp_solve_batch(int32_t count, const sov_model* models, const sov_options* opt,
                        int32_t opt_stride, sov_result* results);
 
 /* Device-resident batch: prepare once (host standard form + upload), solve many times (device
- * only, stream-ordered), read back. Used to time the solver with inputs already in HBM. */
+ * only, stream-ordered), read back. Used to time the solver with inputs already in HBM. opt and
+ * opt_stride as in sov_lp_solve_batch (one shared block, or one block per LP). */
 typedef struct sov_batch sov_batch;
 int sov_batch_create(int32_t count, const sov_model* models, const sov_options* opt,
-                     sov_batch** out);
+                     int32_t opt_stride, sov_batch** out);
 int sov_batch_solve(sov_batch* batch, void* cuda_stream);
 int sov_batch_results(sov_batch* batch, sov_result* results);
 /* Kernel launches issued by the last sov_batch_solve, and the device time of its kernels. */

@@ -48,7 +48,7 @@ def load(build_if_missing: bool = True):
     lib.sov_lp_solve.argtypes = [M, O, R]
     lib.sov_qp_solve.argtypes = [M, O, R]
     lib.sov_lp_solve_batch.argtypes = [C.c_int32, M, O, C.c_int32, R]
-    lib.sov_batch_create.argtypes = [C.c_int32, M, O, C.POINTER(C.c_void_p)]
+    lib.sov_batch_create.argtypes = [C.c_int32, M, O, C.c_int32, C.POINTER(C.c_void_p)]
     lib.sov_batch_solve.argtypes = [C.c_void_p, C.c_void_p]
     lib.sov_batch_results.argtypes = [C.c_void_p, R]
     lib.sov_batch_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),

@@ -34,6 +34,7 @@
 namespace sov {
 
 constexpr int kBatchMaxRows = 128;
+constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the Mehrotra restart
 
 // offset of row i of a row-packed lower triangle
 __host__ __device__ constexpr int tri(int i) { return i * (i + 1) / 2; }
@@ -42,12 +43,13 @@ struct LpMeta {
   int m, n, nnz, pad1;
   int max_iter, pad0;
   long long a_off, cp_off, rp_off, mv_off, nv_off;
+  long long w_off;  // caller's start [x (n) | y (m) | s (n)] in `warm`, or -1
   double bnorm, cnorm, ftol, otol, tau;
 };
 
 struct LpOut {
   int status, iterations, best_it, use_best;
-  int drops, fail, pad0, pad1;
+  int drops, fail, warm_used, pad1;
   double gap, p_res, d_res, cx;
 };
 
@@ -64,6 +66,7 @@ struct BatchDev {
   const double* rval;
   const double* b;
   const double* c;
+  const double* warm;
   double *x, *s, *dx, *ds, *dxa, *dsa, *rd, *bx, *bs;
   double *y, *by;
   LpOut* out;
@@ -391,41 +394,98 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   // the update of one iteration and the direction pass that overwrites them)
   double* dvec = ds;
   double* tvec = dx;
-  for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
-  __syncthreads();
-  for (int j = tid; j < n; j += NT) offdiag(cp[j], cp[j + 1], 1.0);
-  __syncthreads();
-  row_pass(0, nullptr, nullptr);
-  __syncthreads();
-  factor();
-  solve();
-  const bool start_ok = !fail;
-  for (int j = tid; j < n; j += NT) {
-    double xs = 1.0, ss = 1.0;
-    if (start_ok) {
-      double atdy = 0.0;
-      for (int p = cp[j]; p < cp[j + 1]; ++p) atdy += cv[p] * vz[ri[p]];
-      xs = fmax(1.0, fabs(atdy));
-      ss = fmax(1.0, fabs(c[j] - atdy));
+  auto mehrotra_start = [&]() {
+    for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
+    __syncthreads();
+    for (int j = tid; j < n; j += NT) offdiag(cp[j], cp[j + 1], 1.0);
+    __syncthreads();
+    row_pass(0, nullptr, nullptr);
+    __syncthreads();
+    factor();
+    solve();
+    const bool start_ok = !fail;
+    for (int j = tid; j < n; j += NT) {
+      double xs = 1.0, ss = 1.0;
+      if (start_ok) {
+        double atdy = 0.0;
+        for (int p = cp[j]; p < cp[j + 1]; ++p) atdy += cv[p] * vz[ri[p]];
+        xs = fmax(1.0, fabs(atdy));
+        ss = fmax(1.0, fabs(c[j] - atdy));
+      }
+      x[j] = xs;
+      s[j] = ss;
+      bx[j] = xs;
+      bs[j] = ss;
     }
-    x[j] = xs;
-    s[j] = ss;
-    bx[j] = xs;
-    bs[j] = ss;
+    for (int i = tid; i < m; i += NT) {
+      vy[i] = start_ok ? vz[i] : 0.0;
+      gby[i] = vy[i];
+    }
+    for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
+    fail = 0;
+    __syncthreads();
+  };
+  mehrotra_start();
+
+  const int ops_res[4] = {1, 1, 0, 0};
+  // ---- caller-supplied start (a learned prediction, a neighbouring LP's iterate) ----
+  // Same rule as the single-problem engine: kept when its residual metric is within 10x of the
+  // Mehrotra start's and its complementarity mu is not larger; otherwise the Mehrotra start stays.
+  int warm_used = 0;
+  if (mt.w_off >= 0) {
+    // residual metric max(p_res, d_res, gap) and mu of the point in (x, vy, s)
+    auto point_metric = [&](double& metric, double& mu) {
+      double rpm = 0.0;
+      for (int i = warp; i < m; i += NW) {
+        double acc = 0.0;
+        for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) acc += rv[p] * x[ci[p]];
+        acc = warp_sum(acc);
+        rpm = fmax(rpm, fabs(b[i] - acc));
+      }
+      double rdm = 0.0, xs = 0.0, cx = 0.0;
+      for (int j = tid; j < n; j += NT) {
+        const double r = c[j] - (col_dot(cp[j], cp[j + 1], vy) + s[j]);
+        rdm = fmax(rdm, fabs(r));
+        xs += x[j] * s[j];
+        cx += c[j] * x[j];
+      }
+      double v[4] = {rpm, rdm, xs, cx};
+      cta_reduce4<NT>(v, ops_res, red);
+      if (tid == 0) {
+        cs.v[S_MU] = v[2] / n;
+        cs.v[S_METRIC] = fmax(fmax(v[0] / mt.bnorm, v[1] / mt.cnorm), fabs(v[2]) / (1.0 + fabs(v[3])));
+      }
+      __syncthreads();
+      metric = cs.v[S_METRIC];
+      mu = cs.v[S_MU];
+      __syncthreads();
+    };
+    double met_d, mu_d, met_w, mu_w;
+    point_metric(met_d, mu_d);
+    const double* wx = bd.warm + mt.w_off;
+    for (int j = tid; j < n; j += NT) {
+      x[j] = wx[j];
+      s[j] = wx[n + m + j];
+    }
+    for (int i = tid; i < m; i += NT) vy[i] = wx[n + i];
+    __syncthreads();
+    point_metric(met_w, mu_w);
+    if (isfinite(met_w) && isfinite(mu_w) && met_w <= 10.0 * met_d && mu_w <= mu_d) {
+      warm_used = 1;
+    } else {
+      for (int j = tid; j < n; j += NT) {
+        x[j] = bx[j];
+        s[j] = bs[j];
+      }
+      for (int i = tid; i < m; i += NT) vy[i] = gby[i];
+    }
+    __syncthreads();
   }
-  for (int i = tid; i < m; i += NT) {
-    vy[i] = start_ok ? vz[i] : 0.0;
-    gby[i] = vy[i];
-  }
-  for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
-  fail = 0;
-  __syncthreads();
 
   double best_metric = INFINITY, best_gap = INFINITY, best_p = INFINITY, best_d = INFINITY;
   int best_it = 0;
   int status = -1, iters = 0;
   double last_gap = 0, last_p = 0, last_d = 0, last_cx = 0;
-  const int ops_res[4] = {1, 1, 0, 0};
   for (int it = 0; it < mt.max_iter; ++it) {
     // residuals, with the predictor's right-hand side and the normal matrix built in the same two
     // passes (interior_point.cpp:572-582, :418-432, :74-101)
@@ -500,6 +560,16 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       status = SOV_OPTIMAL;
       iters = it + 1;
       break;
+    }
+    // a supplied start that has not converged after kWarmGiveUp iterations is abandoned once: the
+    // LP restarts from the Mehrotra start (its best-iterate record restarts too), so one poor
+    // prediction costs at most kWarmGiveUp extra iterations instead of running to the limit
+    if (warm_used == 1 && it + 1 == kWarmGiveUp) {
+      mehrotra_start();
+      warm_used = 2;
+      best_metric = best_gap = best_p = best_d = INFINITY;
+      best_it = 0;
+      continue;
     }
     // factor A diag(x/s) A' (assembled by the residual passes)
     factor();
@@ -643,6 +713,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     LpOut o{};
     o.drops = drops;
     o.fail = fail;
+    o.warm_used = warm_used == 1 ? 1 : 0;
     if (status == SOV_OPTIMAL) {
       o.status = SOV_OPTIMAL;
       o.iterations = iters;
@@ -906,6 +977,7 @@ struct Batch {
   HBuf<double> pubdata;
   std::vector<int> fallback;  // LPs too large for the batched kernel
   sov_options opt{};
+  std::vector<sov_options> opts;  // per-LP options (empty: `opt` for all)
   struct Bucket {
     int mmax, threads, grid, count;
     const int* order;  // device: this bucket's LP indices, largest first (inside `in`)
@@ -967,15 +1039,21 @@ size_t align8(size_t v) { return (v + 7) & ~size_t(7); }
 
 }  // namespace
 
-Batch* batch_create(int count, const sov_model* models, const sov_options* opt_in) {
+Batch* batch_create(int count, const sov_model* models, const sov_options* opt_in, int opt_stride) {
   auto B = std::make_unique<Batch>();
   B->count = count;
   B->models.assign(models, models + count);
   B->forms.resize(count);
   if (opt_in) B->opt = *opt_in;
   else sov_default_lp_options(&B->opt);
-  const sov_options& opt = B->opt;
-  const bool scaling = opt.enable_scaling != 0;
+  // per-LP option blocks (opt_stride bytes apart) or one shared block
+  if (opt_in && opt_stride > 0) {
+    B->opts.resize(count);
+    for (int i = 0; i < count; ++i)
+      B->opts[i] = *reinterpret_cast<const sov_options*>(reinterpret_cast<const char*>(opt_in) +
+                                                         static_cast<size_t>(i) * opt_stride);
+  }
+  auto opt_of = [&](int i) -> const sov_options& { return B->opts.empty() ? B->opt : B->opts[i]; };
   ensure_smem_limits();
   // 1. shapes, in parallel. LPs with plain columns are later built in place, straight into the
   //    pinned staging; the others get a StdForm here (build_ipm_form semantics,
@@ -991,7 +1069,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
       return;
     }
     try {
-      B->forms[i] = build_std_form(models[i], false, scaling);
+      B->forms[i] = build_std_form(models[i], false, opt_of(i).enable_scaling != 0);
     } catch (const std::exception& e) {
       throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
     }
@@ -1002,14 +1080,15 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   // 2. offsets (serial prefix over the LPs)
   B->meta.resize(count);
   B->pub.resize(count);
-  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0, pubn = 0;
+  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0, pubn = 0, wv = 0;
   struct Run {
-    long long nnz, cols, rows, mv, nv;
+    long long nnz, cols, rows, mv, nv, wv;
   };
   std::vector<Run> run(count + 1);  // running totals before LP i (chunk boundaries of the staging)
   for (int i = 0; i < count; ++i) {
-    run[i] = Run{nnz, cols, rows, mv, nv};
+    run[i] = Run{nnz, cols, rows, mv, nv, wv};
     const LpShape& sh = shape[i];
+    const sov_options& opt = opt_of(i);
     LpMeta& mt = B->meta[i];
     std::memset(&mt, 0, sizeof(mt));
     if (kind[i] == kSingle) {
@@ -1029,6 +1108,11 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     mt.ftol = opt.feasibility_tol;
     mt.otol = opt.optimality_tol;
     mt.tau = opt.fraction_to_boundary;
+    mt.w_off = -1;
+    if (opt.warm_x && opt.warm_y && opt.warm_s) {
+      mt.w_off = wv;
+      wv += 2LL * sh.n + sh.m;
+    }
     Batch::Pub& pb = B->pub[i];
     pb.n_struct = sh.n_struct;
     pb.m0 = sh.m0;
@@ -1047,7 +1131,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     B->bytes += 6.0 * (12.0 * sh.nnz + 8.0 * (sh.m + sh.n)) + 15.0 * 8.0 * sh.n + 10.0 * 8.0 * sh.m;
     B->flops += (2.0 / 3.0) * std::pow(static_cast<double>(sh.m), 3.0);
   }
-  run[count] = Run{nnz, cols, rows, mv, nv};
+  run[count] = Run{nnz, cols, rows, mv, nv, wv};
   B->total_n = nv;
   B->total_m = mv;
   B->total_nnz = nnz;
@@ -1078,7 +1162,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     all_orders.insert(all_orders.end(), ids.begin(), ids.end());
     B->buckets.push_back(std::move(bk));
   }
-  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c | orders
+  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c | warm | orders
   const size_t o_meta = 0;
   const size_t o_cp = align8(o_meta + sizeof(LpMeta) * count);
   const size_t o_ri = o_cp + sizeof(int) * cols;
@@ -1088,7 +1172,8 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   const size_t o_rv = o_cv + sizeof(double) * nnz;
   const size_t o_b = o_rv + sizeof(double) * nnz;
   const size_t o_c = o_b + sizeof(double) * mv;
-  const size_t o_ord = o_c + sizeof(double) * nv;
+  const size_t o_w = o_c + sizeof(double) * nv;
+  const size_t o_ord = o_w + sizeof(double) * wv;
   const size_t total = o_ord + sizeof(int) * all_orders.size();
   B->h2d_bytes = static_cast<double>(total);
   B->in.alloc(total);
@@ -1124,10 +1209,17 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
         double* rv = reinterpret_cast<double*>(h + o_rv) + mt.a_off;
         double* bb = reinterpret_cast<double*>(h + o_b) + mt.mv_off;
         double* cc = reinterpret_cast<double*>(h + o_c) + mt.nv_off;
+        if (mt.w_off >= 0) {
+          const sov_options& o = opt_of(i);
+          double* wd = reinterpret_cast<double*>(h + o_w) + mt.w_off;
+          std::memcpy(wd, o.warm_x, sizeof(double) * mt.n);
+          std::memcpy(wd + mt.n, o.warm_y, sizeof(double) * mt.m);
+          std::memcpy(wd + mt.n + mt.m, o.warm_s, sizeof(double) * mt.n);
+        }
         if (kind[i] == kInPlace) {
           const LpFormOut out{cp, ri, cv, rp, ci, rv, bb, cc, pubd + pb.shift_off, pubd + pb.cs_off, pubd + pb.rs_off};
           try {
-            build_plain_lp_into(models[i], shape[i], scaling, out, &pb.info);
+            build_plain_lp_into(models[i], shape[i], opt_of(i).enable_scaling != 0, out, &pb.info);
           } catch (const std::exception& e) {
             throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
           }
@@ -1163,6 +1255,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
       copy_range(o_rv + sizeof(double) * r0.nnz, sizeof(double) * (r1.nnz - r0.nnz));
       copy_range(o_b + sizeof(double) * r0.mv, sizeof(double) * (r1.mv - r0.mv));
       copy_range(o_c + sizeof(double) * r0.nv, sizeof(double) * (r1.nv - r0.nv));
+      copy_range(o_w + sizeof(double) * r0.wv, sizeof(double) * (r1.wv - r0.wv));
     }
     std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
     if (!all_orders.empty()) std::memcpy(h + o_ord, all_orders.data(), sizeof(int) * all_orders.size());
@@ -1190,6 +1283,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   d.rval = reinterpret_cast<const double*>(base + o_rv);
   d.b = reinterpret_cast<const double*>(base + o_b);
   d.c = reinterpret_cast<const double*>(base + o_c);
+  d.warm = reinterpret_cast<const double*>(base + o_w);
   double* w = B->work.p;
   d.x = w;
   d.s = w + nv;
@@ -1340,6 +1434,7 @@ void batch_results(Batch* B, sov_result* results) {
       r->diagnostics->coefficient_min_abs_after = f.info.coef_min_after;
       r->diagnostics->coefficient_max_abs_after = f.info.coef_max_after;
       r->diagnostics->refactorizations = o.iterations + 1;
+      r->diagnostics->warm_start_used = o.warm_used;
       r->diagnostics->stall_iteration = -1;
     }
   });
@@ -1356,7 +1451,7 @@ void batch_results(Batch* B, sov_result* results) {
     cudaStream_t st;
     SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     try {
-      solve_single(B->models[i], f, B->opt, r, st, nullptr);
+      solve_single(B->models[i], f, B->opts.empty() ? B->opt : B->opts[i], r, st, nullptr);
     } catch (...) {
       cudaStreamDestroy(st);
       throw;
@@ -1380,9 +1475,8 @@ void batch_transfer_bytes(const Batch* B, double* h2d, double* d2h) {
 void batch_destroy(Batch* B) { delete B; }
 
 int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results) {
-  (void)opt_stride;
   if (count == 0) return SOV_OK;
-  std::unique_ptr<Batch> B(batch_create(count, models, opt));
+  std::unique_ptr<Batch> B(batch_create(count, models, opt, opt_stride));
   cudaStream_t st;
   SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   try {

@@ -12,7 +12,7 @@ namespace sov {
 struct Batch;
 
 int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results);
-Batch* batch_create(int count, const sov_model* models, const sov_options* opt);
+Batch* batch_create(int count, const sov_model* models, const sov_options* opt, int opt_stride = 0);
 void batch_solve(Batch* b, cudaStream_t st);
 void batch_results(Batch* b, sov_result* results);
 void batch_stats(const Batch* b, int* launches, double* kernel_ms, double* bytes, double* flops);

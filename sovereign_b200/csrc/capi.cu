@@ -252,12 +252,13 @@ int sov_lp_solve_batch(int32_t count, const sov_model* models, const sov_options
   }
 }
 
-int sov_batch_create(int32_t count, const sov_model* models, const sov_options* opt, sov_batch** out) {
+int sov_batch_create(int32_t count, const sov_model* models, const sov_options* opt, int32_t opt_stride,
+                     sov_batch** out) {
   if (count <= 0 || !models || !out) return set_error(SOV_E_ARGUMENT, "bad batch arguments");
   try {
     int rc = check_device();
     if (rc) return rc;
-    *out = reinterpret_cast<sov_batch*>(sov::batch_create(count, models, opt));
+    *out = reinterpret_cast<sov_batch*>(sov::batch_create(count, models, opt, opt_stride));
     return SOV_OK;
   } catch (const sov::CudaError& e) {
     return set_error(SOV_E_CUDA, e.what());

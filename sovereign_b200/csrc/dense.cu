@@ -381,6 +381,17 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int l
   __shared__ int ok;
   const int t = threadIdx.x, r = t & (kNB - 1), g = t >> 6;
   for (int i = blockIdx.x; i < nb; i += gridDim.x) {
+    // this thread's 16 entries of Linv_ii and of L_{i,i-1} (the last dependency), loaded before any
+    // wait: once block i-1 releases its flag, the remaining path has no global loads of L
+    double li[16], lp[16];
+    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
+#pragma unroll
+    for (int u = 0; u < 16; ++u) li[u] = static_cast<double>(Li[(g * 16 + u) * kNB + r]);
+    if (i > 0) {
+      const T* Lp = M + static_cast<int64_t>((i - 1) * kNB) * ld + i * kNB + r;
+#pragma unroll
+      for (int u = 0; u < 16; ++u) lp[u] = static_cast<double>(Lp[static_cast<int64_t>(g * 16 + u) * ld]);
+    }
     double acc = 0.0;
     for (int j = 0; j < i; ++j) {
       if (t == 0) ok = wait_flag(flags + j, epoch);
@@ -390,19 +401,23 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int l
       }
       if (t < kNB) yj[t] = __ldcg(z + j * kNB + t);
       __syncthreads();
-      const T* Lij = M + static_cast<int64_t>(j * kNB) * ld + i * kNB + r;
+      if (j == i - 1) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc += lp[u] * yj[g * 16 + u];
+      } else {
+        const T* Lij = M + static_cast<int64_t>(j * kNB) * ld + i * kNB + r;
 #pragma unroll 4
-      for (int c = g * 16; c < g * 16 + 16; ++c) acc += static_cast<double>(Lij[static_cast<int64_t>(c) * ld]) * yj[c];
+        for (int c = g * 16; c < g * 16 + 16; ++c) acc += static_cast<double>(Lij[static_cast<int64_t>(c) * ld]) * yj[c];
+      }
       __syncthreads();
     }
     part[g][r] = acc;
     __syncthreads();
     if (t < kNB) rhs[t] = z[i * kNB + t] - (part[0][t] + part[1][t] + part[2][t] + part[3][t]);
     __syncthreads();
-    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
     double y = 0.0;
-#pragma unroll 4
-    for (int c = g * 16; c < g * 16 + 16; ++c) y += static_cast<double>(Li[c * kNB + r]) * rhs[c];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) y += li[u] * rhs[g * 16 + u];
     part[g][r] = y;
     __syncthreads();
     if (t < kNB) z[i * kNB + t] = part[0][t] + part[1][t] + part[2][t] + part[3][t];
@@ -423,6 +438,20 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   for (int q = blockIdx.x; q < nb; q += gridDim.x) {
     const int i = nb - 1 - q;
+    // this thread's entries of Linv_ii and of L_{i+1,i} (the last dependency), loaded before any wait
+    double li[8][2], lp[8][2];
+    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = w * 8 + u;
+      li[u][0] = static_cast<double>(Li[c * kNB + lane]);
+      li[u][1] = static_cast<double>(Li[c * kNB + lane + 32]);
+      if (i + 1 < nb) {
+        const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + (i + 1) * kNB;
+        lp[u][0] = static_cast<double>(col[lane]);
+        lp[u][1] = static_cast<double>(col[lane + 32]);
+      }
+    }
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int j = nb - 1; j > i; --j) {
       if (t == 0) ok = wait_flag(flags + j, epoch);
@@ -431,11 +460,16 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
       if (t < kNB) xj[t] = __ldcg(z + j * kNB + t);
       __syncthreads();
       // acc_c += sum_r L[j*64 + r][i*64 + c] * x_j[r]
+      if (j == i + 1) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int c = w * 8 + u;
-        const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + j * kNB;
-        acc[u] += static_cast<double>(col[lane]) * xj[lane] + static_cast<double>(col[lane + 32]) * xj[lane + 32];
+        for (int u = 0; u < 8; ++u) acc[u] += lp[u][0] * xj[lane] + lp[u][1] * xj[lane + 32];
+      } else {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int c = w * 8 + u;
+          const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + j * kNB;
+          acc[u] += static_cast<double>(col[lane]) * xj[lane] + static_cast<double>(col[lane + 32]) * xj[lane + 32];
+        }
       }
       __syncthreads();
     }
@@ -448,11 +482,10 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
     if (t < kNB) rhs[t] = z[i * kNB + t] - acc_s[t];
     __syncthreads();
     // x_c = sum_r Linv[r][c] rhs[r] = sum_r Li[c * 64 + r] rhs[r]
-    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int c = w * 8 + u;
-      double v = static_cast<double>(Li[c * kNB + lane]) * rhs[lane] + static_cast<double>(Li[c * kNB + lane + 32]) * rhs[lane + 32];
+      double v = li[u][0] * rhs[lane] + li[u][1] * rhs[lane + 32];
       v = warp_sum(v);
       if (lane == 0) acc_s[c] = v;
     }

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "band.cuh"
@@ -29,16 +30,38 @@
 namespace sov {
 namespace {
 
+// Device buffers of one solve are stream-ordered allocations on the solve's stream (the default
+// memory pool of the device, kept cached up to kPoolKeep bytes): concurrent solves on other
+// streams neither pay cudaMalloc nor wait on the device-wide synchronisation of cudaFree.
+thread_local cudaStream_t tl_alloc_stream = nullptr;  // set by Engine::setup for its buffers
+constexpr uint64_t kPoolKeep = uint64_t(4) << 30;
+
+void keep_pool_memory() {
+  static std::mutex mu;
+  static std::vector<int> done;
+  int dev = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+  cudaMemPool_t pool;
+  SOV_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t keep = kPoolKeep;
+  SOV_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  done.push_back(dev);
+}
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t st = nullptr;
   DevBuf() = default;
   explicit DevBuf(size_t count) { alloc(count); }
   void alloc(size_t count) {
     release();
     n = count;
-    if (count) SOV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+    st = tl_alloc_stream;
+    if (count) SOV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * count, st));
   }
   void zero(cudaStream_t st) {
     if (n) SOV_CUDA(cudaMemsetAsync(p, 0, sizeof(T) * n, st));
@@ -47,7 +70,7 @@ struct DevBuf {
     if (count) SOV_CUDA(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, st));
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     n = 0;
   }
@@ -56,10 +79,42 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
 };
 
+// Pinned 256-byte slots for the few scalars a solve reads back every iteration, from one pinned
+// block shared by all solves of the process (pinning and unpinning per solve would serialise
+// concurrent solves).
+class PinnedSlots {
+ public:
+  void* acquire() {
+    std::lock_guard<std::mutex> g(mu_);
+    if (free_.empty()) {
+      unsigned char* block = nullptr;
+      SOV_CUDA(cudaMallocHost(&block, kSlot * kPerBlock));
+      for (int k = kPerBlock - 1; k >= 0; --k) free_.push_back(block + kSlot * k);
+    }
+    void* p = free_.back();
+    free_.pop_back();
+    return p;
+  }
+  void release(void* p) {
+    std::lock_guard<std::mutex> g(mu_);
+    free_.push_back(p);
+  }
+
+ private:
+  static constexpr size_t kSlot = 256;
+  static constexpr int kPerBlock = 256;
+  std::mutex mu_;
+  std::vector<void*> free_;
+};
+PinnedSlots g_pinned_slots;
+
 struct PinnedScalars {
   IpmScalars* h = nullptr;
-  PinnedScalars() { SOV_CUDA(cudaMallocHost(&h, sizeof(IpmScalars))); }
-  ~PinnedScalars() { cudaFreeHost(h); }
+  PinnedScalars() {
+    static_assert(sizeof(IpmScalars) <= 256, "scalar block larger than a pinned slot");
+    h = static_cast<IpmScalars*>(g_pinned_slots.acquire());
+  }
+  ~PinnedScalars() { g_pinned_slots.release(h); }
 };
 
 // -------------------------------------------------------------------------------------------
@@ -206,6 +261,7 @@ class Engine {
   // matrix only gets worse conditioned as the iterates approach the boundary): from the next
   // factorization on, the engine factors in FP64
   static constexpr int kPcgSwitch = 12;
+  static constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the default restart
   bool to_fp64_ = false;
   // x-space QP
   XSpace xs_;
@@ -216,6 +272,8 @@ class Engine {
 };
 
 void Engine::setup() {
+  tl_alloc_stream = st_;
+  keep_pool_memory();
   const int m = f_.m, n = f_.n;
   row_ptr_.alloc(m + 1);
   row_ptr_.upload(f_.row_ptr.data(), m + 1, st_);
@@ -298,7 +356,7 @@ void Engine::setup() {
       }
       pcg_tmp_.alloc(n);
       pcg_s_.alloc(1);
-      SOV_CUDA(cudaMallocHost(&pcg_h_, sizeof(PcgScalars)));
+      pcg_h_ = static_cast<PcgScalars*>(g_pinned_slots.acquire());
     }
   }
   if (xspace_) {
@@ -566,12 +624,15 @@ void Engine::run(sov_result* r) {
   SOV_CUDA(cudaEventRecord(e0, st_));
 
   // starting point (interior_point.cpp:488-506 / qp_interior_point.cpp:2881-2950, default start)
-  assemble_and_factor(kWeightOnes);
-  if (xspace_) launch_start_rhs_x(dev_, st_, &launches_);
-  else launch_start_rhs(dev_, st_, &launches_);
-  newton_solve();
-  if (xspace_) launch_start_dy_x(dev_, st_, &launches_);
-  launch_start_point(dev_, st_, &launches_);
+  auto default_start = [&]() {
+    assemble_and_factor(kWeightOnes);
+    if (xspace_) launch_start_rhs_x(dev_, st_, &launches_);
+    else launch_start_rhs(dev_, st_, &launches_);
+    newton_solve();
+    if (xspace_) launch_start_dy_x(dev_, st_, &launches_);
+    launch_start_point(dev_, st_, &launches_);
+  };
+  default_start();
   bool warm_used = false;
   if (opt_.warm_x && opt_.warm_y && opt_.warm_s) {
     // keep the supplied point when its residual metric beats the default start's
@@ -680,6 +741,18 @@ void Engine::run(sov_result* r) {
       done = true;
       break;
     }
+    // a supplied start that has not converged after kWarmGiveUp iterations is abandoned once: the
+    // solve restarts from the default start (and so does its best-iterate record)
+    if (warm_used && it + 1 == kWarmGiveUp) {
+      warm_used = false;
+      if (dg) dg->warm_start_used = 0;
+      default_start();
+      SOV_CUDA(cudaMemsetAsync(&sc_.p->fail, 0, sizeof(int), st_));
+      best_metric = best_gap = best_p = best_d = INFINITY;
+      best_it = 0;
+      stale = 0;
+      continue;
+    }
     assemble_and_factor(f_.qp ? kWeightQp : kWeightLp);
     for (int pass : {kRhsAffine, kRhsCorrector}) {
       if (xspace_) launch_newton_rhs_x(dev_, pass, st_, &launches_);
@@ -731,7 +804,7 @@ void Engine::run(sov_result* r) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (pcg_h_) cudaFreeHost(pcg_h_);
+  if (pcg_h_) g_pinned_slots.release(pcg_h_);
 }
 
 }  // namespace

@@ -101,17 +101,37 @@ class QpInteriorPointSolver:
         return _solve(model, self.options.to_abi(qp=True), True, with_ipm, with_diag, None)
 
 
-def solve_batch(models: list[Model], options: InteriorPointOptions | None = None, with_ipm: bool = False
-                ) -> list[Result]:
-    """Independent LPs in one persistent batched launch (sov_lp_solve_batch)."""
+def _per_lp_options(opt: abi.SovOptions, warm_starts: list):
+    """One option block per LP (copies of opt) carrying each LP's warm start, if any; the arrays
+    the blocks point at are returned too and must outlive the call."""
+    keep = []
+    opts = (abi.SovOptions * len(warm_starts))()
+    for k, w in enumerate(warm_starts):
+        C.memmove(C.byref(opts[k]), C.byref(opt), C.sizeof(abi.SovOptions))
+        if w is not None:
+            a = [np.ascontiguousarray(v, dtype=np.float64) for v in w]
+            keep.append(a)
+            opts[k].warm_x, opts[k].warm_y, opts[k].warm_s = (abi.dptr(v) for v in a)
+    return opts, keep
+
+
+def solve_batch(models: list[Model], options: InteriorPointOptions | None = None, with_ipm: bool = False,
+                warm_starts: list | None = None, with_diag: bool = False) -> list[Result]:
+    """Independent LPs in one persistent batched launch (sov_lp_solve_batch). warm_starts: one
+    (x, y, s) tuple (engine standard form) or None per LP; passed as per-LP option blocks."""
     opt = (options or InteriorPointOptions()).to_abi()
     bufs = []
     for m in models:
         n_ipm, m_ipm = _dims(m) if with_ipm else (0, 0)
-        bufs.append(ResultBuffers(m, with_ipm=with_ipm, n_ipm=n_ipm, m_ipm=m_ipm))
+        bufs.append(ResultBuffers(m, with_ipm=with_ipm, with_diag=with_diag, n_ipm=n_ipm, m_ipm=m_ipm))
     arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
     res = (abi.SovResult * len(models))(*[b.raw for b in bufs])
-    check(load().sov_lp_solve_batch(len(models), arr, C.byref(opt), 0, res))
+    if warm_starts is None:
+        check(load().sov_lp_solve_batch(len(models), arr, C.byref(opt), 0, res))
+    else:
+        opts, keep = _per_lp_options(opt, warm_starts)
+        check(load().sov_lp_solve_batch(len(models), arr, opts, C.sizeof(abi.SovOptions), res))
+        del keep
     out = []
     for b, r in zip(bufs, res):
         b.raw = r
@@ -122,12 +142,18 @@ def solve_batch(models: list[Model], options: InteriorPointOptions | None = None
 class DeviceBatch:
     """A prepared batch resident on the device (sov_batch_*): upload once, solve many times."""
 
-    def __init__(self, models: list[Model], options: InteriorPointOptions | None = None):
+    def __init__(self, models: list[Model], options: InteriorPointOptions | None = None,
+                 warm_starts: list | None = None):
         self.models = models
         self._arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
         self._opt = (options or InteriorPointOptions()).to_abi()
         h = C.c_void_p()
-        check(load().sov_batch_create(len(models), self._arr, C.byref(self._opt), C.byref(h)))
+        if warm_starts is None:
+            check(load().sov_batch_create(len(models), self._arr, C.byref(self._opt), 0, C.byref(h)))
+        else:
+            opts, keep = _per_lp_options(self._opt, warm_starts)
+            check(load().sov_batch_create(len(models), self._arr, opts, C.sizeof(abi.SovOptions), C.byref(h)))
+            del keep
         self.handle = h
 
     def solve(self, stream: int = 0) -> None:

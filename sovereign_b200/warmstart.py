@@ -142,10 +142,7 @@ class WarmStart:
         """Warm starts floored into the interior: x, s >= delta (scaled problem units)."""
         out = self.fout.invert(self.mlp.forward(self.fin.apply(np.atleast_2d(params))).astype(np.float64))
         n, m = self.n_ipm, self.m_ipm
-        starts = []
-        for row in out:
-            x = np.maximum(np.exp(np.clip(row[:n], -40, 40)), delta)
-            y = row[n:n + m].copy()
-            s = np.maximum(np.exp(np.clip(row[n + m:], -40, 40)), delta)
-            starts.append((x, y, s))
-        return starts
+        xs = np.maximum(np.exp(np.clip(out[:, :n], -40, 40)), delta)
+        ys = np.ascontiguousarray(out[:, n:n + m])
+        ss = np.maximum(np.exp(np.clip(out[:, n + m:], -40, 40)), delta)
+        return [(xs[k], ys[k], ss[k]) for k in range(out.shape[0])]

@@ -155,3 +155,46 @@ def test_dependent_rows_are_dropped():
     A = mdl.dense_A()
     Mm = A @ np.diag(d) @ A.T
     np.testing.assert_allclose(Mm @ z, rhs, rtol=1e-8, atol=1e-7 * np.abs(rhs).max())
+
+
+def test_batch_per_lp_options():
+    # option blocks one per LP (opt_stride): LP 0 gets a 3-iteration cap, the others the defaults
+    from sovereign_b200 import _lib
+    import ctypes as C
+    models = P.transport_batch(6, seed=21)
+    opts = (abi.SovOptions * len(models))(*[abi.default_options() for _ in models])
+    opts[0].max_iterations = 3
+    res = solve_batch_raw(models, opts, C.sizeof(abi.SovOptions))
+    assert res[0].status_name in ("FEASIBLE", "NUMERICAL_ERROR") and res[0].iterations <= 3
+    for r in res[1:]:
+        assert r.status_name == "OPTIMAL"
+
+
+def solve_batch_raw(models, opts, stride):
+    import ctypes as C
+    from sovereign_b200 import _lib
+    from sovereign_b200.model import ResultBuffers
+    bufs = [ResultBuffers(m) for m in models]
+    arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
+    res = (abi.SovResult * len(models))(*[b.raw for b in bufs])
+    _lib.check(_lib.load().sov_lp_solve_batch(len(models), arr, opts, stride, res))
+    out = []
+    for b, r in zip(bufs, res):
+        b.raw = r
+        out.append(b.to_result())
+    return out
+
+
+def test_batch_warm_start_saves_iterations():
+    # start each LP of the batch from its own iterate at the start of iteration 6 (single engine):
+    # the batched kernel takes it (safeguard passed), converges to the same optimum, in fewer steps
+    models = P.transport_batch(24, seed=33)
+    early = [InteriorPointSolver(InteriorPointOptions(ipm_iterate_at=6)).solve(m, with_ipm=True) for m in models]
+    cold = solve_batch(models, with_diag=True)
+    warm = solve_batch(models, warm_starts=[(e.ipm_x, e.ipm_y, e.ipm_s) for e in early], with_diag=True)
+    for c, w in zip(cold, warm):
+        assert c.status_name == "OPTIMAL" and w.status_name == "OPTIMAL"
+        assert rel(w.objective_value, c.objective_value) < 1e-8
+    assert sum(w.diagnostics["warm_start_used"] for w in warm) >= len(models) - 2
+    assert not any(c.diagnostics["warm_start_used"] for c in cold)
+    assert np.mean([w.iterations for w in warm]) <= np.mean([c.iterations for c in cold]) - 3
