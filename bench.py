@@ -302,8 +302,10 @@ def run_batched_warm_start(args):
 
     run(C.byref(base), 0, 1)  # warm-up
     t_cold, cold = run(C.byref(base), 0, max(1, args.steps))
+    params = np.stack([p for _, p in test])
+    ws.predict(params)  # untimed: sizes the network's work buffers for this batch
     t0 = time.perf_counter()
-    starts = ws.predict(np.stack([p for _, p in test]))
+    starts = ws.predict(params)
     t_pred = time.perf_counter() - t0
     opts = (A.SovOptions * count)()
     keep = []
