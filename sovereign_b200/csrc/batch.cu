@@ -97,7 +97,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   const int m = mt.m, n = mt.n;
   // M: lower triangle, packed by rows (row i at tri(i)); then six m-vectors
   double* M = sm;
-  double* vy = sm + tri(mmax);
+  double* vy = sm + tri(mmax + 1);
   double* vrp = vy + mmax;
   double* vz = vrp + mmax;
   double* vacc = vz + mmax;
@@ -195,12 +195,10 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         if (lane == 0) {
           M[tri(i) + i] = s1 + 1e-12;
           vdiag[i] = s1 + 1e-12;
-          if (mode == 1) {
-            vrp[i] = r;
-            vz[i] = r + s2;
-          } else {
-            vz[i] = r;
-          }
+          const double rhs = mode == 1 ? r + s2 : r;
+          if (mode == 1) vrp[i] = r;
+          vz[i] = rhs;
+          M[tri(m) + i] = rhs;  // the augmented row of the factorization that follows
         }
       }
     }
@@ -216,10 +214,14 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   //      (8 shared loads per 16 FMAs instead of 3 shared accesses per FMA).
   // Every entry sees the same operations in the same order as the column-at-a-time algorithm
   // (M[i][j] -= (M[i][k] / D_k) * M[j][k] for k = 0, 1, ...), so the factor is bit-identical to it.
+  // With `augmented`, row m holds a right-hand side r: it takes every column's update like any row
+  // below the panels, which is the forward substitution, so afterwards M[m][k] = (L^-1 r)_k and
+  // only the backward substitution is left for that right-hand side.
   // vdiag[k] (the assembled diagonal, the reference for the dependent-row test) is overwritten
   // with the pivot outcome of column k once it has been used: 0 kept, 1 dropped, 2 not finite.
-  auto factor = [&]() {
+  auto factor = [&](bool augmented) {
     constexpr int KB = 8;
+    const int mr = augmented ? m + 1 : m;  // rows factored: row m carries a right-hand side
     for (int k0 = 0; k0 < m; k0 += KB) {
       const int k1 = min(k0 + KB, m);
       if (warp == 0) {
@@ -257,7 +259,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         if (code == 1.0) ++drops;
         if (code == 2.0) fail = 1;
       }
-      for (int i = k1 + tid; i < m; i += NT) {
+      for (int i = k1 + tid; i < mr; i += NT) {
         double r[KB];
         double* Mi = M + tri(i) + k0;
 #pragma unroll
@@ -276,7 +278,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
           if (k0 + a < k1) Mi[a] = r[a];
       }
       __syncthreads();
-      const int tt = (m - k1 + 3) >> 2;
+      const int tt = (mr - k1 + 3) >> 2;
       const int ntiles = tt * (tt + 1) / 2;
       for (int tile = tid; tile < ntiles; tile += NT) {
         int ti = static_cast<int>((sqrtf(8.0f * tile + 1.0f) - 1.0f) * 0.5f);
@@ -284,13 +286,13 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
         const int tj = tile - ti * (ti + 1) / 2;
         const int i0 = k1 + 4 * ti, j0 = k1 + 4 * tj;
-        // rows past m are clamped to m - 1 and columns to the row (in-bounds loads, stores masked)
+        // rows past mr are clamped to mr - 1 and columns to the row (in-bounds loads, stores masked)
         int ri4[4], rj4[4], iq[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          iq[q] = min(i0 + q, m - 1);
+          iq[q] = min(i0 + q, mr - 1);
           ri4[q] = tri(iq[q]);
-          rj4[q] = tri(min(j0 + q, m - 1));
+          rj4[q] = tri(min(j0 + q, mr - 1));
         }
         double acc[4][4];
 #pragma unroll
@@ -314,7 +316,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         for (int q = 0; q < 4; ++q)
 #pragma unroll
           for (int r = 0; r < 4; ++r)
-            if (i0 + q < m && j0 + r <= i0 + q) M[ri4[q] + j0 + r] = acc[q][r];
+            if (i0 + q < mr && j0 + r <= i0 + q) M[ri4[q] + j0 + r] = acc[q][r];
       }
       __syncthreads();
     }
@@ -326,20 +328,22 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   // shared-memory loads of L~ off the chain. Same operations, in the same order, as the
   // row-at-a-time substitution: forward w_k = z_k / D_k, z_i -= L~_ik w_k (L~ = L D); backward
   // x_k = w_k - (1/D_k) sum_{j>k} L~_jk x_j.
-  auto solve = [&]() {
+  // fwd_done: the forward substitution was done by an augmented factorization (row m of M holds
+  // L^-1 rhs), so w = D^-1 (row m) and only the backward substitution runs.
+  auto solve = [&](bool fwd_done) {
     if (warp == 0) {
       double zr[4], ir[4], ar[4];
       int ro[4];
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int i = t * 32 + lane;
-        zr[t] = i < m ? vz[i] : 0.0;
         ir[t] = i < m ? vinv[i] : 0.0;
+        zr[t] = i < m ? (fwd_done ? M[tri(m) + i] * ir[t] : vz[i]) : 0.0;
         ar[t] = 0.0;
         ro[t] = tri(min(i, m - 1));
       }
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < 4 && !fwd_done; ++t) {
         const int kend = min(32, m - t * 32);
         for (int kk = 0; kk < kend; ++kk) {
           const int k = t * 32 + kk;
@@ -395,14 +399,14 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   double* dvec = ds;
   double* tvec = dx;
   auto mehrotra_start = [&]() {
-    for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
+    for (int i = tid; i < tri(m + 1); i += NT) M[i] = 0.0;
     __syncthreads();
     for (int j = tid; j < n; j += NT) offdiag(cp[j], cp[j + 1], 1.0);
     __syncthreads();
     row_pass(0, nullptr, nullptr);
     __syncthreads();
-    factor();
-    solve();
+    factor(true);
+    solve(true);
     const bool start_ok = !fail;
     for (int j = tid; j < n; j += NT) {
       double xs = 1.0, ss = 1.0;
@@ -421,7 +425,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       vy[i] = start_ok ? vz[i] : 0.0;
       gby[i] = vy[i];
     }
-    for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
+    for (int i = tid; i < tri(m + 1); i += NT) M[i] = 0.0;
     fail = 0;
     __syncthreads();
   };
@@ -571,8 +575,9 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       best_it = 0;
       continue;
     }
-    // factor A diag(x/s) A' (assembled by the residual passes)
-    factor();
+    // factor A diag(x/s) A' (assembled by the residual passes), with the predictor's right-hand
+    // side as the augmented row
+    factor(true);
     if (fail) {
       status = -2;  // factorization failure: best iterate
       break;
@@ -607,7 +612,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         row_pass(2, nullptr, tvec);
         __syncthreads();
       }
-      solve();
+      solve(pass == 0);
       double* ddx = pass ? dx : dxa;
       double* dds = pass ? ds : dsa;
       double rpmin = 1.0, rdmin = 1.0;
@@ -704,7 +709,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       }
     }
     for (int i = tid; i < m; i += NT) vy[i] += ad * vz[i];
-    for (int i = tid; i < tri(m); i += NT) M[i] = 0.0;
+    for (int i = tid; i < tri(m + 1); i += NT) M[i] = 0.0;
     iters = it + 1;
     __syncthreads();
   }
@@ -753,7 +758,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT <= 256 ? 2 : 1)) k_bat
   }
 }
 
-size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(mmax)) + 6 * mmax); }
+size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(mmax + 1)) + 6 * mmax); }
 
 // The dynamic shared-memory limit of every instantiation is raised once to the largest bucket's
 // footprint, so launches (and launches captured in a graph) need no per-launch attribute call.
