@@ -263,12 +263,32 @@ bool plain_lp_shape(const sov_model& p, LpShape* s) {
 
 void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scaling, const LpFormOut& o,
                          LpFormInfo* info) {
-  thread_local std::vector<double> rs;
+  // The same arithmetic as build_std_form + scale_two_pass + csr_from_csc, fused into four passes
+  // over the entries: (1) copy, with the row counts, the coefficient range and the first row
+  // maxima; (2), (3) one scaling pass each, column by column (row scale, column maximum, column
+  // scale), the first one also collecting the second pass's row maxima and the second one the
+  // final coefficient range; (4) the CSR fill. Every value sees the same multiplications in the
+  // same order, so the result is bit for bit the general builder's.
+  thread_local std::vector<double> rs1, rs2;
   thread_local std::vector<int> fill;
+  constexpr double kInf = std::numeric_limits<double>::infinity();
   const int ns = s.n_struct, m0 = s.m0, m = s.m, n = s.n;
+  rs1.assign(m, 0.0);
+  std::fill(o.row_ptr, o.row_ptr + m + 1, 0);
+  double lo = kInf, hi = 0.0;
+  auto put = [&](int q, int r, double v) {
+    o.row_idx[q] = r;
+    o.val[q] = v;
+    o.row_ptr[r + 1]++;
+    const double a = std::abs(v);
+    const bool use = a > 0.0 && a < kInf;
+    lo = std::min(lo, use ? a : kInf);
+    hi = std::max(hi, use ? a : 0.0);
+    rs1[r] = std::max(rs1[r], a);
+  };
   for (int i = 0; i < m0; ++i) o.b[i] = p.rhs[i];
-  // structural columns: shift by lb, the column's entries, then its upper-bound row
-  // (interior_point.cpp:238-247, :289-293)
+  // (1) structural columns: shift by lb, the column's entries, then its upper-bound row
+  // (interior_point.cpp:238-247, :289-293); slack (+1) / surplus (-1) columns (:339-350)
   int q = 0, k_ub = 0;
   o.col_ptr[0] = 0;
   for (int j = 0; j < ns; ++j) {
@@ -278,29 +298,22 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
     for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) {
       const int r = p.row_idx[k];
       o.b[r] -= p.values[k] * lb;
-      o.row_idx[q] = r;
-      o.val[q] = p.values[k];
-      ++q;
+      put(q++, r, p.values[k]);
     }
     if (std::isfinite(ub) && ub < 1e29) {
       const double u = ub - lb;
       if (u < -1e-12) throw std::runtime_error("Inconsistent bounds for variable x" + std::to_string(j));
       const int r = m0 + k_ub++;
       o.b[r] = u;
-      o.row_idx[q] = r;
-      o.val[q] = 1.0;
-      ++q;
+      put(q++, r, 1.0);
     }
     o.col_ptr[j + 1] = q;
   }
-  // slack (+1) / surplus (-1) columns (:339-350)
   int col = ns;
   for (int r = 0; r < m; ++r) {
     const int kind = r < m0 ? p.sense[r] : SOV_LE;
     if (kind == SOV_EQ) continue;
-    o.row_idx[q] = r;
-    o.val[q] = kind == SOV_LE ? 1.0 : -1.0;
-    ++q;
+    put(q++, r, kind == SOV_LE ? 1.0 : -1.0);
     o.col_ptr[++col] = q;
   }
   const double sign = p.maximize ? -1.0 : 1.0;
@@ -309,11 +322,66 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
     o.col_scale[j] = 1.0;
   }
   for (int i = 0; i < m; ++i) o.row_scale[i] = 1.0;
-  coefficient_range(o.val, q, info->coef_min_before, info->coef_max_before);
+  info->coef_min_before = lo < kInf ? lo : 0.0;
+  info->coef_max_before = hi;
   info->scaling_applied = enable_scaling && m > 0 && n > 0;
-  if (info->scaling_applied) scale_two_pass(m, n, o.col_ptr, o.row_idx, o.val, o.b, o.c, o.row_scale, o.col_scale, rs);
-  coefficient_range(o.val, q, info->coef_min_after, info->coef_max_after);
-  csr_from_csc(m, n, o.col_ptr, o.row_idx, o.val, o.row_ptr, o.col_idx, o.rval, fill);
+  if (info->scaling_applied) {
+    // scale factors computed in loops of independent iterations (no carried state), so the
+    // square roots and divisions overlap
+    thread_local std::vector<double> cmx;
+    cmx.resize(n);
+    rs2.assign(m, 0.0);
+    lo = kInf;
+    hi = 0.0;
+    // (2), (3): rows by 1/sqrt(max|a|), then columns (interior_point.cpp:370-405), twice
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<double>& rs = pass == 0 ? rs1 : rs2;
+      for (int i = 0; i < m; ++i) rs[i] = rs[i] > 0.0 ? 1.0 / std::sqrt(rs[i]) : 1.0;
+      for (int i = 0; i < m; ++i) {
+        o.row_scale[i] *= rs[i];
+        o.b[i] *= rs[i];
+      }
+      for (int j = 0; j < n; ++j) {
+        double mx = 0.0;
+        for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
+          o.val[k] *= rs[o.row_idx[k]];
+          mx = std::max(mx, std::abs(o.val[k]));
+        }
+        cmx[j] = mx;
+      }
+      for (int j = 0; j < n; ++j) cmx[j] = cmx[j] > 0.0 ? 1.0 / std::sqrt(cmx[j]) : 1.0;
+      for (int j = 0; j < n; ++j) {
+        const double sc = cmx[j];
+        for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
+          o.val[k] *= sc;
+          const double a = std::abs(o.val[k]);
+          if (pass == 0) {
+            rs2[o.row_idx[k]] = std::max(rs2[o.row_idx[k]], a);
+          } else {
+            const bool use = a > 0.0 && a < kInf;
+            lo = std::min(lo, use ? a : kInf);
+            hi = std::max(hi, use ? a : 0.0);
+          }
+        }
+        o.c[j] *= sc;
+        o.col_scale[j] *= sc;
+      }
+    }
+    info->coef_min_after = lo < kInf ? lo : 0.0;
+    info->coef_max_after = hi;
+  } else {
+    info->coef_min_after = info->coef_min_before;
+    info->coef_max_after = info->coef_max_before;
+  }
+  // (4) CSR: row counts were taken in (1)
+  for (int i = 0; i < m; ++i) o.row_ptr[i + 1] += o.row_ptr[i];
+  fill.assign(o.row_ptr, o.row_ptr + m);
+  for (int j = 0; j < n; ++j)
+    for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
+      const int t = fill[o.row_idx[k]]++;
+      o.col_idx[t] = j;
+      o.rval[t] = o.val[k];
+    }
 }
 
 namespace {
