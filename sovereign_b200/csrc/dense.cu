@@ -202,20 +202,73 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
     }
     __syncthreads();
   }
-  // inverse, column c by forward substitution on e_c; 4 threads per column split each dot product
+  // inverse of the 64 x 64 factor, blocked: the four 16 x 16 diagonal blocks by forward
+  // substitution (warp b, lane c = column c of block b, the column in registers), then the
+  // off-diagonal blocks in three stages by distance from the diagonal,
+  // X_ij = -X_ii (sum_{k=j}^{i-1} L_ik X_kj), each 16 x 16 block on 64 threads
   {
-    const int c = tid >> 2, part = tid & 3;
-    for (int r = 0; r < kNB; ++r) {
-      T acc = T(0);
-      if (r > c)
-        for (int k = c + part; k < r; k += 4) acc += A[r][k] * I[k][c];
-      acc += __shfl_xor_sync(kFull, acc, 1);
-      acc += __shfl_xor_sync(kFull, acc, 2);
-      if (part == 0) I[r][c] = r < c ? T(0) : (r == c ? T(1) / A[r][r] : -acc / A[r][r]);
-      __syncwarp();
+    constexpr int kB = 16;
+    if (warp < 4 && lane < kB) {
+      const int R = warp * kB, c = lane;
+      T x[kB];
+#pragma unroll
+      for (int r = 0; r < kB; ++r) {
+        if (r < c) {
+          x[r] = T(0);
+        } else if (r == c) {
+          x[r] = T(1) / A[R + r][R + r];
+        } else {
+          T acc = T(0);
+#pragma unroll
+          for (int k = 0; k < kB; ++k)
+            if (k >= c && k < r) acc += A[R + r][R + k] * x[k];
+          x[r] = -acc / A[R + r][R + r];
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kB; ++r) I[R + r][R + c] = x[r];
+    }
+    // zero the strictly upper blocks
+    for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
+      const int r = idx / kNB, c = idx % kNB;
+      if (r / kB < c / kB) I[r][c] = T(0);
+    }
+    __syncthreads();
+    const int g = tid >> 6, t = tid & 63, rr = t >> 2, c4 = (t & 3) * 4;
+    for (int dist = 1; dist < 4; ++dist) {
+      const int j = g, i = g + dist;
+      const bool act = i < 4;
+      T v[4] = {T(0), T(0), T(0), T(0)};
+      if (act) {
+        // T = sum_{k=j}^{i-1} L_ik X_kj  (rows of block i, columns of block j)
+        for (int k = j; k < i; ++k)
+#pragma unroll
+          for (int q = 0; q < kB; ++q) {
+            const T l = A[i * kB + rr][k * kB + q];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] += l * I[k * kB + q][j * kB + c4 + u];
+          }
+      }
+      __syncthreads();
+      if (act)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) I[i * kB + rr][j * kB + c4 + u] = v[u];
+      __syncthreads();
+      T w[4] = {T(0), T(0), T(0), T(0)};
+      if (act)
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+          const T xi = I[i * kB + rr][i * kB + q];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) w[u] -= xi * I[i * kB + q][j * kB + c4 + u];
+        }
+      __syncthreads();
+      if (act)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) I[i * kB + rr][j * kB + c4 + u] = w[u];
+      __syncthreads();
     }
   }
-  __syncthreads();
   for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
     const int cc = idx / kNB, r = idx % kNB;
     if (r >= cc) M[static_cast<int64_t>(r0 + cc) * ld + r0 + r] = A[r][cc];
