@@ -27,6 +27,9 @@ __device__ __forceinline__ float big_pivot<float>() {
   return kBigPivotF;
 }
 
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+
 __device__ __forceinline__ double column_weight(int mode, int k, const double* x, const double* s,
                                                 const double* qdiag, const uint8_t* free_col) {
   if (mode == kWeightOnes) return 1.0;
@@ -90,10 +93,12 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------------------------
 // Diagonal block (64 x 64) on 256 threads, right-looking over 8-column panels, three barriers per
-// panel: warp 0 factors the 8 x 8 diagonal block (lane = row, the pivot rule per column), one
-// thread per row below solves its 8 panel entries against it in registers, and the trailing lower
-// triangle takes the panel's rank-8 update in 4 x 4 register tiles (one tile per thread). Then
-// the inverse of the 64 x 64 factor, four threads per column (shuffle-reduced dot products).
+// panel: warp 0 factors the 8 x 8 diagonal block in registers (lane = row, pivots and column
+// entries exchanged by shuffles, the pivot rule per column), one thread per row below solves its
+// 8 panel entries against it in registers, and the trailing lower triangle takes the panel's
+// rank-8 update in 4 x 4 register tiles (one tile per thread). Then the blocked inverse of the
+// 64 x 64 factor. Pivots come from one reciprocal square root (l_jj = p * rsqrt(p)), whose
+// reciprocal is kept for the panel solves and the inverse.
 // ---------------------------------------------------------------------------------------------
 constexpr int kPanel = 8;
 
@@ -105,8 +110,10 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
   T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
   T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
   __shared__ T rinv[kNB];
+  __shared__ double dref[kNB];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = kb * kNB;
+  if (tid < kNB) dref[tid] = r0 + tid < m ? fabs(diag[r0 + tid]) : 1.0;
   for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
     const int c = idx / kNB, r = idx % kNB;
     A[r][c] = r >= c ? M[static_cast<int64_t>(r0 + c) * ld + r0 + r] : T(0);
@@ -115,37 +122,39 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
   int drops = 0, bad = 0;
   for (int k0 = 0; k0 < kNB; k0 += kPanel) {
     const int k1 = k0 + kPanel;
-    // 1. the 8 x 8 diagonal block (warp 0, lane c = row k0 + c)
+    // 1. the 8 x 8 diagonal block (warp 0, lane c = row k0 + c, lanes 8..31 mirror lanes 0..7)
     if (warp == 0) {
-      const int i = k0 + lane;
-      for (int j = k0; j < k1; ++j) {
-        const T p = A[j][j];
-        const int gj = r0 + j;
-        const double dref = gj < m ? diag[gj] : 1.0;
+      const int lr = lane & (kPanel - 1), i = k0 + lr;
+      T r[kPanel];
+#pragma unroll
+      for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        const T p = __shfl_sync(kFull, r[j], j);
         bool drop = false;
         if (!isfinite(static_cast<double>(p))) {
           bad = 1;
           drop = true;
-        } else if (static_cast<double>(p) <= drop_tol * fabs(dref)) {
+        } else if (static_cast<double>(p) <= drop_tol * dref[k0 + j]) {
           drop = true;  // dependent row (sparse_ldlt.cpp:165-173)
         }
-        const T ljj = drop ? big_pivot<T>() : sqrt(p);
-        const T inv = T(1) / ljj;
-        if (drop && gj < m) ++drops;
-        if (lane < kPanel && i > j) A[i][j] *= inv;
-        if (lane == 0) {
-          A[j][j] = ljj;
-          rinv[j] = inv;
-        }
-        __syncwarp();
-        if (lane < kPanel && i > j) {
-          const T lij = A[i][j];
+        const T inv = drop ? T(1) / big_pivot<T>() : rsqrt_t(p);
+        const T ljj = drop ? big_pivot<T>() : p * inv;
+        if (drop && r0 + k0 + j < m) ++drops;
+        if (lr == j) r[j] = ljj;
+        else if (lr > j) r[j] *= inv;
+        if (lane == 0) rinv[k0 + j] = inv;
+        const T lj = r[j];
 #pragma unroll
-          for (int k = 1; k < kPanel; ++k)
-            if (j + k <= i) A[i][j + k] -= lij * A[j + k][j];
+        for (int k = j + 1; k < kPanel; ++k) {
+          const T lkj = __shfl_sync(kFull, lj, k);
+          if (lr >= k) r[k] -= lj * lkj;
         }
-        __syncwarp();
       }
+      if (lane < kPanel)
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c)
+          if (c <= lr) A[i][k0 + c] = r[c];
     }
     __syncthreads();
     if (k1 >= kNB) break;
@@ -216,13 +225,13 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
         if (r < c) {
           x[r] = T(0);
         } else if (r == c) {
-          x[r] = T(1) / A[R + r][R + r];
+          x[r] = rinv[R + r];
         } else {
           T acc = T(0);
 #pragma unroll
           for (int k = 0; k < kB; ++k)
             if (k >= c && k < r) acc += A[R + r][R + k] * x[k];
-          x[r] = -acc / A[R + r][R + r];
+          x[r] = -acc * rinv[R + r];
         }
       }
 #pragma unroll
