@@ -92,11 +92,11 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Diagonal block (64 x 64) on 256 threads, right-looking over 8-column panels, three barriers per
-// panel: warp 0 factors the 8 x 8 diagonal block in registers (lane = row, pivots and column
-// entries exchanged by shuffles, the pivot rule per column), one thread per row below solves its
-// 8 panel entries against it in registers, and the trailing lower triangle takes the panel's
-// rank-8 update in 4 x 4 register tiles (one tile per thread). Then the blocked inverse of the
+// Diagonal block (64 x 64) on 256 threads, right-looking over 8-column panels, two barriers per
+// panel: the 64 threads of warps 0-1 each factor the 8 x 8 diagonal block in registers (the pivot
+// rule per column), and those with a row below solve its 8 panel entries against that factor
+// without a barrier between; then the trailing lower triangle takes the panel's rank-8 update in
+// 4 x 4 register tiles (one tile per thread). Then the blocked inverse of the
 // 64 x 64 factor. Pivots come from one reciprocal square root (l_jj = p * rsqrt(p)), whose
 // reciprocal is kept for the panel solves and the inverse.
 // ---------------------------------------------------------------------------------------------
@@ -122,15 +122,18 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
   int drops = 0, bad = 0;
   for (int k0 = 0; k0 < kNB; k0 += kPanel) {
     const int k1 = k0 + kPanel;
-    // 1. the 8 x 8 diagonal block (warp 0, lane c = row k0 + c, lanes 8..31 mirror lanes 0..7)
-    if (warp == 0) {
-      const int lr = lane & (kPanel - 1), i = k0 + lr;
-      T r[kPanel];
+    // 1. the 8 x 8 diagonal block, factored in registers by every thread of warps 0-1 with the
+    // same arithmetic in every lane (no exchange on the pivot chain); thread 0 stores it
+    // 2. rows below: L[i][k0:k1] = A[i][k0:k1] L_kk^-T, one row per thread, from those registers
+    if (tid < kNB) {
+      T d[kPanel][kPanel], dinv[kPanel];
 #pragma unroll
-      for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
+      for (int i = 0; i < kPanel; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) d[i][j] = A[k0 + i][k0 + j];
 #pragma unroll
       for (int j = 0; j < kPanel; ++j) {
-        const T p = __shfl_sync(kFull, r[j], j);
+        const T p = d[j][j];
         bool drop = false;
         if (!isfinite(static_cast<double>(p))) {
           bad = 1;
@@ -139,41 +142,41 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
           drop = true;  // dependent row (sparse_ldlt.cpp:165-173)
         }
         const T inv = drop ? T(1) / big_pivot<T>() : rsqrt_t(p);
-        const T ljj = drop ? big_pivot<T>() : p * inv;
         if (drop && r0 + k0 + j < m) ++drops;
-        if (lr == j) r[j] = ljj;
-        else if (lr > j) r[j] *= inv;
-        if (lane == 0) rinv[k0 + j] = inv;
-        const T lj = r[j];
+        d[j][j] = drop ? big_pivot<T>() : p * inv;
+        dinv[j] = inv;
 #pragma unroll
-        for (int k = j + 1; k < kPanel; ++k) {
-          const T lkj = __shfl_sync(kFull, lj, k);
-          if (lr >= k) r[k] -= lj * lkj;
+        for (int i = j + 1; i < kPanel; ++i) d[i][j] *= inv;
+#pragma unroll
+        for (int i = j + 1; i < kPanel; ++i)
+#pragma unroll
+          for (int k = j + 1; k <= i; ++k) d[i][k] -= d[i][j] * d[k][j];
+      }
+      if (tid == 0) {
+#pragma unroll
+        for (int i = 0; i < kPanel; ++i) {
+          rinv[k0 + i] = dinv[i];
+#pragma unroll
+          for (int j = 0; j <= i; ++j) A[k0 + i][k0 + j] = d[i][j];
         }
       }
-      if (lane < kPanel)
+      if (tid < kNB - k1) {
+        const int i = k1 + tid;
+        T r[kPanel];
 #pragma unroll
-        for (int c = 0; c < kPanel; ++c)
-          if (c <= lr) A[i][k0 + c] = r[c];
+        for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c) {
+          r[c] *= dinv[c];
+#pragma unroll
+          for (int e = c + 1; e < kPanel; ++e) r[e] -= r[c] * d[e][c];
+        }
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c) A[i][k0 + c] = r[c];
+      }
     }
     __syncthreads();
     if (k1 >= kNB) break;
-    // 2. rows below: L[i][k0:k1] = A[i][k0:k1] L_kk^-T, one row per thread, in registers
-    if (tid < kNB - k1) {
-      const int i = k1 + tid;
-      T r[kPanel];
-#pragma unroll
-      for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
-#pragma unroll
-      for (int c = 0; c < kPanel; ++c) {
-        r[c] *= rinv[k0 + c];
-#pragma unroll
-        for (int d = c + 1; d < kPanel; ++d) r[d] -= r[c] * A[k0 + d][k0 + c];
-      }
-#pragma unroll
-      for (int c = 0; c < kPanel; ++c) A[i][k0 + c] = r[c];
-    }
-    __syncthreads();
     // 3. trailing lower triangle: A[i][j] -= sum_k L[i][k] L[j][k], 4 x 4 tiles
     {
       const int nt = (kNB - k1) / 4;
