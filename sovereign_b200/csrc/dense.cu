@@ -10,6 +10,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cfloat>
 
 #include "common.cuh"
 #include "dense.cuh"
@@ -29,6 +30,21 @@ __device__ __forceinline__ float big_pivot<float>() {
 
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+// four consecutive elements from 16-byte-aligned shared memory
+__device__ __forceinline__ void load4(const double* p, double v[4]) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+__device__ __forceinline__ void load4(const float* p, float v[4]) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
 
 __device__ __forceinline__ double column_weight(int mode, int k, const double* x, const double* s,
                                                 const double* qdiag, const uint8_t* free_col) {
@@ -120,51 +136,58 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
   }
   __syncthreads();
   int drops = 0, bad = 0;
+  // the panel's columns below its diagonal block, transposed (Lt[c][i] = L[i][k0 + c]), so the
+  // trailing update reads four consecutive rows per vector load; aliases I, which is unused until
+  // the inverse
+  T(*Lt)[kNB] = reinterpret_cast<T(*)[kNB]>(&I[0][0]);
+  // 4 x 4 tile of this thread in the trailing update: tid = ti (ti + 1) / 2 + tj, the same for
+  // every panel (a panel with nt tile rows uses tids below nt (nt + 1) / 2)
+  int ti = static_cast<int>((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
+  while (ti * (ti + 1) / 2 > tid) --ti;
+  while ((ti + 1) * (ti + 2) / 2 <= tid) ++ti;
+  const int tj = tid - ti * (ti + 1) / 2;
   for (int k0 = 0; k0 < kNB; k0 += kPanel) {
     const int k1 = k0 + kPanel;
     // 1. the 8 x 8 diagonal block, factored in registers by every thread of warps 0-1 with the
-    // same arithmetic in every lane (no exchange on the pivot chain); thread 0 stores it
+    // same arithmetic in every lane (no exchange on the pivot chain, the pivot rule without
+    // branches); thread 0 stores it
     // 2. rows below: L[i][k0:k1] = A[i][k0:k1] L_kk^-T, one row per thread, from those registers
     if (tid < kNB) {
+      const bool has_row = tid < kNB - k1;
+      const int i = k1 + tid;
+      T r[kPanel];
+      if (has_row)
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
       T d[kPanel][kPanel], dinv[kPanel];
+      double thr[kPanel];
 #pragma unroll
-      for (int i = 0; i < kPanel; ++i)
+      for (int j = 0; j < kPanel; ++j) {
+        thr[j] = drop_tol * dref[k0 + j];
 #pragma unroll
-        for (int j = 0; j <= i; ++j) d[i][j] = A[k0 + i][k0 + j];
+        for (int c = 0; c <= j; ++c) d[j][c] = A[k0 + j][k0 + c];
+      }
 #pragma unroll
       for (int j = 0; j < kPanel; ++j) {
         const T p = d[j][j];
-        bool drop = false;
-        if (!isfinite(static_cast<double>(p))) {
-          bad = 1;
-          drop = true;
-        } else if (static_cast<double>(p) <= drop_tol * dref[k0 + j]) {
-          drop = true;  // dependent row (sparse_ldlt.cpp:165-173)
-        }
-        const T inv = drop ? T(1) / big_pivot<T>() : rsqrt_t(p);
-        if (drop && r0 + k0 + j < m) ++drops;
-        d[j][j] = drop ? big_pivot<T>() : p * inv;
+        const double pd = static_cast<double>(p);
+        // dependent row (sparse_ldlt.cpp:165-173): pivot not finite, or at most tol * |diag|
+        const bool finite = fabs(pd) <= DBL_MAX;
+        const bool drop = !(finite && pd > thr[j]);
+        bad |= !finite;
+        drops += (drop && r0 + k0 + j < m);
+        const T inv_p = rsqrt_t(p);
+        const T inv = drop ? T(1) / big_pivot<T>() : inv_p;
+        d[j][j] = drop ? big_pivot<T>() : p * inv_p;
         dinv[j] = inv;
 #pragma unroll
-        for (int i = j + 1; i < kPanel; ++i) d[i][j] *= inv;
+        for (int q = j + 1; q < kPanel; ++q) d[q][j] *= inv;
 #pragma unroll
-        for (int i = j + 1; i < kPanel; ++i)
+        for (int q = j + 1; q < kPanel; ++q)
 #pragma unroll
-          for (int k = j + 1; k <= i; ++k) d[i][k] -= d[i][j] * d[k][j];
+          for (int k = j + 1; k <= q; ++k) d[q][k] -= d[q][j] * d[k][j];
       }
-      if (tid == 0) {
-#pragma unroll
-        for (int i = 0; i < kPanel; ++i) {
-          rinv[k0 + i] = dinv[i];
-#pragma unroll
-          for (int j = 0; j <= i; ++j) A[k0 + i][k0 + j] = d[i][j];
-        }
-      }
-      if (tid < kNB - k1) {
-        const int i = k1 + tid;
-        T r[kPanel];
-#pragma unroll
-        for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
+      if (has_row) {
 #pragma unroll
         for (int c = 0; c < kPanel; ++c) {
           r[c] *= dinv[c];
@@ -172,7 +195,18 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
           for (int e = c + 1; e < kPanel; ++e) r[e] -= r[c] * d[e][c];
         }
 #pragma unroll
-        for (int c = 0; c < kPanel; ++c) A[i][k0 + c] = r[c];
+        for (int c = 0; c < kPanel; ++c) {
+          A[i][k0 + c] = r[c];
+          Lt[c][i] = r[c];
+        }
+      }
+      if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < kPanel; ++q) {
+          rinv[k0 + q] = dinv[q];
+#pragma unroll
+          for (int c = 0; c <= q; ++c) A[k0 + q][k0 + c] = d[q][c];
+        }
       }
     }
     __syncthreads();
@@ -180,12 +214,7 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
     // 3. trailing lower triangle: A[i][j] -= sum_k L[i][k] L[j][k], 4 x 4 tiles
     {
       const int nt = (kNB - k1) / 4;
-      const int ntiles = nt * (nt + 1) / 2;
-      if (tid < ntiles) {
-        int ti = static_cast<int>((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
-        while (ti * (ti + 1) / 2 > tid) --ti;
-        while ((ti + 1) * (ti + 2) / 2 <= tid) ++ti;
-        const int tj = tid - ti * (ti + 1) / 2;
+      if (ti < nt) {
         const int i0 = k1 + 4 * ti, j0 = k1 + 4 * tj;
         T acc[4][4];
 #pragma unroll
@@ -193,13 +222,10 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
 #pragma unroll
           for (int u = 0; u < 4; ++u) acc[q][u] = A[i0 + q][j0 + u];
 #pragma unroll
-        for (int k = k0; k < k1; ++k) {
+        for (int k = 0; k < kPanel; ++k) {
           T li[4], lj[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            li[q] = A[i0 + q][k];
-            lj[q] = A[j0 + q][k];
-          }
+          load4(&Lt[k][i0], li);
+          load4(&Lt[k][j0], lj);
 #pragma unroll
           for (int q = 0; q < 4; ++q)
 #pragma unroll
