@@ -1,16 +1,19 @@
 // dense.cu -- dense normal-matrix path on the GPU.
 //
 // Assembly: one gather pass over a precomputed contribution map (no atomics, deterministic).
-// Factorization: blocked right-looking Cholesky, 64-wide panels; per panel one CTA factors the
-// diagonal block in shared memory and inverts it, the panel below is L_ik = A_ik L_kk^-T (a GEMM
-// with the inverse), and the trailing lower triangle gets A_ij -= L_ik L_jk^T.
+// Factorization: blocked right-looking Cholesky, 64-wide panels; one CTA factors a diagonal block
+// in shared memory and inverts it, the panel below is L_ik = A_ik L_kk^-T (a GEMM with the
+// inverse), and the trailing lower triangle gets A_ij -= L_ik L_jk^T. One launch per panel does
+// both as flag-ordered work items, the next diagonal block's factor among them (look-ahead).
 // Solves: dataflow triangular solves, one cooperative launch per direction; row block i waits
 // (acquire flag, bounded spin) for the blocks it depends on, so the off-diagonal GEMV work of all
 // blocks overlaps and only the 64x64 diagonal products sit on the critical path.
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
+#include <stdexcept>
 
 #include "common.cuh"
 #include "dense.cuh"
@@ -130,9 +133,19 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = kb * kNB;
   if (tid < kNB) dref[tid] = r0 + tid < m ? fabs(diag[r0 + tid]) : 1.0;
-  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
-    const int c = idx / kNB, r = idx % kNB;
-    A[r][c] = r >= c ? M[static_cast<int64_t>(r0 + c) * ld + r0 + r] : T(0);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {  // 8 loads in flight per thread
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = tid + 256 * (8 * h + u), c = idx / kNB, r = idx % kNB;
+      v[u] = r >= c ? M[static_cast<int64_t>(r0 + c) * ld + r0 + r] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = tid + 256 * (8 * h + u);
+      A[idx % kNB][idx / kNB] = v[u];
+    }
   }
   __syncthreads();
   int drops = 0, bad = 0;
@@ -321,12 +334,15 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
 template <class T>
 __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag,
                                                     int m, T* __restrict__ Linv, int* drop_count, int* fail,
-                                                    double drop_tol) {
+                                                    double drop_tol, unsigned* tickets) {
   extern __shared__ __align__(16) unsigned char potrf_raw[];
+  if (tickets != nullptr && threadIdx.x == 0) *tickets = 0u;
   potrf_block<T>(M, ld, kb, diag, m, Linv, drop_count, fail, drop_tol, potrf_raw);
 }
 
-// C (64x64 at rows r0, cols c0 of M) = beta * C + sign * X Y^T, X/Y given as [k][64] slices.
+// acc[p][q] += sum_k Xs[k][tx + 16 p] Ys[k][ty + 16 q], tx = tid % 16, ty = tid / 16 (256 threads):
+// a half-warp reads 16 consecutive entries of Xs (one wavefront) and one entry of Ys (broadcast),
+// and its results are 16 consecutive rows of a column-major tile (coalesced stores)
 template <class T>
 __device__ __forceinline__ void tile_nt(const T (*Xs)[kNB], const T (*Ys)[kNB], T (&acc)[4][4]) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -335,8 +351,8 @@ __device__ __forceinline__ void tile_nt(const T (*Xs)[kNB], const T (*Ys)[kNB], 
     T a[4], b[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      a[q] = Xs[k][ty * 4 + q];
-      b[q] = Ys[k][tx * 4 + q];
+      a[q] = Xs[k][tx + 16 * q];
+      b[q] = Ys[k][ty + 16 * q];
     }
 #pragma unroll
     for (int p = 0; p < 4; ++p)
@@ -345,112 +361,30 @@ __device__ __forceinline__ void tile_nt(const T (*Xs)[kNB], const T (*Ys)[kNB], 
   }
 }
 
-// Panel: L_ik = A_ik * Linv_kk^T for every row block i > kb.
-template <class T>
-__global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ M, int ld, int kb, const T* __restrict__ Linv) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T(*Xs)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw);
-  T(*Ys)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw + sizeof(T) * kNB * kNB);
-  const int i = kb + 1 + blockIdx.x;
-  const int r0 = i * kNB, k0 = kb * kNB;
-  const T* Lk = Linv + static_cast<int64_t>(kb) * kNB * kNB;
-  for (int idx = threadIdx.x; idx < kNB * kNB; idx += blockDim.x) {
-    const int k = idx / kNB, r = idx % kNB;
-    Xs[k][r] = M[static_cast<int64_t>(k0 + k) * ld + r0 + r];
-    Ys[k][r] = Lk[idx];  // Ys[k][c] = Linv[c][k] = Lk[k * 64 + c]
-  }
-  __syncthreads();
-  T acc[4][4] = {};
-  tile_nt<T>(Xs, Ys, acc);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+// Two 64 x 64 slices into shared memory, dst[k][r] = src[k * ld + r], on 256 threads with 16
+// loads in flight per thread; kBypassL1 reads past L1 (data written by other CTAs of this launch).
+template <bool kBypassL1, class T>
+__device__ __forceinline__ void load_slices(T (*Xs)[kNB], const T* __restrict__ xsrc, int64_t xld, T (*Ys)[kNB],
+                                            const T* __restrict__ ysrc, int64_t yld) {
+  const int tid = threadIdx.x;
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+  for (int h = 0; h < 2; ++h) {
+    T vx[8], vy[8];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) M[static_cast<int64_t>(k0 + tx * 4 + q) * ld + r0 + ty * 4 + p] = acc[p][q];
-}
-
-// Trailing update: A_ij -= L_ik L_jk^T for kb < j <= i (tile index enumerates the lower triangle).
-// Look-ahead: tile 0 is the next diagonal block (kb+1, kb+1); the CTA that updates it goes on to
-// factor and invert it (potrf_block), so the next panel's diagonal factor overlaps the rest of this
-// update instead of running alone on one SM afterwards.
-template <class T>
-__global__ void __launch_bounds__(256) k_syrk_update(T* __restrict__ M, int ld, int kb, int nb, const double* __restrict__ diag,
-                                                     int m, T* __restrict__ Linv, int* drop_count, int* fail,
-                                                     double drop_tol) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T(*Xs)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw);
-  T(*Ys)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw + sizeof(T) * kNB * kNB);
-  // tile t -> (ii, jj) with 0 <= jj <= ii < R
-  const int t = blockIdx.x;
-  int ii = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-  while ((ii + 1) * (ii + 2) / 2 <= t) ++ii;
-  while (ii * (ii + 1) / 2 > t) --ii;
-  const int jj = t - ii * (ii + 1) / 2;
-  const int i = kb + 1 + ii, j = kb + 1 + jj;
-  (void)nb;
-  const int r0 = i * kNB, c0 = j * kNB, k0 = kb * kNB;
-  for (int idx = threadIdx.x; idx < kNB * kNB; idx += blockDim.x) {
-    const int k = idx / kNB, r = idx % kNB;
-    Xs[k][r] = M[static_cast<int64_t>(k0 + k) * ld + r0 + r];
-    Ys[k][r] = M[static_cast<int64_t>(k0 + k) * ld + c0 + r];
-  }
-  __syncthreads();
-  T acc[4][4] = {};
-  tile_nt<T>(Xs, Ys, acc);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      T* dst = M + static_cast<int64_t>(c0 + tx * 4 + q) * ld + r0 + ty * 4 + p;
-      *dst -= acc[p][q];
+    for (int u = 0; u < 8; ++u) {
+      const int idx = tid + 256 * (8 * h + u), k = idx / kNB, r = idx % kNB;
+      vx[u] = kBypassL1 ? __ldcg(xsrc + k * xld + r) : xsrc[k * xld + r];
+      vy[u] = kBypassL1 ? __ldcg(ysrc + k * yld + r) : ysrc[k * yld + r];
     }
-  if (t == 0) {
-    __syncthreads();
-    potrf_block<T>(M, ld, kb + 1, diag, m, Linv, drop_count, fail, drop_tol, smem_raw);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = tid + 256 * (8 * h + u);
+      Xs[idx / kNB][idx % kNB] = vx[u];
+      Ys[idx / kNB][idx % kNB] = vy[u];
+    }
   }
 }
 
-template <class T>
-void dense_potrf_block(const DenseSystem<T>& s, int kb, cudaStream_t st) {
-  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
-  static bool attr_set = false;
-  if (!attr_set) {
-    SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
-    attr_set = true;
-  }
-  k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
-}
-
-template <class T>
-void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
-  const size_t smem = 2 * sizeof(T) * kNB * kNB;
-  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
-  static bool attr_set = false;
-  if (!attr_set) {
-    SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
-    SOV_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SOV_CUDA(cudaFuncSetAttribute(k_syrk_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
-    attr_set = true;
-  }
-  // panel 0's diagonal block alone; every later one is factored by its look-ahead CTA inside the
-  // previous panel's trailing update
-  k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, 0, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol);
-  int n = 1;
-  for (int kb = 0; kb + 1 < s.nb; ++kb) {
-    const int R = s.nb - kb - 1;
-    k_trsm_panel<T><<<R, 256, smem, st>>>(s.M, s.mp, kb, s.Linv);
-    k_syrk_update<T><<<R * (R + 1) / 2, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.nb, s.diag, s.m, s.Linv,
-                                                                s.drop_count, s.fail, s.drop_tol);
-    n += 2;
-  }
-  SOV_LAUNCH_CHECK();
-  if (launches) *launches += n;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Dataflow triangular solves
-// ---------------------------------------------------------------------------------------------
 constexpr long long kSpinLimit = 1ll << 22;  // bounded wait (x >= 64 ns per poll -> > 0.25 s)
 
 __device__ __forceinline__ bool wait_flag(const unsigned* flag, unsigned epoch) {
@@ -462,6 +396,145 @@ __device__ __forceinline__ bool wait_flag(const unsigned* flag, unsigned epoch) 
   return true;
 }
 
+__device__ __forceinline__ void tile_triangle(int t, int& ii, int& jj) {
+  // t -> (ii, jj) with 0 <= jj <= ii, t = ii (ii + 1) / 2 + jj
+  ii = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((ii + 1) * (ii + 2) / 2 <= t) ++ii;
+  while (ii * (ii + 1) / 2 > t) --ii;
+  jj = t - ii * (ii + 1) / 2;
+}
+
+// One launch per panel kb < nb - 1: the panel solves L_ik = A_ik Linv_kk^T of the R = nb - kb - 1
+// row blocks below it and the trailing updates A_ij -= L_ik L_jk^T of the tiles kb < j <= i, as
+// R + R (R + 1) / 2 - 1 work items taken in ticket order (an atomic counter):
+//   item 0      the look-ahead chain: row block kb + 1's panel solve, then its diagonal tile's
+//               update from the solved block still in shared memory, then the factor and inverse
+//               of that diagonal block (potrf_block), so the next panel's diagonal factor starts
+//               as soon as its own inputs exist rather than after the whole panel;
+//   1 .. R-1    the other panel solves, each publishing its row block with a release flag;
+//   R ..        the other trailing tiles, each waiting (acquire, bounded) for its two row blocks.
+// A trailing tile only waits for panel solves, which never wait and hold lower tickets, so every
+// item it waits for was taken by a CTA that is already running. Blocks solved by other CTAs of
+// the launch are read past L1 (ld.global.cg).
+template <class T>
+__global__ void __launch_bounds__(256) k_panel_update(T* __restrict__ M, int ld, int kb, int nb,
+                                                      const double* __restrict__ diag, int m, T* __restrict__ Linv,
+                                                      int* drop_count, int* fail, double drop_tol, unsigned* flags,
+                                                      unsigned stamp, unsigned* tickets, unsigned base) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*Xs)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw);
+  T(*Ys)[kNB] = reinterpret_cast<T(*)[kNB]>(smem_raw + sizeof(T) * kNB * kNB);
+  __shared__ unsigned item_s;
+  __shared__ int ok_s;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  if (tid == 0) item_s = atomicAdd(tickets, 1u) - base;
+  __syncthreads();
+  const int item = static_cast<int>(item_s);
+  const int R = nb - kb - 1, k0 = kb * kNB;
+  if (item < R) {
+    const int i = kb + 1 + item, r0 = i * kNB;
+    // Ys[k][c] = Linv[c][k] = Lk[k * 64 + c]
+    load_slices<false>(Xs, M + static_cast<int64_t>(k0) * ld + r0, ld, Ys, Linv + static_cast<int64_t>(kb) * kNB * kNB,
+                       kNB);
+    __syncthreads();
+    T acc[4][4] = {};
+    tile_nt<T>(Xs, Ys, acc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int p = 0; p < 4; ++p) M[static_cast<int64_t>(k0 + ty + 16 * q) * ld + r0 + tx + 16 * p] = acc[p][q];
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      st_release(flags + i, stamp);
+    }
+    if (item != 0) return;
+    // look-ahead: A_ii -= L_ik L_ik^T from the block just solved, then its factor and inverse
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int p = 0; p < 4; ++p) Xs[ty + 16 * q][tx + 16 * p] = acc[p][q];
+    __syncthreads();
+    T upd[4][4] = {};
+    tile_nt<T>(Xs, Xs, upd);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int p = 0; p < 4; ++p) M[static_cast<int64_t>(r0 + ty + 16 * q) * ld + r0 + tx + 16 * p] -= upd[p][q];
+    __syncthreads();
+    potrf_block<T>(M, ld, kb + 1, diag, m, Linv, drop_count, fail, drop_tol, smem_raw);
+    return;
+  }
+  int ii, jj;
+  tile_triangle(item - R + 1, ii, jj);
+  const int i = kb + 1 + ii, j = kb + 1 + jj;
+  if (tid == 0) ok_s = wait_flag(flags + i, stamp) && wait_flag(flags + j, stamp);
+  __syncthreads();
+  if (!ok_s) {
+    if (tid == 0) atomicExch(fail, 1);
+    return;
+  }
+  const int r0 = i * kNB, c0 = j * kNB;
+  load_slices<true>(Xs, M + static_cast<int64_t>(k0) * ld + r0, ld, Ys, M + static_cast<int64_t>(k0) * ld + c0, ld);
+  __syncthreads();
+  T acc[4][4] = {};
+  tile_nt<T>(Xs, Ys, acc);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int p = 0; p < 4; ++p) M[static_cast<int64_t>(c0 + ty + 16 * q) * ld + r0 + tx + 16 * p] -= acc[p][q];
+}
+
+template <class T>
+void dense_potrf_block(const DenseSystem<T>& s, int kb, cudaStream_t st) {
+  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    attr_set = true;
+  }
+  k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol,
+                                              nullptr);
+}
+
+// panel stamps: top bit set, so they never equal a triangular-solve epoch on the same flags;
+// a generation per factorization and the panel index below it
+constexpr int kStampPanelBits = 11;
+std::atomic<unsigned> g_factor_generation{0};
+
+template <class T>
+void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
+  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    SOV_CUDA(cudaFuncSetAttribute(k_panel_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    attr_set = true;
+  }
+  if (s.nb >= (1 << kStampPanelBits)) throw std::runtime_error("dense factor: too many row blocks");
+  const unsigned gen = (g_factor_generation.fetch_add(1) & ((1u << (31 - kStampPanelBits)) - 1)) << kStampPanelBits;
+  // panel 0's diagonal block alone (it also resets the ticket counter); every later one is
+  // factored by item 0 of the previous panel's launch
+  k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, 0, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol,
+                                              s.tickets);
+  int n = 1;
+  unsigned base = 0;
+  for (int kb = 0; kb + 1 < s.nb; ++kb) {
+    const int R = s.nb - kb - 1;
+    const int items = R + R * (R + 1) / 2 - 1;
+    const unsigned stamp = 0x80000000u | gen | static_cast<unsigned>(kb);
+    k_panel_update<T><<<items, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.nb, s.diag, s.m, s.Linv, s.drop_count, s.fail,
+                                                       s.drop_tol, s.flags, stamp, s.tickets, base);
+    base += static_cast<unsigned>(items);
+    ++n;
+  }
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += n;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Dataflow triangular solves
+// ---------------------------------------------------------------------------------------------
 // Forward: L y = r, row block order. z holds r on entry and y on exit.
 template <class T>
 __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int ld, const T* __restrict__ Linv, int nb,

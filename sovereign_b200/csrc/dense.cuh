@@ -20,7 +20,8 @@ struct DenseSystem {
   int m, mp, nb;
   int* drop_count;   // dropped pivots (dependent rows)
   int* fail;         // non-finite pivot
-  unsigned* flags;   // nb: dataflow flags for the triangular solves
+  unsigned* flags;   // nb: dataflow flags for the factor's panels and the triangular solves
+  unsigned* tickets; // 1: work-item counter of the factor's panel launches
   double drop_tol;   // pivot <= drop_tol * diag is a dependent row (1e-13 FP64, looser for FP32)
 };
 

@@ -343,7 +343,7 @@ void Engine::setup() {
     mp_ = nb_ * kNB;
     am_ = xspace_ ? build_assembly_xspace(f_, xs_, mp_) : build_assembly_dense(f_, mp_);
     diag_.alloc(order_);
-    flags_.alloc(nb_);
+    flags_.alloc(nb_ + 1);  // + the factor's ticket counter
     flags_.zero(st_);
     z_.alloc(mp_);
     z_.zero(st_);
@@ -386,7 +386,7 @@ void Engine::setup() {
     bandsys_.drop_count = drop_ptr;
     bandsys_.fail = fail_ptr;
   } else {
-    ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, order_, mp_, nb_, drop_ptr, fail_ptr, flags_.p, 1e-6};
+    ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, order_, mp_, nb_, drop_ptr, fail_ptr, flags_.p, flags_.p + nb_, 1e-6};
   }
 
   dev_.m = m;
@@ -457,7 +457,7 @@ void Engine::assemble_and_factor(int mode) {
     if (!M64_.p) {
       M64_.alloc(static_cast<size_t>(mp_) * mp_);
       Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
-      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
+      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, flags_.p + nb_, 1e-13};
     }
     launch_dense_clear<double>(M64_.p, order_, mp_, st_);
     launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, amode, reg, M64_.p, diag_.p, order_, mp_, st_);
@@ -521,7 +521,7 @@ bool Engine::newton_solve() {
     if (!M64_.p) {
       M64_.alloc(static_cast<size_t>(mp_) * mp_);
       Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
-      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, 1e-13};
+      ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, flags_.p + nb_, 1e-13};
     }
     launch_dense_clear<double>(M64_.p, f_.m, mp_, st_);
     launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, last_mode_, reg, M64_.p, diag_.p, f_.m, mp_, st_);

@@ -120,14 +120,15 @@ extern "C" int sov_normal_factor_solve_noalloc(int32_t m, int32_t n, const int32
     double* z = Linv + kScratchLinv;
     double* diag = z + kNoAllocMaxRows;
     unsigned* flags = reinterpret_cast<unsigned*>(sp.i);
-    int* counters = sp.i + 64;  // [0] dropped pivots, [1] non-finite pivot, [2] solve timeout
+    int* counters = sp.i + 64;  // [0] dropped pivots, [1] non-finite pivot, [2] solve timeout, [3] tickets
     // clear what must start at zero: the matrix, the flags and the counters
     SOV_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * static_cast<size_t>(mp) * mp, st));
     SOV_CUDA(cudaMemsetAsync(sp.i, 0, sizeof(int) * kScratchInts, st));
     if (n > 0) k_scatter_normal<<<ceil_div(n, 128), 128, 0, st>>>(n, col_ptr, row_idx, values, d, M, mp);
     k_finish_diag<<<ceil_div(mp, 128), 128, 0, st>>>(M, m, mp, diag);
     SOV_LAUNCH_CHECK();
-    DenseSystem<double> s{M, Linv, diag, m, mp, nb, counters, counters + 1, flags, 1e-13};
+    DenseSystem<double> s{M, Linv, diag, m, mp, nb, counters, counters + 1, flags,
+                          reinterpret_cast<unsigned*>(counters + 3), 1e-13};
     dense_cholesky<double>(s, st, nullptr);
     unsigned epoch = 0;
     for (int r = 0; r < nrhs; ++r) {

@@ -114,7 +114,7 @@ int normal_factor_solve_device(int m, int n, const int* col_ptr, const int* row_
   Tmp<double> dx(n), ds(n), ddiag(m);
   dx.put(d, n);
   ds.put(ones.data(), n);
-  Tmp<int> counters(2);
+  Tmp<int> counters(3);
   SOV_CUDA(cudaMemset(counters.p, 0, 2 * sizeof(int)));
   const int kd = normal_bandwidth(f);
   const bool band = factorization == SOV_FACTOR_BANDED || (factorization == SOV_FACTOR_AUTO && kd <= kBandMax && m > 256);
@@ -162,7 +162,8 @@ int normal_factor_solve_device(int m, int n, const int* col_ptr, const int* row_
       Tmp<double> M(static_cast<size_t>(mp) * mp), Linv(static_cast<size_t>(nb) * kNB * kNB);
       launch_dense_clear<double>(M.p, m, mp, 0);
       launch_assemble<double>(ad, dx.p, ds.p, nullptr, nullptr, kWeightLp, 1e-12, M.p, ddiag.p, m, mp, 0);
-      DenseSystem<double> s{M.p, Linv.p, ddiag.p, m, mp, nb, counters.p, counters.p + 1, flags.p, 1e-13};
+      DenseSystem<double> s{M.p, Linv.p, ddiag.p, m, mp, nb, counters.p, counters.p + 1, flags.p,
+                                reinterpret_cast<unsigned*>(counters.p + 2), 1e-13};
       dense_cholesky<double>(s, 0, nullptr);
       for (int r = 0; r < nrhs; ++r) {
         z.put(rhs + static_cast<size_t>(r) * m, m);
@@ -173,7 +174,8 @@ int normal_factor_solve_device(int m, int n, const int* col_ptr, const int* row_
       Tmp<float> M(static_cast<size_t>(mp) * mp), Linv(static_cast<size_t>(nb) * kNB * kNB);
       launch_dense_clear<float>(M.p, m, mp, 0);
       launch_assemble<float>(ad, dx.p, ds.p, nullptr, nullptr, kWeightLp, 1e-12, M.p, ddiag.p, m, mp, 0);
-      DenseSystem<float> s{M.p, Linv.p, ddiag.p, m, mp, nb, counters.p, counters.p + 1, flags.p, 1e-6};
+      DenseSystem<float> s{M.p, Linv.p, ddiag.p, m, mp, nb, counters.p, counters.p + 1, flags.p,
+                               reinterpret_cast<unsigned*>(counters.p + 2), 1e-6};
       dense_cholesky_tc(s, err.p, 0, nullptr);
       for (int r = 0; r < nrhs; ++r) {
         z.put(rhs + static_cast<size_t>(r) * m, m);
