@@ -111,28 +111,81 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Diagonal block (64 x 64) on 256 threads, right-looking over 8-column panels, two barriers per
-// panel: the 64 threads of warps 0-1 each factor the 8 x 8 diagonal block in registers (the pivot
-// rule per column), and those with a row below solve its 8 panel entries against that factor
-// without a barrier between; then the trailing lower triangle takes the panel's rank-8 update in
-// 4 x 4 register tiles (one tile per thread). Then the blocked inverse of the
-// 64 x 64 factor. Pivots come from one reciprocal square root (l_jj = p * rsqrt(p)), whose
-// reciprocal is kept for the panel solves and the inverse.
+// Diagonal block (64 x 64) on 256 threads, right-looking over 8-column panels with look-ahead (one
+// barrier per panel), then the blocked inverse of the 64 x 64 factor. Pivots come from one
+// reciprocal square root (l_jj = p * rsqrt(p)), whose reciprocal is kept for the panel solves and
+// the inverse.
 // ---------------------------------------------------------------------------------------------
 constexpr int kPanel = 8;
 
-// Runs on a CTA of 256 threads; `potrf_raw` is at least 2 * 64 * 65 elements of dynamic shared memory.
+// One 8-column panel of the diagonal block on the 64 threads of warps 0-1: every one of them
+// factors the 8 x 8 diagonal block (rows/cols k0..k0+7 of A) in registers with the same
+// arithmetic (no exchange on the pivot chain, the pivot rule without branches), and the thread
+// with a row below (row k0 + 8 + tid, already updated, in r) solves it against that factor and
+// stores it to A and, transposed, to Lw (Lw[c][i] = L[i][k0 + c]). Thread 0 stores the factored
+// 8 x 8 block and the pivot reciprocals.
 template <class T>
-__device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag, int m,
-                            T* __restrict__ Linv, int* drop_count, int* fail, double drop_tol,
-                            unsigned char* potrf_raw) {
+__device__ __forceinline__ void factor_panel(T (*A)[kNB + 1], T (*Lw)[kNB], T* rinv, const double* dref, int k0,
+                                             int r0, int m, double drop_tol, T (&r)[kPanel], bool has_row,
+                                             int& drops, int& bad) {
+  const int tid = threadIdx.x;
+  T d[kPanel][kPanel], dinv[kPanel];
+  double thr[kPanel];
+#pragma unroll
+  for (int j = 0; j < kPanel; ++j) {
+    thr[j] = drop_tol * dref[k0 + j];
+#pragma unroll
+    for (int c = 0; c <= j; ++c) d[j][c] = A[k0 + j][k0 + c];
+  }
+#pragma unroll
+  for (int j = 0; j < kPanel; ++j) {
+    const T p = d[j][j];
+    const double pd = static_cast<double>(p);
+    // dependent row (sparse_ldlt.cpp:165-173): pivot not finite, or at most tol * |diag|
+    const bool finite = fabs(pd) <= DBL_MAX;
+    const bool drop = !(finite && pd > thr[j]);
+    bad |= !finite;
+    drops += (drop && r0 + k0 + j < m);
+    const T inv_p = rsqrt_t(p);
+    const T inv = drop ? T(1) / big_pivot<T>() : inv_p;
+    d[j][j] = drop ? big_pivot<T>() : p * inv_p;
+    dinv[j] = inv;
+#pragma unroll
+    for (int q = j + 1; q < kPanel; ++q) d[q][j] *= inv;
+#pragma unroll
+    for (int q = j + 1; q < kPanel; ++q)
+#pragma unroll
+      for (int k = j + 1; k <= q; ++k) d[q][k] -= d[q][j] * d[k][j];
+  }
+  if (has_row) {
+    const int i = k0 + kPanel + tid;
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) {
+      r[c] *= dinv[c];
+#pragma unroll
+      for (int e = c + 1; e < kPanel; ++e) r[e] -= r[c] * d[e][c];
+    }
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) {
+      A[i][k0 + c] = r[c];
+      Lw[c][i] = r[c];
+    }
+  }
+  if (tid == 0) {
+#pragma unroll
+    for (int q = 0; q < kPanel; ++q) {
+      rinv[k0 + q] = dinv[q];
+#pragma unroll
+      for (int c = 0; c <= q; ++c) A[k0 + q][k0 + c] = d[q][c];
+    }
+  }
+}
+
+// The diagonal block's lower triangle from M into A (upper entries zero); 256 threads.
+template <class T>
+__device__ __forceinline__ void potrf_load(const T* __restrict__ M, int ld, int kb, unsigned char* potrf_raw) {
   T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
-  T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
-  __shared__ T rinv[kNB];
-  __shared__ double dref[kNB];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int r0 = kb * kNB;
-  if (tid < kNB) dref[tid] = r0 + tid < m ? fabs(diag[r0 + tid]) : 1.0;
+  const int tid = threadIdx.x, r0 = kb * kNB;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {  // 8 loads in flight per thread
     T v[8];
@@ -147,108 +200,108 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
       A[idx % kNB][idx / kNB] = v[u];
     }
   }
+}
+
+// Factor and invert the diagonal block held in A (the first 64 x 65 elements of `potrf_raw`,
+// lower triangle, upper entries zero); stores L to M and L^-1 to Linv. Runs on a CTA of 256
+// threads; `potrf_raw` is at least 2 * 64 * 65 elements of dynamic shared memory.
+// Panels with look-ahead: while warps 0-1 apply panel p's update to panel p+1's eight columns and
+// factor panel p+1, warps 2-7 apply panel p's update to the trailing triangle right of them, so
+// each panel costs one barrier and the longer of the two.
+template <class T>
+__device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag, int m,
+                           T* __restrict__ Linv, int* drop_count, int* fail, double drop_tol,
+                           unsigned char* potrf_raw) {
+  T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw);
+  T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
+  __shared__ T rinv[kNB];
+  __shared__ double dref[kNB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = kb * kNB;
+  if (tid < kNB) dref[tid] = r0 + tid < m ? fabs(diag[r0 + tid]) : 1.0;
   __syncthreads();
   int drops = 0, bad = 0;
-  // the panel's columns below its diagonal block, transposed (Lt[c][i] = L[i][k0 + c]), so the
-  // trailing update reads four consecutive rows per vector load; aliases I, which is unused until
-  // the inverse
-  T(*Lt)[kNB] = reinterpret_cast<T(*)[kNB]>(&I[0][0]);
-  // 4 x 4 tile of this thread in the trailing update: tid = ti (ti + 1) / 2 + tj, the same for
-  // every panel (a panel with nt tile rows uses tids below nt (nt + 1) / 2)
-  int ti = static_cast<int>((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
-  while (ti * (ti + 1) / 2 > tid) --ti;
-  while ((ti + 1) * (ti + 2) / 2 <= tid) ++ti;
-  const int tj = tid - ti * (ti + 1) / 2;
-  for (int k0 = 0; k0 < kNB; k0 += kPanel) {
-    const int k1 = k0 + kPanel;
-    // 1. the 8 x 8 diagonal block, factored in registers by every thread of warps 0-1 with the
-    // same arithmetic in every lane (no exchange on the pivot chain, the pivot rule without
-    // branches); thread 0 stores it
-    // 2. rows below: L[i][k0:k1] = A[i][k0:k1] L_kk^-T, one row per thread, from those registers
+  // two panels' columns below their diagonal blocks, transposed (Lt[c][i] = L[i][k0 + c]), so an
+  // update reads consecutive rows per vector load; alias I, which is unused until the inverse
+  T(*Lt0)[kNB] = reinterpret_cast<T(*)[kNB]>(&I[0][0]);
+  T(*Lt1)[kNB] = Lt0 + kPanel;
+  // warps 2-7: 4 x 4 tile (ti, tj) of the trailing update, u = ti (ti + 1) / 2 + tj, the same for
+  // every panel (a triangle of nt tile rows uses u below nt (nt + 1) / 2)
+  const int u = tid - kNB;
+  int ti = 0, tj = 0;
+  if (u >= 0) {
+    ti = static_cast<int>((sqrtf(8.0f * u + 1.0f) - 1.0f) * 0.5f);
+    while (ti * (ti + 1) / 2 > u) --ti;
+    while ((ti + 1) * (ti + 2) / 2 <= u) ++ti;
+    tj = u - ti * (ti + 1) / 2;
+  }
+  if (tid < kNB) {
+    T r[kPanel];
+    const bool has_row = tid < kNB - kPanel;
+    if (has_row)
+#pragma unroll
+      for (int c = 0; c < kPanel; ++c) r[c] = A[kPanel + tid][c];
+    factor_panel<T>(A, Lt0, rinv, dref, 0, r0, m, drop_tol, r, has_row, drops, bad);
+  }
+  __syncthreads();
+  for (int p = 0; p + 1 < kNB / kPanel; ++p) {
+    const int K0 = (p + 1) * kPanel, K1 = K0 + kPanel;  // panel p+1's first column, and the next
+    T(*Lc)[kNB] = (p & 1) ? Lt1 : Lt0;                 // panel p
+    T(*Ln)[kNB] = (p & 1) ? Lt0 : Lt1;                 // panel p + 1
     if (tid < kNB) {
-      const bool has_row = tid < kNB - k1;
-      const int i = k1 + tid;
+      // panel p's update of panel p+1's columns: the 36 entries of its diagonal block (one per
+      // thread, shared through A) and each row below (in registers)
+      if (tid < kPanel * (kPanel + 1) / 2) {
+        int q = 0;
+        while ((q + 1) * (q + 2) / 2 <= tid) ++q;
+        const int c = tid - q * (q + 1) / 2;
+        T a = A[K0 + q][K0 + c];
+#pragma unroll
+        for (int k = 0; k < kPanel; ++k) a -= Lc[k][K0 + q] * Lc[k][K0 + c];
+        A[K0 + q][K0 + c] = a;
+      }
+      const bool has_row = tid < kNB - K1;
       T r[kPanel];
-      if (has_row)
-#pragma unroll
-        for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
-      T d[kPanel][kPanel], dinv[kPanel];
-      double thr[kPanel];
-#pragma unroll
-      for (int j = 0; j < kPanel; ++j) {
-        thr[j] = drop_tol * dref[k0 + j];
-#pragma unroll
-        for (int c = 0; c <= j; ++c) d[j][c] = A[k0 + j][k0 + c];
-      }
-#pragma unroll
-      for (int j = 0; j < kPanel; ++j) {
-        const T p = d[j][j];
-        const double pd = static_cast<double>(p);
-        // dependent row (sparse_ldlt.cpp:165-173): pivot not finite, or at most tol * |diag|
-        const bool finite = fabs(pd) <= DBL_MAX;
-        const bool drop = !(finite && pd > thr[j]);
-        bad |= !finite;
-        drops += (drop && r0 + k0 + j < m);
-        const T inv_p = rsqrt_t(p);
-        const T inv = drop ? T(1) / big_pivot<T>() : inv_p;
-        d[j][j] = drop ? big_pivot<T>() : p * inv_p;
-        dinv[j] = inv;
-#pragma unroll
-        for (int q = j + 1; q < kPanel; ++q) d[q][j] *= inv;
-#pragma unroll
-        for (int q = j + 1; q < kPanel; ++q)
-#pragma unroll
-          for (int k = j + 1; k <= q; ++k) d[q][k] -= d[q][j] * d[k][j];
-      }
       if (has_row) {
+        const int i = K1 + tid;
+        T li[kPanel];
+#pragma unroll
+        for (int k = 0; k < kPanel; ++k) li[k] = Lc[k][i];
 #pragma unroll
         for (int c = 0; c < kPanel; ++c) {
-          r[c] *= dinv[c];
+          T a = A[i][K0 + c];
 #pragma unroll
-          for (int e = c + 1; e < kPanel; ++e) r[e] -= r[c] * d[e][c];
-        }
-#pragma unroll
-        for (int c = 0; c < kPanel; ++c) {
-          A[i][k0 + c] = r[c];
-          Lt[c][i] = r[c];
+          for (int k = 0; k < kPanel; ++k) a -= li[k] * Lc[k][K0 + c];
+          r[c] = a;
         }
       }
-      if (tid == 0) {
-#pragma unroll
-        for (int q = 0; q < kPanel; ++q) {
-          rinv[k0 + q] = dinv[q];
-#pragma unroll
-          for (int c = 0; c <= q; ++c) A[k0 + q][k0 + c] = d[q][c];
-        }
-      }
-    }
-    __syncthreads();
-    if (k1 >= kNB) break;
-    // 3. trailing lower triangle: A[i][j] -= sum_k L[i][k] L[j][k], 4 x 4 tiles
-    {
-      const int nt = (kNB - k1) / 4;
+      asm volatile("bar.sync 1, 64;" ::: "memory");  // warps 0-1: the diagonal block is updated
+      factor_panel<T>(A, Ln, rinv, dref, K0, r0, m, drop_tol, r, has_row, drops, bad);
+    } else {
+      // panel p's update of the trailing triangle (rows and columns from K1)
+      const int nt = (kNB - K1) / 4;
       if (ti < nt) {
-        const int i0 = k1 + 4 * ti, j0 = k1 + 4 * tj;
+        const int i0 = K1 + 4 * ti, j0 = K1 + 4 * tj;
         T acc[4][4];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int u = 0; u < 4; ++u) acc[q][u] = A[i0 + q][j0 + u];
+          for (int v = 0; v < 4; ++v) acc[q][v] = A[i0 + q][j0 + v];
 #pragma unroll
         for (int k = 0; k < kPanel; ++k) {
           T li[4], lj[4];
-          load4(&Lt[k][i0], li);
-          load4(&Lt[k][j0], lj);
+          load4(&Lc[k][i0], li);
+          load4(&Lc[k][j0], lj);
 #pragma unroll
           for (int q = 0; q < 4; ++q)
 #pragma unroll
-            for (int u = 0; u < 4; ++u) acc[q][u] -= li[q] * lj[u];
+            for (int v = 0; v < 4; ++v) acc[q][v] -= li[q] * lj[v];
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
-            if (j0 + u <= i0 + q) A[i0 + q][j0 + u] = acc[q][u];
+          for (int v = 0; v < 4; ++v)
+            if (j0 + v <= i0 + q) A[i0 + q][j0 + v] = acc[q][v];
       }
     }
     __syncthreads();
@@ -329,6 +382,14 @@ __device__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __r
     if (drops) atomicAdd(drop_count, drops);
     if (bad) atomicExch(fail, 1);
   }
+}
+
+template <class T>
+__device__ __forceinline__ void potrf_block(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag, int m,
+                                            T* __restrict__ Linv, int* drop_count, int* fail, double drop_tol,
+                                            unsigned char* potrf_raw) {
+  potrf_load<T>(M, ld, kb, potrf_raw);
+  potrf_core<T>(M, ld, kb, diag, m, Linv, drop_count, fail, drop_tol, potrf_raw);
 }
 
 template <class T>
@@ -449,20 +510,33 @@ __global__ void __launch_bounds__(256) k_panel_update(T* __restrict__ M, int ld,
       st_release(flags + i, stamp);
     }
     if (item != 0) return;
-    // look-ahead: A_ii -= L_ik L_ik^T from the block just solved, then its factor and inverse
+    // look-ahead: A_ii - L_ik L_ik^T from the block just solved, straight into the diagonal
+    // factor's shared-memory tile, then its factor and inverse
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int p = 0; p < 4; ++p) Xs[ty + 16 * q][tx + 16 * p] = acc[p][q];
-    __syncthreads();
-    T upd[4][4] = {};
-    tile_nt<T>(Xs, Xs, upd);
+    T cur[4][4];  // the diagonal tile's lower triangle, loaded while the product runs
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int p = 0; p < 4; ++p) M[static_cast<int64_t>(r0 + ty + 16 * q) * ld + r0 + tx + 16 * p] -= upd[p][q];
+      for (int p = 0; p < 4; ++p) {
+        const int r = tx + 16 * p, c = ty + 16 * q;
+        cur[p][q] = r >= c ? M[static_cast<int64_t>(r0 + c) * ld + r0 + r] : T(0);
+      }
     __syncthreads();
-    potrf_block<T>(M, ld, kb + 1, diag, m, Linv, drop_count, fail, drop_tol, smem_raw);
+    T upd[4][4] = {};
+    tile_nt<T>(Xs, Xs, upd);
+    __syncthreads();  // Xs, which the factor's tile overlays, is fully read
+    T(*A)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(smem_raw);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int r = tx + 16 * p, c = ty + 16 * q;
+        A[r][c] = r >= c ? cur[p][q] - upd[p][q] : T(0);
+      }
+    potrf_core<T>(M, ld, kb + 1, diag, m, Linv, drop_count, fail, drop_tol, smem_raw);
     return;
   }
   int ii, jj;
