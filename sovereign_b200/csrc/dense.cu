@@ -117,18 +117,96 @@ void launch_dense_clear(T* M, int m, int mp, cudaStream_t st) {
 // the inverse.
 // ---------------------------------------------------------------------------------------------
 constexpr int kPanel = 8;
+// diagonal factor's shared memory: A and I (64 x 65 each) and two transposed panels (8 x 64 each)
+template <class T>
+constexpr size_t potrf_smem_bytes() {
+  return sizeof(T) * (2 * kNB * (kNB + 1) + 2 * kPanel * kNB);
+}
+
+template <int kId, int kCount>
+__device__ __forceinline__ void bar_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(kId), "n"(kCount) : "memory");
+}
+
+// Row block p (rows 8p..8p+7) of X = L^-1, into I, once L's rows 8p..8p+7 are final in A and the
+// earlier row blocks of X are in I: X_pp = L_pp^-1 by forward substitution (threads kX1..kX1+7,
+// one column each), T_pj = sum_{k=j}^{8p-1} L[8p+q][k] X[k][j] for every column j < 8p (threads
+// from kX2, one entry at a time, two partial sums), then X_pj = -X_pp T_pj (one column per
+// thread). kThreads threads from index u = 0, synchronised on barrier kBar.
+template <int kThreads, int kBar, int kX1, int kX2, class T>
+__device__ __forceinline__ void inverse_row_block(const T (*A)[kNB + 1], T (*I)[kNB + 1], const T* rinv, int p, int u) {
+  const int R = p * kPanel;
+  if (u >= kX1 && u < kX1 + kPanel) {
+    // column c of X_pp: L_pp x = e_c, right-looking with every index static (x starts as e_c,
+    // so the entries above c stay zero)
+    const int c = u - kX1;
+    T l[kPanel * (kPanel + 1) / 2], ri[kPanel], x[kPanel];
+#pragma unroll
+    for (int r = 0; r < kPanel; ++r) {
+      ri[r] = rinv[R + r];
+      x[r] = r == c ? T(1) : T(0);
+#pragma unroll
+      for (int k = 0; k < r; ++k) l[r * (r - 1) / 2 + k] = A[R + r][R + k];
+    }
+#pragma unroll
+    for (int k = 0; k < kPanel; ++k) {
+      x[k] *= ri[k];
+#pragma unroll
+      for (int r = k + 1; r < kPanel; ++r) x[r] -= l[r * (r - 1) / 2 + k] * x[k];
+    }
+#pragma unroll
+    for (int r = 0; r < kPanel; ++r) I[R + r][R + c] = x[r];
+  }
+  if (R == 0) return;
+  for (int e = u - kX2; e >= 0 && e < kPanel * R; e += kThreads - kX2) {
+    const int q = e % kPanel, j = e / kPanel;
+    // by 8-row blocks of X from j's own (X is lower triangular: rows above j in it are zero),
+    // each block's 16 loads issued together
+    T a0 = T(0), a1 = T(0);
+    for (int k0 = j & ~(kPanel - 1); k0 < R; k0 += kPanel) {
+      T l[kPanel], x[kPanel];
+#pragma unroll
+      for (int t = 0; t < kPanel; ++t) {
+        l[t] = A[R + q][k0 + t];
+        x[t] = I[k0 + t][j];
+      }
+#pragma unroll
+      for (int t = 0; t < kPanel; t += 2) {
+        a0 += l[t] * x[t];
+        a1 += l[t + 1] * x[t + 1];
+      }
+    }
+    I[R + q][j] = a0 + a1;
+  }
+  bar_sync<kBar, kThreads>();
+  for (int j = u; j < R; j += kThreads) {
+    T t[kPanel], o[kPanel];
+#pragma unroll
+    for (int r = 0; r < kPanel; ++r) t[r] = I[R + r][j];
+#pragma unroll
+    for (int q = 0; q < kPanel; ++q) {
+      T acc = T(0);
+#pragma unroll
+      for (int r = 0; r <= q; ++r) acc += I[R + q][R + r] * t[r];
+      o[q] = -acc;
+    }
+#pragma unroll
+    for (int q = 0; q < kPanel; ++q) I[R + q][j] = o[q];
+  }
+}
 
 // One 8-column panel of the diagonal block on the 64 threads of warps 0-1: every one of them
 // factors the 8 x 8 diagonal block (rows/cols k0..k0+7 of A) in registers with the same
-// arithmetic (no exchange on the pivot chain, the pivot rule without branches), and the thread
-// with a row below (row k0 + 8 + tid, already updated, in r) solves it against that factor and
-// stores it to A and, transposed, to Lw (Lw[c][i] = L[i][k0 + c]). Thread 0 stores the factored
-// 8 x 8 block and the pivot reciprocals.
-template <class T>
+// arithmetic (no exchange on the pivot chain, the pivot rule without branches); then (after
+// barrier 2, where warps 2-7 signal that the rows below are updated, if kWaitRows) the thread
+// with a row below (row k0 + 8 + tid) solves it against that factor and stores it to A and,
+// transposed, to Lw (Lw[c][i] = L[i][k0 + c]). Warps 0 and 1 store halves of the factored 8 x 8
+// block and the pivot reciprocals.
+template <bool kWaitRows, class T>
 __device__ __forceinline__ void factor_panel(T (*A)[kNB + 1], T (*Lw)[kNB], T* rinv, const double* dref, int k0,
-                                             int r0, int m, double drop_tol, T (&r)[kPanel], bool has_row,
-                                             int& drops, int& bad) {
+                                             int r0, int m, double drop_tol, int& drops, int& bad) {
   const int tid = threadIdx.x;
+  const bool has_row = tid < kNB - k0 - kPanel;
   T d[kPanel][kPanel], dinv[kPanel];
   double thr[kPanel];
 #pragma unroll
@@ -157,8 +235,12 @@ __device__ __forceinline__ void factor_panel(T (*A)[kNB + 1], T (*Lw)[kNB], T* r
 #pragma unroll
       for (int k = j + 1; k <= q; ++k) d[q][k] -= d[q][j] * d[k][j];
   }
+  if (kWaitRows) asm volatile("bar.sync 2, 256;" ::: "memory");
   if (has_row) {
     const int i = k0 + kPanel + tid;
+    T r[kPanel];
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) r[c] = A[i][k0 + c];
 #pragma unroll
     for (int c = 0; c < kPanel; ++c) {
       r[c] *= dinv[c];
@@ -173,7 +255,14 @@ __device__ __forceinline__ void factor_panel(T (*A)[kNB + 1], T (*Lw)[kNB], T* r
   }
   if (tid == 0) {
 #pragma unroll
-    for (int q = 0; q < kPanel; ++q) {
+    for (int q = 0; q < kPanel / 2; ++q) {
+      rinv[k0 + q] = dinv[q];
+#pragma unroll
+      for (int c = 0; c <= q; ++c) A[k0 + q][k0 + c] = d[q][c];
+    }
+  } else if (tid == 32) {
+#pragma unroll
+    for (int q = kPanel / 2; q < kPanel; ++q) {
       rinv[k0 + q] = dinv[q];
 #pragma unroll
       for (int c = 0; c <= q; ++c) A[k0 + q][k0 + c] = d[q][c];
@@ -204,10 +293,13 @@ __device__ __forceinline__ void potrf_load(const T* __restrict__ M, int ld, int 
 
 // Factor and invert the diagonal block held in A (the first 64 x 65 elements of `potrf_raw`,
 // lower triangle, upper entries zero); stores L to M and L^-1 to Linv. Runs on a CTA of 256
-// threads; `potrf_raw` is at least 2 * 64 * 65 elements of dynamic shared memory.
-// Panels with look-ahead: while warps 0-1 apply panel p's update to panel p+1's eight columns and
-// factor panel p+1, warps 2-7 apply panel p's update to the trailing triangle right of them, so
-// each panel costs one barrier and the longer of the two.
+// threads; `potrf_raw` is potrf_smem_bytes<T>() of dynamic shared memory.
+// Panels with look-ahead: while warps 0-1 apply panel p's update to panel p+1's diagonal block and
+// factor it, warps 2-7 apply panel p's update to the rows below it (handed over on a barrier the
+// row solves wait on) and then to the trailing triangle right of panel p+1, so each panel costs
+// one block-wide barrier and the longer of the two chains. Warps 2-7 then also compute row block p
+// of the inverse (rows of L up to panel p are final), so only the last row block follows the
+// panels.
 template <class T>
 __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __restrict__ diag, int m,
                            T* __restrict__ Linv, int* drop_count, int* fail, double drop_tol,
@@ -216,14 +308,14 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
   T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
   __shared__ T rinv[kNB];
   __shared__ double dref[kNB];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const int r0 = kb * kNB;
   if (tid < kNB) dref[tid] = r0 + tid < m ? fabs(diag[r0 + tid]) : 1.0;
   __syncthreads();
   int drops = 0, bad = 0;
   // two panels' columns below their diagonal blocks, transposed (Lt[c][i] = L[i][k0 + c]), so an
-  // update reads consecutive rows per vector load; alias I, which is unused until the inverse
-  T(*Lt0)[kNB] = reinterpret_cast<T(*)[kNB]>(&I[0][0]);
+  // update reads consecutive rows per vector load
+  T(*Lt0)[kNB] = reinterpret_cast<T(*)[kNB]>(potrf_raw + 2 * sizeof(T) * kNB * (kNB + 1));
   T(*Lt1)[kNB] = Lt0 + kPanel;
   // warps 2-7: 4 x 4 tile (ti, tj) of the trailing update, u = ti (ti + 1) / 2 + tj, the same for
   // every panel (a triangle of nt tile rows uses u below nt (nt + 1) / 2)
@@ -235,22 +327,14 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
     while ((ti + 1) * (ti + 2) / 2 <= u) ++ti;
     tj = u - ti * (ti + 1) / 2;
   }
-  if (tid < kNB) {
-    T r[kPanel];
-    const bool has_row = tid < kNB - kPanel;
-    if (has_row)
-#pragma unroll
-      for (int c = 0; c < kPanel; ++c) r[c] = A[kPanel + tid][c];
-    factor_panel<T>(A, Lt0, rinv, dref, 0, r0, m, drop_tol, r, has_row, drops, bad);
-  }
+  if (tid < kNB) factor_panel<false, T>(A, Lt0, rinv, dref, 0, r0, m, drop_tol, drops, bad);
   __syncthreads();
   for (int p = 0; p + 1 < kNB / kPanel; ++p) {
     const int K0 = (p + 1) * kPanel, K1 = K0 + kPanel;  // panel p+1's first column, and the next
     T(*Lc)[kNB] = (p & 1) ? Lt1 : Lt0;                 // panel p
     T(*Ln)[kNB] = (p & 1) ? Lt0 : Lt1;                 // panel p + 1
     if (tid < kNB) {
-      // panel p's update of panel p+1's columns: the 36 entries of its diagonal block (one per
-      // thread, shared through A) and each row below (in registers)
+      // panel p's update of panel p+1's diagonal block, one entry per thread, shared through A
       if (tid < kPanel * (kPanel + 1) / 2) {
         int q = 0;
         while ((q + 1) * (q + 2) / 2 <= tid) ++q;
@@ -260,24 +344,27 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
         for (int k = 0; k < kPanel; ++k) a -= Lc[k][K0 + q] * Lc[k][K0 + c];
         A[K0 + q][K0 + c] = a;
       }
-      const bool has_row = tid < kNB - K1;
-      T r[kPanel];
-      if (has_row) {
-        const int i = K1 + tid;
-        T li[kPanel];
+      asm volatile("bar.sync 1, 64;" ::: "memory");  // warps 0-1: the diagonal block is updated
+      factor_panel<true, T>(A, Ln, rinv, dref, K0, r0, m, drop_tol, drops, bad);
+    } else {
+      // panel p's update of panel p+1's columns below its diagonal block (two entries per
+      // thread), signalled to warps 0-1 on barrier 2 without waiting
+      {
+        const int i = K1 + (u >> 2), c0 = (u & 3) * 2;
+        if (i < kNB) {
+          T li[kPanel];
 #pragma unroll
-        for (int k = 0; k < kPanel; ++k) li[k] = Lc[k][i];
+          for (int k = 0; k < kPanel; ++k) li[k] = Lc[k][i];
 #pragma unroll
-        for (int c = 0; c < kPanel; ++c) {
-          T a = A[i][K0 + c];
+          for (int c = c0; c < c0 + 2; ++c) {
+            T a = A[i][K0 + c];
 #pragma unroll
-          for (int k = 0; k < kPanel; ++k) a -= li[k] * Lc[k][K0 + c];
-          r[c] = a;
+            for (int k = 0; k < kPanel; ++k) a -= li[k] * Lc[k][K0 + c];
+            A[i][K0 + c] = a;
+          }
         }
       }
-      asm volatile("bar.sync 1, 64;" ::: "memory");  // warps 0-1: the diagonal block is updated
-      factor_panel<T>(A, Ln, rinv, dref, K0, r0, m, drop_tol, r, has_row, drops, bad);
-    } else {
+      asm volatile("bar.arrive 2, 256;" ::: "memory");
       // panel p's update of the trailing triangle (rows and columns from K1)
       const int nt = (kNB - K1) / 4;
       if (ti < nt) {
@@ -303,80 +390,17 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
           for (int v = 0; v < 4; ++v)
             if (j0 + v <= i0 + q) A[i0 + q][j0 + v] = acc[q][v];
       }
+      inverse_row_block<192, 3, 88, 96, T>(A, I, rinv, p, u);
     }
     __syncthreads();
   }
-  // inverse of the 64 x 64 factor, blocked: the four 16 x 16 diagonal blocks by forward
-  // substitution (warp b, lane c = column c of block b, the column in registers), then the
-  // off-diagonal blocks in three stages by distance from the diagonal,
-  // X_ij = -X_ii (sum_{k=j}^{i-1} L_ik X_kj), each 16 x 16 block on 64 threads
-  {
-    constexpr int kB = 16;
-    if (warp < 4 && lane < kB) {
-      const int R = warp * kB, c = lane;
-      T x[kB];
-#pragma unroll
-      for (int r = 0; r < kB; ++r) {
-        if (r < c) {
-          x[r] = T(0);
-        } else if (r == c) {
-          x[r] = rinv[R + r];
-        } else {
-          T acc = T(0);
-#pragma unroll
-          for (int k = 0; k < kB; ++k)
-            if (k >= c && k < r) acc += A[R + r][R + k] * x[k];
-          x[r] = -acc * rinv[R + r];
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < kB; ++r) I[R + r][R + c] = x[r];
-    }
-    // zero the strictly upper blocks
-    for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
-      const int r = idx / kNB, c = idx % kNB;
-      if (r / kB < c / kB) I[r][c] = T(0);
-    }
-    __syncthreads();
-    const int g = tid >> 6, t = tid & 63, rr = t >> 2, c4 = (t & 3) * 4;
-    for (int dist = 1; dist < 4; ++dist) {
-      const int j = g, i = g + dist;
-      const bool act = i < 4;
-      T v[4] = {T(0), T(0), T(0), T(0)};
-      if (act) {
-        // T = sum_{k=j}^{i-1} L_ik X_kj  (rows of block i, columns of block j)
-        for (int k = j; k < i; ++k)
-#pragma unroll
-          for (int q = 0; q < kB; ++q) {
-            const T l = A[i * kB + rr][k * kB + q];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] += l * I[k * kB + q][j * kB + c4 + u];
-          }
-      }
-      __syncthreads();
-      if (act)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) I[i * kB + rr][j * kB + c4 + u] = v[u];
-      __syncthreads();
-      T w[4] = {T(0), T(0), T(0), T(0)};
-      if (act)
-#pragma unroll
-        for (int q = 0; q < kB; ++q) {
-          const T xi = I[i * kB + rr][i * kB + q];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) w[u] -= xi * I[i * kB + q][j * kB + c4 + u];
-        }
-      __syncthreads();
-      if (act)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) I[i * kB + rr][j * kB + c4 + u] = w[u];
-      __syncthreads();
-    }
-  }
+  // the inverse's last row block, on all threads
+  inverse_row_block<256, 0, 248, 0, T>(A, I, rinv, kNB / kPanel - 1, tid);
+  __syncthreads();
   for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
     const int cc = idx / kNB, r = idx % kNB;
     if (r >= cc) M[static_cast<int64_t>(r0 + cc) * ld + r0 + r] = A[r][cc];
-    Linv[static_cast<int64_t>(kb) * kNB * kNB + idx] = I[r][cc];
+    Linv[static_cast<int64_t>(kb) * kNB * kNB + idx] = r >= cc ? I[r][cc] : T(0);
   }
   if (tid == 0) {
     if (drops) atomicAdd(drop_count, drops);
@@ -561,7 +585,7 @@ __global__ void __launch_bounds__(256) k_panel_update(T* __restrict__ M, int ld,
 
 template <class T>
 void dense_potrf_block(const DenseSystem<T>& s, int kb, cudaStream_t st) {
-  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
+  const size_t smem_potrf = potrf_smem_bytes<T>();
   static bool attr_set = false;
   if (!attr_set) {
     SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
@@ -578,7 +602,7 @@ std::atomic<unsigned> g_factor_generation{0};
 
 template <class T>
 void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
-  const size_t smem_potrf = 2 * sizeof(T) * kNB * (kNB + 1);
+  const size_t smem_potrf = potrf_smem_bytes<T>();
   static bool attr_set = false;
   if (!attr_set) {
     SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
