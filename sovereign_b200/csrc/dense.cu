@@ -129,36 +129,38 @@ __device__ __forceinline__ void bar_sync() {
 }
 
 // Row block p (rows 8p..8p+7) of X = L^-1, into I, once L's rows 8p..8p+7 are final in A and the
-// earlier row blocks of X are in I: X_pp = L_pp^-1 by forward substitution (threads kX1..kX1+7,
-// one column each), T_pj = sum_{k=j}^{8p-1} L[8p+q][k] X[k][j] for every column j < 8p (threads
-// from kX2, one entry at a time, two partial sums), then X_pj = -X_pp T_pj (one column per
-// thread). kThreads threads from index u = 0, synchronised on barrier kBar.
-template <int kThreads, int kBar, int kX1, int kX2, class T>
-__device__ __forceinline__ void inverse_row_block(const T (*A)[kNB + 1], T (*I)[kNB + 1], const T* rinv, int p, int u) {
+// earlier row blocks of X are in I, in three steps:
+//   x1  X_pp = L_pp^-1, one column per thread (eight threads), by forward substitution;
+//   x2  T_pj = sum_{k=j}^{8p-1} L[8p+q][k] X[k][j] for every column j < 8p, one entry at a time
+//       from a shared counter, so threads join as they come free; T goes to X's place;
+//   x3  X_pj = -X_pp T_pj, one entry per thread, written after a barrier (in place of T).
+template <class T>
+__device__ __forceinline__ void inverse_x1(const T (*A)[kNB + 1], T (*I)[kNB + 1], const T* rinv, int p, int c) {
+  // L_pp x = e_c, right-looking with every index static (x starts as e_c, so the entries above c
+  // stay zero)
   const int R = p * kPanel;
-  if (u >= kX1 && u < kX1 + kPanel) {
-    // column c of X_pp: L_pp x = e_c, right-looking with every index static (x starts as e_c,
-    // so the entries above c stay zero)
-    const int c = u - kX1;
-    T l[kPanel * (kPanel + 1) / 2], ri[kPanel], x[kPanel];
+  T l[kPanel * (kPanel - 1) / 2], ri[kPanel], x[kPanel];
 #pragma unroll
-    for (int r = 0; r < kPanel; ++r) {
-      ri[r] = rinv[R + r];
-      x[r] = r == c ? T(1) : T(0);
+  for (int r = 0; r < kPanel; ++r) {
+    ri[r] = rinv[R + r];
+    x[r] = r == c ? T(1) : T(0);
 #pragma unroll
-      for (int k = 0; k < r; ++k) l[r * (r - 1) / 2 + k] = A[R + r][R + k];
-    }
-#pragma unroll
-    for (int k = 0; k < kPanel; ++k) {
-      x[k] *= ri[k];
-#pragma unroll
-      for (int r = k + 1; r < kPanel; ++r) x[r] -= l[r * (r - 1) / 2 + k] * x[k];
-    }
-#pragma unroll
-    for (int r = 0; r < kPanel; ++r) I[R + r][R + c] = x[r];
+    for (int k = 0; k < r; ++k) l[r * (r - 1) / 2 + k] = A[R + r][R + k];
   }
-  if (R == 0) return;
-  for (int e = u - kX2; e >= 0 && e < kPanel * R; e += kThreads - kX2) {
+#pragma unroll
+  for (int k = 0; k < kPanel; ++k) {
+    x[k] *= ri[k];
+#pragma unroll
+    for (int r = k + 1; r < kPanel; ++r) x[r] -= l[r * (r - 1) / 2 + k] * x[k];
+  }
+#pragma unroll
+  for (int r = 0; r < kPanel; ++r) I[R + r][R + c] = x[r];
+}
+
+template <class T>
+__device__ __forceinline__ void inverse_x2(const T (*A)[kNB + 1], T (*I)[kNB + 1], int p, int* next) {
+  const int R = p * kPanel;
+  for (int e = atomicAdd(next, 1); e < kPanel * R; e = atomicAdd(next, 1)) {
     const int q = e % kPanel, j = e / kPanel;
     // by 8-row blocks of X from j's own (X is lower triangular: rows above j in it are zero),
     // each block's 16 loads issued together
@@ -178,20 +180,30 @@ __device__ __forceinline__ void inverse_row_block(const T (*A)[kNB + 1], T (*I)[
     }
     I[R + q][j] = a0 + a1;
   }
-  bar_sync<kBar, kThreads>();
-  for (int j = u; j < R; j += kThreads) {
-    T t[kPanel], o[kPanel];
+}
+
+// kThreads threads from u = 0, on barrier kBar; every 8p * 8 <= 2 * kThreads
+template <int kThreads, int kBar, class T>
+__device__ __forceinline__ void inverse_x3(T (*I)[kNB + 1], int p, int u) {
+  const int R = p * kPanel;
+  T x[2];
 #pragma unroll
-    for (int r = 0; r < kPanel; ++r) t[r] = I[R + r][j];
-#pragma unroll
-    for (int q = 0; q < kPanel; ++q) {
+  for (int v = 0; v < 2; ++v) {
+    const int e = u + v * kThreads;
+    if (e < kPanel * R) {
+      const int q = e % kPanel, j = e / kPanel;
       T acc = T(0);
 #pragma unroll
-      for (int r = 0; r <= q; ++r) acc += I[R + q][R + r] * t[r];
-      o[q] = -acc;
+      for (int r = 0; r < kPanel; ++r)
+        if (r <= q) acc += I[R + q][R + r] * I[R + r][j];
+      x[v] = -acc;
     }
+  }
+  bar_sync<kBar, kThreads>();
 #pragma unroll
-    for (int q = 0; q < kPanel; ++q) I[R + q][j] = o[q];
+  for (int v = 0; v < 2; ++v) {
+    const int e = u + v * kThreads;
+    if (e < kPanel * R) I[R + e % kPanel][e / kPanel] = x[v];
   }
 }
 
@@ -308,9 +320,11 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
   T(*I)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(potrf_raw + sizeof(T) * kNB * (kNB + 1));
   __shared__ T rinv[kNB];
   __shared__ double dref[kNB];
+  __shared__ int x2_next[kNB / kPanel];  // per row block of the inverse: next entry of its x2 step
   const int tid = threadIdx.x;
   const int r0 = kb * kNB;
   if (tid < kNB) dref[tid] = r0 + tid < m ? fabs(diag[r0 + tid]) : 1.0;
+  if (tid < kNB / kPanel) x2_next[tid] = 0;
   __syncthreads();
   int drops = 0, bad = 0;
   // two panels' columns below their diagonal blocks, transposed (Lt[c][i] = L[i][k0 + c]), so an
@@ -365,6 +379,8 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
         }
       }
       asm volatile("bar.arrive 2, 256;" ::: "memory");
+      // row block p of the inverse: x1 on threads that have no tiles, x2 shared by all
+      if (u >= 88 && u < 88 + kPanel) inverse_x1<T>(A, I, rinv, p, u - 88);
       // panel p's update of the trailing triangle (rows and columns from K1)
       const int nt = (kNB - K1) / 4;
       if (ti < nt) {
@@ -390,15 +406,24 @@ __device__ void potrf_core(T* __restrict__ M, int ld, int kb, const double* __re
           for (int v = 0; v < 4; ++v)
             if (j0 + v <= i0 + q) A[i0 + q][j0 + v] = acc[q][v];
       }
-      inverse_row_block<192, 3, 88, 96, T>(A, I, rinv, p, u);
+      inverse_x2<T>(A, I, p, &x2_next[p]);
+      if (p > 0) {
+        bar_sync<3, 192>();
+        inverse_x3<192, 3, T>(I, p, u);
+      }
     }
     __syncthreads();
   }
   // the inverse's last row block, on all threads
-  inverse_row_block<256, 0, 248, 0, T>(A, I, rinv, kNB / kPanel - 1, tid);
+  constexpr int kLast = kNB / kPanel - 1;
+  if (tid >= 256 - kPanel) inverse_x1<T>(A, I, rinv, kLast, tid - (256 - kPanel));
+  inverse_x2<T>(A, I, kLast, &x2_next[kLast]);
   __syncthreads();
-  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
-    const int cc = idx / kNB, r = idx % kNB;
+  inverse_x3<256, 0, T>(I, kLast, tid);
+  __syncthreads();
+#pragma unroll 8
+  for (int v = 0; v < kNB * kNB / 256; ++v) {
+    const int idx = tid + 256 * v, cc = idx / kNB, r = idx % kNB;
     if (r >= cc) M[static_cast<int64_t>(r0 + cc) * ld + r0 + r] = A[r][cc];
     Linv[static_cast<int64_t>(kb) * kNB * kNB + idx] = r >= cc ? I[r][cc] : T(0);
   }
