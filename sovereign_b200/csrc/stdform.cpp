@@ -386,37 +386,82 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
 
 namespace {
 
+// Indices 0..n-1 in key order, equal keys in index order: an LSD radix sort (11-bit digits) over
+// the key's significant bits, carrying the keys along. Keys are non-negative.
+std::vector<uint32_t> stable_key_order(const std::vector<int64_t>& key) {
+  const std::size_t n = key.size();
+  constexpr int kDigit = 11;
+  constexpr std::size_t kBuckets = std::size_t(1) << kDigit;
+  std::vector<uint32_t> ia(n), ib(n);
+  std::vector<uint64_t> ka(n), kb(n);
+  uint64_t mx = 0;
+  for (std::size_t i = 0; i < n; ++i) {
+    ia[i] = static_cast<uint32_t>(i);
+    ka[i] = static_cast<uint64_t>(key[i]);
+    mx = std::max(mx, ka[i]);
+  }
+  int bits = 0;
+  while (bits < 64 && (mx >> bits) != 0) ++bits;
+  std::vector<std::size_t> cnt(kBuckets);
+  for (int sh = 0; sh < bits; sh += kDigit) {
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (std::size_t i = 0; i < n; ++i) ++cnt[(ka[i] >> sh) & (kBuckets - 1)];
+    std::size_t run = 0;
+    for (std::size_t d = 0; d < kBuckets; ++d) {
+      const std::size_t c = cnt[d];
+      cnt[d] = run;
+      run += c;
+    }
+    for (std::size_t i = 0; i < n; ++i) {
+      const std::size_t at = cnt[(ka[i] >> sh) & (kBuckets - 1)]++;
+      ib[at] = ia[i];
+      kb[at] = ka[i];
+    }
+    ia.swap(ib);
+    ka.swap(kb);
+  }
+  return ia;
+}
+
 template <class Index>
 AssemblyMap build_assembly(const StdForm& f, Index index) {
-  // contributions (target, column, weight) for every pair p >= q of a column's entries
-  struct Contrib {
-    int64_t t;
-    int col;
-    double w;
-  };
-  std::vector<Contrib> cs;
+  // contributions (target, column, weight) for every pair p >= q of a column's entries, grouped
+  // by target in generation order (column, then entry pair): the gather sums in that order
   std::size_t total = 0;
   for (int j = 0; j < f.n; ++j) {
     const std::size_t k = static_cast<std::size_t>(f.col_ptr[j + 1] - f.col_ptr[j]);
     total += k * (k + 1) / 2;
   }
-  cs.reserve(total + f.m);
+  std::vector<int64_t> ct;
+  std::vector<int> cc;
+  std::vector<double> cw;
+  ct.reserve(total);
+  cc.reserve(total);
+  cw.reserve(total);
   for (int j = 0; j < f.n; ++j)
     for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p)
-      for (int q = f.col_ptr[j]; q <= p; ++q)
-        cs.push_back({index(f.row_idx[p], f.row_idx[q]), j, f.val[p] * f.val[q]});
-  std::stable_sort(cs.begin(), cs.end(), [](const Contrib& a, const Contrib& b) { return a.t < b.t; });
+      for (int q = f.col_ptr[j]; q <= p; ++q) {
+        ct.push_back(index(f.row_idx[p], f.row_idx[q]));
+        cc.push_back(j);
+        cw.push_back(f.val[p] * f.val[q]);
+      }
+  const std::vector<uint32_t> order = stable_key_order(ct);
   AssemblyMap am;
+  am.ptr.reserve(total + 1);
+  am.target.reserve(total);
+  am.col.resize(total);
+  am.w.resize(total);
   am.ptr.push_back(0);
-  for (std::size_t k = 0; k < cs.size(); ++k) {
-    if (am.target.empty() || am.target.back() != cs[k].t) {
+  for (std::size_t k = 0; k < total; ++k) {
+    const uint32_t o = order[k];
+    if (am.target.empty() || am.target.back() != ct[o]) {
       if (!am.target.empty()) am.ptr.push_back(static_cast<int>(k));
-      am.target.push_back(cs[k].t);
+      am.target.push_back(ct[o]);
     }
-    am.col.push_back(cs[k].col);
-    am.w.push_back(cs[k].w);
+    am.col[k] = cc[o];
+    am.w[k] = cw[o];
   }
-  am.ptr.push_back(static_cast<int>(cs.size()));
+  am.ptr.push_back(static_cast<int>(total));
   if (am.target.empty()) am.ptr.assign(1, 0);
   // every diagonal entry gets a target (rows with no entries still carry the 1e-12 shift)
   am.diag_target.assign(f.m, -1);
@@ -462,8 +507,94 @@ AssemblyMap build_assembly(const StdForm& f, Index index) {
 
 }  // namespace
 
+// Column-major targets t = c * ld + r (r >= c) come out in order without a global sort: for each
+// row c of A (its row-wise copy), the columns j holding it in ascending order, and each entry of j
+// at a row r >= c, contribute a_rj a_cj to (r, c). Appending each to a per-row list keeps every
+// target's contributions in ascending j, the order the generic builder produces (one entry pair
+// per column and target), so the gather sums identically; only the group's distinct rows are sorted.
 AssemblyMap build_assembly_dense(const StdForm& f, int ld) {
-  return build_assembly(f, [ld](int r, int c) { return static_cast<int64_t>(c) * ld + r; });
+  // needs strictly increasing rows in every column (as build_std_form leaves them); other input
+  // goes through the generic builder
+  for (int j = 0; j < f.n; ++j)
+    for (int p = f.col_ptr[j] + 1; p < f.col_ptr[j + 1]; ++p)
+      if (f.row_idx[p] <= f.row_idx[p - 1])
+        return build_assembly(f, [ld](int r, int c) { return static_cast<int64_t>(c) * ld + r; });
+  // the row-wise copy, when the form carries none
+  std::vector<int> own_ptr, own_idx, fill;
+  std::vector<double> own_val;
+  const int* row_ptr = f.row_ptr.data();
+  const int* col_idx = f.col_idx.data();
+  const double* rval = f.rval.data();
+  if (static_cast<int>(f.row_ptr.size()) != f.m + 1) {
+    own_ptr.resize(f.m + 1);
+    own_idx.resize(f.col_ptr[f.n]);
+    own_val.resize(f.col_ptr[f.n]);
+    csr_from_csc(f.m, f.n, f.col_ptr.data(), f.row_idx.data(), f.val.data(), own_ptr.data(), own_idx.data(),
+                 own_val.data(), fill);
+    row_ptr = own_ptr.data();
+    col_idx = own_idx.data();
+    rval = own_val.data();
+  }
+  AssemblyMap am;
+  std::size_t total = 0;
+  for (int j = 0; j < f.n; ++j) {
+    const std::size_t k = static_cast<std::size_t>(f.col_ptr[j + 1] - f.col_ptr[j]);
+    total += k * (k + 1) / 2;
+  }
+  am.col.resize(total);
+  am.w.resize(total);
+  am.target.reserve(total + f.m);
+  am.ptr.reserve(total + f.m + 1);
+  am.ptr.push_back(0);
+  am.diag_target.assign(f.m, -1);
+  std::vector<int> head(f.m, -1), tail(f.m, -1), rows;
+  std::vector<int> next, gcol;
+  std::vector<double> gw;
+  std::size_t out = 0;
+  for (int c = 0; c < f.m; ++c) {
+    rows.clear();
+    next.clear();
+    gcol.clear();
+    gw.clear();
+    for (int pp = row_ptr[c]; pp < row_ptr[c + 1]; ++pp) {
+      const int j = col_idx[pp];
+      const double vc = rval[pp];
+      for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p) {
+        const int r = f.row_idx[p];
+        if (r < c) continue;
+        const int k = static_cast<int>(gcol.size());
+        gcol.push_back(j);
+        gw.push_back(f.val[p] * vc);
+        next.push_back(-1);
+        if (head[r] < 0) {
+          head[r] = k;
+          rows.push_back(r);
+        } else {
+          next[tail[r]] = k;
+        }
+        tail[r] = k;
+      }
+    }
+    std::sort(rows.begin(), rows.end());
+    const int64_t base = static_cast<int64_t>(c) * ld;
+    if (rows.empty() || rows.front() != c) {  // every diagonal entry gets a target (the 1e-12 shift)
+      am.diag_target[c] = static_cast<int>(am.target.size());
+      am.target.push_back(base + c);
+      am.ptr.push_back(static_cast<int>(out));
+    }
+    for (const int r : rows) {
+      if (r == c) am.diag_target[c] = static_cast<int>(am.target.size());
+      am.target.push_back(base + r);
+      for (int k = head[r]; k >= 0; k = next[k]) {
+        am.col[out] = gcol[k];
+        am.w[out] = gw[k];
+        ++out;
+      }
+      am.ptr.push_back(static_cast<int>(out));
+      head[r] = -1;
+    }
+  }
+  return am;
 }
 
 AssemblyMap build_assembly_rowmajor(const StdForm& f, int ld) {
