@@ -6,6 +6,7 @@
 #include <limits>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 #include <utility>
 
 namespace sov {
@@ -535,64 +536,105 @@ AssemblyMap build_assembly_dense(const StdForm& f, int ld) {
     col_idx = own_idx.data();
     rval = own_val.data();
   }
-  AssemblyMap am;
   std::size_t total = 0;
   for (int j = 0; j < f.n; ++j) {
     const std::size_t k = static_cast<std::size_t>(f.col_ptr[j + 1] - f.col_ptr[j]);
     total += k * (k + 1) / 2;
   }
-  am.col.resize(total);
-  am.w.resize(total);
-  am.target.reserve(total + f.m);
-  am.ptr.reserve(total + f.m + 1);
+  // rows c of A in contiguous ranges, one per thread, balanced by the entries each row's columns
+  // hold; each range builds its own piece, the pieces are concatenated in row order
+  struct Piece {
+    std::vector<int64_t> target;
+    std::vector<int> end;  // end of each target's contributions within the piece
+    std::vector<int> col;
+    std::vector<double> w;
+    std::vector<std::pair<int, int>> diag;  // (row, target index within the piece)
+  };
+  auto build_rows = [&](int c0, int c1, Piece& pc) {
+    std::vector<int> head(f.m, -1), tail(f.m, -1), rows, next, gcol;
+    std::vector<double> gw;
+    for (int c = c0; c < c1; ++c) {
+      rows.clear();
+      next.clear();
+      gcol.clear();
+      gw.clear();
+      for (int pp = row_ptr[c]; pp < row_ptr[c + 1]; ++pp) {
+        const int j = col_idx[pp];
+        const double vc = rval[pp];
+        for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p) {
+          const int r = f.row_idx[p];
+          if (r < c) continue;
+          const int k = static_cast<int>(gcol.size());
+          gcol.push_back(j);
+          gw.push_back(f.val[p] * vc);
+          next.push_back(-1);
+          if (head[r] < 0) {
+            head[r] = k;
+            rows.push_back(r);
+          } else {
+            next[tail[r]] = k;
+          }
+          tail[r] = k;
+        }
+      }
+      std::sort(rows.begin(), rows.end());
+      const int64_t base = static_cast<int64_t>(c) * ld;
+      if (rows.empty() || rows.front() != c) {  // every diagonal entry gets a target (the 1e-12 shift)
+        pc.diag.push_back({c, static_cast<int>(pc.target.size())});
+        pc.target.push_back(base + c);
+        pc.end.push_back(static_cast<int>(pc.col.size()));
+      }
+      for (const int r : rows) {
+        if (r == c) pc.diag.push_back({c, static_cast<int>(pc.target.size())});
+        pc.target.push_back(base + r);
+        for (int k = head[r]; k >= 0; k = next[k]) {
+          pc.col.push_back(gcol[k]);
+          pc.w.push_back(gw[k]);
+        }
+        pc.end.push_back(static_cast<int>(pc.col.size()));
+        head[r] = -1;
+      }
+    }
+  };
+  int nthreads = 1;
+  if (total >= 100000) nthreads = static_cast<int>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())));
+  std::vector<int> cut(nthreads + 1, f.m);
+  cut[0] = 0;
+  if (nthreads > 1) {
+    std::vector<std::size_t> work(f.m + 1, 0);
+    for (int c = 0; c < f.m; ++c) {
+      std::size_t wc = 1;
+      for (int pp = row_ptr[c]; pp < row_ptr[c + 1]; ++pp) wc += f.col_ptr[col_idx[pp] + 1] - f.col_ptr[col_idx[pp]];
+      work[c + 1] = work[c] + wc;
+    }
+    for (int t = 1; t < nthreads; ++t)
+      cut[t] = static_cast<int>(std::lower_bound(work.begin(), work.end(), work[f.m] * t / nthreads) - work.begin());
+    for (int t = 1; t <= nthreads; ++t) cut[t] = std::max(cut[t], cut[t - 1]);
+  }
+  std::vector<Piece> pieces(nthreads);
+  if (nthreads == 1) {
+    build_rows(0, f.m, pieces[0]);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t) pool.emplace_back(build_rows, cut[t], cut[t + 1], std::ref(pieces[t]));
+    for (std::thread& th : pool) th.join();
+  }
+  AssemblyMap am;
+  std::size_t ntargets = 0;
+  for (const Piece& pc : pieces) ntargets += pc.target.size();
+  am.target.reserve(ntargets);
+  am.ptr.reserve(ntargets + 1);
+  am.col.reserve(total);
+  am.w.reserve(total);
   am.ptr.push_back(0);
   am.diag_target.assign(f.m, -1);
-  std::vector<int> head(f.m, -1), tail(f.m, -1), rows;
-  std::vector<int> next, gcol;
-  std::vector<double> gw;
-  std::size_t out = 0;
-  for (int c = 0; c < f.m; ++c) {
-    rows.clear();
-    next.clear();
-    gcol.clear();
-    gw.clear();
-    for (int pp = row_ptr[c]; pp < row_ptr[c + 1]; ++pp) {
-      const int j = col_idx[pp];
-      const double vc = rval[pp];
-      for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p) {
-        const int r = f.row_idx[p];
-        if (r < c) continue;
-        const int k = static_cast<int>(gcol.size());
-        gcol.push_back(j);
-        gw.push_back(f.val[p] * vc);
-        next.push_back(-1);
-        if (head[r] < 0) {
-          head[r] = k;
-          rows.push_back(r);
-        } else {
-          next[tail[r]] = k;
-        }
-        tail[r] = k;
-      }
-    }
-    std::sort(rows.begin(), rows.end());
-    const int64_t base = static_cast<int64_t>(c) * ld;
-    if (rows.empty() || rows.front() != c) {  // every diagonal entry gets a target (the 1e-12 shift)
-      am.diag_target[c] = static_cast<int>(am.target.size());
-      am.target.push_back(base + c);
-      am.ptr.push_back(static_cast<int>(out));
-    }
-    for (const int r : rows) {
-      if (r == c) am.diag_target[c] = static_cast<int>(am.target.size());
-      am.target.push_back(base + r);
-      for (int k = head[r]; k >= 0; k = next[k]) {
-        am.col[out] = gcol[k];
-        am.w[out] = gw[k];
-        ++out;
-      }
-      am.ptr.push_back(static_cast<int>(out));
-      head[r] = -1;
-    }
+  for (const Piece& pc : pieces) {
+    const int t0 = static_cast<int>(am.target.size()), k0 = static_cast<int>(am.col.size());
+    am.target.insert(am.target.end(), pc.target.begin(), pc.target.end());
+    for (const int e : pc.end) am.ptr.push_back(k0 + e);
+    am.col.insert(am.col.end(), pc.col.begin(), pc.col.end());
+    am.w.insert(am.w.end(), pc.w.begin(), pc.w.end());
+    for (const auto& d : pc.diag) am.diag_target[d.first] = t0 + d.second;
   }
   return am;
 }
