@@ -658,14 +658,31 @@ void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
 // ---------------------------------------------------------------------------------------------
 // Dataflow triangular solves
 // ---------------------------------------------------------------------------------------------
+constexpr int kSolveBatch = 8;  // dependencies a triangular-solve block takes per flag check
+
+// Warp 0: how many consecutive flags first, first + step, ... (at most n <= 32) are released,
+// waiting (bounded) until the first one is; 0 when the wait gives up.
+__device__ __forceinline__ int released_run(const unsigned* flags, int first, int step, int n, unsigned epoch) {
+  const int lane = threadIdx.x & 31;
+  long long spins = 0;
+  for (;;) {
+    const bool ready = lane < n && ld_acquire(flags + first + step * lane) == epoch;
+    const unsigned mask = __ballot_sync(kFull, ready);
+    const int run = __ffs(~mask) - 1;
+    if (run > 0) return run;
+    if (++spins > kSpinLimit) return 0;
+    __nanosleep(64);
+  }
+}
+
 // Forward: L y = r, row block order. z holds r on entry and y on exit.
 template <class T>
 __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int ld, const T* __restrict__ Linv, int nb,
                                                   double* z, unsigned* flags, unsigned epoch, int* err) {
   __shared__ double part[4][kNB];
-  __shared__ double yj[kNB];
+  __shared__ double ys[kSolveBatch][kNB];
   __shared__ double rhs[kNB];
-  __shared__ int ok;
+  __shared__ int s_run;
   const int t = threadIdx.x, r = t & (kNB - 1), g = t >> 6;
   for (int i = blockIdx.x; i < nb; i += gridDim.x) {
     // this thread's 16 entries of Linv_ii and of L_{i,i-1} (the last dependency), loaded before any
@@ -680,24 +697,48 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int l
       for (int u = 0; u < 16; ++u) lp[u] = static_cast<double>(Lp[static_cast<int64_t>(g * 16 + u) * ld]);
     }
     double acc = 0.0;
-    for (int j = 0; j < i; ++j) {
-      if (t == 0) ok = wait_flag(flags + j, epoch);
-      __syncthreads();
-      if (!ok) {
-        if (t == 0) atomicExch(err, 1);
+    bool bad = false;
+    // blocks 0 .. i-2 in runs of released ones (one flag check per run, not per block)
+    for (int done = 0; done < i - 1;) {
+      if (t < 32) {
+        const int run = released_run(flags, done, 1, min(kSolveBatch, i - 1 - done), epoch);
+        if (t == 0) s_run = run;
       }
-      if (t < kNB) yj[t] = __ldcg(z + j * kNB + t);
       __syncthreads();
-      if (j == i - 1) {
+      const int run = s_run;
+      if (run == 0) {
+        bad = true;
+        break;
+      }
+      for (int idx = t; idx < run * kNB; idx += blockDim.x)
+        ys[idx / kNB][idx % kNB] = __ldcg(z + (done + idx / kNB) * kNB + idx % kNB);
+      __syncthreads();
+#pragma unroll 2
+      for (int b = 0; b < run; ++b) {
+        const T* Lij = M + static_cast<int64_t>((done + b) * kNB) * ld + i * kNB + r;
 #pragma unroll
-        for (int u = 0; u < 16; ++u) acc += lp[u] * yj[g * 16 + u];
-      } else {
-        const T* Lij = M + static_cast<int64_t>(j * kNB) * ld + i * kNB + r;
-#pragma unroll 4
-        for (int c = g * 16; c < g * 16 + 16; ++c) acc += static_cast<double>(Lij[static_cast<int64_t>(c) * ld]) * yj[c];
+        for (int u = 0; u < 16; ++u)
+          acc += static_cast<double>(Lij[static_cast<int64_t>(g * 16 + u) * ld]) * ys[b][g * 16 + u];
       }
       __syncthreads();
+      done += run;
     }
+    if (i > 0 && !bad) {
+      if (t < 32) {
+        const int run = released_run(flags, i - 1, 1, 1, epoch);
+        if (t == 0) s_run = run;
+      }
+      __syncthreads();
+      if (s_run == 0) {
+        bad = true;
+      } else {
+        if (t < kNB) ys[0][t] = __ldcg(z + (i - 1) * kNB + t);
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc += lp[u] * ys[0][g * 16 + u];
+      }
+    }
+    if (bad && t == 0) atomicExch(err, 1);
     part[g][r] = acc;
     __syncthreads();
     if (t < kNB) rhs[t] = z[i * kNB + t] - (part[0][t] + part[1][t] + part[2][t] + part[3][t]);
@@ -718,10 +759,10 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int l
 template <class T>
 __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int ld, const T* __restrict__ Linv, int nb,
                                                   double* z, unsigned* flags, unsigned epoch, int* err) {
-  __shared__ double xj[kNB];
+  __shared__ double xs[kSolveBatch][kNB];
   __shared__ double acc_s[kNB];
   __shared__ double rhs[kNB];
-  __shared__ int ok;
+  __shared__ int s_run;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   for (int q = blockIdx.x; q < nb; q += gridDim.x) {
     const int i = nb - 1 - q;
@@ -740,26 +781,53 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
       }
     }
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int j = nb - 1; j > i; --j) {
-      if (t == 0) ok = wait_flag(flags + j, epoch);
+    bool bad = false;
+    // blocks nb-1 down to i+2 in runs of released ones
+    const int deps = nb - i - 2;
+    for (int done = 0; done < deps;) {
+      const int j0 = nb - 1 - done;
+      if (t < 32) {
+        const int run = released_run(flags, j0, -1, min(kSolveBatch, deps - done), epoch);
+        if (t == 0) s_run = run;
+      }
       __syncthreads();
-      if (!ok && t == 0) atomicExch(err, 1);
-      if (t < kNB) xj[t] = __ldcg(z + j * kNB + t);
+      const int run = s_run;
+      if (run == 0) {
+        bad = true;
+        break;
+      }
+      for (int idx = t; idx < run * kNB; idx += blockDim.x)
+        xs[idx / kNB][idx % kNB] = __ldcg(z + (j0 - idx / kNB) * kNB + idx % kNB);
       __syncthreads();
       // acc_c += sum_r L[j*64 + r][i*64 + c] * x_j[r]
-      if (j == i + 1) {
-#pragma unroll
-        for (int u = 0; u < 8; ++u) acc[u] += lp[u][0] * xj[lane] + lp[u][1] * xj[lane + 32];
-      } else {
+#pragma unroll 2
+      for (int b = 0; b < run; ++b) {
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int c = w * 8 + u;
-          const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + j * kNB;
-          acc[u] += static_cast<double>(col[lane]) * xj[lane] + static_cast<double>(col[lane + 32]) * xj[lane + 32];
+          const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + (j0 - b) * kNB;
+          acc[u] += static_cast<double>(col[lane]) * xs[b][lane] + static_cast<double>(col[lane + 32]) * xs[b][lane + 32];
         }
       }
       __syncthreads();
+      done += run;
     }
+    if (i + 1 < nb && !bad) {
+      if (t < 32) {
+        const int run = released_run(flags, i + 1, 1, 1, epoch);
+        if (t == 0) s_run = run;
+      }
+      __syncthreads();
+      if (s_run == 0) {
+        bad = true;
+      } else {
+        if (t < kNB) xs[0][t] = __ldcg(z + (i + 1) * kNB + t);
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc[u] += lp[u][0] * xs[0][lane] + lp[u][1] * xs[0][lane + 32];
+      }
+    }
+    if (bad && t == 0) atomicExch(err, 1);
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const double v = warp_sum(acc[u]);
