@@ -11,6 +11,7 @@
 // bucket launches of a batch run concurrently on forked streams, captured once in a CUDA graph.
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -228,18 +229,9 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         for (int k = k0; k < k1; ++k) {
           const double p = M[tri(k) + k];
           const double dref = vdiag[k];
-          double Dk, code;
-          if (!isfinite(p)) {
-            Dk = 1e128;
-            code = 2.0;
-          } else if (p <= 1e-13 * fabs(dref)) {
-            Dk = 1e128;  // dependent row (sparse_ldlt.cpp:167-173)
-            code = 1.0;
-          } else {
-            Dk = p;
-            code = 0.0;
-          }
-          const double inv = 1.0 / Dk;
+          // 2: not finite, 1: dependent row (sparse_ldlt.cpp:167-173), 0: kept; no branches
+          const double code = !(fabs(p) <= DBL_MAX) ? 2.0 : (p <= 1e-13 * fabs(dref) ? 1.0 : 0.0);
+          const double inv = 1.0 / (code != 0.0 ? 1e128 : p);
           const int i = k + 1 + lane;
           if (i < k1) {
             const double lik = M[tri(i) + k] * inv;
