@@ -9,14 +9,18 @@
 // the working set of the resident CTAs fits in the 126 MB L2. Size buckets (by m) get their own
 // launch with a shared-memory footprint and thread count chosen per bucket by the autotuner; the
 // bucket launches of a batch run concurrently on forked streams, captured once in a CUDA graph.
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -932,28 +936,90 @@ std::map<int, int> g_tuned_threads;  // bucket mmax -> threads
 
 int bucket_of(int m) { return std::max(32, ((m + 31) / 32) * 32); }
 
+// Host worker threads, started once and kept for the life of the process (never destroyed: they
+// wait on a condition variable when idle): the batch builds and publishes run several parallel
+// loops per call, and starting threads for each of them cost milliseconds per call. One loop at a
+// time uses the pool; a loop that finds it busy (another host thread's batch), or runs in a forked
+// child (which has none of the parent's threads), runs on its own thread instead.
+class WorkerPool {
+ public:
+  static WorkerPool& get() {
+    static WorkerPool* pool = new WorkerPool;
+    return *pool;
+  }
+  int width() const { return static_cast<int>(threads_.size()) + 1; }
+  // fn(i) for i in [0, count) on the workers and the calling thread; false when the pool is busy
+  bool run(int count, const std::function<void(int)>& fn) {
+    if (getpid() != owner_) return false;
+    std::unique_lock<std::mutex> job(busy_, std::try_to_lock);
+    if (!job.owns_lock()) return false;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &fn;
+      count_ = count;
+      next_.store(0);
+      error_.clear();
+      active_ = static_cast<int>(threads_.size());
+      ++generation_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [&] { return active_ == 0; });
+    fn_ = nullptr;
+    if (!error_.empty()) throw std::runtime_error(error_);
+    return true;
+  }
+
+ private:
+  WorkerPool() : owner_(getpid()) {
+    const int nt = std::max(1, std::min<int>(16, static_cast<int>(std::thread::hardware_concurrency())));
+    for (int w = 1; w < nt; ++w) threads_.emplace_back([this] { loop(); });
+  }
+  void work() {
+    for (int i = next_.fetch_add(1); i < count_; i = next_.fetch_add(1)) {
+      try {
+        (*fn_)(i);
+      } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lk(err_mu_);
+        if (error_.empty()) error_ = e.what();
+        next_.store(count_);
+      }
+    }
+  }
+  void loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return generation_ != seen; });
+        seen = generation_;
+      }
+      work();
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--active_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex busy_, mu_, err_mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)>* fn_ = nullptr;
+  int count_ = 0, active_ = 0;
+  std::atomic<int> next_{0};
+  unsigned long long generation_ = 0;
+  std::string error_;
+  const pid_t owner_;
+};
+
 template <class F>
 void parallel_for(int count, F fn) {
-  const int nt = std::max(1, std::min<int>(16, static_cast<int>(std::thread::hardware_concurrency())));
-  if (count < 64 || nt == 1) {
+  if (count < 64) {
     for (int i = 0; i < count; ++i) fn(i);
     return;
   }
-  std::atomic<int> next{0};
-  std::vector<std::thread> pool;
-  std::vector<std::string> errors(nt);
-  for (int w = 0; w < nt; ++w)
-    pool.emplace_back([&, w]() {
-      try {
-        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) fn(i);
-      } catch (const std::exception& e) {
-        errors[w] = e.what();
-        next.store(count);
-      }
-    });
-  for (auto& t : pool) t.join();
-  for (auto& e : errors)
-    if (!e.empty()) throw std::runtime_error(e);
+  const std::function<void(int)> f = fn;
+  if (WorkerPool::get().width() > 1 && WorkerPool::get().run(count, f)) return;
+  for (int i = 0; i < count; ++i) fn(i);
 }
 
 }  // namespace
@@ -1298,7 +1364,8 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   return B.release();
 }
 
-void batch_solve(Batch* B, cudaStream_t st) {
+// The batch's graph launched on `st` between two timing events; batch_finish waits for it.
+void batch_launch(Batch* B, cudaStream_t st) {
   // Buckets run concurrently: each on its own stream forked from (and joined back into) one
   // capture stream, so the few large LPs do not hold the SMs the smaller buckets could use. The
   // fork / reset / launch / join sequence is captured once into a CUDA graph and replayed on the
@@ -1340,11 +1407,19 @@ void batch_solve(Batch* B, cudaStream_t st) {
   SOV_CUDA(cudaEventRecord(B->t0, st));
   SOV_CUDA(cudaGraphLaunch(B->graph, st));
   SOV_CUDA(cudaEventRecord(B->t1, st));
+}
+
+void batch_finish(Batch* B) {
   SOV_CUDA(cudaEventSynchronize(B->t1));
   float ms = 0.f;
   SOV_CUDA(cudaEventElapsedTime(&ms, B->t0, B->t1));
   B->launches = static_cast<int>(B->buckets.size());
   B->kernel_ms = ms;
+}
+
+void batch_solve(Batch* B, cudaStream_t st) {
+  batch_launch(B, st);
+  batch_finish(B);
 }
 
 void batch_results(Batch* B, sov_result* results) {
@@ -1474,17 +1549,39 @@ void batch_destroy(Batch* B) { delete B; }
 
 int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results) {
   if (count == 0) return SOV_OK;
-  std::unique_ptr<Batch> B(batch_create(count, models, opt, opt_stride));
-  cudaStream_t st;
-  SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  // Large batches in parts, pipelined: each part's graph is launched as soon as its inputs are on
+  // the device, so the host standard form and the copies of the next part overlap the solves of the
+  // ones before; the results are read back in order once all parts are launched. A part's LPs are
+  // solved exactly as in one batch (per-LP work, bucket widths by m).
+  const int parts = count >= 2048 ? 4 : 1;
+  std::vector<std::unique_ptr<Batch>> batches;
+  std::vector<cudaStream_t> streams;
+  auto part_lo = [&](int k) { return static_cast<int>(static_cast<long long>(count) * k / parts); };
   try {
-    batch_solve(B.get(), st);
+    for (int k = 0; k < parts; ++k) {
+      const int lo = part_lo(k), hi = part_lo(k + 1);
+      const sov_options* o = (opt && opt_stride > 0)
+                                 ? reinterpret_cast<const sov_options*>(reinterpret_cast<const char*>(opt) +
+                                                                        static_cast<size_t>(lo) * opt_stride)
+                                 : opt;
+      batches.emplace_back(batch_create(hi - lo, models + lo, o, opt_stride));
+      cudaStream_t st;
+      SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      streams.push_back(st);
+      batch_launch(batches.back().get(), st);
+    }
+    for (int k = 0; k < parts; ++k) {
+      batch_finish(batches[k].get());
+      batch_results(batches[k].get(), results + part_lo(k));
+    }
   } catch (...) {
-    cudaStreamDestroy(st);
+    for (cudaStream_t st : streams) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
     throw;
   }
-  cudaStreamDestroy(st);
-  batch_results(B.get(), results);
+  for (cudaStream_t st : streams) SOV_CUDA(cudaStreamDestroy(st));
   return SOV_OK;
 }
 
