@@ -48,6 +48,25 @@ __device__ __forceinline__ void load4(const float* p, float v[4]) {
   v[2] = a.z;
   v[3] = a.w;
 }
+// sixteen consecutive elements from 16-byte-aligned global memory, widened to double
+__device__ __forceinline__ void load16(const double* p, double v[16]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const double2 a = reinterpret_cast<const double2*>(p)[k];
+    v[2 * k] = a.x;
+    v[2 * k + 1] = a.y;
+  }
+}
+__device__ __forceinline__ void load16(const float* p, double v[16]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float4 a = reinterpret_cast<const float4*>(p)[k];
+    v[4 * k] = a.x;
+    v[4 * k + 1] = a.y;
+    v[4 * k + 2] = a.z;
+    v[4 * k + 3] = a.w;
+  }
+}
 
 __device__ __forceinline__ double column_weight(int mode, int k, const double* x, const double* s,
                                                 const double* qdiag, const uint8_t* free_col) {
@@ -759,28 +778,23 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const T* __restrict__ M, int l
 template <class T>
 __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int ld, const T* __restrict__ Linv, int nb,
                                                   double* z, unsigned* flags, unsigned epoch, int* err) {
+  __shared__ double part[4][kNB];
   __shared__ double xs[kSolveBatch][kNB];
-  __shared__ double acc_s[kNB];
   __shared__ double rhs[kNB];
   __shared__ int s_run;
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  // thread (c, g): column c of the row block's L entries, rows 16g .. 16g+15 of each tile, so a
+  // thread's entries of a tile are 16 consecutive values (vector loads) and the four groups' partial
+  // sums meet in shared memory once per block
+  const int t = threadIdx.x, c = t & (kNB - 1), g = t >> 6;
   for (int q = blockIdx.x; q < nb; q += gridDim.x) {
     const int i = nb - 1 - q;
     // this thread's entries of Linv_ii and of L_{i+1,i} (the last dependency), loaded before any wait
-    double li[8][2], lp[8][2];
-    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int c = w * 8 + u;
-      li[u][0] = static_cast<double>(Li[c * kNB + lane]);
-      li[u][1] = static_cast<double>(Li[c * kNB + lane + 32]);
-      if (i + 1 < nb) {
-        const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + (i + 1) * kNB;
-        lp[u][0] = static_cast<double>(col[lane]);
-        lp[u][1] = static_cast<double>(col[lane + 32]);
-      }
-    }
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double li[16], lp[16];
+    const T* Li = Linv + static_cast<int64_t>(i) * kNB * kNB + c * kNB + g * 16;
+    load16(Li, li);
+    const T* colc = M + static_cast<int64_t>(i * kNB + c) * ld + g * 16;  // column i*64+c of L
+    if (i + 1 < nb) load16(colc + (i + 1) * kNB, lp);
+    double acc = 0.0;
     bool bad = false;
     // blocks nb-1 down to i+2 in runs of released ones
     const int deps = nb - i - 2;
@@ -799,15 +813,13 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
       for (int idx = t; idx < run * kNB; idx += blockDim.x)
         xs[idx / kNB][idx % kNB] = __ldcg(z + (j0 - idx / kNB) * kNB + idx % kNB);
       __syncthreads();
-      // acc_c += sum_r L[j*64 + r][i*64 + c] * x_j[r]
+      // acc_c += sum_r L[j*64 + r][i*64 + c] * x_j[r], this thread's 16 rows r
 #pragma unroll 2
       for (int b = 0; b < run; ++b) {
+        double l[16];
+        load16(colc + (j0 - b) * kNB, l);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int c = w * 8 + u;
-          const T* col = M + static_cast<int64_t>(i * kNB + c) * ld + (j0 - b) * kNB;
-          acc[u] += static_cast<double>(col[lane]) * xs[b][lane] + static_cast<double>(col[lane + 32]) * xs[b][lane + 32];
-        }
+        for (int u = 0; u < 16; ++u) acc += l[u] * xs[b][g * 16 + u];
       }
       __syncthreads();
       done += run;
@@ -824,28 +836,21 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
         if (t < kNB) xs[0][t] = __ldcg(z + (i + 1) * kNB + t);
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < 8; ++u) acc[u] += lp[u][0] * xs[0][lane] + lp[u][1] * xs[0][lane + 32];
+        for (int u = 0; u < 16; ++u) acc += lp[u] * xs[0][g * 16 + u];
       }
     }
     if (bad && t == 0) atomicExch(err, 1);
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const double v = warp_sum(acc[u]);
-      if (lane == 0) acc_s[w * 8 + u] = v;
-    }
+    part[g][c] = acc;
     __syncthreads();
-    if (t < kNB) rhs[t] = z[i * kNB + t] - acc_s[t];
+    if (t < kNB) rhs[t] = z[i * kNB + t] - (part[0][t] + part[1][t] + part[2][t] + part[3][t]);
     __syncthreads();
     // x_c = sum_r Linv[r][c] rhs[r] = sum_r Li[c * 64 + r] rhs[r]
+    double y = 0.0;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int c = w * 8 + u;
-      double v = li[u][0] * rhs[lane] + li[u][1] * rhs[lane + 32];
-      v = warp_sum(v);
-      if (lane == 0) acc_s[c] = v;
-    }
+    for (int u = 0; u < 16; ++u) y += li[u] * rhs[g * 16 + u];
+    part[g][c] = y;
     __syncthreads();
-    if (t < kNB) z[i * kNB + t] = acc_s[t];
+    if (t < kNB) z[i * kNB + t] = part[0][t] + part[1][t] + part[2][t] + part[3][t];
     __threadfence();
     __syncthreads();
     if (t == 0) st_release(flags + i, epoch);
