@@ -264,12 +264,13 @@ bool plain_lp_shape(const sov_model& p, LpShape* s) {
 
 void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scaling, const LpFormOut& o,
                          LpFormInfo* info) {
-  // The same arithmetic as build_std_form + scale_two_pass + csr_from_csc, fused into four passes
+  // The same arithmetic as build_std_form + scale_two_pass + csr_from_csc, fused into three passes
   // over the entries: (1) copy, with the row counts, the coefficient range and the first row
   // maxima; (2), (3) one scaling pass each, column by column (row scale, column maximum, column
   // scale), the first one also collecting the second pass's row maxima and the second one the
-  // final coefficient range; (4) the CSR fill. Every value sees the same multiplications in the
-  // same order, so the result is bit for bit the general builder's.
+  // final coefficient range and (4) the CSR fill (a pass of its own without scaling). Every value
+  // sees the same multiplications in the same order, so the result is bit for bit the general
+  // builder's.
   thread_local std::vector<double> rs1, rs2;
   thread_local std::vector<int> fill;
   constexpr double kInf = std::numeric_limits<double>::infinity();
@@ -326,9 +327,23 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
   info->coef_min_before = lo < kInf ? lo : 0.0;
   info->coef_max_before = hi;
   info->scaling_applied = enable_scaling && m > 0 && n > 0;
+  // CSR row starts from the counts taken in (1); the entries are filled by the last pass
+  for (int i = 0; i < m; ++i) o.row_ptr[i + 1] += o.row_ptr[i];
+  fill.assign(o.row_ptr, o.row_ptr + m);
   if (info->scaling_applied) {
-    // scale factors computed in loops of independent iterations (no carried state), so the
-    // square roots and divisions overlap
+    // scale factors 1/sqrt(max|a|): a run of equal maxima (common: many rows and columns share
+    // their largest magnitude) reuses the last factor, the same value computed once
+    auto inv_sqrt_runs = [](double* v, int len) {
+      double last_in = std::numeric_limits<double>::quiet_NaN(), last_out = 1.0;
+      for (int k = 0; k < len; ++k) {
+        const double x = v[k];
+        if (!(x == last_in)) {
+          last_in = x;
+          last_out = x > 0.0 ? 1.0 / std::sqrt(x) : 1.0;
+        }
+        v[k] = last_out;
+      }
+    };
     thread_local std::vector<double> cmx;
     cmx.resize(n);
     rs2.assign(m, 0.0);
@@ -337,7 +352,7 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
     // (2), (3): rows by 1/sqrt(max|a|), then columns (interior_point.cpp:370-405), twice
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<double>& rs = pass == 0 ? rs1 : rs2;
-      for (int i = 0; i < m; ++i) rs[i] = rs[i] > 0.0 ? 1.0 / std::sqrt(rs[i]) : 1.0;
+      inv_sqrt_runs(rs.data(), m);
       for (int i = 0; i < m; ++i) {
         o.row_scale[i] *= rs[i];
         o.b[i] *= rs[i];
@@ -350,7 +365,7 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
         }
         cmx[j] = mx;
       }
-      for (int j = 0; j < n; ++j) cmx[j] = cmx[j] > 0.0 ? 1.0 / std::sqrt(cmx[j]) : 1.0;
+      inv_sqrt_runs(cmx.data(), n);
       for (int j = 0; j < n; ++j) {
         const double sc = cmx[j];
         for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
@@ -362,6 +377,9 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
             const bool use = a > 0.0 && a < kInf;
             lo = std::min(lo, use ? a : kInf);
             hi = std::max(hi, use ? a : 0.0);
+            const int t = fill[o.row_idx[k]]++;  // (4) the CSR entry, in column order per row
+            o.col_idx[t] = j;
+            o.rval[t] = o.val[k];
           }
         }
         o.c[j] *= sc;
@@ -373,16 +391,14 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
   } else {
     info->coef_min_after = info->coef_min_before;
     info->coef_max_after = info->coef_max_before;
+    // (4) CSR
+    for (int j = 0; j < n; ++j)
+      for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
+        const int t = fill[o.row_idx[k]]++;
+        o.col_idx[t] = j;
+        o.rval[t] = o.val[k];
+      }
   }
-  // (4) CSR: row counts were taken in (1)
-  for (int i = 0; i < m; ++i) o.row_ptr[i + 1] += o.row_ptr[i];
-  fill.assign(o.row_ptr, o.row_ptr + m);
-  for (int j = 0; j < n; ++j)
-    for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
-      const int t = fill[o.row_idx[k]]++;
-      o.col_idx[t] = j;
-      o.rval[t] = o.val[k];
-    }
 }
 
 namespace {
