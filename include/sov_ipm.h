@@ -192,8 +192,10 @@ int sov_ipm_dims(const sov_model* model, int32_t qp, int32_t* n_ipm, int32_t* m_
 /* One LP through the GPU IPM. Synchronous; host pointers are borrowed for the call. */
 int sov_lp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
 
-/* One convex QP through the GPU IPM, normal-equation path: separable (diagonal) Hessians; a model
- * with off-diagonal Hessian entries returns SOV_ERROR with a message saying so. */
+/* One convex QP through the GPU IPM (QpInteriorPointSolver::solve, qp_interior_point.cpp:3123-3186).
+ * Separable (diagonal) Hessians take the y-space normal equations A (Q + X^-1 S)^-1 A'; a Hessian
+ * that couples variables is held dense as H = Q + X^-1 S (FP64 Cholesky on the GPU, at most 16384
+ * IPM columns) and the same reduced system A H^-1 A' is formed from it. */
 int sov_qp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
 
 /* count independent LPs in one persistent batched launch (one CTA per LP, the whole IPM loop

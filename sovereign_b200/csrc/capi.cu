@@ -120,8 +120,6 @@ int solve_one(const sov_model* model, const sov_options* opt_in, sov_result* res
       std::snprintf(result->message, sizeof(result->message), "Optimal (no constraints) via IPM path.");
       return SOV_OK;
     }
-    if (qp && !f.q_diagonal)
-      throw std::runtime_error("the GPU QP path takes separable (diagonal) Hessians; this model couples variables in Q");
     if (qp) {
       for (int j = 0; j < f.n; ++j)
         if (f.free_col[j] && !(f.qdiag[j] > 0.0))

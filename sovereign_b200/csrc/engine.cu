@@ -262,6 +262,7 @@ class Engine {
   // factorization on, the engine factors in FP64
   static constexpr int kPcgSwitch = 12;
   static constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the default restart
+  static constexpr int kCoupledMaxColumns = 16384;  // dense H of a coupled-Hessian QP: at most 2 GB
   bool to_fp64_ = false;
   // x-space QP
   XSpace xs_;
@@ -269,6 +270,15 @@ class Engine {
   int order_ = 0;  // order of the factored system: m (y-space) or structural columns (x-space)
   DevBuf<int> slack_of_row_;
   DevBuf<double> sigma_, tr_, dyv_;
+  // QP with a coupled Hessian: dense H = Q + diag(h) (order n, padded to nph_), its factor, and
+  // Y = H^-1 A' for the reduced system M = A H^-1 A'
+  bool coupled_ = false;
+  int nph_ = 0, nbh_ = 0;
+  DevBuf<int> q_ptr_, q_idx_;
+  DevBuf<double> q_val_, qdense_, hmat_, hlinv_, hdiag_, ymat_, hvec_;
+  DevBuf<unsigned> hflags_;
+  DenseSystem<double> dsh_{};
+  void coupled_newton(int mode);
 };
 
 void Engine::setup() {
@@ -313,11 +323,21 @@ void Engine::setup() {
     throw std::runtime_error("x-space factorization needs a QP whose rows are all inequalities and whose structural "
                              "columns all have Q_jj > 0");
   xspace_ = opt_.factorization == SOV_FACTOR_XSPACE;
+  coupled_ = f_.qp && !f_.q_diagonal;
+  if (coupled_) {
+    // the y-space system needs H^-1 of the coupled Hessian: dense H, FP64, no band / x-space
+    if (opt_.factorization == SOV_FACTOR_BANDED)
+      throw std::runtime_error("banded factorization needs a separable Hessian; this QP couples variables in Q");
+    if (n > kCoupledMaxColumns)
+      throw std::runtime_error("coupled-Hessian QP with " + std::to_string(n) + " IPM columns exceeds the dense "
+                               "Hessian path's limit of " + std::to_string(kCoupledMaxColumns));
+  }
   order_ = xspace_ ? f_.n_struct : m;
   // backend choice: band when the half-bandwidth is small, else dense (mixed or FP64)
   kd_ = xspace_ ? xs_.kd : normal_bandwidth(f_);
   const bool auto_pick = opt_.factorization == SOV_FACTOR_AUTO || opt_.factorization == SOV_FACTOR_XSPACE;
-  const bool want_band = opt_.factorization == SOV_FACTOR_BANDED || (auto_pick && kd_ <= kBandMax && order_ > 256);
+  const bool want_band =
+      !coupled_ && (opt_.factorization == SOV_FACTOR_BANDED || (auto_pick && kd_ <= kBandMax && order_ > 256));
   if (want_band) {
     if (kd_ > kBandMax) throw std::runtime_error("banded factorization requested but half-bandwidth " +
                                                  std::to_string(kd_) + " exceeds " + std::to_string(kBandMax));
@@ -327,7 +347,7 @@ void Engine::setup() {
                                                  " is too large for the dense factorization (band width " +
                                                  std::to_string(kd_) + ")");
     // the x-space system has no matrix-free PCG operator: it is factored in FP64
-    backend_ = (opt_.precision == SOV_PRECISION_MIXED && !xspace_) ? kDenseMixed : kDense64;
+    backend_ = (opt_.precision == SOV_PRECISION_MIXED && !xspace_ && !coupled_) ? kDenseMixed : kDense64;
   }
   if (backend_ == kBand) {
     am_ = xspace_ ? build_assembly_xspace_band(f_, xs_) : build_assembly_band(f_, kd_);
@@ -359,6 +379,31 @@ void Engine::setup() {
       pcg_h_ = static_cast<PcgScalars*>(g_pinned_slots.acquire());
     }
   }
+  if (coupled_) {
+    nbh_ = ceil_div(n, kNB);
+    nph_ = nbh_ * kNB;
+    q_ptr_.alloc(n + 1);
+    q_ptr_.upload(f_.q_ptr.data(), n + 1, st_);
+    q_idx_.alloc(f_.q_idx.size());
+    q_idx_.upload(f_.q_idx.data(), f_.q_idx.size(), st_);
+    q_val_.alloc(f_.q_val.size());
+    q_val_.upload(f_.q_val.data(), f_.q_val.size(), st_);
+    // dense Q (column-major, both triangles) with the padding's diagonal 1
+    std::vector<double> qd(static_cast<size_t>(nph_) * nph_, 0.0);
+    for (int j = 0; j < n; ++j)
+      for (int k = f_.q_ptr[j]; k < f_.q_ptr[j + 1]; ++k) qd[static_cast<size_t>(j) * nph_ + f_.q_idx[k]] = f_.q_val[k];
+    for (int j = n; j < nph_; ++j) qd[static_cast<size_t>(j) * nph_ + j] = 1.0;
+    qdense_.alloc(qd.size());
+    qdense_.upload(qd.data(), qd.size(), st_);
+    hmat_.alloc(qd.size());
+    hlinv_.alloc(static_cast<size_t>(nbh_) * kNB * kNB);
+    hdiag_.alloc(n);
+    hflags_.alloc(nbh_ + 1);
+    hflags_.zero(st_);
+    ymat_.alloc(static_cast<size_t>(nph_) * std::max(1, m));
+    hvec_.alloc(nph_);
+    hvec_.zero(st_);
+  }
   if (xspace_) {
     slack_of_row_.alloc(m);
     slack_of_row_.upload(xs_.slack_of_row.data(), m, st_);
@@ -388,6 +433,9 @@ void Engine::setup() {
   } else {
     ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, order_, mp_, nb_, drop_ptr, fail_ptr, flags_.p, flags_.p + nb_, 1e-6};
   }
+  if (coupled_)
+    dsh_ = DenseSystem<double>{hmat_.p, hlinv_.p, hdiag_.p, n, nph_, nbh_, drop_ptr, fail_ptr, hflags_.p,
+                               hflags_.p + nbh_, 1e-13};
 
   dev_.m = m;
   dev_.n = n;
@@ -401,6 +449,10 @@ void Engine::setup() {
   dev_.c = c_.p;
   dev_.qdiag = qdiag_.p;
   dev_.free_col = free_.p;
+  dev_.q_ptr = q_ptr_.p;
+  dev_.q_idx = q_idx_.p;
+  dev_.q_val = q_val_.p;
+  dev_.q_coupled = coupled_ ? 1 : 0;
   dev_.qp = f_.qp ? 1 : 0;
   dev_.has_quadratic = f_.has_quadratic ? 1 : 0;
   int n_bounded = 0;
@@ -459,12 +511,30 @@ void Engine::assemble_and_factor(int mode) {
       Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
       ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, flags_.p + nb_, 1e-13};
     }
-    launch_dense_clear<double>(M64_.p, order_, mp_, st_);
-    launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, amode, reg, M64_.p, diag_.p, order_, mp_, st_);
-    if (xspace_) launch_xspace_diag(dev_, mode == kWeightOnes ? 0 : 1, M64_.p, mp_, diag_.p, st_);
-    dense_cholesky<double>(ds64_, st_, &launches_);
-    launches_ += xspace_ ? 3 : 2;
-    fp64_ready_ = true;
+    if (coupled_) {
+      // H = Q + diag(h) (h = 1 at the start), factored; Y = H^-1 A'; M = A Y + reg I, factored
+      SOV_CUDA(cudaMemcpyAsync(hmat_.p, qdense_.p, sizeof(double) * static_cast<size_t>(nph_) * nph_,
+                               cudaMemcpyDeviceToDevice, st_));
+      launch_hessian_diag(dev_, mode == kWeightOnes, hmat_.p, nph_, hdiag_.p, st_);
+      dense_cholesky<double>(dsh_, st_, &launches_);
+      SOV_CUDA(cudaMemsetAsync(ymat_.p, 0, sizeof(double) * static_cast<size_t>(nph_) * std::max(1, f_.m), st_));
+      launch_rows_to_columns(dev_, ymat_.p, nph_, st_);
+      for (int i = 0; i < f_.m; ++i)
+        dense_solve<double>(dsh_, ymat_.p + static_cast<size_t>(i) * nph_, epoch_, err_.p, st_, &launches_);
+      launch_dense_clear<double>(M64_.p, order_, mp_, st_);
+      launch_form_normal(dev_, ymat_.p, nph_, M64_.p, mp_, reg, diag_.p, st_);
+      dense_cholesky<double>(ds64_, st_, &launches_);
+      launches_ += 5;
+      fp64_ready_ = true;
+      if (stats_) stats_->factor_flops += (2.0 / 3.0) * std::pow(static_cast<double>(f_.n), 3.0);
+    } else {
+      launch_dense_clear<double>(M64_.p, order_, mp_, st_);
+      launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, amode, reg, M64_.p, diag_.p, order_, mp_, st_);
+      if (xspace_) launch_xspace_diag(dev_, mode == kWeightOnes ? 0 : 1, M64_.p, mp_, diag_.p, st_);
+      dense_cholesky<double>(ds64_, st_, &launches_);
+      launches_ += xspace_ ? 3 : 2;
+      fp64_ready_ = true;
+    }
   } else {
     launch_dense_clear<float>(M32_.p, f_.m, mp_, st_);
     launch_assemble<float>(amd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, M32_.p, diag_.p, f_.m, mp_, st_);
@@ -472,6 +542,19 @@ void Engine::assemble_and_factor(int mode) {
     launches_ += 2;
   }
   if (stats_) stats_->factor_flops += (2.0 / 3.0) * std::pow(static_cast<double>(order_), 3.0);
+}
+
+// One Newton pass of a coupled-Hessian QP: z = rp - A H^-1 r1, M dy = z, dx = H^-1 (r1 + A'dy),
+// then ds, the ratio tests and the step lengths as in the separable path.
+void Engine::coupled_newton(int mode) {
+  launch_hessian_r1(dev_, mode, hvec_.p, st_);
+  dense_solve<double>(dsh_, hvec_.p, epoch_, err_.p, st_, &launches_);
+  launch_rows_minus(dev_, hvec_.p, st_);
+  newton_solve();
+  launch_hessian_w(dev_, mode, hvec_.p, st_);
+  dense_solve<double>(dsh_, hvec_.p, epoch_, err_.p, st_, &launches_);
+  launch_direction_dx(dev_, mode, hvec_.p, st_, &launches_);
+  launches_ += 3;
 }
 
 bool Engine::newton_solve() {
@@ -540,6 +623,12 @@ void Engine::read_scalars() {
 std::string Engine::describe() const {
   char buf[256];
   const char* space = xspace_ ? "x-space Q + A'ZW^-1A, " : "";
+  if (coupled_) {
+    std::snprintf(buf, sizeof buf,
+                  "A H^-1 A' with H = Q + X^-1 S dense, dense Cholesky on the GPU, FP64 (H %d x %d, %d x %d)", f_.n,
+                  f_.n, order_, order_);
+    return buf;
+  }
   if (backend_ == kBand)
     std::snprintf(buf, sizeof buf, "%sbanded LDL^T on the GPU (order %d, half-bandwidth %d)", space, order_, kd_);
   else if (backend_ == kDense64)
@@ -755,6 +844,10 @@ void Engine::run(sov_result* r) {
     }
     assemble_and_factor(f_.qp ? kWeightQp : kWeightLp);
     for (int pass : {kRhsAffine, kRhsCorrector}) {
+      if (coupled_) {
+        coupled_newton(pass);
+        continue;
+      }
       if (xspace_) launch_newton_rhs_x(dev_, pass, st_, &launches_);
       else launch_newton_rhs(dev_, pass, st_, &launches_);
       newton_solve();

@@ -110,7 +110,13 @@ __global__ void __launch_bounds__(kThreads) k_residual_cols(IpmDev d) {
     for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) aty += d.cval[p] * d.y[d.row_idx[p]];
     const double xj = d.x[j], sj = d.s[j];
     double qx = 0.0;
-    if (d.qp) qx = d.qdiag[j] * xj;
+    if (d.qp) {
+      if (d.q_coupled) {  // (Q x)_j from column j of the symmetric Q
+        for (int k = d.q_ptr[j]; k < d.q_ptr[j + 1]; ++k) qx += d.q_val[k] * d.x[d.q_idx[k]];
+      } else {
+        qx = d.qdiag[j] * xj;
+      }
+    }
     // LP: rd = c - (A'y + s) (interior_point.cpp:578-582); QP: Qx + c - A'y - s (:2986-2992)
     const double r = d.qp ? qx + d.c[j] - aty - sj : d.c[j] - (aty + sj);
     d.rd[j] = r;
@@ -176,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_rhs(IpmDev d, int mode) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_direction(IpmDev d, int mode) {
+__global__ void __launch_bounds__(kThreads) k_direction(IpmDev d, int mode, const double* dxv) {
   const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
   double* dx = mode == kRhsAffine ? d.dxa : d.dx;
   double* ds = mode == kRhsAffine ? d.dsa : d.ds;
@@ -197,9 +203,13 @@ __global__ void __launch_bounds__(kThreads) k_direction(IpmDev d, int mode) {
       // dx = D (r1 + A'dy); ds = (rxs - s dx)/x (qp_interior_point.cpp:2832-2844)
       fr = d.free_col[j];
       const double xf = fmax(xj, 1e-16);
-      const double D = 1.0 / (d.qdiag[j] + (fr ? 0.0 : fmax(sj, 1e-16) / xf));
-      const double r1 = fr ? -d.rd[j] : -d.rd[j] + rxs / xf;
-      dxj = D * (r1 + atdy);
+      if (dxv) {  // coupled Hessian: dx = H^-1 (r1 + A'dy), solved by the caller
+        dxj = dxv[j];
+      } else {
+        const double D = 1.0 / (d.qdiag[j] + (fr ? 0.0 : fmax(sj, 1e-16) / xf));
+        const double r1 = fr ? -d.rd[j] : -d.rd[j] + rxs / xf;
+        dxj = D * (r1 + atdy);
+      }
       dsj = fr ? 0.0 : (rxs - sj * dxj) / xf;
     }
     dx[j] = dxj;
@@ -292,8 +302,13 @@ __global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
         } else if (d.free_col[j]) {
           x = 1.0 + atdy;
         } else {
+          double qones = d.qdiag[j];  // (Q 1)_j (qp_interior_point.cpp:2933-2941)
+          if (d.q_coupled) {
+            qones = 0.0;
+            for (int k = d.q_ptr[j]; k < d.q_ptr[j + 1]; ++k) qones += d.q_val[k];
+          }
           x = fmax(1.0, fabs(atdy));
-          s = fmax(1.0, fabs(d.qdiag[j] + d.c[j] - atdy));
+          s = fmax(1.0, fabs(qones + d.c[j] - atdy));
         }
       }
       if (d.qp && d.free_col[j]) s = 0.0;
@@ -446,6 +461,79 @@ __global__ void __launch_bounds__(kThreads) k_xdiag(IpmDev d, int mode, double* 
   }
 }
 
+// ---- coupled-Hessian QP ----
+__global__ void __launch_bounds__(kThreads) k_hessian_diag(IpmDev d, int start, double* H, int ld, double* diag) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    const double xf = fmax(d.x[j], 1e-16), sf = fmax(d.s[j], 1e-16);
+    const double h = d.free_col[j] ? 0.0 : (start ? 1.0 : sf / xf);
+    double* hjj = H + static_cast<int64_t>(j) * ld + j;
+    *hjj += h;
+    diag[j] = *hjj;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_rows_to_columns(IpmDev d, double* Y, int ld) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = warp_row(); i < d.m; i += warps)
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32)
+      Y[static_cast<int64_t>(i) * ld + d.col_idx[p]] = d.rval[p];
+}
+
+// one warp per lower-triangle entry (i, k), k <= i: sum over row i of A of a_ij Y[j][k]
+__global__ void __launch_bounds__(kThreads) k_form_normal(IpmDev d, const double* Y, int ld_y, double* M, int ld_m,
+                                                          double reg, double* diag) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int64_t pairs = static_cast<int64_t>(d.m) * (d.m + 1) / 2;
+  for (int64_t t = warp_row(); t < pairs; t += warps) {
+    int i = static_cast<int>((sqrt(8.0 * static_cast<double>(t) + 1.0) - 1.0) * 0.5);
+    while (static_cast<int64_t>(i + 1) * (i + 2) / 2 <= t) ++i;
+    while (static_cast<int64_t>(i) * (i + 1) / 2 > t) --i;
+    const int k = static_cast<int>(t - static_cast<int64_t>(i) * (i + 1) / 2);
+    const double* yk = Y + static_cast<int64_t>(k) * ld_y;
+    double acc = 0.0;
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * yk[d.col_idx[p]];
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      const double v = i == k ? acc + reg : acc;
+      M[static_cast<int64_t>(k) * ld_m + i] = v;
+      if (i == k) diag[i] = v;
+    }
+  }
+}
+
+__device__ __forceinline__ double hessian_r1(const IpmDev& d, int mode, int j, double sigma_mu) {
+  const double rxs = rxs_of(d, mode, j, sigma_mu);
+  return d.free_col[j] ? -d.rd[j] : -d.rd[j] + rxs / fmax(d.x[j], 1e-16);
+}
+
+__global__ void __launch_bounds__(kThreads) k_hessian_r1(IpmDev d, int mode, double* v) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x)
+    v[j] = hessian_r1(d, mode, j, sigma_mu);
+}
+
+__global__ void __launch_bounds__(kThreads) k_rows_minus(IpmDev d, const double* v) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = warp_row(); i < d.m; i += warps) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * v[d.col_idx[p]];
+    acc = warp_sum(acc);
+    if (lane == 0) d.z[i] = d.rp[i] - acc;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_hessian_w(IpmDev d, int mode, double* v) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double atdy = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+    v[j] = hessian_r1(d, mode, j, sigma_mu) + atdy;
+  }
+}
+
 int row_blocks(int m) { return std::max(1, std::min(kMaxBlocks, ceil_div(static_cast<long long>(m) * 32, kThreads))); }
 
 }  // namespace
@@ -466,7 +554,14 @@ void launch_newton_rhs(const IpmDev& d, int mode, cudaStream_t st, int* launches
 }
 
 void launch_direction(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
-  k_direction<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode);
+  k_direction<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode, nullptr);
+  if (mode == kRhsAffine) k_mu_aff<<<blocks_for(d.n), kThreads, 0, st>>>(d);
+  SOV_LAUNCH_CHECK();
+  if (launches) *launches += mode == kRhsAffine ? 2 : 1;
+}
+
+void launch_direction_dx(const IpmDev& d, int mode, const double* dxv, cudaStream_t st, int* launches) {
+  k_direction<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode, dxv);
   if (mode == kRhsAffine) k_mu_aff<<<blocks_for(d.n), kThreads, 0, st>>>(d);
   SOV_LAUNCH_CHECK();
   if (launches) *launches += mode == kRhsAffine ? 2 : 1;
@@ -525,6 +620,43 @@ void launch_xspace_diag(const IpmDev& d, int mode, double* M, int layout_ld, dou
 void launch_normal_matvec(const IpmDev& d, const double* v, double* tmp_n, double* out, double reg, cudaStream_t st) {
   k_normal_cols<<<blocks_for(d.n), kThreads, 0, st>>>(d, v, tmp_n);
   k_normal_rows<<<row_blocks(d.m), kThreads, 0, st>>>(d, v, tmp_n, out, reg);
+  SOV_LAUNCH_CHECK();
+}
+
+}  // namespace sov
+
+namespace sov {
+
+void launch_hessian_diag(const IpmDev& d, bool start, double* H, int ld, double* diag, cudaStream_t st) {
+  k_hessian_diag<<<blocks_for(d.n), kThreads, 0, st>>>(d, start ? 1 : 0, H, ld, diag);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_rows_to_columns(const IpmDev& d, double* Y, int ld, cudaStream_t st) {
+  k_rows_to_columns<<<row_blocks(d.m), kThreads, 0, st>>>(d, Y, ld);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_form_normal(const IpmDev& d, const double* Y, int ld_y, double* M, int ld_m, double reg, double* diag,
+                        cudaStream_t st) {
+  const long long pairs = static_cast<long long>(d.m) * (d.m + 1) / 2;
+  k_form_normal<<<std::max(1, std::min(kMaxBlocks, ceil_div(pairs * 32, kThreads))), kThreads, 0, st>>>(
+      d, Y, ld_y, M, ld_m, reg, diag);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_hessian_r1(const IpmDev& d, int mode, double* v, cudaStream_t st) {
+  k_hessian_r1<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode, v);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_rows_minus(const IpmDev& d, const double* v, cudaStream_t st) {
+  k_rows_minus<<<row_blocks(d.m), kThreads, 0, st>>>(d, v);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_hessian_w(const IpmDev& d, int mode, double* v, cudaStream_t st) {
+  k_hessian_w<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode, v);
   SOV_LAUNCH_CHECK();
 }
 

@@ -35,6 +35,12 @@ struct IpmDev {
   const uint8_t* free_col;  // QP: 1 = no barrier (null for LP)
   int qp;
   int has_quadratic;
+  // QP whose Hessian couples variables: Q over the IPM columns, CSC with both triangles (null and
+  // 0 for separable Hessians, which use qdiag alone)
+  const int* q_ptr;
+  const int* q_idx;
+  const double* q_val;
+  int q_coupled;
   double comp_count;        // n (LP) or max(1, #bounded) (QP)
   double bnorm, cnorm, objective_offset, tau;
   // iterate and work vectors
@@ -80,6 +86,26 @@ void launch_start_rhs_x(const IpmDev& d, cudaStream_t st, int* launches);
 void launch_start_dy_x(const IpmDev& d, cudaStream_t st, int* launches);
 // K_jj += Q_jj + h_j (mode 1) or += 1 (start, mode 0); same on the recorded diagonal
 void launch_xspace_diag(const IpmDev& d, int mode, double* M, int layout_ld, double* diag, cudaStream_t st);
+
+// Coupled-Hessian QP (q_coupled == 1): the Newton system is reduced with H = Q + diag(h) held dense
+// and factored (h_j = s_j/x_j, 0 for free columns, 1 at the start), so that
+//   M = A H^-1 A' (+ reg on the diagonal) dy = rp - A H^-1 r1,   dx = H^-1 (r1 + A'dy)
+// with r1 = -rd + rxs/x (free: -rd) as in the separable path (qp_interior_point.cpp:2832-2844).
+// H += diag(h) on a copy of dense Q (column-major, ld); diag[j] = H_jj for the pivot rule
+void launch_hessian_diag(const IpmDev& d, bool start, double* H, int ld, double* diag, cudaStream_t st);
+// Y[:, i] = row i of A (Y zeroed by the caller, column-major, ld)
+void launch_rows_to_columns(const IpmDev& d, double* Y, int ld, cudaStream_t st);
+// lower triangle of M = A Y (Y = H^-1 A', ld_y), reg added on the diagonal; diag[i] = M_ii
+void launch_form_normal(const IpmDev& d, const double* Y, int ld_y, double* M, int ld_m, double reg, double* diag,
+                        cudaStream_t st);
+// r1 of the current mode into v (entries n.. untouched)
+void launch_hessian_r1(const IpmDev& d, int mode, double* v, cudaStream_t st);
+// z = rp - A v (v = H^-1 r1)
+void launch_rows_minus(const IpmDev& d, const double* v, cudaStream_t st);
+// v = r1 + A'dy (dy = z)
+void launch_hessian_w(const IpmDev& d, int mode, double* v, cudaStream_t st);
+// dx = dxv (= H^-1 (r1 + A'dy)), ds, ratio tests and step lengths as launch_direction
+void launch_direction_dx(const IpmDev& d, int mode, const double* dxv, cudaStream_t st, int* launches);
 
 int reduction_blocks(int n);
 

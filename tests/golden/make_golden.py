@@ -42,7 +42,7 @@ LP_SPECS = [
 BATCH_SPEC = dict(count=64, seed=3)          # transport_batch sample of the 4096-LP workload
 MULTICOMMODITY_SEEDS = [100, 101]            # MulticommodityFamily() instances
 QP_SPECS = [("small_qp_offdiagonal", []), ("convex_sequence_qp", [52, 3]), ("convex_sequence_qp", [202, 3]),
-            ("convex_sequence_qp", [2002, 3])]
+            ("convex_sequence_qp", [2002, 3]), ("reference_portfolio", [300, 12]), ("reference_portfolio", [60, 5])]
 
 
 def build(name, args):

@@ -1,5 +1,7 @@
 """GPU QP parity: the convex-sequence (LISWET) shape against the reference's results, including
-its published n = 20000 projection (golden vector from the reference's benchmark report)."""
+its published n = 20000 projection (golden vector from the reference's benchmark report), and QPs
+whose Hessian couples variables (the reference's off-diagonal regression QP and its portfolio QP
+with a diagonally dominant coupled covariance, test_correctness_regressions.cpp:263-330)."""
 import json
 import os
 
@@ -62,3 +64,27 @@ def test_xspace_option_small_sequence_exact():
     rx = _solve(P.convex_sequence_qp(52, 3), o, True, False, False, None)
     assert rx.status_name == "OPTIMAL" and "x-space" in rx.message
     assert rel(rx.objective_value, QP["convex_sequence_qp(52,3)"]["objective"]) < 1e-8
+
+
+# the reference's own bar between its dense and sparse KKT paths on the portfolio QP
+# (test_correctness_regressions.cpp:318-320)
+COUPLED_TOL = 1e-7
+
+
+@pytest.mark.parametrize("key", ["small_qp_offdiagonal()", "reference_portfolio(60,5)", "reference_portfolio(300,12)"])
+def test_coupled_hessian_matches_reference(key):
+    g = QP[key]
+    name, args = g["spec"]
+    r = QpInteriorPointSolver().solve(getattr(P, name)(*args))
+    assert r.status_name == "OPTIMAL", r.message
+    assert "H = Q + X^-1 S dense" in r.message
+    assert rel(r.objective_value, g["objective"]) < COUPLED_TOL
+    assert np.all(np.abs(np.asarray(r.primal[:len(g["primal_head"])]) - np.asarray(g["primal_head"])) < 1e-6)
+
+
+def test_coupled_hessian_known_answer():
+    # QpAccuracy.OffDiagonalHessianTermsCountOnce: x = y = 0.4, objective -0.4
+    r = QpInteriorPointSolver().solve(P.small_qp_offdiagonal())
+    assert r.status_name == "OPTIMAL", r.message
+    assert abs(r.primal[0] - 0.4) < 1e-7 and abs(r.primal[1] - 0.4) < 1e-7
+    assert abs(r.objective_value + 0.4) < 1e-8

@@ -43,7 +43,8 @@ def test_restatement_matches_reference_golden_batch():
         assert rel(r.objective_value, g["objectives"][k]) < 1e-12
 
 
-@pytest.mark.parametrize("key", ["small_qp_offdiagonal()", "convex_sequence_qp(52,3)", "convex_sequence_qp(202,3)"])
+@pytest.mark.parametrize("key", ["small_qp_offdiagonal()", "convex_sequence_qp(52,3)", "convex_sequence_qp(202,3)",
+                                 "reference_portfolio(60,5)", "reference_portfolio(300,12)"])
 def test_qp_restatement_matches_reference_golden(key):
     g = QP[key]
     name, args = g["spec"]
@@ -51,7 +52,8 @@ def test_qp_restatement_matches_reference_golden(key):
     assert r.status_name == "OPTIMAL"
     # the reference takes its LISWET active-set path on the convex-sequence shape; the generic
     # interior point agrees to its 1e-8 tolerance
-    assert rel(r.objective_value, g["objective"]) < (1e-12 if "offdiagonal" in key else 1e-8)
+    exact = "offdiagonal" in key or "portfolio" in key  # same generic interior point as the reference
+    assert rel(r.objective_value, g["objective"]) < (1e-12 if exact else 1e-8)
 
 
 def test_qp_offdiagonal_known_answer():
