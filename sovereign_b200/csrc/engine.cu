@@ -515,7 +515,7 @@ void Engine::assemble_and_factor(int mode) {
       // H = Q + diag(h) (h = 1 at the start), factored; Y = H^-1 A'; M = A Y + reg I, factored
       SOV_CUDA(cudaMemcpyAsync(hmat_.p, qdense_.p, sizeof(double) * static_cast<size_t>(nph_) * nph_,
                                cudaMemcpyDeviceToDevice, st_));
-      launch_hessian_diag(dev_, mode == kWeightOnes, hmat_.p, nph_, hdiag_.p, st_);
+      launch_hessian_diag(dev_, mode == kWeightOnes || mode == kWeightQpStart, hmat_.p, nph_, hdiag_.p, st_);
       dense_cholesky<double>(dsh_, st_, &launches_);
       SOV_CUDA(cudaMemsetAsync(ymat_.p, 0, sizeof(double) * static_cast<size_t>(nph_) * std::max(1, f_.m), st_));
       launch_rows_to_columns(dev_, ymat_.p, nph_, st_);
@@ -714,7 +714,11 @@ void Engine::run(sov_result* r) {
 
   // starting point (interior_point.cpp:488-506 / qp_interior_point.cpp:2881-2950, default start)
   auto default_start = [&]() {
-    assemble_and_factor(kWeightOnes);
+    // x = s = 0 before the start system: the mixed path's matrix-free operator then weighs every
+    // column as x = s = 1 would (max(x, 1e-16) / max(s, 1e-16) = 1), like the factored start system
+    SOV_CUDA(cudaMemsetAsync(x_.p, 0, sizeof(double) * n, st_));
+    SOV_CUDA(cudaMemsetAsync(s_.p, 0, sizeof(double) * n, st_));
+    assemble_and_factor(f_.qp && !xspace_ ? kWeightQpStart : kWeightOnes);
     if (xspace_) launch_start_rhs_x(dev_, st_, &launches_);
     else launch_start_rhs(dev_, st_, &launches_);
     newton_solve();
