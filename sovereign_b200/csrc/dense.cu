@@ -71,7 +71,6 @@ __device__ __forceinline__ void load16(const float* p, double v[16]) {
 __device__ __forceinline__ double column_weight(int mode, int k, const double* x, const double* s,
                                                 const double* qdiag, const uint8_t* free_col) {
   if (mode == kWeightOnes) return 1.0;
-  if (mode == kWeightQpStart) return 1.0 / (qdiag[k] + (free_col[k] ? 0.0 : 1.0));
   const double xk = fmax(x[k], 1e-16), sk = fmax(s[k], 1e-16);
   if (mode == kWeightLp) return xk / sk;
   if (mode == kWeightTheta) return sk / xk;

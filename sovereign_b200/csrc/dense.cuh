@@ -29,11 +29,10 @@ struct DenseSystem {
 // weight d_k is computed on the fly from the iterate:
 //   LP: d = max(x,1e-16)/max(s,1e-16)                  (interior_point.cpp:411-415)
 //   QP: d = 1/(qdiag + h), h = free ? 0 : max(s,1e-16)/max(x,1e-16)  (qp_interior_point.cpp:449-456)
-//   ones: d = 1 (the LP starting-point system, interior_point.cpp:490-491)
-//   QP start: d = 1/(qdiag + h) at x = s = 1, h = free ? 0 : 1 (the QP starting-point system, H = Q + I,
-//   qp_interior_point.cpp:2884-2885)
+//   ones: d = 1 (the starting-point system: LP interior_point.cpp:490-491; QP H = I, the KKT factored
+//   without the Hessian, qp_interior_point.cpp:2884 and :449-456)
 //   theta: d = max(s,1e-16)/max(x,1e-16) of the given column (x-space QP: the slack's barrier weight)
-enum WeightMode : int { kWeightLp = 0, kWeightQp = 1, kWeightOnes = 2, kWeightTheta = 3, kWeightQpStart = 4 };
+enum WeightMode : int { kWeightLp = 0, kWeightQp = 1, kWeightOnes = 2, kWeightTheta = 3 };
 
 struct AssemblyDev {
   const int64_t* target;

@@ -16,9 +16,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "band.cuh"
@@ -199,8 +201,9 @@ __global__ void __launch_bounds__(1024) k_pcg_step(int m, const double* p, const
 
 class Engine {
  public:
-  Engine(const sov_model& model, const StdForm& f, const sov_options& opt, cudaStream_t st, EngineStats* stats)
-      : model_(model), f_(f), opt_(opt), st_(st), stats_(stats) {}
+  Engine(const sov_model& model, const StdForm& f, const sov_options& opt, cudaStream_t st, EngineStats* stats,
+         bool mehrotra_start = false)
+      : model_(model), f_(f), opt_(opt), st_(st), stats_(stats), mehrotra_start_(mehrotra_start) {}
 
   void run(sov_result* r);
 
@@ -279,6 +282,9 @@ class Engine {
   DevBuf<unsigned> hflags_;
   DenseSystem<double> dsh_{};
   void coupled_newton(int mode);
+  // QP second attempt: Mehrotra's starting point in place of the default one
+  bool mehrotra_start_ = false;
+  void mehrotra_qp_start();
 };
 
 void Engine::setup() {
@@ -511,11 +517,12 @@ void Engine::assemble_and_factor(int mode) {
       Linv64_.alloc(static_cast<size_t>(nb_) * kNB * kNB);
       ds64_ = DenseSystem<double>{M64_.p, Linv64_.p, diag_.p, order_, mp_, nb_, &sc_.p->drops, &sc_.p->fail, flags_.p, flags_.p + nb_, 1e-13};
     }
-    if (coupled_) {
-      // H = Q + diag(h) (h = 1 at the start), factored; Y = H^-1 A'; M = A Y + reg I, factored
+    if (coupled_ && mode != kWeightOnes) {
+      // H = Q + diag(h), factored; Y = H^-1 A'; M = A Y + reg I, factored (the starting-point
+      // system has H = I and takes the ordinary assembly below)
       SOV_CUDA(cudaMemcpyAsync(hmat_.p, qdense_.p, sizeof(double) * static_cast<size_t>(nph_) * nph_,
                                cudaMemcpyDeviceToDevice, st_));
-      launch_hessian_diag(dev_, mode == kWeightOnes || mode == kWeightQpStart, hmat_.p, nph_, hdiag_.p, st_);
+      launch_hessian_diag(dev_, false, hmat_.p, nph_, hdiag_.p, st_);
       dense_cholesky<double>(dsh_, st_, &launches_);
       SOV_CUDA(cudaMemsetAsync(ymat_.p, 0, sizeof(double) * static_cast<size_t>(nph_) * std::max(1, f_.m), st_));
       launch_rows_to_columns(dev_, ymat_.p, nph_, st_);
@@ -544,12 +551,65 @@ void Engine::assemble_and_factor(int mode) {
   if (stats_) stats_->factor_flops += (2.0 / 3.0) * std::pow(static_cast<double>(order_), 3.0);
 }
 
+// Mehrotra's QP starting point (qp_interior_point.cpp:2891-2928), after the default start's system
+// (the KKT without the Hessian: H = I, so M = A A') is factored and z holds its dy: xt = 1 + A'dy;
+// (u, y) from the same system with r1 = -(c + Q xt), r2 = 0, i.e. A A' y = -A r1 and u = r1 + A'y;
+// x and s = xt and -u shifted into the interior and balanced so that the products x_j s_j spread
+// evenly; y = the least-squares dual.
+void Engine::mehrotra_qp_start() {
+  const int n = f_.n, m = f_.m;
+  double* xt = dxa_.p;
+  double* r1 = dsa_.p;
+  double* w = ds_.p;
+  launch_mehrotra_r1(dev_, xt, r1, st_);
+  launch_rows_minus(dev_, r1, nullptr, st_);  // z = 0 - A r1
+  newton_solve();                              // z = y_ls
+  launch_add_atz(dev_, r1, w, st_);            // u = r1 + A'y_ls
+  launches_ += 5;
+  std::vector<double> hxt(n), hu(n), hy(m);
+  std::vector<uint8_t> fr(f_.free_col.begin(), f_.free_col.end());
+  SOV_CUDA(cudaMemcpyAsync(hxt.data(), xt, sizeof(double) * n, cudaMemcpyDeviceToHost, st_));
+  SOV_CUDA(cudaMemcpyAsync(hu.data(), w, sizeof(double) * n, cudaMemcpyDeviceToHost, st_));
+  if (m) SOV_CUDA(cudaMemcpyAsync(hy.data(), z_.p, sizeof(double) * m, cudaMemcpyDeviceToHost, st_));
+  SOV_CUDA(cudaStreamSynchronize(st_));
+  double min_x = INFINITY, min_s = INFINITY;
+  for (int j = 0; j < n; ++j) {
+    if (fr[j]) continue;
+    min_x = std::min(min_x, hxt[j]);
+    min_s = std::min(min_s, -hu[j]);
+  }
+  const double shift_x = std::max(-1.5 * min_x, 0.0), shift_s = std::max(-1.5 * min_s, 0.0);
+  double xs = 0.0, sum_x = 0.0, sum_s = 0.0;
+  for (int j = 0; j < n; ++j) {
+    if (fr[j]) continue;
+    const double xh = hxt[j] + shift_x, sh = -hu[j] + shift_s;
+    xs += xh * sh;
+    sum_x += xh;
+    sum_s += sh;
+  }
+  const double bal_x = sum_s > 0.0 ? 0.5 * xs / sum_s : 1.0;
+  const double bal_s = sum_x > 0.0 ? 0.5 * xs / sum_x : 1.0;
+  std::vector<double> hx(n), hs(n);
+  for (int j = 0; j < n; ++j) {
+    if (fr[j]) {
+      hx[j] = hxt[j];
+      hs[j] = 0.0;
+      continue;
+    }
+    hx[j] = std::max(1e-8, hxt[j] + shift_x + bal_x);
+    hs[j] = std::max(1e-8, -hu[j] + shift_s + bal_s);
+  }
+  x_.upload(hx.data(), n, st_);
+  s_.upload(hs.data(), n, st_);
+  if (m) y_.upload(hy.data(), m, st_);
+}
+
 // One Newton pass of a coupled-Hessian QP: z = rp - A H^-1 r1, M dy = z, dx = H^-1 (r1 + A'dy),
 // then ds, the ratio tests and the step lengths as in the separable path.
 void Engine::coupled_newton(int mode) {
   launch_hessian_r1(dev_, mode, hvec_.p, st_);
   dense_solve<double>(dsh_, hvec_.p, epoch_, err_.p, st_, &launches_);
-  launch_rows_minus(dev_, hvec_.p, st_);
+  launch_rows_minus(dev_, hvec_.p, rp_.p, st_);
   newton_solve();
   launch_hessian_w(dev_, mode, hvec_.p, st_);
   dense_solve<double>(dsh_, hvec_.p, epoch_, err_.p, st_, &launches_);
@@ -714,16 +774,18 @@ void Engine::run(sov_result* r) {
 
   // starting point (interior_point.cpp:488-506 / qp_interior_point.cpp:2881-2950, default start)
   auto default_start = [&]() {
-    // x = s = 0 before the start system: the mixed path's matrix-free operator then weighs every
-    // column as x = s = 1 would (max(x, 1e-16) / max(s, 1e-16) = 1), like the factored start system
-    SOV_CUDA(cudaMemsetAsync(x_.p, 0, sizeof(double) * n, st_));
-    SOV_CUDA(cudaMemsetAsync(s_.p, 0, sizeof(double) * n, st_));
-    assemble_and_factor(f_.qp && !xspace_ ? kWeightQpStart : kWeightOnes);
+    assemble_and_factor(kWeightOnes);
     if (xspace_) launch_start_rhs_x(dev_, st_, &launches_);
     else launch_start_rhs(dev_, st_, &launches_);
+    dev_.start_system = 1;  // the mixed path's matrix-free operator weighs every column 1 as well
     newton_solve();
     if (xspace_) launch_start_dy_x(dev_, st_, &launches_);
-    launch_start_point(dev_, st_, &launches_);
+    if (mehrotra_start_ && f_.qp && !xspace_ && f_.m > 0) {
+      mehrotra_qp_start();
+    } else {
+      launch_start_point(dev_, st_, &launches_);
+    }
+    dev_.start_system = 0;
   };
   default_start();
   bool warm_used = false;
@@ -908,8 +970,55 @@ void Engine::run(sov_result* r) {
 
 int solve_single(const sov_model& model, const StdForm& f, const sov_options& opt, sov_result* result,
                  cudaStream_t stream, EngineStats* stats) {
-  Engine e(model, f, opt, stream, stats);
-  e.run(result);
+  {
+    Engine e(model, f, opt, stream, stats);
+    e.run(result);
+  }
+  // QP: a second attempt from Mehrotra's starting point when the default start does not reach
+  // OPTIMAL (qp_interior_point.cpp:3166-3180; SOVEREIGN_QP_DISABLE=retry turns it off, as there)
+  if (!f.qp || result->status == SOV_OPTIMAL || f.m == 0 || opt.factorization == SOV_FACTOR_XSPACE) return SOV_OK;
+  if (const char* off = std::getenv("SOVEREIGN_QP_DISABLE"))
+    if ((std::string(",") + off + ",").find(",retry,") != std::string::npos) return SOV_OK;
+  sov_result second = *result;
+  std::vector<double> primal(f.n_struct), dual_col(f.n_struct), dual_row(f.m0), ix(f.n), iy(f.m), is(f.n);
+  sov_diagnostics diag{};
+  second.primal = result->primal ? primal.data() : nullptr;
+  second.dual_col = result->dual_col ? dual_col.data() : nullptr;
+  second.dual_row = result->dual_row ? dual_row.data() : nullptr;
+  second.ipm_x = result->ipm_x ? ix.data() : nullptr;
+  second.ipm_y = result->ipm_y ? iy.data() : nullptr;
+  second.ipm_s = result->ipm_s ? is.data() : nullptr;
+  second.diagnostics = result->diagnostics ? &diag : nullptr;
+  {
+    Engine e(model, f, opt, stream, stats, true);
+    e.run(&second);
+  }
+  if (second.status == SOV_OPTIMAL) {
+    auto put = [](double* dst, const std::vector<double>& src) {
+      if (dst) std::copy(src.begin(), src.end(), dst);
+    };
+    put(result->primal, primal);
+    put(result->dual_col, dual_col);
+    put(result->dual_row, dual_row);
+    put(result->ipm_x, ix);
+    put(result->ipm_y, iy);
+    put(result->ipm_s, is);
+    if (result->diagnostics) *result->diagnostics = diag;
+    const int first_iterations = result->iterations;
+    sov_result keep = *result;  // the caller's array pointers
+    *result = second;
+    result->primal = keep.primal;
+    result->dual_col = keep.dual_col;
+    result->dual_row = keep.dual_row;
+    result->ipm_x = keep.ipm_x;
+    result->ipm_y = keep.ipm_y;
+    result->ipm_s = keep.ipm_s;
+    result->diagnostics = keep.diagnostics;
+    result->iterations += first_iterations;
+  } else {
+    const std::string msg = std::string(result->message) + " | Mehrotra starting point: " + second.message;
+    std::snprintf(result->message, sizeof(result->message), "%s", msg.c_str());
+  }
   return SOV_OK;
 }
 

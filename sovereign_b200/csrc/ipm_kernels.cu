@@ -325,7 +325,8 @@ __global__ void __launch_bounds__(kThreads) k_normal_cols(IpmDev d, const double
     for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) a += d.cval[p] * v[d.row_idx[p]];
     const double xj = fmax(d.x[j], 1e-16), sj = fmax(d.s[j], 1e-16);
     double w;
-    if (!d.qp) w = xj / sj;
+    if (d.start_system) w = 1.0;
+    else if (!d.qp) w = xj / sj;
     else w = 1.0 / (d.qdiag[j] + (d.free_col[j] ? 0.0 : sj / xj));
     tmp[j] = w * a;
   }
@@ -514,14 +515,42 @@ __global__ void __launch_bounds__(kThreads) k_hessian_r1(IpmDev d, int mode, dou
     v[j] = hessian_r1(d, mode, j, sigma_mu);
 }
 
-__global__ void __launch_bounds__(kThreads) k_rows_minus(IpmDev d, const double* v) {
+__global__ void __launch_bounds__(kThreads) k_rows_minus(IpmDev d, const double* v, const double* base) {
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
   for (int i = warp_row(); i < d.m; i += warps) {
     double acc = 0.0;
     for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * v[d.col_idx[p]];
     acc = warp_sum(acc);
-    if (lane == 0) d.z[i] = d.rp[i] - acc;
+    if (lane == 0) d.z[i] = (base ? base[i] : 0.0) - acc;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_mehrotra_xt(IpmDev d, double* xt) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double atdy = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+    xt[j] = 1.0 + atdy;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_mehrotra_r1(IpmDev d, const double* xt, double* r1) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double qx = 0.0;
+    if (d.q_coupled) {
+      for (int k = d.q_ptr[j]; k < d.q_ptr[j + 1]; ++k) qx += d.q_val[k] * xt[d.q_idx[k]];
+    } else {
+      qx = d.qdiag[j] * xt[j];
+    }
+    r1[j] = -(d.c[j] + qx);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_add_atz(IpmDev d, const double* r1, double* w) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+    double atz = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atz += d.cval[p] * d.z[d.row_idx[p]];
+    w[j] = r1[j] + atz;
   }
 }
 
@@ -650,8 +679,19 @@ void launch_hessian_r1(const IpmDev& d, int mode, double* v, cudaStream_t st) {
   SOV_LAUNCH_CHECK();
 }
 
-void launch_rows_minus(const IpmDev& d, const double* v, cudaStream_t st) {
-  k_rows_minus<<<row_blocks(d.m), kThreads, 0, st>>>(d, v);
+void launch_rows_minus(const IpmDev& d, const double* v, const double* base, cudaStream_t st) {
+  k_rows_minus<<<row_blocks(d.m), kThreads, 0, st>>>(d, v, base);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_mehrotra_r1(const IpmDev& d, double* xt, double* r1, cudaStream_t st) {
+  k_mehrotra_xt<<<blocks_for(d.n), kThreads, 0, st>>>(d, xt);
+  k_mehrotra_r1<<<blocks_for(d.n), kThreads, 0, st>>>(d, xt, r1);
+  SOV_LAUNCH_CHECK();
+}
+
+void launch_add_atz(const IpmDev& d, const double* r1, double* w, cudaStream_t st) {
+  k_add_atz<<<blocks_for(d.n), kThreads, 0, st>>>(d, r1, w);
   SOV_LAUNCH_CHECK();
 }
 

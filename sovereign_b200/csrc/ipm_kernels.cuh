@@ -41,6 +41,9 @@ struct IpmDev {
   const int* q_idx;
   const double* q_val;
   int q_coupled;
+  // 1 while the starting-point system (every column weight 1) is solved: the matrix-free normal
+  // operator of the mixed path then uses weight 1 too
+  int start_system;
   double comp_count;        // n (LP) or max(1, #bounded) (QP)
   double bnorm, cnorm, objective_offset, tau;
   // iterate and work vectors
@@ -100,12 +103,18 @@ void launch_form_normal(const IpmDev& d, const double* Y, int ld_y, double* M, i
                         cudaStream_t st);
 // r1 of the current mode into v (entries n.. untouched)
 void launch_hessian_r1(const IpmDev& d, int mode, double* v, cudaStream_t st);
-// z = rp - A v (v = H^-1 r1)
-void launch_rows_minus(const IpmDev& d, const double* v, cudaStream_t st);
+// z = base - A v (v = H^-1 r1; base = rp, or zero when null)
+void launch_rows_minus(const IpmDev& d, const double* v, const double* base, cudaStream_t st);
 // v = r1 + A'dy (dy = z)
 void launch_hessian_w(const IpmDev& d, int mode, double* v, cudaStream_t st);
 // dx = dxv (= H^-1 (r1 + A'dy)), ds, ratio tests and step lengths as launch_direction
 void launch_direction_dx(const IpmDev& d, int mode, const double* dxv, cudaStream_t st, int* launches);
+
+// Mehrotra's QP start (qp_interior_point.cpp:2891-2928), with dy of the start system in z:
+// xt = 1 + A'dy into xt, r1 = -(c + Q xt) into r1
+void launch_mehrotra_r1(const IpmDev& d, double* xt, double* r1, cudaStream_t st);
+// w = r1 + A'z
+void launch_add_atz(const IpmDev& d, const double* r1, double* w, cudaStream_t st);
 
 int reduction_blocks(int n);
 

@@ -43,6 +43,8 @@ BATCH_SPEC = dict(count=64, seed=3)          # transport_batch sample of the 409
 MULTICOMMODITY_SEEDS = [100, 101]            # MulticommodityFamily() instances
 QP_SPECS = [("small_qp_offdiagonal", []), ("convex_sequence_qp", [52, 3]), ("convex_sequence_qp", [202, 3]),
             ("convex_sequence_qp", [2002, 3]), ("reference_portfolio", [300, 12]), ("reference_portfolio", [60, 5])]
+QP_RETRY_SPECS = [("reference_portfolio", [60, 5], 8), ("reference_portfolio", [60, 5], 5),
+                  ("reference_portfolio", [300, 12], 10)]
 
 
 def build(name, args):
@@ -89,6 +91,13 @@ def main():
         key = f"{name}({','.join(map(str, args))})"
         qp[key] = dict(spec=[name, args], **summarize(oracle.solve(mdl, qp=True, kind="reference")))
         print("qp", key, qp[key]["objective"], flush=True)
+    # the default start stopped by a short iteration limit, then the retry from Mehrotra's start
+    for name, args, limit in QP_RETRY_SPECS:
+        mdl = build(name, args)
+        key = f"{name}({','.join(map(str, args))})@max{limit}"
+        qp[key] = dict(spec=[name, args], max_iterations=limit,
+                       **summarize(oracle.solve(mdl, qp=True, kind="reference", max_iterations=limit)))
+        print("qp", key, qp[key]["status"], qp[key]["iterations"], flush=True)
     with open(os.path.join(HERE, "qp_reference.json"), "w") as f:
         json.dump(qp, f, indent=1)
 

@@ -88,3 +88,20 @@ def test_coupled_hessian_known_answer():
     assert r.status_name == "OPTIMAL", r.message
     assert abs(r.primal[0] - 0.4) < 1e-7 and abs(r.primal[1] - 0.4) < 1e-7
     assert abs(r.objective_value + 0.4) < 1e-8
+
+
+@pytest.mark.parametrize("key", ["reference_portfolio(60,5)@max8", "reference_portfolio(300,12)@max10",
+                                 "reference_portfolio(60,5)@max5"])
+def test_mehrotra_retry_matches_reference(key):
+    # an iteration limit short enough to stop the default start: the reference then retries from
+    # Mehrotra's starting point and reports both attempts' iterations (qp_interior_point.cpp:3166-3180)
+    g = QP[key]
+    name, args = g["spec"]
+    r = QpInteriorPointSolver(QpInteriorPointOptions(max_iterations=g["max_iterations"])).solve(getattr(P, name)(*args))
+    assert r.status_name == g["status"], r.message
+    if g["status"] == "OPTIMAL":
+        assert r.iterations > g["max_iterations"]  # the second attempt ran
+        assert abs(r.iterations - g["iterations"]) <= 2
+        assert rel(r.objective_value, g["objective"]) < COUPLED_TOL
+    else:
+        assert "| Mehrotra starting point:" in r.message
