@@ -75,9 +75,12 @@ enum {
   SOV_FACTOR_AUTO = 0,   /* banded when the bandwidth is small, else dense */
   SOV_FACTOR_DENSE = 1,  /* dense m x m Cholesky (dense-Schur) */
   SOV_FACTOR_BANDED = 2, /* banded LDL^T in the natural row order */
-  SOV_FACTOR_XSPACE = 3  /* QP only: eliminate the slacks and factor Q + H + A'ZW^-1A over the structural
+  SOV_FACTOR_XSPACE = 3, /* QP only: eliminate the slacks and factor Q + H + A'ZW^-1A over the structural
                             columns (rows must all be inequalities, Q_jj > 0); exact Newton step, but
                             with FP64 iterates it stalls once slack weights exceed ~1e12 */
+  SOV_FACTOR_SPARSE = 4  /* sparse L D L' on the GPU after a minimum-degree order (NormalEquations'
+                            sparse path, interior_point.cpp:129-182, sparse_ldlt.cpp:19-223); AUTO takes
+                            it when the normal matrix is too large for the dense factorization */
 };
 
 /* One LP or convex QP in index form.

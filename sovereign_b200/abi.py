@@ -17,7 +17,7 @@ STATUS_NAMES = ["OPTIMAL", "FEASIBLE", "INFEASIBLE", "UNBOUNDED", "TIME_LIMIT", 
 # sovereign::ConstraintSense (types.hpp:12)
 LE, GE, EQ = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-FACTOR_AUTO, FACTOR_DENSE, FACTOR_BANDED, FACTOR_XSPACE = 0, 1, 2, 3
+FACTOR_AUTO, FACTOR_DENSE, FACTOR_BANDED, FACTOR_XSPACE, FACTOR_SPARSE = 0, 1, 2, 3, 4
 HISTORY_MAX = 128
 
 _dp = C.POINTER(C.c_double)

@@ -28,6 +28,8 @@
 #include "dense.cuh"
 #include "engine.hpp"
 #include "ipm_kernels.cuh"
+#include "sparse.hpp"
+#include "sparse_gpu.cuh"
 
 namespace sov {
 namespace {
@@ -237,7 +239,14 @@ class Engine {
   IpmDev dev_{};
 
   // factorization
-  enum Backend { kDense64, kDenseMixed, kBand } backend_ = kDense64;
+  enum Backend { kDense64, kDenseMixed, kBand, kSparse } backend_ = kDense64;
+  // sparse L D L' (kSparse): symbolic analysis on the host, numeric factor and solves on the GPU
+  SparseSymbolic sym_;
+  SparseFactor sparse_;
+  DevBuf<int64_t> sp_target_;
+  DevBuf<int> sp_ptr_, sp_col_;
+  DevBuf<double> sp_w_;
+  AssemblyDev spd_{};
   int mp_ = 0, nb_ = 0, kd_ = 0;
   AssemblyMap am_;
   DevBuf<int64_t> am_target_;
@@ -266,6 +275,7 @@ class Engine {
   static constexpr int kPcgSwitch = 12;
   static constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the default restart
   static constexpr int kCoupledMaxColumns = 16384;  // dense H of a coupled-Hessian QP: at most 2 GB
+  static constexpr int kDenseMaxOrder = 16384;      // dense normal matrix: at most 2 GB
   bool to_fp64_ = false;
   // x-space QP
   XSpace xs_;
@@ -344,18 +354,44 @@ void Engine::setup() {
   const bool auto_pick = opt_.factorization == SOV_FACTOR_AUTO || opt_.factorization == SOV_FACTOR_XSPACE;
   const bool want_band =
       !coupled_ && (opt_.factorization == SOV_FACTOR_BANDED || (auto_pick && kd_ <= kBandMax && order_ > 256));
-  if (want_band) {
+  // sparse L D L' when asked for, or when the normal matrix is beyond the dense factorization
+  const bool want_sparse = !want_band && !xspace_ && !coupled_ &&
+                           (opt_.factorization == SOV_FACTOR_SPARSE ||
+                            (opt_.factorization == SOV_FACTOR_AUTO && order_ > kDenseMaxOrder));
+  if (opt_.factorization == SOV_FACTOR_SPARSE && (xspace_ || coupled_))
+    throw std::runtime_error("the sparse factorization takes the y-space normal equations of an LP or a "
+                             "separable QP");
+  if (want_sparse) {
+    if (!sparse_analyze(f_, 0, sym_))
+      throw std::runtime_error("sparse L D L' of the order-" + std::to_string(order_) +
+                               " normal matrix needs more than " + std::to_string(kMaxUpdates) +
+                               " rank-1 update terms");
+    backend_ = kSparse;
+  } else if (want_band) {
     if (kd_ > kBandMax) throw std::runtime_error("banded factorization requested but half-bandwidth " +
                                                  std::to_string(kd_) + " exceeds " + std::to_string(kBandMax));
     backend_ = kBand;
   } else {
-    if (order_ > 16384) throw std::runtime_error("normal matrix of order " + std::to_string(order_) +
+    if (order_ > kDenseMaxOrder) throw std::runtime_error("normal matrix of order " + std::to_string(order_) +
                                                  " is too large for the dense factorization (band width " +
                                                  std::to_string(kd_) + ")");
     // the x-space system has no matrix-free PCG operator: it is factored in FP64
     backend_ = (opt_.precision == SOV_PRECISION_MIXED && !xspace_ && !coupled_) ? kDenseMixed : kDense64;
   }
-  if (backend_ == kBand) {
+  if (backend_ == kSparse) {
+    std::vector<int64_t> tg(sym_.asm_target.begin(), sym_.asm_target.end());
+    sp_target_.alloc(tg.size());
+    sp_target_.upload(tg.data(), tg.size(), st_);
+    sp_ptr_.alloc(sym_.asm_ptr.size());
+    sp_ptr_.upload(sym_.asm_ptr.data(), sym_.asm_ptr.size(), st_);
+    sp_col_.alloc(sym_.asm_col.size());
+    sp_col_.upload(sym_.asm_col.data(), sym_.asm_col.size(), st_);
+    sp_w_.alloc(sym_.asm_w.size());
+    sp_w_.upload(sym_.asm_w.data(), sym_.asm_w.size(), st_);
+    spd_ = AssemblyDev{sp_target_.p, sp_ptr_.p, sp_col_.p, sp_w_.p, nullptr, static_cast<int>(tg.size())};
+    z_.alloc(order_);
+    z_.zero(st_);
+  } else if (backend_ == kBand) {
     am_ = xspace_ ? build_assembly_xspace_band(f_, xs_) : build_assembly_band(f_, kd_);
     band_.alloc(static_cast<size_t>(kBandMax + 1) * order_);
     band_.zero(st_);
@@ -417,6 +453,10 @@ void Engine::setup() {
     sigma_.upload(xs_.sigma.data(), m, st_);
     tr_.alloc(m);
     dyv_.alloc(m);
+  }
+  if (backend_ == kSparse) {
+    IpmScalars* sc0 = sc_.p;
+    sparse_.upload(sym_, &sc0->drops, &sc0->fail, 1e-13, st_);
   }
   am_target_.alloc(am_.target.size());
   am_target_.upload(am_.target.data(), am_.target.size(), st_);
@@ -500,6 +540,15 @@ void Engine::assemble_and_factor(int mode) {
   if (to_fp64_ && backend_ == kDenseMixed) backend_ = kDense64;
   // x-space: K = A_x' Theta A_x (+ diag Q + H after assembly); start system: Theta = 1, diag 1
   const int amode = xspace_ ? (mode == kWeightOnes ? kWeightOnes : kWeightTheta) : mode;
+  if (backend_ == kSparse) {
+    SOV_CUDA(cudaMemsetAsync(sparse_.values(), 0, sizeof(double) * (order_ + sparse_.nnz_l()), st_));
+    launch_assemble<double>(spd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, sparse_.values(), sparse_.assembled_diag(),
+                            order_, 0, st_);
+    sparse_.factor(st_, &launches_);
+    launches_ += 2;
+    if (stats_) stats_->factor_flops += sym_.flops;
+    return;
+  }
   if (backend_ == kBand) {
     launch_assemble<double>(amd_, x_.p, s_.p, qdiag_.p, free_.p, amode, reg, band_.p, diag_.p, order_, -order_, st_);
     if (xspace_) launch_xspace_diag(dev_, mode == kWeightOnes ? 0 : 1, band_.p, -1, diag_.p, st_);
@@ -623,6 +672,10 @@ bool Engine::newton_solve() {
     band_solve(bandsys_, z_.p, st_, &launches_);
     return true;
   }
+  if (backend_ == kSparse) {
+    sparse_.solve(z_.p, st_, &launches_);
+    return true;
+  }
   if (backend_ == kDense64) {
     dense_solve<double>(ds64_, z_.p, epoch_, err_.p, st_, &launches_);
     return true;
@@ -689,7 +742,10 @@ std::string Engine::describe() const {
                   f_.n, order_, order_);
     return buf;
   }
-  if (backend_ == kBand)
+  if (backend_ == kSparse)
+    std::snprintf(buf, sizeof buf, "sparse LDL^T on the GPU with minimum-degree ordering (order %d, nnz(L) = %lld, %d levels)",
+                  order_, sym_.nnz_l, sym_.levels());
+  else if (backend_ == kBand)
     std::snprintf(buf, sizeof buf, "%sbanded LDL^T on the GPU (order %d, half-bandwidth %d)", space, order_, kd_);
   else if (backend_ == kDense64)
     std::snprintf(buf, sizeof buf, "%sdense Cholesky on the GPU, FP64 (%d x %d)", space, order_, order_);

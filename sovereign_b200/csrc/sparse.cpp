@@ -134,6 +134,8 @@ bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& s)
     const double cc = static_cast<double>(cols[k].size());
     s.flops += cc * cc;
   }
+  // the update schedule below holds one entry per rank-1 term: bounded (3.2 GB at the limit)
+  if (s.flops > 2.0 * kMaxUpdates) return false;
   // heights and level schedule
   std::vector<int> height(m, 0);
   int hmax = 0;

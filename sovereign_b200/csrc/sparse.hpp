@@ -33,7 +33,11 @@ struct SparseSymbolic {
   int levels() const { return static_cast<int>(lvl_ptr.size()) - 1; }
 };
 
-// Returns false when the predicted fill exceeds fill_limit entries (0 = no limit).
+// rank-1 update terms the schedule may hold (16 bytes each on the device)
+constexpr double kMaxUpdates = 2e8;
+
+// Returns false when the predicted fill exceeds fill_limit entries (0 = no limit) or the update
+// schedule would exceed kMaxUpdates terms.
 bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& out);
 
 }  // namespace sov

@@ -1,0 +1,181 @@
+// sparse_gpu.cu -- numeric sparse L D L' and its solves on the GPU (see sparse_gpu.cuh).
+#include "sparse_gpu.cuh"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <stdexcept>
+
+#include "common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace sov {
+namespace {
+
+constexpr int kSparseThreads = 256;
+
+__global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
+  cg::grid_group g = cg::this_grid();
+  const int rank = static_cast<int>(g.thread_rank()), size = static_cast<int>(g.size());
+  int drops = 0, bad = 0;
+  for (int h = 0; h < s.levels; ++h) {
+    // pivots of the level's columns
+    for (int q = s.lvl_ptr[h] + rank; q < s.lvl_ptr[h + 1]; q += size) {
+      const int k = s.lvl_col[q];
+      const double p = s.V[k];
+      const bool finite = fabs(p) <= 1.7976931348623157e308;
+      const bool drop = !(finite && p > s.drop_tol * fabs(s.diag[k]));
+      bad |= !finite;
+      drops += drop;
+      s.inv_d[k] = 1.0 / (drop ? 1e128 : p);
+    }
+    g.sync();
+    // their rank-1 updates, one destination per thread
+    for (int r = s.run_lvl[h] + rank; r < s.run_lvl[h + 1]; r += size) {
+      double acc = 0.0;
+      for (int u = s.run_ptr[r]; u < s.run_ptr[r + 1]; ++u)
+        acc += s.V[s.m + s.up_a[u]] * s.V[s.m + s.up_b[u]] * s.inv_d[s.up_col[u]];
+      s.V[s.run_dst[r]] -= acc;
+    }
+    g.sync();
+  }
+  if (drops) atomicAdd(s.drop_count, drops);
+  if (bad) atomicExch(s.fail, 1);
+}
+
+// L D L' x = z: forward y_k = z_k - sum_j L~_kj (1/D_j) y_j (row k of L, descendants: earlier
+// levels), backward x_k = (1/D_k) (y_k - sum_i L~_ik x_i) (column k, ancestors: later levels)
+__global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, double* z) {
+  cg::grid_group g = cg::this_grid();
+  const int rank = static_cast<int>(g.thread_rank()), size = static_cast<int>(g.size());
+  for (int k = rank; k < s.m; k += size) s.work[k] = z[s.perm[k]];
+  g.sync();
+  for (int h = 0; h < s.levels; ++h) {
+    for (int q = s.lvl_ptr[h] + rank; q < s.lvl_ptr[h + 1]; q += size) {
+      const int k = s.lvl_col[q];
+      double acc = s.work[k];
+      for (int t = s.row_ptr[k]; t < s.row_ptr[k + 1]; ++t)
+        acc -= s.V[s.m + s.row_pos[t]] * s.inv_d[s.row_col[t]] * s.work[s.row_col[t]];
+      s.work[k] = acc;
+    }
+    g.sync();
+  }
+  for (int h = s.levels - 1; h >= 0; --h) {
+    for (int q = s.lvl_ptr[h] + rank; q < s.lvl_ptr[h + 1]; q += size) {
+      const int k = s.lvl_col[q];
+      double acc = s.work[k];
+      for (int p = s.lp[k]; p < s.lp[k + 1]; ++p) acc -= s.V[s.m + p] * s.work[s.li[p]];
+      s.work[k] = acc * s.inv_d[k];
+    }
+    g.sync();
+  }
+  for (int k = rank; k < s.m; k += size) z[s.perm[k]] = s.work[k];
+}
+
+template <class T>
+T* put(std::vector<void*>& bufs, const std::vector<T>& h, cudaStream_t st) {
+  T* p = nullptr;
+  SOV_CUDA(cudaMalloc(&p, sizeof(T) * std::max<size_t>(1, h.size())));
+  bufs.push_back(p);
+  if (!h.empty()) SOV_CUDA(cudaMemcpyAsync(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st));
+  return p;
+}
+
+}  // namespace
+
+void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, double drop_tol, cudaStream_t st) {
+  release();
+  const int m = s.m, levels = s.levels();
+  nnz_l_ = s.nnz_l;
+  // updates of each level grouped by destination (stable: a destination's terms in schedule order)
+  std::vector<int> run_lvl(levels + 1, 0), run_ptr(1, 0), run_dst, up_col, up_a, up_b;
+  std::vector<int> order;
+  for (int h = 0; h < levels; ++h) {
+    const int u0 = s.pair_ptr[h], u1 = s.pair_ptr[h + 1];
+    order.resize(u1 - u0);
+    std::iota(order.begin(), order.end(), u0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return s.pairs[4 * x + 3] < s.pairs[4 * y + 3]; });
+    for (size_t q = 0; q < order.size(); ++q) {
+      const int u = order[q];
+      if (q == 0 || s.pairs[4 * u + 3] != run_dst.back()) {
+        if (q > 0) run_ptr.push_back(static_cast<int>(up_col.size()));
+        run_dst.push_back(s.pairs[4 * u + 3]);
+      }
+      up_col.push_back(s.pairs[4 * u]);
+      up_a.push_back(s.pairs[4 * u + 1]);
+      up_b.push_back(s.pairs[4 * u + 2]);
+    }
+    if (!order.empty()) run_ptr.push_back(static_cast<int>(up_col.size()));
+    run_lvl[h + 1] = static_cast<int>(run_dst.size());
+  }
+  // rows of L for the forward solve
+  std::vector<int> row_ptr(m + 1, 0), row_pos(s.li.size()), row_col(s.li.size());
+  for (int i : s.li) row_ptr[i + 1]++;
+  for (int i = 0; i < m; ++i) row_ptr[i + 1] += row_ptr[i];
+  {
+    std::vector<int> fill(row_ptr.begin(), row_ptr.end() - 1);
+    for (int k = 0; k < m; ++k)
+      for (int p = s.lp[k]; p < s.lp[k + 1]; ++p) {
+        const int t = fill[s.li[p]]++;
+        row_pos[t] = p;
+        row_col[t] = k;
+      }
+  }
+  d_.m = m;
+  d_.levels = levels;
+  std::vector<double> zeros;
+  d_.V = put(bufs_, std::vector<double>(m + s.li.size(), 0.0), st);
+  d_.diag = put(bufs_, std::vector<double>(m, 0.0), st);
+  d_.inv_d = put(bufs_, std::vector<double>(m, 0.0), st);
+  d_.work = put(bufs_, std::vector<double>(m, 0.0), st);
+  d_.perm = put(bufs_, s.perm, st);
+  d_.lp = put(bufs_, s.lp, st);
+  d_.li = put(bufs_, s.li, st);
+  d_.lvl_ptr = put(bufs_, s.lvl_ptr, st);
+  d_.lvl_col = put(bufs_, s.lvl_col, st);
+  d_.run_lvl = put(bufs_, run_lvl, st);
+  d_.run_ptr = put(bufs_, run_ptr, st);
+  d_.run_dst = put(bufs_, run_dst, st);
+  d_.up_col = put(bufs_, up_col, st);
+  d_.up_a = put(bufs_, up_a, st);
+  d_.up_b = put(bufs_, up_b, st);
+  d_.row_ptr = put(bufs_, row_ptr, st);
+  d_.row_pos = put(bufs_, row_pos, st);
+  d_.row_col = put(bufs_, row_col, st);
+  d_.drop_count = drop_count;
+  d_.fail = fail;
+  d_.drop_tol = drop_tol;
+  SOV_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+  int dev = 0, sms = 0, per_sm = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  SOV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sparse_factor, kSparseThreads, 0));
+  int per_sm2 = 0;
+  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_sparse_solve, kSparseThreads, 0));
+  grid_ = std::max(1, sms * std::max(1, std::min(per_sm, per_sm2)));
+}
+
+void SparseFactor::release() {
+  for (void* p : bufs_) cudaFree(p);
+  bufs_.clear();
+  d_ = SparseDev{};
+}
+
+void SparseFactor::factor(cudaStream_t st, int* launches) {
+  SparseDev d = d_;
+  void* args[] = {&d};
+  SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_factor, dim3(grid_), dim3(kSparseThreads), args, 0, st));
+  if (launches) *launches += 1;
+}
+
+void SparseFactor::solve(double* z, cudaStream_t st, int* launches) {
+  SparseDev d = d_;
+  void* args[] = {&d, &z};
+  SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_solve, dim3(grid_), dim3(kSparseThreads), args, 0, st));
+  if (launches) *launches += 1;
+}
+
+}  // namespace sov

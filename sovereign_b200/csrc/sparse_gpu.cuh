@@ -1,0 +1,67 @@
+// sparse_gpu.cuh -- numeric sparse L D L' of the normal matrix on the GPU, on the host's symbolic
+// analysis (sparse.hpp: minimum-degree order, column patterns, elimination tree, level schedule).
+//
+// Storage V = [D | L~] in the elimination order: D_k at V[k], the strict-lower entries of column k
+// (rows li[lp[k]..lp[k+1])) at V[m + p], kept unscaled (L~ = L D), so an update is
+// a_ab -= L~_ak L~_bk / D_k. Columns of one level of the elimination tree have no ancestor relation:
+// a level's pivots are taken together, then its rank-1 updates are applied, grouped per destination
+// (each destination's contributions summed by one thread in a fixed order: deterministic). One
+// cooperative launch per factorization and per solve, a grid barrier between levels.
+// Pivot rule of the reference's sparse LDL' (sparse_ldlt.cpp:165-173): a pivot at most
+// drop_tol * |assembled diagonal| (or not finite) marks a dependent row, D = 1e128.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "sparse.hpp"
+
+namespace sov {
+
+struct SparseDev {
+  int m, levels;
+  double* V;            // m + nnz(L)
+  double* diag;         // m: assembled diagonal (elimination order), the pivot reference
+  double* inv_d;        // m
+  double* work;         // m: permuted right-hand side / solution
+  const int* perm;      // perm[k] = original row of the k-th pivot
+  const int* lp;        // m + 1
+  const int* li;        // nnz(L)
+  const int* lvl_ptr;   // levels + 1
+  const int* lvl_col;   // m
+  const int* run_lvl;   // levels + 1: first destination run of each level
+  const int* run_ptr;   // runs + 1: first update of each run
+  const int* run_dst;   // runs: index into V
+  const int* up_col;    // updates: pivot column k
+  const int* up_a;      // updates: position of l_ak
+  const int* up_b;      // updates: position of l_bk
+  const int* row_ptr;   // m + 1: entries of L in row k (forward solve)
+  const int* row_pos;   // their positions in L
+  const int* row_col;   // their columns
+  int* drop_count;
+  int* fail;
+  double drop_tol;
+};
+
+// Device copies of the schedule; owns its buffers.
+class SparseFactor {
+ public:
+  void upload(const SparseSymbolic& s, int* drop_count, int* fail, double drop_tol, cudaStream_t st);
+  void release();
+  ~SparseFactor() { release(); }
+  const SparseDev& dev() const { return d_; }
+  double* values() const { return d_.V; }
+  double* assembled_diag() const { return d_.diag; }
+  long long nnz_l() const { return nnz_l_; }
+  void factor(cudaStream_t st, int* launches);
+  void solve(double* z, cudaStream_t st, int* launches);  // z in the original row order, in place
+
+ private:
+  SparseDev d_{};
+  std::vector<void*> bufs_;
+  long long nnz_l_ = 0;
+  int grid_ = 1;
+};
+
+}  // namespace sov

@@ -44,7 +44,8 @@ class InteriorPointOptions:
         o.pcg_max_iterations = self.pcg_max_iterations
         o.ipm_iterate_at = self.ipm_iterate_at
         mode = os.environ.get("SOVEREIGN_IPM_NORMAL_EQUATIONS", "auto")  # interior_point.cpp:132-133
-        o.factorization = {"dense": abi.FACTOR_DENSE, "banded": abi.FACTOR_BANDED}.get(mode, abi.FACTOR_AUTO)
+        o.factorization = {"dense": abi.FACTOR_DENSE, "banded": abi.FACTOR_BANDED,
+                           "sparse": abi.FACTOR_SPARSE}.get(mode, abi.FACTOR_AUTO)
         return o
 
 

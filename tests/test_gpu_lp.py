@@ -42,6 +42,21 @@ def test_fp64_matches_reference(key):
     assert "Normal equations" in r.message
 
 
+@pytest.mark.parametrize("key", ["reference_staircase(8,40)", "transport(50,50,0)", "reference_transport(60)",
+                                 "random_sparse_lp(100,500,8,1)", "bounded_lp_example()", "multicommodity(100)"])
+def test_sparse_factorization_matches_reference(key, monkeypatch):
+    # the reference's sparse path (SOVEREIGN_IPM_NORMAL_EQUATIONS=sparse): minimum-degree order on the
+    # host, numeric L D L' and its solves on the GPU level by level in the elimination tree
+    monkeypatch.setenv("SOVEREIGN_IPM_NORMAL_EQUATIONS", "sparse")
+    g = LP[key]
+    r = InteriorPointSolver().solve(model_of(g["spec"]), with_diag=True)
+    assert r.status_name == "OPTIMAL", r.message
+    assert "sparse LDL^T on the GPU" in r.message
+    assert rel(r.objective_value, g["objective"]) < TOL
+    assert r.primal_residual < 1e-9 and r.dual_residual < 1e-9 and r.duality_gap < 1e-9
+    assert r.iterations <= g["iterations"] + 1
+
+
 @pytest.mark.parametrize("key", ["transport(50,50,0)", "random_sparse_lp(200,1000,8,2)", "reference_transport(40)",
                                  "multicommodity(101)"])
 def test_mixed_precision_matches_reference(key):
