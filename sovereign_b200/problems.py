@@ -83,6 +83,34 @@ def transport_batch(count: int, seed: int, lo: int = 10, hi: int = 60) -> list[M
     return [transport(int(a), int(b), seed * 1_000_003 + k) for k, (a, b) in enumerate(sizes)]
 
 
+def grid_network_lp(g: int) -> Model:
+    """Min-cost flow on a g x g grid: both directions of every edge an arc (cost 1..10 by a fixed
+    rule), 5 units from the corner node 0 to the opposite corner, conservation rows (all Eq). The
+    normal matrix is the grid Laplacian: order g^2, sparse after a minimum-degree order."""
+    m = g * g
+    rows, vals, cost = [], [], []
+    for i in range(g):
+        for j in range(g):
+            a = i * g + j
+            for di, dj in ((1, 0), (0, 1)):
+                ni, nj = i + di, j + dj
+                if ni >= g or nj >= g:
+                    continue
+                b = ni * g + nj
+                for d in (0, 1):
+                    frm, to = (b, a) if d else (a, b)
+                    r0, r1 = min(frm, to), max(frm, to)
+                    rows += [r0, r1]
+                    vals += [-1.0 if r0 == frm else 1.0, -1.0 if r1 == frm else 1.0]
+                    cost.append(1.0 + ((a * 7 + b * 3 + d) % 10))
+    n = len(cost)
+    col_ptr = np.arange(0, 2 * n + 1, 2, dtype=np.int32)
+    rhs = np.zeros(m)
+    rhs[0], rhs[m - 1] = -5.0, 5.0
+    return _lp(n, m, col_ptr, np.array(rows, dtype=np.int32), np.array(vals), np.array(cost), rhs,
+               np.full(m, EQ, dtype=np.int8), f"grid_network_{g}x{g}")
+
+
 def random_sparse_lp(m: int, n: int, k: int, seed: int) -> Model:
     rng = np.random.Generator(np.random.PCG64(seed))
     rows = np.argsort(rng.random((n, m)), axis=1)[:, :k] if m <= 4096 else \

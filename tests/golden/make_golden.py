@@ -37,7 +37,7 @@ LP_SPECS = [
     ("transport", [50, 50, 0]), ("transport", [50, 50, 1]), ("transport", [50, 50, 2]),
     ("transport", [13, 37, 5]), ("transport", [60, 10, 7]),
     ("random_sparse_lp", [100, 500, 8, 1]), ("random_sparse_lp", [200, 1000, 8, 2]),
-    ("random_sparse_lp", [500, 2500, 8, 1]),
+    ("random_sparse_lp", [500, 2500, 8, 1]), ("grid_network_lp", [130]),
 ]
 BATCH_SPEC = dict(count=64, seed=3)          # transport_batch sample of the 4096-LP workload
 MULTICOMMODITY_SEEDS = [100, 101]            # MulticommodityFamily() instances

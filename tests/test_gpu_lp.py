@@ -213,3 +213,13 @@ def test_batch_warm_start_saves_iterations():
     assert sum(w.diagnostics["warm_start_used"] for w in warm) >= len(models) - 2
     assert not any(c.diagnostics["warm_start_used"] for c in cold)
     assert np.mean([w.iterations for w in warm]) <= np.mean([c.iterations for c in cold]) - 3
+
+
+def test_large_network_takes_the_sparse_path():
+    # a 130 x 130 grid min-cost flow: normal matrix of order 16900, past the dense factorization, so
+    # AUTO takes the sparse L D L' (the reference: sparse LDL^T, nnz(L) = 409164)
+    g = LP["grid_network_lp(130)"]
+    r = InteriorPointSolver().solve(P.grid_network_lp(130))
+    assert r.status_name == "OPTIMAL", r.message
+    assert "sparse LDL^T on the GPU" in r.message
+    assert rel(r.objective_value, g["objective"]) < TOL
