@@ -5,7 +5,7 @@
 // (rows li[lp[k]..lp[k+1])) at V[m + p], kept unscaled (L~ = L D), so an update is
 // a_ab -= L~_ak L~_bk / D_k. Columns of one level of the elimination tree have no ancestor relation:
 // a level's pivots are taken together, then its rank-1 updates are applied, grouped per destination
-// (each destination's contributions summed by one thread in a fixed order: deterministic). One
+// (each destination's contributions summed by one warp in a fixed order: deterministic). One
 // cooperative launch per factorization and per solve, a grid barrier between levels.
 // Pivot rule of the reference's sparse LDL' (sparse_ldlt.cpp:165-173): a pivot at most
 // drop_tol * |assembled diagonal| (or not finite) marks a dependent row, D = 1e128.
