@@ -272,6 +272,14 @@ int64_t sov_mlp_param_count(const sov_mlp* mlp);
 int sov_mlp_get_params(const sov_mlp* mlp, float* params, int64_t count);
 int sov_mlp_set_params(sov_mlp* mlp, const float* params, int64_t count);
 int sov_mlp_forward(sov_mlp* mlp, const float* x, int32_t batch, float* y);
+/* Warm starts for a batch in one call, normalization and decoding on the GPU: the network input is
+ * (params - in_mean) / in_std (FP64, rounded to FP32); its output o, with 2 n_ipm + m_ipm columns
+ * (log x, y, log s normalized), becomes v = o * out_std + out_mean, and x = max(exp(clip(v, -40,
+ * 40)), delta), y = v, s likewise, into x (batch x n_ipm), y (batch x m_ipm), s (batch x n_ipm),
+ * row-major host arrays. */
+int sov_mlp_predict_start(sov_mlp* mlp, const double* params, int32_t batch, const double* in_mean,
+                          const double* in_std, const double* out_mean, const double* out_std, int32_t n_ipm,
+                          int32_t m_ipm, double delta, double* x, double* y, double* s);
 /* loss = mean((f(x) - t)^2); grad (param_count floats, or NULL) = its gradient */
 int sov_mlp_loss_grad(sov_mlp* mlp, const float* x, const float* t, int32_t batch, double* loss, float* grad);
 /* epochs of shuffled mini-batches over count samples; final_loss = mean loss of the last epoch */

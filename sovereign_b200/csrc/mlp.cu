@@ -207,6 +207,39 @@ __global__ void k_gather_rows(const float* src, const int* idx, int rows, int co
   }
 }
 
+// network input from raw parameters: (p - mean) / std in FP64, rounded to FP32
+__global__ void k_normalize_in(const double* __restrict__ p, const double* __restrict__ mean,
+                               const double* __restrict__ sd, long long count, int cols, float* __restrict__ out) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(i % cols);
+    out[i] = static_cast<float>((p[i] - mean[c]) / sd[c]);
+  }
+}
+
+// warm start from the network output o (log x, y, log s normalized): v = o * std + mean in FP64,
+// x = max(exp(clip(v, -40, 40)), delta) on the first n columns, y = v on the next m, s like x on
+// the last n; written as three row-major arrays
+__global__ void k_decode_start(const float* __restrict__ o, const double* __restrict__ mean,
+                               const double* __restrict__ sd, long long rows, int n, int m, double delta,
+                               double* __restrict__ x, double* __restrict__ y, double* __restrict__ s) {
+  const int cols = 2 * n + m;
+  const long long count = rows * cols;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long r = i / cols;
+    const int c = static_cast<int>(i % cols);
+    const double v = static_cast<double>(o[i]) * sd[c] + mean[c];
+    if (c < n) {
+      x[r * n + c] = fmax(exp(fmin(fmax(v, -40.0), 40.0)), delta);
+    } else if (c < n + m) {
+      y[r * m + (c - n)] = v;
+    } else {
+      s[r * n + (c - n - m)] = fmax(exp(fmin(fmax(v, -40.0), 40.0)), delta);
+    }
+  }
+}
+
 template <class T>
 struct Buf {
   T* p = nullptr;
@@ -234,6 +267,7 @@ struct Mlp {
   std::vector<Buf<float>> dact;  // gradients of the activations
   Buf<float> target;
   Buf<double> part;
+  Buf<double> raw_in, norm, start;  // warm-start prediction: parameters, normalizers, decoded start
   Buf<int> err;
   long long step = 0;
   cudaStream_t st = nullptr;
@@ -376,6 +410,45 @@ int sov_mlp_forward(sov_mlp* h, const float* x, int32_t batch, float* y) {
     m->forward(batch);
     SOV_CUDA(cudaMemcpyAsync(y, m->act.back().p, sizeof(float) * batch * m->dims.back(), cudaMemcpyDeviceToHost,
                              m->st));
+    SOV_CUDA(cudaStreamSynchronize(m->st));
+    return SOV_OK;
+  } catch (const std::exception&) {
+    return SOV_E_CUDA;
+  }
+}
+
+int sov_mlp_predict_start(sov_mlp* h, const double* params, int32_t batch, const double* in_mean,
+                          const double* in_std, const double* out_mean, const double* out_std, int32_t n_ipm,
+                          int32_t m_ipm, double delta, double* x, double* y, double* s) {
+  auto m = reinterpret_cast<Mlp*>(h);
+  if (!m || !params || !in_mean || !in_std || !out_mean || !out_std || !x || !y || !s || batch <= 0 || n_ipm < 0 ||
+      m_ipm < 0 || 2 * n_ipm + m_ipm != m->dims.back())
+    return SOV_E_ARGUMENT;
+  try {
+    const int n_in = m->dims[0], n_out = m->dims.back();
+    m->ensure_batch(batch);
+    const size_t cnt_in = static_cast<size_t>(batch) * n_in, cnt_out = static_cast<size_t>(batch) * n_out;
+    if (m->raw_in.n < cnt_in) m->raw_in.alloc(cnt_in);
+    if (m->norm.n < static_cast<size_t>(2 * (n_in + n_out))) m->norm.alloc(2 * (n_in + n_out));
+    if (m->start.n < cnt_out) m->start.alloc(cnt_out);
+    double* nm = m->norm.p;
+    SOV_CUDA(cudaMemcpyAsync(m->raw_in.p, params, sizeof(double) * cnt_in, cudaMemcpyHostToDevice, m->st));
+    SOV_CUDA(cudaMemcpyAsync(nm, in_mean, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
+    SOV_CUDA(cudaMemcpyAsync(nm + n_in, in_std, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
+    SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in, out_mean, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
+    SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in + n_out, out_std, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
+    sov::k_normalize_in<<<1184, 256, 0, m->st>>>(m->raw_in.p, nm, nm + n_in, static_cast<long long>(cnt_in), n_in,
+                                                m->act[0].p);
+    m->forward(batch);
+    double* dx = m->start.p;
+    double* dy = dx + static_cast<size_t>(batch) * n_ipm;
+    double* ds = dy + static_cast<size_t>(batch) * m_ipm;
+    sov::k_decode_start<<<1184, 256, 0, m->st>>>(m->act.back().p, nm + 2 * n_in, nm + 2 * n_in + n_out, batch, n_ipm,
+                                                m_ipm, delta, dx, dy, ds);
+    SOV_CUDA(cudaGetLastError());
+    SOV_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * batch * n_ipm, cudaMemcpyDeviceToHost, m->st));
+    SOV_CUDA(cudaMemcpyAsync(y, dy, sizeof(double) * batch * m_ipm, cudaMemcpyDeviceToHost, m->st));
+    SOV_CUDA(cudaMemcpyAsync(s, ds, sizeof(double) * batch * n_ipm, cudaMemcpyDeviceToHost, m->st));
     SOV_CUDA(cudaStreamSynchronize(m->st));
     return SOV_OK;
   } catch (const std::exception&) {

@@ -139,10 +139,14 @@ class WarmStart:
         return self.mlp.train(self.fin.apply(x), self.fout.apply(t), epochs, batch, lr, seed)
 
     def predict(self, params: np.ndarray, delta: float = 1e-6) -> list[tuple[np.ndarray, np.ndarray, np.ndarray]]:
-        """Warm starts floored into the interior: x, s >= delta (scaled problem units)."""
-        out = self.fout.invert(self.mlp.forward(self.fin.apply(np.atleast_2d(params))).astype(np.float64))
-        n, m = self.n_ipm, self.m_ipm
-        xs = np.maximum(np.exp(np.clip(out[:, :n], -40, 40)), delta)
-        ys = np.ascontiguousarray(out[:, n:n + m])
-        ss = np.maximum(np.exp(np.clip(out[:, n + m:], -40, 40)), delta)
-        return [(xs[k], ys[k], ss[k]) for k in range(out.shape[0])]
+        """Warm starts floored into the interior: x, s >= delta (scaled problem units). Normalization,
+        the network and the decoding (x = max(exp(clip(log x, -40, 40)), delta), likewise s) run on
+        the GPU in one call (sov_mlp_predict_start)."""
+        p = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+        n, m, b = self.n_ipm, self.m_ipm, p.shape[0]
+        xs, ys, ss = np.empty((b, n)), np.empty((b, m)), np.empty((b, n))
+        f = [np.ascontiguousarray(v, dtype=np.float64) for v in (self.fin.mean, self.fin.std, self.fout.mean,
+                                                                  self.fout.std)]
+        check(load().sov_mlp_predict_start(self.mlp.h, p.ctypes.data, b, *(v.ctypes.data for v in f), n, m, delta,
+                                           xs.ctypes.data, ys.ctypes.data, ss.ctypes.data))
+        return [(xs[k], ys[k], ss[k]) for k in range(b)]

@@ -7,7 +7,7 @@ import pytest
 from oracle import mlp_oracle
 from sovereign_b200 import problems as P
 from sovereign_b200.ipm import InteriorPointOptions
-from sovereign_b200.warmstart import Mlp, WarmStart, solve_many
+from sovereign_b200.warmstart import Mlp, Normalizer, WarmStart, solve_many
 
 pytestmark = pytest.mark.gpu
 
@@ -69,3 +69,22 @@ def test_warm_start_saves_iterations_on_a_parametric_family():
     info = (gain, used, [c.iterations for c in cold], [w.iterations for w in warm])
     assert gain > 0.5, info
     assert used >= len(test) // 2, info
+
+
+def test_predict_start_matches_host_decoding():
+    # sov_mlp_predict_start (normalization, network, decoding on the GPU) against the network's
+    # plain forward pass decoded on the host with the same formulas
+    rng = np.random.default_rng(3)
+    n_param, n, m = 24, 30, 11
+    ws = WarmStart(n_param, n, m, hidden=64, layers=2, seed=1)
+    ws.fin = Normalizer(rng.normal(size=n_param), rng.uniform(0.5, 2.0, size=n_param))
+    ws.fout = Normalizer(rng.normal(size=2 * n + m), rng.uniform(0.5, 2.0, size=2 * n + m))
+    params = rng.normal(size=(37, n_param))
+    got = ws.predict(params)
+    out = ws.fout.invert(ws.mlp.forward(ws.fin.apply(params)).astype(np.float64))
+    xs = np.maximum(np.exp(np.clip(out[:, :n], -40, 40)), 1e-6)
+    ss = np.maximum(np.exp(np.clip(out[:, n + m:], -40, 40)), 1e-6)
+    for k in range(len(params)):
+        np.testing.assert_allclose(got[k][0], xs[k], rtol=1e-12)
+        np.testing.assert_allclose(got[k][1], out[k, n:n + m], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(got[k][2], ss[k], rtol=1e-12)
