@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <set>
+#include <thread>
 #include <utility>
 
 namespace sov {
@@ -151,19 +152,46 @@ bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& s)
     std::vector<int> fill(s.lvl_ptr.begin(), s.lvl_ptr.end() - 1);
     for (int k = 0; k < m; ++k) s.lvl_col[fill[height[k]]++] = k;
   }
-  // rank-1 updates per level
+  // rank-1 updates per level, column by column in level order; each column's block of updates is
+  // sized up front, so the blocks are filled on several host threads
+  std::vector<std::size_t> at(m + 1, 0);
+  for (int q = 0; q < m; ++q) {
+    const std::size_t nk = static_cast<std::size_t>(s.lp[s.lvl_col[q] + 1] - s.lp[s.lvl_col[q]]);
+    at[q + 1] = at[q] + nk * (nk + 1) / 2;
+  }
+  s.pairs.resize(4 * at[m]);
   s.pair_ptr.assign(hmax + 2, 0);
-  for (int h = 0; h <= hmax; ++h) {
-    for (int q = s.lvl_ptr[h]; q < s.lvl_ptr[h + 1]; ++q) {
+  for (int h = 0; h <= hmax; ++h) s.pair_ptr[h + 1] = static_cast<int>(at[s.lvl_ptr[h + 1]]);
+  auto fill_columns = [&](int q0, int q1) {
+    for (int q = q0; q < q1; ++q) {
       const int k = s.lvl_col[q];
+      int* out = s.pairs.data() + 4 * at[q];
       for (int a = s.lp[k]; a < s.lp[k + 1]; ++a)
         for (int b = s.lp[k]; b <= a; ++b) {
           const int ia = s.li[a], ib = s.li[b];
-          const int dst = ia == ib ? ia : m + position(s, ib, ia);
-          s.pairs.insert(s.pairs.end(), {k, a, b, dst});
+          out[0] = k;
+          out[1] = a;
+          out[2] = b;
+          out[3] = ia == ib ? ia : m + position(s, ib, ia);
+          out += 4;
         }
     }
-    s.pair_ptr[h + 1] = static_cast<int>(s.pairs.size() / 4);
+  };
+  const int nthreads = at[m] > 1000000 ? std::max(1, std::min(16, static_cast<int>(std::thread::hardware_concurrency()))) : 1;
+  if (nthreads == 1) {
+    fill_columns(0, m);
+  } else {
+    std::vector<std::thread> pool;
+    int q0 = 0;
+    for (int t = 0; t < nthreads; ++t) {  // ranges of about equal update counts
+      const std::size_t target = at[m] * (t + 1) / nthreads;
+      int q1 = static_cast<int>(std::lower_bound(at.begin(), at.end(), target) - at.begin());
+      q1 = std::min(m, std::max(q0, q1));
+      if (t == nthreads - 1) q1 = m;
+      pool.emplace_back(fill_columns, q0, q1);
+      q0 = q1;
+    }
+    for (std::thread& th : pool) th.join();
   }
   // assembly map into [D | L]: A's column j couples rows p >= q with weight a_p a_q
   struct Contrib {
