@@ -1075,6 +1075,55 @@ struct Batch {
 
 namespace {
 
+// The row-wise copy (col_idx, rval) of every batched LP from its columns, one CTA per LP, on the
+// device: the host sends the columns and the row starts only. Columns are taken in chunks of
+// 256 in ascending order; in a chunk, thread t (column c0 + t) sets bit t of each of its rows'
+// masks, and an entry's place in its row is the row's running count plus the bits below t, so
+// every row lists its columns in ascending order, exactly as the host's fill does.
+constexpr int kRowsThreads = 256;
+
+__global__ void __launch_bounds__(kRowsThreads) k_batch_rows(const LpMeta* __restrict__ meta, const int* __restrict__ cpa,
+                                                             const int* __restrict__ ria, const double* __restrict__ cva,
+                                                             const int* __restrict__ rpa, int* __restrict__ cia,
+                                                             double* __restrict__ rva) {
+  __shared__ unsigned mask[kBatchMaxRows][kRowsThreads / 32];
+  __shared__ int base[kBatchMaxRows];
+  const LpMeta mt = meta[blockIdx.x];
+  if (mt.m < 0) return;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int* cp = cpa + mt.cp_off;
+  const int* ri = ria + mt.a_off;
+  const double* cv = cva + mt.a_off;
+  const int* rp = rpa + mt.rp_off;
+  int* ci = cia + mt.a_off;
+  double* rv = rva + mt.a_off;
+  for (int r = tid; r < mt.m; r += kRowsThreads) base[r] = rp[r];
+  for (int c0 = 0; c0 < mt.n; c0 += kRowsThreads) {
+    for (int q = tid; q < mt.m * (kRowsThreads / 32); q += kRowsThreads) mask[q / (kRowsThreads / 32)][q % (kRowsThreads / 32)] = 0u;
+    __syncthreads();
+    const int j = c0 + tid;
+    const int pb = j < mt.n ? cp[j] : 0, pe = j < mt.n ? cp[j + 1] : 0;
+    for (int p = pb; p < pe; ++p) atomicOr(&mask[ri[p]][w], 1u << lane);
+    __syncthreads();
+    for (int p = pb; p < pe; ++p) {
+      const int r = ri[p];
+      int rank = __popc(mask[r][w] & ((1u << lane) - 1u));
+      for (int v = 0; v < w; ++v) rank += __popc(mask[r][v]);
+      const int at = base[r] + rank;
+      ci[at] = j;
+      rv[at] = cv[p];
+    }
+    __syncthreads();
+    for (int r = tid; r < mt.m; r += kRowsThreads) {
+      int c = 0;
+#pragma unroll
+      for (int v = 0; v < kRowsThreads / 32; ++v) c += __popc(mask[r][v]);
+      base[r] += c;
+    }
+    __syncthreads();
+  }
+}
+
 int threads_for(int mmax) {
   // SOVEREIGN_BATCH_THREADS=128|256|512 pins every bucket (tests run each width this way)
   if (const char* e = std::getenv("SOVEREIGN_BATCH_THREADS")) {
@@ -1227,6 +1276,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     B->buckets.push_back(std::move(bk));
   }
   // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c | warm | orders
+  // (col_idx and rval are not copied: k_batch_rows fills them on the device)
   const size_t o_meta = 0;
   const size_t o_cp = align8(o_meta + sizeof(LpMeta) * count);
   const size_t o_ri = o_cp + sizeof(int) * cols;
@@ -1239,7 +1289,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   const size_t o_w = o_c + sizeof(double) * nv;
   const size_t o_ord = o_w + sizeof(double) * wv;
   const size_t total = o_ord + sizeof(int) * all_orders.size();
-  B->h2d_bytes = static_cast<double>(total);
+  B->h2d_bytes = static_cast<double>(total - (sizeof(int) + sizeof(double)) * nnz);  // rows built on the device
   B->in.alloc(total);
   B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
   B->out.alloc(count);
@@ -1283,7 +1333,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
         if (kind[i] == kInPlace) {
           const LpFormOut out{cp, ri, cv, rp, ci, rv, bb, cc, pubd + pb.shift_off, pubd + pb.cs_off, pubd + pb.rs_off};
           try {
-            build_plain_lp_into(models[i], shape[i], opt_of(i).enable_scaling != 0, out, &pb.info);
+            build_plain_lp_into(models[i], shape[i], opt_of(i).enable_scaling != 0, out, &pb.info, false);
           } catch (const std::exception& e) {
             throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
           }
@@ -1292,9 +1342,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
           std::memcpy(cp, f.col_ptr.data(), sizeof(int) * (f.n + 1));
           std::memcpy(ri, f.row_idx.data(), sizeof(int) * f.nnz());
           std::memcpy(rp, f.row_ptr.data(), sizeof(int) * (f.m + 1));
-          std::memcpy(ci, f.col_idx.data(), sizeof(int) * f.nnz());
           std::memcpy(cv, f.val.data(), sizeof(double) * f.nnz());
-          std::memcpy(rv, f.rval.data(), sizeof(double) * f.nnz());
           std::memcpy(bb, f.b.data(), sizeof(double) * f.m);
           std::memcpy(cc, f.c.data(), sizeof(double) * f.n);
           std::copy(f.shift.begin(), f.shift.end(), pubd + pb.shift_off);
@@ -1314,9 +1362,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
       copy_range(o_cp + sizeof(int) * r0.cols, sizeof(int) * (r1.cols - r0.cols));
       copy_range(o_ri + sizeof(int) * r0.nnz, sizeof(int) * (r1.nnz - r0.nnz));
       copy_range(o_rp + sizeof(int) * r0.rows, sizeof(int) * (r1.rows - r0.rows));
-      copy_range(o_ci + sizeof(int) * r0.nnz, sizeof(int) * (r1.nnz - r0.nnz));
       copy_range(o_cv + sizeof(double) * r0.nnz, sizeof(double) * (r1.nnz - r0.nnz));
-      copy_range(o_rv + sizeof(double) * r0.nnz, sizeof(double) * (r1.nnz - r0.nnz));
       copy_range(o_b + sizeof(double) * r0.mv, sizeof(double) * (r1.mv - r0.mv));
       copy_range(o_c + sizeof(double) * r0.nv, sizeof(double) * (r1.nv - r0.nv));
       copy_range(o_w + sizeof(double) * r0.wv, sizeof(double) * (r1.wv - r0.wv));
@@ -1325,6 +1371,14 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     if (!all_orders.empty()) std::memcpy(h + o_ord, all_orders.data(), sizeof(int) * all_orders.size());
     copy_range(o_meta, sizeof(LpMeta) * count);
     copy_range(o_ord, sizeof(int) * all_orders.size());
+    // the row-wise copies, built on the device from the columns
+    unsigned char* din = B->in.p;
+    k_batch_rows<<<count, kRowsThreads, 0, cs>>>(
+        reinterpret_cast<const LpMeta*>(din + o_meta), reinterpret_cast<const int*>(din + o_cp),
+        reinterpret_cast<const int*>(din + o_ri), reinterpret_cast<const double*>(din + o_cv),
+        reinterpret_cast<const int*>(din + o_rp), reinterpret_cast<int*>(din + o_ci),
+        reinterpret_cast<double*>(din + o_rv));
+    SOV_CUDA(cudaGetLastError());
     SOV_CUDA(cudaStreamSynchronize(cs));
   } catch (...) {
     cudaStreamSynchronize(cs);  // the staging is reused by the next batch: no copy may still read it

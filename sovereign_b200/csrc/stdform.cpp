@@ -263,7 +263,7 @@ bool plain_lp_shape(const sov_model& p, LpShape* s) {
 }
 
 void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scaling, const LpFormOut& o,
-                         LpFormInfo* info) {
+                         LpFormInfo* info, bool with_rows) {
   // The same arithmetic as build_std_form + scale_two_pass + csr_from_csc, fused into three passes
   // over the entries: (1) copy, with the row counts, the coefficient range and the first row
   // maxima; (2), (3) one scaling pass each, column by column (row scale, column maximum, column
@@ -377,9 +377,11 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
             const bool use = a > 0.0 && a < kInf;
             lo = std::min(lo, use ? a : kInf);
             hi = std::max(hi, use ? a : 0.0);
-            const int t = fill[o.row_idx[k]]++;  // (4) the CSR entry, in column order per row
-            o.col_idx[t] = j;
-            o.rval[t] = o.val[k];
+            if (with_rows) {
+              const int t = fill[o.row_idx[k]]++;  // (4) the CSR entry, in column order per row
+              o.col_idx[t] = j;
+              o.rval[t] = o.val[k];
+            }
           }
         }
         o.c[j] *= sc;
@@ -392,12 +394,13 @@ void build_plain_lp_into(const sov_model& p, const LpShape& s, bool enable_scali
     info->coef_min_after = info->coef_min_before;
     info->coef_max_after = info->coef_max_before;
     // (4) CSR
-    for (int j = 0; j < n; ++j)
-      for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
-        const int t = fill[o.row_idx[k]]++;
-        o.col_idx[t] = j;
-        o.rval[t] = o.val[k];
-      }
+    if (with_rows)
+      for (int j = 0; j < n; ++j)
+        for (int k = o.col_ptr[j]; k < o.col_ptr[j + 1]; ++k) {
+          const int t = fill[o.row_idx[k]]++;
+          o.col_idx[t] = j;
+          o.rval[t] = o.val[k];
+        }
   }
 }
 

@@ -69,8 +69,10 @@ struct LpFormInfo {
   bool scaling_applied;
   double coef_min_before, coef_max_before, coef_min_after, coef_max_after;
 };
+// with_rows false: the row-wise copy is left to the caller except its row starts (out.row_ptr),
+// which are always written (the batched path fills col_idx / rval on the GPU)
 void build_plain_lp_into(const sov_model& model, const LpShape& shape, bool enable_scaling, const LpFormOut& out,
-                         LpFormInfo* info);
+                         LpFormInfo* info, bool with_rows = true);
 
 // Lower-triangle pattern of M = A diag(d) A' as a gather map: target entry t (position in the
 // caller's matrix layout, from `index(row, col)`) receives sum over its contributions
