@@ -45,10 +45,12 @@ constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the 
 __host__ __device__ constexpr int tri(int i) { return i * (i + 1) / 2; }
 
 struct LpMeta {
-  int m, n, nnz, pad1;
-  int max_iter, pad0;
+  int m, n, nnz, n_struct;  // IPM rows / columns / entries; the model's columns
+  int max_iter, m0;         // the model's rows
+  int scale_mode, pad0;     // scaling: 0 none, 1 on the device (k_batch_scale), 2 by the host
   long long a_off, cp_off, rp_off, mv_off, nv_off;
   long long w_off;  // caller's start [x (n) | y (m) | s (n)] in `warm`, or -1
+  long long p_off;  // published [cs*x (n_struct) | s/cs (n_struct) | rs*y (m0)] in `pout`
   double bnorm, cnorm, ftol, otol, tau;
 };
 
@@ -1011,6 +1013,13 @@ class WorkerPool {
   const pid_t owner_;
 };
 
+// the device's highest stream priority (numerically the least value)
+int high_priority() {
+  int least = 0, greatest = 0;
+  SOV_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  return greatest;
+}
+
 template <class F>
 void parallel_for(int count, F fn) {
   if (count < 64) {
@@ -1029,8 +1038,9 @@ struct Batch {
   std::vector<sov_model> models;
   std::vector<StdForm> forms;  // only for LPs not built in place (non-plain columns, or too large)
   std::vector<LpMeta> meta;
-  // publishing (interior_point.cpp:521-569): per LP its sizes and where its shift / column and
-  // row scales sit in `pubdata`
+  // publishing (interior_point.cpp:521-569): per LP its sizes and where its shift sits in
+  // `pubdata` (followed by room for the unit scales the in-place builder writes; the scales used
+  // are on the device, `scl`)
   struct Pub {
     int n_struct, m0, n, m;
     long long shift_off, cs_off, rs_off;
@@ -1052,7 +1062,11 @@ struct Batch {
   DBuf<double> work;  // 9 n-vectors + 2 m-vectors
   DBuf<LpOut> out;
   DBuf<int> nexts;
-  long long total_n = 0, total_m = 0, total_nnz = 0, total_cols = 0, total_rows = 0;
+  // published scale products of every LP (k_batch_publish), then per LP the coefficient range
+  // after scaling (k_batch_scale)
+  DBuf<double> pout;
+  double* scl = nullptr;  // device: column scales (total_n) | row scales (total_m), inside `in`
+  long long total_n = 0, total_m = 0, total_nnz = 0, total_cols = 0, total_rows = 0, total_pub = 0;
   BatchDev dev{};
   int launches = 0;
   double kernel_ms = 0.0, bytes = 0.0, flops = 0.0;
@@ -1060,6 +1074,9 @@ struct Batch {
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> joins;
   cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t ready = nullptr;      // inputs scaled and row copies built (k_batch_scale, k_batch_rows)
+  cudaEvent_t published = nullptr;  // k_batch_publish of the last solve done
+  bool publish_queued = false;      // k_batch_publish already enqueued behind the last solve
   cudaStream_t cap = nullptr;
   cudaGraphExec_t graph = nullptr;  // the bucket launches of one solve
   ~Batch() {
@@ -1070,6 +1087,8 @@ struct Batch {
     if (fork) cudaEventDestroy(fork);
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
+    if (ready) cudaEventDestroy(ready);
+    if (published) cudaEventDestroy(published);
   }
 };
 
@@ -1122,6 +1141,131 @@ __global__ void __launch_bounds__(kRowsThreads) k_batch_rows(const LpMeta* __res
     }
     __syncthreads();
   }
+}
+
+// The two-pass scaling of every batched LP built in place (interior_point.cpp:370-405: rows by
+// 1/sqrt(max|a|), then columns, twice), one CTA per LP, on the device: the host sends the unscaled
+// columns. Every value sees the host builder's products in the host builder's order, and the row,
+// column and range maxima are exact whatever order the threads take (a NaN never replaces a running
+// maximum, as in std::max(cur, a)), so values, b, c, the scales and the coefficient range are bit
+// for bit the host's. Also, for every LP, bnorm = max(1, max|b|) and cnorm = max(1, max|c|) of the
+// scaled data (interior_point.cpp:586).
+constexpr int kScaleThreads = 256;
+
+__device__ __forceinline__ double inv_sqrt_or_one(double x) { return x > 0.0 ? 1.0 / sqrt(x) : 1.0; }
+
+// running maximum of non-negative doubles held as their bit patterns (ordered like the values)
+__device__ __forceinline__ void max_bits(unsigned long long* slot, double a) {
+  if (a > 0.0) atomicMax(slot, static_cast<unsigned long long>(__double_as_longlong(a)));
+}
+
+__global__ void __launch_bounds__(kScaleThreads) k_batch_scale(LpMeta* __restrict__ meta, const int* __restrict__ cpa,
+                                                               const int* __restrict__ ria, double* __restrict__ cva,
+                                                               double* __restrict__ ba, double* __restrict__ ca,
+                                                               double* __restrict__ scl, long long total_n,
+                                                               double* __restrict__ crange) {
+  __shared__ unsigned long long rmax[kBatchMaxRows];
+  __shared__ double rsc[kBatchMaxRows];
+  __shared__ unsigned long long lo_bits, hi_bits, bmax_bits, cmax_bits;
+  LpMeta* mp = meta + blockIdx.x;
+  const int m = mp->m, n = mp->n, mode = mp->scale_mode;
+  if (m < 0) return;
+  const int tid = threadIdx.x;
+  const int* cp = cpa + mp->cp_off;
+  const int* ri = ria + mp->a_off;
+  double* cv = cva + mp->a_off;
+  double* b = ba + mp->mv_off;
+  double* c = ca + mp->nv_off;
+  double* cs = scl + mp->nv_off;
+  double* rs = scl + total_n + mp->mv_off;
+  constexpr unsigned long long inf_bits = 0x7ff0000000000000ull;  // +infinity
+  if (tid == 0) {
+    lo_bits = inf_bits;
+    hi_bits = 0ull;
+    bmax_bits = 0ull;
+    cmax_bits = 0ull;
+  }
+  if (mode == 1) {
+    for (int r = tid; r < m; r += kScaleThreads) rmax[r] = 0ull;
+    __syncthreads();
+    for (int j = tid; j < n; j += kScaleThreads)
+      for (int p = cp[j]; p < cp[j + 1]; ++p) max_bits(&rmax[ri[p]], fabs(cv[p]));
+    for (int pass = 0; pass < 2; ++pass) {
+      __syncthreads();
+      for (int r = tid; r < m; r += kScaleThreads) {
+        const double f = inv_sqrt_or_one(__longlong_as_double(static_cast<long long>(rmax[r])));
+        rsc[r] = f;
+        rs[r] = pass == 0 ? f : __dmul_rn(rs[r], f);
+        b[r] = __dmul_rn(b[r], f);
+        rmax[r] = 0ull;
+      }
+      __syncthreads();
+      for (int j = tid; j < n; j += kScaleThreads) {
+        const int pb = cp[j], pe = cp[j + 1];
+        double mx = 0.0;
+        for (int p = pb; p < pe; ++p) {
+          const double v = __dmul_rn(cv[p], rsc[ri[p]]);
+          cv[p] = v;
+          const double a = fabs(v);
+          mx = mx < a ? a : mx;
+        }
+        const double f = inv_sqrt_or_one(mx);
+        for (int p = pb; p < pe; ++p) {
+          const double v = __dmul_rn(cv[p], f);
+          cv[p] = v;
+          const double a = fabs(v);
+          if (pass == 0) {
+            max_bits(&rmax[ri[p]], a);
+          } else if (a > 0.0 && a <= DBL_MAX) {
+            const unsigned long long ab = static_cast<unsigned long long>(__double_as_longlong(a));
+            atomicMin(&lo_bits, ab);
+            atomicMax(&hi_bits, ab);
+          }
+        }
+        c[j] = __dmul_rn(c[j], f);
+        cs[j] = pass == 0 ? f : __dmul_rn(cs[j], f);
+      }
+    }
+  } else if (mode == 0) {
+    for (int j = tid; j < n; j += kScaleThreads) cs[j] = 1.0;
+    for (int r = tid; r < m; r += kScaleThreads) rs[r] = 1.0;
+  }
+  __syncthreads();
+  for (int r = tid; r < m; r += kScaleThreads) max_bits(&bmax_bits, fabs(b[r]));
+  for (int j = tid; j < n; j += kScaleThreads) max_bits(&cmax_bits, fabs(c[j]));
+  __syncthreads();
+  if (tid == 0) {
+    const double bm = __longlong_as_double(static_cast<long long>(bmax_bits));
+    const double cm = __longlong_as_double(static_cast<long long>(cmax_bits));
+    mp->bnorm = 1.0 < bm ? bm : 1.0;
+    mp->cnorm = 1.0 < cm ? cm : 1.0;
+    crange[2 * blockIdx.x] = __longlong_as_double(static_cast<long long>(lo_bits));
+    crange[2 * blockIdx.x + 1] = __longlong_as_double(static_cast<long long>(hi_bits));
+  }
+}
+
+// publish_iterate's scale products (interior_point.cpp:541-563) for every batched LP, one CTA per
+// LP, from the final or the best iterate as the solve chose: cs*x and s/cs for the model's columns,
+// rs*y for its rows. The host adds the shift (primal = shift + cs*x), so the published values are
+// the ones the host arithmetic gives.
+__global__ void __launch_bounds__(kScaleThreads) k_batch_publish(const LpMeta* __restrict__ meta, const LpOut* __restrict__ out,
+                                                                 BatchDev d, const double* __restrict__ scl,
+                                                                 long long total_n, double* __restrict__ pout) {
+  const LpMeta& mt = meta[blockIdx.x];
+  if (mt.m < 0) return;
+  const bool best = out[blockIdx.x].use_best != 0;
+  const double* x = (best ? d.bx : d.x) + mt.nv_off;
+  const double* s = (best ? d.bs : d.s) + mt.nv_off;
+  const double* y = (best ? d.by : d.y) + mt.mv_off;
+  const double* cs = scl + mt.nv_off;
+  const double* rs = scl + total_n + mt.mv_off;
+  double* P = pout + mt.p_off;
+  const int ns = mt.n_struct;
+  for (int j = threadIdx.x; j < ns; j += kScaleThreads) {
+    P[j] = __dmul_rn(cs[j], x[j]);
+    P[ns + j] = __ddiv_rn(s[j], cs[j]);
+  }
+  for (int k = threadIdx.x; k < mt.m0; k += kScaleThreads) P[2 * ns + k] = __dmul_rn(rs[k], y[k]);
 }
 
 int threads_for(int mmax) {
@@ -1193,7 +1337,8 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   // 2. offsets (serial prefix over the LPs)
   B->meta.resize(count);
   B->pub.resize(count);
-  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0, pubn = 0, wv = 0;
+  long long nnz = 0, cols = 0, rows = 0, nv = 0, mv = 0, pubn = 0, wv = 0, pv = 0;
+  int from_form = 0;
   struct Run {
     long long nnz, cols, rows, mv, nv, wv;
   };
@@ -1212,6 +1357,12 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     mt.m = sh.m;
     mt.n = sh.n;
     mt.nnz = sh.nnz;
+    mt.n_struct = sh.n_struct;
+    mt.m0 = sh.m0;
+    mt.scale_mode = kind[i] == kFromForm ? 2 : (opt.enable_scaling != 0 && sh.m > 0 && sh.n > 0) ? 1 : 0;
+    if (kind[i] == kFromForm) ++from_form;
+    mt.p_off = pv;
+    pv += 2LL * sh.n_struct + sh.m0;
     mt.max_iter = opt.max_iterations;
     mt.a_off = nnz;
     mt.cp_off = cols;
@@ -1250,6 +1401,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   B->total_nnz = nnz;
   B->total_cols = cols;
   B->total_rows = rows;
+  B->total_pub = pv;
   B->pubdata.alloc(static_cast<size_t>(std::max(1LL, pubn)));
   // buckets by m, each ordered largest-first (cost ~ m^3 + nnz); their orders travel with the inputs
   std::map<int, std::vector<int>> groups;
@@ -1275,8 +1427,10 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     all_orders.insert(all_orders.end(), ids.begin(), ids.end());
     B->buckets.push_back(std::move(bk));
   }
-  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c | warm | orders
-  // (col_idx and rval are not copied: k_batch_rows fills them on the device)
+  // layout: meta | col_ptr | row_idx | row_ptr | col_idx | (8-aligned) cval | rval | b | c | warm | orders |
+  // (8-aligned) column scales | row scales. col_idx and rval are not copied (k_batch_rows fills
+  // them on the device), nor the scales, except those of LPs scaled by the host (k_batch_scale
+  // computes the others)
   const size_t o_meta = 0;
   const size_t o_cp = align8(o_meta + sizeof(LpMeta) * count);
   const size_t o_ri = o_cp + sizeof(int) * cols;
@@ -1288,20 +1442,25 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   const size_t o_c = o_b + sizeof(double) * mv;
   const size_t o_w = o_c + sizeof(double) * nv;
   const size_t o_ord = o_w + sizeof(double) * wv;
-  const size_t total = o_ord + sizeof(int) * all_orders.size();
-  B->h2d_bytes = static_cast<double>(total - (sizeof(int) + sizeof(double)) * nnz);  // rows built on the device
+  const size_t o_scl = align8(o_ord + sizeof(int) * all_orders.size());
+  const size_t total = o_scl + sizeof(double) * (nv + mv);
+  B->h2d_bytes = static_cast<double>(o_ord + sizeof(int) * all_orders.size() - (sizeof(int) + sizeof(double)) * nnz);
   B->in.alloc(total);
   B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
   B->out.alloc(count);
   B->nexts.alloc(std::max<size_t>(1, B->buckets.size()));
+  B->pout.alloc(static_cast<size_t>(pv + 2LL * count));
   // 3. every LP's standard form written into its slots of the pinned staging, chunk by chunk in
   //    LP order; each finished chunk's slots are copied to the device (async) while the next
   //    chunk is built
   std::lock_guard<std::mutex> lock(g_arena.mu);
   unsigned char* h = g_arena.get(total);
   double* pubd = B->pubdata.p;
+  // the copies and the input kernels on a high-priority stream: while an earlier batch's persistent
+  // kernels hold the SMs, this batch's short kernels take the first slots that free up
   cudaStream_t cs = nullptr;
-  SOV_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  SOV_CUDA(cudaStreamCreateWithPriority(&cs, cudaStreamNonBlocking, high_priority()));
+  cudaEvent_t copied = nullptr;
   auto copy_range = [&](size_t off, size_t bytes) {
     if (bytes) SOV_CUDA(cudaMemcpyAsync(B->in.p + off, h + off, bytes, cudaMemcpyHostToDevice, cs));
   };
@@ -1331,12 +1490,14 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
           std::memcpy(wd + mt.n + mt.m, o.warm_s, sizeof(double) * mt.n);
         }
         if (kind[i] == kInPlace) {
+          // unscaled here; k_batch_scale scales on the device (coefficient range after: see batch_results)
           const LpFormOut out{cp, ri, cv, rp, ci, rv, bb, cc, pubd + pb.shift_off, pubd + pb.cs_off, pubd + pb.rs_off};
           try {
-            build_plain_lp_into(models[i], shape[i], opt_of(i).enable_scaling != 0, out, &pb.info, false);
+            build_plain_lp_into(models[i], shape[i], false, out, &pb.info, false);
           } catch (const std::exception& e) {
             throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
           }
+          pb.info.scaling_applied = mt.scale_mode == 1;
         } else {
           const StdForm& f = B->forms[i];
           std::memcpy(cp, f.col_ptr.data(), sizeof(int) * (f.n + 1));
@@ -1346,16 +1507,12 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
           std::memcpy(bb, f.b.data(), sizeof(double) * f.m);
           std::memcpy(cc, f.c.data(), sizeof(double) * f.n);
           std::copy(f.shift.begin(), f.shift.end(), pubd + pb.shift_off);
-          std::copy(f.col_scale.begin(), f.col_scale.end(), pubd + pb.cs_off);
-          std::copy(f.row_scale.begin(), f.row_scale.end(), pubd + pb.rs_off);
+          double* hs = reinterpret_cast<double*>(h + o_scl);
+          std::copy(f.col_scale.begin(), f.col_scale.end(), hs + mt.nv_off);
+          std::copy(f.row_scale.begin(), f.row_scale.end(), hs + nv + mt.mv_off);
           pb.info = LpFormInfo{f.scaling_applied, f.coef_min_before, f.coef_max_before, f.coef_min_after,
                                f.coef_max_after};
         }
-        double bmax = 0.0, cmax = 0.0;
-        for (int k = 0; k < mt.m; ++k) bmax = std::max(bmax, std::abs(bb[k]));
-        for (int k = 0; k < mt.n; ++k) cmax = std::max(cmax, std::abs(cc[k]));
-        mt.bnorm = std::max(1.0, bmax);
-        mt.cnorm = std::max(1.0, cmax);
       });
       const Run& r0 = run[lo];
       const Run& r1 = run[hi];
@@ -1371,21 +1528,43 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     if (!all_orders.empty()) std::memcpy(h + o_ord, all_orders.data(), sizeof(int) * all_orders.size());
     copy_range(o_meta, sizeof(LpMeta) * count);
     copy_range(o_ord, sizeof(int) * all_orders.size());
-    // the row-wise copies, built on the device from the columns
+    SOV_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+    if (from_form > 0)  // the scales of the LPs the host scaled
+      for (int i = 0; i < count; ++i) {
+        const LpMeta& mt = B->meta[i];
+        if (mt.m < 0 || mt.scale_mode != 2) continue;
+        copy_range(o_scl + sizeof(double) * mt.nv_off, sizeof(double) * mt.n);
+        copy_range(o_scl + sizeof(double) * (nv + mt.mv_off), sizeof(double) * mt.m);
+        B->h2d_bytes += sizeof(double) * (mt.n + mt.m);
+      }
+    SOV_CUDA(cudaEventRecord(copied, cs));
+    // the scaling, then the row-wise copies built on the device from the (scaled) columns
     unsigned char* din = B->in.p;
+    B->scl = reinterpret_cast<double*>(din + o_scl);
+    k_batch_scale<<<count, kScaleThreads, 0, cs>>>(
+        reinterpret_cast<LpMeta*>(din + o_meta), reinterpret_cast<const int*>(din + o_cp),
+        reinterpret_cast<const int*>(din + o_ri), reinterpret_cast<double*>(din + o_cv),
+        reinterpret_cast<double*>(din + o_b), reinterpret_cast<double*>(din + o_c), B->scl, nv, B->pout.p + pv);
+    SOV_CUDA(cudaGetLastError());
     k_batch_rows<<<count, kRowsThreads, 0, cs>>>(
         reinterpret_cast<const LpMeta*>(din + o_meta), reinterpret_cast<const int*>(din + o_cp),
         reinterpret_cast<const int*>(din + o_ri), reinterpret_cast<const double*>(din + o_cv),
         reinterpret_cast<const int*>(din + o_rp), reinterpret_cast<int*>(din + o_ci),
         reinterpret_cast<double*>(din + o_rv));
     SOV_CUDA(cudaGetLastError());
-    SOV_CUDA(cudaStreamSynchronize(cs));
+    SOV_CUDA(cudaEventCreateWithFlags(&B->ready, cudaEventDisableTiming));
+    SOV_CUDA(cudaEventRecord(B->ready, cs));
+    // the staging is reused by the next batch: wait for the copies (the kernels run on; every
+    // launch of this batch waits for `ready`)
+    SOV_CUDA(cudaEventSynchronize(copied));
   } catch (...) {
-    cudaStreamSynchronize(cs);  // the staging is reused by the next batch: no copy may still read it
+    cudaStreamSynchronize(cs);
     cudaStreamDestroy(cs);
+    if (copied) cudaEventDestroy(copied);
     throw;
   }
-  SOV_CUDA(cudaStreamDestroy(cs));
+  SOV_CUDA(cudaEventDestroy(copied));
+  SOV_CUDA(cudaStreamDestroy(cs));  // its pending kernels still run
   for (size_t k = 0; k < B->buckets.size(); ++k) {
     B->buckets[k]->order = reinterpret_cast<const int*>(B->in.p + o_ord) + order_at[k];
     B->buckets[k]->next = B->nexts.p + k;
@@ -1454,6 +1633,16 @@ void enqueue_buckets(Batch* B, cudaStream_t from) {
   }
 }
 
+// k_batch_publish on `st` behind the solve, then the `published` event batch_results waits for
+void enqueue_publish(Batch* B, cudaStream_t st) {
+  if (!B->published) SOV_CUDA(cudaEventCreateWithFlags(&B->published, cudaEventDisableTiming));
+  const BatchDev& d = B->dev;
+  k_batch_publish<<<B->count, kScaleThreads, 0, st>>>(d.meta, d.out, d, B->scl, B->total_n, B->pout.p);
+  SOV_CUDA(cudaGetLastError());
+  SOV_CUDA(cudaEventRecord(B->published, st));
+  B->publish_queued = true;
+}
+
 }  // namespace
 
 // The batch's bucket launches on `st` between two timing events; batch_finish waits for them.
@@ -1464,12 +1653,15 @@ void enqueue_buckets(Batch* B, cudaStream_t from) {
 // would cost more than it saves).
 void batch_launch(Batch* B, cudaStream_t st, bool one_shot) {
   make_streams(B);
+  SOV_CUDA(cudaStreamWaitEvent(st, B->ready, 0));
   if (one_shot) {
     SOV_CUDA(cudaEventRecord(B->t0, st));
     enqueue_buckets(B, st);
     SOV_CUDA(cudaEventRecord(B->t1, st));
+    enqueue_publish(B, st);  // read back by batch_results; outside the timed events
     return;
   }
+  B->publish_queued = false;
   if (!B->graph) {
     SOV_CUDA(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
     SOV_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
@@ -1499,21 +1691,37 @@ void batch_solve(Batch* B, cudaStream_t st) {
 }
 
 void batch_results(Batch* B, sov_result* results) {
-  const long long nv = B->total_n, mv = B->total_m;
-  // D2H: statuses, then x, s, y of every LP; the best iterate only for LPs that need it
+  const long long nv = B->total_n, mv = B->total_m, pv = B->total_pub;
+  const BatchDev& d = B->dev;
+  // D2H: statuses, then the published scale products of every LP and the coefficient ranges
+  // (k_batch_publish picks the final or the best iterate on the device); the IPM-space iterates
+  // only when a result asks for them
+  if (!B->publish_queued) {
+    cudaStream_t ps;
+    SOV_CUDA(cudaStreamCreateWithPriority(&ps, cudaStreamNonBlocking, high_priority()));
+    if (B->t1) SOV_CUDA(cudaStreamWaitEvent(ps, B->t1, 0));
+    enqueue_publish(B, ps);
+    SOV_CUDA(cudaStreamDestroy(ps));
+  }
+  SOV_CUDA(cudaEventSynchronize(B->published));
+  B->publish_queued = false;
   std::vector<LpOut> out(B->count);
   SOV_CUDA(cudaMemcpy(out.data(), B->out.p, sizeof(LpOut) * B->count, cudaMemcpyDeviceToHost));
-  const size_t bytes = sizeof(double) * (2 * nv + mv);
+  bool want_ipm = false;
+  for (int i = 0; i < B->count && !want_ipm; ++i)
+    want_ipm = B->meta[i].m >= 0 && (results[i].ipm_x || results[i].ipm_s || results[i].ipm_y);
+  const size_t pbytes = sizeof(double) * (pv + 2LL * B->count);
+  const size_t bytes = want_ipm ? sizeof(double) * (2 * nv + mv) : 0;
   std::lock_guard<std::mutex> lock(g_arena.mu);
-  double* h = reinterpret_cast<double*>(g_arena.get(std::max<size_t>(bytes, 8)));
-  const BatchDev& d = B->dev;
-  if (nv) {
-    SOV_CUDA(cudaMemcpy(h, d.x, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost));  // x, s adjacent
-  }
-  if (mv) SOV_CUDA(cudaMemcpy(h + 2 * nv, d.y, sizeof(double) * mv, cudaMemcpyDeviceToHost));
-  double d2h = sizeof(LpOut) * B->count + static_cast<double>(bytes);
+  double* hp = reinterpret_cast<double*>(g_arena.get(std::max<size_t>(pbytes + bytes, 8)));
+  double* h = hp + pv + 2LL * B->count;
+  SOV_CUDA(cudaMemcpy(hp, B->pout.p, pbytes, cudaMemcpyDeviceToHost));
+  const double* crange = hp + pv;
+  if (want_ipm && nv) SOV_CUDA(cudaMemcpy(h, d.x, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost));  // x, s adjacent
+  if (want_ipm && mv) SOV_CUDA(cudaMemcpy(h + 2 * nv, d.y, sizeof(double) * mv, cudaMemcpyDeviceToHost));
+  double d2h = sizeof(LpOut) * B->count + static_cast<double>(pbytes + bytes);
   std::vector<std::vector<double>> best(B->count);
-  for (int i = 0; i < B->count; ++i) {
+  for (int i = 0; i < B->count && want_ipm; ++i) {
     const LpMeta& mt = B->meta[i];
     if (mt.m < 0 || !out[i].use_best) continue;
     best[i].resize(2 * mt.n + mt.m);
@@ -1529,14 +1737,9 @@ void batch_results(Batch* B, sov_result* results) {
     if (mt.m < 0) return;  // solved by the fallback path below
     const Batch::Pub& f = B->pub[i];
     const double* shift = B->pubdata.p + f.shift_off;
-    const double* col_scale = B->pubdata.p + f.cs_off;
-    const double* row_scale = B->pubdata.p + f.rs_off;
+    const double* px = hp + mt.p_off;  // cs*x | s/cs | rs*y
     const sov_model& mdl = B->models[i];
     const LpOut& o = out[i];
-    const bool use_best = o.use_best != 0;
-    const double* hx = use_best ? best[i].data() : h + mt.nv_off;
-    const double* hs = use_best ? best[i].data() + mt.n : h + nv + mt.nv_off;
-    const double* hy = use_best ? best[i].data() + 2 * mt.n : h + 2 * nv + mt.mv_off;
     r->status = o.status;
     r->iterations = o.iterations;
     r->has_objective_value = 1;
@@ -1548,16 +1751,21 @@ void batch_results(Batch* B, sov_result* results) {
     // publish_iterate (interior_point.cpp:541-563)
     double obj = mdl.obj_constant;
     for (int j = 0; j < f.n_struct; ++j) {
-      const double v = shift[j] + col_scale[j] * hx[j];
+      const double v = shift[j] + px[j];
       if (r->primal) r->primal[j] = v;
-      if (r->dual_col) r->dual_col[j] = hs[j] / col_scale[j];
       obj += (mdl.obj ? mdl.obj[j] : 0.0) * v;
     }
-    if (r->dual_row)
-      for (int k = 0; k < f.m0; ++k) r->dual_row[k] = row_scale[k] * hy[k];
-    if (r->ipm_x) std::copy(hx, hx + f.n, r->ipm_x);
-    if (r->ipm_s) std::copy(hs, hs + f.n, r->ipm_s);
-    if (r->ipm_y) std::copy(hy, hy + f.m, r->ipm_y);
+    if (r->dual_col) std::copy(px + f.n_struct, px + 2 * f.n_struct, r->dual_col);
+    if (r->dual_row) std::copy(px + 2 * f.n_struct, px + 2 * f.n_struct + f.m0, r->dual_row);
+    if (want_ipm) {  // the IPM-space iterate the published values came from
+      const bool use_best = o.use_best != 0;
+      const double* hx = use_best ? best[i].data() : h + mt.nv_off;
+      const double* hs = use_best ? best[i].data() + mt.n : h + nv + mt.nv_off;
+      const double* hy = use_best ? best[i].data() + 2 * mt.n : h + 2 * nv + mt.mv_off;
+      if (r->ipm_x) std::copy(hx, hx + f.n, r->ipm_x);
+      if (r->ipm_s) std::copy(hs, hs + f.n, r->ipm_s);
+      if (r->ipm_y) std::copy(hy, hy + f.m, r->ipm_y);
+    }
     r->objective_value = obj;
     r->solve_seconds = B->kernel_ms * 1e-3;
     if (o.status == SOV_OPTIMAL)
@@ -1580,8 +1788,14 @@ void batch_results(Batch* B, sov_result* results) {
       r->diagnostics->scaling_applied = f.info.scaling_applied;
       r->diagnostics->coefficient_min_abs_before = f.info.coef_min_before;
       r->diagnostics->coefficient_max_abs_before = f.info.coef_max_before;
-      r->diagnostics->coefficient_min_abs_after = f.info.coef_min_after;
-      r->diagnostics->coefficient_max_abs_after = f.info.coef_max_after;
+      if (mt.scale_mode == 1) {  // range after the device scaling (+inf: no entry in range)
+        const double lo = crange[2 * i];
+        r->diagnostics->coefficient_min_abs_after = lo <= DBL_MAX ? lo : 0.0;
+        r->diagnostics->coefficient_max_abs_after = crange[2 * i + 1];
+      } else {
+        r->diagnostics->coefficient_min_abs_after = f.info.coef_min_after;
+        r->diagnostics->coefficient_max_abs_after = f.info.coef_max_after;
+      }
       r->diagnostics->refactorizations = o.iterations + 1;
       r->diagnostics->warm_start_used = o.warm_used;
       r->diagnostics->stall_iteration = -1;
@@ -1629,7 +1843,10 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
   // the device, so the host standard form and the copies of the next part overlap the solves of the
   // ones before; the results are read back in order once all parts are launched. A part's LPs are
   // solved exactly as in one batch (per-LP work, bucket widths by m).
-  const int parts = count >= 2048 ? 4 : 1;  // 4096 LPs: 27.5 ms per call; 8 parts 31.7, 16 parts 44.6
+  // 4096 LPs per call (median of 6 calls): 1 part 29.5 ms, 2 25.9, 3 24.2, 4 24.4, 6 23.7, 8 24.0,
+  // 12 32.4
+  int parts = count >= 3072 ? 6 : count >= 2048 ? 4 : 1;
+  if (const char* e = std::getenv("SOVEREIGN_BATCH_PARTS")) parts = std::max(1, std::min(count, std::atoi(e)));
   std::vector<std::unique_ptr<Batch>> batches;
   std::vector<cudaStream_t> streams;
   auto part_lo = [&](int k) { return static_cast<int>(static_cast<long long>(count) * k / parts); };
@@ -1664,6 +1881,7 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
 std::string autotune(int count, const sov_model* models, const sov_options* opt, const std::string& file) {
   // Per bucket: time the bucket alone with 128 / 256 / 512 threads per CTA and keep the fastest.
   std::unique_ptr<Batch> B(batch_create(count, models, opt));
+  SOV_CUDA(cudaEventSynchronize(B->ready));
   cudaStream_t st;
   SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   std::ostringstream rep;

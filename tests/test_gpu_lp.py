@@ -116,6 +116,48 @@ def test_batch_equals_single_engine_primal():
         np.testing.assert_allclose(r.primal, s.primal, rtol=1e-6, atol=1e-6)
 
 
+def with_explicit_zero(mdl):
+    """The same LP with an explicit 0.0 entry in its first column: not a plain column layout, so the
+    batch builds it on the host (build_std_form) instead of in place."""
+    import dataclasses
+    rows = set(mdl.row_idx[mdl.col_ptr[0]:mdl.col_ptr[1]].tolist())
+    r = next(i for i in range(mdl.m) if i not in rows)
+    e = int(mdl.col_ptr[0]) + int(np.searchsorted(mdl.row_idx[mdl.col_ptr[0]:mdl.col_ptr[1]], r))
+    col_ptr = mdl.col_ptr.copy()
+    col_ptr[1:] += 1
+    return dataclasses.replace(mdl, col_ptr=col_ptr, row_idx=np.insert(mdl.row_idx, e, r).astype(np.int32),
+                               values=np.insert(mdl.values, e, 0.0), name=mdl.name + "_zero", _keep=[])
+
+
+def test_batch_device_scaling_matches_host_builder():
+    # LPs built in place are scaled on the device (k_batch_scale) and their results unscaled there
+    # (k_batch_publish); the single engine scales on the host. The arithmetic is the same, so the
+    # coefficient range after scaling is equal bit for bit and the published solutions agree to the
+    # engines' tolerance (row duals through A'y). Covers bounds (shift, UB rows), Le/Ge slacks, a
+    # maximisation, an LP the batch scales on the host (explicit zero entry), scaling off, and the
+    # IPM-space copies.
+    models = [P.bounded_lp_example(), P.transport(12, 9, 2), with_explicit_zero(P.transport(8, 7, 1)),
+              P.random_sparse_lp(40, 90, 3, 4)]
+    for opts in (InteriorPointOptions(), InteriorPointOptions(enable_scaling=False)):
+        res = solve_batch(models, opts, with_diag=True)
+        res_ipm = solve_batch(models, opts, with_ipm=True)
+        for k, (mdl, r, ri) in enumerate(zip(models, res, res_ipm)):
+            s = InteriorPointSolver(opts).solve(mdl, with_diag=True)
+            assert r.status_name == "OPTIMAL" and s.status_name == "OPTIMAL", (k, r.message)
+            for key in ("scaling_applied", "coefficient_min_abs_before", "coefficient_max_abs_before",
+                        "coefficient_min_abs_after", "coefficient_max_abs_after"):
+                assert r.diagnostics[key] == s.diagnostics[key], (k, key)
+            assert rel(r.objective_value, s.objective_value) < 1e-9, k
+            np.testing.assert_allclose(r.primal, s.primal, rtol=1e-6, atol=1e-6)
+            np.testing.assert_allclose(r.dual_col, s.dual_col, rtol=1e-5, atol=1e-6)
+            # row duals are unique up to the null space of A' (a transportation LP's supply and demand
+            # duals can shift by opposite constants): compare A' y
+            A = mdl.dense_A()
+            np.testing.assert_allclose(A.T @ r.dual_row, A.T @ s.dual_row, rtol=1e-5, atol=1e-5)
+            np.testing.assert_array_equal(ri.primal, r.primal)
+            assert np.all(np.isfinite(ri.ipm_x)) and np.any(ri.ipm_x != 0.0)
+
+
 def test_result_contract_matches_restatement():
     mdl = P.bounded_lp_example()
     r = InteriorPointSolver().solve(mdl, with_diag=True)
