@@ -1900,6 +1900,15 @@ void batch_transfer_bytes(const Batch* B, double* h2d, double* d2h) {
 
 void batch_destroy(Batch* B) { delete B; }
 
+void parallel_memcpy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kChunk = size_t(1) << 18;
+  const int chunks = static_cast<int>((bytes + kChunk - 1) / kChunk);
+  parallel_for(chunks, [&](int c) {
+    const size_t off = static_cast<size_t>(c) * kChunk;
+    std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, std::min(kChunk, bytes - off));
+  });
+}
+
 int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results) {
   if (count == 0) return SOV_OK;
   // Large batches in parts, pipelined: each part's graph is launched as soon as its inputs are on

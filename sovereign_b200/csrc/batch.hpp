@@ -19,6 +19,8 @@ void batch_stats(const Batch* b, int* launches, double* kernel_ms, double* bytes
 void batch_transfer_bytes(const Batch* b, double* h2d, double* d2h);
 void batch_destroy(Batch* b);
 std::string autotune(int count, const sov_model* models, const sov_options* opt, const std::string& file);
+// memcpy of a large host range on the library's worker threads (chunks of 256 KB)
+void parallel_memcpy(void* dst, const void* src, size_t bytes);
 
 // y = A x / A' x for a host CSC matrix (device kernels; host buffers in and out)
 int spmv_csc_device(int nrows, int ncols, const int* col_ptr, const int* row_idx, const double* values,

@@ -20,6 +20,7 @@
 #include <stdexcept>
 #include <vector>
 
+#include "batch.hpp"
 #include "common.cuh"
 #include "sov_ipm.h"
 #include "tc.cuh"
@@ -268,6 +269,25 @@ struct Mlp {
   Buf<float> target;
   Buf<double> part;
   Buf<double> raw_in, norm, start;  // warm-start prediction: parameters, normalizers, decoded start
+  // pinned landing buffer of the decoded starts (grow-only): the D2H runs at full speed, and the
+  // caller's (pageable) arrays are filled from it on several threads
+  struct Pinned {
+    void* p = nullptr;
+    size_t cap = 0;
+    void* get(size_t bytes) {
+      if (bytes > cap) {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        SOV_CUDA(cudaMallocHost(&p, bytes));
+        cap = bytes;
+      }
+      return p;
+    }
+    ~Pinned() {
+      if (p) cudaFreeHost(p);
+    }
+  } landing, staging;  // the decoded starts out; the parameters in
   Buf<int> err;
   long long step = 0;
   cudaStream_t st = nullptr;
@@ -432,7 +452,9 @@ int sov_mlp_predict_start(sov_mlp* h, const double* params, int32_t batch, const
     if (m->norm.n < static_cast<size_t>(2 * (n_in + n_out))) m->norm.alloc(2 * (n_in + n_out));
     if (m->start.n < cnt_out) m->start.alloc(cnt_out);
     double* nm = m->norm.p;
-    SOV_CUDA(cudaMemcpyAsync(m->raw_in.p, params, sizeof(double) * cnt_in, cudaMemcpyHostToDevice, m->st));
+    double* hs = static_cast<double*>(m->staging.get(sizeof(double) * cnt_in));
+    sov::parallel_memcpy(hs, params, sizeof(double) * cnt_in);
+    SOV_CUDA(cudaMemcpyAsync(m->raw_in.p, hs, sizeof(double) * cnt_in, cudaMemcpyHostToDevice, m->st));
     SOV_CUDA(cudaMemcpyAsync(nm, in_mean, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
     SOV_CUDA(cudaMemcpyAsync(nm + n_in, in_std, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
     SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in, out_mean, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
@@ -446,10 +468,14 @@ int sov_mlp_predict_start(sov_mlp* h, const double* params, int32_t batch, const
     sov::k_decode_start<<<1184, 256, 0, m->st>>>(m->act.back().p, nm + 2 * n_in, nm + 2 * n_in + n_out, batch, n_ipm,
                                                 m_ipm, delta, dx, dy, ds);
     SOV_CUDA(cudaGetLastError());
-    SOV_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * batch * n_ipm, cudaMemcpyDeviceToHost, m->st));
-    SOV_CUDA(cudaMemcpyAsync(y, dy, sizeof(double) * batch * m_ipm, cudaMemcpyDeviceToHost, m->st));
-    SOV_CUDA(cudaMemcpyAsync(s, ds, sizeof(double) * batch * n_ipm, cudaMemcpyDeviceToHost, m->st));
+    // [x | y | s] are adjacent on the device: one copy into the pinned landing buffer
+    double* hl = static_cast<double*>(m->landing.get(sizeof(double) * cnt_out));
+    SOV_CUDA(cudaMemcpyAsync(hl, dx, sizeof(double) * cnt_out, cudaMemcpyDeviceToHost, m->st));
     SOV_CUDA(cudaStreamSynchronize(m->st));
+    const size_t nx = static_cast<size_t>(batch) * n_ipm, ny = static_cast<size_t>(batch) * m_ipm;
+    sov::parallel_memcpy(x, hl, sizeof(double) * nx);
+    sov::parallel_memcpy(y, hl + nx, sizeof(double) * ny);
+    sov::parallel_memcpy(s, hl + nx + ny, sizeof(double) * nx);
     return SOV_OK;
   } catch (const std::exception&) {
     return SOV_E_CUDA;
