@@ -1950,19 +1950,18 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
 }
 
 std::string autotune(int count, const sov_model* models, const sov_options* opt, const std::string& file) {
-  // Per bucket: time the bucket alone with 128 / 256 / 512 threads per CTA and keep the fastest.
+  // Per bucket: time the bucket alone with 128 / 256 / 512 threads per CTA and take the fastest.
   std::unique_ptr<Batch> B(batch_create(count, models, opt));
   SOV_CUDA(cudaEventSynchronize(B->ready));
   cudaStream_t st;
   SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  std::ostringstream rep;
-  rep << "{";
-  bool first = true;
-  for (auto& bk : B->buckets) {
+  std::vector<std::string> alone(B->buckets.size());
+  std::vector<int> alone_t(B->buckets.size());
+  for (size_t k = 0; k < B->buckets.size(); ++k) {
+    auto& bk = B->buckets[k];
     float best_ms = 1e30f;
     int best_t = bk->threads;
-    rep << (first ? "" : ", ") << "\"m<=" << bk->mmax << "\": {";
-    first = false;
+    std::ostringstream part;
     bool f2 = true;
     for (int threads : {128, 256, 512}) {
       const int grid = grid_for(bk->mmax, threads, bk->count);
@@ -1986,24 +1985,69 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
       }
-      rep << (f2 ? "" : ", ") << "\"" << threads << "\": " << ms_min;
+      part << (f2 ? "" : ", ") << "\"" << threads << "\": " << ms_min;
       f2 = false;
       if (ms_min < best_ms) {
         best_ms = ms_min;
         best_t = threads;
       }
     }
-    rep << ", \"chosen\": " << best_t << ", \"count\": " << bk->count << "}";
+    alone[k] = part.str();
+    alone_t[k] = best_t;
+    bk->threads = best_t;
+    bk->grid = grid_for(bk->mmax, best_t, bk->count);
+  }
+  // Then the buckets together, as a solve runs them (concurrently, on forked streams): one pass
+  // over the buckets trying each other width with the rest fixed, timing the whole step (best of
+  // two); a change is kept only if the step gets at least 1 % faster.
+  auto step_ms = [&]() {
+    float best = 1e30f;
+    for (int r = 0; r < 2; ++r) {
+      batch_launch(B.get(), st, true);
+      batch_finish(B.get());
+      best = std::min(best, static_cast<float>(B->kernel_ms));
+    }
+    return best;
+  };
+  float cur = step_ms();
+  for (auto& bk : B->buckets) {
+    const int first_t = bk->threads;
+    for (int threads : {128, 256, 512}) {
+      if (threads == first_t) continue;
+      const int old_t = bk->threads, old_g = bk->grid;
+      bk->threads = threads;
+      bk->grid = grid_for(bk->mmax, threads, bk->count);
+      const float ms = step_ms();
+      if (ms < 0.99f * cur) {
+        cur = ms;
+      } else {
+        bk->threads = old_t;
+        bk->grid = old_g;
+      }
+    }
+  }
+  SOV_CUDA(cudaStreamSynchronize(st));
+  cudaStreamDestroy(st);
+  // per bucket: the widths timed alone (ms), the width fastest alone, the width kept for the
+  // concurrent step, its LPs; then the step time with the alone choices and with the kept ones
+  std::ostringstream rep;
+  rep << "{";
+  {
     std::lock_guard<std::mutex> g(g_tune_mu);
-    g_tuned_threads[bk->mmax] = best_t;
+    for (size_t k = 0; k < B->buckets.size(); ++k) {
+      const auto& bk = B->buckets[k];
+      g_tuned_threads[bk->mmax] = bk->threads;
+      rep << (k ? ", " : "") << "\"m<=" << bk->mmax << "\": {" << alone[k] << ", \"alone\": " << alone_t[k]
+          << ", \"chosen\": " << bk->threads << ", \"count\": " << bk->count << "}";
+    }
   }
   rep << "}";
-  cudaStreamDestroy(st);
+  std::string out = rep.str();
   if (!file.empty()) {
     std::ofstream o(file);
-    o << rep.str() << "\n";
+    o << out << "\n";
   }
-  return rep.str();
+  return out;
 }
 
 }  // namespace sov
