@@ -315,6 +315,23 @@ def run_batched_warm_start(args):
         keep.append(a)
         opts[k].warm_x, opts[k].warm_y, opts[k].warm_s = (A.dptr(v) for v in a)
     t_warm, warm = run(opts, C.sizeof(A.SovOptions), max(1, args.steps))
+    # the same starts handed over on the device (sov_lp_solve_batch_predicted): prediction and solve
+    # in one call, the starts never in host memory
+    norms = [np.ascontiguousarray(v, dtype=np.float64) for v in (ws.fin.mean, ws.fin.std, ws.fout.mean, ws.fout.std)]
+    params_c = np.ascontiguousarray(params, dtype=np.float64)
+
+    def run_pred(steps):
+        best = float("inf")
+        for _ in range(steps):
+            t = time.perf_counter()
+            _lib.check(lib.sov_lp_solve_batch_predicted(ws.mlp.h, params_c.ctypes.data, *(v.ctypes.data for v in norms),
+                                                        ws.n_ipm, ws.m_ipm, 1e-6, count, arr, C.byref(base), res))
+            best = min(best, time.perf_counter() - t)
+        return best, [(r.status, r.iterations, r.objective_value, r.diagnostics.contents.warm_start_used) for r in res]
+
+    run_pred(1)  # warm-up
+    t_pred_dev, warm_dev = run_pred(max(1, args.steps))
+    same_dev = all(a == b for a, b in zip(warm, warm_dev))
     ok = [k for k in range(count) if cold[k][0] == A.OPTIMAL and warm[k][0] == A.OPTIMAL]
     err = max(abs(cold[k][2] - warm[k][2]) / max(1.0, abs(cold[k][2])) for k in ok) if ok else None
     del keep
@@ -341,7 +358,8 @@ def run_batched_warm_start(args):
           cold=dict(lps_per_s=count / (ms_cold * 1e-3), mean_iterations=float(np.mean([c[1] for c in cold])),
                     e2e_lps_per_s=count / t_cold),
           warm=dict(lps_per_s=value, mean_iterations=float(np.mean([w[1] for w in warm])),
-                    used=int(sum(w[3] for w in warm)), e2e_lps_per_s=count / (t_warm + t_pred), predict_s=t_pred),
+                    used=int(sum(w[3] for w in warm)), e2e_lps_per_s=count / (t_warm + t_pred), predict_s=t_pred,
+                    e2e_device_starts_lps_per_s=count / t_pred_dev, device_starts_identical=same_dev),
           speedup_warm_vs_cold=ms_cold / ms_warm, optimal=f"{len(ok)}/{count}",
           max_rel_obj_diff_warm_vs_cold=err, train_loss=loss, seconds=dict(generate=t_gen, train=t_train),
           e2e=dict(value=count / (t_warm + t_pred), unit=UNIT,

@@ -280,6 +280,16 @@ int sov_mlp_forward(sov_mlp* mlp, const float* x, int32_t batch, float* y);
 int sov_mlp_predict_start(sov_mlp* mlp, const double* params, int32_t batch, const double* in_mean,
                           const double* in_std, const double* out_mean, const double* out_std, int32_t n_ipm,
                           int32_t m_ipm, double delta, double* x, double* y, double* s);
+/* sov_lp_solve_batch with every LP started from the network's prediction for its parameters (row k
+ * of params, batch = count), without the starts leaving the device: the prediction as in
+ * sov_mlp_predict_start, then each LP's start gathered into the batch on the GPU. One options block
+ * (or NULL) for all LPs; its warm_x/y/s are ignored. Every batched LP's IPM form must have n_ipm
+ * columns and m_ipm rows (else SOV_E_ARGUMENT); each start is judged by the batch's safeguard like a
+ * caller's. Results are those of sov_lp_solve_batch given the same starts from host arrays. */
+int sov_lp_solve_batch_predicted(sov_mlp* mlp, const double* params, const double* in_mean, const double* in_std,
+                                 const double* out_mean, const double* out_std, int32_t n_ipm, int32_t m_ipm,
+                                 double delta, int32_t count, const sov_model* models, const sov_options* opt,
+                                 sov_result* results);
 /* loss = mean((f(x) - t)^2); grad (param_count floats, or NULL) = its gradient */
 int sov_mlp_loss_grad(sov_mlp* mlp, const float* x, const float* t, int32_t batch, double* loss, float* grad);
 /* epochs of shuffled mini-batches over count samples; final_loss = mean loss of the last epoch */

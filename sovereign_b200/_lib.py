@@ -20,6 +20,7 @@ EXPORTS = [
     "sov_batch_transfer_bytes", "sov_batch_destroy", "sov_autotune", "sov_spmv_csc", "sov_normal_factor_solve", "sov_normal_factor_solve_noalloc", "sov_device_info",
     "sov_last_error", "sov_mlp_create", "sov_mlp_param_count", "sov_mlp_get_params", "sov_mlp_set_params",
     "sov_mlp_forward", "sov_mlp_predict_start", "sov_mlp_loss_grad", "sov_mlp_train", "sov_mlp_destroy",
+    "sov_lp_solve_batch_predicted",
 ]
 
 _lib = None
@@ -74,6 +75,9 @@ def load(build_if_missing: bool = True):
     lib.sov_mlp_predict_start.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                           C.c_void_p]
+    lib.sov_lp_solve_batch_predicted.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p]
     lib.sov_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_void_p]
     lib.sov_mlp_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                   C.c_uint64, C.POINTER(C.c_double)]

@@ -1304,6 +1304,21 @@ __global__ void __launch_bounds__(kScaleThreads) k_batch_scale(LpMeta* __restric
   }
 }
 
+// Each LP's start [x | y | s] gathered into its slots of the batch's warm region from starts that
+// are already on the device (a warm-start network's output, LP k at offset k of each array).
+__global__ void __launch_bounds__(kScaleThreads) k_batch_starts(const LpMeta* __restrict__ meta, double* __restrict__ warm,
+                                                                DeviceStarts st, int first_lp) {
+  const LpMeta& mt = meta[blockIdx.x];
+  if (mt.m < 0 || mt.w_off < 0) return;
+  const size_t k = static_cast<size_t>(first_lp) + blockIdx.x;
+  double* w = warm + mt.w_off;
+  for (int j = threadIdx.x; j < st.n; j += kScaleThreads) {
+    w[j] = st.x[k * st.n + j];
+    w[st.n + st.m + j] = st.s[k * st.n + j];
+  }
+  for (int i = threadIdx.x; i < st.m; i += kScaleThreads) w[st.n + i] = st.y[k * st.m + i];
+}
+
 // publish_iterate's scale products (interior_point.cpp:541-563) for every batched LP, one CTA per
 // LP, from the final or the best iterate as the solve chose: cs*x and s/cs for the model's columns,
 // rs*y for its rows. The host adds the shift (primal = shift + cs*x), so the published values are
@@ -1356,7 +1371,8 @@ size_t align8(size_t v) { return (v + 7) & ~size_t(7); }
 
 }  // namespace
 
-Batch* batch_create(int count, const sov_model* models, const sov_options* opt_in, int opt_stride) {
+Batch* batch_create(int count, const sov_model* models, const sov_options* opt_in, int opt_stride,
+                    const DeviceStarts* starts, int first_lp) {
   auto B = std::make_unique<Batch>();
   B->count = count;
   B->models.assign(models, models + count);
@@ -1433,7 +1449,14 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     mt.otol = opt.optimality_tol;
     mt.tau = opt.fraction_to_boundary;
     mt.w_off = -1;
-    if (opt.warm_x && opt.warm_y && opt.warm_s) {
+    if (starts) {
+      if (sh.n != starts->n || sh.m != starts->m)
+        throw std::runtime_error("model " + std::to_string(first_lp + i) + ": IPM form " + std::to_string(sh.m) +
+                                 " x " + std::to_string(sh.n) + " does not match the starts' " +
+                                 std::to_string(starts->m) + " x " + std::to_string(starts->n));
+      mt.w_off = wv;
+      wv += 2LL * sh.n + sh.m;
+    } else if (opt.warm_x && opt.warm_y && opt.warm_s) {
       mt.w_off = wv;
       wv += 2LL * sh.n + sh.m;
     }
@@ -1505,6 +1528,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   const size_t o_scl = align8(o_ord + sizeof(int) * all_orders.size());
   const size_t total = o_scl + sizeof(double) * (nv + mv);
   B->h2d_bytes = static_cast<double>(o_ord + sizeof(int) * all_orders.size() - (sizeof(int) + sizeof(double)) * nnz);
+  if (starts) B->h2d_bytes -= static_cast<double>(sizeof(double) * wv);  // gathered on the device
   B->in.alloc(total);
   B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
   B->out.alloc(count);
@@ -1543,7 +1567,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
         double* rv = reinterpret_cast<double*>(h + o_rv) + mt.a_off;
         double* bb = reinterpret_cast<double*>(h + o_b) + mt.mv_off;
         double* cc = reinterpret_cast<double*>(h + o_c) + mt.nv_off;
-        if (mt.w_off >= 0) {
+        if (mt.w_off >= 0 && !starts) {
           const sov_options& o = opt_of(i);
           double* wd = reinterpret_cast<double*>(h + o_w) + mt.w_off;
           std::memcpy(wd, o.warm_x, sizeof(double) * mt.n);
@@ -1583,7 +1607,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
       copy_range(o_cv + sizeof(double) * r0.nnz, sizeof(double) * (r1.nnz - r0.nnz));
       copy_range(o_b + sizeof(double) * r0.mv, sizeof(double) * (r1.mv - r0.mv));
       copy_range(o_c + sizeof(double) * r0.nv, sizeof(double) * (r1.nv - r0.nv));
-      copy_range(o_w + sizeof(double) * r0.wv, sizeof(double) * (r1.wv - r0.wv));
+      if (!starts) copy_range(o_w + sizeof(double) * r0.wv, sizeof(double) * (r1.wv - r0.wv));
     }
     std::memcpy(h + o_meta, B->meta.data(), sizeof(LpMeta) * count);
     if (!all_orders.empty()) std::memcpy(h + o_ord, all_orders.data(), sizeof(int) * all_orders.size());
@@ -1602,6 +1626,12 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     // the scaling, then the row-wise copies built on the device from the (scaled) columns
     unsigned char* din = B->in.p;
     B->scl = reinterpret_cast<double*>(din + o_scl);
+    if (starts) {
+      if (starts->ready) SOV_CUDA(cudaStreamWaitEvent(cs, starts->ready, 0));
+      k_batch_starts<<<count, kScaleThreads, 0, cs>>>(reinterpret_cast<const LpMeta*>(din + o_meta),
+                                                      reinterpret_cast<double*>(din + o_w), *starts, first_lp);
+      SOV_CUDA(cudaGetLastError());
+    }
     k_batch_scale<<<count, kScaleThreads, 0, cs>>>(
         reinterpret_cast<LpMeta*>(din + o_meta), reinterpret_cast<const int*>(din + o_cp),
         reinterpret_cast<const int*>(din + o_ri), reinterpret_cast<double*>(din + o_cv),
@@ -1909,7 +1939,8 @@ void parallel_memcpy(void* dst, const void* src, size_t bytes) {
   });
 }
 
-int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results) {
+int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results,
+                const DeviceStarts* starts) {
   if (count == 0) return SOV_OK;
   // Large batches in parts, pipelined: each part's graph is launched as soon as its inputs are on
   // the device, so the host standard form and the copies of the next part overlap the solves of the
@@ -1929,7 +1960,7 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
                                  ? reinterpret_cast<const sov_options*>(reinterpret_cast<const char*>(opt) +
                                                                         static_cast<size_t>(lo) * opt_stride)
                                  : opt;
-      batches.emplace_back(batch_create(hi - lo, models + lo, o, opt_stride));
+      batches.emplace_back(batch_create(hi - lo, models + lo, o, opt_stride, starts, lo));
       cudaStream_t st = CudaObjectPool::get().stream(false);
       streams.push_back(st);
       batch_launch(batches.back().get(), st, true);

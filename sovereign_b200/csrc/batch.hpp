@@ -11,8 +11,18 @@ namespace sov {
 
 struct Batch;
 
-int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results);
-Batch* batch_create(int count, const sov_model* models, const sov_options* opt, int opt_stride = 0);
+// Starts already on the device for every LP of a call (a warm-start network's output): LP k's
+// x at x + k*n, y at y + k*m, s at s + k*n; every batched LP must have n IPM columns and m rows.
+struct DeviceStarts {
+  const double *x, *y, *s;
+  int n, m;
+  cudaEvent_t ready;  // recorded when the starts are written (or null: already written)
+};
+
+int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results,
+                const DeviceStarts* starts = nullptr);
+Batch* batch_create(int count, const sov_model* models, const sov_options* opt, int opt_stride = 0,
+                    const DeviceStarts* starts = nullptr, int first_lp = 0);
 void batch_solve(Batch* b, cudaStream_t st);
 void batch_results(Batch* b, sov_result* results);
 void batch_stats(const Batch* b, int* launches, double* kernel_ms, double* bytes, double* flops);

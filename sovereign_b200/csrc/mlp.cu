@@ -288,6 +288,7 @@ struct Mlp {
       if (p) cudaFreeHost(p);
     }
   } landing, staging;  // the decoded starts out; the parameters in
+  cudaEvent_t predicted = nullptr;  // starts written (sov_lp_solve_batch_predicted)
   Buf<int> err;
   long long step = 0;
   cudaStream_t st = nullptr;
@@ -437,6 +438,40 @@ int sov_mlp_forward(sov_mlp* h, const float* x, int32_t batch, float* y) {
   }
 }
 
+namespace {
+
+// Normalization, the network and the decoding of `batch` starts on the device: returns the decoded
+// [x (batch*n_ipm) | y (batch*m_ipm) | s (batch*n_ipm)] in m->start, stream m->st (not synchronized).
+double* predict_on_device(Mlp* m, const double* params, int batch, const double* in_mean, const double* in_std,
+                          const double* out_mean, const double* out_std, int n_ipm, int m_ipm, double delta) {
+  const int n_in = m->dims[0], n_out = m->dims.back();
+  m->ensure_batch(batch);
+  const size_t cnt_in = static_cast<size_t>(batch) * n_in, cnt_out = static_cast<size_t>(batch) * n_out;
+  if (m->raw_in.n < cnt_in) m->raw_in.alloc(cnt_in);
+  if (m->norm.n < static_cast<size_t>(2 * (n_in + n_out))) m->norm.alloc(2 * (n_in + n_out));
+  if (m->start.n < cnt_out) m->start.alloc(cnt_out);
+  double* nm = m->norm.p;
+  double* hs = static_cast<double*>(m->staging.get(sizeof(double) * cnt_in));
+  sov::parallel_memcpy(hs, params, sizeof(double) * cnt_in);
+  SOV_CUDA(cudaMemcpyAsync(m->raw_in.p, hs, sizeof(double) * cnt_in, cudaMemcpyHostToDevice, m->st));
+  SOV_CUDA(cudaMemcpyAsync(nm, in_mean, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
+  SOV_CUDA(cudaMemcpyAsync(nm + n_in, in_std, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
+  SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in, out_mean, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
+  SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in + n_out, out_std, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
+  sov::k_normalize_in<<<1184, 256, 0, m->st>>>(m->raw_in.p, nm, nm + n_in, static_cast<long long>(cnt_in), n_in,
+                                              m->act[0].p);
+  m->forward(batch);
+  double* dx = m->start.p;
+  double* dy = dx + static_cast<size_t>(batch) * n_ipm;
+  double* ds = dy + static_cast<size_t>(batch) * m_ipm;
+  sov::k_decode_start<<<1184, 256, 0, m->st>>>(m->act.back().p, nm + 2 * n_in, nm + 2 * n_in + n_out, batch, n_ipm,
+                                              m_ipm, delta, dx, dy, ds);
+  SOV_CUDA(cudaGetLastError());
+  return dx;
+}
+
+}  // namespace
+
 int sov_mlp_predict_start(sov_mlp* h, const double* params, int32_t batch, const double* in_mean,
                           const double* in_std, const double* out_mean, const double* out_std, int32_t n_ipm,
                           int32_t m_ipm, double delta, double* x, double* y, double* s) {
@@ -445,30 +480,9 @@ int sov_mlp_predict_start(sov_mlp* h, const double* params, int32_t batch, const
       m_ipm < 0 || 2 * n_ipm + m_ipm != m->dims.back())
     return SOV_E_ARGUMENT;
   try {
-    const int n_in = m->dims[0], n_out = m->dims.back();
-    m->ensure_batch(batch);
-    const size_t cnt_in = static_cast<size_t>(batch) * n_in, cnt_out = static_cast<size_t>(batch) * n_out;
-    if (m->raw_in.n < cnt_in) m->raw_in.alloc(cnt_in);
-    if (m->norm.n < static_cast<size_t>(2 * (n_in + n_out))) m->norm.alloc(2 * (n_in + n_out));
-    if (m->start.n < cnt_out) m->start.alloc(cnt_out);
-    double* nm = m->norm.p;
-    double* hs = static_cast<double*>(m->staging.get(sizeof(double) * cnt_in));
-    sov::parallel_memcpy(hs, params, sizeof(double) * cnt_in);
-    SOV_CUDA(cudaMemcpyAsync(m->raw_in.p, hs, sizeof(double) * cnt_in, cudaMemcpyHostToDevice, m->st));
-    SOV_CUDA(cudaMemcpyAsync(nm, in_mean, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
-    SOV_CUDA(cudaMemcpyAsync(nm + n_in, in_std, sizeof(double) * n_in, cudaMemcpyHostToDevice, m->st));
-    SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in, out_mean, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
-    SOV_CUDA(cudaMemcpyAsync(nm + 2 * n_in + n_out, out_std, sizeof(double) * n_out, cudaMemcpyHostToDevice, m->st));
-    sov::k_normalize_in<<<1184, 256, 0, m->st>>>(m->raw_in.p, nm, nm + n_in, static_cast<long long>(cnt_in), n_in,
-                                                m->act[0].p);
-    m->forward(batch);
-    double* dx = m->start.p;
-    double* dy = dx + static_cast<size_t>(batch) * n_ipm;
-    double* ds = dy + static_cast<size_t>(batch) * m_ipm;
-    sov::k_decode_start<<<1184, 256, 0, m->st>>>(m->act.back().p, nm + 2 * n_in, nm + 2 * n_in + n_out, batch, n_ipm,
-                                                m_ipm, delta, dx, dy, ds);
-    SOV_CUDA(cudaGetLastError());
+    double* dx = predict_on_device(m, params, batch, in_mean, in_std, out_mean, out_std, n_ipm, m_ipm, delta);
     // [x | y | s] are adjacent on the device: one copy into the pinned landing buffer
+    const size_t cnt_out = static_cast<size_t>(batch) * m->dims.back();
     double* hl = static_cast<double*>(m->landing.get(sizeof(double) * cnt_out));
     SOV_CUDA(cudaMemcpyAsync(hl, dx, sizeof(double) * cnt_out, cudaMemcpyDeviceToHost, m->st));
     SOV_CUDA(cudaStreamSynchronize(m->st));
@@ -479,6 +493,34 @@ int sov_mlp_predict_start(sov_mlp* h, const double* params, int32_t batch, const
     return SOV_OK;
   } catch (const std::exception&) {
     return SOV_E_CUDA;
+  }
+}
+
+int sov_lp_solve_batch_predicted(sov_mlp* h, const double* params, const double* in_mean, const double* in_std,
+                                 const double* out_mean, const double* out_std, int32_t n_ipm, int32_t m_ipm,
+                                 double delta, int32_t count, const sov_model* models, const sov_options* opt,
+                                 sov_result* results) {
+  auto m = reinterpret_cast<Mlp*>(h);
+  if (!m || !params || !in_mean || !in_std || !out_mean || !out_std || !models || !results || count <= 0 ||
+      n_ipm < 0 || m_ipm < 0 || 2 * n_ipm + m_ipm != m->dims.back())
+    return SOV_E_ARGUMENT;
+  try {
+    // the prediction runs on the network's stream while the host builds the first part; each part
+    // gathers its starts after the event
+    double* dx = predict_on_device(m, params, count, in_mean, in_std, out_mean, out_std, n_ipm, m_ipm, delta);
+    if (!m->predicted) SOV_CUDA(cudaEventCreateWithFlags(&m->predicted, cudaEventDisableTiming));
+    SOV_CUDA(cudaEventRecord(m->predicted, m->st));
+    const sov::DeviceStarts st{dx, dx + static_cast<size_t>(count) * n_ipm,
+                               dx + static_cast<size_t>(count) * (n_ipm + m_ipm), n_ipm, m_ipm, m->predicted};
+    const int rc = sov::solve_batch(count, models, opt, 0, results, &st);
+    SOV_CUDA(cudaStreamSynchronize(m->st));
+    return rc;
+  } catch (const sov::CudaError&) {
+    cudaStreamSynchronize(m->st);  // the pinned input staging is reused by the next call
+    return SOV_E_CUDA;
+  } catch (const std::exception&) {
+    cudaStreamSynchronize(m->st);
+    return SOV_E_ARGUMENT;
   }
 }
 
@@ -545,6 +587,7 @@ void sov_mlp_destroy(sov_mlp* h) {
   auto m = reinterpret_cast<Mlp*>(h);
   if (!m) return;
   if (m->st) cudaStreamDestroy(m->st);
+  if (m->predicted) cudaEventDestroy(m->predicted);
   delete m;
 }
 

@@ -150,3 +150,28 @@ class WarmStart:
         check(load().sov_mlp_predict_start(self.mlp.h, p.ctypes.data, b, *(v.ctypes.data for v in f), n, m, delta,
                                            xs.ctypes.data, ys.ctypes.data, ss.ctypes.data))
         return [(xs[k], ys[k], ss[k]) for k in range(b)]
+
+    def solve_batch(self, models, params: np.ndarray, delta: float = 1e-6, options=None, with_diag: bool = False):
+        """The batch solved from the network's starts without their leaving the device
+        (sov_lp_solve_batch_predicted): the same results as solve_batch(models,
+        warm_starts=self.predict(params)), minus the starts' round trip through host memory."""
+        import ctypes as C
+        from . import abi
+        from .ipm import InteriorPointOptions
+        from .model import ResultBuffers
+        p = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+        if p.shape[0] != len(models):
+            raise ValueError("one parameter row per model")
+        f = [np.ascontiguousarray(v, dtype=np.float64) for v in (self.fin.mean, self.fin.std, self.fout.mean,
+                                                                  self.fout.std)]
+        opt = (options or InteriorPointOptions()).to_abi()
+        bufs = [ResultBuffers(m, with_diag=with_diag) for m in models]
+        arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
+        res = (abi.SovResult * len(models))(*[b.raw for b in bufs])
+        check(load().sov_lp_solve_batch_predicted(self.mlp.h, p.ctypes.data, *(v.ctypes.data for v in f), self.n_ipm,
+                                                  self.m_ipm, delta, len(models), arr, C.byref(opt), res))
+        out = []
+        for b, r in zip(bufs, res):
+            b.raw = r
+            out.append(b.to_result())
+        return out

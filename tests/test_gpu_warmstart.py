@@ -88,3 +88,27 @@ def test_predict_start_matches_host_decoding():
         np.testing.assert_allclose(got[k][0], xs[k], rtol=1e-12)
         np.testing.assert_allclose(got[k][1], out[k, n:n + m], rtol=1e-12, atol=1e-12)
         np.testing.assert_allclose(got[k][2], ss[k], rtol=1e-12)
+
+
+def test_batch_from_device_starts_equals_host_starts():
+    # sov_lp_solve_batch_predicted keeps the predicted starts on the device; given the same network
+    # and parameters it must give exactly what the batch gives with the same starts from host arrays
+    from sovereign_b200.ipm import solve_batch
+    fam = P.TransportFamily()
+    train = [fam.instance_from_seed(300 + k) for k in range(64)]
+    test = [fam.instance_from_seed(900 + k) for k in range(48)]
+    early, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=5))
+    ws = WarmStart(fam.param_dim, early[0].n_ipm, early[0].m_ipm, hidden=64, layers=2, seed=0)
+    ws.fit(np.stack([p for _, p in train]), early, epochs=30, batch=32, lr=2e-3)
+    models, params = [m for m, _ in test], np.stack([p for _, p in test])
+    host = solve_batch(models, warm_starts=ws.predict(params), with_diag=True)
+    dev = ws.solve_batch(models, params, with_diag=True)
+    for h, d in zip(host, dev):
+        assert d.status_name == "OPTIMAL" and h.status == d.status and h.iterations == d.iterations
+        assert h.objective_value == d.objective_value
+        np.testing.assert_array_equal(h.primal, d.primal)
+        assert h.diagnostics["warm_start_used"] == d.diagnostics["warm_start_used"]
+    assert sum(d.diagnostics["warm_start_used"] for d in dev) > 0
+    # an LP whose IPM form does not match the network's output is refused
+    with pytest.raises(Exception):
+        ws.solve_batch([P.transport(5, 6, 1)], params[:1])
