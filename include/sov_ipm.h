@@ -60,7 +60,8 @@ enum {
   SOV_E_NO_DEVICE = -2,  /* no CUDA device or the sm_100a kernels cannot load */
   SOV_E_CUDA = -3,       /* a CUDA call failed; the message names it */
   SOV_E_TOO_LARGE = -4,  /* model exceeds the engine's size limits */
-  SOV_E_UNSUPPORTED = -5 /* model shape this engine does not solve (message says why) */
+  SOV_E_UNSUPPORTED = -5, /* model shape this engine does not solve (message says why) */
+  SOV_E_NUMERICAL = -6    /* a factorization met a non-finite pivot (NaN or Inf in the inputs) */
 };
 
 /* Arithmetic of the Newton solves. */
@@ -249,7 +250,12 @@ int sov_normal_factor_solve(int32_t m, int32_t n, const int32_t* col_ptr, const 
  * memory limit): the dense FP64 factor of A diag(d) A' + 1e-12 I and the solve for nrhs
  * right-hand sides, like sov_normal_factor_solve, but col_ptr, row_idx, values, d and rhs
  * (column-major m x nrhs, overwritten by the solution) are DEVICE pointers, rows within a column
- * must be distinct, and the work runs on cuda_stream. It calls no cudaMalloc or cudaFree: its
+ * must be distinct, and the work runs on cuda_stream. The device arrays cannot be checked on the
+ * host: entries whose row lies outside [0, m), and columns whose col_ptr decreases, are skipped on
+ * the device and the call returns SOV_E_ARGUMENT; col_ptr[n] must not exceed the length of
+ * row_idx and values. A non-finite pivot returns SOV_E_NUMERICAL. The normal matrix is summed
+ * with FP64 atomics, so results can differ from run to run in the last bits (the allocating
+ * entry point sums in a fixed order). It calls no cudaMalloc or cudaFree: its
  * working storage is one fixed device array sized for m <= SOV_NOALLOC_MAX_ROWS (about 2.3 MB,
  * held by every GPU that loads the library until the process exits); larger m returns
  * SOV_E_TOO_LARGE. The first call on a device looks that array up (cudaGetSymbolAddress), so it
@@ -283,9 +289,11 @@ int sov_mlp_predict_start(sov_mlp* mlp, const double* params, int32_t batch, con
 /* sov_lp_solve_batch with every LP started from the network's prediction for its parameters (row k
  * of params, batch = count), without the starts leaving the device: the prediction as in
  * sov_mlp_predict_start, then each LP's start gathered into the batch on the GPU. One options block
- * (or NULL) for all LPs; its warm_x/y/s are ignored. Every batched LP's IPM form must have n_ipm
- * columns and m_ipm rows (else SOV_E_ARGUMENT); each start is judged by the batch's safeguard like a
- * caller's. Results are those of sov_lp_solve_batch given the same starts from host arrays. */
+ * (or NULL) for all LPs; its warm_x/y/s are ignored. Every LP's IPM form must have n_ipm columns
+ * and m_ipm rows (else SOV_E_ARGUMENT); each start is judged by the batch's safeguard like a
+ * caller's. LPs the batched kernel does not take (more than 128 IPM rows) get their start copied
+ * to the host and passed to the single-problem engine as its warm start. Results are those of
+ * sov_lp_solve_batch given the same starts from host arrays. */
 int sov_lp_solve_batch_predicted(sov_mlp* mlp, const double* params, const double* in_mean, const double* in_std,
                                  const double* out_mean, const double* out_std, int32_t n_ipm, int32_t m_ipm,
                                  double delta, int32_t count, const sov_model* models, const sov_options* opt,

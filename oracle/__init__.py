@@ -22,13 +22,15 @@ from sovereign_b200.model import Model, ResultBuffers
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_PATH = os.path.join(HERE, "libsovoracle.so")
 REFERENCE_PATH = os.path.join(HERE, "_ref", "libsovref.so")
-REFERENCE_SRC = "/root/reference/solver/lp/src/interior_point.cpp"
+# the reference checkout: the one place its location is set (SOVEREIGN_REFERENCE_DIR overrides)
+REFERENCE_DIR = os.environ.get("SOVEREIGN_REFERENCE_DIR", "/root/reference")
+REFERENCE_SRC = os.path.join(REFERENCE_DIR, "solver", "lp", "src", "interior_point.cpp")
 
 
 def build(reference: bool = True) -> None:
     """Compile the restatement, and the reference library when its sources are present."""
     target = ["all"] if reference and os.path.exists(REFERENCE_SRC) else ["oracle"]
-    subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_DIR}"] + target, check=True)
 
 
 _libs: dict = {}

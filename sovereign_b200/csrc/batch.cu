@@ -762,9 +762,11 @@ size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(m
 // footprint, so launches (and launches captured in a graph) need no per-launch attribute call.
 void ensure_smem_limits() {
   const int smem = static_cast<int>(batch_smem(kBatchMaxRows));
-  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  once_per_device((const void*)k_batch_ipm<128>, [&] {
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  });
 }
 
 template <int NT>
@@ -1104,6 +1106,11 @@ struct Batch {
   std::vector<Pub> pub;
   HBuf<double> pubdata;
   std::vector<int> fallback;  // LPs too large for the batched kernel
+  // starts handed over on the device (DeviceStarts), kept for the fallback LPs, which take theirs
+  // as host warm starts
+  bool has_dstarts = false;
+  DeviceStarts dstarts{};
+  int first_lp = 0;
   sov_options opt{};
   std::vector<sov_options> opts;  // per-LP options (empty: `opt` for all)
   struct Bucket {
@@ -1387,6 +1394,11 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
                                                          static_cast<size_t>(i) * opt_stride);
   }
   auto opt_of = [&](int i) -> const sov_options& { return B->opts.empty() ? B->opt : B->opts[i]; };
+  if (starts) {
+    B->has_dstarts = true;
+    B->dstarts = *starts;
+    B->first_lp = first_lp;
+  }
   ensure_smem_limits();
   // 1. shapes, in parallel. LPs with plain columns are later built in place, straight into the
   //    pinned staging; the others get a StdForm here (build_ipm_form semantics,
@@ -1425,6 +1437,10 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     const sov_options& opt = opt_of(i);
     LpMeta& mt = B->meta[i];
     std::memset(&mt, 0, sizeof(mt));
+    if (starts && (sh.n != starts->n || sh.m != starts->m))
+      throw std::runtime_error("model " + std::to_string(first_lp + i) + ": IPM form " + std::to_string(sh.m) +
+                               " x " + std::to_string(sh.n) + " does not match the starts' " +
+                               std::to_string(starts->m) + " x " + std::to_string(starts->n));
     if (kind[i] == kSingle) {
       B->fallback.push_back(i);
       mt.m = -1;
@@ -1450,10 +1466,6 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     mt.tau = opt.fraction_to_boundary;
     mt.w_off = -1;
     if (starts) {
-      if (sh.n != starts->n || sh.m != starts->m)
-        throw std::runtime_error("model " + std::to_string(first_lp + i) + ": IPM form " + std::to_string(sh.m) +
-                                 " x " + std::to_string(sh.n) + " does not match the starts' " +
-                                 std::to_string(starts->m) + " x " + std::to_string(starts->n));
       mt.w_off = wv;
       wv += 2LL * sh.n + sh.m;
     } else if (opt.warm_x && opt.warm_y && opt.warm_s) {
@@ -1904,10 +1916,26 @@ void batch_results(Batch* B, sov_result* results) {
       std::snprintf(r->message, sizeof(r->message), "IPM: empty model.");
       continue;
     }
+    sov_options o = B->opts.empty() ? B->opt : B->opts[i];
+    std::vector<double> wx, wy, ws;
+    if (B->has_dstarts) {  // this LP's start from the device, used exactly as a host warm start
+      const DeviceStarts& ds = B->dstarts;
+      const size_t k = static_cast<size_t>(B->first_lp) + i;
+      if (ds.ready) SOV_CUDA(cudaEventSynchronize(ds.ready));
+      wx.resize(ds.n);
+      wy.resize(ds.m);
+      ws.resize(ds.n);
+      SOV_CUDA(cudaMemcpy(wx.data(), ds.x + k * ds.n, sizeof(double) * ds.n, cudaMemcpyDeviceToHost));
+      SOV_CUDA(cudaMemcpy(wy.data(), ds.y + k * ds.m, sizeof(double) * ds.m, cudaMemcpyDeviceToHost));
+      SOV_CUDA(cudaMemcpy(ws.data(), ds.s + k * ds.n, sizeof(double) * ds.n, cudaMemcpyDeviceToHost));
+      o.warm_x = wx.data();
+      o.warm_y = wy.data();
+      o.warm_s = ws.data();
+    }
     cudaStream_t st;
     SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     try {
-      solve_single(B->models[i], f, B->opts.empty() ? B->opt : B->opts[i], r, st, nullptr);
+      solve_single(B->models[i], f, o, r, st, nullptr);
     } catch (...) {
       cudaStreamDestroy(st);
       throw;

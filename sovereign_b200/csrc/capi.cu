@@ -43,6 +43,16 @@ int check_device() {
   return SOV_OK;
 }
 
+}  // namespace
+
+namespace sov {
+// The same error record and device check for entry points defined in other files.
+int record_error(int code, const std::string& msg) { return set_error(code, msg); }
+int require_device() { return check_device(); }
+}  // namespace sov
+
+namespace {
+
 int validate(const sov_model* p) {
   if (!p) return set_error(SOV_E_ARGUMENT, "null model");
   if (p->n < 0 || p->m < 0) return set_error(SOV_E_ARGUMENT, "negative dimensions");

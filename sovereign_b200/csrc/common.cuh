@@ -4,8 +4,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace sov {
 
@@ -73,6 +76,33 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+
+// Runs fn() once per (current device, key), thread-safe: kernel attributes such as the opt-in to
+// more than 48 KB of dynamic shared memory are set per device, so every device gets its own call,
+// and host threads that launch concurrently wait for the first one's call to finish.
+inline std::mutex& once_mutex() {
+  static std::mutex m;
+  return m;
+}
+inline std::set<std::pair<int, const void*>>& once_done() {
+  static std::set<std::pair<int, const void*>> s;
+  return s;
+}
+template <class F>
+void once_per_device(const void* key, F&& fn) {
+  int dev = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(once_mutex());
+  if (once_done().count({dev, key})) return;
+  fn();
+  once_done().insert({dev, key});
+}
+constexpr int kMaxDevices = 64;
+
+// Record `msg` as the calling thread's sov_last_error() and return `code` (capi.cu).
+int record_error(int code, const std::string& msg);
+// SOV_OK when an sm_100 device is current, else the recorded SOV_E_NO_DEVICE (capi.cu).
+int require_device();
 
 inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 

@@ -630,11 +630,9 @@ __global__ void __launch_bounds__(256) k_panel_update(T* __restrict__ M, int ld,
 template <class T>
 void dense_potrf_block(const DenseSystem<T>& s, int kb, cudaStream_t st) {
   const size_t smem_potrf = potrf_smem_bytes<T>();
-  static bool attr_set = false;
-  if (!attr_set) {
+  once_per_device((const void*)k_potrf_diag<T>, [&] {
     SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
-    attr_set = true;
-  }
+  });
   k_potrf_diag<T><<<1, 256, smem_potrf, st>>>(s.M, s.mp, kb, s.diag, s.m, s.Linv, s.drop_count, s.fail, s.drop_tol,
                                               nullptr);
 }
@@ -647,12 +645,10 @@ std::atomic<unsigned> g_factor_generation{0};
 template <class T>
 void dense_cholesky(const DenseSystem<T>& s, cudaStream_t st, int* launches) {
   const size_t smem_potrf = potrf_smem_bytes<T>();
-  static bool attr_set = false;
-  if (!attr_set) {
+  once_per_device((const void*)k_panel_update<T>, [&] {
     SOV_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
     SOV_CUDA(cudaFuncSetAttribute(k_panel_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
-    attr_set = true;
-  }
+  });
   if (s.nb >= (1 << kStampPanelBits)) throw std::runtime_error("dense factor: too many row blocks");
   const unsigned gen = (g_factor_generation.fetch_add(1) & ((1u << (31 - kStampPanelBits)) - 1)) << kStampPanelBits;
   // panel 0's diagonal block alone (it also resets the ticket counter); every later one is
@@ -857,16 +853,20 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const T* __restrict__ M, int l
   }
 }
 
+// Co-resident blocks of the cooperative solves, per device (queried once per device).
 int dataflow_grid(int nb) {
-  static int max_blocks = 0;
-  if (max_blocks == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    SOV_CUDA(cudaGetDevice(&dev));
+  static int max_blocks[kMaxDevices] = {};
+  int dev = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  if (dev >= kMaxDevices) throw std::runtime_error("dense solve: device index beyond the supported 64");
+  once_per_device((const void*)&max_blocks, [&] {
+    int sms = 0, per_sm = 0;
     SOV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trsv_fwd<double>, 256, 0));
-    max_blocks = std::max(1, sms * std::max(1, per_sm));
-  }
-  return std::min(nb, max_blocks);
+    max_blocks[dev] = std::max(1, sms * std::max(1, per_sm));
+  });
+  std::lock_guard<std::mutex> g(once_mutex());  // the write above happened under this lock
+  return std::min(nb, max_blocks[dev]);
 }
 
 template <class T>

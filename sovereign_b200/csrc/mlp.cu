@@ -144,12 +144,10 @@ __global__ void __launch_bounds__(kGThreads) k_gemm_bf16(GemmArgs g) {
 }
 
 void gemm(const GemmArgs& g, cudaStream_t st) {
-  static bool attr = false;
   const size_t smem = static_cast<size_t>(kGM + kGN) * kGK * 2;
-  if (!attr) {
+  once_per_device((const void*)k_gemm_bf16, [&] {
     SOV_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  });
   dim3 grid(ceil_div(g.N, kGN), ceil_div(g.M, kGM));
   k_gemm_bf16<<<grid, kGThreads, smem, st>>>(g);
   SOV_LAUNCH_CHECK();

@@ -62,17 +62,33 @@ int resolve(int dev, ScratchPtrs& out) {
 }
 
 // M (column-major, leading dimension ld, lower triangle) += a_p d_k a_q for every pair of
-// entries p, q of column k; rows within a column must be distinct.
-__global__ void k_scatter_normal(int n, const int* __restrict__ cp, const int* __restrict__ ri,
-                                 const double* __restrict__ v, const double* __restrict__ d, double* M, int ld) {
+// entries p, q of column k; rows within a column must be distinct. The caller's device arrays
+// were never seen by the host, so a column whose col_ptr decreases and an entry whose row lies
+// outside [0, m) are skipped and counted in *bad instead of being written.
+__global__ void k_scatter_normal(int n, int m, const int* __restrict__ cp, const int* __restrict__ ri,
+                                 const double* __restrict__ v, const double* __restrict__ d, double* M, int ld,
+                                 int* bad) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
+  const int p0 = cp[k], p1 = cp[k + 1];
+  if (p0 < 0 || p1 < p0) {
+    atomicAdd(bad, 1);
+    return;
+  }
   const double dk = d[k];
-  for (int p = cp[k]; p < cp[k + 1]; ++p)
-    for (int q = cp[k]; q <= p; ++q) {
-      const int r = max(ri[p], ri[q]), c = min(ri[p], ri[q]);
+  for (int p = p0; p < p1; ++p) {
+    const int rp = ri[p];
+    if (rp < 0 || rp >= m) {
+      atomicAdd(bad, 1);
+      continue;
+    }
+    for (int q = p0; q <= p; ++q) {
+      const int rq = ri[q];
+      if (rq < 0 || rq >= m) continue;  // counted once, as entry p
+      const int r = max(rp, rq), c = min(rp, rq);
       atomicAdd(M + static_cast<int64_t>(c) * ld + r, v[p] * dk * v[q]);
     }
+  }
 }
 
 // diag[i] = M_ii + 1e-12 (interior_point.cpp:96-100); padding rows get the identity.
@@ -106,12 +122,16 @@ extern "C" int sov_normal_factor_solve_noalloc(int32_t m, int32_t n, const int32
                                                int32_t* dropped_pivots, void* cuda_stream) {
   using namespace sov;
   if (m <= 0 || n < 0 || nrhs < 0 || !col_ptr || !d || !rhs || (n > 0 && (!row_idx || !values)))
-    return SOV_E_ARGUMENT;
-  if (m > kNoAllocMaxRows) return SOV_E_TOO_LARGE;
+    return record_error(SOV_E_ARGUMENT, "noalloc factor/solve: null array or negative size");
+  if (m > kNoAllocMaxRows)
+    return record_error(SOV_E_TOO_LARGE, "noalloc factor/solve: m = " + std::to_string(m) + " exceeds the fixed "
+                                             "working array (m <= " + std::to_string(kNoAllocMaxRows) + ")");
+  if (int rc = require_device()) return rc;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return SOV_E_NO_DEVICE;
+  if (cudaGetDevice(&dev) != cudaSuccess) return record_error(SOV_E_NO_DEVICE, "noalloc factor/solve: no device");
   ScratchPtrs sp;
-  if (resolve(dev, sp) != SOV_OK) return SOV_E_CUDA;
+  if (resolve(dev, sp) != SOV_OK)
+    return record_error(SOV_E_CUDA, "noalloc factor/solve: cudaGetSymbolAddress of the working array failed");
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
   try {
     const int nb = ceil_div(m, kNB), mp = nb * kNB;
@@ -120,11 +140,19 @@ extern "C" int sov_normal_factor_solve_noalloc(int32_t m, int32_t n, const int32
     double* z = Linv + kScratchLinv;
     double* diag = z + kNoAllocMaxRows;
     unsigned* flags = reinterpret_cast<unsigned*>(sp.i);
-    int* counters = sp.i + 64;  // [0] dropped pivots, [1] non-finite pivot, [2] solve timeout, [3] tickets
+    // [0] dropped pivots, [1] non-finite pivot, [2] solve timeout, [3] tickets, [4] bad entries
+    int* counters = sp.i + 64;
     // clear what must start at zero: the matrix, the flags and the counters
     SOV_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * static_cast<size_t>(mp) * mp, st));
     SOV_CUDA(cudaMemsetAsync(sp.i, 0, sizeof(int) * kScratchInts, st));
-    if (n > 0) k_scatter_normal<<<ceil_div(n, 128), 128, 0, st>>>(n, col_ptr, row_idx, values, d, M, mp);
+    if (n > 0) k_scatter_normal<<<ceil_div(n, 128), 128, 0, st>>>(n, m, col_ptr, row_idx, values, d, M, mp, counters + 4);
+    SOV_LAUNCH_CHECK();
+    int bad = 0;
+    SOV_CUDA(cudaMemcpyAsync(&bad, counters + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SOV_CUDA(cudaStreamSynchronize(st));
+    if (bad)
+      return record_error(SOV_E_ARGUMENT, "noalloc factor/solve: " + std::to_string(bad) +
+                                              " column(s) or entries with col_ptr decreasing or a row outside [0, m)");
     k_finish_diag<<<ceil_div(mp, 128), 128, 0, st>>>(M, m, mp, diag);
     SOV_LAUNCH_CHECK();
     DenseSystem<double> s{M, Linv, diag, m, mp, nb, counters, counters + 1, flags,
@@ -141,9 +169,10 @@ extern "C" int sov_normal_factor_solve_noalloc(int32_t m, int32_t n, const int32
     SOV_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
     SOV_CUDA(cudaStreamSynchronize(st));
     if (dropped_pivots) *dropped_pivots = h[0];
-    if (h[1] || h[2]) return SOV_E_CUDA;  // non-finite pivot, or a solve wait ran out
-  } catch (const std::exception&) {
-    return SOV_E_CUDA;
+    if (h[1]) return record_error(SOV_E_NUMERICAL, "noalloc factor/solve: non-finite pivot");
+    if (h[2]) return record_error(SOV_E_CUDA, "noalloc factor/solve: a triangular-solve wait ran out");
+  } catch (const std::exception& e) {
+    return record_error(SOV_E_CUDA, std::string("noalloc factor/solve: ") + e.what());
   }
   return SOV_OK;
 }

@@ -3,7 +3,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <set>
 #include <thread>
 #include <utility>
 
@@ -24,62 +23,136 @@ std::vector<std::vector<int>> normal_graph(const StdForm& f) {
   return adj;
 }
 
-// Greedy exact minimum degree on the elimination graph (the rule of amd_ordering.cpp:12-130).
-bool minimum_degree(std::vector<std::vector<int>> adj, std::size_t fill_limit, std::vector<int>& perm) {
-  const int n = static_cast<int>(adj.size());
-  perm.assign(n, -1);
-  const double dense_degree = std::max(16.0, 10.0 * std::sqrt(static_cast<double>(n)));
-  std::vector<char> dense(n, 0);
-  std::vector<std::pair<int, int>> dense_nodes;
-  for (int i = 0; i < n; ++i)
-    if (static_cast<double>(adj[i].size()) > dense_degree) {
-      dense[i] = 1;
-      dense_nodes.push_back({static_cast<int>(adj[i].size()), i});
-    }
-  if (!dense_nodes.empty()) {
-    for (int i = 0; i < n; ++i) {
-      if (dense[i]) {
-        std::vector<int>().swap(adj[i]);
-        continue;
-      }
-      auto& l = adj[i];
-      l.erase(std::remove_if(l.begin(), l.end(), [&](int w) { return dense[w] != 0; }), l.end());
-    }
-    std::sort(dense_nodes.begin(), dense_nodes.end());
+// Rows of the elimination graph kept in buckets by their current degree bound: O(1) insert and
+// remove, and the next pivot is the head of the lowest non-empty bucket.
+class DegreeBuckets {
+ public:
+  explicit DegreeBuckets(int n) : head_(n + 1, -1), next_(n, -1), prev_(n, -1), deg_(n, 0) {}
+  void insert(int i, int d) {
+    deg_[i] = d;
+    prev_[i] = -1;
+    next_[i] = head_[d];
+    if (head_[d] >= 0) prev_[head_[d]] = i;
+    head_[d] = i;
+    lowest_ = std::min(lowest_, d);
   }
-  const int n_sparse = n - static_cast<int>(dense_nodes.size());
-  for (int k = n_sparse; k < n; ++k) perm[k] = dense_nodes[k - n_sparse].second;
-  std::set<std::pair<int, int>> queue;
+  void remove(int i) {
+    if (prev_[i] >= 0) next_[prev_[i]] = next_[i];
+    else head_[deg_[i]] = next_[i];
+    if (next_[i] >= 0) prev_[next_[i]] = prev_[i];
+  }
+  int pop_lowest() {
+    while (head_[lowest_] < 0) ++lowest_;
+    const int i = head_[lowest_];
+    remove(i);
+    return i;
+  }
+  int degree(int i) const { return deg_[i]; }
+
+ private:
+  std::vector<int> head_, next_, prev_, deg_;
+  int lowest_ = 0;
+};
+
+// Approximate minimum degree on the quotient graph (P. R. Amestoy, T. A. Davis, I. S. Duff, "An
+// approximate minimum degree ordering algorithm", SIAM J. Matrix Anal. Appl. 17(4), 1996). The
+// elimination graph is never formed: an eliminated row becomes an element standing for the clique
+// of its uneliminated neighbours, each row keeps the rows it still touches directly plus the
+// elements it belongs to, and its degree is the paper's bound
+//   |rows adjacent to i| + |L_p \ i| + sum over its other elements e of |L_e \ L_p|,
+// so one pivot costs the element lists it touches instead of the square of its clique. Elements
+// that fall inside the new one are absorbed. Rows denser than max(16, 10 sqrt(m)) (the paper's
+// dense-row cut) are held back and ordered last, sparsest first. Returns false as soon as the
+// predicted entries of L pass fill_limit (0 = no limit).
+bool minimum_degree(const std::vector<std::vector<int>>& graph, std::size_t fill_limit, std::vector<int>& perm) {
+  enum : char { kRow, kElement, kAbsorbed, kHeld };
+  const int n = static_cast<int>(graph.size());
+  perm.assign(n, -1);
+  const double dense_cut = std::max(16.0, 10.0 * std::sqrt(static_cast<double>(n)));
+  std::vector<char> state(n, kRow);
+  std::vector<std::pair<int, int>> held;  // (degree, row)
   for (int i = 0; i < n; ++i)
-    if (!dense[i]) queue.insert({static_cast<int>(adj[i].size()), i});
-  std::size_t nd = dense_nodes.size();
-  std::size_t predicted = nd * (nd > 0 ? nd - 1 : 0) / 2;
-  std::vector<int> mark(n, -1);
-  int stamp = 0;
-  for (int k = 0; k < n_sparse; ++k) {
-    const int node = queue.begin()->second;
-    queue.erase(queue.begin());
-    perm[k] = node;
-    std::vector<int> clique;
-    clique.swap(adj[node]);
-    predicted += clique.size();
-    if (fill_limit > 0 && predicted > fill_limit) return false;
-    for (int v : clique) {
-      auto& l = adj[v];
-      queue.erase({static_cast<int>(l.size()), v});
-      ++stamp;
-      std::size_t keep = 0;
-      for (int w : l) {
-        if (w == node) continue;
-        mark[w] = stamp;
-        l[keep++] = w;
-      }
-      l.resize(keep);
-      mark[v] = stamp;
-      for (int w : clique)
-        if (mark[w] != stamp) l.push_back(w);
-      queue.insert({static_cast<int>(l.size()), v});
+    if (static_cast<double>(graph[i].size()) > dense_cut) {
+      state[i] = kHeld;
+      held.push_back({static_cast<int>(graph[i].size()), i});
     }
+  std::sort(held.begin(), held.end());
+  const int sparse_rows = n - static_cast<int>(held.size());
+  for (std::size_t h = 0; h < held.size(); ++h) perm[sparse_rows + static_cast<int>(h)] = held[h].second;
+  std::vector<std::vector<int>> rows(n), elems(n), members(n);
+  DegreeBuckets buckets(n);
+  for (int i = 0; i < n; ++i) {
+    if (state[i] != kRow) continue;
+    for (int j : graph[i])
+      if (state[j] == kRow) rows[i].push_back(j);
+    buckets.insert(i, static_cast<int>(rows[i].size()));
+  }
+  std::size_t predicted = held.size() * (held.size() > 0 ? held.size() - 1 : 0) / 2;
+  std::vector<int> in_lp(n, 0), wtag(n, 0), w(n, 0);
+  int remaining = sparse_rows;
+  for (int k = 0; k < sparse_rows; ++k) {
+    const int p = buckets.pop_lowest();
+    const int tag = k + 1;
+    perm[k] = p;
+    in_lp[p] = tag;
+    // L_p: rows adjacent to p directly or through one of its elements, which p absorbs
+    std::vector<int> lp;
+    for (int j : rows[p])
+      if (state[j] == kRow && in_lp[j] != tag) {
+        in_lp[j] = tag;
+        lp.push_back(j);
+      }
+    for (int e : elems[p]) {
+      if (state[e] != kElement) continue;
+      for (int j : members[e])
+        if (state[j] == kRow && in_lp[j] != tag) {
+          in_lp[j] = tag;
+          lp.push_back(j);
+        }
+      state[e] = kAbsorbed;
+      std::vector<int>().swap(members[e]);
+    }
+    state[p] = kElement;
+    std::vector<int>().swap(rows[p]);
+    std::vector<int>().swap(elems[p]);
+    --remaining;
+    predicted += lp.size();
+    if (fill_limit > 0 && predicted > fill_limit) return false;
+    // every row of L_p: drop absorbed elements and the rows now reached through p, join p
+    for (int i : lp) {
+      buckets.remove(i);
+      auto& E = elems[i];
+      E.erase(std::remove_if(E.begin(), E.end(), [&](int e) { return state[e] != kElement; }), E.end());
+      auto& R = rows[i];
+      R.erase(std::remove_if(R.begin(), R.end(), [&](int j) { return state[j] != kRow || in_lp[j] == tag; }),
+              R.end());
+    }
+    // w[e] = |L_e \ L_p| for the other elements of L_p's rows
+    for (int i : lp)
+      for (int e : elems[i]) {
+        if (wtag[e] != tag) {
+          wtag[e] = tag;
+          w[e] = static_cast<int>(members[e].size());
+        }
+        --w[e];
+      }
+    const int lsize = static_cast<int>(lp.size());
+    for (int i : lp) {
+      long long d = static_cast<long long>(rows[i].size()) + (lsize - 1);
+      for (int e : elems[i]) {
+        if (state[e] != kElement) continue;
+        if (w[e] == 0) {  // e lies inside L_p: absorbed by p
+          state[e] = kAbsorbed;
+          std::vector<int>().swap(members[e]);
+          continue;
+        }
+        d += w[e];
+      }
+      d = std::min<long long>({d, remaining - 1, static_cast<long long>(buckets.degree(i)) + lsize - 1});
+      elems[i].push_back(p);
+      buckets.insert(i, static_cast<int>(std::max<long long>(d, 0)));
+    }
+    members[p] = std::move(lp);
   }
   return true;
 }

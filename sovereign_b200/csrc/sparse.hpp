@@ -1,11 +1,13 @@
 // sparse.hpp -- host ordering and symbolic analysis for the sparse LDL' of the normal matrix.
 //
-// Minimum-degree ordering on the explicit elimination graph of A A' (the rule of the reference's
-// AMDOrdering::compute, solver/numerical/src/amd_ordering.cpp:12-130: rows whose degree exceeds
-// max(16, 10 sqrt(m)) are ordered last, ties go to the lowest row, an optional fill limit aborts
-// the analysis), then the column patterns of L, the elimination tree and a level schedule for the
-// GPU: columns of equal height in the tree have no ancestor relation, so a level's columns are
-// finished together and their rank-1 updates applied together.
+// Approximate minimum-degree ordering of A A' on its quotient graph (Amestoy, Davis & Duff 1996:
+// eliminated rows become elements, degrees are the paper's upper bound, rows denser than
+// max(16, 10 sqrt(m)) are ordered last, an optional fill limit aborts the analysis), then the
+// column patterns of L, the elimination tree and a level schedule for the GPU: columns of equal
+// height in the tree have no ancestor relation, so a level's columns are finished together and
+// their rank-1 updates applied together. The reference orders with its own minimum degree
+// (solver/numerical/src/amd_ordering.cpp:12-130); the orders differ, the factorization does not
+// depend on which fill-reducing order is used.
 #pragma once
 
 #include <cstdint>

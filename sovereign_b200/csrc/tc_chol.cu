@@ -158,12 +158,10 @@ size_t tc3_smem_bytes(int N) { return static_cast<size_t>(2 * kTcM * kTcK * 4 + 
 
 // FP32 blocked Cholesky with the panel and trailing products on the tensor cores.
 void dense_cholesky_tc(const DenseSystem<float>& s, int* err, cudaStream_t st, int* launches) {
-  static bool attr = false;
-  if (!attr) {
+  once_per_device((const void*)k_tc3_syrk, [&] {
     SOV_CUDA(cudaFuncSetAttribute(k_tc3_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc3_smem_bytes(kTcM)));
     SOV_CUDA(cudaFuncSetAttribute(k_tc3_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc3_smem_bytes(kNB)));
-    attr = true;
-  }
+  });
   int n = 0;
   for (int kb = 0; kb < s.nb; ++kb) {
     dense_potrf_block<float>(s, kb, st);

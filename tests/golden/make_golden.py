@@ -29,7 +29,7 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from sovereign_b200 import problems as P  # noqa: E402
 
-LISWET_DIR = "/root/reference/benchmarks/reports/liswet_step6/n20000"
+LISWET_DIR = os.path.join(oracle.REFERENCE_DIR, "benchmarks", "reports", "liswet_step6", "n20000")
 
 LP_SPECS = [
     ("reference_transport", [20]), ("reference_transport", [40]), ("reference_transport", [60]),

@@ -7,8 +7,10 @@ import subprocess
 
 import pytest
 
+import oracle
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference/solver"
+REF = os.path.join(oracle.REFERENCE_DIR, "solver")
 
 pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference headers not present")
 

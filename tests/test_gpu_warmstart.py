@@ -90,9 +90,10 @@ def test_predict_start_matches_host_decoding():
         np.testing.assert_allclose(got[k][2], ss[k], rtol=1e-12)
 
 
-def test_batch_from_device_starts_equals_host_starts():
+def test_batch_from_device_starts_equals_host_starts(monkeypatch):
     # sov_lp_solve_batch_predicted keeps the predicted starts on the device; given the same network
-    # and parameters it must give exactly what the batch gives with the same starts from host arrays
+    # and parameters it must give exactly what the batch gives with the same starts from host arrays.
+    # The call is split into three parts, so each part gathers its starts from an offset other than 0.
     from sovereign_b200.ipm import solve_batch
     fam = P.TransportFamily()
     train = [fam.instance_from_seed(300 + k) for k in range(64)]
@@ -102,6 +103,7 @@ def test_batch_from_device_starts_equals_host_starts():
     ws.fit(np.stack([p for _, p in train]), early, epochs=30, batch=32, lr=2e-3)
     models, params = [m for m, _ in test], np.stack([p for _, p in test])
     host = solve_batch(models, warm_starts=ws.predict(params), with_diag=True)
+    monkeypatch.setenv("SOVEREIGN_BATCH_PARTS", "3")
     dev = ws.solve_batch(models, params, with_diag=True)
     for h, d in zip(host, dev):
         assert d.status_name == "OPTIMAL" and h.status == d.status and h.iterations == d.iterations

@@ -5,6 +5,7 @@ device array; sizes beyond its limit must be refused cleanly.
 
 Collected last on purpose (file name), so a failure here does not hide the rest of the suite."""
 import ctypes as C
+import dataclasses
 
 import numpy as np
 import pytest
@@ -60,3 +61,23 @@ def test_noalloc_rejects_sizes_beyond_its_array():
     rhs = np.ones(mdl.m)
     rc, _, _ = _device_call(torch, mdl.m, mdl.n, mdl, d, rhs)
     assert rc == -4  # SOV_E_TOO_LARGE
+
+
+def test_noalloc_refuses_bad_device_indices_without_writing():
+    # the device arrays are never seen by the host: a row index outside [0, m) must be skipped on the
+    # device and reported as SOV_E_ARGUMENT, and the next call must work as before
+    torch = pytest.importorskip("torch")
+    mdl = P.random_sparse_lp(40, 120, 3, 9)
+    d = np.ones(mdl.n)
+    rhs = np.ones(mdl.m)
+    bad = mdl.row_idx.copy()
+    bad[7] = mdl.m + 1000
+    bad[11] = -3
+    broken = dataclasses.replace(mdl, row_idx=bad)
+    rc, _, _ = _device_call(torch, mdl.m, mdl.n, broken, d, rhs)
+    assert rc == -1  # SOV_E_ARGUMENT
+    assert b"row outside" in _lib.load().sov_last_error()
+    want, _ = normal_factor_solve(mdl.m, mdl.n, mdl.col_ptr, mdl.row_idx, mdl.values, d, rhs)
+    rc, got, _ = _device_call(torch, mdl.m, mdl.n, mdl, d, rhs)
+    assert rc == 0
+    np.testing.assert_allclose(got, want, rtol=1e-7, atol=1e-9 * np.abs(want).max())
