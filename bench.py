@@ -10,8 +10,8 @@ keeps every objective within 1e-8 of the reference's) by the batched persistent 
           stream. Per step the kernels read ~0.6 GB of per-LP data, several times the 126 MB L2.
   e2e     the public C-ABI call sov_lp_solve_batch with host buffers: host standard form,
           host->device copy, solve, device->host copy and publishing, per step.
-  plain_fp64_gpu   the same LPs one at a time through the single-problem FP64 engine
-          (sov_lp_solve), a bounded sample, for the mixed+batched vs plain-FP64 comparison.
+  plain_fp64_gpu   the same 4096 LPs through the single-problem FP64 engine (sov_lp_solve), 16
+          concurrent solves on separate CUDA streams, for the batched vs plain-FP64 comparison.
   cpu_baseline     the reference's own CPU IPM (oracle/_ref, compiled from the reference sources)
           on a bounded sample of the same LPs with all host threads.
 
@@ -37,6 +37,7 @@ METRIC = "LPs solved/sec at 1e-8 rel gap on 1 B200: mixed+batched+warm-start vs 
 UNIT = "LPs/s"
 WORKLOAD = "4096 uneven transportation LPs (ns, nt ~ U{10..60}), batched persistent launch"
 COUNT = 4096
+PLAIN_WORKERS = 16  # concurrent single-problem solves of the plain FP64 baseline
 
 
 def peaks() -> dict:
@@ -123,6 +124,14 @@ def per_lp_bytes(mdl) -> float:
     # m-vector passes (standard form of a transport LP has no slacks: n_ipm = n, nnz = 2n)
     n, m, nnz = mdl.n, mdl.m, mdl.nnz
     return 6.0 * (12.0 * nnz + 8.0 * (m + n)) + 15.0 * 8.0 * n + 10.0 * 8.0 * m
+
+
+def per_lp_flops(mdl) -> float:
+    # FP64 flops of one IPM iteration of the batched kernel: the dense L D L' of the m x m normal
+    # matrix, two right-hand sides forward and backward, and the assembly (2 k_j^2 per column)
+    m = mdl.m
+    k = np.diff(mdl.col_ptr).astype(np.float64)
+    return (2.0 / 3.0) * m ** 3 + 8.0 * m * m + 2.0 * float(np.sum(k * k))
 
 
 def cpu_reference_sample(models, seconds_target: float = 15.0) -> dict:
@@ -404,22 +413,25 @@ def main():
     from sovereign_b200.shard import shard_seed
     models = P.transport_batch(count, seed=shard_seed(2026, rank))
     bytes_iter = np.array([per_lp_bytes(m) for m in models])
+    flops_iter = np.array([per_lp_flops(m) for m in models])
 
     import torch
     torch.cuda.set_device(local)
     if rank == 0:
-        # plain FP64 single-problem engine on a bounded sample of the same LPs, measured first
-        # (after one untimed solve) so that it runs in a clean process state
-        sample = models[:48]
-        InteriorPointSolver().solve(sample[0])
-        t_plain = float("inf")
-        for _ in range(2):  # the faster of two passes (single solves are sensitive to host load)
+        # the plain FP64 GPU IPM: the same LPs through the single-problem engine (sov_lp_solve, FP64),
+        # PLAIN_WORKERS solves in flight at a time, each on its own CUDA stream, measured first
+        # (after an untimed pass over a slice) so that it runs in a clean process state
+        import concurrent.futures as cf
+        solver = InteriorPointSolver()
+        with cf.ThreadPoolExecutor(max_workers=PLAIN_WORKERS) as ex:
+            list(ex.map(solver.solve, models[:2 * PLAIN_WORKERS]))
             t0 = time.perf_counter()
-            single = [InteriorPointSolver().solve(m) for m in sample]
-            t_plain = min(t_plain, time.perf_counter() - t0)
-        plain = dict(value=len(sample) / t_plain, unit=UNIT,
-                     sample=f"first {len(sample)} LPs one at a time through sov_lp_solve (FP64), wall clock, "
-                            "faster of two passes")
+            single = list(ex.map(solver.solve, models))
+            t_plain = time.perf_counter() - t0
+        plain = dict(value=len(models) / t_plain, unit=UNIT,
+                     sample=f"all {len(models)} LPs through sov_lp_solve (FP64 single-problem engine), "
+                            f"{PLAIN_WORKERS} concurrent solves on separate streams, wall clock",
+                     optimal=f"{sum(r.status_name == 'OPTIMAL' for r in single)}/{len(models)}")
     # untimed: threads per CTA for each size bucket, picked by timing the bucket alone
     tuning = json.loads(autotune(models))
     batch = DeviceBatch(models)
@@ -444,24 +456,38 @@ def main():
     stats = batch.stats()
     value = world * count * args.steps / (dev_ms * 1e-3)
 
-    # roofline of the (only) kernel: algorithmic bytes of all IPM iterations / kernel time
+    # roofline of the (only) kernel: algorithmic bytes of all IPM iterations / device time per step
+    # (the same CUDA-event timing as ms_per_step: all bucket launches of a step, concurrent)
     alg_bytes = float(np.sum(bytes_iter * (iters + 1)))
-    kernel_s = stats["kernel_ms"] * 1e-3
+    alg_flops = float(np.sum(flops_iter * (iters + 1)))
+    step_s = dev_ms * 1e-3 / args.steps
     pk = peaks()
-    achieved = alg_bytes / kernel_s / 1e9
-    traffic = None
-    try:  # DRAM bytes of one full-size step from the committed ncu capture (profiles/)
-        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")) as fh:
-            if count == COUNT:
-                traffic = json.load(fh)["k_batch_ipm"]["dram_bytes_per_step"]
+    achieved = alg_bytes / step_s / 1e9
+    chosen = {k: v["chosen"] for k, v in tuning.items()}
+    traffic_ncu = None
+    try:  # DRAM bytes of one full-size step from an ncu capture, used only if its widths are this run's
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            t = json.load(fh)["k_batch_ipm"]
+        if count == COUNT and t.get("threads_per_bucket") == chosen:
+            traffic_ncu = dict(bytes_per_step=t["dram_bytes_per_step"], source="profiles/traffic.json",
+                               widths="same threads per bucket as this run")
     except (OSError, KeyError, ValueError):
         pass
     roofline = dict(bound="hbm", achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
-                    frac=achieved / pk["hbm_gbs"], traffic=traffic,
-                    algorithmic_bytes_per_step=alg_bytes, traffic_unit="bytes per step (ncu, serialised buckets)",
-                    kernel="k_batch_ipm", peak_source=pk["source"],
+                    frac=achieved / pk["hbm_gbs"], traffic=None,
+                    algorithmic_bytes_per_step=alg_bytes, kernel="k_batch_ipm", peak_source=pk["source"],
+                    traffic_ncu=traffic_ncu,
                     note="algorithmic bytes = sum over LPs of (iterations + 1) x [6 SpMV x (12 nnz + 8(m+n)) + "
-                         "15 x 8n + 10 x 8m]; kernel time from CUDA events of the last step")
+                         "15 x 8n + 10 x 8m] / device time per step. traffic is null: DRAM counters need an ncu "
+                         "capture, which a timed run cannot take; traffic_ncu holds a capture's figure when its "
+                         "widths match this run's",
+                    binding=dict(limit="latency: shared-memory dependency chains of the per-LP L D L' and "
+                                       "triangular solves, CTA barriers; the per-LP data stays in L2",
+                                 fp64_tflops=alg_flops / step_s / 1e12,
+                                 fp64_flops_per_step=alg_flops,
+                                 note="FP64 flops = sum over LPs of (iterations + 1) x [(2/3) m^3 + 8 m^2 + "
+                                      "2 sum_j k_j^2]; against the B200's nominal FP64 rate (about 37 TFLOP/s) "
+                                      "this is the chain-latency bound, not a throughput one"))
 
     # end to end through the C ABI, sov_lp_solve_batch, with caller-owned host buffers (the models'
     # CSC arrays in, primal/dual arrays out), as a C or C++ caller holds them: host standard form,
@@ -509,18 +535,29 @@ def main():
         line["plain_fp64_gpu"] = plain
         line["speedup_vs_plain_fp64"] = value / plain["value"]
         err = max(abs(a.objective_value - b.objective_value) / max(1.0, abs(b.objective_value))
-                  for a, b in zip(res[:48], single))
+                  for a, b in zip(res, single) if b.status_name == "OPTIMAL")
         line["max_rel_obj_diff_batched_vs_plain"] = err
         if not args.no_cpu_baseline and world == 1:
             try:
                 cb = cpu_reference_sample(models)
                 k = len(cb["objectives"])
-                both = [i for i in range(k) if cb["statuses"][i] == 0 and res[i].status_name == "OPTIMAL"]
+                ref_obj = np.array(cb["objectives"], dtype=np.float64)
+                ref_st = np.array(cb["statuses"])
+                # where the reference's dense LU stops short of OPTIMAL (a pivot under its 1e-14 floor
+                # on a dependent row), its own sparse L D L' path gives the comparison (untimed)
+                import oracle
+                os.environ["SOVEREIGN_IPM_NORMAL_EQUATIONS"] = "sparse"
+                try:
+                    for i in np.flatnonzero(ref_st != 0):
+                        rr = oracle.solve(models[i], kind="reference")
+                        ref_obj[i], ref_st[i] = rr.objective_value, rr.status
+                finally:
+                    del os.environ["SOVEREIGN_IPM_NORMAL_EQUATIONS"]
+                both = [i for i in range(k) if ref_st[i] == 0 and res[i].status_name == "OPTIMAL"]
                 line["max_rel_obj_err_vs_reference"] = float(max(
-                    abs(res[i].objective_value - cb["objectives"][i]) / max(1.0, abs(cb["objectives"][i]))
-                    for i in both))
+                    abs(res[i].objective_value - ref_obj[i]) / max(1.0, abs(ref_obj[i])) for i in both))
                 line["reference_compared"] = len(both)
-                line["reference_non_optimal"] = int(sum(1 for i in range(k) if cb["statuses"][i] != 0))
+                line["reference_dense_lu_non_optimal"] = int(sum(1 for i in range(k) if cb["statuses"][i] != 0))
                 for key in ("objectives", "statuses", "seconds"):
                     cb.pop(key)
                 line["cpu_baseline"] = cb

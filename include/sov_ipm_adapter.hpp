@@ -16,9 +16,20 @@
 //       return InteriorPointSolver(opt).solve(model);
 //     };
 // and for QP (solver/qp/src/qp_solver.cpp:36) sovereign::b200::solve_qp(model).
+//
+// Batched callers (no reference counterpart for the batching itself):
+//   solve_lp_batch(models)        N independent LPs in one sov_lp_solve_batch call, in place of N
+//                                 InteriorPointSolver::solve calls (the node LPs of a
+//                                 branch-and-bound round, solver/milp/src/branch_and_bound.cpp:497)
+//   solve_branch_children(relax, candidates, x)
+//                                 the down/up children of strong branching
+//                                 (branch_and_bound.cpp:726-779, 829-856: ub = min(ub, floor v),
+//                                 lb = max(lb, ceil v)) for every candidate, all in one call
 #pragma once
 
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -198,7 +209,138 @@ inline SolverResult solve(const OptimizationModel& model, bool qp, const sov_opt
   }
 }
 
+// Output arrays of one LP of a batch.
+struct BatchSlot {
+  std::vector<double> x, dcol, drow;
+  sov_diagnostics dg;
+  sov_result r;
+  void bind(int n, int m) {
+    x.assign(n, 0.0);
+    dcol.assign(n, 0.0);
+    drow.assign(m, 0.0);
+    std::memset(&dg, 0, sizeof(dg));
+    std::memset(&r, 0, sizeof(r));
+    r.primal = x.data();
+    r.dual_col = dcol.data();
+    r.dual_row = drow.data();
+    r.diagnostics = &dg;
+  }
+};
+
+inline SolverResult error_result(const std::string& what) {
+  SolverResult r;
+  r.status = SolverStatus::Error;
+  r.message = "IPM error: " + what;
+  return r;
+}
+
+// One sov_lp_solve_batch call over `views` (model k of the caller is views[k]'s source); a failed
+// call marks every LP of it with the recorded error.
+inline std::vector<SolverResult> run_batch(const std::vector<const OptimizationModel*>& sources,
+                                           std::vector<sov_model>& views, const sov_options* opt) {
+  const int count = static_cast<int>(views.size());
+  std::vector<BatchSlot> slots(count);
+  std::vector<sov_result> res(count);
+  for (int k = 0; k < count; ++k) {
+    slots[k].bind(views[k].n, views[k].m);
+    res[k] = slots[k].r;
+  }
+  std::vector<SolverResult> out;
+  out.reserve(count);
+  const int rc = count > 0 ? sov_lp_solve_batch(count, views.data(), opt, 0, res.data()) : SOV_OK;
+  for (int k = 0; k < count; ++k) {
+    if (rc != SOV_OK) {
+      out.push_back(error_result(sov_last_error()));
+      continue;
+    }
+    out.push_back(to_result(*sources[k], res[k], slots[k].x, slots[k].dcol, slots[k].drow, slots[k].dg));
+  }
+  return out;
+}
+
 }  // namespace detail
+
+// N independent LPs in one batched GPU call. Results in input order; a model that cannot be
+// converted (unknown variable, ...) gets SolverStatus::Error with the reference's "IPM error: ..."
+// message and does not stop the others.
+inline std::vector<SolverResult> solve_lp_batch(const std::vector<OptimizationModel>& models,
+                                                const sov_options* opt = nullptr) {
+  std::vector<SolverResult> out(models.size());
+  std::vector<detail::IndexModel> ims;
+  std::vector<std::size_t> at;
+  ims.reserve(models.size());
+  for (std::size_t k = 0; k < models.size(); ++k) {
+    try {
+      ims.push_back(detail::to_index(models[k], false));
+      at.push_back(k);
+    } catch (const std::exception& ex) {
+      out[k] = detail::error_result(ex.what());
+    }
+  }
+  std::vector<sov_model> views;
+  std::vector<const OptimizationModel*> sources;
+  for (std::size_t q = 0; q < ims.size(); ++q) {
+    views.push_back(ims[q].view);
+    sources.push_back(&models[at[q]]);
+  }
+  std::vector<SolverResult> solved = detail::run_batch(sources, views, opt);
+  for (std::size_t q = 0; q < at.size(); ++q) out[at[q]] = std::move(solved[q]);
+  return out;
+}
+
+// The two children of branching on variable `var` at LP value `value`.
+struct BranchChildren {
+  int var = -1;
+  SolverResult down, up;
+};
+
+// Strong-branching children of one LP relaxation, all candidates in one batched call: for each
+// candidate index i (into relax.variables) with LP value x.at(name), the down child
+// (upper_bound = min(ub, floor v)) and the up child (lower_bound = max(lb, ceil v)), exactly the
+// models pick_strong_branch / pick_reliability_branch build (branch_and_bound.cpp:758-764,
+// 834-839). The constraint matrix is converted once and shared by every child.
+inline std::vector<BranchChildren> solve_branch_children(const OptimizationModel& relax,
+                                                         const std::vector<int>& candidates,
+                                                         const std::unordered_map<std::string, double>& x,
+                                                         const sov_options* opt = nullptr) {
+  std::vector<BranchChildren> out(candidates.size());
+  detail::IndexModel im;
+  try {
+    im = detail::to_index(relax, false);
+  } catch (const std::exception& ex) {
+    for (std::size_t c = 0; c < candidates.size(); ++c) {
+      out[c].var = candidates[c];
+      out[c].down = out[c].up = detail::error_result(ex.what());
+    }
+    return out;
+  }
+  const std::size_t n = relax.variables.size();
+  // per child its own bounds (down, up per candidate), everything else shared
+  std::vector<std::vector<double>> lb(2 * candidates.size(), im.lb), ub(2 * candidates.size(), im.ub);
+  std::vector<sov_model> views;
+  std::vector<const OptimizationModel*> sources;
+  for (std::size_t c = 0; c < candidates.size(); ++c) {
+    const int i = candidates[c];
+    out[c].var = i;
+    if (i < 0 || static_cast<std::size_t>(i) >= n) throw std::out_of_range("branch candidate out of range");
+    const double v = x.at(relax.variables[i].name);
+    ub[2 * c][i] = std::min(ub[2 * c][i], std::floor(v));
+    lb[2 * c + 1][i] = std::max(lb[2 * c + 1][i], std::ceil(v));
+    for (int side = 0; side < 2; ++side) {
+      sov_model view = im.view;
+      view.lb = lb[2 * c + side].data();
+      view.ub = ub[2 * c + side].data();
+      views.push_back(view);
+      sources.push_back(&relax);  // same names: results map back through the relaxation
+    }
+  }
+  std::vector<SolverResult> solved = detail::run_batch(sources, views, opt);
+  for (std::size_t c = 0; c < candidates.size(); ++c) {
+    out[c].down = std::move(solved[2 * c]);
+    out[c].up = std::move(solved[2 * c + 1]);
+  }
+  return out;
+}
 
 inline SolverResult solve_lp(const OptimizationModel& model, const sov_options* opt = nullptr) {
   return detail::solve(model, false, opt);

@@ -5,9 +5,19 @@ oracle/_ref/libsovref.so from them):
 
     python tests/golden/make_golden.py
 
+    python tests/golden/make_golden.py headline c1   # only these sections
+
 Writes
   lp_reference.json   InteriorPointSolver results (status, iterations, objective, gap, residuals,
                       primal checksum) on the seeded and regression LP models below
+  transport4096_reference.npz
+                      the reference's objective and status for every LP of the 4096-LP batched
+                      workload (transport_batch(4096, seed=2026)); where its dense LU stops short of
+                      OPTIMAL (a pivot under its 1e-14 floor), also the objective of its own sparse
+                      L D L' path (SOVEREIGN_IPM_NORMAL_EQUATIONS=sparse), which drops dependent rows
+  c1_reference.npz    the reference's solution of the random LP m=2000, n=10000, 8 nnz per column
+                      (random_sparse_lp(2000, 10000, 8, 1)): objective, residuals, primal, row duals
+                      (about ten minutes of CPU)
   qp_reference.json   QpInteriorPointSolver results on the QP models below
   liswet_n20000.npz   the reference's published LISWET projection at n = 20000
                       (benchmarks/reports/liswet_step6/n20000: input_c.txt, x.txt and the
@@ -63,8 +73,46 @@ def summarize(r, model=None):
     return d
 
 
-def main():
+def headline():
+    """Every LP of the 4096-LP batched workload through the reference (all host threads)."""
+    models = P.transport_batch(4096, seed=2026)
+    secs, obj, its, st = oracle.solve_many_reference(models)
+    bad = np.flatnonzero(st != 0)
+    sparse_obj = np.full(len(models), np.nan)
+    sparse_st = np.full(len(models), -1, dtype=np.int32)
+    os.environ["SOVEREIGN_IPM_NORMAL_EQUATIONS"] = "sparse"
+    try:
+        for i in bad:
+            r = oracle.solve(models[i], kind="reference")
+            sparse_obj[i], sparse_st[i] = r.objective_value, r.status
+    finally:
+        del os.environ["SOVEREIGN_IPM_NORMAL_EQUATIONS"]
+    np.savez_compressed(os.path.join(HERE, "transport4096_reference.npz"), objective=obj, status=st, iterations=its,
+                        sparse_objective=sparse_obj, sparse_status=sparse_st)
+    print(f"headline: {len(models)} LPs in {secs:.1f} s, {len(bad)} not OPTIMAL on the dense path, "
+          f"sparse path statuses {sparse_st[bad].tolist()}", flush=True)
+
+
+def c1():
+    """Config 1 at full size: random LP m=2000, n=10000, 8 nnz per column, seed 1."""
+    mdl = P.random_sparse_lp(2000, 10000, 8, 1)
+    r = oracle.solve(mdl, kind="reference")
+    np.savez_compressed(os.path.join(HERE, "c1_reference.npz"), objective=r.objective_value, status=r.status,
+                        iterations=r.iterations, duality_gap=r.duality_gap, primal_residual=r.primal_residual,
+                        dual_residual=r.dual_residual, primal=r.primal, dual_row=r.dual_row,
+                        seconds=r.solve_seconds, message=r.message)
+    print("c1", r.status_name, r.iterations, r.objective_value, r.solve_seconds, flush=True)
+
+
+def main(sections=()):
     oracle.build(reference=True)
+    if "headline" in sections:
+        headline()
+    if "c1" in sections:
+        c1()
+    if sections:
+        return
+    headline()
     lp = {}
     for name, args in LP_SPECS:
         mdl = build(name, args)
@@ -109,7 +157,8 @@ def main():
         obj = float(ind["independent"]["objective_qp"])
         np.savez_compressed(os.path.join(HERE, "liswet_n20000.npz"), c=c, x=x, objective=obj)
         print("liswet", len(c), obj)
+    c1()
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

@@ -1,7 +1,12 @@
-"""The reference-side adapter (include/sov_ipm_adapter.hpp) compiles against the reference's own
-types.hpp and links with libsovipm.so and the reference core; on a machine without an sm_100 GPU
-the call must come back as SolverStatus::Error naming the device, never as a CPU answer.
-Needs the reference headers, so it runs where the reference tree is present (CPU only)."""
+"""The reference-side adapter (include/sov_ipm_adapter.hpp).
+
+* CPU: it compiles against the reference's own types.hpp and links with libsovipm.so and the
+  reference core; on a machine without an sm_100 GPU the call comes back as SolverStatus::Error
+  naming the device, never as a CPU answer (needs the reference headers).
+* GPU: oracle/_ref/adapter_check (tests/adapter_check.cpp, built with the reference library by
+  oracle/Makefile) runs solve_lp, solve_qp, solve_lp_batch and solve_branch_children on name-keyed
+  OptimizationModels next to the reference's InteriorPointSolver / QpInteriorPointSolver and
+  compares status, objective, the primal and dual maps and lp_diagnostics["ipm"]."""
 import os
 import subprocess
 
@@ -12,7 +17,8 @@ import oracle
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(oracle.REFERENCE_DIR, "solver")
 
-pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference headers not present")
+ADAPTER_CHECK = os.path.join(ROOT, "oracle", "_ref", "adapter_check")
+needs_headers = pytest.mark.skipif(not os.path.isdir(REF), reason="reference headers not present")
 
 PROGRAM = r"""
 #include <cstdio>
@@ -37,6 +43,7 @@ int main() {
 """
 
 
+@needs_headers
 def test_adapter_compiles_links_and_reports_errors(tmp_path):
     from sovereign_b200 import _lib
     _lib.load()
@@ -60,3 +67,16 @@ def test_adapter_compiles_links_and_reports_errors(tmp_path):
         assert status == 0  # OPTIMAL
     else:
         assert status == 7 and "no CUDA device" in msg
+
+
+@pytest.mark.skipif(not os.path.exists(ADAPTER_CHECK), reason="adapter check not built (needs the reference)")
+def test_adapter_check_models_solve_in_the_reference():
+    r = subprocess.run([ADAPTER_CHECK, "--reference-only"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "failures 0" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_adapter_matches_reference_solvers_on_gpu():
+    assert os.path.exists(ADAPTER_CHECK), "oracle/_ref/adapter_check is built with the reference library"
+    r = subprocess.run([ADAPTER_CHECK], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "failures 0" in r.stdout, r.stdout + r.stderr
