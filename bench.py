@@ -221,21 +221,36 @@ def run_single_workload(args):
         if args.workload == "c0":
             rr = oracle.solve(mdl, kind="reference")
             ref = dict(objective=rr.objective_value, seconds=rr.solve_seconds, iterations=rr.iterations)
+        else:  # the reference's solve takes ~10 minutes of CPU: its result is a committed fixture
+            g = np.load(os.path.join(ROOT, "tests", "golden", "c1_reference.npz"))
+            ref = dict(objective=float(g["objective"]), seconds=float(g["seconds"]), iterations=int(g["iterations"]),
+                       source="tests/golden/c1_reference.npz (reference InteriorPointSolver, dense LU, one CPU thread)")
+        for v in lines.values():
+            v["rel_obj_err_vs_reference"] = abs(v["objective"] - ref["objective"]) / max(1.0, abs(ref["objective"]))
         best = min(lines.values(), key=lambda v: v["wall_s"])
         _line(METRIC, 1.0 / best["wall_s"], UNIT, args, 1e3 * best["wall_s"], "f64",
               dict(workload="transport 50x50 (single LP)" if args.workload == "c0" else
                    "random sparse LP m=2000 n=10000, 8 nnz/column (single LP)"),
-              variants=lines, cpu_reference=ref or None,
-              max_rel_obj_err_vs_reference=(abs(best["objective"] - ref["objective"]) / max(1.0, abs(ref["objective"]))
-                                            if ref else None))
+              variants=lines, cpu_reference=ref,
+              max_rel_obj_err_vs_reference=max(v["rel_obj_err_vs_reference"] for v in lines.values()))
         return
     if args.workload == "c2":
         mdl = P.convex_sequence_qp(20002, 2)
         r, wall, dev = timed(QpInteriorPointSolver(), mdl)
-        _line(METRIC, 1.0 / wall, UNIT, args, 1e3 * wall, "f64",
+        # the reference's structured LISWET path takes ~3 minutes of CPU: its answer is a fixture
+        g = np.load(os.path.join(ROOT, "tests", "golden", "c2_reference.npz"))
+        ref_obj = float(g["objective"])
+        _line(METRIC, 1.0 / wall, UNIT, args, 1e3 * wall, "dd (double-double) + f64",
               dict(workload="convex-sequence QP n=20002, m=20000 (single QP)"),
               status=r.status_name, iterations=r.iterations, objective=r.objective_value, device_s=dev,
-              duality_gap=r.duality_gap, message=r.message[:160])
+              duality_gap=r.duality_gap, primal_residual=r.primal_residual, dual_residual=r.dual_residual,
+              message=r.message[:200],
+              max_rel_obj_err_vs_reference=abs(r.objective_value - ref_obj) / max(1.0, abs(ref_obj)),
+              max_abs_primal_diff_vs_reference=float(np.max(np.abs(r.primal - g["primal"]))),
+              cpu_reference=dict(objective=ref_obj, seconds=float(g["seconds"]),
+                                 status="ERROR (its certifier: dual residual 1.2e-7)",
+                                 source="tests/golden/c2_reference.npz (reference structured LISWET path, one CPU "
+                                        "thread)"))
         return
     if args.workload == "c3w":
         run_batched_warm_start(args)

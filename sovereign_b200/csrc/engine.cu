@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "dense.cuh"
 #include "engine.hpp"
+#include "xband.hpp"
 #include "ipm_kernels.cuh"
 #include "sparse.hpp"
 #include "sparse_gpu.cuh"
@@ -1026,6 +1027,16 @@ void Engine::run(sov_result* r) {
 
 int solve_single(const sov_model& model, const StdForm& f, const sov_options& opt, sov_result* result,
                  cudaStream_t stream, EngineStats* stats) {
+  // separable QPs with free variables and narrow banded inequality rows (the convex-sequence
+  // shape): the x-space double-double path; anything it does not bring to OPTIMAL under AUTO is
+  // solved again by the general engine below
+  if (f.qp && (opt.factorization == SOV_FACTOR_AUTO || opt.factorization == SOV_FACTOR_XSPACE)) {
+    XBandModel xb;
+    if (xband_prepare(model, &xb)) {
+      solve_xband(model, xb, opt, result, stream, stats);
+      if (result->status == SOV_OPTIMAL || opt.factorization == SOV_FACTOR_XSPACE) return SOV_OK;
+    }
+  }
   {
     Engine e(model, f, opt, stream, stats);
     e.run(result);

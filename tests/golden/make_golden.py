@@ -18,6 +18,10 @@ Writes
   c1_reference.npz    the reference's solution of the random LP m=2000, n=10000, 8 nnz per column
                       (random_sparse_lp(2000, 10000, 8, 1)): objective, residuals, primal, row duals
                       (about ten minutes of CPU)
+  c2_reference.npz    the reference's answer on the convex-sequence QP n=20002, m=20000
+                      (convex_sequence_qp(20002, 2)): its structured LISWET path (Goldfarb-Idnani in
+                      extended precision, about three minutes) returns the objective and primal but
+                      status ERROR, because its certifier measures a dual residual of 1.2e-7
   qp_reference.json   QpInteriorPointSolver results on the QP models below
   liswet_n20000.npz   the reference's published LISWET projection at n = 20000
                       (benchmarks/reports/liswet_step6/n20000: input_c.txt, x.txt and the
@@ -104,12 +108,23 @@ def c1():
     print("c1", r.status_name, r.iterations, r.objective_value, r.solve_seconds, flush=True)
 
 
+def c2():
+    """Config 2: the convex-sequence QP n=20002 (t = sin(4 pi i / n) + 0.1 N(0,1), seed 2)."""
+    mdl = P.convex_sequence_qp(20002, 2)
+    r = oracle.solve(mdl, qp=True, kind="reference")
+    np.savez_compressed(os.path.join(HERE, "c2_reference.npz"), objective=r.objective_value, status=r.status,
+                        primal=r.primal, seconds=r.solve_seconds, message=r.message[:300])
+    print("c2", r.status_name, r.objective_value, r.solve_seconds, flush=True)
+
+
 def main(sections=()):
     oracle.build(reference=True)
     if "headline" in sections:
         headline()
     if "c1" in sections:
         c1()
+    if "c2" in sections:
+        c2()
     if sections:
         return
     headline()
@@ -158,6 +173,7 @@ def main(sections=()):
         np.savez_compressed(os.path.join(HERE, "liswet_n20000.npz"), c=c, x=x, objective=obj)
         print("liswet", len(c), obj)
     c1()
+    c2()
 
 
 if __name__ == "__main__":

@@ -316,3 +316,19 @@ def test_large_network_takes_the_sparse_path():
     assert r.status_name == "OPTIMAL", r.message
     assert "sparse LDL^T on the GPU" in r.message
     assert rel(r.objective_value, g["objective"]) < TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config1_full_size_matches_reference(precision):
+    # the random LP at its full size (m = 2000, n = 10000, 8 nonzeros per column), FP64 and mixed
+    # precision (FP32 tensor-core Cholesky preconditioning FP64 PCG), against the reference's solution
+    g = np.load(os.path.join(GOLDEN, "c1_reference.npz"))
+    prec = abi.PRECISION_FP64 if precision == "fp64" else abi.PRECISION_MIXED
+    r = InteriorPointSolver(InteriorPointOptions(precision=prec)).solve(P.random_sparse_lp(2000, 10000, 8, 1),
+                                                                        with_diag=True)
+    assert r.status_name == "OPTIMAL", r.message
+    assert rel(r.objective_value, float(g["objective"])) < TOL
+    assert r.primal_residual <= 1e-8 and r.dual_residual <= 1e-8 and r.duality_gap <= 1e-8
+    assert r.iterations <= int(g["iterations"]) + 1
+    # the optimum of a random LP is unique: the primal agrees with the reference's
+    np.testing.assert_allclose(r.primal, g["primal"], rtol=0, atol=1e-6 * max(1.0, np.abs(g["primal"]).max()))
