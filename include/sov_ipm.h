@@ -305,6 +305,34 @@ int sov_mlp_train(sov_mlp* mlp, const float* x, const float* t, int32_t count, i
                   float lr, uint64_t seed, double* final_loss);
 void sov_mlp_destroy(sov_mlp* mlp);
 
+/* Certificate of an answer against the original model, computed on the GPU (verify.cu): the
+ * checks of sovereign::SolutionVerifier::verify (solver/core/src/verifier.cpp:10-150; default
+ * tolerance 1e-6 there) and the dual side an interior point carries, so that an IPM answer can be
+ * accepted without a simplex crossover. result must hold primal (n) and dual_row (m: the published
+ * "row_<i>" multipliers of the minimisation form), status, objective_value and duality_gap. */
+enum {
+  SOV_CERT_NO_FEASIBLE_STATUS = 1, /* status gives no feasible primal (verifier.cpp:17-27) */
+  SOV_CERT_UNCHECKABLE_STATUS = 2, /* INFEASIBLE / UNBOUNDED without a certificate (:29-38) */
+  SOV_CERT_NONFINITE = 4,          /* a non-finite primal value or row activity */
+  SOV_CERT_BOUND = 8,              /* max bound violation > tol */
+  SOV_CERT_CONSTRAINT = 16,        /* max row violation > tol */
+  SOV_CERT_OBJECTIVE = 32,         /* reported objective differs from the recomputed one by > tol (1 + |obj|) */
+  SOV_CERT_GAP = 64                /* OPTIMAL with a reported duality gap > tol */
+};
+typedef struct sov_certificate {
+  int32_t is_valid;                 /* the verifier's verdict: no issue bit set */
+  int32_t issues;                   /* SOV_CERT_* bits */
+  int32_t nonfinite;                /* non-finite primal values and row activities */
+  int32_t reserved;
+  double max_bound_violation;       /* max(0, max_j max(lb_j - x_j, x_j - ub_j)) */
+  double max_constraint_violation;  /* max(0, max_i (<=: a_i x - b_i, >=: b_i - a_i x, =: |a_i x - b_i|)) */
+  double recomputed_objective;      /* constant + c'x + 1/2 sum of stored q_ij x_i x_j */
+  double dual_objective;            /* b'y - 1/2 x'Qx + sum_j (lb_j max(d_j, 0) + ub_j min(d_j, 0)), model sense */
+  double max_dual_infeasibility;    /* sign violations of d = c + Qx - A'y (min form) and of y */
+  double relative_gap;              /* |primal - dual objective| / (1 + |primal|) */
+} sov_certificate;
+int sov_verify_solution(const sov_model* model, const sov_result* result, double tol, sov_certificate* cert);
+
 /* Device name, SM count, memory; returns SOV_E_NO_DEVICE when no usable sm_100 GPU exists. */
 int sov_device_info(char* buf, int32_t len);
 

@@ -21,6 +21,9 @@
 //   solve_lp_batch(models)        N independent LPs in one sov_lp_solve_batch call, in place of N
 //                                 InteriorPointSolver::solve calls (the node LPs of a
 //                                 branch-and-bound round, solver/milp/src/branch_and_bound.cpp:497)
+//   verify(model, result, tol)    SolutionVerifier::verify (solver/core/src/verifier.cpp:10-150)
+//                                 computed on the GPU by sov_verify_solution, for an answer
+//                                 accepted without a simplex crossover; also returns the dual side
 //   solve_branch_children(relax, candidates, x)
 //                                 the down/up children of strong branching
 //                                 (branch_and_bound.cpp:726-779, 829-856: ub = min(ub, floor v),
@@ -339,6 +342,82 @@ inline std::vector<BranchChildren> solve_branch_children(const OptimizationModel
     out[c].down = std::move(solved[2 * c]);
     out[c].up = std::move(solved[2 * c + 1]);
   }
+  return out;
+}
+
+// The verifier's checks of `result` against `model` on the GPU, as a VerificationResult with the
+// verifier's messages; `cert` (optional) receives every figure, the dual side included. Integrality
+// is not checked (the interior-point path solves continuous models).
+inline VerificationResult verify(const OptimizationModel& model, const SolverResult& result, double tol = 1e-6,
+                                 sov_certificate* cert = nullptr) {
+  VerificationResult out;
+  out.message = "Verifier executed.";
+  sov_certificate c;
+  std::memset(&c, 0, sizeof(c));
+  try {
+    detail::IndexModel im = detail::to_index(model, !model.objective.quadratic.empty());
+    std::vector<double> x(im.view.n, 0.0), y(im.view.m, 0.0);
+    for (std::size_t j = 0; j < model.variables.size(); ++j) {
+      auto it = result.primal.find(model.variables[j].name);
+      if (it == result.primal.end()) {
+        out.issues.push_back("Missing primal value for variable " + model.variables[j].name);
+      } else {
+        x[j] = it->second;
+      }
+    }
+    for (std::size_t i = 0; i < model.constraints.size(); ++i) {
+      auto it = result.dual.find("row_" + std::to_string(i));
+      if (it != result.dual.end()) y[i] = it->second;
+    }
+    sov_result r;
+    std::memset(&r, 0, sizeof(r));
+    r.status = static_cast<int32_t>(result.status);
+    r.has_objective_value = result.has_objective_value ? 1 : 0;
+    r.objective_value = result.objective_value;
+    r.duality_gap = result.duality_gap;
+    r.primal = x.data();
+    r.dual_row = y.data();
+    if (sov_verify_solution(&im.view, &r, tol, &c) != SOV_OK) {
+      out.issues.push_back(std::string("GPU verification failed: ") + sov_last_error());
+      out.message = "Solution failed verification.";
+      return out;
+    }
+  } catch (const std::exception& ex) {
+    out.issues.push_back(std::string("IPM error: ") + ex.what());
+    out.message = "Solution failed verification.";
+    return out;
+  }
+  if (cert) *cert = c;
+  out.max_bound_violation = c.max_bound_violation;
+  out.max_constraint_violation = c.max_constraint_violation;
+  out.recomputed_objective = c.recomputed_objective;
+  if (c.issues & SOV_CERT_NO_FEASIBLE_STATUS) {
+    out.issues.push_back("Solver status does not provide a feasible primal solution: " + to_string(result.status));
+    out.message = "Verification skipped for non-feasible status.";
+    return out;
+  }
+  if (c.issues & SOV_CERT_UNCHECKABLE_STATUS) {
+    out.issues.push_back("Status " + to_string(result.status) + " has no independently checkable certificate.");
+    out.message = "Status claim is unverified.";
+    return out;
+  }
+  if (c.issues & SOV_CERT_NONFINITE) out.issues.push_back("Non-finite primal value or constraint activity.");
+  if (c.issues & SOV_CERT_BOUND) out.issues.push_back("Bound violation exceeds tolerance.");
+  if (c.issues & SOV_CERT_CONSTRAINT) out.issues.push_back("Constraint violation exceeds tolerance.");
+  if (c.issues & SOV_CERT_OBJECTIVE) {
+    char buf[96];
+    std::snprintf(buf, sizeof buf, "Reported objective differs from recomputed value by %g",
+                  std::fabs(result.objective_value - c.recomputed_objective));
+    out.issues.push_back(buf);
+  }
+  if (c.issues & SOV_CERT_GAP) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "OPTIMAL status contradicted by reported relative duality gap %g (tolerance %g).",
+                  result.duality_gap, tol);
+    out.issues.push_back(buf);
+  }
+  out.is_valid = out.issues.empty();
+  out.message = out.is_valid ? "Solution verified." : "Solution failed verification.";
   return out;
 }
 

@@ -20,7 +20,7 @@ EXPORTS = [
     "sov_batch_transfer_bytes", "sov_batch_destroy", "sov_autotune", "sov_spmv_csc", "sov_normal_factor_solve", "sov_normal_factor_solve_noalloc", "sov_device_info",
     "sov_last_error", "sov_mlp_create", "sov_mlp_param_count", "sov_mlp_get_params", "sov_mlp_set_params",
     "sov_mlp_forward", "sov_mlp_predict_start", "sov_mlp_loss_grad", "sov_mlp_train", "sov_mlp_destroy",
-    "sov_lp_solve_batch_predicted",
+    "sov_lp_solve_batch_predicted", "sov_verify_solution",
 ]
 
 _lib = None
@@ -83,6 +83,7 @@ def load(build_if_missing: bool = True):
                                   C.c_uint64, C.POINTER(C.c_double)]
     lib.sov_mlp_destroy.argtypes = [C.c_void_p]
     lib.sov_mlp_destroy.restype = None
+    lib.sov_verify_solution.argtypes = [M, R, C.c_double, C.POINTER(abi.SovCertificate)]
     lib.sov_last_error.restype = C.c_char_p
     _lib = lib
     return lib

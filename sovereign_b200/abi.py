@@ -79,6 +79,19 @@ class SovResult(C.Structure):
     ]
 
 
+class SovCertificate(C.Structure):
+    _fields_ = [
+        ("is_valid", C.c_int32), ("issues", C.c_int32), ("nonfinite", C.c_int32), ("reserved", C.c_int32),
+        ("max_bound_violation", C.c_double), ("max_constraint_violation", C.c_double),
+        ("recomputed_objective", C.c_double), ("dual_objective", C.c_double),
+        ("max_dual_infeasibility", C.c_double), ("relative_gap", C.c_double),
+    ]
+
+
+CERT_ISSUES = {1: "no feasible status", 2: "uncheckable status", 4: "non-finite", 8: "bound", 16: "constraint",
+               32: "objective", 64: "gap"}
+
+
 def dptr(a: np.ndarray | None):
     if a is None:
         return None

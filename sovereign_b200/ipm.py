@@ -224,3 +224,21 @@ def normal_factor_solve(m: int, n: int, col_ptr, row_idx, values, d, rhs, precis
                                          d.ctypes.data, precision, factorization, rhs.ctypes.data, nrhs,
                                          C.byref(dropped)))
     return rhs, dropped.value
+
+
+def verify_solution(model: Model, result: Result, tol: float = 1e-6) -> dict:
+    """Certificate of `result` against `model` on the GPU (sov_verify_solution): the checks of
+    SolutionVerifier::verify (solver/core/src/verifier.cpp:10-150, default tolerance 1e-6) plus the
+    dual side (reduced-cost and row-dual signs, dual objective, relative gap)."""
+    r = abi.SovResult()
+    primal = np.ascontiguousarray(result.primal, dtype=np.float64)
+    dual_row = np.ascontiguousarray(result.dual_row, dtype=np.float64)
+    r.primal, r.dual_row = abi.dptr(primal), abi.dptr(dual_row)
+    r.status, r.has_objective_value = result.status, int(result.has_objective_value)
+    r.objective_value, r.duality_gap = result.objective_value, result.duality_gap
+    cert = abi.SovCertificate()
+    check(load().sov_verify_solution(C.byref(model.to_abi()), C.byref(r), tol, C.byref(cert)))
+    out = {k: getattr(cert, k) for k, _ in abi.SovCertificate._fields_ if k != "reserved"}
+    out["is_valid"] = bool(cert.is_valid)
+    out["issue_names"] = [v for k, v in abi.CERT_ISSUES.items() if cert.issues & k]
+    return out

@@ -17,6 +17,7 @@
 #include "sov_ipm_adapter.hpp"
 #include "sovereign/interior_point.hpp"
 #include "sovereign/qp_interior_point.hpp"
+#include "sovereign/verifier.hpp"
 
 using namespace sovereign;
 
@@ -178,6 +179,14 @@ void compare(const std::string& name, const OptimizationModel& m, const SolverRe
       return fail(name + ": scaling diagnostics");
     if (a.gap_history.empty() || a.final_gap > 1e-8) return fail(name + ": gap history");
   }
+  // the GPU certificate against the reference's SolutionVerifier on the same answer
+  const VerificationResult vg = b200::verify(m, got), vr = SolutionVerifier().verify(m, got);
+  auto near = [](double a, double b) { return std::fabs(a - b) <= 1e-12 * std::max(1.0, std::fabs(b)); };
+  if (vg.is_valid != vr.is_valid || vg.issues.size() != vr.issues.size() ||
+      !near(vg.max_bound_violation, vr.max_bound_violation) ||
+      !near(vg.max_constraint_violation, vr.max_constraint_violation) ||
+      !near(vg.recomputed_objective, vr.recomputed_objective))
+    return fail(name + ": GPU verification differs from SolutionVerifier (" + vg.message + " / " + vr.message + ")");
   std::printf("ok %s: %s objective %.12g (reference %.12g), %d vs %d iterations\n", name.c_str(),
               got.message.substr(0, 40).c_str(), got.objective_value, want.objective_value,
               static_cast<int>(got.iterations), static_cast<int>(want.iterations));
@@ -211,6 +220,19 @@ int main(int argc, char** argv) {
   {
     const OptimizationModel q = portfolio(30, 4);
     compare("portfolio 30", q, b200::solve_qp(q), QpInteriorPointSolver(QpInteriorPointOptions{}).solve(q), 1e-4);
+  }
+  // a perturbed answer: both verifiers reject it with the same issues
+  {
+    const OptimizationModel m = transport(8, 9, 5);
+    SolverResult r = b200::solve_lp(m);
+    r.primal[m.variables[0].name] = -0.01;
+    r.objective_value += 1.0;
+    const VerificationResult vg = b200::verify(m, r), vr = SolutionVerifier().verify(m, r);
+    if (vg.is_valid || vr.is_valid || vg.issues.size() != vr.issues.size())
+      fail("perturbed answer: " + std::to_string(vg.issues.size()) + " vs " + std::to_string(vr.issues.size()) +
+           " issues");
+    for (std::size_t k = 0; k < vg.issues.size() && k < vr.issues.size(); ++k)
+      if (vg.issues[k].substr(0, 20) != vr.issues[k].substr(0, 20)) fail("issue text: " + vg.issues[k] + " / " + vr.issues[k]);
   }
   // node LPs in one batch (one of them refers to an unknown variable: an error for it alone)
   {
