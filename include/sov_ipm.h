@@ -333,6 +333,21 @@ typedef struct sov_certificate {
 } sov_certificate;
 int sov_verify_solution(const sov_model* model, const sov_result* result, double tol, sov_certificate* cert);
 
+/* Model ingest without name-keyed maps: the reference's JSON model format
+ * (solver/core/src/json_io.cpp:13-80, load_model_from_json_file / _string, :112-130) parsed in one
+ * pass straight into the index form above (A column-compressed, rows ascending in each column).
+ * Unknown variables in a constraint return SOV_E_ARGUMENT with the IPM's message ("Unknown
+ * variable in constraint: <name>"); parse errors name the byte offset. The handle owns the arrays;
+ * sov_json_model_view stays valid until sov_json_model_destroy. Host only (no GPU needed). */
+typedef struct sov_json_model sov_json_model;
+int sov_model_from_json(const char* text, size_t len, sov_json_model** out);
+const sov_model* sov_json_model_view(const sov_json_model* jm);
+int32_t sov_json_model_problem_type(const sov_json_model* jm);          /* 0 LP, 1 QP, 2 MILP */
+int32_t sov_json_model_variable_type(const sov_json_model* jm, int32_t j); /* 0 continuous, 1 integer, 2 binary */
+const char* sov_json_model_variable_name(const sov_json_model* jm, int32_t j);
+const char* sov_json_model_row_name(const sov_json_model* jm, int32_t i);
+void sov_json_model_destroy(sov_json_model* jm);
+
 /* Device name, SM count, memory; returns SOV_E_NO_DEVICE when no usable sm_100 GPU exists. */
 int sov_device_info(char* buf, int32_t len);
 

@@ -20,7 +20,9 @@ EXPORTS = [
     "sov_batch_transfer_bytes", "sov_batch_destroy", "sov_autotune", "sov_spmv_csc", "sov_normal_factor_solve", "sov_normal_factor_solve_noalloc", "sov_device_info",
     "sov_last_error", "sov_mlp_create", "sov_mlp_param_count", "sov_mlp_get_params", "sov_mlp_set_params",
     "sov_mlp_forward", "sov_mlp_predict_start", "sov_mlp_loss_grad", "sov_mlp_train", "sov_mlp_destroy",
-    "sov_lp_solve_batch_predicted", "sov_verify_solution",
+    "sov_lp_solve_batch_predicted", "sov_verify_solution", "sov_model_from_json", "sov_json_model_view",
+    "sov_json_model_problem_type", "sov_json_model_variable_type", "sov_json_model_variable_name",
+    "sov_json_model_row_name", "sov_json_model_destroy",
 ]
 
 _lib = None
@@ -84,6 +86,17 @@ def load(build_if_missing: bool = True):
     lib.sov_mlp_destroy.argtypes = [C.c_void_p]
     lib.sov_mlp_destroy.restype = None
     lib.sov_verify_solution.argtypes = [M, R, C.c_double, C.POINTER(abi.SovCertificate)]
+    lib.sov_model_from_json.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p)]
+    lib.sov_json_model_view.argtypes = [C.c_void_p]
+    lib.sov_json_model_view.restype = M
+    lib.sov_json_model_problem_type.argtypes = [C.c_void_p]
+    lib.sov_json_model_variable_type.argtypes = [C.c_void_p, C.c_int32]
+    lib.sov_json_model_variable_name.argtypes = [C.c_void_p, C.c_int32]
+    lib.sov_json_model_variable_name.restype = C.c_char_p
+    lib.sov_json_model_row_name.argtypes = [C.c_void_p, C.c_int32]
+    lib.sov_json_model_row_name.restype = C.c_char_p
+    lib.sov_json_model_destroy.argtypes = [C.c_void_p]
+    lib.sov_json_model_destroy.restype = None
     lib.sov_last_error.restype = C.c_char_p
     _lib = lib
     return lib

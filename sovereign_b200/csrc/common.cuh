@@ -10,6 +10,8 @@
 #include <string>
 #include <utility>
 
+#include "errors.hpp"
+
 namespace sov {
 
 struct CudaError : std::runtime_error {
@@ -98,11 +100,6 @@ void once_per_device(const void* key, F&& fn) {
   once_done().insert({dev, key});
 }
 constexpr int kMaxDevices = 64;
-
-// Record `msg` as the calling thread's sov_last_error() and return `code` (capi.cu).
-int record_error(int code, const std::string& msg);
-// SOV_OK when an sm_100 device is current, else the recorded SOV_E_NO_DEVICE (capi.cu).
-int require_device();
 
 inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 

@@ -242,3 +242,35 @@ def verify_solution(model: Model, result: Result, tol: float = 1e-6) -> dict:
     out["is_valid"] = bool(cert.is_valid)
     out["issue_names"] = [v for k, v in abi.CERT_ISSUES.items() if cert.issues & k]
     return out
+
+
+def load_model_json(text: str | bytes) -> tuple[Model, list[str], list[str]]:
+    """A model in the reference's JSON format (solver/core/src/json_io.cpp:13-80), read by the
+    CSC-native ingest (sov_model_from_json, host only): (Model, variable names, row names)."""
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    h = C.c_void_p()
+    lib = load()
+    check(lib.sov_model_from_json(data, len(data), C.byref(h)))
+    try:
+        v = lib.sov_json_model_view(h).contents
+        n, m = v.n, v.m
+        nnz = v.col_ptr[n] if n > 0 else 0
+
+        def arr(ptr, count, dtype):
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True) if count else np.zeros(0, dtype)
+
+        mdl = Model(n=n, m=m, col_ptr=arr(v.col_ptr, n + 1, np.int32) if n else np.zeros(1, np.int32),
+                    row_idx=arr(v.row_idx, nnz, np.int32), values=arr(v.values, nnz, np.float64),
+                    obj=arr(v.obj, n, np.float64), rhs=arr(v.rhs, m, np.float64),
+                    sense=np.array([v.sense[i] for i in range(m)], dtype=np.int8), lb=arr(v.lb, n, np.float64),
+                    ub=arr(v.ub, n, np.float64), obj_constant=v.obj_constant, maximize=bool(v.maximize))
+        if v.q_col_ptr:
+            qn = v.q_col_ptr[n]
+            mdl.q_col_ptr = arr(v.q_col_ptr, n + 1, np.int32)
+            mdl.q_row_idx = arr(v.q_row_idx, qn, np.int32)
+            mdl.q_values = arr(v.q_values, qn, np.float64)
+        names = [lib.sov_json_model_variable_name(h, j).decode() for j in range(n)]
+        rows = [lib.sov_json_model_row_name(h, i).decode() for i in range(m)]
+    finally:
+        lib.sov_json_model_destroy(h)
+    return mdl, names, rows
