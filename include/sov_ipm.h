@@ -348,6 +348,27 @@ const char* sov_json_model_variable_name(const sov_json_model* jm, int32_t j);
 const char* sov_json_model_row_name(const sov_json_model* jm, int32_t i);
 void sov_json_model_destroy(sov_json_model* jm);
 
+/* LP presolve and postsolve in index form (presolve.cpp; the reference presolves every LP in its
+ * engine, solver/core/src/engine.cpp:108-176, with solver/presolve/src/presolve.cpp): fixed columns,
+ * empty rows, singleton rows (to bounds) and empty columns, repeated until nothing changes.
+ * sov_presolve_lp borrows `model` for the handle's lifetime; sov_presolve_reduced is the model to
+ * solve (when the info status is -1; otherwise presolve decided: OPTIMAL with every column fixed,
+ * INFEASIBLE or UNBOUNDED); sov_postsolve_lp maps a reduced result (or none, when presolve
+ * decided) back to the original columns and rows: primal, row multipliers (removed singleton rows
+ * recover theirs from their column's reduced cost), reduced costs, and the objective evaluated on
+ * the original model. Host only. sov_lp_solve_presolved does all three around sov_lp_solve and,
+ * as the reference's engine does (engine.cpp:160-176), solves the original model again when
+ * presolve claims infeasibility or its answer violates the original rows by more than 1e-6
+ * relative (the message then says so). */
+typedef struct sov_presolve sov_presolve;
+int sov_presolve_lp(const sov_model* model, sov_presolve** out);
+const sov_model* sov_presolve_reduced(const sov_presolve* pre);
+int sov_presolve_info(const sov_presolve* pre, int32_t* status, int32_t* rows_removed, int32_t* cols_removed,
+                      int32_t* bounds_tightened, char* message, int32_t message_len);
+int sov_postsolve_lp(const sov_presolve* pre, const sov_result* reduced, sov_result* full);
+void sov_presolve_destroy(sov_presolve* pre);
+int sov_lp_solve_presolved(const sov_model* model, const sov_options* opt, sov_result* result);
+
 /* Device name, SM count, memory; returns SOV_E_NO_DEVICE when no usable sm_100 GPU exists. */
 int sov_device_info(char* buf, int32_t len);
 

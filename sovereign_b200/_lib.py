@@ -22,7 +22,8 @@ EXPORTS = [
     "sov_mlp_forward", "sov_mlp_predict_start", "sov_mlp_loss_grad", "sov_mlp_train", "sov_mlp_destroy",
     "sov_lp_solve_batch_predicted", "sov_verify_solution", "sov_model_from_json", "sov_json_model_view",
     "sov_json_model_problem_type", "sov_json_model_variable_type", "sov_json_model_variable_name",
-    "sov_json_model_row_name", "sov_json_model_destroy",
+    "sov_json_model_row_name", "sov_json_model_destroy", "sov_presolve_lp", "sov_presolve_reduced",
+    "sov_presolve_info", "sov_postsolve_lp", "sov_presolve_destroy", "sov_lp_solve_presolved",
 ]
 
 _lib = None
@@ -97,6 +98,14 @@ def load(build_if_missing: bool = True):
     lib.sov_json_model_row_name.restype = C.c_char_p
     lib.sov_json_model_destroy.argtypes = [C.c_void_p]
     lib.sov_json_model_destroy.restype = None
+    lib.sov_presolve_lp.argtypes = [M, C.POINTER(C.c_void_p)]
+    lib.sov_presolve_reduced.argtypes = [C.c_void_p]
+    lib.sov_presolve_reduced.restype = M
+    lib.sov_presolve_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int32)] * 4 + [C.c_char_p, C.c_int32]
+    lib.sov_postsolve_lp.argtypes = [C.c_void_p, R, R]
+    lib.sov_presolve_destroy.argtypes = [C.c_void_p]
+    lib.sov_presolve_destroy.restype = None
+    lib.sov_lp_solve_presolved.argtypes = [M, O, R]
     lib.sov_last_error.restype = C.c_char_p
     _lib = lib
     return lib

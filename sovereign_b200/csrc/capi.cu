@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -196,6 +197,75 @@ int sov_lp_solve(const sov_model* model, const sov_options* opt, sov_result* res
 
 int sov_qp_solve(const sov_model* model, const sov_options* opt, sov_result* result) {
   return solve_one(model, opt, result, true);
+}
+
+// Largest bound or row violation of x relative to 1 + |bound| (engine.cpp:60-85); a non-finite
+// value counts as infinite.
+static double max_relative_violation(const sov_model* p, const double* x) {
+  double worst = 0.0;
+  std::vector<double> act(p->m, 0.0);
+  for (int j = 0; j < p->n; ++j) {
+    if (!std::isfinite(x[j])) return INFINITY;
+    const double lo = p->lb ? p->lb[j] : 0.0, hi = p->ub ? p->ub[j] : 1e30;
+    if (x[j] < lo) worst = std::max(worst, (lo - x[j]) / (1.0 + std::fabs(lo)));
+    if (x[j] > hi) worst = std::max(worst, (x[j] - hi) / (1.0 + std::fabs(hi)));
+    for (int k = p->col_ptr[j]; k < p->col_ptr[j + 1]; ++k) act[p->row_idx[k]] += p->values[k] * x[j];
+  }
+  for (int i = 0; i < p->m; ++i) {
+    const double v = p->sense[i] == SOV_LE ? act[i] - p->rhs[i]
+                     : p->sense[i] == SOV_GE ? p->rhs[i] - act[i]
+                                             : std::fabs(act[i] - p->rhs[i]);
+    worst = std::max(worst, v / (1.0 + std::fabs(p->rhs[i])));
+  }
+  return worst;
+}
+
+int sov_lp_solve_presolved(const sov_model* model, const sov_options* opt, sov_result* result) {
+  if (!result) return set_error(SOV_E_ARGUMENT, "null result");
+  reset_result(result);
+  int rc = validate(model);
+  if (rc) {
+    std::snprintf(result->message, sizeof(result->message), "IPM error: %s", g_last_error.c_str());
+    return rc;
+  }
+  sov_presolve* pre = nullptr;
+  rc = sov_presolve_lp(model, &pre);
+  if (rc) return rc;
+  int32_t status = -1;
+  sov_presolve_info(pre, &status, nullptr, nullptr, nullptr, nullptr, 0);
+  if (status < 0) {
+    const sov_model* red = sov_presolve_reduced(pre);
+    std::vector<double> x(red->n), dc(red->n), y(red->m);
+    sov_result rr = *result;
+    rr.primal = x.data();
+    rr.dual_col = dc.data();
+    rr.dual_row = y.data();
+    rr.ipm_x = rr.ipm_y = rr.ipm_s = nullptr;
+    rc = solve_one(red, opt, &rr, false);
+    if (rc) {
+      std::snprintf(result->message, sizeof(result->message), "%s", rr.message);
+      sov_presolve_destroy(pre);
+      return rc;
+    }
+    sov_postsolve_lp(pre, &rr, result);
+  } else {
+    sov_postsolve_lp(pre, nullptr, result);
+  }
+  sov_presolve_destroy(pre);
+  // presolve is checked rather than trusted (engine.cpp:156-176)
+  std::string why;
+  if (status == SOV_INFEASIBLE) {
+    why = std::string("presolve reported infeasibility (") + result->message + ")";
+  } else if ((result->status == SOV_OPTIMAL || result->status == SOV_FEASIBLE) && result->primal &&
+             max_relative_violation(model, result->primal) > 1e-6) {
+    why = "the presolved solution violated the original model";
+  }
+  if (!why.empty()) {
+    rc = solve_one(model, opt, result, false);
+    const std::string msg = std::string(result->message) + " | Re-solved without presolve because " + why + ".";
+    std::snprintf(result->message, sizeof(result->message), "%s", msg.c_str());
+  }
+  return rc;
 }
 
 int sov_device_info(char* buf, int32_t len) {

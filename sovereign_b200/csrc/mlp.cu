@@ -14,15 +14,18 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <random>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "batch.hpp"
 #include "common.cuh"
 #include "sov_ipm.h"
+#include "gemm_ws.cuh"
 #include "tc.cuh"
 
 namespace sov {
@@ -143,7 +146,19 @@ __global__ void __launch_bounds__(kGThreads) k_gemm_bf16(GemmArgs g) {
   if (warp == 0) tc::tmem_dealloc(tmem, kGN);
 }
 
+// Every product of the network: the warp-specialised multi-stage tcgen05 GEMM (gemm_ws.cuh), BF16
+// operands, FP32 accumulation. SOVEREIGN_MLP_GEMM=single selects the single-stage kernel above.
 void gemm(const GemmArgs& g, cudaStream_t st) {
+  static const bool single = [] {
+    const char* e = std::getenv("SOVEREIGN_MLP_GEMM");
+    return e && std::string(e) == "single";
+  }();
+  if (!single) {
+    WsGemmArgs w{g.A, g.a_rs, g.a_ks, g.B, g.b_rs, g.b_ks, g.C, g.c_rs, g.c_cs, g.M, g.N, g.K,
+                 g.alpha, g.beta, g.bias, g.relu, g.err, 0};
+    launch_gemm_ws<1>(w, st);
+    return;
+  }
   const size_t smem = static_cast<size_t>(kGM + kGN) * kGK * 2;
   once_per_device((const void*)k_gemm_bf16, [&] {
     SOV_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

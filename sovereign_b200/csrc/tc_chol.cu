@@ -9,9 +9,12 @@
 // three kind::tf32 MMAs into the same accumulator, which recovers close to FP32 accuracy.
 // Operand layout in memory: column-major with leading dimension ld (element (r, k) at k*ld + r).
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 #include "common.cuh"
 #include "dense.cuh"
+#include "gemm_ws.cuh"
 #include "tc.cuh"
 
 namespace sov {
@@ -156,21 +159,42 @@ __global__ void __launch_bounds__(kTcThreads) k_tc3_trsm(float* M, int ld, int k
 
 size_t tc3_smem_bytes(int N) { return static_cast<size_t>(2 * kTcM * kTcK * 4 + 2 * N * kTcK * 4); }
 
-// FP32 blocked Cholesky with the panel and trailing products on the tensor cores.
+// FP32 blocked Cholesky with the panel and trailing products on the tensor cores: per 64-wide
+// panel kb the diagonal block (FP32 factor and inverse), then the panel L_ik = A_ik Linv_kk^T and the
+// trailing update A_ij -= L_ik L_jk^T on the lower tiles, both 3xTF32 products of the warp-specialised
+// pipelined GEMM (gemm_ws.cuh). SOVEREIGN_TC_GEMM=single selects the single-stage tile kernels above.
 void dense_cholesky_tc(const DenseSystem<float>& s, int* err, cudaStream_t st, int* launches) {
+  static const bool single = [] {
+    const char* e = std::getenv("SOVEREIGN_TC_GEMM");
+    return e && std::string(e) == "single";
+  }();
   once_per_device((const void*)k_tc3_syrk, [&] {
     SOV_CUDA(cudaFuncSetAttribute(k_tc3_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc3_smem_bytes(kTcM)));
     SOV_CUDA(cudaFuncSetAttribute(k_tc3_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc3_smem_bytes(kNB)));
   });
+  const long long ld = s.mp;
   int n = 0;
   for (int kb = 0; kb < s.nb; ++kb) {
     dense_potrf_block<float>(s, kb, st);
     ++n;
-    const int rows = s.mp - (kb + 1) * kNB;
+    const int o = (kb + 1) * kNB;
+    const int rows = s.mp - o;
     if (rows > 0) {
       const int tiles = ceil_div(rows, kTcM);
-      k_tc3_trsm<<<tiles, kTcThreads, tc3_smem_bytes(kNB), st>>>(s.M, s.mp, kb, s.mp, s.Linv, err);
-      k_tc3_syrk<<<tiles * (tiles + 1) / 2, kTcThreads, tc3_smem_bytes(kTcM), st>>>(s.M, s.mp, kb, s.mp, err);
+      if (single) {
+        k_tc3_trsm<<<tiles, kTcThreads, tc3_smem_bytes(kNB), st>>>(s.M, s.mp, kb, s.mp, s.Linv, err);
+        k_tc3_syrk<<<tiles * (tiles + 1) / 2, kTcThreads, tc3_smem_bytes(kTcM), st>>>(s.M, s.mp, kb, s.mp, err);
+      } else {
+        float* panel = s.M + static_cast<long long>(kb) * kNB * ld + o;  // rows o.. of panel kb (column-major)
+        // L_ik(r, n) = sum_k A_ik(r, k) Linv_kk(n, k); Linv_kk(n, k) sits at k * 64 + n
+        WsGemmArgs t{panel, 1, ld, s.Linv + static_cast<long long>(kb) * kNB * kNB, 1, kNB, panel, 1, ld,
+                     rows, kNB, kNB, 1.0f, 0.0f, nullptr, 0, err, 0};
+        launch_gemm_ws<0>(t, st);
+        // A_ij(r, c) -= sum_k L(r, k) L(c, k) on the trailing matrix's lower tiles
+        WsGemmArgs u{panel, 1, ld, panel, 1, ld, s.M + o * ld + o, 1, ld, rows, rows, kNB, -1.0f, 1.0f, nullptr, 0,
+                     err, 1};
+        launch_gemm_ws<0>(u, st);
+      }
       n += 2;
     }
   }

@@ -274,3 +274,64 @@ def load_model_json(text: str | bytes) -> tuple[Model, list[str], list[str]]:
     finally:
         lib.sov_json_model_destroy(h)
     return mdl, names, rows
+
+
+class Presolved:
+    """LP presolve in index form (sov_presolve_lp): `reduced` is the model to solve (when `status`
+    is None; else presolve decided the status), `postsolve(result)` maps its answer back to the
+    original columns and rows (sov_postsolve_lp). Host only."""
+
+    def __init__(self, model: Model):
+        self.model = model
+        self._abi = model.to_abi()
+        self.h = C.c_void_p()
+        check(load().sov_presolve_lp(C.byref(self._abi), C.byref(self.h)))
+        st, rr, cr, bt = (C.c_int32() for _ in range(4))
+        msg = C.create_string_buffer(512)
+        check(load().sov_presolve_info(self.h, C.byref(st), C.byref(rr), C.byref(cr), C.byref(bt), msg, 512))
+        self.status = None if st.value < 0 else st.value
+        self.rows_removed, self.cols_removed, self.bounds_tightened = rr.value, cr.value, bt.value
+        self.message = msg.value.decode()
+        v = load().sov_presolve_reduced(self.h).contents
+        n, m = v.n, v.m
+        nnz = v.col_ptr[n] if n > 0 else 0
+
+        def arr(ptr, count, dtype):
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True) if count else np.zeros(0, dtype)
+
+        self.reduced = Model(n=n, m=m, col_ptr=arr(v.col_ptr, n + 1, np.int32), row_idx=arr(v.row_idx, nnz, np.int32),
+                             values=arr(v.values, nnz, np.float64), obj=arr(v.obj, n, np.float64),
+                             rhs=arr(v.rhs, m, np.float64), sense=np.array([v.sense[i] for i in range(m)], np.int8),
+                             lb=arr(v.lb, n, np.float64), ub=arr(v.ub, n, np.float64),
+                             obj_constant=v.obj_constant, maximize=bool(v.maximize))
+
+    def postsolve(self, reduced: Result | None) -> Result:
+        full = ResultBuffers(self.model, with_diag=False)
+        if reduced is None:
+            check(load().sov_postsolve_lp(self.h, None, C.byref(full.raw)))
+            return full.to_result()
+        rb = ResultBuffers(self.reduced)
+        r = rb.raw
+        r.status, r.iterations, r.has_objective_value = reduced.status, reduced.iterations, int(reduced.has_objective_value)
+        r.objective_value, r.duality_gap = reduced.objective_value, reduced.duality_gap
+        r.primal_residual, r.dual_residual = reduced.primal_residual, reduced.dual_residual
+        r.message = reduced.message.encode()[:511]
+        rb.primal[:] = reduced.primal
+        rb.dual_row[:] = reduced.dual_row
+        if reduced.dual_col is not None:
+            rb.dual_col[:] = reduced.dual_col
+        check(load().sov_postsolve_lp(self.h, C.byref(r), C.byref(full.raw)))
+        return full.to_result()
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            load().sov_presolve_destroy(self.h)
+            self.h = C.c_void_p()
+
+
+def solve_presolved(model: Model, options: InteriorPointOptions | None = None, with_diag: bool = False) -> Result:
+    """Presolve, the GPU IPM on the reduced LP, postsolve (sov_lp_solve_presolved)."""
+    opt = (options or InteriorPointOptions()).to_abi()
+    buf = ResultBuffers(model, with_diag=with_diag)
+    check(load().sov_lp_solve_presolved(C.byref(model.to_abi()), C.byref(opt), C.byref(buf.raw)))
+    return buf.to_result()

@@ -154,6 +154,53 @@ def convex_sequence_qp(n: int, seed: int, target: np.ndarray | None = None,
     return mdl
 
 
+def presolve_lp_example(m: int, n: int, seed: int) -> Model:
+    """A random feasible, bounded LP (random_sparse_lp's construction, k = 4) with what presolve
+    removes added: fixed columns (lb = ub = x0_j), singleton rows of every sense satisfied by x0
+    (x_j <= x0_j + 0.3, -2 x_j >= -2 (x0_j + 0.4), x_j >= x0_j / 2, 3 x_j = 3 x0_j), an empty row
+    (0 <= 5) and an empty column with a positive cost; some columns carry finite upper bounds."""
+    base = random_sparse_lp(m, n, 4, seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 7))
+    # x0 of random_sparse_lp: redraw its stream up to the point where it draws x0
+    r2 = np.random.Generator(np.random.PCG64(seed))
+    np.argsort(r2.random((n, m)), axis=1)
+    r2.standard_normal((n, 4))
+    x0 = r2.uniform(0.1, 1.0, size=n)
+    cols = [list(zip(base.row_idx[base.col_ptr[j]:base.col_ptr[j + 1]].tolist(),
+                     base.values[base.col_ptr[j]:base.col_ptr[j + 1]].tolist())) for j in range(n)]
+    rhs, sense = list(base.rhs), list(base.sense)
+    picks = rng.choice(n, size=min(n, 24), replace=False)
+    lb, ub = np.zeros(n + 1), np.full(n + 1, INF)
+    for q, j in enumerate(picks):
+        kind = q % 6
+        if kind == 0:  # fixed column
+            lb[j] = ub[j] = x0[j]
+            continue
+        if kind == 5:  # a finite upper bound
+            ub[j] = x0[j] + 0.25
+            continue
+        row = len(rhs)
+        a, b, s = [(1.0, x0[j] + 0.3, LE), (-2.0, -2.0 * (x0[j] + 0.4), GE), (1.0, 0.5 * x0[j], GE),
+                   (3.0, 3.0 * x0[j], EQ)][kind - 1]
+        cols[j].append((row, a))
+        rhs.append(b)
+        sense.append(s)
+    rhs.append(5.0)  # an empty row
+    sense.append(LE)
+    cols.append([])  # an empty column, positive cost
+    m2, n2 = len(rhs), n + 1
+    col_ptr = np.zeros(n2 + 1, dtype=np.int32)
+    ri, va = [], []
+    for j, c in enumerate(cols):
+        for r, v in sorted(c):
+            ri.append(r)
+            va.append(v)
+        col_ptr[j + 1] = len(ri)
+    obj = np.concatenate([base.obj, [2.5]])
+    return _lp(n2, m2, col_ptr, np.array(ri, dtype=np.int32), np.array(va), obj, np.array(rhs),
+               np.array(sense, dtype=np.int8), f"presolve_example_{m}x{n}_s{seed}", lb=lb, ub=ub)
+
+
 class TransportFamily:
     """A fixed ns x nt transportation network whose data vary per instance: supplies x(1 + 0.2 N),
     demands x(1 + 0.2 N) rebalanced to the total supply, costs x(1 + 0.1 N) around base values

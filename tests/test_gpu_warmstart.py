@@ -39,6 +39,55 @@ def test_forward_and_gradients_match_fp64_restatement():
             off += size
 
 
+def test_production_shape_gradients_match_restatement():
+    # the multicommodity network's own shape (4040 -> 512 x 3 -> 11800): many K chunks and N tiles per
+    # product, and a weight-gradient reduction over the batch, through the pipelined GEMM
+    rng = np.random.default_rng(7)
+    dims = (4040, 512, 3, 11800)
+    mlp = Mlp(dims[0], dims[3], dims[1], dims[2], seed=5)
+    x = rng.standard_normal((128, dims[0])).astype(np.float32)
+    t = rng.standard_normal((128, dims[3])).astype(np.float32)
+    loss, g = mlp.loss_grad(x, t)
+    bf_loss, bf_g, bf_y = mlp_oracle.loss_and_grad(mlp.params, mlp.dims, x, t, bf16_operands=True)
+    y = mlp.forward(x)
+    assert np.linalg.norm(y - bf_y) <= 1e-3 * np.linalg.norm(bf_y)
+    assert abs(loss - bf_loss) <= 1e-3 * bf_loss
+    off = 0
+    for l in range(len(mlp.dims) - 1):
+        for size in (mlp.dims[l + 1] * mlp.dims[l], mlp.dims[l + 1]):
+            a, b = g[off:off + size], bf_g[off:off + size]
+            assert np.linalg.norm(a - b) <= 5e-3 * np.linalg.norm(b) + 1e-7, (l, size)
+            off += size
+
+
+def test_pipelined_gemm_equals_single_stage_kernel(monkeypatch):
+    # the same products through the single-stage kernel (SOVEREIGN_MLP_GEMM=single, read when the
+    # library first runs a product in a process) and through the pipelined one agree to accumulation
+    # order; run in a child process so the switch takes effect
+    import subprocess
+    import sys
+    code = ("import numpy as np, sys; sys.path.insert(0, '.');"
+            "from sovereign_b200.warmstart import Mlp;"
+            "r = np.random.default_rng(2); m = Mlp(300, 200, 160, 2, seed=1);"
+            "x = r.standard_normal((70, 300)).astype(np.float32); t = r.standard_normal((70, 200)).astype(np.float32);"
+            "l, g = m.loss_grad(x, t); np.save(sys.argv[1], np.concatenate([[l], g, m.forward(x).ravel()]))")
+    import os
+    import tempfile
+    out = {}
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for mode in ("single", "pipelined"):
+        env = dict(os.environ)
+        if mode == "single":
+            env["SOVEREIGN_MLP_GEMM"] = "single"
+        else:
+            env.pop("SOVEREIGN_MLP_GEMM", None)
+        f = os.path.join(tempfile.mkdtemp(), f"{mode}.npy")
+        subprocess.run([sys.executable, "-c", code, f], check=True, cwd=root, env=env, timeout=300)
+        out[mode] = np.load(f)
+    a, b = out["single"], out["pipelined"]
+    assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(a)
+
+
 def test_training_reduces_loss():
     rng = np.random.default_rng(1)
     x = rng.standard_normal((512, 32)).astype(np.float32)
