@@ -48,7 +48,7 @@ namespace wsg {
 constexpr int kTile = 128;
 constexpr int kThreads = 160;       // warps 0-3: producers and epilogue; warp 4: MMA issue
 constexpr int kOperandBytes = 16384;  // 128 rows x 128 bytes of K
-constexpr long long kWaitLimit = 1ll << 26;
+constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls: a few seconds at most
 
 template <int KIND>
 struct Cfg;
