@@ -21,9 +21,11 @@
 // and the reference QP's residual and gap measures (:2975-2994): p_res = |rp|_inf / max(1, |b|_inf),
 // d_res = |rd|_inf / max(1, |c|_inf + |Qx|_inf), gap = w'z / (1 + |objective|).
 //
-// The whole solve is one launch of one CTA: the vector passes are spread over its threads, the
-// banded factorization and the two triangular sweeps per solve run on thread 0 (a dependent chain;
-// the band window lives in registers, the next column's entries are loaded ahead).
+// The whole solve is one launch of one CTA: the vector passes are spread over its threads, and so
+// is the banded factorization: the columns are cut into up to 512 segments, one per thread, each an
+// interior factored as a band chain (window in registers, next column loaded ahead) plus a
+// separator of kd columns; the separators' Schur complement, block tridiagonal, is factored by one
+// thread (part_factor / part_solve below). SOVEREIGN_XBAND_SEGMENTS=1 gives the single chain.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +62,12 @@ struct XbDev {
   // work
   double *th, *rph, *rpl, *rd, *uh, *ul, *dxh, *dxl, *dw, *dzh, *dzl, *dwa, *dza;
   double *Kh, *Kl;  // (kd + 1) x n: K[j][j - p] at p * n + j, overwritten by L (p >= 1) and 1 / D (p = 0)
+  // partitioned factorization: P segments, each an interior and (but the last) a separator of kd
+  int P;
+  double *Wh, *Wl;  // 2 kd x n: the interiors' spikes K_II^-1 K_IS (left kd columns, then right kd)
+  double *Ch, *Cl;  // P x 3 x kd^2: Schur contributions of each interior (to S_{s-1}, to S_s, block (s, s-1))
+  double *Th, *Tl;  // P x 2 x kd^2: separator chain factors (L_t, then D_t^-1)
+  double *Rh, *Rl;  // P x 2 x kd: the interiors' contributions to the separators' right-hand sides
   XbOut* out;
 };
 
@@ -69,10 +77,12 @@ __device__ __forceinline__ void st_dd(double* h, double* l, long long i, dd v) {
   l[i] = v.lo;
 }
 
-// Banded L D L' of K in place, thread 0 alone. Returns false on a pivot that is not positive and
-// finite (K = Q + A' theta A is positive definite, so only a breakdown of the iterate gives one).
+// Banded L D L' of rows [a, e) of K in place, by one thread: entries that reach left of a (the
+// coupling to the separator before the range) are neither used nor overwritten. Returns false on a
+// pivot that is not positive and finite (K = Q + A' theta A is positive definite, so only a
+// breakdown of the iterate gives one).
 template <int KD>
-__device__ bool band_factor_dd(double* Kh, double* Kl, int n) {
+__device__ bool band_factor_dd(double* Kh, double* Kl, int n, int a, int e) {
   dd L[KD + 1][KD + 1];  // L[p][q] = L(j - p, j - p - q) of the rows above
   dd Dv[KD + 1];         // D(j - p)
   dd Di[KD + 1];         // 1 / D(j - p)
@@ -85,35 +95,35 @@ __device__ bool band_factor_dd(double* Kh, double* Kl, int n) {
   }
   dd row[KD + 1];  // K(j, j - p)
 #pragma unroll
-  for (int p = 0; p <= KD; ++p) row[p] = p == 0 ? ld_dd(Kh, Kl, 0) : dd_from(0.0);
-  for (int j = 0; j < n; ++j) {
+  for (int p = 0; p <= KD; ++p) row[p] = (p == 0 && a < e) ? ld_dd(Kh, Kl, a) : dd_from(0.0);
+  for (int j = a; j < e; ++j) {
     dd next[KD + 1];
 #pragma unroll
     for (int p = 0; p <= KD; ++p)
-      next[p] = (j + 1 < n && j + 1 - p >= 0) ? ld_dd(Kh, Kl, static_cast<long long>(p) * n + j + 1) : dd_from(0.0);
+      next[p] = (j + 1 < e && j + 1 - p >= a) ? ld_dd(Kh, Kl, static_cast<long long>(p) * n + j + 1) : dd_from(0.0);
     dd l[KD + 1];
     l[0] = dd_from(1.0);
 #pragma unroll
     for (int p = KD; p >= 1; --p) {
-      if (j - p < 0) {
+      if (j - p < a) {
         l[p] = dd_from(0.0);
         continue;
       }
       dd v = row[p];
 #pragma unroll
       for (int q = p + 1; q <= KD; ++q)  // L(j, j-q) D(j-q) L(j-p, j-q)
-        if (j - q >= 0) v = dd_sub(v, dd_mul(dd_mul(l[q], Dv[q]), L[p][q - p]));
+        if (j - q >= a) v = dd_sub(v, dd_mul(dd_mul(l[q], Dv[q]), L[p][q - p]));
       l[p] = dd_mul(v, Di[p]);
     }
     dd d = row[0];
 #pragma unroll
     for (int p = 1; p <= KD; ++p)
-      if (j - p >= 0) d = dd_sub(d, dd_mul(dd_mul(l[p], l[p]), Dv[p]));
+      if (j - p >= a) d = dd_sub(d, dd_mul(dd_mul(l[p], l[p]), Dv[p]));
     if (!(d.hi > 0.0) || !isfinite(d.hi)) return false;
     const dd di = dd_recip(d);
 #pragma unroll
     for (int p = 1; p <= KD; ++p)
-      if (j - p >= 0) st_dd(Kh, Kl, static_cast<long long>(p) * n + j, l[p]);
+      if (j - p >= a) st_dd(Kh, Kl, static_cast<long long>(p) * n + j, l[p]);
     st_dd(Kh, Kl, j, di);
 #pragma unroll
     for (int p = KD; p >= 2; --p) {
@@ -132,17 +142,17 @@ __device__ bool band_factor_dd(double* Kh, double* Kl, int n) {
   return true;
 }
 
-// K dx = rhs with the factor above (in place in rh/rl), thread 0 alone.
+// K_[a,e) x = rhs with the factor above, in place in rh/rl (global indexing), one thread.
 template <int KD>
-__device__ void band_solve_dd(const double* Kh, const double* Kl, int n, double* rh, double* rl) {
+__device__ void band_solve_dd(const double* Kh, const double* Kl, int n, int a, int e, double* rh, double* rl) {
   dd win[KD + 1];
 #pragma unroll
   for (int p = 0; p <= KD; ++p) win[p] = dd_from(0.0);
-  for (int j = 0; j < n; ++j) {  // L y = rhs, then y / D
+  for (int j = a; j < e; ++j) {  // L y = rhs, then y / D
     dd v = ld_dd(rh, rl, j);
 #pragma unroll
     for (int p = 1; p <= KD; ++p)
-      if (j - p >= 0) v = dd_sub(v, dd_mul(ld_dd(Kh, Kl, static_cast<long long>(p) * n + j), win[p]));
+      if (j - p >= a) v = dd_sub(v, dd_mul(ld_dd(Kh, Kl, static_cast<long long>(p) * n + j), win[p]));
 #pragma unroll
     for (int p = KD; p >= 2; --p) win[p] = win[p - 1];
     win[1] = v;
@@ -150,16 +160,253 @@ __device__ void band_solve_dd(const double* Kh, const double* Kl, int n, double*
   }
 #pragma unroll
   for (int p = 0; p <= KD; ++p) win[p] = dd_from(0.0);
-  for (int j = n - 1; j >= 0; --j) {  // L' x = v
+  for (int j = e - 1; j >= a; --j) {  // L' x = v
     dd v = ld_dd(rh, rl, j);
 #pragma unroll
     for (int p = 1; p <= KD; ++p)
-      if (j + p < n) v = dd_sub(v, dd_mul(ld_dd(Kh, Kl, static_cast<long long>(p) * n + j + p), win[p]));
+      if (j + p < e) v = dd_sub(v, dd_mul(ld_dd(Kh, Kl, static_cast<long long>(p) * n + j + p), win[p]));
 #pragma unroll
     for (int p = KD; p >= 2; --p) win[p] = win[p - 1];
     win[1] = v;
     st_dd(rh, rl, j, v);
   }
+}
+
+// ---- partitioned factorization and solve (all threads of the CTA) ----
+// Segment s of P covers [lo_s, hi_s): its interior [lo_s, e_s) with e_s = hi_s - KD, and (but the
+// last) the separator S_s = [e_s, hi_s). Interiors couple only to the separators on either side,
+// so with the separators ordered last K = [K_II K_IS; K_SI K_SS] has a block-diagonal K_II: every
+// thread factors its own interior (band L D L'), solves for its spikes W = K_II^-1 K_IS (nonzero
+// right-hand sides only next to the separators) and forms its part of the Schur complement
+// S = K_SS - K_SI W, which is block tridiagonal with KD x KD blocks. Thread 0 factors S as a
+// chain of P - 1 blocks. A solve runs the interiors, the separator chain and the back-substitution
+// y_I - W x_S. It is the band L D L' of a symmetric permutation of K, as stable as the natural one.
+template <int KD>
+__device__ __forceinline__ void seg_range(int s, int P, int n, int& lo, int& e, int& hi) {
+  lo = static_cast<int>(static_cast<long long>(s) * n / P);
+  hi = static_cast<int>(static_cast<long long>(s + 1) * n / P);
+  e = s < P - 1 ? hi - KD : hi;
+}
+
+// K(i, j), |i - j| <= KD, from the band rows; only entries the interior factors leave intact
+// (separator rows, and interior entries that reach the previous separator) are read this way
+template <int KD>
+__device__ __forceinline__ dd k_at(const XbDev& d, int i, int j) {
+  const int hi = max(i, j), p = abs(i - j);
+  return ld_dd(d.Kh, d.Kl, static_cast<long long>(p) * d.n + hi);
+}
+
+template <int KD>
+__device__ __forceinline__ void small_inverse(dd (&A)[KD][KD], dd (&inv)[KD][KD], bool& ok) {
+#pragma unroll
+  for (int r = 0; r < KD; ++r)
+#pragma unroll
+    for (int c = 0; c < KD; ++c) inv[r][c] = dd_from(r == c ? 1.0 : 0.0);
+#pragma unroll
+  for (int k = 0; k < KD; ++k) {  // Gauss-Jordan without pivoting (A is positive definite)
+    if (!(A[k][k].hi > 0.0) || !isfinite(A[k][k].hi)) ok = false;
+    const dd ip = dd_recip(A[k][k]);
+#pragma unroll
+    for (int c = 0; c < KD; ++c) {
+      A[k][c] = dd_mul(A[k][c], ip);
+      inv[k][c] = dd_mul(inv[k][c], ip);
+    }
+#pragma unroll
+    for (int r = 0; r < KD; ++r) {
+      if (r == k) continue;
+      const dd f = A[r][k];
+#pragma unroll
+      for (int c = 0; c < KD; ++c) {
+        A[r][c] = dd_sub(A[r][c], dd_mul(f, A[k][c]));
+        inv[r][c] = dd_sub(inv[r][c], dd_mul(f, inv[k][c]));
+      }
+    }
+  }
+}
+
+template <int KD>
+__device__ void part_factor(const XbDev& d, int* bad) {
+  const int P = d.P, n = d.n, s = threadIdx.x;
+  constexpr int KK = KD * KD;
+  if (s < P) {
+    int lo, e, hi;
+    seg_range<KD>(s, P, n, lo, e, hi);
+    if (!band_factor_dd<KD>(d.Kh, d.Kl, n, lo, e)) {
+      atomicExch(bad, 1);
+    } else {
+      for (int c = 0; c < 2 * KD; ++c) {  // spikes
+        const bool left = c < KD;
+        if ((left && s == 0) || (!left && s == P - 1)) continue;
+        const int sep = left ? lo - KD + c : e + (c - KD);
+        double* wh = d.Wh + static_cast<long long>(c) * n;
+        double* wl = d.Wl + static_cast<long long>(c) * n;
+        for (int j = lo; j < e; ++j) st_dd(wh, wl, j, abs(j - sep) <= KD ? k_at<KD>(d, j, sep) : dd_from(0.0));
+        band_solve_dd<KD>(d.Kh, d.Kl, n, lo, e, wh, wl);
+      }
+      for (int which = 0; which < 3; ++which) {  // Schur contributions
+        if ((which == 0 && s == 0) || (which == 1 && s == P - 1) || (which == 2 && (s == 0 || s == P - 1))) continue;
+#pragma unroll
+        for (int r = 0; r < KD; ++r) {
+          const int sep = which == 0 ? lo - KD + r : e + r;
+          const int j0 = which == 0 ? lo : max(lo, sep - KD), j1 = which == 0 ? min(e, sep + KD + 1) : e;
+#pragma unroll
+          for (int c = 0; c < KD; ++c) {
+            const int col = which == 1 ? KD + c : c;
+            dd acc = dd_from(0.0);
+            for (int j = j0; j < j1; ++j)
+              acc = dd_add(acc, dd_mul(k_at<KD>(d, sep, j), ld_dd(d.Wh + static_cast<long long>(col) * n,
+                                                                  d.Wl + static_cast<long long>(col) * n, j)));
+            st_dd(d.Ch, d.Cl, (static_cast<long long>(s) * 3 + which) * KK + r * KD + c, dd_neg(acc));
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && P > 1 && !*bad) {  // block tridiagonal L D L' of S
+    bool ok = true;
+    dd Dprev[KD][KD];
+    for (int t = 0; t < P - 1; ++t) {
+      int lo, e, hi;
+      seg_range<KD>(t, P, n, lo, e, hi);
+      dd A[KD][KD];
+#pragma unroll
+      for (int r = 0; r < KD; ++r)
+#pragma unroll
+        for (int c = 0; c < KD; ++c)
+          A[r][c] = dd_add(dd_add(k_at<KD>(d, e + r, e + c), ld_dd(d.Ch, d.Cl, (static_cast<long long>(t) * 3 + 1) * KK + r * KD + c)),
+                           ld_dd(d.Ch, d.Cl, (static_cast<long long>(t + 1) * 3 + 0) * KK + r * KD + c));
+      if (t >= 1) {
+        dd B[KD][KD], L[KD][KD];
+#pragma unroll
+        for (int r = 0; r < KD; ++r)
+#pragma unroll
+          for (int c = 0; c < KD; ++c) B[r][c] = ld_dd(d.Ch, d.Cl, (static_cast<long long>(t) * 3 + 2) * KK + r * KD + c);
+#pragma unroll
+        for (int r = 0; r < KD; ++r)
+#pragma unroll
+          for (int c = 0; c < KD; ++c) {
+            dd v = dd_from(0.0);
+#pragma unroll
+            for (int q = 0; q < KD; ++q) v = dd_add(v, dd_mul(B[r][q], Dprev[q][c]));
+            L[r][c] = v;
+            st_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 0) * KK + r * KD + c, v);
+          }
+#pragma unroll
+        for (int r = 0; r < KD; ++r)
+#pragma unroll
+          for (int c = 0; c < KD; ++c) {
+            dd v = A[r][c];
+#pragma unroll
+            for (int q = 0; q < KD; ++q) v = dd_sub(v, dd_mul(L[r][q], B[c][q]));
+            A[r][c] = v;
+          }
+      }
+      small_inverse<KD>(A, Dprev, ok);
+#pragma unroll
+      for (int r = 0; r < KD; ++r)
+#pragma unroll
+        for (int c = 0; c < KD; ++c) st_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 1) * KK + r * KD + c, Dprev[r][c]);
+    }
+    if (!ok) atomicExch(bad, 1);
+  }
+  __syncthreads();
+}
+
+// K x = rhs in place in xh/xl with the partitioned factor.
+template <int KD>
+__device__ void part_solve(const XbDev& d, double* xh, double* xl) {
+  const int P = d.P, n = d.n, s = threadIdx.x;
+  constexpr int KK = KD * KD;
+  if (s < P) {
+    int lo, e, hi;
+    seg_range<KD>(s, P, n, lo, e, hi);
+    band_solve_dd<KD>(d.Kh, d.Kl, n, lo, e, xh, xl);  // y_I
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {  // K(S, I_s) y_I onto S_{s-1} (side 0) and S_s (side 1)
+      if ((side == 0 && s == 0) || (side == 1 && s == P - 1)) continue;
+#pragma unroll
+      for (int r = 0; r < KD; ++r) {
+        const int sep = side == 0 ? lo - KD + r : e + r;
+        const int j0 = side == 0 ? lo : max(lo, sep - KD), j1 = side == 0 ? min(e, sep + KD + 1) : e;
+        dd acc = dd_from(0.0);
+        for (int j = j0; j < j1; ++j) acc = dd_add(acc, dd_mul(k_at<KD>(d, sep, j), ld_dd(xh, xl, j)));
+        st_dd(d.Rh, d.Rl, (static_cast<long long>(s) * 2 + side) * KD + r, acc);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && P > 1) {
+    // forward: z_t = (r_St - contributions) - L_t z_{t-1}, kept in the separator slots of x
+    for (int t = 0; t < P - 1; ++t) {
+      int lo, e, hi;
+      seg_range<KD>(t, P, n, lo, e, hi);
+      dd zp[KD];
+      if (t >= 1) {
+        int lo2, e2, hi2;
+        seg_range<KD>(t - 1, P, n, lo2, e2, hi2);
+#pragma unroll
+        for (int c = 0; c < KD; ++c) zp[c] = ld_dd(xh, xl, e2 + c);
+      }
+#pragma unroll
+      for (int r = 0; r < KD; ++r) {
+        dd v = dd_sub(dd_sub(ld_dd(xh, xl, e + r), ld_dd(d.Rh, d.Rl, (static_cast<long long>(t) * 2 + 1) * KD + r)),
+                      ld_dd(d.Rh, d.Rl, (static_cast<long long>(t + 1) * 2 + 0) * KD + r));
+        if (t >= 1)
+#pragma unroll
+          for (int c = 0; c < KD; ++c)
+            v = dd_sub(v, dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 0) * KK + r * KD + c), zp[c]));
+        st_dd(xh, xl, e + r, v);
+      }
+    }
+    // w_t = D_t^-1 z_t, then backward x_t = w_t - L_{t+1}' x_{t+1}
+    dd xn[KD];
+    for (int t = P - 2; t >= 0; --t) {
+      int lo, e, hi;
+      seg_range<KD>(t, P, n, lo, e, hi);
+      dd z[KD], w[KD];
+#pragma unroll
+      for (int c = 0; c < KD; ++c) z[c] = ld_dd(xh, xl, e + c);
+#pragma unroll
+      for (int r = 0; r < KD; ++r) {
+        dd v = dd_from(0.0);
+#pragma unroll
+        for (int c = 0; c < KD; ++c) v = dd_add(v, dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 1) * KK + r * KD + c), z[c]));
+        w[r] = v;
+      }
+      if (t < P - 2)
+#pragma unroll
+        for (int r = 0; r < KD; ++r)
+#pragma unroll
+          for (int c = 0; c < KD; ++c)  // (L_{t+1}')[r][c] = L_{t+1}[c][r]
+            w[r] = dd_sub(w[r], dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(t + 1) * 2 + 0) * KK + c * KD + r), xn[c]));
+#pragma unroll
+      for (int r = 0; r < KD; ++r) {
+        st_dd(xh, xl, e + r, w[r]);
+        xn[r] = w[r];
+      }
+    }
+  }
+  __syncthreads();
+  if (s < P && P > 1) {  // x_I = y_I - W_left x_S(s-1) - W_right x_S(s)
+    int lo, e, hi;
+    seg_range<KD>(s, P, n, lo, e, hi);
+    dd xs[2 * KD];
+#pragma unroll
+    for (int c = 0; c < 2 * KD; ++c) {
+      const bool left = c < KD;
+      xs[c] = ((left && s == 0) || (!left && s == P - 1)) ? dd_from(0.0) : ld_dd(xh, xl, left ? lo - KD + c : e + (c - KD));
+    }
+    for (int j = lo; j < e; ++j) {
+      dd v = ld_dd(xh, xl, j);
+#pragma unroll
+      for (int c = 0; c < 2 * KD; ++c)
+        if (xs[c].hi != 0.0 || xs[c].lo != 0.0)
+          v = dd_sub(v, dd_mul(ld_dd(d.Wh + static_cast<long long>(c) * n, d.Wl + static_cast<long long>(c) * n, j), xs[c]));
+      st_dd(xh, xl, j, v);
+    }
+  }
+  __syncthreads();
 }
 
 // (A v)_r in double-double
@@ -180,7 +427,7 @@ template <int KD>
 __global__ void __launch_bounds__(kXbThreads, 1) k_xband_ipm(XbDev d) {
   __shared__ double red[4 * 32];
   __shared__ double s_mu, s_sigma, s_alpha_p, s_alpha_d;
-  __shared__ int s_stop;
+  __shared__ int s_stop, s_bad;
   const int tid = threadIdx.x;
   const int n = d.n, m = d.m;
   const double inf = INFINITY;
@@ -274,12 +521,13 @@ __global__ void __launch_bounds__(kXbThreads, 1) k_xband_ipm(XbDev d) {
       for (int p = 0; p <= KD; ++p) st_dd(d.Kh, d.Kl, static_cast<long long>(p) * n + j, acc[p]);
     }
     __syncthreads();
-    if (tid == 0) {
-      if (!band_factor_dd<KD>(d.Kh, d.Kl, n)) {
-        d.out->status = SOV_NUMERICAL_ERROR;
-        d.out->failed = 2;
-        s_stop = 1;
-      }
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    part_factor<KD>(d, &s_bad);
+    if (tid == 0 && s_bad) {
+      d.out->status = SOV_NUMERICAL_ERROR;
+      d.out->failed = 2;
+      s_stop = 1;
     }
     __syncthreads();
     if (s_stop) break;
@@ -296,8 +544,7 @@ __global__ void __launch_bounds__(kXbThreads, 1) k_xband_ipm(XbDev d) {
       for (int j = tid; j < n; j += kXbThreads)
         st_dd(d.dxh, d.dxl, j, dd_neg(dd_add_d(col_dot(d, j, d.uh, d.ul), d.rd[j])));
       __syncthreads();
-      if (tid == 0) band_solve_dd<KD>(d.Kh, d.Kl, n, d.dxh, d.dxl);
-      __syncthreads();
+      part_solve<KD>(d, d.dxh, d.dxl);
       // dw = A dx + rp, dz = -rc / w - theta dw; largest steps to the boundary
       double a[2] = {inf, inf};
       for (int r = tid; r < m; r += kXbThreads) {
@@ -498,8 +745,12 @@ int solve_xband(const sov_model& model, const XBandModel& xb, const sov_options&
   c.put(xb.c);
   b.put(xb.b);
   // n-vectors: xh xl rd dxh dxl; m-vectors: zh zl w th rph rpl uh ul dw dzh dzl dwa dza; band 2 (kd+1) n
-  const size_t nv = 5, mv = 13;
-  XbBuf<double> work(nv * n + mv * m + 2 * static_cast<size_t>(kd + 1) * n, st);
+  // segments of the partitioned factorization: one per thread, at least 16 kd columns each
+  int P = std::max(1, std::min(kXbThreads, n / (16 * kd)));
+  if (const char* e = std::getenv("SOVEREIGN_XBAND_SEGMENTS")) P = std::max(1, std::min(P, std::atoi(e)));
+  const size_t nv = 5, mv = 13, kk = static_cast<size_t>(kd) * kd;
+  const size_t part = 2 * (2 * static_cast<size_t>(kd) * n + 3 * P * kk + 2 * P * kk + 2 * static_cast<size_t>(P) * kd);
+  XbBuf<double> work(nv * n + mv * m + 2 * static_cast<size_t>(kd + 1) * n + part, st);
   XbBuf<XbOut> out(1, st);
   SOV_CUDA(cudaMemsetAsync(out.p, 0, sizeof(XbOut), st));
   XbDev d{};
@@ -550,6 +801,15 @@ int solve_xband(const sov_model& model, const XBandModel& xb, const sov_options&
   d.dza = take(m);
   d.Kh = take(static_cast<size_t>(kd + 1) * n);
   d.Kl = take(static_cast<size_t>(kd + 1) * n);
+  d.P = P;
+  d.Wh = take(2 * static_cast<size_t>(kd) * n);
+  d.Wl = take(2 * static_cast<size_t>(kd) * n);
+  d.Ch = take(3 * P * kk);
+  d.Cl = take(3 * P * kk);
+  d.Th = take(2 * P * kk);
+  d.Tl = take(2 * P * kk);
+  d.Rh = take(2 * static_cast<size_t>(P) * kd);
+  d.Rl = take(2 * static_cast<size_t>(P) * kd);
   d.out = out.p;
   cudaEvent_t e0, e1;
   SOV_CUDA(cudaEventCreate(&e0));

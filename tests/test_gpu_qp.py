@@ -133,3 +133,15 @@ def test_config2_full_size_matches_reference():
     assert r.primal_residual <= 1e-8 and r.dual_residual <= 1e-8 and r.duality_gap <= 1e-8
     assert np.max(np.abs(r.primal - g["primal"])) < 1e-5
     assert np.min(r.primal[:-2] - 2 * r.primal[1:-1] + r.primal[2:]) > -1e-9
+
+
+def test_partitioned_band_factor_equals_single_chain(monkeypatch):
+    # the x-space path's factorization cut into segments (one per thread, separators last) against
+    # the single chain over all columns (SOVEREIGN_XBAND_SEGMENTS=1): the same optimum
+    mdl = P.convex_sequence_qp(4002, 5)
+    part = QpInteriorPointSolver().solve(mdl)
+    monkeypatch.setenv("SOVEREIGN_XBAND_SEGMENTS", "1")
+    chain = QpInteriorPointSolver().solve(mdl)
+    assert part.status_name == chain.status_name == "OPTIMAL", (part.message, chain.message)
+    assert rel(part.objective_value, chain.objective_value) < 1e-12
+    assert np.max(np.abs(part.primal - chain.primal)) < 1e-8
