@@ -262,12 +262,22 @@ def run_single_workload(args):
     test = [fam.instance_from_seed(900000 + k) for k in range(args.eval)]
     opts = InteriorPointOptions()
     t0 = time.perf_counter()
-    # training targets: the iterate at the start of iteration 6 (early central-path stretch)
-    cold_train, _ = solve_many([m for m, _ in train], InteriorPointOptions(ipm_iterate_at=6), workers=args.workers)
+    # training targets: the iterate at the start of iteration 6 (early central-path stretch), made
+    # in chunks so that a 50k-instance set keeps only its float32 targets in host memory
+    xs, ts, ws = [], [], None
+    for c0 in range(0, len(train), 2048):
+        chunk = train[c0:c0 + 2048]
+        res, _ = solve_many([m for m, _ in chunk], InteriorPointOptions(ipm_iterate_at=6), workers=args.workers)
+        if ws is None:
+            ws = WarmStart(fam.param_dim, res[0].n_ipm, res[0].m_ipm, hidden=512, layers=3, seed=0)
+        ok, t = ws.targets(res)
+        xs.append(np.stack([p for _, p in chunk])[ok])
+        ts.append(t.astype(np.float32))
+        del res
     t_gen = time.perf_counter() - t0
-    ws = WarmStart(fam.param_dim, cold_train[0].n_ipm, cold_train[0].m_ipm, hidden=512, layers=3, seed=0)
     t0 = time.perf_counter()
-    loss = ws.fit(np.stack([p for _, p in train]), cold_train, epochs=40, batch=128, lr=1e-3)
+    loss = ws.fit_arrays(np.concatenate(xs), np.concatenate(ts), epochs=args.epochs, batch=128,
+                         lr=1e-3)
     t_train = time.perf_counter() - t0
     cold, t_cold = solve_many([m for m, _ in test], opts, workers=args.workers)
     t0 = time.perf_counter()
@@ -279,7 +289,8 @@ def run_single_workload(args):
               for k in ok) if ok else None
     _line(METRIC, len(test) / (t_warm + t_pred), UNIT, args, 1e3 * (t_warm + t_pred) / len(test), "f64",
           dict(workload=f"multicommodity 200 nodes / 1000 arcs / 4 commodities, {args.eval} eval instances, "
-                        f"MLP 4040-512x3-11800 trained on {args.train} IPM solutions, {args.workers} concurrent solves"),
+                        f"MLP 4040-512x3-11800 trained on {args.train} IPM solutions ({args.epochs} epochs), "
+                        f"{args.workers} concurrent solves"),
           cold=dict(lps_per_s=len(test) / t_cold, mean_iterations=float(np.mean([r.iterations for r in cold]))),
           warm=dict(lps_per_s=len(test) / (t_warm + t_pred), mean_iterations=float(np.mean([r.iterations for r in warm])),
                     used=int(sum(r.diagnostics["warm_start_used"] for r in warm))),
@@ -406,6 +417,7 @@ def main():
     ap.add_argument("--train", type=int, default=1024, help="c4: training instances")
     ap.add_argument("--workers", type=int, default=16, help="c4: concurrent single-LP solves (one stream each)")
     ap.add_argument("--eval", type=int, default=128, help="c4: evaluation instances")
+    ap.add_argument("--epochs", type=int, default=40, help="c4: training epochs")
     args = ap.parse_args()
     if args.workload != "batch":
         run_single_workload(args)

@@ -130,13 +130,22 @@ class WarmStart:
                                       np.log(np.maximum(r.ipm_s, self.FLOOR))]) for r in results])
         return t
 
+    def targets(self, results: list[Result]) -> tuple[np.ndarray, np.ndarray]:
+        """(indices of the OPTIMAL results, their training targets): log x, y, log s of the captured
+        iterate. Lets a caller generate a large training set in chunks and drop the results."""
+        ok = [k for k, r in enumerate(results) if r.status_name == "OPTIMAL"]
+        return np.array(ok, dtype=np.int64), self._targets([results[k] for k in ok])
+
     def fit(self, params: np.ndarray, results: list[Result], epochs: int = 60, batch: int = 128, lr: float = 1e-3,
             seed: int = 0) -> float:
-        ok = [k for k, r in enumerate(results) if r.status_name == "OPTIMAL"]
-        x = params[ok]
-        t = self._targets([results[k] for k in ok])
-        self.fin, self.fout = Normalizer.fit(x), Normalizer.fit(t)
-        return self.mlp.train(self.fin.apply(x), self.fout.apply(t), epochs, batch, lr, seed)
+        ok, t = self.targets(results)
+        return self.fit_arrays(params[ok], t, epochs, batch, lr, seed)
+
+    def fit_arrays(self, params: np.ndarray, targets: np.ndarray, epochs: int = 60, batch: int = 128,
+                   lr: float = 1e-3, seed: int = 0) -> float:
+        """Normalizers and network from parameter rows and their targets (see targets())."""
+        self.fin, self.fout = Normalizer.fit(params), Normalizer.fit(targets)
+        return self.mlp.train(self.fin.apply(params), self.fout.apply(targets), epochs, batch, lr, seed)
 
     def predict(self, params: np.ndarray, delta: float = 1e-6) -> list[tuple[np.ndarray, np.ndarray, np.ndarray]]:
         """Warm starts floored into the interior: x, s >= delta (scaled problem units). Normalization,
