@@ -381,6 +381,18 @@ def run_batched_warm_start(args):
             times.append(batch.stats()["kernel_ms"])
         return float(np.mean(times))
 
+    # the plain FP64 GPU IPM on the same instances: the single-problem engine, PLAIN_WORKERS solves
+    # in flight on separate streams (the composition's baseline: batched cold, then batched warm)
+    import concurrent.futures as cf
+    from sovereign_b200.ipm import InteriorPointSolver
+    solver = InteriorPointSolver()
+    with cf.ThreadPoolExecutor(max_workers=PLAIN_WORKERS) as ex:
+        list(ex.map(solver.solve, models[:2 * PLAIN_WORKERS]))
+        t0 = time.perf_counter()
+        plain_res = list(ex.map(solver.solve, models))
+        t_plain = time.perf_counter() - t0
+    plain_err = max(abs(p.objective_value - c[2]) / max(1.0, abs(c[2])) for p, c in zip(plain_res, cold)
+                    if p.status_name == "OPTIMAL" and c[0] == A.OPTIMAL)
     with DeviceBatch(models) as b:
         ms_cold = device_ms(b)
     with DeviceBatch(models, warm_starts=starts) as b:
@@ -396,6 +408,13 @@ def run_batched_warm_start(args):
                     used=int(sum(w[3] for w in warm)), e2e_lps_per_s=count / (t_warm + t_pred), predict_s=t_pred,
                     e2e_device_starts_lps_per_s=count / t_pred_dev, device_starts_identical=same_dev),
           speedup_warm_vs_cold=ms_cold / ms_warm, optimal=f"{len(ok)}/{count}",
+          plain_fp64_gpu=dict(lps_per_s=count / t_plain, workers=PLAIN_WORKERS,
+                              max_rel_obj_diff_vs_batched=plain_err,
+                              sample=f"the same {count} LPs through sov_lp_solve (FP64), {PLAIN_WORKERS} concurrent "
+                                     "solves, wall clock"),
+          composition=dict(batched_cold_vs_plain=(count / (ms_cold * 1e-3)) / (count / t_plain),
+                           batched_warm_vs_plain=value / (count / t_plain),
+                           e2e_batched_warm_device_starts_vs_plain=(count / t_pred_dev) / (count / t_plain)),
           max_rel_obj_diff_warm_vs_cold=err, train_loss=loss, seconds=dict(generate=t_gen, train=t_train),
           e2e=dict(value=count / (t_warm + t_pred), unit=UNIT,
                    note="sov_lp_solve_batch with per-LP warm starts from host buffers, plus the MLP prediction"))
