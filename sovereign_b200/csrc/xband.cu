@@ -481,16 +481,16 @@ __global__ void __launch_bounds__(kXbThreads, 1) k_xband_ipm(XbDev d) {
       s_mu = mu;
       s_stop = 0;
       if (!isfinite(mu) || !isfinite(p_res) || !isfinite(d_res)) {
-        o->status = SOV_NUMERICAL_ERROR;
+        o->status = SOV_ERROR;
         o->failed = 1;
         s_stop = 1;
       } else if (p_res <= ftol && d_res <= ftol && gap <= otol) {
         o->status = SOV_OPTIMAL;
         s_stop = 1;
       } else if (it >= d.max_iter) {
-        o->status = (p_res <= d.feas_tol && d_res <= d.feas_tol && gap <= d.opt_tol) ? SOV_OPTIMAL
-                    : p_res <= d.feas_tol                                           ? SOV_FEASIBLE
-                                                                                    : SOV_ITERATION_LIMIT;
+        // at the limit the reference QP's own tolerances decide; otherwise ERROR without an
+        // objective, as its failure exits publish (qp_interior_point.cpp:3042-3048, :3112-3115)
+        o->status = (p_res <= d.feas_tol && d_res <= d.feas_tol && gap <= d.opt_tol) ? SOV_OPTIMAL : SOV_ERROR;
         s_stop = 1;
       }
     }
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kXbThreads, 1) k_xband_ipm(XbDev d) {
     __syncthreads();
     part_factor<KD>(d, &s_bad);
     if (tid == 0 && s_bad) {
-      d.out->status = SOV_NUMERICAL_ERROR;
+      d.out->status = SOV_ERROR;
       d.out->failed = 2;
       s_stop = 1;
     }
@@ -841,7 +841,7 @@ int solve_xband(const sov_model& model, const XBandModel& xb, const sov_options&
   }
   r->status = o.status;
   r->iterations = o.iterations;
-  r->has_objective_value = 1;
+  r->has_objective_value = o.status == SOV_OPTIMAL ? 1 : 0;
   r->duality_gap = o.gap;
   r->primal_residual = o.p_res;
   r->dual_residual = o.d_res;
