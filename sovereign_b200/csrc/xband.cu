@@ -263,25 +263,51 @@ __device__ void part_factor(const XbDev& d, int* bad) {
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0 && P > 1 && !*bad) {  // block tridiagonal L D L' of S
+  // the separators' diagonal blocks A_t = K(S_t, S_t) + the Schur parts of both neighbouring
+  // interiors, formed in parallel (into the slot of interior t's right contribution)
+  if (s < P - 1 && !*bad) {
+    int lo, e, hi;
+    seg_range<KD>(s, P, n, lo, e, hi);
+#pragma unroll
+    for (int r = 0; r < KD; ++r)
+#pragma unroll
+      for (int c = 0; c < KD; ++c) {
+        const long long at = (static_cast<long long>(s) * 3 + 1) * KK + r * KD + c;
+        st_dd(d.Ch, d.Cl, at,
+              dd_add(dd_add(k_at<KD>(d, e + r, e + c), ld_dd(d.Ch, d.Cl, at)),
+                     ld_dd(d.Ch, d.Cl, (static_cast<long long>(s + 1) * 3 + 0) * KK + r * KD + c)));
+      }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && P > 1 && !*bad) {  // block tridiagonal L D L' of S, one chain
     bool ok = true;
-    dd Dprev[KD][KD];
+    dd Dprev[KD][KD], An[KD][KD], Bn[KD][KD];
+#pragma unroll
+    for (int r = 0; r < KD; ++r)
+#pragma unroll
+      for (int c = 0; c < KD; ++c) {
+        An[r][c] = ld_dd(d.Ch, d.Cl, 1 * KK + r * KD + c);
+        Bn[r][c] = dd_from(0.0);
+      }
     for (int t = 0; t < P - 1; ++t) {
-      int lo, e, hi;
-      seg_range<KD>(t, P, n, lo, e, hi);
-      dd A[KD][KD];
+      dd A[KD][KD], B[KD][KD];
 #pragma unroll
       for (int r = 0; r < KD; ++r)
 #pragma unroll
-        for (int c = 0; c < KD; ++c)
-          A[r][c] = dd_add(dd_add(k_at<KD>(d, e + r, e + c), ld_dd(d.Ch, d.Cl, (static_cast<long long>(t) * 3 + 1) * KK + r * KD + c)),
-                           ld_dd(d.Ch, d.Cl, (static_cast<long long>(t + 1) * 3 + 0) * KK + r * KD + c));
-      if (t >= 1) {
-        dd B[KD][KD], L[KD][KD];
+        for (int c = 0; c < KD; ++c) {
+          A[r][c] = An[r][c];
+          B[r][c] = Bn[r][c];
+        }
+      if (t + 1 < P - 1)  // the next step's blocks, loaded while this one computes
 #pragma unroll
         for (int r = 0; r < KD; ++r)
 #pragma unroll
-          for (int c = 0; c < KD; ++c) B[r][c] = ld_dd(d.Ch, d.Cl, (static_cast<long long>(t) * 3 + 2) * KK + r * KD + c);
+          for (int c = 0; c < KD; ++c) {
+            An[r][c] = ld_dd(d.Ch, d.Cl, (static_cast<long long>(t + 1) * 3 + 1) * KK + r * KD + c);
+            Bn[r][c] = ld_dd(d.Ch, d.Cl, (static_cast<long long>(t + 1) * 3 + 2) * KK + r * KD + c);
+          }
+      if (t >= 1) {
+        dd L[KD][KD];
 #pragma unroll
         for (int r = 0; r < KD; ++r)
 #pragma unroll
@@ -336,50 +362,87 @@ __device__ void part_solve(const XbDev& d, double* xh, double* xl) {
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0 && P > 1) {
-    // forward: z_t = (r_St - contributions) - L_t z_{t-1}, kept in the separator slots of x
-    for (int t = 0; t < P - 1; ++t) {
+  // separators' right-hand sides less the interiors' contributions, in parallel
+  if (s < P - 1) {
+    int lo, e, hi;
+    seg_range<KD>(s, P, n, lo, e, hi);
+#pragma unroll
+    for (int r = 0; r < KD; ++r)
+      st_dd(xh, xl, e + r,
+            dd_sub(dd_sub(ld_dd(xh, xl, e + r), ld_dd(d.Rh, d.Rl, (static_cast<long long>(s) * 2 + 1) * KD + r)),
+                   ld_dd(d.Rh, d.Rl, (static_cast<long long>(s + 1) * 2 + 0) * KD + r)));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && P > 1) {  // forward chain z_t = r_t - L_t z_{t-1}, in the separator slots
+    dd z[KD], rn[KD], Ln[KD][KD];
+    {
+      int lo, e, hi;
+      seg_range<KD>(0, P, n, lo, e, hi);
+#pragma unroll
+      for (int r = 0; r < KD; ++r) z[r] = ld_dd(xh, xl, e + r);  // z_0 = r_0
+    }
+    for (int t = 1; t < P - 1; ++t) {
       int lo, e, hi;
       seg_range<KD>(t, P, n, lo, e, hi);
-      dd zp[KD];
-      if (t >= 1) {
-        int lo2, e2, hi2;
-        seg_range<KD>(t - 1, P, n, lo2, e2, hi2);
 #pragma unroll
-        for (int c = 0; c < KD; ++c) zp[c] = ld_dd(xh, xl, e2 + c);
+      for (int r = 0; r < KD; ++r) {
+        rn[r] = ld_dd(xh, xl, e + r);
+#pragma unroll
+        for (int c = 0; c < KD; ++c) Ln[r][c] = ld_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 0) * KK + r * KD + c);
+      }
+      dd zn[KD];
+#pragma unroll
+      for (int r = 0; r < KD; ++r) {
+        dd v = rn[r];
+#pragma unroll
+        for (int c = 0; c < KD; ++c) v = dd_sub(v, dd_mul(Ln[r][c], z[c]));
+        zn[r] = v;
       }
 #pragma unroll
       for (int r = 0; r < KD; ++r) {
-        dd v = dd_sub(dd_sub(ld_dd(xh, xl, e + r), ld_dd(d.Rh, d.Rl, (static_cast<long long>(t) * 2 + 1) * KD + r)),
-                      ld_dd(d.Rh, d.Rl, (static_cast<long long>(t + 1) * 2 + 0) * KD + r));
-        if (t >= 1)
-#pragma unroll
-          for (int c = 0; c < KD; ++c)
-            v = dd_sub(v, dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 0) * KK + r * KD + c), zp[c]));
-        st_dd(xh, xl, e + r, v);
+        z[r] = zn[r];
+        st_dd(xh, xl, e + r, zn[r]);
       }
     }
-    // w_t = D_t^-1 z_t, then backward x_t = w_t - L_{t+1}' x_{t+1}
+  }
+  __syncthreads();
+  if (s < P - 1) {  // w_t = D_t^-1 z_t, in parallel
+    int lo, e, hi;
+    seg_range<KD>(s, P, n, lo, e, hi);
+    dd z[KD];
+#pragma unroll
+    for (int c = 0; c < KD; ++c) z[c] = ld_dd(xh, xl, e + c);
+#pragma unroll
+    for (int r = 0; r < KD; ++r) {
+      dd v = dd_from(0.0);
+#pragma unroll
+      for (int c = 0; c < KD; ++c) v = dd_add(v, dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(s) * 2 + 1) * KK + r * KD + c), z[c]));
+      st_dd(xh, xl, e + r, v);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && P > 2) {  // backward chain x_t = w_t - L_{t+1}' x_{t+1}
     dd xn[KD];
-    for (int t = P - 2; t >= 0; --t) {
+    {
+      int lo, e, hi;
+      seg_range<KD>(P - 2, P, n, lo, e, hi);
+#pragma unroll
+      for (int r = 0; r < KD; ++r) xn[r] = ld_dd(xh, xl, e + r);
+    }
+    for (int t = P - 3; t >= 0; --t) {
       int lo, e, hi;
       seg_range<KD>(t, P, n, lo, e, hi);
-      dd z[KD], w[KD];
-#pragma unroll
-      for (int c = 0; c < KD; ++c) z[c] = ld_dd(xh, xl, e + c);
+      dd w[KD], Lt[KD][KD];
 #pragma unroll
       for (int r = 0; r < KD; ++r) {
-        dd v = dd_from(0.0);
+        w[r] = ld_dd(xh, xl, e + r);
 #pragma unroll
-        for (int c = 0; c < KD; ++c) v = dd_add(v, dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(t) * 2 + 1) * KK + r * KD + c), z[c]));
-        w[r] = v;
+        for (int c = 0; c < KD; ++c) Lt[r][c] = ld_dd(d.Th, d.Tl, (static_cast<long long>(t + 1) * 2 + 0) * KK + c * KD + r);
       }
-      if (t < P - 2)
 #pragma unroll
-        for (int r = 0; r < KD; ++r)
+      for (int r = 0; r < KD; ++r)
 #pragma unroll
-          for (int c = 0; c < KD; ++c)  // (L_{t+1}')[r][c] = L_{t+1}[c][r]
-            w[r] = dd_sub(w[r], dd_mul(ld_dd(d.Th, d.Tl, (static_cast<long long>(t + 1) * 2 + 0) * KK + c * KD + r), xn[c]));
+        for (int c = 0; c < KD; ++c) w[r] = dd_sub(w[r], dd_mul(Lt[r][c], xn[c]));
 #pragma unroll
       for (int r = 0; r < KD; ++r) {
         st_dd(xh, xl, e + r, w[r]);
