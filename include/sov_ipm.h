@@ -161,7 +161,8 @@ typedef struct sov_diagnostics {
   int32_t fp64_fallbacks;      /* mixed precision: iterations refactored in FP64 */
   int32_t pcg_iterations;      /* mixed precision: total PCG iterations */
   int32_t warm_start_used;     /* 1 when the supplied warm start was kept */
-  int32_t reserved;
+  int32_t structured_qp;       /* 1: the QP took the structured convex-sequence path; its dual map holds
+                                  the model's rows only (qp_interior_point.cpp:2198-2202) */
 } sov_diagnostics;
 
 /* Result of one solve (sovereign::SolverResult, types.hpp:117-155, in index form).

@@ -6,7 +6,8 @@
 // calls the GPU engine, and maps the answer back into a sovereign::SolverResult
 // (types.hpp:117-155) with the keys the reference's IPM publishes: primal and dual-slack values by
 // variable name, row multipliers as "row_<i>", dual_certificate_space "original_model" and
-// lp_diagnostics["ipm"] (solver/lp/src/interior_point.cpp:521-569).
+// lp_diagnostics["ipm"] (solver/lp/src/interior_point.cpp:521-569); for a QP, the keys of the
+// reference's QP-IPM (row multipliers of the upper-bound rows included, no certificate space).
 //
 // Drop-in use (solver/lp/src/lp_solver.cpp:59-62):
 //     auto run_ipm = [&]() {
@@ -135,9 +136,15 @@ inline IndexModel to_index(const OptimizationModel& model, bool qp) {
   return im;
 }
 
+// qp: the QP solver's result maps (qp_interior_point.cpp): the general QP-IPM publishes the dual
+// slack of every variable under its name and the multiplier of every IPM row -- the model's rows,
+// then one per finite upper bound -- as "row_<i>" (capture_diagnostics, :2862-2870), and sets no
+// certificate space; the structured path for the convex-sequence shape publishes the model's rows
+// only (:2198-2202). ipm_y: the final IPM multipliers (m_ipm), or empty.
 inline SolverResult to_result(const OptimizationModel& model, const sov_result& r, const std::vector<double>& x,
                               const std::vector<double>& dcol, const std::vector<double>& drow,
-                              const sov_diagnostics& dg) {
+                              const sov_diagnostics& dg, bool qp = false,
+                              const std::vector<double>& ipm_y = std::vector<double>()) {
   SolverResult out;
   out.status = static_cast<SolverStatus>(r.status);
   out.iterations = r.iterations;
@@ -149,12 +156,16 @@ inline SolverResult to_result(const OptimizationModel& model, const sov_result& 
   out.message = r.message;
   out.runtime_seconds = r.solve_seconds;
   if (out.has_objective_value) {
-    out.dual_certificate_space = "original_model";
+    if (!qp) out.dual_certificate_space = "original_model";
+    const bool structured = qp && dg.structured_qp;
     for (std::size_t j = 0; j < model.variables.size(); ++j) {
       out.primal[model.variables[j].name] = x[j];
-      out.dual[model.variables[j].name] = dcol[j];
+      if (!structured) out.dual[model.variables[j].name] = dcol[j];
     }
     for (std::size_t i = 0; i < model.constraints.size(); ++i) out.dual["row_" + std::to_string(i)] = drow[i];
+    if (qp && !structured)
+      for (std::size_t i = model.constraints.size(); i < ipm_y.size(); ++i)
+        out.dual["row_" + std::to_string(i)] = ipm_y[i];
   }
   LpDiagnostics& d = out.lp_diagnostics["ipm"];
   d.scaling_applied = dg.scaling_applied != 0;
@@ -190,7 +201,7 @@ inline SolverResult to_result(const OptimizationModel& model, const sov_result& 
 inline SolverResult solve(const OptimizationModel& model, bool qp, const sov_options* opt) {
   try {
     IndexModel im = to_index(model, qp);
-    std::vector<double> x(im.view.n), dcol(im.view.n), drow(im.view.m);
+    std::vector<double> x(im.view.n), dcol(im.view.n), drow(im.view.m), ipm_y;
     sov_diagnostics dg;
     std::memset(&dg, 0, sizeof(dg));
     sov_result r;
@@ -199,10 +210,16 @@ inline SolverResult solve(const OptimizationModel& model, bool qp, const sov_opt
     r.dual_col = dcol.data();
     r.dual_row = drow.data();
     r.diagnostics = &dg;
+    int32_t n_ipm = 0, m_ipm = 0;
+    if (qp && sov_ipm_dims(&im.view, 1, &n_ipm, &m_ipm) == SOV_OK && m_ipm > 0) {
+      ipm_y.assign(m_ipm, 0.0);
+      r.ipm_y = ipm_y.data();
+    }
     const int rc = qp ? sov_qp_solve(&im.view, opt, &r) : sov_lp_solve(&im.view, opt, &r);
     if (rc != SOV_OK && r.message[0] == '\0')
       std::snprintf(r.message, sizeof(r.message), "%s error: %s", qp ? "QP-IPM" : "IPM", sov_last_error());
-    return to_result(model, r, x, dcol, drow, dg);
+    if (r.m_ipm != m_ipm) ipm_y.clear();
+    return to_result(model, r, x, dcol, drow, dg, qp, ipm_y);
   } catch (const std::exception& ex) {
     // same convention as InteriorPointSolver::solve (interior_point.cpp:748-756)
     SolverResult r;

@@ -61,7 +61,7 @@ class SovDiagnostics(C.Structure):
         ("primal_step_history", C.c_double * HISTORY_MAX),
         ("dual_step_history", C.c_double * HISTORY_MAX),
         ("fp64_fallbacks", C.c_int32), ("pcg_iterations", C.c_int32),
-        ("warm_start_used", C.c_int32), ("reserved", C.c_int32),
+        ("warm_start_used", C.c_int32), ("structured_qp", C.c_int32),
     ]
 
 

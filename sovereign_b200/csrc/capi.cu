@@ -131,12 +131,6 @@ int solve_one(const sov_model* model, const sov_options* opt_in, sov_result* res
       std::snprintf(result->message, sizeof(result->message), "Optimal (no constraints) via IPM path.");
       return SOV_OK;
     }
-    if (qp) {
-      for (int j = 0; j < f.n; ++j)
-        if (f.free_col[j] && !(f.qdiag[j] > 0.0))
-          throw std::runtime_error("free variable x" + std::to_string(j) +
-                                   " has no curvature; the normal-equation QP path needs Q_jj > 0 for free columns");
-    }
     StreamGuard sg;
     sov::solve_single(*model, f, opt, result, sg.s, nullptr);
     return SOV_OK;

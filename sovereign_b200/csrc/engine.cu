@@ -12,6 +12,10 @@
 //   dense mixed   FP32 Cholesky as the preconditioner of FP64 PCG on the exact normal operator;
 //                 an iteration whose PCG does not converge is refactored in FP64
 //   band          banded LDL^T, natural order, for small half-bandwidths
+//   sparse        sparse LDL^T after a minimum-degree order, level-scheduled on the GPU
+// A QP whose Hessian couples variables takes its Newton step from y-space normal equations with a
+// dense H = Q + X^-1 S (up to kCoupledMaxColumns columns), or from the quasi-definite KKT system
+// [H + delta I, A'; A, -delta I] as a sparse LDL^T (kkt.cuh) -- the reference's QpKkt form.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -29,6 +33,7 @@
 #include "engine.hpp"
 #include "xband.hpp"
 #include "ipm_kernels.cuh"
+#include "kkt.cuh"
 #include "sparse.hpp"
 #include "sparse_gpu.cuh"
 
@@ -240,7 +245,9 @@ class Engine {
   IpmDev dev_{};
 
   // factorization
-  enum Backend { kDense64, kDenseMixed, kBand, kSparse } backend_ = kDense64;
+  enum Backend { kDense64, kDenseMixed, kBand, kSparse, kKkt } backend_ = kDense64;
+  // sparse quasi-definite KKT system of a coupled-Hessian QP (kKkt)
+  std::unique_ptr<KktSystem> kkt_;
   // sparse L D L' (kSparse): symbolic analysis on the host, numeric factor and solves on the GPU
   SparseSymbolic sym_;
   SparseFactor sparse_;
@@ -276,6 +283,10 @@ class Engine {
   static constexpr int kPcgSwitch = 12;
   static constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the default restart
   static constexpr int kCoupledMaxColumns = 16384;  // dense H of a coupled-Hessian QP: at most 2 GB
+  // automatic choice of the sparse KKT system for a coupled-Hessian QP: a KKT order of at least
+  // this and at most kKktSparseCoupling off-diagonal Q entries per column
+  static constexpr int kKktAutoOrder = 2048;
+  static constexpr int kKktSparseCoupling = 32;
   static constexpr int kDenseMaxOrder = 16384;      // dense normal matrix: at most 2 GB
   bool to_fp64_ = false;
   // x-space QP
@@ -341,13 +352,23 @@ void Engine::setup() {
                              "columns all have Q_jj > 0");
   xspace_ = opt_.factorization == SOV_FACTOR_XSPACE;
   coupled_ = f_.qp && !f_.q_diagonal;
+  // a free column without curvature (Q_jj no more than the 1e-14 every column carries) makes H^-1
+  // blow up in the normal equations; the KKT system takes it with the pivot Q_jj + delta
+  bool flat_free = false;
+  if (f_.qp)
+    for (int j = 0; j < n && !flat_free; ++j) flat_free = f_.free_col[j] && !(f_.qdiag[j] > 1e-12);
+  bool want_kkt = flat_free;
+  if (flat_free && opt_.factorization != SOV_FACTOR_AUTO && opt_.factorization != SOV_FACTOR_SPARSE)
+    throw std::runtime_error("a free variable without curvature (Q_jj = 0) needs the KKT system: factorization "
+                             "AUTO or SPARSE");
   if (coupled_) {
-    // the y-space system needs H^-1 of the coupled Hessian: dense H, FP64, no band / x-space
+    // the y-space system needs H^-1 of the coupled Hessian (dense H, FP64); the KKT system does not
     if (opt_.factorization == SOV_FACTOR_BANDED)
       throw std::runtime_error("banded factorization needs a separable Hessian; this QP couples variables in Q");
-    if (n > kCoupledMaxColumns)
-      throw std::runtime_error("coupled-Hessian QP with " + std::to_string(n) + " IPM columns exceeds the dense "
-                               "Hessian path's limit of " + std::to_string(kCoupledMaxColumns));
+    const long long q_off = static_cast<long long>(f_.q_idx.size()) - n;
+    want_kkt = want_kkt || opt_.factorization == SOV_FACTOR_SPARSE || n > kCoupledMaxColumns ||
+               (opt_.factorization == SOV_FACTOR_AUTO && n + m >= kKktAutoOrder &&
+                q_off <= static_cast<long long>(kKktSparseCoupling) * n);
   }
   order_ = xspace_ ? f_.n_struct : m;
   // backend choice: band when the half-bandwidth is small, else dense (mixed or FP64)
@@ -359,10 +380,12 @@ void Engine::setup() {
   const bool want_sparse = !want_band && !xspace_ && !coupled_ &&
                            (opt_.factorization == SOV_FACTOR_SPARSE ||
                             (opt_.factorization == SOV_FACTOR_AUTO && order_ > kDenseMaxOrder));
-  if (opt_.factorization == SOV_FACTOR_SPARSE && (xspace_ || coupled_))
-    throw std::runtime_error("the sparse factorization takes the y-space normal equations of an LP or a "
-                             "separable QP");
-  if (want_sparse) {
+  if (opt_.factorization == SOV_FACTOR_SPARSE && xspace_)
+    throw std::runtime_error("the sparse factorization takes the y-space normal equations or the KKT system, not "
+                             "the x-space system");
+  if (want_kkt) {
+    backend_ = kKkt;
+  } else if (want_sparse) {
     if (!sparse_analyze(f_, 0, sym_))
       throw std::runtime_error("sparse L D L' of the order-" + std::to_string(order_) +
                                " normal matrix needs more than " + std::to_string(kMaxUpdates) +
@@ -379,7 +402,10 @@ void Engine::setup() {
     // the x-space system has no matrix-free PCG operator: it is factored in FP64
     backend_ = (opt_.precision == SOV_PRECISION_MIXED && !xspace_ && !coupled_) ? kDenseMixed : kDense64;
   }
-  if (backend_ == kSparse) {
+  if (backend_ == kKkt) {
+    z_.alloc(std::max(1, m));
+    z_.zero(st_);
+  } else if (backend_ == kSparse) {
     std::vector<int64_t> tg(sym_.asm_target.begin(), sym_.asm_target.end());
     sp_target_.alloc(tg.size());
     sp_target_.upload(tg.data(), tg.size(), st_);
@@ -422,15 +448,20 @@ void Engine::setup() {
       pcg_h_ = static_cast<PcgScalars*>(g_pinned_slots.acquire());
     }
   }
-  if (coupled_) {
-    nbh_ = ceil_div(n, kNB);
-    nph_ = nbh_ * kNB;
+  if (coupled_ || backend_ == kKkt) {
     q_ptr_.alloc(n + 1);
     q_ptr_.upload(f_.q_ptr.data(), n + 1, st_);
     q_idx_.alloc(f_.q_idx.size());
     q_idx_.upload(f_.q_idx.data(), f_.q_idx.size(), st_);
     q_val_.alloc(f_.q_val.size());
     q_val_.upload(f_.q_val.data(), f_.q_val.size(), st_);
+  }
+  if (backend_ == kKkt) {
+    hvec_.alloc(n);
+    hvec_.zero(st_);
+  } else if (coupled_) {
+    nbh_ = ceil_div(n, kNB);
+    nph_ = nbh_ * kNB;
     // dense Q (column-major, both triangles) with the padding's diagonal 1
     std::vector<double> qd(static_cast<size_t>(nph_) * nph_, 0.0);
     for (int j = 0; j < n; ++j)
@@ -480,9 +511,14 @@ void Engine::setup() {
   } else {
     ds32_ = DenseSystem<float>{M32_.p, Linv32_.p, diag_.p, order_, mp_, nb_, drop_ptr, fail_ptr, flags_.p, flags_.p + nb_, 1e-6};
   }
-  if (coupled_)
+  if (backend_ == kKkt) {
+    kkt_ = std::make_unique<KktSystem>();
+    kkt_->build(f_, q_ptr_.p, q_idx_.p, q_val_.p, qdiag_.p, col_ptr_.p, row_idx_.p, cval_.p, row_ptr_.p, col_idx_.p,
+                rval_.p, free_.p, drop_ptr, fail_ptr, st_);
+  } else if (coupled_) {
     dsh_ = DenseSystem<double>{hmat_.p, hlinv_.p, hdiag_.p, n, nph_, nbh_, drop_ptr, fail_ptr, hflags_.p,
                                hflags_.p + nbh_, 1e-13};
+  }
 
   dev_.m = m;
   dev_.n = n;
@@ -541,6 +577,12 @@ void Engine::assemble_and_factor(int mode) {
   if (to_fp64_ && backend_ == kDenseMixed) backend_ = kDense64;
   // x-space: K = A_x' Theta A_x (+ diag Q + H after assembly); start system: Theta = 1, diag 1
   const int amode = xspace_ ? (mode == kWeightOnes ? kWeightOnes : kWeightTheta) : mode;
+  if (backend_ == kKkt) {
+    // a failure leaves the fail flag set: the iteration loop stops with the factorization error
+    kkt_->assemble_and_factor(mode == kWeightOnes, x_.p, s_.p, st_, &launches_);
+    if (stats_) stats_->factor_flops += kkt_->flops();
+    return;
+  }
   if (backend_ == kSparse) {
     SOV_CUDA(cudaMemsetAsync(sparse_.values(), 0, sizeof(double) * (order_ + sparse_.nnz_l()), st_));
     launch_assemble<double>(spd_, x_.p, s_.p, qdiag_.p, free_.p, mode, reg, sparse_.values(), sparse_.assembled_diag(),
@@ -657,6 +699,15 @@ void Engine::mehrotra_qp_start() {
 // One Newton pass of a coupled-Hessian QP: z = rp - A H^-1 r1, M dy = z, dx = H^-1 (r1 + A'dy),
 // then ds, the ratio tests and the step lengths as in the separable path.
 void Engine::coupled_newton(int mode) {
+  if (backend_ == kKkt) {
+    // K [dx; -dy] = [r1; rp] in one refined solve
+    if (stats_) stats_->solves++;
+    launch_hessian_r1(dev_, mode, hvec_.p, st_);
+    kkt_->solve_newton(hvec_.p, rp_.p, z_.p, st_, &launches_);
+    launch_direction_dx(dev_, mode, hvec_.p, st_, &launches_);
+    launches_ += 1;
+    return;
+  }
   launch_hessian_r1(dev_, mode, hvec_.p, st_);
   dense_solve<double>(dsh_, hvec_.p, epoch_, err_.p, st_, &launches_);
   launch_rows_minus(dev_, hvec_.p, rp_.p, st_);
@@ -675,6 +726,10 @@ bool Engine::newton_solve() {
   }
   if (backend_ == kSparse) {
     sparse_.solve(z_.p, st_, &launches_);
+    return true;
+  }
+  if (backend_ == kKkt) {
+    kkt_->solve_normal(z_.p, st_, &launches_);
     return true;
   }
   if (backend_ == kDense64) {
@@ -737,6 +792,15 @@ void Engine::read_scalars() {
 std::string Engine::describe() const {
   char buf[256];
   const char* space = xspace_ ? "x-space Q + A'ZW^-1A, " : "";
+  if (backend_ == kKkt) {
+    int len = std::snprintf(buf, sizeof buf,
+                            "sparse quasi-definite LDL^T on the GPU with minimum-degree ordering (order %d, nnz(L) = "
+                            "%lld, %d levels)",
+                            kkt_->order(), kkt_->nnz_l(), kkt_->levels());
+    if (kkt_->delta() > 1e-9 && len > 0 && len < static_cast<int>(sizeof buf))
+      std::snprintf(buf + len, sizeof buf - len, ", regularization raised to %g", kkt_->delta());
+    return buf;
+  }
   if (coupled_) {
     std::snprintf(buf, sizeof buf,
                   "A H^-1 A' with H = Q + X^-1 S dense, dense Cholesky on the GPU, FP64 (H %d x %d, %d x %d)", f_.n,
@@ -945,8 +1009,8 @@ void Engine::run(sov_result* r) {
     if (s.p_res < opt_.feasibility_tol && s.d_res < opt_.feasibility_tol && s.gap < opt_.optimality_tol) {
       SOV_CUDA(cudaEventRecord(e1, st_));
       const std::string msg =
-          f_.qp ? "Optimal convex QP found by Mehrotra predictor-corrector IPM. KKT system: normal equations, " +
-                      describe() + "."
+          f_.qp ? "Optimal convex QP found by Mehrotra predictor-corrector IPM. KKT system: " +
+                      std::string(backend_ == kKkt ? "" : "normal equations, ") + describe() + "."
                 : "Optimal solution found by primal-dual interior-point (Mehrotra). Normal equations: " + describe() +
                       ".";
       publish(x_, y_, s_, SOV_OPTIMAL, it + 1, s.gap, s.p_res, s.d_res, msg, r);
@@ -967,7 +1031,7 @@ void Engine::run(sov_result* r) {
     }
     assemble_and_factor(f_.qp ? kWeightQp : kWeightLp);
     for (int pass : {kRhsAffine, kRhsCorrector}) {
-      if (coupled_) {
+      if (coupled_ || backend_ == kKkt) {
         coupled_newton(pass);
         continue;
       }

@@ -157,6 +157,175 @@ bool minimum_degree(const std::vector<std::vector<int>>& graph, std::size_t fill
   return true;
 }
 
+// Nested dissection by level structures (A. George, J. W. H. Liu, "An automatic nested dissection
+// algorithm for irregular finite element problems", SIAM J. Numer. Anal. 15(5), 1978): a
+// connected part is split by one level of a breadth-first search from a pseudo-peripheral node --
+// the smallest level that leaves at least a quarter of the part on each side, cut down to the
+// nodes with a neighbour beyond it -- its two sides are ordered first and the separator last;
+// parts of at most kNdLeaf nodes, or whose search is too shallow to split, take the minimum-degree
+// order of their own subgraph. Dense rows (the same cut as minimum_degree) go last. Separators are
+// small and the tree is shallow wherever the graph is long and thin, where minimum degree walks
+// the graph from its ends and builds an elimination tree as deep as the graph is long.
+constexpr int kNdLeaf = 32;
+
+void nested_dissection(const std::vector<std::vector<int>>& graph, std::vector<int>& perm) {
+  const int n = static_cast<int>(graph.size());
+  perm.assign(n, -1);
+  const double dense_cut = std::max(16.0, 10.0 * std::sqrt(static_cast<double>(n)));
+  std::vector<int> part(n, 0);  // part id of each node; -1: ordered (separator, leaf or dense)
+  std::vector<std::pair<int, int>> held;
+  for (int i = 0; i < n; ++i)
+    if (static_cast<double>(graph[i].size()) > dense_cut) {
+      part[i] = -1;
+      held.push_back({static_cast<int>(graph[i].size()), i});
+    }
+  std::sort(held.begin(), held.end());
+  const int sparse_n = n - static_cast<int>(held.size());
+  for (std::size_t h = 0; h < held.size(); ++h) perm[sparse_n + static_cast<int>(h)] = held[h].second;
+  struct Task {
+    std::vector<int> nodes;
+    int lo;
+  };
+  std::vector<Task> stack;
+  {
+    Task t{{}, 0};
+    for (int i = 0; i < n; ++i)
+      if (part[i] == 0) t.nodes.push_back(i);
+    stack.push_back(std::move(t));
+  }
+  int next_id = 1;
+  std::vector<int> dist(n, -1), loc(n, -1), queue;
+  queue.reserve(n);
+  // breadth-first search from r inside part id; returns the nodes in visit order, dist set
+  auto bfs = [&](int r, int id, std::vector<int>& order) {
+    order.clear();
+    dist[r] = 0;
+    order.push_back(r);
+    for (std::size_t h = 0; h < order.size(); ++h) {
+      const int u = order[h];
+      for (int v : graph[u])
+        if (part[v] == id && dist[v] < 0) {
+          dist[v] = dist[u] + 1;
+          order.push_back(v);
+        }
+    }
+  };
+  auto leaf = [&](const std::vector<int>& nodes, int lo) {
+    const int k = static_cast<int>(nodes.size());
+    for (int q = 0; q < k; ++q) loc[nodes[q]] = q;
+    std::vector<std::vector<int>> sub(k);
+    for (int q = 0; q < k; ++q)
+      for (int v : graph[nodes[q]])
+        if (loc[v] >= 0 && part[v] == part[nodes[q]]) sub[q].push_back(loc[v]);
+    std::vector<int> sp;
+    minimum_degree(sub, 0, sp);
+    for (int q = 0; q < k; ++q) perm[lo + q] = nodes[sp[q]];
+    for (int v : nodes) {
+      loc[v] = -1;
+      part[v] = -1;
+    }
+  };
+  std::vector<int> order, order2;
+  while (!stack.empty()) {
+    Task t = std::move(stack.back());
+    stack.pop_back();
+    const int id = part[t.nodes[0]];
+    // components of the part, each with its own range
+    for (int v : t.nodes) dist[v] = -1;
+    std::vector<std::vector<int>> comps;
+    for (int v : t.nodes)
+      if (dist[v] < 0) {
+        bfs(v, id, order);
+        comps.push_back(order);
+      }
+    int lo = t.lo;
+    for (auto& comp : comps) {
+      const int k = static_cast<int>(comp.size());
+      const int cid = next_id++;
+      for (int v : comp) part[v] = cid;
+      if (k <= kNdLeaf) {
+        leaf(comp, lo);
+        lo += k;
+        continue;
+      }
+      // pseudo-peripheral node: restart from a sparsest node of the last level while the
+      // eccentricity grows
+      int r = comp[0];
+      for (int v : comp)
+        if (graph[v].size() < graph[r].size()) r = v;
+      for (int v : comp) dist[v] = -1;
+      bfs(r, cid, order);
+      int ecc = dist[order.back()];
+      for (int round = 0; round < 8; ++round) {
+        int cand = order.back();
+        for (auto it = order.rbegin(); it != order.rend() && dist[*it] == ecc; ++it)
+          if (graph[*it].size() < graph[cand].size()) cand = *it;
+        for (int v : comp) dist[v] = -1;
+        bfs(cand, cid, order2);
+        const int ecc2 = dist[order2.back()];
+        if (ecc2 <= ecc) {
+          for (int v : comp) dist[v] = -1;
+          bfs(r, cid, order);  // restore r's levels
+          break;
+        }
+        r = cand;
+        ecc = ecc2;
+        order.swap(order2);
+      }
+      if (ecc < 2) {  // too shallow to split
+        leaf(comp, lo);
+        lo += k;
+        continue;
+      }
+      std::vector<int> width(ecc + 1, 0);
+      for (int v : comp) width[dist[v]]++;
+      int best = -1, below = 0;
+      for (int l = 0; l <= ecc; ++l) {
+        const int above = k - below - width[l];
+        if (below >= k / 4 && above >= k / 4 && (best < 0 || width[l] < width[best])) best = l;
+        below += width[l];
+      }
+      if (best < 0) {  // no balanced level: the middle one
+        below = 0;
+        for (int l = 0; l <= ecc; ++l) {
+          if (below + width[l] >= k / 2) {
+            best = std::max(1, std::min(l, ecc - 1));
+            break;
+          }
+          below += width[l];
+        }
+      }
+      std::vector<int> sideA, sideB, sep;
+      for (int v : comp) {
+        if (dist[v] < best) {
+          sideA.push_back(v);
+        } else if (dist[v] > best) {
+          sideB.push_back(v);
+        } else {
+          bool beyond = false;
+          for (int u : graph[v])
+            if (part[u] == cid && dist[u] == best + 1) {
+              beyond = true;
+              break;
+            }
+          (beyond ? sep : sideA).push_back(v);
+        }
+      }
+      const int a = static_cast<int>(sideA.size()), b = static_cast<int>(sideB.size());
+      for (int q = 0; q < static_cast<int>(sep.size()); ++q) {
+        perm[lo + a + b + q] = sep[q];
+        part[sep[q]] = -1;
+      }
+      const int ida = next_id++, idb = next_id++;
+      for (int v : sideA) part[v] = ida;
+      for (int v : sideB) part[v] = idb;
+      if (a) stack.push_back(Task{std::move(sideA), lo});
+      if (b) stack.push_back(Task{std::move(sideB), lo + a});
+      lo += k;
+    }
+  }
+}
+
 int position(const SparseSymbolic& s, int col, int row) {
   const auto b = s.li.begin() + s.lp[col], e = s.li.begin() + s.lp[col + 1];
   const auto it = std::lower_bound(b, e, row);
@@ -165,58 +334,152 @@ int position(const SparseSymbolic& s, int col, int row) {
 
 }  // namespace
 
-bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& s) {
+int sparse_slot(const SparseSymbolic& s, int i, int j) {
+  const int a = s.iperm[i], b = s.iperm[j];
+  if (a == b) return a;
+  const int lo = std::min(a, b), hi = std::max(a, b);
+  const int p = position(s, lo, hi);
+  return p < 0 ? -1 : s.m + p;
+}
+
+bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& s, SparseOrder order) {
+  if (!sparse_analyze_graph(normal_graph(f), fill_limit, s, order)) return false;
   const int m = f.m;
-  s = SparseSymbolic{};
-  s.m = m;
-  const auto adj0 = normal_graph(f);
-  if (!minimum_degree(adj0, fill_limit, s.perm)) return false;
-  s.iperm.assign(m, 0);
-  for (int k = 0; k < m; ++k) s.iperm[s.perm[k]] = k;
-  // column patterns: col(k) = {i > k adjacent to k} U (col(c) \ {k}) over children c
-  std::vector<std::vector<int>> cols(m), children(m);
-  s.parent.assign(m, -1);
+  // assembly map into [D | L]: A's column j couples rows p >= q with weight a_p a_q
+  struct Contrib {
+    int t, col;
+    double w;
+  };
+  std::vector<Contrib> cs;
+  for (int j = 0; j < f.n; ++j)
+    for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p)
+      for (int q = f.col_ptr[j]; q <= p; ++q) {
+        const int i = s.iperm[f.row_idx[p]], k = s.iperm[f.row_idx[q]];
+        const int hi = std::max(i, k), lo = std::min(i, k);
+        const int t = hi == lo ? hi : m + position(s, lo, hi);
+        cs.push_back({t, j, f.val[p] * f.val[q]});
+      }
+  for (int i = 0; i < m; ++i) cs.push_back({i, -1, 0.0});  // every diagonal gets a target
+  std::stable_sort(cs.begin(), cs.end(), [](const Contrib& a, const Contrib& b) { return a.t < b.t; });
+  s.asm_ptr.push_back(0);
+  for (std::size_t q = 0; q < cs.size(); ++q) {
+    if (s.asm_target.empty() || s.asm_target.back() != cs[q].t) {
+      if (!s.asm_target.empty()) s.asm_ptr.push_back(static_cast<int>(s.asm_col.size()));
+      s.asm_target.push_back(cs[q].t);
+    }
+    if (cs[q].col >= 0) {
+      s.asm_col.push_back(cs[q].col);
+      s.asm_w.push_back(cs[q].w);
+    }
+  }
+  s.asm_ptr.push_back(static_cast<int>(s.asm_col.size()));
+  return true;
+}
+
+namespace {
+
+// Column patterns of L in the order perm: col(k) = {i > k adjacent to k} U (col(c) \ {k}) over the
+// children c of k; the elimination tree and each column's height in it. False when the entries of
+// L pass fill_limit (0 = no limit).
+struct Patterns {
+  std::vector<int> perm, iperm, parent, height;
+  std::vector<std::vector<int>> cols;
+  long long nnz_l = 0;
+  double flops = 0.0;
+  int hmax = 0;
+};
+
+bool column_patterns(const std::vector<std::vector<int>>& adj, std::vector<int> perm, std::size_t fill_limit,
+                     Patterns& P) {
+  const int m = static_cast<int>(adj.size());
+  P = Patterns{};
+  P.perm = std::move(perm);
+  P.iperm.assign(m, 0);
+  for (int k = 0; k < m; ++k) P.iperm[P.perm[k]] = k;
+  P.cols.assign(m, {});
+  std::vector<std::vector<int>> children(m);
+  P.parent.assign(m, -1);
+  P.height.assign(m, 0);
   std::vector<int> mark(m, -1);
   for (int k = 0; k < m; ++k) {
-    std::vector<int>& c = cols[k];
-    for (int r : adj0[s.perm[k]]) {
-      const int i = s.iperm[r];
+    std::vector<int>& c = P.cols[k];
+    for (int r : adj[P.perm[k]]) {
+      const int i = P.iperm[r];
       if (i > k && mark[i] != k) {
         mark[i] = k;
         c.push_back(i);
       }
     }
-    for (int ch : children[k])
-      for (int i : cols[ch])
+    for (int ch : children[k]) {
+      for (int i : P.cols[ch])
         if (i > k && mark[i] != k) {
           mark[i] = k;
           c.push_back(i);
         }
+      P.height[k] = std::max(P.height[k], P.height[ch] + 1);
+    }
+    P.hmax = std::max(P.hmax, P.height[k]);
     std::sort(c.begin(), c.end());
     if (!c.empty()) {
-      s.parent[k] = c.front();
+      P.parent[k] = c.front();
       children[c.front()].push_back(k);
     }
-    if (fill_limit > 0 && static_cast<std::size_t>(s.nnz_l) + c.size() > fill_limit) return false;
-    s.nnz_l += static_cast<long long>(c.size());
+    P.nnz_l += static_cast<long long>(c.size());
+    if (fill_limit > 0 && static_cast<std::size_t>(P.nnz_l) > fill_limit) return false;
+    const double cc = static_cast<double>(c.size());
+    P.flops += cc * cc;
   }
+  return true;
+}
+
+// Estimated GPU time of one factorization: every level costs its grid barriers, every rank-1
+// term its loads.
+double factor_cost(const Patterns& P) { return (P.hmax + 1) * 5e-6 + P.flops * 1e-11; }
+
+}  // namespace
+
+bool sparse_analyze_graph(const std::vector<std::vector<int>>& adj0, std::size_t fill_limit, SparseSymbolic& s,
+                          SparseOrder order) {
+  const int m = static_cast<int>(adj0.size());
+  s = SparseSymbolic{};
+  s.m = m;
+  Patterns P, Q;
+  bool have = false;
+  if (order != SparseOrder::kNestedDissection) {
+    std::vector<int> perm;
+    have = minimum_degree(adj0, fill_limit, perm) && column_patterns(adj0, std::move(perm), fill_limit, P);
+    s.ordering = SparseOrder::kMinimumDegree;
+  }
+  // nested dissection when asked for, or when the minimum-degree tree is deep enough for its
+  // barriers to dominate and the dissection order costs less
+  if (order == SparseOrder::kNestedDissection || (order == SparseOrder::kAuto && (!have || P.hmax >= 64))) {
+    std::vector<int> perm;
+    nested_dissection(adj0, perm);
+    const bool ok = column_patterns(adj0, std::move(perm), fill_limit, Q);
+    if (ok && (order == SparseOrder::kNestedDissection || !have || factor_cost(Q) < 0.8 * factor_cost(P))) {
+      P = std::move(Q);
+      have = true;
+      s.ordering = SparseOrder::kNestedDissection;
+    } else if (order == SparseOrder::kNestedDissection) {
+      return false;
+    }
+  }
+  if (!have) return false;
+  s.perm = std::move(P.perm);
+  s.iperm = std::move(P.iperm);
+  s.parent = std::move(P.parent);
+  s.nnz_l = P.nnz_l;
+  s.flops = P.flops;
+  std::vector<std::vector<int>>& cols = P.cols;
+  const std::vector<int>& height = P.height;
+  const int hmax = P.hmax;
   s.lp.assign(m + 1, 0);
   for (int k = 0; k < m; ++k) s.lp[k + 1] = s.lp[k] + static_cast<int>(cols[k].size());
   s.li.reserve(s.nnz_l);
-  for (int k = 0; k < m; ++k) {
-    s.li.insert(s.li.end(), cols[k].begin(), cols[k].end());
-    const double cc = static_cast<double>(cols[k].size());
-    s.flops += cc * cc;
-  }
+  for (int k = 0; k < m; ++k) s.li.insert(s.li.end(), cols[k].begin(), cols[k].end());
   // the update schedule below holds one entry per rank-1 term: bounded (3.2 GB at the limit)
   if (s.flops > 2.0 * kMaxUpdates) return false;
-  // heights and level schedule
-  std::vector<int> height(m, 0);
-  int hmax = 0;
-  for (int k = 0; k < m; ++k) {
-    for (int ch : children[k]) height[k] = std::max(height[k], height[ch] + 1);
-    hmax = std::max(hmax, height[k]);
-  }
+  // level schedule
   s.lvl_ptr.assign(hmax + 2, 0);
   for (int k = 0; k < m; ++k) s.lvl_ptr[height[k] + 1]++;
   for (int h = 0; h <= hmax; ++h) s.lvl_ptr[h + 1] += s.lvl_ptr[h];
@@ -266,34 +529,6 @@ bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& s)
     }
     for (std::thread& th : pool) th.join();
   }
-  // assembly map into [D | L]: A's column j couples rows p >= q with weight a_p a_q
-  struct Contrib {
-    int t, col;
-    double w;
-  };
-  std::vector<Contrib> cs;
-  for (int j = 0; j < f.n; ++j)
-    for (int p = f.col_ptr[j]; p < f.col_ptr[j + 1]; ++p)
-      for (int q = f.col_ptr[j]; q <= p; ++q) {
-        const int i = s.iperm[f.row_idx[p]], k = s.iperm[f.row_idx[q]];
-        const int hi = std::max(i, k), lo = std::min(i, k);
-        const int t = hi == lo ? hi : m + position(s, lo, hi);
-        cs.push_back({t, j, f.val[p] * f.val[q]});
-      }
-  for (int i = 0; i < m; ++i) cs.push_back({i, -1, 0.0});  // every diagonal gets a target
-  std::stable_sort(cs.begin(), cs.end(), [](const Contrib& a, const Contrib& b) { return a.t < b.t; });
-  s.asm_ptr.push_back(0);
-  for (std::size_t q = 0; q < cs.size(); ++q) {
-    if (s.asm_target.empty() || s.asm_target.back() != cs[q].t) {
-      if (!s.asm_target.empty()) s.asm_ptr.push_back(static_cast<int>(s.asm_col.size()));
-      s.asm_target.push_back(cs[q].t);
-    }
-    if (cs[q].col >= 0) {
-      s.asm_col.push_back(cs[q].col);
-      s.asm_w.push_back(cs[q].w);
-    }
-  }
-  s.asm_ptr.push_back(static_cast<int>(s.asm_col.size()));
   return true;
 }
 

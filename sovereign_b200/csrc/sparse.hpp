@@ -17,8 +17,14 @@
 
 namespace sov {
 
+// Fill-reducing order: approximate minimum degree, nested dissection, or (kAuto) minimum degree
+// unless its elimination tree is deep and the dissection order's estimated GPU factor time is
+// lower.
+enum class SparseOrder { kAuto, kMinimumDegree, kNestedDissection };
+
 struct SparseSymbolic {
   int m = 0;
+  SparseOrder ordering = SparseOrder::kMinimumDegree;  // the order taken
   std::vector<int> perm, iperm;  // perm[k] = row eliminated k-th; iperm[row] = k
   std::vector<int> lp, li;       // L (permuted): column k's strict-lower rows li[lp[k]..lp[k+1]), ascending
   std::vector<int> parent;       // elimination tree (permuted), -1 at roots
@@ -40,6 +46,16 @@ constexpr double kMaxUpdates = 2e8;
 
 // Returns false when the predicted fill exceeds fill_limit entries (0 = no limit) or the update
 // schedule would exceed kMaxUpdates terms.
-bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& out);
+bool sparse_analyze(const StdForm& f, std::size_t fill_limit, SparseSymbolic& out,
+                    SparseOrder order = SparseOrder::kAuto);
+
+// The same analysis for any symmetric pattern (adjacency lists without the diagonal, both
+// directions), without an assembly map: the caller places its values with sparse_slot.
+bool sparse_analyze_graph(const std::vector<std::vector<int>>& adj, std::size_t fill_limit, SparseSymbolic& out,
+                          SparseOrder order = SparseOrder::kAuto);
+
+// Index into the [D | L] value storage of entry (i, j) of the original ordering (-1 if it is not
+// in the pattern of L).
+int sparse_slot(const SparseSymbolic& s, int i, int j);
 
 }  // namespace sov

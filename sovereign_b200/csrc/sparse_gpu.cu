@@ -35,11 +35,12 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
     for (int q = s.lvl_ptr[h] + rank; q < s.lvl_ptr[h + 1]; q += size) {
       const int k = s.lvl_col[q];
       const double p = s.V[k];
+      const double sg = s.sign ? static_cast<double>(s.sign[k]) : 1.0;
       const bool finite = fabs(p) <= 1.7976931348623157e308;
-      const bool drop = !(finite && p > s.drop_tol * fabs(s.diag[k]));
+      const bool drop = !(finite && sg * p > s.drop_tol * fabs(s.diag[k]));
       bad |= !finite;
       drops += drop;
-      s.inv_d[k] = 1.0 / (drop ? 1e128 : p);
+      s.inv_d[k] = 1.0 / (drop ? sg * 1e128 : p);
     }
     g.sync();
     for (int r = s.run_lvl[h] + warp; r < s.run_lvl[h + 1]; r += warps) {
@@ -58,7 +59,8 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
 // L D L' x = z: forward y_k = z_k - sum_j L~_kj (1/D_j) y_j (row k of L, descendants: earlier
 // levels), backward x_k = (1/D_k) (y_k - sum_i L~_ik x_i) (column k, ancestors: later levels);
 // one warp per column, partial sums added in a fixed tree
-__global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, double* z) {
+__global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, double* z, const int* run) {
+  if (run && !*run) return;  // written by an earlier launch: every block takes the same exit
   cg::grid_group g = cg::this_grid();
   const int rank = static_cast<int>(g.thread_rank()), size = static_cast<int>(g.size());
   const int lane = threadIdx.x & 31, warp = rank >> 5, warps = size >> 5;
@@ -99,7 +101,8 @@ T* put(std::vector<void*>& bufs, const std::vector<T>& h, cudaStream_t st) {
 
 }  // namespace
 
-void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, double drop_tol, cudaStream_t st) {
+void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, double drop_tol, cudaStream_t st,
+                          const std::vector<int8_t>* sign) {
   release();
   const int m = s.m, levels = s.levels();
   nnz_l_ = s.nnz_l;
@@ -178,6 +181,13 @@ void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, d
   d_.drop_count = drop_count;
   d_.fail = fail;
   d_.drop_tol = drop_tol;
+  d_.sign = nullptr;
+  std::vector<int8_t> sign_elim;
+  if (sign) {
+    sign_elim.resize(m);
+    for (int k = 0; k < m; ++k) sign_elim[k] = (*sign)[s.perm[k]];
+    d_.sign = put(bufs_, sign_elim, st);
+  }
   SOV_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
   int dev = 0, sms = 0, per_sm = 0;
   SOV_CUDA(cudaGetDevice(&dev));
@@ -202,9 +212,9 @@ void SparseFactor::factor(cudaStream_t st, int* launches) {
   if (launches) *launches += 1;
 }
 
-void SparseFactor::solve(double* z, cudaStream_t st, int* launches) {
+void SparseFactor::solve(double* z, cudaStream_t st, int* launches, const int* run) {
   SparseDev d = d_;
-  void* args[] = {&d, &z};
+  void* args[] = {&d, &z, &run};
   SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_solve, dim3(grid_), dim3(kSparseThreads), args, 0, st));
   if (launches) *launches += 1;
 }

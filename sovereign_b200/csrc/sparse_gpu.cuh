@@ -8,11 +8,13 @@
 // (each destination's contributions summed by one warp in a fixed order: deterministic). One
 // cooperative launch per factorization and per solve, a grid barrier between levels.
 // Pivot rule of the reference's sparse LDL' (sparse_ldlt.cpp:165-173): a pivot at most
-// drop_tol * |assembled diagonal| (or not finite) marks a dependent row, D = 1e128.
+// drop_tol * |assembled diagonal| (or not finite) marks a dependent row, D = 1e128; with a sign
+// per pivot (quasi-definite systems) the test is sign * pivot, and a dropped pivot keeps its sign.
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <vector>
 
 #include "sparse.hpp"
@@ -42,12 +44,16 @@ struct SparseDev {
   int* drop_count;
   int* fail;
   double drop_tol;
+  const int8_t* sign;   // m (elimination order): the expected sign of each pivot, or null (all +1);
+                        // a quasi-definite KKT matrix has +1 on its primal block, -1 on its dual
 };
 
 // Device copies of the schedule; owns its buffers.
 class SparseFactor {
  public:
-  void upload(const SparseSymbolic& s, int* drop_count, int* fail, double drop_tol, cudaStream_t st);
+  // sign (optional, original ordering): the expected sign of each pivot (default all +1)
+  void upload(const SparseSymbolic& s, int* drop_count, int* fail, double drop_tol, cudaStream_t st,
+              const std::vector<int8_t>* sign = nullptr);
   void release();
   ~SparseFactor() { release(); }
   const SparseDev& dev() const { return d_; }
@@ -55,7 +61,8 @@ class SparseFactor {
   double* assembled_diag() const { return d_.diag; }
   long long nnz_l() const { return nnz_l_; }
   void factor(cudaStream_t st, int* launches);
-  void solve(double* z, cudaStream_t st, int* launches);  // z in the original row order, in place
+  // z in the original row order, in place; run (optional, device): the solve is skipped when *run == 0
+  void solve(double* z, cudaStream_t st, int* launches, const int* run = nullptr);
 
  private:
   SparseDev d_{};

@@ -920,6 +920,7 @@ int solve_xband(const sov_model& model, const XBandModel& xb, const sov_options&
     for (int i = 0; i < m; ++i) r->dual_row[i] = xb.row_sign[i] * z[i];
   if (sov_diagnostics* g = r->diagnostics) {
     std::memset(g, 0, sizeof(*g));
+    g->structured_qp = 1;
     g->refactorizations = o.iterations;
     g->history_len = o.history_len;
     for (int h = 0; h < o.history_len; ++h) {

@@ -43,7 +43,12 @@ class InteriorPointOptions:
         o.precision = self.precision
         o.pcg_max_iterations = self.pcg_max_iterations
         o.ipm_iterate_at = self.ipm_iterate_at
-        mode = os.environ.get("SOVEREIGN_IPM_NORMAL_EQUATIONS", "auto")  # interior_point.cpp:132-133
+        if qp:
+            # SOVEREIGN_QP_KKT (qp_interior_point.cpp:418-422): "sparse" takes the quasi-definite KKT
+            # system, "dense" a dense factorization of the engine's system
+            mode = os.environ.get("SOVEREIGN_QP_KKT", "auto")
+        else:
+            mode = os.environ.get("SOVEREIGN_IPM_NORMAL_EQUATIONS", "auto")  # interior_point.cpp:132-133
         o.factorization = {"dense": abi.FACTOR_DENSE, "banded": abi.FACTOR_BANDED,
                            "sparse": abi.FACTOR_SPARSE}.get(mode, abi.FACTOR_AUTO)
         return o
@@ -93,7 +98,8 @@ class InteriorPointSolver:
 
 
 class QpInteriorPointSolver:
-    """Convex-QP interior point (diagonal Hessian, normal equations) on the B200."""
+    """Convex-QP interior point on the B200: y-space normal equations for separable Hessians, a
+    dense H or the sparse quasi-definite KKT system for Hessians that couple variables."""
 
     def __init__(self, options: QpInteriorPointOptions | None = None):
         self.options = options or QpInteriorPointOptions()

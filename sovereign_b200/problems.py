@@ -14,6 +14,12 @@ the CPU oracles always see the same arrays):
 * ``multicommodity``       a fixed random graph with arc capacities and costs, K commodities,
                            coupling (capacity) rows plus per-commodity conservation rows; each
                            instance perturbs demands and costs.
+* ``coupled_chain_qp``     min sum_i w_i/2 (x_{i+1} - x_i)^2 + sum_i d_i/2 x_i^2 - t'x over
+                           0 <= x <= 2, a covering row per block of columns and one budget row:
+                           a Hessian that couples neighbours (tridiagonal), the sparse coupled
+                           shape that the quasi-definite KKT system takes at any size.
+* ``free_intercept_qp``    ridge regression with a free, unpenalised intercept and box-bounded
+                           coefficients: a free column without curvature.
 * ``reference_transport`` / ``reference_staircase`` / ``reference_portfolio``: the deterministic
                            models of the reference's own regression tests
                            (tests/unit/test_correctness_regressions.cpp:74-111,157-180,263-290).
@@ -384,6 +390,65 @@ def reference_portfolio(assets: int, sectors: int) -> Model:
     keys = sorted(q.keys(), key=lambda rc: (rc[1], rc[0]))
     qc = np.array([c for _, c in keys]); qr = np.array([r for r, _ in keys]); qv = np.array([q[k] for k in keys])
     mdl.q_col_ptr, mdl.q_row_idx, mdl.q_values = _csc_from_triplets(assets, qc, qr, qv)
+    return mdl
+
+
+def coupled_chain_qp(n: int, seed: int, block: int = 8) -> Model:
+    """min 1/2 sum_i w_i (x_{i+1} - x_i)^2 + 1/2 sum_i d_i x_i^2 - t'x, 0 <= x <= 2, with
+    w ~ 1 + U(0,1), d ~ 0.01 + 0.1 U(0,1), t ~ N(0,1); a covering row sum_j a_j x_j >= r_k over each
+    block of `block` consecutive columns (a ~ 0.5 + U(0,1), r ~ 0.2 block U(0,1)) and the budget
+    row sum_j x_j = n / 4. Strictly convex, so the primal optimum is unique."""
+    rng = np.random.default_rng(seed)
+    w = 1.0 + rng.random(n - 1)
+    d = 0.01 + 0.1 * rng.random(n)
+    t = rng.standard_normal(n)
+    a = 0.5 + rng.random(n)
+    nb = (n + block - 1) // block
+    r = 0.2 * block * rng.random(nb)
+    j = np.arange(n)
+    rows = np.concatenate([j // block, np.full(n, nb)])
+    cols = np.concatenate([j, j])
+    vals = np.concatenate([a, np.ones(n)])
+    col_ptr, row_idx, values = _csc_from_triplets(n, cols, rows, vals)
+    rhs = np.concatenate([r, [n / 4.0]])
+    sense = np.array([GE] * nb + [EQ], dtype=np.int8)
+    mdl = _lp(n, nb + 1, col_ptr, row_idx, values, -t, rhs, sense, f"coupled_chain_qp_{n}",
+              lb=np.zeros(n), ub=np.full(n, 2.0))
+    diag = d.copy()
+    diag[:-1] += w
+    diag[1:] += w
+    # stored terms: (j, j), and (j, j+1), (j+1, j) with -w_j each (the pair adds up to -w_j x_j x_{j+1})
+    qc = np.concatenate([j, j[:-1], j[1:]])
+    qr = np.concatenate([j, j[1:], j[:-1]])
+    qv = np.concatenate([diag, -w, -w])
+    mdl.q_col_ptr, mdl.q_row_idx, mdl.q_values = _csc_from_triplets(n, qc, qr, qv)
+    return mdl
+
+
+def free_intercept_qp(points: int, features: int, seed: int) -> Model:
+    """Ridge regression with a free intercept: min 1/2 ||r||^2 + lam/2 ||beta||^2 subject to
+    r_i + X_i beta + b0 = y_i, -1 <= beta_k <= 1, r and b0 free; X ~ N(0,1), y = X beta0 + 3 + noise,
+    lam = 0.1. The intercept b0 is free and carries no curvature: its column of the Hessian is zero."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((points, features))
+    beta0 = rng.uniform(-1.5, 1.5, features)
+    y = X @ beta0 + 3.0 + 0.1 * rng.standard_normal(points)
+    n = points + features + 1  # r, beta, b0
+    rows, cols, vals = [], [], []
+    i = np.arange(points)
+    rows.append(i); cols.append(i); vals.append(np.ones(points))
+    for k in range(features):
+        rows.append(i); cols.append(np.full(points, points + k)); vals.append(X[:, k])
+    rows.append(i); cols.append(np.full(points, n - 1)); vals.append(np.ones(points))
+    col_ptr, row_idx, values = _csc_from_triplets(n, np.concatenate(cols), np.concatenate(rows),
+                                                  np.concatenate(vals))
+    lb = np.concatenate([np.full(points, -INF), np.full(features, -1.0), [-INF]])
+    ub = np.concatenate([np.full(points, INF), np.full(features, 1.0), [INF]])
+    mdl = _lp(n, points, col_ptr, row_idx, values, np.zeros(n), y, np.full(points, EQ, dtype=np.int8),
+              f"free_intercept_qp_{points}x{features}", lb=lb, ub=ub)
+    jq = np.arange(points + features)
+    qv = np.concatenate([np.ones(points), np.full(features, 0.1)])
+    mdl.q_col_ptr, mdl.q_row_idx, mdl.q_values = _csc_from_triplets(n, jq, jq, qv)
     return mdl
 
 

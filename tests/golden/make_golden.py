@@ -23,6 +23,11 @@ Writes
                       extended precision, about three minutes) returns the objective and primal but
                       status ERROR, because its certifier measures a dual residual of 1.2e-7
   qp_reference.json   QpInteriorPointSolver results on the QP models below
+  kkt_reference.json  QpInteriorPointSolver results on QPs that take its sparse quasi-definite KKT
+                      path (qp_interior_point.cpp:415-655): the tridiagonal-Hessian coupled_chain_qp
+                      at n = 2000, 20000 and 200000 and the free-intercept regression QP (a free
+                      column without curvature); objective, status, iterations, the primal's sum
+                      and every KKT_STRIDE-th primal value
   liswet_n20000.npz   the reference's published LISWET projection at n = 20000
                       (benchmarks/reports/liswet_step6/n20000: input_c.txt, x.txt and the
                       objective printed in solver.stdout.json / independent.json)
@@ -57,6 +62,9 @@ BATCH_SPEC = dict(count=64, seed=3)          # transport_batch sample of the 409
 MULTICOMMODITY_SEEDS = [100, 101]            # MulticommodityFamily() instances
 QP_SPECS = [("small_qp_offdiagonal", []), ("convex_sequence_qp", [52, 3]), ("convex_sequence_qp", [202, 3]),
             ("convex_sequence_qp", [2002, 3]), ("reference_portfolio", [300, 12]), ("reference_portfolio", [60, 5])]
+KKT_SPECS = [("coupled_chain_qp", [2000, 1]), ("coupled_chain_qp", [20000, 2]), ("coupled_chain_qp", [200000, 5]),
+             ("free_intercept_qp", [400, 12, 3]), ("free_intercept_qp", [2000, 30, 4])]
+KKT_STRIDE = 97
 QP_RETRY_SPECS = [("reference_portfolio", [60, 5], 8), ("reference_portfolio", [60, 5], 5),
                   ("reference_portfolio", [300, 12], 10)]
 
@@ -117,6 +125,22 @@ def c2():
     print("c2", r.status_name, r.objective_value, r.solve_seconds, flush=True)
 
 
+def kkt():
+    """QPs on the reference's sparse quasi-definite KKT path."""
+    out = {}
+    for name, args in KKT_SPECS:
+        mdl = build(name, args)
+        r = oracle.solve(mdl, qp=True, kind="reference")
+        key = f"{name}({','.join(map(str, args))})"
+        d = summarize(r)
+        d["primal_stride"] = KKT_STRIDE
+        d["primal_sample"] = [float(v) for v in r.primal[::KKT_STRIDE]]
+        out[key] = dict(spec=[name, args], **d)
+        print("kkt", key, r.status_name, r.iterations, r.objective_value, flush=True)
+    with open(os.path.join(HERE, "kkt_reference.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def main(sections=()):
     oracle.build(reference=True)
     if "headline" in sections:
@@ -125,6 +149,8 @@ def main(sections=()):
         c1()
     if "c2" in sections:
         c2()
+    if "kkt" in sections:
+        kkt()
     if sections:
         return
     headline()
@@ -172,6 +198,7 @@ def main(sections=()):
         obj = float(ind["independent"]["objective_qp"])
         np.savez_compressed(os.path.join(HERE, "liswet_n20000.npz"), c=c, x=x, objective=obj)
         print("liswet", len(c), obj)
+    kkt()
     c1()
     c2()
 
