@@ -140,7 +140,8 @@ inline IndexModel to_index(const OptimizationModel& model, bool qp) {
 // slack of every variable under its name and the multiplier of every IPM row -- the model's rows,
 // then one per finite upper bound -- as "row_<i>" (capture_diagnostics, :2862-2870), and sets no
 // certificate space; the structured path for the convex-sequence shape publishes the model's rows
-// only (:2198-2202). ipm_y: the final IPM multipliers (m_ipm), or empty.
+// only (:2198-2202); neither records lp_diagnostics. ipm_y: the final IPM multipliers (m_ipm), or
+// empty.
 inline SolverResult to_result(const OptimizationModel& model, const sov_result& r, const std::vector<double>& x,
                               const std::vector<double>& dcol, const std::vector<double>& drow,
                               const sov_diagnostics& dg, bool qp = false,
@@ -167,6 +168,7 @@ inline SolverResult to_result(const OptimizationModel& model, const sov_result& 
       for (std::size_t i = model.constraints.size(); i < ipm_y.size(); ++i)
         out.dual["row_" + std::to_string(i)] = ipm_y[i];
   }
+  if (qp) return out;  // the QP solver records no lp_diagnostics
   LpDiagnostics& d = out.lp_diagnostics["ipm"];
   d.scaling_applied = dg.scaling_applied != 0;
   d.coefficient_min_abs_before = dg.coefficient_min_abs_before;

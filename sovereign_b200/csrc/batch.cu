@@ -739,8 +739,15 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   __syncthreads();
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT <= 256 ? 2 : 1)) k_batch_ipm(BatchDev bd, int mmax) {
+// Kernel shapes: the CTA width NT and the CTAs per SM its register budget is sized for. The plain
+// shapes get 128 registers per thread (4 x 128, 2 x 256, 1 x 512 threads per SM); the lean ones
+// are capped at 80 registers (6 x 128, 3 x 256 per SM), which spills a little but keeps more LPs
+// resident to cover each other's barrier waits. A shape code is the width, plus 1 for lean.
+constexpr int min_ctas(int nt, bool lean) { return lean ? (nt <= 128 ? 6 : 3) : (nt <= 128 ? 4 : nt <= 256 ? 2 : 1); }
+constexpr int kShapes[] = {128, 129, 256, 257, 512};
+
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_batch_ipm(BatchDev bd, int mmax) {
   extern __shared__ double sm[];
   __shared__ double red[4 * 32];
   __shared__ CtaScalars cs;
@@ -762,24 +769,26 @@ size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(m
 // footprint, so launches (and launches captured in a graph) need no per-launch attribute call.
 void ensure_smem_limits() {
   const int smem = static_cast<int>(batch_smem(kBatchMaxRows));
-  once_per_device((const void*)k_batch_ipm<128>, [&] {
-    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  once_per_device((const void*)k_batch_ipm<128, min_ctas(128, false)>, [&] {
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<128, min_ctas(128, false)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<128, min_ctas(128, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<256, min_ctas(256, false)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<256, min_ctas(256, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SOV_CUDA(cudaFuncSetAttribute(k_batch_ipm<512, min_ctas(512, false)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   });
 }
 
-template <int NT>
+template <int NT, bool LEAN>
 void launch_bucket(const BatchDev& bd, int mmax, int grid, cudaStream_t st) {
-  k_batch_ipm<NT><<<grid, NT, batch_smem(mmax), st>>>(bd, mmax);
+  k_batch_ipm<NT, min_ctas(NT, LEAN)><<<grid, NT, batch_smem(mmax), st>>>(bd, mmax);
   SOV_LAUNCH_CHECK();
 }
 
-template <int NT>
+template <int NT, bool LEAN>
 int max_ctas(int mmax) {
   int per_sm = 0;
   const size_t smem = batch_smem(mmax);
-  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_ipm<NT>, NT, smem));
+  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_ipm<NT, min_ctas(NT, LEAN)>, NT, smem));
   int dev = 0, sms = 0;
   SOV_CUDA(cudaGetDevice(&dev));
   SOV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -936,7 +945,7 @@ struct PinnedArena {
 PinnedArena g_arena;
 
 std::mutex g_tune_mu;
-std::map<int, int> g_tuned_threads;  // bucket mmax -> threads
+std::map<int, int> g_tuned_threads;  // bucket mmax -> kernel shape code
 
 int bucket_of(int m) { return std::max(32, ((m + 31) / 32) * 32); }
 
@@ -1351,10 +1360,12 @@ __global__ void __launch_bounds__(kScaleThreads) k_batch_publish(const LpMeta* _
 }
 
 int threads_for(int mmax) {
-  // SOVEREIGN_BATCH_THREADS=128|256|512 pins every bucket (tests run each width this way)
+  // SOVEREIGN_BATCH_THREADS=128|129|256|257|512 pins every bucket to a shape (tests run each one
+  // this way; odd codes are the lean shapes)
   if (const char* e = std::getenv("SOVEREIGN_BATCH_THREADS")) {
     const int t = std::atoi(e);
-    if (t == 128 || t == 256 || t == 512) return t;
+    for (int code : kShapes)
+      if (t == code) return t;
   }
   std::lock_guard<std::mutex> g(g_tune_mu);
   auto it = g_tuned_threads.find(mmax);
@@ -1363,14 +1374,25 @@ int threads_for(int mmax) {
   return 128;  // measured best on average without tuning (4 CTAs of 128 per SM)
 }
 
-void launch_any(const BatchDev& bd, int mmax, int threads, int grid, cudaStream_t st) {
-  if (threads == 128) launch_bucket<128>(bd, mmax, grid, st);
-  else if (threads == 512) launch_bucket<512>(bd, mmax, grid, st);
-  else launch_bucket<256>(bd, mmax, grid, st);
+void launch_any(const BatchDev& bd, int mmax, int code, int grid, cudaStream_t st) {
+  switch (code) {
+    case 128: launch_bucket<128, false>(bd, mmax, grid, st); break;
+    case 129: launch_bucket<128, true>(bd, mmax, grid, st); break;
+    case 257: launch_bucket<256, true>(bd, mmax, grid, st); break;
+    case 512: launch_bucket<512, false>(bd, mmax, grid, st); break;
+    default: launch_bucket<256, false>(bd, mmax, grid, st); break;
+  }
 }
 
-int grid_for(int mmax, int threads, int count) {
-  const int cap = threads == 128 ? max_ctas<128>(mmax) : threads == 512 ? max_ctas<512>(mmax) : max_ctas<256>(mmax);
+int grid_for(int mmax, int code, int count) {
+  int cap;
+  switch (code) {
+    case 128: cap = max_ctas<128, false>(mmax); break;
+    case 129: cap = max_ctas<128, true>(mmax); break;
+    case 257: cap = max_ctas<256, true>(mmax); break;
+    case 512: cap = max_ctas<512, false>(mmax); break;
+    default: cap = max_ctas<256, false>(mmax); break;
+  }
   return std::max(1, std::min(cap, count));
 }
 
@@ -2009,7 +2031,8 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
 }
 
 std::string autotune(int count, const sov_model* models, const sov_options* opt, const std::string& file) {
-  // Per bucket: time the bucket alone with 128 / 256 / 512 threads per CTA and take the fastest.
+  // Per bucket: time the bucket alone with every kernel shape (128 / 256 / 512 threads per CTA, and
+  // the lean 128 / 256) and take the fastest.
   std::unique_ptr<Batch> B(batch_create(count, models, opt));
   SOV_CUDA(cudaEventSynchronize(B->ready));
   cudaStream_t st;
@@ -2022,7 +2045,7 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
     int best_t = bk->threads;
     std::ostringstream part;
     bool f2 = true;
-    for (int threads : {128, 256, 512}) {
+    for (int threads : kShapes) {
       const int grid = grid_for(bk->mmax, threads, bk->count);
       BatchDev d = B->dev;
       d.order = bk->order;
@@ -2071,7 +2094,7 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
   float cur = step_ms();
   for (auto& bk : B->buckets) {
     const int first_t = bk->threads;
-    for (int threads : {128, 256, 512}) {
+    for (int threads : kShapes) {
       if (threads == first_t) continue;
       const int old_t = bk->threads, old_g = bk->grid;
       bk->threads = threads;

@@ -289,11 +289,16 @@ class Engine {
   static constexpr int kKktSparseCoupling = 32;
   static constexpr int kDenseMaxOrder = 16384;      // dense normal matrix: at most 2 GB
   bool to_fp64_ = false;
+  bool sparse_refused_ = false;  // the sparse factor was asked for but is nearly dense: dense instead
   // x-space QP
   XSpace xs_;
   bool xspace_ = false;
   int order_ = 0;  // order of the factored system: m (y-space) or structural columns (x-space)
   DevBuf<int> slack_of_row_;
+  DevBuf<double> coltmp_;
+  DevBuf<int> row_piece_, row_comb_;
+  DevBuf<double> row_partial_;
+  static constexpr int kLongRow = 512;
   DevBuf<double> sigma_, tr_, dyv_;
   // QP with a coupled Hessian: dense H = Q + diag(h) (order n, padded to nph_), its factor, and
   // Y = H^-1 A' for the reduced system M = A H^-1 A'
@@ -383,13 +388,19 @@ void Engine::setup() {
   if (opt_.factorization == SOV_FACTOR_SPARSE && xspace_)
     throw std::runtime_error("the sparse factorization takes the y-space normal equations or the KKT system, not "
                              "the x-space system");
-  if (want_kkt) {
-    backend_ = kKkt;
-  } else if (want_sparse) {
-    if (!sparse_analyze(f_, 0, sym_))
+  // a normal matrix whose sparse factor would need more rank-1 terms than the update schedule
+  // holds is nearly dense: it is factored densely when it fits
+  bool sparse_ok = want_sparse && sparse_analyze(f_, 0, sym_);
+  if (want_sparse && !sparse_ok) {
+    if (order_ > kDenseMaxOrder)
       throw std::runtime_error("sparse L D L' of the order-" + std::to_string(order_) +
                                " normal matrix needs more than " + std::to_string(kMaxUpdates) +
                                " rank-1 update terms");
+    sparse_refused_ = true;
+  }
+  if (want_kkt) {
+    backend_ = kKkt;
+  } else if (sparse_ok) {
     backend_ = kSparse;
   } else if (want_band) {
     if (kd_ > kBandMax) throw std::runtime_error("banded factorization requested but half-bandwidth " +
@@ -565,6 +576,31 @@ void Engine::setup() {
   dev_.sigma = sigma_.p;
   dev_.tr = tr_.p;
   dev_.sc = sc_.p;
+  // rows of at least kLongRow entries on average: a CTA per row, column terms computed once; a
+  // row longer than a piece: the row kernels walk pieces
+  if (!xspace_ && m > 0 && static_cast<long long>(f_.nnz()) >= static_cast<long long>(kLongRow) * m) {
+    dev_.row_block = 1;
+    coltmp_.alloc(n);
+    dev_.coltmp = coltmp_.p;
+  }
+  int longest = 0;
+  for (int i = 0; i < m; ++i) longest = std::max(longest, f_.row_ptr[i + 1] - f_.row_ptr[i]);
+  if (!xspace_ && longest > kSparsePiece && dev_.row_block == 0) {
+    int slots = 0;
+    const SparsePieces rp = row_pieces(f_.row_ptr, &slots);
+    static_assert(sizeof(SparsePiece) == sizeof(int4) && sizeof(SparseCombine) == sizeof(int4), "piece layout");
+    row_piece_.alloc(4 * rp.piece.size());
+    row_piece_.upload(reinterpret_cast<const int*>(rp.piece.data()), 4 * rp.piece.size(), st_);
+    row_comb_.alloc(4 * rp.comb.size());
+    row_comb_.upload(reinterpret_cast<const int*>(rp.comb.data()), 4 * rp.comb.size(), st_);
+    row_partial_.alloc(std::max(1, slots));
+    dev_.row_piece = reinterpret_cast<const int4*>(row_piece_.p);
+    dev_.row_pieces = static_cast<int>(rp.piece.size());
+    dev_.row_comb = reinterpret_cast<const int4*>(row_comb_.p);
+    dev_.row_combs = static_cast<int>(rp.comb.size());
+    dev_.row_partial = row_partial_.p;
+    SOV_CUDA(cudaStreamSynchronize(st_));  // rp goes out of scope
+  }
   dev_.partials = partials_.p;
   dev_.counter = counter_.p;
 }
@@ -794,9 +830,8 @@ std::string Engine::describe() const {
   const char* space = xspace_ ? "x-space Q + A'ZW^-1A, " : "";
   if (backend_ == kKkt) {
     int len = std::snprintf(buf, sizeof buf,
-                            "sparse quasi-definite LDL^T on the GPU with minimum-degree ordering (order %d, nnz(L) = "
-                            "%lld, %d levels)",
-                            kkt_->order(), kkt_->nnz_l(), kkt_->levels());
+                            "sparse quasi-definite LDL^T on the GPU with %s ordering (order %d, nnz(L) = %lld, %d levels)",
+                            kkt_->ordering(), kkt_->order(), kkt_->nnz_l(), kkt_->levels());
     if (kkt_->delta() > 1e-9 && len > 0 && len < static_cast<int>(sizeof buf))
       std::snprintf(buf + len, sizeof buf - len, ", regularization raised to %g", kkt_->delta());
     return buf;
@@ -808,12 +843,14 @@ std::string Engine::describe() const {
     return buf;
   }
   if (backend_ == kSparse)
-    std::snprintf(buf, sizeof buf, "sparse LDL^T on the GPU with minimum-degree ordering (order %d, nnz(L) = %lld, %d levels)",
-                  order_, sym_.nnz_l, sym_.levels());
+    std::snprintf(buf, sizeof buf, "sparse LDL^T on the GPU with %s ordering (order %d, nnz(L) = %lld, %d levels)",
+                  sym_.ordering == SparseOrder::kNestedDissection ? "nested-dissection" : "minimum-degree", order_,
+                  sym_.nnz_l, sym_.levels());
   else if (backend_ == kBand)
     std::snprintf(buf, sizeof buf, "%sbanded LDL^T on the GPU (order %d, half-bandwidth %d)", space, order_, kd_);
   else if (backend_ == kDense64)
-    std::snprintf(buf, sizeof buf, "%sdense Cholesky on the GPU, FP64 (%d x %d)", space, order_, order_);
+    std::snprintf(buf, sizeof buf, "%sdense Cholesky on the GPU, FP64 (%d x %d)%s", space, order_, order_,
+                  sparse_refused_ ? "; the sparse factor would be nearly dense" : "");
   else
     std::snprintf(buf, sizeof buf,
                   "dense Cholesky on the GPU, FP32 preconditioned FP64 PCG (%d x %d, %d PCG iterations, %d FP64 "

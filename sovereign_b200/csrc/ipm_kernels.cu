@@ -85,29 +85,119 @@ int blocks_for(int n) { return std::max(1, std::min(kMaxBlocks, ceil_div(n, kThr
 // sum_j a_ij v_j over row i, one warp per row
 __device__ __forceinline__ int warp_row() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 
-// ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_residual_rows(IpmDev d) {
+// sum over p = first, first + stride, ... < end of term(p), accumulated in that order, four terms'
+// loads issued before their products are added (the dependent gathers of several entries overlap)
+template <class Term>
+__device__ __forceinline__ double strided_sum(int first, int end, int stride, Term term) {
+  double acc = 0.0;
+  int p = first;
+  for (; p + 3 * stride < end; p += 4 * stride) {
+    const double t0 = term(p), t1 = term(p + stride), t2 = term(p + 2 * stride), t3 = term(p + 3 * stride);
+    acc += t0;
+    acc += t1;
+    acc += t2;
+    acc += t3;
+  }
+  for (; p < end; p += stride) acc += term(p);
+  return acc;
+}
+
+// sum_p a_pj v[row_p] over column j, in entry order
+__device__ __forceinline__ double col_dot(const IpmDev& d, int j, const double* v) {
+  return strided_sum(d.col_ptr[j], d.col_ptr[j + 1], 1, [&](int p) { return d.cval[p] * v[d.row_idx[p]]; });
+}
+
+// Row sums sum_p term(p) over the entries of each row, handed to out(i, sum) on one thread: a warp
+// per row; for long rows on average (d.row_block), the whole CTA per row so that enough loads are
+// in flight to stream A from HBM; when some row is longer than a piece (d.row_piece: a dense row),
+// a warp per piece -- rows cut into pieces leave their piece sums in d.row_partial for the
+// kernel's combine launch (for_each_cut_row). Partial sums are added in a fixed order throughout.
+template <class Term, class Out>
+__device__ __forceinline__ void for_each_row(const IpmDev& d, Term term, Out out) {
+  if (d.row_piece) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int q = warp_row(); q < d.row_pieces; q += warps) {
+      const int4 pc = d.row_piece[q];
+      double acc = strided_sum(pc.x + lane, pc.y, 32, term);
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        if (pc.w < 0) out(pc.z, acc);
+        else d.row_partial[pc.w] = acc;
+      }
+    }
+    return;
+  }
+  if (d.row_block) {
+    __shared__ double part[kThreads / 32];
+    for (int i = blockIdx.x; i < d.m; i += gridDim.x) {  // uniform over the CTA: barriers are safe
+      double acc = strided_sum(d.row_ptr[i] + threadIdx.x, d.row_ptr[i + 1], blockDim.x, term);
+      acc = warp_sum(acc);
+      if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += part[w];
+        out(i, t);
+      }
+      __syncthreads();
+    }
+    return;
+  }
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
-  double mx = 0.0;
   for (int i = warp_row(); i < d.m; i += warps) {
-    double acc = 0.0;
-    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * d.x[d.col_idx[p]];
+    double acc = strided_sum(d.row_ptr[i] + lane, d.row_ptr[i + 1], 32, term);
     acc = warp_sum(acc);
-    const double r = d.b[i] - acc;
-    if (lane == 0) d.rp[i] = r;
-    mx = fmax(mx, fabs(r));
+    if (lane == 0) out(i, acc);
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The rows that for_each_row cut into pieces: their piece sums added in order, handed to out.
+template <class Out>
+__device__ __forceinline__ void for_each_cut_row(const IpmDev& d, Out out) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.row_combs; c += gridDim.x * blockDim.x) {
+    const int4 cb = d.row_comb[c];
+    double acc = 0.0;
+    for (int k = 0; k < cb.z; ++k) acc += d.row_partial[cb.y + k];
+    out(cb.x, acc);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_residual_rows(IpmDev d) {
+  double mx = 0.0;
+  for_each_row(
+      d, [&](int p) { return d.rval[p] * d.x[d.col_idx[p]]; },
+      [&](int i, double acc) {
+        const double r = d.b[i] - acc;
+        d.rp[i] = r;
+        mx = fmax(mx, fabs(r));
+      });
   double v[1] = {mx};
   const int ops[1] = {1};
   if (grid_reduce<1>(v, ops, d.partials, d.counter) && threadIdx.x == 0) d.sc->rp_max = v[0];
 }
 
+// one CTA: the cut rows' residuals, and their maximum folded into sc->rp_max
+__global__ void __launch_bounds__(kThreads) k_residual_rows_cut(IpmDev d) {
+  __shared__ double red[4 * 32];
+  double mx = 0.0;
+  for_each_cut_row(d, [&](int i, double acc) {
+    const double r = d.b[i] - acc;
+    d.rp[i] = r;
+    mx = fmax(mx, fabs(r));
+  });
+  double v[1] = {mx};
+  const int ops[1] = {1};
+  block_reduce<1>(v, ops, red);
+  if (threadIdx.x == 0) d.sc->rp_max = fmax(d.sc->rp_max, v[0]);
+}
+
 __global__ void __launch_bounds__(kThreads) k_residual_cols(IpmDev d) {
   double rdm = 0.0, xs = 0.0, cx = 0.0, xqx = 0.0, qxm = 0.0;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
-    double aty = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) aty += d.cval[p] * d.y[d.row_idx[p]];
+    const double aty = col_dot(d, j, d.y);
     const double xj = d.x[j], sj = d.s[j];
     double qx = 0.0;
     if (d.qp) {
@@ -170,16 +260,22 @@ __device__ __forceinline__ double newton_tmp(const IpmDev& d, int mode, int j, d
 }
 
 __global__ void __launch_bounds__(kThreads) k_newton_rhs(IpmDev d, int mode) {
-  const int lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
   const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
-  for (int i = warp_row(); i < d.m; i += warps) {
-    double acc = 0.0;
-    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32)
-      acc += d.rval[p] * newton_tmp(d, mode, d.col_idx[p], sigma_mu);
-    acc = warp_sum(acc);
-    if (lane == 0) d.z[i] = d.rp[i] + acc;
-  }
+  auto out = [&](int i, double acc) { d.z[i] = d.rp[i] + acc; };
+  if (d.coltmp)  // tmp_j computed once per column by k_newton_tmp
+    for_each_row(d, [&](int p) { return d.rval[p] * d.coltmp[d.col_idx[p]]; }, out);
+  else
+    for_each_row(d, [&](int p) { return d.rval[p] * newton_tmp(d, mode, d.col_idx[p], sigma_mu); }, out);
+}
+
+__global__ void __launch_bounds__(kThreads) k_newton_rhs_cut(IpmDev d) {
+  for_each_cut_row(d, [&](int i, double acc) { d.z[i] = d.rp[i] + acc; });
+}
+
+__global__ void __launch_bounds__(kThreads) k_newton_tmp(IpmDev d, int mode) {
+  const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x)
+    d.coltmp[j] = newton_tmp(d, mode, j, sigma_mu);
 }
 
 __global__ void __launch_bounds__(kThreads) k_direction(IpmDev d, int mode, const double* dxv) {
@@ -188,8 +284,7 @@ __global__ void __launch_bounds__(kThreads) k_direction(IpmDev d, int mode, cons
   double* ds = mode == kRhsAffine ? d.dsa : d.ds;
   double rp_min = 1.0, rd_min = 1.0;  // step_to_bound starts at alpha = 1
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
-    double atdy = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+    const double atdy = col_dot(d, j, d.z);
     const double xj = d.x[j], sj = d.s[j];
     const double rxs = rxs_of(d, mode, j, sigma_mu);
     double dxj, dsj;
@@ -277,14 +372,11 @@ __global__ void __launch_bounds__(kThreads) k_update(IpmDev d) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_start_rhs(IpmDev d) {
-  const int lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int i = warp_row(); i < d.m; i += warps) {
-    double acc = 0.0;
-    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p];
-    acc = warp_sum(acc);
-    if (lane == 0) d.z[i] = d.b[i] - acc;
-  }
+  for_each_row(d, [&](int p) { return d.rval[p]; }, [&](int i, double acc) { d.z[i] = d.b[i] - acc; });
+}
+
+__global__ void __launch_bounds__(kThreads) k_start_rhs_cut(IpmDev d) {
+  for_each_cut_row(d, [&](int i, double acc) { d.z[i] = d.b[i] - acc; });
 }
 
 __global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
@@ -294,8 +386,7 @@ __global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
     if (j < d.n) {
       double x = 1.0, s = 1.0;
       if (ok) {
-        double atdy = 0.0;
-        for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.dy[d.row_idx[p]];
+        const double atdy = col_dot(d, j, d.dy);
         if (!d.qp) {
           x = fmax(1.0, fabs(atdy));
           s = fmax(1.0, fabs(d.c[j] - atdy));
@@ -321,8 +412,7 @@ __global__ void __launch_bounds__(kThreads) k_start_point(IpmDev d) {
 
 __global__ void __launch_bounds__(kThreads) k_normal_cols(IpmDev d, const double* v, double* tmp) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
-    double a = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) a += d.cval[p] * v[d.row_idx[p]];
+    const double a = col_dot(d, j, v);
     const double xj = fmax(d.x[j], 1e-16), sj = fmax(d.s[j], 1e-16);
     double w;
     if (d.start_system) w = 1.0;
@@ -334,14 +424,12 @@ __global__ void __launch_bounds__(kThreads) k_normal_cols(IpmDev d, const double
 
 __global__ void __launch_bounds__(kThreads) k_normal_rows(IpmDev d, const double* v, const double* tmp, double* out,
                                                           double reg) {
-  const int lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int i = warp_row(); i < d.m; i += warps) {
-    double acc = 0.0;
-    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * tmp[d.col_idx[p]];
-    acc = warp_sum(acc);
-    if (lane == 0) out[i] = acc + reg * v[i];
-  }
+  for_each_row(
+      d, [&](int p) { return d.rval[p] * tmp[d.col_idx[p]]; }, [&](int i, double acc) { out[i] = acc + reg * v[i]; });
+}
+
+__global__ void __launch_bounds__(kThreads) k_normal_rows_cut(IpmDev d, const double* v, double* out, double reg) {
+  for_each_cut_row(d, [&](int i, double acc) { out[i] = acc + reg * v[i]; });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -369,8 +457,7 @@ __global__ void __launch_bounds__(kThreads) k_xrhs_rows(IpmDev d, int mode) {
 __global__ void __launch_bounds__(kThreads) k_xrhs_cols(IpmDev d, int mode) {
   const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.nx; j += gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) acc += d.cval[p] * d.tr[d.row_idx[p]];
+    const double acc = col_dot(d, j, d.tr);
     d.z[j] = (mode < 0 ? 0.0 : r1_of(d, mode, j, sigma_mu)) + acc;
   }
 }
@@ -516,20 +603,18 @@ __global__ void __launch_bounds__(kThreads) k_hessian_r1(IpmDev d, int mode, dou
 }
 
 __global__ void __launch_bounds__(kThreads) k_rows_minus(IpmDev d, const double* v, const double* base) {
-  const int lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int i = warp_row(); i < d.m; i += warps) {
-    double acc = 0.0;
-    for (int p = d.row_ptr[i] + lane; p < d.row_ptr[i + 1]; p += 32) acc += d.rval[p] * v[d.col_idx[p]];
-    acc = warp_sum(acc);
-    if (lane == 0) d.z[i] = (base ? base[i] : 0.0) - acc;
-  }
+  for_each_row(
+      d, [&](int p) { return d.rval[p] * v[d.col_idx[p]]; },
+      [&](int i, double acc) { d.z[i] = (base ? base[i] : 0.0) - acc; });
+}
+
+__global__ void __launch_bounds__(kThreads) k_rows_minus_cut(IpmDev d, const double* base) {
+  for_each_cut_row(d, [&](int i, double acc) { d.z[i] = (base ? base[i] : 0.0) - acc; });
 }
 
 __global__ void __launch_bounds__(kThreads) k_mehrotra_xt(IpmDev d, double* xt) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
-    double atdy = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+    const double atdy = col_dot(d, j, d.z);
     xt[j] = 1.0 + atdy;
   }
 }
@@ -548,8 +633,7 @@ __global__ void __launch_bounds__(kThreads) k_mehrotra_r1(IpmDev d, const double
 
 __global__ void __launch_bounds__(kThreads) k_add_atz(IpmDev d, const double* r1, double* w) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
-    double atz = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atz += d.cval[p] * d.z[d.row_idx[p]];
+    const double atz = col_dot(d, j, d.z);
     w[j] = r1[j] + atz;
   }
 }
@@ -557,29 +641,37 @@ __global__ void __launch_bounds__(kThreads) k_add_atz(IpmDev d, const double* r1
 __global__ void __launch_bounds__(kThreads) k_hessian_w(IpmDev d, int mode, double* v) {
   const double sigma_mu = mode == kRhsCorrector ? d.sc->sigma * d.sc->mu : 0.0;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
-    double atdy = 0.0;
-    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[d.row_idx[p]];
+    const double atdy = col_dot(d, j, d.z);
     v[j] = hessian_r1(d, mode, j, sigma_mu) + atdy;
   }
 }
 
 int row_blocks(int m) { return std::max(1, std::min(kMaxBlocks, ceil_div(static_cast<long long>(m) * 32, kThreads))); }
+// grid of a for_each_row kernel: a warp per piece or per row, or a CTA per row
+int row_blocks(const IpmDev& d) {
+  if (d.row_piece) return row_blocks(d.row_pieces);
+  return d.row_block ? std::max(1, std::min(kMaxBlocks, d.m)) : row_blocks(d.m);
+}
+int cut_blocks(const IpmDev& d) { return blocks_for(d.row_combs); }
 
 }  // namespace
 
 int reduction_blocks(int n) { return blocks_for(n); }
 
 void launch_residuals(const IpmDev& d, cudaStream_t st, int* launches) {
-  k_residual_rows<<<row_blocks(d.m), kThreads, 0, st>>>(d);
+  k_residual_rows<<<row_blocks(d), kThreads, 0, st>>>(d);
+  if (d.row_combs) k_residual_rows_cut<<<1, kThreads, 0, st>>>(d);
   k_residual_cols<<<blocks_for(d.n), kThreads, 0, st>>>(d);
   SOV_LAUNCH_CHECK();
   if (launches) *launches += 2;
 }
 
 void launch_newton_rhs(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
-  k_newton_rhs<<<row_blocks(d.m), kThreads, 0, st>>>(d, mode);
+  if (d.coltmp) k_newton_tmp<<<blocks_for(d.n), kThreads, 0, st>>>(d, mode);
+  k_newton_rhs<<<row_blocks(d), kThreads, 0, st>>>(d, mode);
+  if (d.row_combs) k_newton_rhs_cut<<<cut_blocks(d), kThreads, 0, st>>>(d);
   SOV_LAUNCH_CHECK();
-  if (launches) *launches += 1;
+  if (launches) *launches += (d.coltmp ? 2 : 1) + (d.row_combs ? 1 : 0);
 }
 
 void launch_direction(const IpmDev& d, int mode, cudaStream_t st, int* launches) {
@@ -603,7 +695,8 @@ void launch_update(const IpmDev& d, cudaStream_t st, int* launches) {
 }
 
 void launch_start_rhs(const IpmDev& d, cudaStream_t st, int* launches) {
-  k_start_rhs<<<row_blocks(d.m), kThreads, 0, st>>>(d);
+  k_start_rhs<<<row_blocks(d), kThreads, 0, st>>>(d);
+  if (d.row_combs) k_start_rhs_cut<<<cut_blocks(d), kThreads, 0, st>>>(d);
   SOV_LAUNCH_CHECK();
   if (launches) *launches += 1;
 }
@@ -648,7 +741,8 @@ void launch_xspace_diag(const IpmDev& d, int mode, double* M, int layout_ld, dou
 
 void launch_normal_matvec(const IpmDev& d, const double* v, double* tmp_n, double* out, double reg, cudaStream_t st) {
   k_normal_cols<<<blocks_for(d.n), kThreads, 0, st>>>(d, v, tmp_n);
-  k_normal_rows<<<row_blocks(d.m), kThreads, 0, st>>>(d, v, tmp_n, out, reg);
+  k_normal_rows<<<row_blocks(d), kThreads, 0, st>>>(d, v, tmp_n, out, reg);
+  if (d.row_combs) k_normal_rows_cut<<<cut_blocks(d), kThreads, 0, st>>>(d, v, out, reg);
   SOV_LAUNCH_CHECK();
 }
 
@@ -680,7 +774,8 @@ void launch_hessian_r1(const IpmDev& d, int mode, double* v, cudaStream_t st) {
 }
 
 void launch_rows_minus(const IpmDev& d, const double* v, const double* base, cudaStream_t st) {
-  k_rows_minus<<<row_blocks(d.m), kThreads, 0, st>>>(d, v, base);
+  k_rows_minus<<<row_blocks(d), kThreads, 0, st>>>(d, v, base);
+  if (d.row_combs) k_rows_minus_cut<<<cut_blocks(d), kThreads, 0, st>>>(d, base);
   SOV_LAUNCH_CHECK();
 }
 

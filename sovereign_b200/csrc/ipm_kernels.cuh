@@ -59,6 +59,17 @@ struct IpmDev {
   const double* sigma;      // m: slack coefficient of the row (+1 / -1)
   double* tr;               // m scratch
   IpmScalars* sc;
+  // long rows (wide LPs): a CTA per row in the row kernels, and the Newton right-hand side's
+  // column terms computed once per column into coltmp (n) instead of once per entry
+  int row_block;
+  double* coltmp;
+  // a row longer than a piece (a dense row): every row kernel walks the rows as warp-sized pieces
+  // (row_pieces in sparse.hpp) and finishes the cut rows in a combine launch
+  const int4* row_piece;
+  int row_pieces;
+  const int4* row_comb;
+  int row_combs;
+  double* row_partial;
   // grid reduction scratch
   double* partials;         // 8 * max_blocks
   unsigned* counter;

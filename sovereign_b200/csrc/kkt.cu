@@ -20,6 +20,12 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+__device__ __forceinline__ double warp_total(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 int blocks_for(long long work) {
   return static_cast<int>(std::max(1LL, std::min(4096LL, (work + kKktThreads - 1) / kKktThreads)));
 }
@@ -64,36 +70,7 @@ struct KktRefine {
 
 __device__ __forceinline__ double bits_to(unsigned long long b) { return __longlong_as_double(static_cast<long long>(b)); }
 
-// res = rhs - K0 (w + c) (c may be null), |res|_inf into *norm; K0 = [Q + X^-1 S, A'; A, 0], the
-// system without delta (start: [I, A'; A, 0]). Skipped when run is given and *run == 0.
-__global__ void k_kkt_residual(KktDev d, const double* x, const double* s, int start, const double* rhs,
-                               const double* w, const double* c, double* res, unsigned long long* norm,
-                               const int* run) {
-  if (run && !*run) return;
-  const int n = d.n, m = d.m;
-  double local = 0.0;
-  bool nan = false;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n + m; t += gridDim.x * blockDim.x) {
-    auto at = [&](int i) { return c ? w[i] + c[i] : w[i]; };
-    double acc = 0.0;
-    if (t < n) {
-      const int j = t;
-      if (start) {
-        acc = at(j);
-      } else {
-        for (int k = d.q_ptr[j]; k < d.q_ptr[j + 1]; ++k) acc += d.q_val[k] * at(d.q_idx[k]);
-        acc += barrier_weight(d, x, s, j) * at(j);
-      }
-      for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) acc += d.cval[p] * at(n + d.row_idx[p]);
-    } else {
-      const int i = t - n;
-      for (int p = d.row_ptr[i]; p < d.row_ptr[i + 1]; ++p) acc += d.rval[p] * at(d.col_idx[p]);
-    }
-    const double e = rhs[t] - acc;
-    res[t] = e;
-    local = fmax(local, fabs(e));
-    nan |= e != e;
-  }
+__device__ __forceinline__ void record_norm(unsigned long long* norm, double local, bool nan) {
   local = warp_max(local);
   // a NaN residual records the quiet-NaN bits, above every finite and infinite norm: neither
   // "err > 0" nor "next < err / 2" holds for it
@@ -101,6 +78,75 @@ __global__ void k_kkt_residual(KktDev d, const double* x, const double* s, int s
   const unsigned long long bits =
       nan ? 0x7ff8000000000000ULL : static_cast<unsigned long long>(__double_as_longlong(local));
   if ((threadIdx.x & 31) == 0) atomicMax(norm, bits);
+}
+
+// Residual res = rhs - K0 (w + c) (c may be null) with K0 = [Q + X^-1 S, A'; A, 0], the system
+// without delta (start: [I, A'; A, 0]); |res|_inf into *norm. Skipped when run is given and
+// *run == 0. Column rows (the first n) one thread each; the rows of A as pieces, a warp each (a
+// dense row is cut into pieces, finished by k_kkt_residual_combine).
+struct ResidualArgs {
+  const double *x, *s;
+  int start;
+  const double *rhs, *w, *c;
+  double* res;
+  unsigned long long* norm;
+  const int* run;
+};
+
+__global__ void k_kkt_residual(KktDev d, ResidualArgs a) {
+  if (a.run && !*a.run) return;
+  const int n = d.n;
+  auto at = [&](int i) { return a.c ? a.w[i] + a.c[i] : a.w[i]; };
+  double local = 0.0;
+  bool nan = false;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  for (int j = tid; j < n; j += nthreads) {
+    double acc = 0.0;
+    if (a.start) {
+      acc = at(j);
+    } else {
+      for (int k = d.q_ptr[j]; k < d.q_ptr[j + 1]; ++k) acc += d.q_val[k] * at(d.q_idx[k]);
+      acc += barrier_weight(d, a.x, a.s, j) * at(j);
+    }
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) acc += d.cval[p] * at(n + d.row_idx[p]);
+    const double e = a.rhs[j] - acc;
+    a.res[j] = e;
+    local = fmax(local, fabs(e));
+    nan |= e != e;
+  }
+  const int lane = threadIdx.x & 31, warp = tid >> 5, warps = nthreads >> 5;
+  for (int q = warp; q < d.row_pieces; q += warps) {
+    const int4 pc = d.row_piece[q];
+    double acc = 0.0;
+    for (int p = pc.x + lane; p < pc.y; p += 32) acc += d.rval[p] * at(d.col_idx[p]);
+    acc = warp_total(acc);
+    if (pc.w < 0) {
+      const double e = a.rhs[n + pc.z] - acc;
+      if (lane == 0) a.res[n + pc.z] = e;
+      local = fmax(local, fabs(e));
+      nan |= e != e;
+    } else if (lane == 0) {
+      d.row_partial[pc.w] = acc;
+    }
+  }
+  record_norm(a.norm, local, nan);
+}
+
+// the rows of A that were cut: their pieces' sums in order
+__global__ void k_kkt_residual_combine(KktDev d, ResidualArgs a) {
+  if (a.run && !*a.run) return;
+  double local = 0.0;
+  bool nan = false;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.row_combs; c += gridDim.x * blockDim.x) {
+    const int4 cb = d.row_comb[c];
+    double acc = 0.0;
+    for (int k = 0; k < cb.z; ++k) acc += d.row_partial[cb.y + k];
+    const double e = a.rhs[d.n + cb.x] - acc;
+    a.res[d.n + cb.x] = e;
+    local = fmax(local, fabs(e));
+    nan |= e != e;
+  }
+  record_norm(a.norm, local, nan);
 }
 
 // rhs = [top (or 0); bottom], sol = rhs; the refinement record is cleared
@@ -230,6 +276,16 @@ void KktSystem::build(const StdForm& f, const int* q_ptr_dev, const int* q_idx_d
   d_.ydiag_slot = put(bufs_, ys, st);
   d_.V = factor_.values();
   d_.diag = factor_.assembled_diag();
+  {
+    int slots = 0;
+    const SparsePieces rp = row_pieces(f.row_ptr, &slots);
+    static_assert(sizeof(SparsePiece) == sizeof(int4) && sizeof(SparseCombine) == sizeof(int4), "piece layout");
+    d_.row_piece = reinterpret_cast<const int4*>(put(bufs_, rp.piece, st));
+    d_.row_pieces = static_cast<int>(rp.piece.size());
+    d_.row_comb = reinterpret_cast<const int4*>(put(bufs_, rp.comb, st));
+    d_.row_combs = static_cast<int>(rp.comb.size());
+    d_.row_partial = put(bufs_, std::vector<double>(std::max(1, slots), 0.0), st);
+  }
   const std::vector<double> zeros(static_cast<size_t>(N), 0.0);
   rhs_ = put(bufs_, zeros, st);
   sol_ = put(bufs_, zeros, st);
@@ -272,6 +328,14 @@ bool KktSystem::assemble_and_factor(bool start, const double* x, const double* s
   return false;
 }
 
+void KktSystem::residual(const double* w, const double* c, double* res, unsigned long long* norm, const int* run,
+                         cudaStream_t st) {
+  const ResidualArgs a{x_, s_, start_ ? 1 : 0, rhs_, w, c, res, norm, run};
+  const long long work = std::max<long long>(n_, 32LL * d_.row_pieces);
+  k_kkt_residual<<<blocks_for(work), kKktThreads, 0, st>>>(d_, a);
+  if (d_.row_combs) k_kkt_residual_combine<<<blocks_for(d_.row_combs), kKktThreads, 0, st>>>(d_, a);
+}
+
 void KktSystem::solve_refined(const double* top, const double* bottom, double* dx, double* dy, cudaStream_t st,
                               int* launches) {
   const int n = n_, m = m_, N = n + m;
@@ -279,18 +343,16 @@ void KktSystem::solve_refined(const double* top, const double* bottom, double* d
   KktRefine* rf = static_cast<KktRefine*>(refine_);
   k_kkt_pack<<<g, kKktThreads, 0, st>>>(n, m, top, bottom, rhs_, sol_, rf);
   factor_.solve(sol_, st, launches);
-  k_kkt_residual<<<g, kKktThreads, 0, st>>>(d_, x_, s_, start_ ? 1 : 0, rhs_, sol_, nullptr, res_, &rf->err[0],
-                                            nullptr);
+  residual(sol_, nullptr, res_, &rf->err[0], nullptr, st);
   for (int r = 0; r < kKktRefineSteps; ++r) {
     k_kkt_begin<<<g, kKktThreads, 0, st>>>(N, r, res_, cor_, rf);
     factor_.solve(cor_, st, launches, &rf->run[r]);
-    k_kkt_residual<<<g, kKktThreads, 0, st>>>(d_, x_, s_, start_ ? 1 : 0, rhs_, sol_, cor_, res2_, &rf->next[r],
-                                              &rf->run[r]);
+    residual(sol_, cor_, res2_, &rf->next[r], &rf->run[r], st);
     k_kkt_accept<<<g, kKktThreads, 0, st>>>(N, r, sol_, cor_, res_, res2_, rf);
   }
   k_kkt_split<<<g, kKktThreads, 0, st>>>(n, m, sol_, dx, dy);
   SOV_LAUNCH_CHECK();
-  if (launches) *launches += 3 + 3 * kKktRefineSteps;
+  if (launches) *launches += (3 + 3 * kKktRefineSteps) + (d_.row_combs ? 1 + kKktRefineSteps : 0);
 }
 
 void KktSystem::solve_newton(double* r1_dx, const double* rp, double* dy, cudaStream_t st, int* launches) {

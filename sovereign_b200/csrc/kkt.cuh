@@ -40,6 +40,11 @@ struct KktDev {
   const int* ydiag_slot;  // m
   double* V;              // the factor's value storage
   double* diag;           // the assembled diagonal in elimination order (pivot reference)
+  const int4* row_piece;  // the rows of A as warp-sized pieces (row_pieces in sparse.hpp)
+  int row_pieces;
+  const int4* row_comb;   // rows cut into pieces: {row, first slot, slots}
+  int row_combs;
+  double* row_partial;
 };
 
 class KktSystem {
@@ -62,6 +67,9 @@ class KktSystem {
   int factorizations() const { return factorizations_; }
   long long nnz_l() const { return sym_.nnz_l; }
   double flops() const { return sym_.flops; }
+  const char* ordering() const {
+    return sym_.ordering == SparseOrder::kNestedDissection ? "nested-dissection" : "minimum-degree";
+  }
   int levels() const { return sym_.levels(); }
   double delta() const { return delta_; }
   ~KktSystem();
@@ -71,6 +79,8 @@ class KktSystem {
   static constexpr double kDeltaMax = 1e-5;  // kKktRegularizationMax (:390)
   void solve_refined(const double* top, const double* bottom, double* dx, double* dy, cudaStream_t st,
                      int* launches);
+  void residual(const double* w, const double* c, double* res, unsigned long long* norm, const int* run,
+                cudaStream_t st);
   int n_ = 0, m_ = 0;
   long long nq_ = 0, na_ = 0;
   double delta_ = kDeltaMin;

@@ -532,4 +532,111 @@ bool sparse_analyze_graph(const std::vector<std::vector<int>>& adj0, std::size_t
   return true;
 }
 
+namespace {
+
+void add_item(SparsePieces& P, int first, int end, int target, int* slots, bool keep_empty) {
+  const int len = end - first;
+  if (len == 0 && !keep_empty) return;
+  if (len <= kSparsePiece) {
+    P.piece.push_back({first, end, target, -1});
+    return;
+  }
+  const int n = (len + kSparsePiece - 1) / kSparsePiece;
+  P.comb.push_back({target, *slots, n, 0});
+  for (int q = 0; q < n; ++q)
+    P.piece.push_back({first + q * kSparsePiece, std::min(end, first + (q + 1) * kSparsePiece), target, *slots + q});
+  *slots += n;
+}
+
+void close_level(SparsePieces& P) {
+  P.piece_lvl.push_back(static_cast<int>(P.piece.size()));
+  P.comb_lvl.push_back(static_cast<int>(P.comb.size()));
+}
+
+}  // namespace
+
+SparsePieces row_pieces(const std::vector<int>& ptr, int* slots) {
+  SparsePieces P;
+  *slots = 0;
+  for (std::size_t i = 0; i + 1 < ptr.size(); ++i) add_item(P, ptr[i], ptr[i + 1], static_cast<int>(i), slots, false);
+  close_level(P);
+  return P;
+}
+
+SparseSchedule sparse_schedule(const SparseSymbolic& s) {
+  SparseSchedule S;
+  const int m = s.m, levels = s.levels();
+  // updates grouped by (level, destination), schedule order kept within a group: two stable
+  // counting sorts (by destination, then by level), linear in the number of updates
+  const size_t n_up = s.pairs.size() / 4;
+  const int n_dst = m + static_cast<int>(s.li.size());
+  std::vector<int> level_of(n_up);
+  for (int h = 0; h < levels; ++h)
+    for (int u = s.pair_ptr[h]; u < s.pair_ptr[h + 1]; ++u) level_of[u] = h;
+  std::vector<int> by_dst(n_up), order(n_up);
+  {
+    std::vector<size_t> cnt(n_dst + 1, 0);
+    for (size_t u = 0; u < n_up; ++u) cnt[s.pairs[4 * u + 3] + 1]++;
+    for (int d = 0; d < n_dst; ++d) cnt[d + 1] += cnt[d];
+    for (size_t u = 0; u < n_up; ++u) by_dst[cnt[s.pairs[4 * u + 3]]++] = static_cast<int>(u);
+    std::vector<size_t> lc(levels + 1, 0);
+    for (size_t u = 0; u < n_up; ++u) lc[level_of[u] + 1]++;
+    for (int h = 0; h < levels; ++h) lc[h + 1] += lc[h];
+    for (size_t q = 0; q < n_up; ++q) {
+      const int u = by_dst[q];
+      order[lc[level_of[u]]++] = u;
+    }
+  }
+  S.up_col.resize(n_up);
+  S.up_a.resize(n_up);
+  S.up_b.resize(n_up);
+  for (size_t q = 0; q < n_up; ++q) {
+    const int u = order[q];
+    S.up_col[q] = s.pairs[4 * u];
+    S.up_a[q] = s.pairs[4 * u + 1];
+    S.up_b[q] = s.pairs[4 * u + 2];
+  }
+  size_t q = 0;
+  for (int h = 0; h < levels; ++h) {
+    while (q < n_up && level_of[order[q]] == h) {
+      const int dst = s.pairs[4 * order[q] + 3];
+      size_t e = q + 1;
+      while (e < n_up && level_of[order[e]] == h && s.pairs[4 * order[e] + 3] == dst) ++e;
+      add_item(S.factor, static_cast<int>(q), static_cast<int>(e), dst, &S.factor_slots, false);
+      q = e;
+    }
+    close_level(S.factor);
+  }
+  // rows of L for the forward solve
+  std::vector<int> row_ptr(m + 1, 0);
+  S.row_pos.resize(s.li.size());
+  S.row_col.resize(s.li.size());
+  for (int i : s.li) row_ptr[i + 1]++;
+  for (int i = 0; i < m; ++i) row_ptr[i + 1] += row_ptr[i];
+  {
+    std::vector<int> fill(row_ptr.begin(), row_ptr.end() - 1);
+    for (int k = 0; k < m; ++k)
+      for (int p = s.lp[k]; p < s.lp[k + 1]; ++p) {
+        const int t = fill[s.li[p]]++;
+        S.row_pos[t] = p;
+        S.row_col[t] = k;
+      }
+  }
+  for (int h = 0; h < levels; ++h) {
+    for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) {
+      const int k = s.lvl_col[c];
+      add_item(S.forward, row_ptr[k], row_ptr[k + 1], k, &S.solve_slots, false);
+    }
+    close_level(S.forward);
+  }
+  for (int h = 0; h < levels; ++h) {  // every column, empty ones too (x_k = y_k / D_k)
+    for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) {
+      const int k = s.lvl_col[c];
+      add_item(S.backward, s.lp[k], s.lp[k + 1], k, &S.solve_slots, true);
+    }
+    close_level(S.backward);
+  }
+  return S;
+}
+
 }  // namespace sov

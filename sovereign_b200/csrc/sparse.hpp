@@ -58,4 +58,39 @@ bool sparse_analyze_graph(const std::vector<std::vector<int>>& adj, std::size_t 
 // in the pattern of L).
 int sparse_slot(const SparseSymbolic& s, int i, int j);
 
+// The GPU work schedule of a symbolic factor. Work items -- a destination's run of rank-1 terms
+// (factor), a row of L (forward solve), a column of L (backward solve) -- are cut into pieces of
+// at most kSparsePiece terms, one warp each, so that one long item (a dense row's diagonal collects
+// a term from nearly every column) spreads over many warps. A piece with slot < 0 applies its sum
+// to its target directly; otherwise the sum goes to partial[slot], and the level's combine entry
+// {target, first slot, slots} adds the item's partial sums in order after one more grid barrier.
+constexpr int kSparsePiece = 1024;
+
+struct SparsePiece {
+  int first, end, target, slot;  // same layout as the device's int4
+};
+struct SparseCombine {
+  int target, first, count, pad;
+};
+struct SparsePieces {
+  std::vector<SparsePiece> piece;
+  std::vector<SparseCombine> comb;
+  std::vector<int> piece_lvl{0}, comb_lvl{0};  // per level
+};
+struct SparseSchedule {
+  // updates in (level, destination) order
+  std::vector<int> up_col, up_a, up_b;  // pivot column, positions of l_ak and l_bk
+  SparsePieces factor;                  // over the update range; target = index into [D | L]
+  std::vector<int> row_pos, row_col;    // entries of L by row: positions in L, columns
+  SparsePieces forward;                 // over row_pos / row_col; target = row k
+  SparsePieces backward;                // over li; target = column k (every column has a piece)
+  int factor_slots = 0, solve_slots = 0;
+};
+
+SparseSchedule sparse_schedule(const SparseSymbolic& s);
+
+// The rows of a CSR pattern (ptr, rows + 1 entries) as pieces of one level: target = row; the
+// combine entries hold the rows that were cut, slots numbered from 0.
+SparsePieces row_pieces(const std::vector<int>& ptr, int* slots);
+
 }  // namespace sov

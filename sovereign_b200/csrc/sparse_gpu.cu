@@ -24,8 +24,8 @@ __device__ __forceinline__ double warp_total(double v) {
 }
 
 // Per level: the pivots of its columns (one thread each), then its rank-1 updates, one warp per
-// destination: lane l sums the destination's terms l, l + 32, ... and the warp adds the 32 partial
-// sums in a fixed tree (deterministic).
+// piece: lane l sums the piece's terms l, l + 32, ... and the warp adds the 32 partial sums in a
+// fixed tree; a run cut into pieces is finished by its combine step (deterministic either way).
 __global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
   cg::grid_group g = cg::this_grid();
   const int rank = static_cast<int>(g.thread_rank()), size = static_cast<int>(g.size());
@@ -43,12 +43,25 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
       s.inv_d[k] = 1.0 / (drop ? sg * 1e128 : p);
     }
     g.sync();
-    for (int r = s.run_lvl[h] + warp; r < s.run_lvl[h + 1]; r += warps) {
+    for (int q = s.fpiece_lvl[h] + warp; q < s.fpiece_lvl[h + 1]; q += warps) {
+      const int4 pc = s.fpiece[q];
       double acc = 0.0;
-      for (int u = s.run_ptr[r] + lane; u < s.run_ptr[r + 1]; u += 32)
+      for (int u = pc.x + lane; u < pc.y; u += 32)
         acc += s.V[s.m + s.up_a[u]] * s.V[s.m + s.up_b[u]] * s.inv_d[s.up_col[u]];
       acc = warp_total(acc);
-      if (lane == 0) s.V[s.run_dst[r]] -= acc;
+      if (lane == 0) {
+        if (pc.w < 0) s.V[pc.z] -= acc;
+        else s.partial[pc.w] = acc;
+      }
+    }
+    if (s.fcomb_lvl[h + 1] > s.fcomb_lvl[h]) {  // uniform: every thread reads the same bounds
+      g.sync();
+      for (int c = s.fcomb_lvl[h] + rank; c < s.fcomb_lvl[h + 1]; c += size) {
+        const int4 cb = s.fcomb[c];
+        double t = 0.0;
+        for (int k = 0; k < cb.z; ++k) t += s.partial[cb.y + k];
+        s.V[cb.x] -= t;
+      }
     }
     g.sync();
   }
@@ -58,7 +71,8 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
 
 // L D L' x = z: forward y_k = z_k - sum_j L~_kj (1/D_j) y_j (row k of L, descendants: earlier
 // levels), backward x_k = (1/D_k) (y_k - sum_i L~_ik x_i) (column k, ancestors: later levels);
-// one warp per column, partial sums added in a fixed tree
+// one warp per piece, partial sums added in a fixed tree, long rows and columns through their
+// combine steps
 __global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, double* z, const int* run) {
   if (run && !*run) return;  // written by an earlier launch: every block takes the same exit
   cg::grid_group g = cg::this_grid();
@@ -67,23 +81,47 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, do
   for (int k = rank; k < s.m; k += size) s.work[k] = z[s.perm[k]];
   g.sync();
   for (int h = 0; h < s.levels; ++h) {
-    for (int q = s.lvl_ptr[h] + warp; q < s.lvl_ptr[h + 1]; q += warps) {
-      const int k = s.lvl_col[q];
+    for (int q = s.lpiece_lvl[h] + warp; q < s.lpiece_lvl[h + 1]; q += warps) {
+      const int4 pc = s.lpiece[q];
       double acc = 0.0;
-      for (int t = s.row_ptr[k] + lane; t < s.row_ptr[k + 1]; t += 32)
+      for (int t = pc.x + lane; t < pc.y; t += 32)
         acc += s.V[s.m + s.row_pos[t]] * s.inv_d[s.row_col[t]] * s.work[s.row_col[t]];
       acc = warp_total(acc);
-      if (lane == 0) s.work[k] -= acc;
+      if (lane == 0) {
+        if (pc.w < 0) s.work[pc.z] -= acc;
+        else s.partial[pc.w] = acc;
+      }
+    }
+    if (s.lcomb_lvl[h + 1] > s.lcomb_lvl[h]) {
+      g.sync();
+      for (int c = s.lcomb_lvl[h] + rank; c < s.lcomb_lvl[h + 1]; c += size) {
+        const int4 cb = s.lcomb[c];
+        double t = 0.0;
+        for (int k = 0; k < cb.z; ++k) t += s.partial[cb.y + k];
+        s.work[cb.x] -= t;
+      }
     }
     g.sync();
   }
   for (int h = s.levels - 1; h >= 0; --h) {
-    for (int q = s.lvl_ptr[h] + warp; q < s.lvl_ptr[h + 1]; q += warps) {
-      const int k = s.lvl_col[q];
+    for (int q = s.upiece_lvl[h] + warp; q < s.upiece_lvl[h + 1]; q += warps) {
+      const int4 pc = s.upiece[q];
       double acc = 0.0;
-      for (int p = s.lp[k] + lane; p < s.lp[k + 1]; p += 32) acc += s.V[s.m + p] * s.work[s.li[p]];
+      for (int p = pc.x + lane; p < pc.y; p += 32) acc += s.V[s.m + p] * s.work[s.li[p]];
       acc = warp_total(acc);
-      if (lane == 0) s.work[k] = (s.work[k] - acc) * s.inv_d[k];
+      if (lane == 0) {
+        if (pc.w < 0) s.work[pc.z] = (s.work[pc.z] - acc) * s.inv_d[pc.z];
+        else s.partial[pc.w] = acc;
+      }
+    }
+    if (s.ucomb_lvl[h + 1] > s.ucomb_lvl[h]) {
+      g.sync();
+      for (int c = s.ucomb_lvl[h] + rank; c < s.ucomb_lvl[h + 1]; c += size) {
+        const int4 cb = s.ucomb[c];
+        double t = 0.0;
+        for (int k = 0; k < cb.z; ++k) t += s.partial[cb.y + k];
+        s.work[cb.x] = (s.work[cb.x] - t) * s.inv_d[cb.x];
+      }
     }
     g.sync();
   }
@@ -106,60 +144,9 @@ void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, d
   release();
   const int m = s.m, levels = s.levels();
   nnz_l_ = s.nnz_l;
-  // updates grouped by (level, destination), schedule order kept within a group: two stable
-  // counting sorts (by destination, then by level), linear in the number of updates
-  const size_t n_up = s.pairs.size() / 4;
-  const int n_dst = m + static_cast<int>(s.li.size());
-  std::vector<int> level_of(n_up);
-  for (int h = 0; h < levels; ++h)
-    for (int u = s.pair_ptr[h]; u < s.pair_ptr[h + 1]; ++u) level_of[u] = h;
-  std::vector<int> by_dst(n_up), order(n_up);
-  {
-    std::vector<size_t> cnt(n_dst + 1, 0);
-    for (size_t u = 0; u < n_up; ++u) cnt[s.pairs[4 * u + 3] + 1]++;
-    for (int d = 0; d < n_dst; ++d) cnt[d + 1] += cnt[d];
-    for (size_t u = 0; u < n_up; ++u) by_dst[cnt[s.pairs[4 * u + 3]]++] = static_cast<int>(u);
-    std::vector<size_t> lc(levels + 1, 0);
-    for (size_t u = 0; u < n_up; ++u) lc[level_of[u] + 1]++;
-    for (int h = 0; h < levels; ++h) lc[h + 1] += lc[h];
-    for (size_t q = 0; q < n_up; ++q) {
-      const int u = by_dst[q];
-      order[lc[level_of[u]]++] = u;
-    }
-  }
-  std::vector<int> run_lvl(levels + 1, 0), run_ptr(1, 0), run_dst, up_col(n_up), up_a(n_up), up_b(n_up);
-  run_dst.reserve(n_up);
-  run_ptr.reserve(n_up + 1);
-  for (size_t q = 0; q < n_up; ++q) {
-    const int u = order[q];
-    const bool new_run = q == 0 || level_of[u] != level_of[order[q - 1]] || s.pairs[4 * u + 3] != run_dst.back();
-    if (new_run) {
-      if (q > 0) run_ptr.push_back(static_cast<int>(q));
-      run_dst.push_back(s.pairs[4 * u + 3]);
-      run_lvl[level_of[u] + 1] = static_cast<int>(run_dst.size());
-    }
-    up_col[q] = s.pairs[4 * u];
-    up_a[q] = s.pairs[4 * u + 1];
-    up_b[q] = s.pairs[4 * u + 2];
-  }
-  if (n_up) run_ptr.push_back(static_cast<int>(n_up));
-  for (int h = 0; h < levels; ++h) run_lvl[h + 1] = std::max(run_lvl[h + 1], run_lvl[h]);
-  // rows of L for the forward solve
-  std::vector<int> row_ptr(m + 1, 0), row_pos(s.li.size()), row_col(s.li.size());
-  for (int i : s.li) row_ptr[i + 1]++;
-  for (int i = 0; i < m; ++i) row_ptr[i + 1] += row_ptr[i];
-  {
-    std::vector<int> fill(row_ptr.begin(), row_ptr.end() - 1);
-    for (int k = 0; k < m; ++k)
-      for (int p = s.lp[k]; p < s.lp[k + 1]; ++p) {
-        const int t = fill[s.li[p]]++;
-        row_pos[t] = p;
-        row_col[t] = k;
-      }
-  }
+  const SparseSchedule S = sparse_schedule(s);
   d_.m = m;
   d_.levels = levels;
-  std::vector<double> zeros;
   d_.V = put(bufs_, std::vector<double>(m + s.li.size(), 0.0), st);
   d_.diag = put(bufs_, std::vector<double>(m, 0.0), st);
   d_.inv_d = put(bufs_, std::vector<double>(m, 0.0), st);
@@ -169,15 +156,26 @@ void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, d
   d_.li = put(bufs_, s.li, st);
   d_.lvl_ptr = put(bufs_, s.lvl_ptr, st);
   d_.lvl_col = put(bufs_, s.lvl_col, st);
-  d_.run_lvl = put(bufs_, run_lvl, st);
-  d_.run_ptr = put(bufs_, run_ptr, st);
-  d_.run_dst = put(bufs_, run_dst, st);
-  d_.up_col = put(bufs_, up_col, st);
-  d_.up_a = put(bufs_, up_a, st);
-  d_.up_b = put(bufs_, up_b, st);
-  d_.row_ptr = put(bufs_, row_ptr, st);
-  d_.row_pos = put(bufs_, row_pos, st);
-  d_.row_col = put(bufs_, row_col, st);
+  static_assert(sizeof(SparsePiece) == sizeof(int4) && sizeof(SparseCombine) == sizeof(int4), "piece layout");
+  auto put4 = [&](const auto& v) { return reinterpret_cast<const int4*>(put(bufs_, v, st)); };
+  d_.fpiece = put4(S.factor.piece);
+  d_.fpiece_lvl = put(bufs_, S.factor.piece_lvl, st);
+  d_.fcomb = put4(S.factor.comb);
+  d_.fcomb_lvl = put(bufs_, S.factor.comb_lvl, st);
+  d_.lpiece = put4(S.forward.piece);
+  d_.lpiece_lvl = put(bufs_, S.forward.piece_lvl, st);
+  d_.lcomb = put4(S.forward.comb);
+  d_.lcomb_lvl = put(bufs_, S.forward.comb_lvl, st);
+  d_.upiece = put4(S.backward.piece);
+  d_.upiece_lvl = put(bufs_, S.backward.piece_lvl, st);
+  d_.ucomb = put4(S.backward.comb);
+  d_.ucomb_lvl = put(bufs_, S.backward.comb_lvl, st);
+  d_.partial = put(bufs_, std::vector<double>(std::max(1, std::max(S.factor_slots, S.solve_slots)), 0.0), st);
+  d_.up_col = put(bufs_, S.up_col, st);
+  d_.up_a = put(bufs_, S.up_a, st);
+  d_.up_b = put(bufs_, S.up_b, st);
+  d_.row_pos = put(bufs_, S.row_pos, st);
+  d_.row_col = put(bufs_, S.row_col, st);
   d_.drop_count = drop_count;
   d_.fail = fail;
   d_.drop_tol = drop_tol;

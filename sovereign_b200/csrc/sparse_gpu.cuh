@@ -32,14 +32,24 @@ struct SparseDev {
   const int* li;        // nnz(L)
   const int* lvl_ptr;   // levels + 1
   const int* lvl_col;   // m
-  const int* run_lvl;   // levels + 1: first destination run of each level
-  const int* run_ptr;   // runs + 1: first update of each run
-  const int* run_dst;   // runs: index into V
+  // the work pieces and combine steps of sparse_schedule (sparse.hpp), per level
+  const int4* fpiece;   // factor pieces (first, end: update range; target: index into V)
+  const int* fpiece_lvl;  // levels + 1
+  const int4* fcomb;    // factor combines {target, first slot, slots, 0}
+  const int* fcomb_lvl;   // levels + 1
+  const int4* lpiece;   // forward pieces (first, end: range of row_pos / row_col; target: row k)
+  const int* lpiece_lvl;
+  const int4* lcomb;
+  const int* lcomb_lvl;
+  const int4* upiece;   // backward pieces (first, end: range of li; target: column k)
+  const int* upiece_lvl;
+  const int4* ucomb;
+  const int* ucomb_lvl;
+  double* partial;      // piece sums awaiting their combine step
   const int* up_col;    // updates: pivot column k
   const int* up_a;      // updates: position of l_ak
   const int* up_b;      // updates: position of l_bk
-  const int* row_ptr;   // m + 1: entries of L in row k (forward solve)
-  const int* row_pos;   // their positions in L
+  const int* row_pos;   // entries of L by row (forward solve): positions in L
   const int* row_col;   // their columns
   int* drop_count;
   int* fail;

@@ -160,6 +160,27 @@ def convex_sequence_qp(n: int, seed: int, target: np.ndarray | None = None,
     return mdl
 
 
+def budget_lp(m: int, n: int, k: int, seed: int, fraction: float = 0.2) -> Model:
+    """random_sparse_lp(m, n, k, seed) plus one dense row: sum_j x_j <= fraction * sum_j x0_j over
+    all n columns (x0 the point the equalities were built from), a budget row longer than a warp's
+    piece of work. Dual feasible (y0 with a zero budget multiplier), so bounded."""
+    base = random_sparse_lp(m, n, k, seed)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rng.random((n, m)) if m <= 4096 else None  # the draws random_sparse_lp made, in order
+    rng.standard_normal((n, k))
+    x0 = rng.uniform(0.1, 1.0, size=n)
+    cols = np.repeat(np.arange(n), k)
+    rows = base.row_idx.astype(np.int64)
+    vals = base.values
+    cols = np.concatenate([cols, np.arange(n)])
+    rows = np.concatenate([rows, np.full(n, m)])
+    vals = np.concatenate([vals, np.ones(n)])
+    col_ptr, row_idx, values = _csc_from_triplets(n, cols, rows, vals)
+    rhs = np.concatenate([base.rhs, [fraction * float(np.sum(x0))]])
+    sense = np.concatenate([base.sense, np.array([LE], dtype=np.int8)])
+    return _lp(n, m + 1, col_ptr, row_idx, values, base.obj, rhs, sense, f"budget_lp_{m}x{n}")
+
+
 def presolve_lp_example(m: int, n: int, seed: int) -> Model:
     """A random feasible, bounded LP (random_sparse_lp's construction, k = 4) with what presolve
     removes added: fixed columns (lb = ub = x0_j), singleton rows of every sense satisfied by x0

@@ -9,7 +9,8 @@ oracle/_ref/libsovref.so from them):
 
 Writes
   lp_reference.json   InteriorPointSolver results (status, iterations, objective, gap, residuals,
-                      primal checksum) on the seeded and regression LP models below
+                      primal checksum) on the seeded and regression LP models below, the LPs
+                      with a dense budget row included
   transport4096_reference.npz
                       the reference's objective and status for every LP of the 4096-LP batched
                       workload (transport_batch(4096, seed=2026)); where its dense LU stops short of
@@ -58,6 +59,7 @@ LP_SPECS = [
     ("random_sparse_lp", [100, 500, 8, 1]), ("random_sparse_lp", [200, 1000, 8, 2]),
     ("random_sparse_lp", [500, 2500, 8, 1]), ("grid_network_lp", [130]),
 ]
+DENSE_ROW_LP_SPECS = [("budget_lp", [400, 4000, 6, 7]), ("budget_lp", [2000, 40000, 6, 3])]
 BATCH_SPEC = dict(count=64, seed=3)          # transport_batch sample of the 4096-LP workload
 MULTICOMMODITY_SEEDS = [100, 101]            # MulticommodityFamily() instances
 QP_SPECS = [("small_qp_offdiagonal", []), ("convex_sequence_qp", [52, 3]), ("convex_sequence_qp", [202, 3]),
@@ -125,6 +127,20 @@ def c2():
     print("c2", r.status_name, r.objective_value, r.solve_seconds, flush=True)
 
 
+def dense_row_lps():
+    """LPs with a dense budget row (rows longer than a warp's piece of work), added to
+    lp_reference.json in place."""
+    path = os.path.join(HERE, "lp_reference.json")
+    with open(path) as f:
+        lp = json.load(f)
+    for name, args in DENSE_ROW_LP_SPECS:
+        key = f"{name}({','.join(map(str, args))})"
+        lp[key] = dict(spec=[name, args], **summarize(oracle.solve(build(name, args), kind="reference")))
+        print("lp", key, lp[key]["status"], lp[key]["objective"], flush=True)
+    with open(path, "w") as f:
+        json.dump(lp, f, indent=1)
+
+
 def kkt():
     """QPs on the reference's sparse quasi-definite KKT path."""
     out = {}
@@ -151,6 +167,8 @@ def main(sections=()):
         c2()
     if "kkt" in sections:
         kkt()
+    if "dense_row" in sections:
+        dense_row_lps()
     if sections:
         return
     headline()
@@ -173,6 +191,7 @@ def main(sections=()):
         print("mc", s, lp[f"multicommodity({s})"]["objective"], flush=True)
     with open(os.path.join(HERE, "lp_reference.json"), "w") as f:
         json.dump(lp, f, indent=1)
+    dense_row_lps()
 
     qp = {}
     for name, args in QP_SPECS:

@@ -43,7 +43,8 @@ def test_fp64_matches_reference(key):
 
 
 @pytest.mark.parametrize("key", ["reference_staircase(8,40)", "transport(50,50,0)", "reference_transport(60)",
-                                 "random_sparse_lp(100,500,8,1)", "bounded_lp_example()", "multicommodity(100)"])
+                                 "random_sparse_lp(100,500,8,1)", "bounded_lp_example()", "multicommodity(100)",
+                                 "budget_lp(400,4000,6,7)", "budget_lp(2000,40000,6,3)"])
 def test_sparse_factorization_matches_reference(key, monkeypatch):
     # the reference's sparse path (SOVEREIGN_IPM_NORMAL_EQUATIONS=sparse): minimum-degree order on the
     # host, numeric L D L' and its solves on the GPU level by level in the elimination tree
@@ -51,7 +52,8 @@ def test_sparse_factorization_matches_reference(key, monkeypatch):
     g = LP[key]
     r = InteriorPointSolver().solve(model_of(g["spec"]), with_diag=True)
     assert r.status_name == "OPTIMAL", r.message
-    assert "sparse LDL^T on the GPU" in r.message
+    # a nearly dense normal matrix (2000 random rows over 40000 columns) is factored densely instead
+    assert "sparse LDL^T on the GPU" in r.message or "the sparse factor would be nearly dense" in r.message
     assert rel(r.objective_value, g["objective"]) < TOL
     assert r.primal_residual < 1e-9 and r.dual_residual < 1e-9 and r.duality_gap < 1e-9
     assert r.iterations <= g["iterations"] + 1
@@ -129,9 +131,10 @@ def test_batch_run_to_run():
     assert max(rel(x.objective_value, y.objective_value) for x, y in zip(a, b)) < 1e-9
 
 
-@pytest.mark.parametrize("threads", ["128", "256", "512"])
+@pytest.mark.parametrize("threads", ["128", "129", "256", "257", "512"])
 def test_batch_every_cta_width(threads, monkeypatch):
-    # the per-bucket thread count is a tuning choice only: every width gives the reference's answers
+    # the per-bucket kernel shape (width; odd codes: the register-capped lean variants) is a tuning
+    # choice only: every shape gives the reference's answers
     monkeypatch.setenv("SOVEREIGN_BATCH_THREADS", threads)
     g = LP["transport_batch"]
     res = solve_batch(P.transport_batch(**g["spec"]))

@@ -14,7 +14,8 @@ LP = json.load(open(os.path.join(GOLDEN, "lp_reference.json")))
 QP = json.load(open(os.path.join(GOLDEN, "qp_reference.json")))
 # the restatement factors M densely; above this size it is too slow for the CPU suite
 SMALL_LP = [k for k, v in LP.items() if "spec" in v and isinstance(v["spec"], list)
-            and v["spec"][0] not in ("multicommodity", "grid_network_lp") and k != "random_sparse_lp(500,2500,8,1)"]
+            and v["spec"][0] not in ("multicommodity", "grid_network_lp")
+            and k not in ("random_sparse_lp(500,2500,8,1)", "budget_lp(2000,40000,6,3)")]
 
 
 def rel(a, b):
