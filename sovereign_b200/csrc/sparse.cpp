@@ -161,12 +161,96 @@ bool minimum_degree(const std::vector<std::vector<int>>& graph, std::size_t fill
 // algorithm for irregular finite element problems", SIAM J. Numer. Anal. 15(5), 1978): a
 // connected part is split by one level of a breadth-first search from a pseudo-peripheral node --
 // the smallest level that leaves at least a quarter of the part on each side, cut down to the
-// nodes with a neighbour beyond it -- its two sides are ordered first and the separator last;
+// nodes with a neighbour beyond it, or, when smaller, the smallest minimum vertex cover of the
+// edges between two adjacent levels over the balanced cuts -- its two sides are ordered first and
+// the separator last;
 // parts of at most kNdLeaf nodes, or whose search is too shallow to split, take the minimum-degree
 // order of their own subgraph. Dense rows (the same cut as minimum_degree) go last. Separators are
 // small and the tree is shallow wherever the graph is long and thin, where minimum degree walks
 // the graph from its ends and builds an elimination tree as deep as the graph is long.
 constexpr int kNdLeaf = 32;
+
+// Minimum vertex cover (Koenig: from a maximum matching) of the bipartite graph of the edges
+// between BFS levels k and k + 1 of a part (lv: the nodes of both levels): removing it separates
+// levels <= k from levels > k, and it is never larger than either level. loc: scratch, -1
+// everywhere, restored.
+void cover_separator(const std::vector<std::vector<int>>& graph, const std::vector<int>& part,
+                     const std::vector<int>& dist, int id, const int* lv, int nlv, int k, std::vector<int>& loc,
+                     std::vector<int>& cover) {
+  std::vector<int> U, V;
+  for (int t = 0; t < nlv; ++t) {  // the nodes of levels k and k + 1
+    const int v = lv[t];
+    bool across = false;
+    for (int u : graph[v])
+      if (part[u] == id && dist[u] == (dist[v] == k ? k + 1 : k)) {
+        across = true;
+        break;
+      }
+    if (!across) continue;
+    if (dist[v] == k) {
+      loc[v] = static_cast<int>(U.size());
+      U.push_back(v);
+    } else {
+      loc[v] = static_cast<int>(V.size());
+      V.push_back(v);
+    }
+  }
+  const int nu = static_cast<int>(U.size()), nv = static_cast<int>(V.size());
+  std::vector<std::vector<int>> adj(nu);
+  for (int a = 0; a < nu; ++a)
+    for (int u : graph[U[a]])
+      if (part[u] == id && dist[u] == k + 1 && loc[u] >= 0) adj[a].push_back(loc[u]);
+  for (int v : U) loc[v] = -1;
+  for (int v : V) loc[v] = -1;
+  // maximum matching, one breadth-first augmenting search per free vertex of U
+  std::vector<int> mate_u(nu, -1), mate_v(nv, -1), prev(nv, -1), seen(nv, -1), queue;
+  for (int a0 = 0; a0 < nu; ++a0) {
+    queue.assign(1, a0);
+    int end_v = -1;
+    for (std::size_t h = 0; h < queue.size() && end_v < 0; ++h) {
+      const int a = queue[h];
+      for (int b : adj[a]) {
+        if (seen[b] == a0) continue;
+        seen[b] = a0;
+        prev[b] = a;
+        if (mate_v[b] < 0) {
+          end_v = b;
+          break;
+        }
+        queue.push_back(mate_v[b]);
+      }
+    }
+    for (int b = end_v; b >= 0;) {  // flip the path
+      const int a = prev[b], next = mate_u[a];
+      mate_u[a] = b;
+      mate_v[b] = a;
+      b = next;
+    }
+  }
+  // Z: reachable from the free vertices of U along alternating paths; cover = (U \ Z) + (V in Z)
+  std::vector<char> zu(nu, 0), zv(nv, 0);
+  queue.clear();
+  for (int a = 0; a < nu; ++a)
+    if (mate_u[a] < 0) {
+      zu[a] = 1;
+      queue.push_back(a);
+    }
+  for (std::size_t h = 0; h < queue.size(); ++h)
+    for (int b : adj[queue[h]]) {
+      if (zv[b]) continue;
+      zv[b] = 1;
+      const int a = mate_v[b];
+      if (a >= 0 && !zu[a]) {
+        zu[a] = 1;
+        queue.push_back(a);
+      }
+    }
+  cover.clear();
+  for (int a = 0; a < nu; ++a)
+    if (!zu[a]) cover.push_back(U[a]);
+  for (int b = 0; b < nv; ++b)
+    if (zv[b]) cover.push_back(V[b]);
+}
 
 void nested_dissection(const std::vector<std::vector<int>>& graph, std::vector<int>& perm) {
   const int n = static_cast<int>(graph.size());
@@ -310,6 +394,33 @@ void nested_dissection(const std::vector<std::vector<int>>& graph, std::vector<i
             }
           (beyond ? sep : sideA).push_back(v);
         }
+      }
+      // a smaller separator: the smallest minimum vertex cover of the edges between two adjacent
+      // levels k, k + 1 among the balanced cuts (at least a quarter of the part on each side);
+      // the search order is nondecreasing in distance, so each level is a span of it
+      std::vector<int> start(ecc + 2, 0);
+      for (int v : order) start[dist[v] + 1]++;
+      for (int l = 0; l <= ecc; ++l) start[l + 1] += start[l];
+      std::vector<int> cover, best_cover;
+      int cut = -1;
+      for (int l = 0; l + 1 <= ecc; ++l) {
+        const int below_incl = start[l + 1], above_excl = k - start[l + 2];
+        if (below_incl < k / 4 || above_excl < k / 4) continue;
+        cover_separator(graph, part, dist, cid, order.data() + start[l], start[l + 2] - start[l], l, loc, cover);
+        if (cut < 0 || cover.size() < best_cover.size()) {
+          best_cover.swap(cover);
+          cut = l;
+        }
+      }
+      if (cut >= 0 && best_cover.size() < sep.size()) {
+        for (int v : best_cover) dist[v] = -2;  // mark: separator
+        sideA.clear();
+        sideB.clear();
+        for (int v : comp) {
+          if (dist[v] == -2) continue;
+          (dist[v] <= cut ? sideA : sideB).push_back(v);
+        }
+        sep.swap(best_cover);
       }
       const int a = static_cast<int>(sideA.size()), b = static_cast<int>(sideB.size());
       for (int q = 0; q < static_cast<int>(sep.size()); ++q) {
@@ -537,18 +648,26 @@ namespace {
 void add_item(SparsePieces& P, int first, int end, int target, int* slots, bool keep_empty) {
   const int len = end - first;
   if (len == 0 && !keep_empty) return;
-  if (len <= kSparsePiece) {
+  if (len <= kSparseShort) {
     P.piece.push_back({first, end, target, -1});
+    return;
+  }
+  if (len <= kSparsePiece) {
+    P.pending_long.push_back({first, end, target, -1});
     return;
   }
   const int n = (len + kSparsePiece - 1) / kSparsePiece;
   P.comb.push_back({target, *slots, n, 0});
   for (int q = 0; q < n; ++q)
-    P.piece.push_back({first + q * kSparsePiece, std::min(end, first + (q + 1) * kSparsePiece), target, *slots + q});
+    P.pending_long.push_back(
+        {first + q * kSparsePiece, std::min(end, first + (q + 1) * kSparsePiece), target, *slots + q});
   *slots += n;
 }
 
 void close_level(SparsePieces& P) {
+  P.warp_lvl.push_back(static_cast<int>(P.piece.size()));
+  P.piece.insert(P.piece.end(), P.pending_long.begin(), P.pending_long.end());
+  P.pending_long.clear();
   P.piece_lvl.push_back(static_cast<int>(P.piece.size()));
   P.comb_lvl.push_back(static_cast<int>(P.comb.size()));
 }

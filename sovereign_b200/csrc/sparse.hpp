@@ -72,10 +72,16 @@ struct SparsePiece {
 struct SparseCombine {
   int target, first, count, pad;
 };
+// Within a level, pieces of at most kSparseShort terms come first, one thread each (most items of
+// a sparse factor are a few terms long: a warp per item would leave most lanes idle); the longer
+// pieces follow from warp_lvl[h] on, one warp each.
+constexpr int kSparseShort = 16;
 struct SparsePieces {
   std::vector<SparsePiece> piece;
   std::vector<SparseCombine> comb;
   std::vector<int> piece_lvl{0}, comb_lvl{0};  // per level
+  std::vector<int> warp_lvl;                   // per level: first piece taken by a warp
+  std::vector<SparsePiece> pending_long;       // while a level is built
 };
 struct SparseSchedule {
   // updates in (level, destination) order

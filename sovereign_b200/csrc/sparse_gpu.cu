@@ -43,7 +43,14 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_factor(SparseDev s) {
       s.inv_d[k] = 1.0 / (drop ? sg * 1e128 : p);
     }
     g.sync();
-    for (int q = s.fpiece_lvl[h] + warp; q < s.fpiece_lvl[h + 1]; q += warps) {
+    for (int q = s.fpiece_lvl[h] + rank; q < s.fwarp_lvl[h]; q += size) {  // short pieces: a thread each
+      const int4 pc = s.fpiece[q];
+      double acc = 0.0;
+      for (int u = pc.x; u < pc.y; ++u) acc += s.V[s.m + s.up_a[u]] * s.V[s.m + s.up_b[u]] * s.inv_d[s.up_col[u]];
+      if (pc.w < 0) s.V[pc.z] -= acc;
+      else s.partial[pc.w] = acc;
+    }
+    for (int q = s.fwarp_lvl[h] + warp; q < s.fpiece_lvl[h + 1]; q += warps) {
       const int4 pc = s.fpiece[q];
       double acc = 0.0;
       for (int u = pc.x + lane; u < pc.y; u += 32)
@@ -81,7 +88,14 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, do
   for (int k = rank; k < s.m; k += size) s.work[k] = z[s.perm[k]];
   g.sync();
   for (int h = 0; h < s.levels; ++h) {
-    for (int q = s.lpiece_lvl[h] + warp; q < s.lpiece_lvl[h + 1]; q += warps) {
+    for (int q = s.lpiece_lvl[h] + rank; q < s.lwarp_lvl[h]; q += size) {
+      const int4 pc = s.lpiece[q];
+      double acc = 0.0;
+      for (int t = pc.x; t < pc.y; ++t) acc += s.V[s.m + s.row_pos[t]] * s.inv_d[s.row_col[t]] * s.work[s.row_col[t]];
+      if (pc.w < 0) s.work[pc.z] -= acc;
+      else s.partial[pc.w] = acc;
+    }
+    for (int q = s.lwarp_lvl[h] + warp; q < s.lpiece_lvl[h + 1]; q += warps) {
       const int4 pc = s.lpiece[q];
       double acc = 0.0;
       for (int t = pc.x + lane; t < pc.y; t += 32)
@@ -104,7 +118,14 @@ __global__ void __launch_bounds__(kSparseThreads) k_sparse_solve(SparseDev s, do
     g.sync();
   }
   for (int h = s.levels - 1; h >= 0; --h) {
-    for (int q = s.upiece_lvl[h] + warp; q < s.upiece_lvl[h + 1]; q += warps) {
+    for (int q = s.upiece_lvl[h] + rank; q < s.uwarp_lvl[h]; q += size) {
+      const int4 pc = s.upiece[q];
+      double acc = 0.0;
+      for (int p = pc.x; p < pc.y; ++p) acc += s.V[s.m + p] * s.work[s.li[p]];
+      if (pc.w < 0) s.work[pc.z] = (s.work[pc.z] - acc) * s.inv_d[pc.z];
+      else s.partial[pc.w] = acc;
+    }
+    for (int q = s.uwarp_lvl[h] + warp; q < s.upiece_lvl[h + 1]; q += warps) {
       const int4 pc = s.upiece[q];
       double acc = 0.0;
       for (int p = pc.x + lane; p < pc.y; p += 32) acc += s.V[s.m + p] * s.work[s.li[p]];
@@ -160,14 +181,17 @@ void SparseFactor::upload(const SparseSymbolic& s, int* drop_count, int* fail, d
   auto put4 = [&](const auto& v) { return reinterpret_cast<const int4*>(put(bufs_, v, st)); };
   d_.fpiece = put4(S.factor.piece);
   d_.fpiece_lvl = put(bufs_, S.factor.piece_lvl, st);
+  d_.fwarp_lvl = put(bufs_, S.factor.warp_lvl, st);
   d_.fcomb = put4(S.factor.comb);
   d_.fcomb_lvl = put(bufs_, S.factor.comb_lvl, st);
   d_.lpiece = put4(S.forward.piece);
   d_.lpiece_lvl = put(bufs_, S.forward.piece_lvl, st);
+  d_.lwarp_lvl = put(bufs_, S.forward.warp_lvl, st);
   d_.lcomb = put4(S.forward.comb);
   d_.lcomb_lvl = put(bufs_, S.forward.comb_lvl, st);
   d_.upiece = put4(S.backward.piece);
   d_.upiece_lvl = put(bufs_, S.backward.piece_lvl, st);
+  d_.uwarp_lvl = put(bufs_, S.backward.warp_lvl, st);
   d_.ucomb = put4(S.backward.comb);
   d_.ucomb_lvl = put(bufs_, S.backward.comb_lvl, st);
   d_.partial = put(bufs_, std::vector<double>(std::max(1, std::max(S.factor_slots, S.solve_slots)), 0.0), st);

@@ -35,14 +35,17 @@ struct SparseDev {
   // the work pieces and combine steps of sparse_schedule (sparse.hpp), per level
   const int4* fpiece;   // factor pieces (first, end: update range; target: index into V)
   const int* fpiece_lvl;  // levels + 1
+  const int* fwarp_lvl;   // levels: first piece of the level taken by a warp (earlier: a thread)
   const int4* fcomb;    // factor combines {target, first slot, slots, 0}
   const int* fcomb_lvl;   // levels + 1
   const int4* lpiece;   // forward pieces (first, end: range of row_pos / row_col; target: row k)
   const int* lpiece_lvl;
+  const int* lwarp_lvl;
   const int4* lcomb;
   const int* lcomb_lvl;
   const int4* upiece;   // backward pieces (first, end: range of li; target: column k)
   const int* upiece_lvl;
+  const int* uwarp_lvl;
   const int4* ucomb;
   const int* ucomb_lvl;
   double* partial;      // piece sums awaiting their combine step

@@ -76,6 +76,23 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
         return;
       }
   };
+  // per level: the thread-sized pieces (at most kSparseShort terms) first, then the warp pieces
+  auto split = [&](const SparsePieces& pc, const char* what) {
+    for (int h = 0; h < s.levels(); ++h) {
+      const int a = pc.piece_lvl[h], w = pc.warp_lvl[h], e = pc.piece_lvl[h + 1];
+      bool ok = a <= w && w <= e;
+      for (int q = a; ok && q < w; ++q) ok = pc.piece[q].end - pc.piece[q].first <= kSparseShort && pc.piece[q].slot < 0;
+      for (int q = w; ok && q < e; ++q) ok = pc.piece[q].end - pc.piece[q].first > kSparseShort || pc.piece[q].slot >= 0;
+      if (!ok) {
+        std::printf("%s: %s level %d mixes thread and warp pieces\n", name, what, h);
+        ++bad;
+        return;
+      }
+    }
+  };
+  split(P.factor, "factor");
+  split(P.forward, "forward");
+  split(P.backward, "backward");
   cover(P.factor, P.up_col.size(), "factor");
   cover(P.forward, P.row_pos.size(), "forward");
   cover(P.backward, s.li.size(), "backward");
