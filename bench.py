@@ -234,6 +234,31 @@ def run_single_workload(args):
               variants=lines, cpu_reference=ref,
               max_rel_obj_err_vs_reference=max(v["rel_obj_err_vs_reference"] for v in lines.values()))
         return
+    if args.workload == "kkt":
+        # a QP whose Hessian couples neighbours, at n = 200000 (KKT order 650001): the sparse
+        # quasi-definite KKT path; the reference's answer and its CPU time are a committed fixture
+        key = "coupled_chain_qp(200000,5)"
+        g = json.load(open(os.path.join(ROOT, "tests", "golden", "kkt_reference.json")))[key]
+        mdl = P.coupled_chain_qp(200000, 5)
+        r, wall, dev = timed(QpInteriorPointSolver(), mdl)
+        _line(METRIC, 1.0 / wall, UNIT, args, 1e3 * wall, "f64",
+              dict(workload="coupled chain QP n=200000 (tridiagonal Hessian, KKT order 650001), single QP"),
+              status=r.status_name, iterations=r.iterations, objective=r.objective_value, device_s=dev,
+              message=r.message[-160:],
+              max_rel_obj_err_vs_reference=abs(r.objective_value - g["objective"]) / max(1.0, abs(g["objective"])),
+              cpu_reference=dict(objective=g["objective"], seconds=g["seconds"], iterations=g["iterations"],
+                                 source="tests/golden/kkt_reference.json (reference QpInteriorPointSolver, sparse "
+                                        "quasi-definite KKT, one CPU thread)"))
+        return
+    if args.workload == "wide":
+        # an LP far wider than L2 (16M nonzeros): the single engine's HBM-bound passes
+        mdl = P.wide_lp(2000, 2_000_000, 8, 1)
+        r, wall, dev = timed(InteriorPointSolver(), mdl)
+        _line(METRIC, 1.0 / wall, UNIT, args, 1e3 * wall, "f64",
+              dict(workload="wide LP m=2000 n=2000000, 8 nnz/column (single LP)"),
+              status=r.status_name, iterations=r.iterations, objective=r.objective_value, device_s=dev,
+              message=r.message[-120:])
+        return
     if args.workload == "c2":
         mdl = P.convex_sequence_qp(20002, 2)
         r, wall, dev = timed(QpInteriorPointSolver(), mdl)
@@ -428,7 +453,7 @@ def main():
     ap.add_argument("--impl", default="sovereign_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=COUNT, help="LPs per step (profiling runs use fewer)")
-    ap.add_argument("--workload", default="batch", choices=["batch", "c0", "c1", "c2", "c3w", "c4"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "c0", "c1", "c2", "c3w", "c4", "kkt", "wide"],
                     help="batch (default, headline): 4096 uneven transportation LPs; c0: one 50x50 transportation "
                          "LP; c1: random LP m=2000 n=10000 (FP64 and mixed); c2: convex-sequence QP n=20002; "
                          "c3w: parametric 40x40 transportation family, batched, learned warm start vs cold; "

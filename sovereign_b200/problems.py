@@ -14,6 +14,9 @@ the CPU oracles always see the same arrays):
 * ``multicommodity``       a fixed random graph with arc capacities and costs, K commodities,
                            coupling (capacity) rows plus per-commodity conservation rows; each
                            instance perturbs demands and costs.
+* ``wide_lp``              an LP far wider than L2 (m = 2000, n = 2M, 8 nnz per column) for the
+                           HBM-bound passes of the single-problem engine.
+* ``budget_lp``            random_sparse_lp plus one dense budget row over all columns.
 * ``coupled_chain_qp``     min sum_i w_i/2 (x_{i+1} - x_i)^2 + sum_i d_i/2 x_i^2 - t'x over
                            0 <= x <= 2, a covering row per block of columns and one budget row:
                            a Hessian that couples neighbours (tridiagonal), the sparse coupled
@@ -158,6 +161,25 @@ def convex_sequence_qp(n: int, seed: int, target: np.ndarray | None = None,
     mdl.q_row_idx = np.arange(n, dtype=np.int32)
     mdl.q_values = np.ones(n)
     return mdl
+
+
+def wide_lp(m: int, n: int, k: int, seed: int) -> Model:
+    """An LP far wider than L2: n columns of k entries N(0,1), one in each of k bands of m/k rows
+    (rows sorted within a column), equality rows b = A x0, c = A'y0 + s0 (feasible, bounded). At
+    m = 2000, n = 2M, k = 8: 16M nonzeros, each pass over A streams ~200 MB from HBM."""
+    rng = np.random.default_rng(seed)
+    band = m // k
+    rows = (rng.integers(0, band, size=(n, k)) + np.arange(k)[None, :] * band).astype(np.int32)
+    vals = rng.standard_normal((n, k))
+    x0 = rng.uniform(0.1, 1.0, n)
+    y0 = rng.standard_normal(m)
+    s0 = rng.uniform(0.1, 1.0, n)
+    row_idx = np.ascontiguousarray(rows.reshape(-1))
+    values = np.ascontiguousarray(vals.reshape(-1))
+    col_ptr = np.arange(0, n * k + 1, k, dtype=np.int32)
+    b = np.bincount(row_idx, weights=values * np.repeat(x0, k), minlength=m)
+    c = (values * y0[row_idx]).reshape(n, k).sum(axis=1) + s0
+    return _lp(n, m, col_ptr, row_idx, values, c, b, np.full(m, EQ, dtype=np.int8), f"wide_lp_{m}x{n}")
 
 
 def budget_lp(m: int, n: int, k: int, seed: int, fraction: float = 0.2) -> Model:

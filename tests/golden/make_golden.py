@@ -149,6 +149,7 @@ def kkt():
         r = oracle.solve(mdl, qp=True, kind="reference")
         key = f"{name}({','.join(map(str, args))})"
         d = summarize(r)
+        d["seconds"] = r.solve_seconds
         d["primal_stride"] = KKT_STRIDE
         d["primal_sample"] = [float(v) for v in r.primal[::KKT_STRIDE]]
         out[key] = dict(spec=[name, args], **d)
