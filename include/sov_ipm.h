@@ -198,9 +198,12 @@ int sov_ipm_dims(const sov_model* model, int32_t qp, int32_t* n_ipm, int32_t* m_
 int sov_lp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
 
 /* One convex QP through the GPU IPM (QpInteriorPointSolver::solve, qp_interior_point.cpp:3123-3186).
- * Separable (diagonal) Hessians take the y-space normal equations A (Q + X^-1 S)^-1 A'; a Hessian
- * that couples variables is held dense as H = Q + X^-1 S (FP64 Cholesky on the GPU, at most 16384
- * IPM columns) and the same reduced system A H^-1 A' is formed from it. */
+ * Separable (diagonal) Hessians take the y-space normal equations A (Q + X^-1 S)^-1 A'. A Hessian
+ * that couples variables takes the quasi-definite KKT system [Q + X^-1 S + delta I, A'; A, -delta I]
+ * as a sparse L D L' on the GPU (QpKkt, :415-655: signed pivots, delta escalation, refinement) when
+ * Q is sparse, beyond 16384 IPM columns, or with SOV_FACTOR_SPARSE; small dense couplings are held
+ * dense as H = Q + X^-1 S and reduced to A H^-1 A'. A free variable without curvature always takes
+ * the KKT system. */
 int sov_qp_solve(const sov_model* model, const sov_options* opt, sov_result* result);
 
 /* count independent LPs in one persistent batched launch (one CTA per LP, the whole IPM loop
@@ -211,6 +214,18 @@ int sov_qp_solve(const sov_model* model, const sov_options* opt, sov_result* res
  * does not fit the batched kernel are solved one by one through sov_lp_solve. */
 int sov_lp_solve_batch(int32_t count, const sov_model* models, const sov_options* opt,
                        int32_t opt_stride, sov_result* results);
+
+/* A parametric family: count LPs that share the constraint matrix, bounds, row senses and sense
+ * of optimisation (only obj, obj_constant and rhs differ), solved together -- one symbolic analysis
+ * of the normal matrix for the family, and every kernel of an iteration (residuals, assembly of
+ * A D_k A', the sparse L D L' and its solves, directions, ratio tests, update) running over up to 64
+ * LPs at once with their vectors interleaved. Each LP follows sov_lp_solve's iteration, stopping
+ * test, best-iterate rule and warm-start safeguard; opt / opt_stride as in sov_lp_solve_batch (the
+ * LPs must agree on enable_scaling and fraction_to_boundary; precision and factorization are not
+ * used: the path is FP64 sparse L D L'). solve_seconds of each result is its chunk's time. LPs
+ * without rows go through sov_lp_solve. SOV_E_ARGUMENT when the models do not share the structure. */
+int sov_lp_solve_family(int32_t count, const sov_model* models, const sov_options* opt, int32_t opt_stride,
+                        sov_result* results);
 
 /* Device-resident batch: prepare once (host standard form + upload), solve many times (device
  * only, stream-ordered), read back. Used to time the solver with inputs already in HBM. opt and

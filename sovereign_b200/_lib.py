@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsovipm.s
 # every symbol include/sov_ipm.h declares
 EXPORTS = [
     "sov_default_lp_options", "sov_default_qp_options", "sov_ipm_dims", "sov_lp_solve", "sov_qp_solve",
-    "sov_lp_solve_batch", "sov_batch_create", "sov_batch_solve", "sov_batch_results", "sov_batch_stats",
+    "sov_lp_solve_batch", "sov_lp_solve_family", "sov_batch_create", "sov_batch_solve", "sov_batch_results", "sov_batch_stats",
     "sov_batch_transfer_bytes", "sov_batch_destroy", "sov_autotune", "sov_spmv_csc", "sov_normal_factor_solve", "sov_normal_factor_solve_noalloc", "sov_device_info",
     "sov_last_error", "sov_mlp_create", "sov_mlp_param_count", "sov_mlp_get_params", "sov_mlp_set_params",
     "sov_mlp_forward", "sov_mlp_predict_start", "sov_mlp_loss_grad", "sov_mlp_train", "sov_mlp_destroy",
@@ -52,6 +52,7 @@ def load(build_if_missing: bool = True):
     lib.sov_lp_solve.argtypes = [M, O, R]
     lib.sov_qp_solve.argtypes = [M, O, R]
     lib.sov_lp_solve_batch.argtypes = [C.c_int32, M, O, C.c_int32, R]
+    lib.sov_lp_solve_family.argtypes = [C.c_int32, M, O, C.c_int32, R]
     lib.sov_batch_create.argtypes = [C.c_int32, M, O, C.c_int32, C.POINTER(C.c_void_p)]
     lib.sov_batch_solve.argtypes = [C.c_void_p, C.c_void_p]
     lib.sov_batch_results.argtypes = [C.c_void_p, R]

@@ -18,6 +18,7 @@
 #include "common.cuh"
 #include "dense.cuh"
 #include "engine.hpp"
+#include "family.cuh"
 #include "ipm_kernels.cuh"
 #include "sov_ipm.h"
 #include "stdform.hpp"
@@ -317,6 +318,24 @@ int sov_lp_solve_batch(int32_t count, const sov_model* models, const sov_options
     int rc = check_device();
     if (rc) return rc;
     return sov::solve_batch(count, models, opt, opt_stride, results);
+  } catch (const sov::CudaError& e) {
+    return set_error(SOV_E_CUDA, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SOV_E_ARGUMENT, e.what());
+  }
+}
+
+int sov_lp_solve_family(int32_t count, const sov_model* models, const sov_options* opt, int32_t opt_stride,
+                        sov_result* results) {
+  if (count < 0 || (count > 0 && (!models || !results))) return set_error(SOV_E_ARGUMENT, "bad family arguments");
+  for (int k = 0; k < count; ++k) {
+    const int rc = validate(&models[k]);
+    if (rc) return rc;
+  }
+  try {
+    int rc = check_device();
+    if (rc) return rc;
+    return sov::solve_family(count, models, opt, opt_stride, results);
   } catch (const sov::CudaError& e) {
     return set_error(SOV_E_CUDA, e.what());
   } catch (const std::exception& e) {

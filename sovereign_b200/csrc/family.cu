@@ -1,0 +1,1334 @@
+// family.cu -- a family of LPs sharing A, solved W at a time in lockstep (see family.cuh).
+#include "family.cuh"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.hpp"
+#include "sparse.hpp"
+#include "stdform.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace sov {
+namespace {
+
+constexpr int kFamThreads = 256;
+constexpr int kFamBlocks = 592;  // 4 CTAs per SM for the grid-stride passes with reductions
+constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the default restart
+constexpr int kNv = 3;           // reduction slots per pass
+
+// Per-LP scalars of one iteration (the single engine's IpmScalars for an LP).
+struct FamScalars {
+  double rp_max, rd_max, xs, cx, mu, p_res, d_res, gap, metric;
+  double ratio_p, ratio_d, alpha_p_aff, alpha_d_aff, mu_aff, sigma, alpha_p, alpha_d;
+  int fail, drops, skipped, pad;
+};
+
+struct FamDev {
+  int m, n, W, G;  // rows, columns, LPs in the chunk, LPs' entries per CTA (blockDim = W * G)
+  const int *row_ptr, *col_idx, *col_ptr, *row_idx;
+  const double *rval, *cval;
+  const double *b, *c;          // m x W, n x W (interleaved: entry-major, LP fastest)
+  const double *bnorm, *cnorm;  // W
+  double *x, *s, *y;
+  double *dx, *ds, *dxa, *dsa, *rd, *rp, *z, *t;
+  FamScalars* sc;    // W
+  const int* step;   // W: 1 when the LP takes this iteration's step
+  double* part;      // reduction partials: kFamBlocks x kNv x W
+  double tau;
+};
+
+// The normal matrices' shared symbolic factor and schedule, values per LP (interleaved).
+struct FamSparse {
+  int m, levels, W;
+  int tail, mt;             // dense trailing block: columns mt .. m-1, factored and solved densely
+  const int* tail_off;      // tail: index into V of column mt + q's first L entry (row mt + q + 1)
+  const int *pivot_ptr, *pivot_col;  // the columns before the tail, per level
+  double *V, *diag, *inv_d, *work, *partial;  // (m + nnz(L)) x W, m x W, m x W, m x W, slots x W
+  const int *perm, *lvl_ptr, *lvl_col, *li;
+  const int4 *fpiece, *fcomb, *lpiece, *lcomb, *upiece, *ucomb;
+  const int *fpiece_lvl, *fcomb_lvl, *lpiece_lvl, *lcomb_lvl, *upiece_lvl, *ucomb_lvl;
+  const int *up_col, *up_a, *up_b, *row_pos, *row_col;
+  FamScalars* sc;
+  double drop_tol;
+};
+
+struct FamAssembly {
+  const int* target;  // into [D | L]
+  const int* ptr;
+  const int* col;
+  const double* w;
+  int ntargets;
+};
+
+// thread -> (first item, LP) of the grid-stride loops: items advance by gridDim.x * G
+struct Lane {
+  int item, k, stride;
+};
+__device__ __forceinline__ Lane lane_of(const FamDev& d) {
+  return Lane{static_cast<int>(blockIdx.x) * d.G + static_cast<int>(threadIdx.x) / d.W,
+              static_cast<int>(threadIdx.x) % d.W, static_cast<int>(gridDim.x) * d.G};
+}
+
+// Combine this thread's values over the CTA's G items per LP (in item order) and leave the CTA's
+// result in part[(block * kNv + q) * W + k]. ops: 0 sum, 1 max, 2 min.
+template <int NV>
+__device__ void cta_partials(const FamDev& d, double (&v)[NV], const int (&ops)[NV], double* sm) {
+  const int tid = threadIdx.x, bd = blockDim.x;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) sm[q * bd + tid] = v[q];
+  __syncthreads();
+  if (tid < d.W) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double acc = sm[q * bd + tid];
+      for (int g = 1; g < d.G; ++g) {
+        const double u = sm[q * bd + g * d.W + tid];
+        acc = ops[q] == 0 ? acc + u : ops[q] == 1 ? fmax(acc, u) : fmin(acc, u);
+      }
+      d.part[(static_cast<size_t>(blockIdx.x) * kNv + q) * d.W + tid] = acc;
+    }
+  }
+}
+
+// the blocks' partials of slot q for LP k, in block order
+__device__ __forceinline__ double fold(const FamDev& d, int blocks, int q, int k, int op, double init) {
+  double acc = init;
+  for (int b = 0; b < blocks; ++b) {
+    const double u = d.part[(static_cast<size_t>(b) * kNv + q) * d.W + k];
+    acc = op == 0 ? acc + u : op == 1 ? fmax(acc, u) : fmin(acc, u);
+  }
+  return acc;
+}
+
+// ---- residuals: rp = b - A x, rd = c - (A'y + s) (interior_point.cpp:572-602) ----
+__global__ void k_fam_res_rows(FamDev d) {
+  extern __shared__ double sm[];
+  const Lane L = lane_of(d);
+  double mx = 0.0;
+  for (int i = L.item; i < d.m; i += L.stride) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i]; p < d.row_ptr[i + 1]; ++p) acc += d.rval[p] * d.x[static_cast<size_t>(d.col_idx[p]) * d.W + L.k];
+    const size_t e = static_cast<size_t>(i) * d.W + L.k;
+    const double r = d.b[e] - acc;
+    d.rp[e] = r;
+    mx = fmax(mx, fabs(r));
+  }
+  double v[1] = {mx};
+  const int ops[1] = {1};
+  cta_partials<1>(d, v, ops, sm);
+}
+
+__global__ void k_fam_res_cols(FamDev d) {
+  extern __shared__ double sm[];
+  const Lane L = lane_of(d);
+  double rdm = 0.0, xs = 0.0, cx = 0.0;
+  for (int j = L.item; j < d.n; j += L.stride) {
+    double aty = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) aty += d.cval[p] * d.y[static_cast<size_t>(d.row_idx[p]) * d.W + L.k];
+    const size_t e = static_cast<size_t>(j) * d.W + L.k;
+    const double xj = d.x[e], sj = d.s[e];
+    const double r = d.c[e] - (aty + sj);
+    d.rd[e] = r;
+    rdm = fmax(rdm, fabs(r));
+    xs += xj * sj;
+    cx += d.c[e] * xj;
+  }
+  double v[3] = {rdm, xs, cx};
+  const int ops[3] = {1, 0, 0};
+  cta_partials<3>(d, v, ops, sm);
+}
+
+// one thread per LP: rows' and columns' partials (two part buffers) into the scalars
+__global__ void k_fam_res_final(FamDev d, const double* rows_part, int rows_blocks, int cols_blocks) {
+  const int k = threadIdx.x;
+  if (k >= d.W) return;
+  double rpm = 0.0;
+  for (int b = 0; b < rows_blocks; ++b) rpm = fmax(rpm, rows_part[(static_cast<size_t>(b) * kNv) * d.W + k]);
+  const double rdm = fold(d, cols_blocks, 0, k, 1, 0.0);
+  const double xs = fold(d, cols_blocks, 1, k, 0, 0.0);
+  const double cx = fold(d, cols_blocks, 2, k, 0, 0.0);
+  FamScalars& sc = d.sc[k];
+  sc.rp_max = rpm;
+  sc.rd_max = rdm;
+  sc.xs = xs;
+  sc.cx = cx;
+  sc.p_res = rpm / d.bnorm[k];
+  sc.mu = xs / static_cast<double>(d.n);
+  sc.d_res = rdm / d.cnorm[k];
+  sc.gap = fabs(xs) / (1.0 + fabs(cx));
+  sc.metric = fmax(sc.p_res, fmax(sc.d_res, sc.gap));
+}
+
+// ---- Newton step (interior_point.cpp:418-452, 640-690) ----
+// rxs of the current mode: affine -x s; corrector -x s - dxa dsa + sigma mu
+__device__ __forceinline__ double fam_rxs(const FamDev& d, int mode, size_t e, double sigma_mu) {
+  const double xj = d.x[e], sj = d.s[e];
+  if (mode == 0) return -xj * sj;
+  return -xj * sj - d.dxa[e] * d.dsa[e] + sigma_mu;
+}
+
+// t = d rd - rxs / s per column (d = x/s with the 1e-16 floors)
+__global__ void k_fam_newton_tmp(FamDev d, int mode) {
+  const Lane L = lane_of(d);
+  const double sigma_mu = mode == 1 ? d.sc[L.k].sigma * d.sc[L.k].mu : 0.0;
+  for (int j = L.item; j < d.n; j += L.stride) {
+    const size_t e = static_cast<size_t>(j) * d.W + L.k;
+    const double xj = fmax(d.x[e], 1e-16), sj = fmax(d.s[e], 1e-16);
+    d.t[e] = (xj / sj) * d.rd[e] - fam_rxs(d, mode, e, sigma_mu) / sj;
+  }
+}
+
+// z = rp + A t
+__global__ void k_fam_newton_rhs(FamDev d) {
+  const Lane L = lane_of(d);
+  for (int i = L.item; i < d.m; i += L.stride) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i]; p < d.row_ptr[i + 1]; ++p) acc += d.rval[p] * d.t[static_cast<size_t>(d.col_idx[p]) * d.W + L.k];
+    const size_t e = static_cast<size_t>(i) * d.W + L.k;
+    d.z[e] = d.rp[e] + acc;
+  }
+}
+
+// dx = d (A'dy - rd) + rxs / s, ds = rd - A'dy with dy = z; ratio tests (step_to_bound from 1)
+__global__ void k_fam_direction(FamDev d, int mode) {
+  extern __shared__ double sm[];
+  const Lane L = lane_of(d);
+  const double sigma_mu = mode == 1 ? d.sc[L.k].sigma * d.sc[L.k].mu : 0.0;
+  double* dxo = mode == 0 ? d.dxa : d.dx;
+  double* dso = mode == 0 ? d.dsa : d.ds;
+  double rp_min = 1.0, rd_min = 1.0;
+  for (int j = L.item; j < d.n; j += L.stride) {
+    double atdy = 0.0;
+    for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[static_cast<size_t>(d.row_idx[p]) * d.W + L.k];
+    const size_t e = static_cast<size_t>(j) * d.W + L.k;
+    const double xj = d.x[e], sj = d.s[e];
+    const double rxs = fam_rxs(d, mode, e, sigma_mu);
+    const double dj = fmax(xj, 1e-16) / fmax(sj, 1e-16);
+    const double dxj = dj * (atdy - d.rd[e]) + rxs / fmax(sj, 1e-16);
+    const double dsj = d.rd[e] - atdy;
+    dxo[e] = dxj;
+    dso[e] = dsj;
+    if (dxj < 0.0) rp_min = fmin(rp_min, -xj / dxj);
+    if (dsj < 0.0) rd_min = fmin(rd_min, -sj / dsj);
+  }
+  double v[2] = {rp_min, rd_min};
+  const int ops[2] = {2, 2};
+  cta_partials<2>(d, v, ops, sm);
+}
+
+__global__ void k_fam_direction_final(FamDev d, int mode, int blocks) {
+  const int k = threadIdx.x;
+  if (k >= d.W) return;
+  const double rp = fold(d, blocks, 0, k, 2, 1.0), rdd = fold(d, blocks, 1, k, 2, 1.0);
+  FamScalars& sc = d.sc[k];
+  sc.ratio_p = rp;
+  sc.ratio_d = rdd;
+  if (mode == 0) {
+    sc.alpha_p_aff = rp;
+    sc.alpha_d_aff = rdd;
+  } else {
+    sc.alpha_p = fmin(1.0, d.tau * rp);
+    sc.alpha_d = fmin(1.0, d.tau * rdd);
+  }
+}
+
+// mu_aff = sum (x + ap dxa)(s + ad dsa) / n, sigma = (mu_aff / mu)^3 (interior_point.cpp:660-673)
+__global__ void k_fam_mu_aff(FamDev d) {
+  extern __shared__ double sm[];
+  const Lane L = lane_of(d);
+  const double ap = d.sc[L.k].alpha_p_aff, ad = d.sc[L.k].alpha_d_aff;
+  double acc = 0.0;
+  for (int j = L.item; j < d.n; j += L.stride) {
+    const size_t e = static_cast<size_t>(j) * d.W + L.k;
+    acc += (d.x[e] + ap * d.dxa[e]) * (d.s[e] + ad * d.dsa[e]);
+  }
+  double v[1] = {acc};
+  const int ops[1] = {0};
+  cta_partials<1>(d, v, ops, sm);
+}
+
+__global__ void k_fam_mu_final(FamDev d, int blocks) {
+  const int k = threadIdx.x;
+  if (k >= d.W) return;
+  FamScalars& sc = d.sc[k];
+  sc.mu_aff = fold(d, blocks, 0, k, 0, 0.0) / static_cast<double>(d.n);
+  const double r = sc.mu_aff / sc.mu;
+  sc.sigma = sc.mu > 0.0 ? fmin(1.0, r * r * r) : 0.0;
+}
+
+// x, s, y step (interior_point.cpp:692-699); an LP whose factorization failed is not moved
+__global__ void k_fam_update(FamDev d) {
+  const Lane L = lane_of(d);
+  const int k = L.k;
+  if (!d.step[k]) return;
+  const FamScalars& sc = d.sc[k];
+  if (sc.fail) {
+    if (L.item == 0) d.sc[k].skipped = 1;
+    return;
+  }
+  const double ap = sc.alpha_p, ad = sc.alpha_d;
+  const int N = d.n > d.m ? d.n : d.m;
+  for (int j = L.item; j < N; j += L.stride) {
+    const size_t e = static_cast<size_t>(j) * d.W + k;
+    if (j < d.n) {
+      d.x[e] = fmax(d.x[e] + ap * d.dx[e], 1e-14);
+      d.s[e] = fmax(d.s[e] + ad * d.ds[e], 1e-14);
+    }
+    if (j < d.m) d.y[e] += ad * d.z[e];
+  }
+}
+
+// ---- Mehrotra-like start (interior_point.cpp:488-506): A A' dy = b - A 1 ----
+__global__ void k_fam_start_rhs(FamDev d) {
+  const Lane L = lane_of(d);
+  for (int i = L.item; i < d.m; i += L.stride) {
+    double acc = 0.0;
+    for (int p = d.row_ptr[i]; p < d.row_ptr[i + 1]; ++p) acc += d.rval[p];
+    const size_t e = static_cast<size_t>(i) * d.W + L.k;
+    d.z[e] = d.b[e] - acc;
+  }
+}
+
+// x = max(1, |A'dy|), s = max(1, |c - A'dy|), y = dy (all 1 / 0 when the factorization failed),
+// into (x, y, s) = the pointers given (the start is kept for restarts)
+__global__ void k_fam_start_point(FamDev d, double* x, double* y, double* s) {
+  const Lane L = lane_of(d);
+  const bool ok = !d.sc[L.k].fail;
+  const int N = d.n > d.m ? d.n : d.m;
+  for (int j = L.item; j < N; j += L.stride) {
+    const size_t e = static_cast<size_t>(j) * d.W + L.k;
+    if (j < d.n) {
+      double xs = 1.0, ss = 1.0;
+      if (ok) {
+        double atdy = 0.0;
+        for (int p = d.col_ptr[j]; p < d.col_ptr[j + 1]; ++p) atdy += d.cval[p] * d.z[static_cast<size_t>(d.row_idx[p]) * d.W + L.k];
+        xs = fmax(1.0, fabs(atdy));
+        ss = fmax(1.0, fabs(d.c[e] - atdy));
+      }
+      x[e] = xs;
+      s[e] = ss;
+    }
+    if (j < d.m) y[e] = ok ? d.z[e] : 0.0;
+  }
+}
+
+// dst = src for the LPs with mask[k] (count entries per LP)
+__global__ void k_fam_copy(int count, int W, const int* mask, double* dst, const double* src) {
+  const long long total = static_cast<long long>(count) * W;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x)
+    if (mask[t % W]) dst[t] = src[t];
+}
+
+// ---- normal matrices A D_k A' + 1e-12 I into the shared pattern (LP weights x/s, or 1) ----
+__global__ void k_fam_assemble(FamAssembly am, FamDev d, FamSparse f, int ones) {
+  const long long total = static_cast<long long>(am.ntargets) * d.W;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int q = static_cast<int>(t / d.W), k = static_cast<int>(t % d.W);
+    double acc = 0.0;
+    for (int p = am.ptr[q]; p < am.ptr[q + 1]; ++p) {
+      const size_t e = static_cast<size_t>(am.col[p]) * d.W + k;
+      acc += am.w[p] * (ones ? 1.0 : fmax(d.x[e], 1e-16) / fmax(d.s[e], 1e-16));
+    }
+    const int tg = am.target[q];
+    if (tg < f.m) {
+      acc += 1e-12;  // kNormalEqRegularization (interior_point.cpp:103)
+      f.diag[static_cast<size_t>(tg) * d.W + k] = acc;
+    }
+    f.V[static_cast<size_t>(tg) * d.W + k] = acc;
+  }
+}
+
+// ---- L D L' of every LP's normal matrix on the shared schedule (sparse_gpu.cu's walk, one
+// thread per (work piece, LP); each piece's terms summed in order) ----
+__global__ void __launch_bounds__(kFamThreads) k_fam_factor(FamSparse f) {
+  cg::grid_group g = cg::this_grid();
+  const long long rank = g.thread_rank(), size = g.size();
+  const int W = f.W;
+  for (int h = 0; h < f.levels; ++h) {
+    const long long cols = static_cast<long long>(f.pivot_ptr[h + 1] - f.pivot_ptr[h]) * W;
+    for (long long t = rank; t < cols; t += size) {
+      const int k = static_cast<int>(t % W);
+      const int c = f.pivot_col[f.pivot_ptr[h] + static_cast<int>(t / W)];
+      const size_t e = static_cast<size_t>(c) * W + k;
+      const double p = f.V[e];
+      const bool finite = fabs(p) <= 1.7976931348623157e308;
+      // dependent row: pivot <= 1e-13 |assembled diagonal| (sparse_ldlt.cpp:165-173)
+      const bool drop = !(finite && p > f.drop_tol * fabs(f.diag[e]));
+      if (drop) atomicAdd(&f.sc[k].drops, 1);
+      if (!finite) atomicExch(&f.sc[k].fail, 1);
+      f.inv_d[e] = 1.0 / (drop ? 1e128 : p);
+    }
+    g.sync();
+    const long long pieces = static_cast<long long>(f.fpiece_lvl[h + 1] - f.fpiece_lvl[h]) * W;
+    for (long long t = rank; t < pieces; t += size) {
+      const int k = static_cast<int>(t % W);
+      const int4 pc = f.fpiece[f.fpiece_lvl[h] + static_cast<int>(t / W)];
+      double acc = 0.0;
+      for (int u = pc.x; u < pc.y; ++u)
+        acc += f.V[static_cast<size_t>(f.m + f.up_a[u]) * W + k] * f.V[static_cast<size_t>(f.m + f.up_b[u]) * W + k] *
+               f.inv_d[static_cast<size_t>(f.up_col[u]) * W + k];
+      if (pc.w < 0) f.V[static_cast<size_t>(pc.z) * W + k] -= acc;
+      else f.partial[static_cast<size_t>(pc.w) * W + k] = acc;
+    }
+    if (f.fcomb_lvl[h + 1] > f.fcomb_lvl[h]) {  // uniform over the grid
+      g.sync();
+      const long long combs = static_cast<long long>(f.fcomb_lvl[h + 1] - f.fcomb_lvl[h]) * W;
+      for (long long t = rank; t < combs; t += size) {
+        const int k = static_cast<int>(t % W);
+        const int4 cb = f.fcomb[f.fcomb_lvl[h] + static_cast<int>(t / W)];
+        double acc = 0.0;
+        for (int q = 0; q < cb.z; ++q) acc += f.partial[static_cast<size_t>(cb.y + q) * W + k];
+        f.V[static_cast<size_t>(cb.x) * W + k] -= acc;
+      }
+    }
+    g.sync();
+  }
+}
+
+// ---- the dense tail (the root clique of the elimination tree), factored per LP by panels of
+// kPanel columns: the panel's diagonal block, the rows below it, then the trailing block's
+// update -- the same operations per entry, in the same column order, as the level schedule ----
+constexpr int kPanel = 16;
+
+__device__ __forceinline__ size_t tail_at(const FamSparse& f, int a, int q, int lp) {  // L~_aq, a > q
+  return static_cast<size_t>(f.tail_off[q] + (a - q - 1)) * f.W + lp;
+}
+
+// one CTA of P x W threads (row r of the panel, LP)
+__global__ void k_tail_diag(FamSparse f, int j0, int j1) {
+  const int W = f.W, P = j1 - j0;
+  const int r = static_cast<int>(threadIdx.x) / W, lp = static_cast<int>(threadIdx.x) % W;
+  const bool on = r < P;
+  for (int j = 0; j < P; ++j) {
+    __syncthreads();
+    if (on && r == j) {
+      const size_t e = static_cast<size_t>(f.mt + j0 + j) * W + lp;
+      const double p = f.V[e];
+      const bool finite = fabs(p) <= 1.7976931348623157e308;
+      const bool drop = !(finite && p > f.drop_tol * fabs(f.diag[e]));
+      if (drop) atomicAdd(&f.sc[lp].drops, 1);
+      if (!finite) atomicExch(&f.sc[lp].fail, 1);
+      f.inv_d[e] = 1.0 / (drop ? 1e128 : p);
+    }
+    __syncthreads();
+    if (on && r > j) {
+      const double lrj = f.V[tail_at(f, j0 + r, j0 + j, lp)];
+      const double inv = f.inv_d[static_cast<size_t>(f.mt + j0 + j) * W + lp];
+      for (int c = j + 1; c <= r; ++c) {
+        const size_t dst = c == r ? static_cast<size_t>(f.mt + j0 + r) * W + lp : tail_at(f, j0 + r, j0 + c, lp);
+        f.V[dst] -= lrj * f.V[tail_at(f, j0 + c, j0 + j, lp)] * inv;
+      }
+    }
+  }
+}
+
+// rows a >= j1 of the panel's columns: the in-panel recurrence on the row held in registers
+__global__ void k_tail_rows(FamSparse f, int j0, int j1) {
+  const int W = f.W, P = j1 - j0;
+  const long long total = static_cast<long long>(f.tail - j1) * W;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int a = j1 + static_cast<int>(t / W), lp = static_cast<int>(t % W);
+    double l[kPanel];
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) l[c] = c < P ? f.V[tail_at(f, a, j0 + c, lp)] : 0.0;
+#pragma unroll
+    for (int j = 1; j < kPanel; ++j) {
+      if (j >= P) break;
+      double v = l[j];
+#pragma unroll
+      for (int c = 0; c < kPanel; ++c) {
+        if (c >= j) break;
+        v -= l[c] * f.V[tail_at(f, j0 + j, j0 + c, lp)] * f.inv_d[static_cast<size_t>(f.mt + j0 + c) * W + lp];
+      }
+      l[j] = v;
+    }
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c)
+      if (c < P) f.V[tail_at(f, a, j0 + c, lp)] = l[c];
+  }
+}
+
+// the trailing block: entry (a, b), j1 <= b <= a, takes the panel's rank-P update
+__global__ void k_tail_update(FamSparse f, int j0, int j1) {
+  const int W = f.W, P = j1 - j0, n = f.tail - j1;
+  const long long pairs = static_cast<long long>(n) * (n + 1) / 2, total = pairs * W;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long pr = t / W;
+    const int lp = static_cast<int>(t % W);
+    long long ai = static_cast<long long>((sqrt(8.0 * static_cast<double>(pr) + 1.0) - 1.0) * 0.5);
+    while (ai * (ai + 1) / 2 > pr) --ai;
+    while ((ai + 1) * (ai + 2) / 2 <= pr) ++ai;
+    const int a = j1 + static_cast<int>(ai), b = j1 + static_cast<int>(pr - ai * (ai + 1) / 2);
+    double acc = 0.0;
+    for (int c = 0; c < P; ++c)
+      acc += f.V[tail_at(f, a, j0 + c, lp)] * f.V[tail_at(f, b, j0 + c, lp)] *
+             f.inv_d[static_cast<size_t>(f.mt + j0 + c) * W + lp];
+    const size_t dst = a == b ? static_cast<size_t>(f.mt + a) * W + lp : tail_at(f, a, b, lp);
+    f.V[dst] -= acc;
+  }
+}
+
+// L D L' w = z for every LP, z (original row order, interleaved) in place
+__global__ void __launch_bounds__(kFamThreads) k_fam_solve(FamSparse f, double* z) {
+  cg::grid_group g = cg::this_grid();
+  const long long rank = g.thread_rank(), size = g.size();
+  const int W = f.W;
+  const long long mw = static_cast<long long>(f.m) * W;
+  for (long long t = rank; t < mw; t += size)
+    f.work[t] = z[static_cast<size_t>(f.perm[t / W]) * W + t % W];
+  g.sync();
+  const int fwd_levels = f.levels + (f.tail > 0 ? 1 : 0);  // + the tail rows' sums before the tail
+  for (int h = 0; h < fwd_levels; ++h) {
+    const long long pieces = static_cast<long long>(f.lpiece_lvl[h + 1] - f.lpiece_lvl[h]) * W;
+    for (long long t = rank; t < pieces; t += size) {
+      const int k = static_cast<int>(t % W);
+      const int4 pc = f.lpiece[f.lpiece_lvl[h] + static_cast<int>(t / W)];
+      double acc = 0.0;
+      for (int q = pc.x; q < pc.y; ++q) {
+        const size_t c = static_cast<size_t>(f.row_col[q]) * W + k;
+        acc += f.V[static_cast<size_t>(f.m + f.row_pos[q]) * W + k] * f.inv_d[c] * f.work[c];
+      }
+      if (pc.w < 0) f.work[static_cast<size_t>(pc.z) * W + k] -= acc;
+      else f.partial[static_cast<size_t>(pc.w) * W + k] = acc;
+    }
+    if (f.lcomb_lvl[h + 1] > f.lcomb_lvl[h]) {
+      g.sync();
+      const long long combs = static_cast<long long>(f.lcomb_lvl[h + 1] - f.lcomb_lvl[h]) * W;
+      for (long long t = rank; t < combs; t += size) {
+        const int k = static_cast<int>(t % W);
+        const int4 cb = f.lcomb[f.lcomb_lvl[h] + static_cast<int>(t / W)];
+        double acc = 0.0;
+        for (int q = 0; q < cb.z; ++q) acc += f.partial[static_cast<size_t>(cb.y + q) * W + k];
+        f.work[static_cast<size_t>(cb.x) * W + k] -= acc;
+      }
+    }
+    g.sync();
+  }
+  if (f.tail > 0) {
+    // the dense tail, forward then backward, column by column: CTA b takes LPs 32b .. 32b + 31
+    // (lane = LP), its 8 warps split the rows; the other CTAs go straight to the barrier
+    const int lanes = 32, groups = kFamThreads / 32;
+    const int lp = static_cast<int>(blockIdx.x) * lanes + (threadIdx.x & 31), grp = threadIdx.x >> 5;
+    if (static_cast<int>(blockIdx.x) * lanes < W) {
+      const bool on = lp < W;
+      const int T = f.tail, mt = f.mt;
+      auto tl = [&](int a, int q) { return static_cast<size_t>(f.tail_off[q] + (a - q - 1)) * W + lp; };
+      for (int q = 0; q < T; ++q) {  // forward: y_a -= L~_aq / D_q y_q for a > q
+        __syncthreads();
+        if (on) {
+          const size_t eq = static_cast<size_t>(mt + q) * W + lp;
+          const double coef = f.work[eq] * f.inv_d[eq];
+          for (int a = q + 1 + grp; a < T; a += groups) f.work[static_cast<size_t>(mt + a) * W + lp] -= f.V[tl(a, q)] * coef;
+        }
+      }
+      // every thread of the CTA passes every barrier (LPs past W only skip the work between them)
+      for (int q = T - 1; q >= 0; --q) {  // backward: x_q = y'_q / D_q, then y'_a -= L~_qa x_q for a < q
+        __syncthreads();
+        const size_t eq = static_cast<size_t>(mt + q) * W + lp;
+        const double xq = on ? f.work[eq] * f.inv_d[eq] : 0.0;
+        __syncthreads();
+        if (on) {
+          if (grp == 0) f.work[eq] = xq;
+          for (int a = grp; a < q; a += groups) f.work[static_cast<size_t>(mt + a) * W + lp] -= f.V[tl(q, a)] * xq;
+        }
+      }
+    }
+    g.sync();
+  }
+  for (int h = f.levels - 1; h >= 0; --h) {
+    const long long pieces = static_cast<long long>(f.upiece_lvl[h + 1] - f.upiece_lvl[h]) * W;
+    for (long long t = rank; t < pieces; t += size) {
+      const int k = static_cast<int>(t % W);
+      const int4 pc = f.upiece[f.upiece_lvl[h] + static_cast<int>(t / W)];
+      double acc = 0.0;
+      for (int p = pc.x; p < pc.y; ++p)
+        acc += f.V[static_cast<size_t>(f.m + p) * W + k] * f.work[static_cast<size_t>(f.li[p]) * W + k];
+      const size_t e = static_cast<size_t>(pc.z) * W + k;
+      if (pc.w < 0) f.work[e] = (f.work[e] - acc) * f.inv_d[e];
+      else f.partial[static_cast<size_t>(pc.w) * W + k] = acc;
+    }
+    if (f.ucomb_lvl[h + 1] > f.ucomb_lvl[h]) {
+      g.sync();
+      const long long combs = static_cast<long long>(f.ucomb_lvl[h + 1] - f.ucomb_lvl[h]) * W;
+      for (long long t = rank; t < combs; t += size) {
+        const int k = static_cast<int>(t % W);
+        const int4 cb = f.ucomb[f.ucomb_lvl[h] + static_cast<int>(t / W)];
+        double acc = 0.0;
+        for (int q = 0; q < cb.z; ++q) acc += f.partial[static_cast<size_t>(cb.y + q) * W + k];
+        const size_t e = static_cast<size_t>(cb.x) * W + k;
+        f.work[e] = (f.work[e] - acc) * f.inv_d[e];
+      }
+    }
+    g.sync();
+  }
+  for (long long t = rank; t < mw; t += size) z[static_cast<size_t>(f.perm[t / W]) * W + t % W] = f.work[t];
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+
+template <class T>
+struct Buf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free_();
+    n = count;
+    SOV_CUDA(cudaMalloc(&p, sizeof(T) * std::max<size_t>(1, count)));
+  }
+  void put(const std::vector<T>& h, cudaStream_t st) {
+    alloc(h.size());
+    if (!h.empty()) SOV_CUDA(cudaMemcpyAsync(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st));
+  }
+  void free_() {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+  ~Buf() { free_(); }
+};
+
+// the arrays a family shares, compared entry by entry (null bounds are the defaults)
+bool same_structure(const sov_model& a, const sov_model& b) {
+  if (a.n != b.n || a.m != b.m || a.maximize != b.maximize) return false;
+  if (!std::equal(a.col_ptr, a.col_ptr + a.n + 1, b.col_ptr)) return false;
+  const int nnz = a.col_ptr[a.n];
+  if (!std::equal(a.row_idx, a.row_idx + nnz, b.row_idx) || !std::equal(a.values, a.values + nnz, b.values))
+    return false;
+  if (!std::equal(a.sense, a.sense + a.m, b.sense)) return false;
+  auto bounds = [&](const double* x, const double* y, double def) {
+    for (int j = 0; j < a.n; ++j)
+      if ((x ? x[j] : def) != (y ? y[j] : def)) return false;
+    return true;
+  };
+  return bounds(a.lb, b.lb, 0.0) && bounds(a.ub, b.ub, 1e30);
+}
+
+// what the chunk loop keeps per LP (the single engine's per-solve state, Engine::run)
+struct LpState {
+  int idx = -1;
+  sov_options o{};
+  bool active = true, warm_used = false, captured = false, optimal = false;
+  int best_it = 0, stale = 0, factorizations = 0, its = 0;
+  double best_metric = INFINITY, best_gap = INFINITY, best_p = INFINITY, best_d = INFINITY;
+  double gap = 0, p_res = 0, d_res = 0;
+  std::string msg;
+  sov_diagnostics dg{};
+};
+
+class Family {
+ public:
+  Family(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results)
+      : count_(count), models_(models), results_(results) {
+    opts_.resize(count);
+    for (int k = 0; k < count; ++k) {
+      if (!opt) sov_default_lp_options(&opts_[k]);
+      else opts_[k] = *reinterpret_cast<const sov_options*>(reinterpret_cast<const char*>(opt) +
+                                                          static_cast<size_t>(opt_stride) * k);
+    }
+  }
+  ~Family() {
+    if (st_) cudaStreamDestroy(st_);
+    if (hsc_) cudaFreeHost(hsc_);
+  }
+  int run();
+
+ private:
+  void setup_shared(const StdForm& f);
+  void solve_chunk(const std::vector<int>& lps);
+  void publish(LpState& L, const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& s,
+               const std::vector<double>& cx, const std::vector<double>& cy, const std::vector<double>& cs, int k,
+               int W, double seconds);
+  std::string describe() const;
+  // launches over (entries, LPs)
+  int grid_for(int items) const { return std::max(1, std::min(kFamBlocks, (items + dev_.G - 1) / dev_.G)); }
+  void residuals();
+  void factor();
+  void solve(double* z);
+  void assemble(bool ones);
+  void copy(int entries, const int* mask_dev, double* dst, const double* src);
+
+  int count_;
+  const sov_model* models_;
+  sov_result* results_;
+  std::vector<sov_options> opts_;
+  std::vector<StdForm> forms_;
+  cudaStream_t st_ = nullptr;
+  int sms_ = 148, per_sm_factor_ = 1, per_sm_solve_ = 1;
+  // shared structure
+  SparseSymbolic sym_;
+  Buf<int> row_ptr_, col_idx_, col_ptr_, row_idx_, asm_target_, asm_ptr_, asm_col_;
+  Buf<double> rval_, cval_, asm_w_;
+  Buf<int> perm_, lvl_ptr_, lvl_col_, li_, up_col_, up_a_, up_b_, row_pos_, row_col_;
+  Buf<int> fpl_, fcl_, lpl_, lcl_, upl_, ucl_, tail_off_, pivot_ptr_, pivot_col_;
+  int tail_ = 0;
+  static constexpr int kMinTail = 32;  // smaller root cliques stay in the level schedule
+  Buf<int4> fp_, fc_, lpc_, lc_, upc_, uc_;
+  // per chunk (capacity kFamilyWidth LPs)
+  Buf<double> b_, c_, bnorm_, cnorm_, x_, s_, y_, dx_, ds_, dxa_, dsa_, rd_, rp_, z_, t_;
+  Buf<double> x0_, y0_, s0_, bx_, by_, bs_, cx_, cy_, cs_, part_, part_rows_;
+  Buf<double> V_, diag_, inv_d_, work_, partial_;
+  Buf<FamScalars> sc_;
+  Buf<int> step_, mask_;
+  FamScalars* hsc_ = nullptr;
+  FamDev dev_{};
+  FamSparse sp_{};
+  FamAssembly am_{};
+  int slots_ = 1;
+};
+
+int Family::run() {
+  for (int k = 1; k < count_; ++k)
+    if (!same_structure(models_[0], models_[k]))
+      throw std::invalid_argument("sov_lp_solve_family: LP " + std::to_string(k) +
+                                  " does not share the first LP's constraint matrix, bounds and row senses");
+  for (int k = 1; k < count_; ++k)
+    if (opts_[k].enable_scaling != opts_[0].enable_scaling ||
+        opts_[k].fraction_to_boundary != opts_[0].fraction_to_boundary)
+      throw std::invalid_argument("sov_lp_solve_family: every LP of a family takes the same scaling option and "
+                                  "fraction to the boundary");
+  SOV_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  // standard forms on the host (several threads); their shared part is checked against the first
+  forms_.resize(count_);
+  std::vector<std::string> errors(count_);
+  {
+    const int threads = std::max(1, std::min<int>(16, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+      pool.emplace_back([&, t] {
+        for (int k = t; k < count_; k += threads) {
+          try {
+            forms_[k] = build_std_form(models_[k], false, opts_[k].enable_scaling != 0);
+          } catch (const std::exception& e) {
+            errors[k] = e.what();
+          }
+        }
+      });
+    for (auto& th : pool) th.join();
+  }
+  std::vector<int> members, singles;
+  int first = -1;
+  for (int k = 0; k < count_; ++k) {
+    const StdForm& f = forms_[k];
+    if (!errors[k].empty() || f.m <= 0 || f.n <= 0) {
+      singles.push_back(k);
+      continue;
+    }
+    if (first < 0) first = k;
+    const StdForm& f0 = forms_[first];
+    const bool shared = f.n == f0.n && f.m == f0.m && f.col_ptr == f0.col_ptr && f.row_idx == f0.row_idx &&
+                        f.val == f0.val && f.col_scale == f0.col_scale && f.row_scale == f0.row_scale;
+    (shared ? members : singles).push_back(k);
+  }
+  // LPs the family path does not take (no rows, a failed standard form, a scaling of their own):
+  // the single engine, one by one
+  for (int k : singles) {
+    sov_result* r = &results_[k];
+    if (!errors[k].empty()) {
+      r->status = SOV_ERROR;
+      r->has_objective_value = 0;
+      std::snprintf(r->message, sizeof(r->message), "IPM error: %s", errors[k].c_str());
+      continue;
+    }
+    const int rc = sov_lp_solve(&models_[k], &opts_[k], r);
+    if (rc != SOV_OK && rc != SOV_E_ARGUMENT) return rc;
+  }
+  if (members.empty()) return SOV_OK;
+  setup_shared(forms_[members[0]]);
+  for (size_t c0 = 0; c0 < members.size(); c0 += kFamilyWidth) {
+    const size_t c1 = std::min(members.size(), c0 + kFamilyWidth);
+    solve_chunk(std::vector<int>(members.begin() + c0, members.begin() + c1));
+  }
+  return SOV_OK;
+}
+
+void Family::setup_shared(const StdForm& f) {
+  // the normal matrices' pattern, its order and symbolic factor, once for the family
+  if (!sparse_analyze(f, 0, sym_))
+    throw std::invalid_argument("sov_lp_solve_family: the sparse L D L' of the order-" + std::to_string(f.m) +
+                                " normal matrix needs more than " + std::to_string(kMaxUpdates) +
+                                " rank-1 update terms");
+  // the root clique of the elimination tree, when large, is factored and solved densely
+  tail_ = sparse_dense_tail(sym_);
+  if (tail_ < kMinTail) tail_ = 0;
+  const SparseSchedule S = sparse_schedule(sym_, tail_);
+  {
+    std::vector<int> off(std::max(1, tail_));
+    for (int q = 0; q < tail_; ++q) off[q] = f.m + sym_.lp[f.m - tail_ + q];
+    tail_off_.put(off, st_);
+  }
+  pivot_ptr_.put(S.pivot_ptr, st_);
+  pivot_col_.put(S.pivot_col, st_);
+  row_ptr_.put(f.row_ptr, st_);
+  col_idx_.put(f.col_idx, st_);
+  rval_.put(f.rval, st_);
+  col_ptr_.put(f.col_ptr, st_);
+  row_idx_.put(f.row_idx, st_);
+  cval_.put(f.val, st_);
+  asm_target_.put(sym_.asm_target, st_);
+  asm_ptr_.put(sym_.asm_ptr, st_);
+  asm_col_.put(sym_.asm_col, st_);
+  asm_w_.put(sym_.asm_w, st_);
+  perm_.put(sym_.perm, st_);
+  lvl_ptr_.put(sym_.lvl_ptr, st_);
+  lvl_col_.put(sym_.lvl_col, st_);
+  li_.put(sym_.li, st_);
+  up_col_.put(S.up_col, st_);
+  up_a_.put(S.up_a, st_);
+  up_b_.put(S.up_b, st_);
+  row_pos_.put(S.row_pos, st_);
+  row_col_.put(S.row_col, st_);
+  static_assert(sizeof(SparsePiece) == sizeof(int4) && sizeof(SparseCombine) == sizeof(int4), "piece layout");
+  auto put4 = [&](Buf<int4>& b, const auto& v) {
+    std::vector<int4> w(v.size());
+    std::memcpy(w.data(), v.data(), sizeof(int4) * v.size());
+    b.put(w, st_);
+  };
+  put4(fp_, S.factor.piece);
+  put4(fc_, S.factor.comb);
+  put4(lpc_, S.forward.piece);
+  put4(lc_, S.forward.comb);
+  put4(upc_, S.backward.piece);
+  put4(uc_, S.backward.comb);
+  fpl_.put(S.factor.piece_lvl, st_);
+  fcl_.put(S.factor.comb_lvl, st_);
+  lpl_.put(S.forward.piece_lvl, st_);
+  lcl_.put(S.forward.comb_lvl, st_);
+  upl_.put(S.backward.piece_lvl, st_);
+  ucl_.put(S.backward.comb_lvl, st_);
+  slots_ = std::max(1, std::max(S.factor_slots, S.solve_slots));
+  SOV_CUDA(cudaStreamSynchronize(st_));  // host vectors above go out of scope
+  // per-chunk storage at the full width
+  const size_t W = kFamilyWidth, n = f.n, m = f.m;
+  for (Buf<double>* v : {&c_, &x_, &s_, &dx_, &ds_, &dxa_, &dsa_, &rd_, &t_, &x0_, &s0_, &bx_, &bs_, &cx_, &cs_})
+    v->alloc(n * W);
+  for (Buf<double>* v : {&b_, &y_, &rp_, &z_, &y0_, &by_, &cy_, &diag_, &inv_d_, &work_}) v->alloc(m * W);
+  bnorm_.alloc(W);
+  cnorm_.alloc(W);
+  part_.alloc(static_cast<size_t>(kFamBlocks) * kNv * W);
+  part_rows_.alloc(static_cast<size_t>(kFamBlocks) * kNv * W);
+  V_.alloc((m + sym_.li.size()) * W);
+  partial_.alloc(static_cast<size_t>(slots_) * W);
+  sc_.alloc(W);
+  step_.alloc(W);
+  mask_.alloc(W);
+  SOV_CUDA(cudaMallocHost(&hsc_, sizeof(FamScalars) * W));
+  int dev = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  SOV_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_factor_, k_fam_factor, kFamThreads, 0));
+  SOV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solve_, k_fam_solve, kFamThreads, 0));
+  per_sm_factor_ = std::max(1, std::min(per_sm_factor_, 2));
+  per_sm_solve_ = std::max(1, std::min(per_sm_solve_, 2));
+  am_ = FamAssembly{asm_target_.p, asm_ptr_.p, asm_col_.p, asm_w_.p, static_cast<int>(sym_.asm_target.size())};
+  sp_.m = f.m;
+  sp_.levels = S.levels;
+  sp_.tail = tail_;
+  sp_.mt = f.m - tail_;
+  sp_.tail_off = tail_off_.p;
+  sp_.pivot_ptr = pivot_ptr_.p;
+  sp_.pivot_col = pivot_col_.p;
+  sp_.V = V_.p;
+  sp_.diag = diag_.p;
+  sp_.inv_d = inv_d_.p;
+  sp_.work = work_.p;
+  sp_.partial = partial_.p;
+  sp_.perm = perm_.p;
+  sp_.lvl_ptr = lvl_ptr_.p;
+  sp_.lvl_col = lvl_col_.p;
+  sp_.li = li_.p;
+  sp_.fpiece = fp_.p;
+  sp_.fcomb = fc_.p;
+  sp_.lpiece = lpc_.p;
+  sp_.lcomb = lc_.p;
+  sp_.upiece = upc_.p;
+  sp_.ucomb = uc_.p;
+  sp_.fpiece_lvl = fpl_.p;
+  sp_.fcomb_lvl = fcl_.p;
+  sp_.lpiece_lvl = lpl_.p;
+  sp_.lcomb_lvl = lcl_.p;
+  sp_.upiece_lvl = upl_.p;
+  sp_.ucomb_lvl = ucl_.p;
+  sp_.up_col = up_col_.p;
+  sp_.up_a = up_a_.p;
+  sp_.up_b = up_b_.p;
+  sp_.row_pos = row_pos_.p;
+  sp_.row_col = row_col_.p;
+  sp_.sc = sc_.p;
+  sp_.drop_tol = 1e-13;
+  dev_.m = f.m;
+  dev_.n = f.n;
+  dev_.row_ptr = row_ptr_.p;
+  dev_.col_idx = col_idx_.p;
+  dev_.col_ptr = col_ptr_.p;
+  dev_.row_idx = row_idx_.p;
+  dev_.rval = rval_.p;
+  dev_.cval = cval_.p;
+  dev_.b = b_.p;
+  dev_.c = c_.p;
+  dev_.bnorm = bnorm_.p;
+  dev_.cnorm = cnorm_.p;
+  dev_.x = x_.p;
+  dev_.s = s_.p;
+  dev_.y = y_.p;
+  dev_.dx = dx_.p;
+  dev_.ds = ds_.p;
+  dev_.dxa = dxa_.p;
+  dev_.dsa = dsa_.p;
+  dev_.rd = rd_.p;
+  dev_.rp = rp_.p;
+  dev_.z = z_.p;
+  dev_.t = t_.p;
+  dev_.sc = sc_.p;
+  dev_.step = step_.p;
+  dev_.part = part_.p;
+}
+
+void Family::residuals() {
+  const int W = dev_.W, bd = W * dev_.G;
+  const size_t smem = sizeof(double) * kNv * bd;
+  FamDev rows = dev_;
+  rows.part = part_rows_.p;
+  const int gr = grid_for(dev_.m), gc = grid_for(dev_.n);
+  k_fam_res_rows<<<gr, bd, smem, st_>>>(rows);
+  k_fam_res_cols<<<gc, bd, smem, st_>>>(dev_);
+  k_fam_res_final<<<1, kFamilyWidth, 0, st_>>>(dev_, part_rows_.p, gr, gc);
+  SOV_LAUNCH_CHECK();
+}
+
+void Family::assemble(bool ones) {
+  SOV_CUDA(cudaMemsetAsync(V_.p, 0, sizeof(double) * (dev_.m + sym_.li.size()) * dev_.W, st_));
+  const long long total = static_cast<long long>(am_.ntargets) * dev_.W;
+  const int blocks = static_cast<int>(std::max(1LL, std::min(8LL * sms_, (total + 255) / 256)));
+  k_fam_assemble<<<blocks, 256, 0, st_>>>(am_, dev_, sp_, ones ? 1 : 0);
+  SOV_LAUNCH_CHECK();
+}
+
+void Family::factor() {
+  FamSparse f = sp_;
+  void* args[] = {&f};
+  SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_fam_factor, dim3(sms_ * per_sm_factor_), dim3(kFamThreads), args,
+                                       0, st_));
+  for (int j0 = 0; j0 < tail_; j0 += kPanel) {
+    const int j1 = std::min(tail_, j0 + kPanel), W = sp_.W;
+    k_tail_diag<<<1, (j1 - j0) * W, 0, st_>>>(sp_, j0, j1);
+    if (j1 < tail_) {
+      const long long rows = static_cast<long long>(tail_ - j1) * W;
+      const long long n = tail_ - j1, pairs = n * (n + 1) / 2 * W;
+      k_tail_rows<<<static_cast<int>(std::max(1LL, std::min(8LL * sms_, (rows + 255) / 256))), 256, 0, st_>>>(sp_, j0, j1);
+      k_tail_update<<<static_cast<int>(std::max(1LL, std::min(16LL * sms_, (pairs + 255) / 256))), 256, 0, st_>>>(sp_, j0,
+                                                                                                            j1);
+    }
+  }
+  SOV_LAUNCH_CHECK();
+}
+
+void Family::solve(double* z) {
+  FamSparse f = sp_;
+  void* args[] = {&f, &z};
+  SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_fam_solve, dim3(sms_ * per_sm_solve_), dim3(kFamThreads), args, 0,
+                                       st_));
+}
+
+void Family::copy(int entries, const int* mask_dev, double* dst, const double* src) {
+  const long long total = static_cast<long long>(entries) * dev_.W;
+  const int blocks = static_cast<int>(std::max(1LL, std::min(8LL * sms_, (total + 255) / 256)));
+  k_fam_copy<<<blocks, 256, 0, st_>>>(entries, dev_.W, mask_dev, dst, src);
+  SOV_LAUNCH_CHECK();
+}
+
+std::string Family::describe() const {
+  char buf[256];
+  std::snprintf(buf, sizeof buf,
+                "sparse LDL^T on the GPU with %s ordering (order %d, nnz(L) = %lld, %d levels, dense trailing "
+                "block of %d columns), one symbolic factor for the family, %d LPs per launch",
+                sym_.ordering == SparseOrder::kNestedDissection ? "nested-dissection" : "minimum-degree", sym_.m,
+                sym_.nnz_l, sp_.levels, tail_, dev_.W);
+  return buf;
+}
+
+__global__ void k_fam_clear_fail(FamScalars* sc, const int* mask, int W) {
+  const int k = threadIdx.x;
+  if (k < W && (!mask || mask[k])) sc[k].fail = 0;
+}
+
+void Family::solve_chunk(const std::vector<int>& lps) {
+  const int W = static_cast<int>(lps.size());
+  const StdForm& f0 = forms_[lps[0]];
+  const int n = f0.n, m = f0.m;
+  dev_.W = W;
+  dev_.G = std::max(1, kFamThreads / W);
+  dev_.tau = opts_[lps[0]].fraction_to_boundary;
+  sp_.W = W;
+  const auto t_start = std::chrono::steady_clock::now();
+  // right-hand sides and costs, interleaved; their norms (max(1, max |.|) of the scaled problem)
+  {
+    std::vector<double> bI(static_cast<size_t>(m) * W), cI(static_cast<size_t>(n) * W), bn(W), cn(W);
+    for (int k = 0; k < W; ++k) {
+      const StdForm& f = forms_[lps[k]];
+      double bm = 0.0, cm = 0.0;
+      for (int i = 0; i < m; ++i) {
+        bI[static_cast<size_t>(i) * W + k] = f.b[i];
+        bm = std::max(bm, std::abs(f.b[i]));
+      }
+      for (int j = 0; j < n; ++j) {
+        cI[static_cast<size_t>(j) * W + k] = f.c[j];
+        cm = std::max(cm, std::abs(f.c[j]));
+      }
+      bn[k] = std::max(1.0, bm);
+      cn[k] = std::max(1.0, cm);
+    }
+    SOV_CUDA(cudaMemcpyAsync(b_.p, bI.data(), sizeof(double) * bI.size(), cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(c_.p, cI.data(), sizeof(double) * cI.size(), cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(bnorm_.p, bn.data(), sizeof(double) * W, cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(cnorm_.p, cn.data(), sizeof(double) * W, cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemsetAsync(sc_.p, 0, sizeof(FamScalars) * W, st_));
+    SOV_CUDA(cudaStreamSynchronize(st_));
+  }
+  std::vector<LpState> L(W);
+  for (int k = 0; k < W; ++k) {
+    const StdForm& f = forms_[lps[k]];
+    L[k].idx = lps[k];
+    L[k].o = opts_[lps[k]];
+    sov_diagnostics& dg = L[k].dg;
+    dg.scaling_applied = f.scaling_applied;
+    dg.coefficient_min_abs_before = f.coef_min_before;
+    dg.coefficient_max_abs_before = f.coef_max_before;
+    dg.coefficient_min_abs_after = f.coef_min_after;
+    dg.coefficient_max_abs_after = f.coef_max_after;
+    dg.stall_iteration = -1;
+  }
+  const int gn = grid_for(n), bd = W * dev_.G;
+  const size_t smem = sizeof(double) * kNv * bd;
+  std::vector<int> hmask(W);
+  auto put_mask = [&](Buf<int>& b) {
+    SOV_CUDA(cudaMemcpyAsync(b.p, hmask.data(), sizeof(int) * W, cudaMemcpyHostToDevice, st_));
+  };
+  auto read_scalars = [&]() {
+    SOV_CUDA(cudaMemcpyAsync(hsc_, sc_.p, sizeof(FamScalars) * W, cudaMemcpyDeviceToHost, st_));
+    SOV_CUDA(cudaStreamSynchronize(st_));
+  };
+  // ---- default start, kept in (x0, y0, s0) for restarts: A A' dy = b - A 1 ----
+  assemble(true);
+  factor();
+  k_fam_start_rhs<<<grid_for(m), bd, 0, st_>>>(dev_);
+  solve(z_.p);
+  k_fam_start_point<<<grid_for(std::max(n, m)), bd, 0, st_>>>(dev_, x0_.p, y0_.p, s0_.p);
+  SOV_LAUNCH_CHECK();
+  SOV_CUDA(cudaMemcpyAsync(x_.p, x0_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
+  SOV_CUDA(cudaMemcpyAsync(s_.p, s0_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
+  SOV_CUDA(cudaMemcpyAsync(y_.p, y0_.p, sizeof(double) * m * W, cudaMemcpyDeviceToDevice, st_));
+  for (auto& l : L) l.factorizations = 1;
+  // ---- supplied starts, kept only when their residual metric is within 10x the default start's
+  // and their mu is not larger (the single engine's safeguard) ----
+  bool any_warm = false;
+  for (auto& l : L) any_warm |= l.o.warm_x && l.o.warm_y && l.o.warm_s;
+  if (any_warm) {
+    residuals();
+    read_scalars();
+    std::vector<double> dmetric(W), dmu(W);
+    for (int k = 0; k < W; ++k) {
+      dmetric[k] = hsc_[k].metric;
+      dmu[k] = hsc_[k].mu;
+    }
+    std::vector<double> hx(static_cast<size_t>(n) * W), hs(hx.size()), hy(static_cast<size_t>(m) * W);
+    SOV_CUDA(cudaMemcpyAsync(hx.data(), x_.p, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st_));
+    SOV_CUDA(cudaMemcpyAsync(hs.data(), s_.p, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st_));
+    SOV_CUDA(cudaMemcpyAsync(hy.data(), y_.p, sizeof(double) * hy.size(), cudaMemcpyDeviceToHost, st_));
+    SOV_CUDA(cudaStreamSynchronize(st_));
+    for (int k = 0; k < W; ++k) {
+      const sov_options& o = L[k].o;
+      if (!(o.warm_x && o.warm_y && o.warm_s)) continue;
+      for (int j = 0; j < n; ++j) {
+        hx[static_cast<size_t>(j) * W + k] = o.warm_x[j];
+        hs[static_cast<size_t>(j) * W + k] = o.warm_s[j];
+      }
+      for (int i = 0; i < m; ++i) hy[static_cast<size_t>(i) * W + k] = o.warm_y[i];
+    }
+    SOV_CUDA(cudaMemcpyAsync(x_.p, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(s_.p, hs.data(), sizeof(double) * hs.size(), cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(y_.p, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice, st_));
+    residuals();
+    read_scalars();
+    for (int k = 0; k < W; ++k) {
+      const sov_options& o = L[k].o;
+      const bool supplied = o.warm_x && o.warm_y && o.warm_s;
+      const FamScalars& sc = hsc_[k];
+      L[k].warm_used = supplied && std::isfinite(sc.metric) && std::isfinite(sc.mu) && sc.metric <= 10.0 * dmetric[k] &&
+                       sc.mu <= dmu[k];
+      hmask[k] = supplied && !L[k].warm_used;  // rejected: back to the default start
+    }
+    put_mask(mask_);
+    copy(n, mask_.p, x_.p, x0_.p);
+    copy(n, mask_.p, s_.p, s0_.p);
+    copy(m, mask_.p, y_.p, y0_.p);
+  }
+  for (auto& l : L) l.dg.warm_start_used = l.warm_used ? 1 : 0;
+  k_fam_clear_fail<<<1, kFamilyWidth, 0, st_>>>(sc_.p, nullptr, W);
+  SOV_CUDA(cudaMemcpyAsync(bx_.p, x_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
+  SOV_CUDA(cudaMemcpyAsync(bs_.p, s_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
+  SOV_CUDA(cudaMemcpyAsync(by_.p, y_.p, sizeof(double) * m * W, cudaMemcpyDeviceToDevice, st_));
+  // ---- the iteration loop (Engine::run's decisions, per LP; stepping LPs move together) ----
+  enum Source { kCurrent, kBest };
+  std::vector<int> source(W, kCurrent);
+  std::vector<int> hstep(W), hbest(W), hrestart(W), hcap(W);
+  const char* fail_text =
+      "IPM stopped because the affine predictor factorization failed; the best iterate is returned with optimality "
+      "unproven.";
+  auto finish_best = [&](LpState& l, int k, const std::string& msg) {
+    l.active = false;
+    source[k] = kBest;
+    l.msg = msg;
+  };
+  for (int it = 0;; ++it) {
+    bool any_active = false, any_cap = false;
+    for (int k = 0; k < W; ++k) {
+      hcap[k] = L[k].active && L[k].o.ipm_iterate_at == it + 1;
+      any_cap |= hcap[k] != 0;
+      if (hcap[k]) L[k].captured = true;
+      any_active |= L[k].active;
+    }
+    if (!any_active) break;
+    if (any_cap) {
+      hmask = hcap;
+      put_mask(mask_);
+      copy(n, mask_.p, cx_.p, x_.p);
+      copy(n, mask_.p, cs_.p, s_.p);
+      copy(m, mask_.p, cy_.p, y_.p);
+    }
+    residuals();
+    read_scalars();
+    bool any_step = false, any_best = false, any_restart = false;
+    for (int k = 0; k < W; ++k) {
+      hstep[k] = hbest[k] = hrestart[k] = 0;
+      LpState& l = L[k];
+      if (!l.active) continue;
+      const FamScalars s = hsc_[k];
+      sov_diagnostics& dg = l.dg;
+      if (it >= l.o.max_iterations) {  // the loop of this LP has ended without convergence
+        char buf[512];
+        std::snprintf(buf, sizeof buf,
+                      "IPM stopped after %d iterations without meeting tolerance; returning best iterate from %d as a "
+                      "lower-accuracy candidate. Relative duality gap = %g (tolerance %g), primal residual = %g, dual "
+                      "residual = %g. Optimality is not proven.",
+                      l.o.max_iterations, l.best_it, l.best_gap, l.o.optimality_tol, l.best_p, l.best_d);
+        finish_best(l, k, buf);
+        continue;
+      }
+      if (it > 0) {
+        const int prev = it - 1;
+        const bool prev_sample = prev < 8 || prev % 10 == 0 || prev + 1 == l.o.max_iterations;
+        if (prev_sample && dg.step_history_len < SOV_HISTORY_MAX) {
+          dg.primal_step_history[dg.step_history_len] = s.alpha_p;
+          dg.dual_step_history[dg.step_history_len] = s.alpha_d;
+          dg.step_history_len++;
+        }
+        if (dg.stall_iteration == prev + 1) {
+          dg.stall_primal_step = s.alpha_p;
+          dg.stall_dual_step = s.alpha_d;
+        }
+      }
+      if (s.fail || s.skipped) {
+        finish_best(l, k, fail_text);
+        continue;
+      }
+      if (s.metric < l.best_metric) {
+        l.best_metric = s.metric;
+        hbest[k] = 1;
+        any_best = true;
+        l.best_gap = s.gap;
+        l.best_p = s.p_res;
+        l.best_d = s.d_res;
+        l.best_it = it + 1;
+        l.stale = 0;
+      } else {
+        ++l.stale;
+      }
+      const bool sample = it < 8 || it % 10 == 0 || it + 1 == l.o.max_iterations;
+      if (sample && dg.history_len < SOV_HISTORY_MAX) {
+        dg.history_iterations[dg.history_len] = it + 1;
+        dg.objective_history[dg.history_len] = s.cx;
+        dg.gap_history[dg.history_len] = s.gap;
+        dg.mu_history[dg.history_len] = s.mu;
+        dg.history_len++;
+      }
+      if (s.gap < l.best_gap) {
+        l.best_gap = s.gap;
+        l.stale = 0;
+      } else if (l.stale >= 8 && dg.stall_iteration < 0) {
+        dg.stall_iteration = it + 1;
+        dg.stall_gap = s.gap;
+        dg.stall_mu = s.mu;
+      }
+      if (s.p_res < l.o.feasibility_tol && s.d_res < l.o.feasibility_tol && s.gap < l.o.optimality_tol) {
+        l.active = false;
+        l.optimal = true;
+        l.its = it + 1;
+        l.gap = s.gap;
+        l.p_res = s.p_res;
+        l.d_res = s.d_res;
+        source[k] = kCurrent;
+        continue;
+      }
+      if (l.warm_used && it + 1 == kWarmGiveUp) {  // the supplied start is abandoned once
+        l.warm_used = false;
+        dg.warm_start_used = 0;
+        hrestart[k] = 1;
+        any_restart = true;
+        l.best_metric = l.best_gap = l.best_p = l.best_d = INFINITY;
+        l.best_it = 0;
+        l.stale = 0;
+        l.factorizations++;
+        continue;
+      }
+      hstep[k] = 1;
+      any_step = true;
+    }
+    if (any_best) {
+      hmask = hbest;
+      put_mask(mask_);
+      copy(n, mask_.p, bx_.p, x_.p);
+      copy(n, mask_.p, bs_.p, s_.p);
+      copy(m, mask_.p, by_.p, y_.p);
+    }
+    if (any_restart) {
+      hmask = hrestart;
+      put_mask(mask_);
+      copy(n, mask_.p, x_.p, x0_.p);
+      copy(n, mask_.p, s_.p, s0_.p);
+      copy(m, mask_.p, y_.p, y0_.p);
+      k_fam_clear_fail<<<1, kFamilyWidth, 0, st_>>>(sc_.p, mask_.p, W);
+    }
+    if (!any_step) continue;
+    SOV_CUDA(cudaMemcpyAsync(step_.p, hstep.data(), sizeof(int) * W, cudaMemcpyHostToDevice, st_));
+    assemble(false);
+    factor();
+    for (int pass = 0; pass < 2; ++pass) {
+      k_fam_newton_tmp<<<gn, bd, 0, st_>>>(dev_, pass);
+      k_fam_newton_rhs<<<grid_for(m), bd, 0, st_>>>(dev_);
+      solve(z_.p);
+      k_fam_direction<<<gn, bd, smem, st_>>>(dev_, pass);
+      k_fam_direction_final<<<1, kFamilyWidth, 0, st_>>>(dev_, pass, gn);
+      if (pass == 0) {
+        k_fam_mu_aff<<<gn, bd, smem, st_>>>(dev_);
+        k_fam_mu_final<<<1, kFamilyWidth, 0, st_>>>(dev_, gn);
+      }
+    }
+    k_fam_update<<<grid_for(std::max(n, m)), bd, 0, st_>>>(dev_);
+    SOV_LAUNCH_CHECK();
+    for (int k = 0; k < W; ++k) L[k].factorizations += hstep[k];
+  }
+  SOV_CUDA(cudaStreamSynchronize(st_));
+  const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  // ---- results ----
+  std::vector<double> hx(static_cast<size_t>(n) * W), hs(hx.size()), hy(static_cast<size_t>(m) * W);
+  std::vector<double> bxh(hx.size()), bsh(hx.size()), byh(hy.size()), cxh, csh, cyh;
+  auto get = [&](std::vector<double>& h, const Buf<double>& b) {
+    SOV_CUDA(cudaMemcpyAsync(h.data(), b.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st_));
+  };
+  get(hx, x_);
+  get(hs, s_);
+  get(hy, y_);
+  get(bxh, bx_);
+  get(bsh, bs_);
+  get(byh, by_);
+  bool any_captured = false;
+  for (auto& l : L) any_captured |= l.captured;
+  if (any_captured) {
+    cxh.resize(hx.size());
+    csh.resize(hx.size());
+    cyh.resize(hy.size());
+    get(cxh, cx_);
+    get(csh, cs_);
+    get(cyh, cy_);
+  }
+  SOV_CUDA(cudaStreamSynchronize(st_));
+  for (int k = 0; k < W; ++k) {
+    LpState& l = L[k];
+    if (source[k] == kBest) publish(l, bxh, byh, bsh, cxh, cyh, csh, k, W, seconds);
+    else publish(l, hx, hy, hs, cxh, cyh, csh, k, W, seconds);
+  }
+}
+
+// Engine::publish for an LP (publish_iterate, interior_point.cpp:541-563), from the chunk's
+// interleaved arrays
+void Family::publish(LpState& l, const std::vector<double>& x, const std::vector<double>& y,
+                     const std::vector<double>& s, const std::vector<double>& cx, const std::vector<double>& cy,
+                     const std::vector<double>& cs, int k, int W, double seconds) {
+  const StdForm& f = forms_[l.idx];
+  const sov_model& model = models_[l.idx];
+  sov_result* r = &results_[l.idx];
+  const int n = f.n, m = f.m;
+  auto at = [&](const std::vector<double>& v, int i) { return v[static_cast<size_t>(i) * W + k]; };
+  r->n_ipm = n;
+  r->m_ipm = m;
+  if (l.optimal) {
+    r->status = SOV_OPTIMAL;
+    r->iterations = l.its;
+    r->duality_gap = l.gap;
+    r->primal_residual = l.p_res;
+    r->dual_residual = l.d_res;
+    l.msg = "Optimal solution found by primal-dual interior-point (Mehrotra). Normal equations: " + describe() + ".";
+  } else {
+    r->status = l.best_p <= l.o.feasibility_tol ? SOV_FEASIBLE : SOV_NUMERICAL_ERROR;
+    r->iterations = l.best_it;
+    r->duality_gap = l.best_gap;
+    r->primal_residual = l.best_p;
+    r->dual_residual = l.best_d;
+  }
+  r->has_objective_value = 1;
+  double obj = model.obj_constant;
+  for (int j = 0; j < f.n_struct; ++j) {
+    const double v = f.shift[j] + f.col_scale[j] * at(x, j);
+    if (r->primal) r->primal[j] = v;
+    if (r->dual_col) r->dual_col[j] = at(s, j) / f.col_scale[j];
+    obj += (model.obj ? model.obj[j] : 0.0) * v;
+  }
+  if (r->dual_row)
+    for (int i = 0; i < f.m0; ++i) r->dual_row[i] = f.row_scale[i] * at(y, i);
+  const bool cap = l.captured && !cx.empty();
+  for (int j = 0; j < n; ++j) {
+    if (r->ipm_x) r->ipm_x[j] = cap ? at(cx, j) : at(x, j);
+    if (r->ipm_s) r->ipm_s[j] = cap ? at(cs, j) : at(s, j);
+  }
+  if (r->ipm_y)
+    for (int i = 0; i < m; ++i) r->ipm_y[i] = cap ? at(cy, i) : at(y, i);
+  r->objective_value = obj;
+  r->solve_seconds = seconds;
+  std::snprintf(r->message, sizeof(r->message), "%s", l.msg.c_str());
+  if (r->diagnostics) {
+    l.dg.refactorizations = l.factorizations;
+    *r->diagnostics = l.dg;
+  }
+}
+
+}  // namespace
+
+int solve_family(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results) {
+  if (count <= 0) return SOV_OK;
+  for (int k = 0; k < count; ++k) {
+    results[k].status = SOV_ERROR;
+    results[k].iterations = 0;
+    results[k].has_objective_value = 0;
+    results[k].message[0] = '\0';
+  }
+  Family fam(count, models, opt, opt_stride, results);
+  return fam.run();
+}
+
+}  // namespace sov

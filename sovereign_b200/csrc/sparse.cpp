@@ -682,24 +682,51 @@ SparsePieces row_pieces(const std::vector<int>& ptr, int* slots) {
   return P;
 }
 
-SparseSchedule sparse_schedule(const SparseSymbolic& s) {
+int sparse_dense_tail(const SparseSymbolic& s) {
+  int t = 0;
+  for (int k = s.m - 1; k >= 0 && s.lp[k + 1] - s.lp[k] == s.m - 1 - k; --k) ++t;
+  return t;
+}
+
+SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail) {
   SparseSchedule S;
-  const int m = s.m, levels = s.levels();
+  const int m = s.m, levels = s.levels(), mt = m - tail;
+  S.tail = tail;
+  // level of each column; the levels that hold a column before the tail
+  std::vector<int> level(m, 0);
+  for (int h = 0; h < levels; ++h)
+    for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) level[s.lvl_col[c]] = h;
+  int hn = 0;
+  for (int k = 0; k < mt; ++k) hn = std::max(hn, level[k] + 1);
+  if (tail == 0) hn = levels;
+  S.levels = hn;
+  S.pivot_ptr.assign(1, 0);
+  for (int h = 0; h < hn; ++h) {
+    for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c)
+      if (s.lvl_col[c] < mt) S.pivot_col.push_back(s.lvl_col[c]);
+    S.pivot_ptr.push_back(static_cast<int>(S.pivot_col.size()));
+  }
   // updates grouped by (level, destination), schedule order kept within a group: two stable
-  // counting sorts (by destination, then by level), linear in the number of updates
-  const size_t n_up = s.pairs.size() / 4;
+  // counting sorts (by destination, then by level), linear in the number of updates; a tail
+  // column's own updates are left to the dense factorization
+  const size_t n_all = s.pairs.size() / 4;
   const int n_dst = m + static_cast<int>(s.li.size());
-  std::vector<int> level_of(n_up);
+  std::vector<int> level_of(n_all);
   for (int h = 0; h < levels; ++h)
     for (int u = s.pair_ptr[h]; u < s.pair_ptr[h + 1]; ++u) level_of[u] = h;
+  std::vector<int> keep;
+  keep.reserve(n_all);
+  for (size_t u = 0; u < n_all; ++u)
+    if (s.pairs[4 * u] < mt) keep.push_back(static_cast<int>(u));
+  const size_t n_up = keep.size();
   std::vector<int> by_dst(n_up), order(n_up);
   {
     std::vector<size_t> cnt(n_dst + 1, 0);
-    for (size_t u = 0; u < n_up; ++u) cnt[s.pairs[4 * u + 3] + 1]++;
+    for (int u : keep) cnt[s.pairs[4 * u + 3] + 1]++;
     for (int d = 0; d < n_dst; ++d) cnt[d + 1] += cnt[d];
-    for (size_t u = 0; u < n_up; ++u) by_dst[cnt[s.pairs[4 * u + 3]]++] = static_cast<int>(u);
+    for (int u : keep) by_dst[cnt[s.pairs[4 * u + 3]]++] = u;
     std::vector<size_t> lc(levels + 1, 0);
-    for (size_t u = 0; u < n_up; ++u) lc[level_of[u] + 1]++;
+    for (int u : keep) lc[level_of[u] + 1]++;
     for (int h = 0; h < levels; ++h) lc[h + 1] += lc[h];
     for (size_t q = 0; q < n_up; ++q) {
       const int u = by_dst[q];
@@ -716,7 +743,7 @@ SparseSchedule sparse_schedule(const SparseSymbolic& s) {
     S.up_b[q] = s.pairs[4 * u + 2];
   }
   size_t q = 0;
-  for (int h = 0; h < levels; ++h) {
+  for (int h = 0; h < hn; ++h) {
     while (q < n_up && level_of[order[q]] == h) {
       const int dst = s.pairs[4 * order[q] + 3];
       size_t e = q + 1;
@@ -726,7 +753,7 @@ SparseSchedule sparse_schedule(const SparseSymbolic& s) {
     }
     close_level(S.factor);
   }
-  // rows of L for the forward solve
+  // rows of L for the forward solve (each row's entries in column order)
   std::vector<int> row_ptr(m + 1, 0);
   S.row_pos.resize(s.li.size());
   S.row_col.resize(s.li.size());
@@ -741,17 +768,25 @@ SparseSchedule sparse_schedule(const SparseSymbolic& s) {
         S.row_col[t] = k;
       }
   }
-  for (int h = 0; h < levels; ++h) {
+  for (int h = 0; h < hn; ++h) {
     for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) {
       const int k = s.lvl_col[c];
-      add_item(S.forward, row_ptr[k], row_ptr[k + 1], k, &S.solve_slots, false);
+      if (k < mt) add_item(S.forward, row_ptr[k], row_ptr[k + 1], k, &S.solve_slots, false);
     }
     close_level(S.forward);
   }
-  for (int h = 0; h < levels; ++h) {  // every column, empty ones too (x_k = y_k / D_k)
+  if (tail > 0) {  // the tail rows' sums over the columns before the tail, in one more level
+    for (int k = mt; k < m; ++k) {
+      int e = row_ptr[k];
+      while (e < row_ptr[k + 1] && S.row_col[e] < mt) ++e;
+      add_item(S.forward, row_ptr[k], e, k, &S.solve_slots, false);
+    }
+    close_level(S.forward);
+  }
+  for (int h = 0; h < hn; ++h) {  // every column, empty ones too (x_k = y_k / D_k)
     for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) {
       const int k = s.lvl_col[c];
-      add_item(S.backward, s.lp[k], s.lp[k + 1], k, &S.solve_slots, true);
+      if (k < mt) add_item(S.backward, s.lp[k], s.lp[k + 1], k, &S.solve_slots, true);
     }
     close_level(S.backward);
   }

@@ -91,9 +91,21 @@ struct SparseSchedule {
   SparsePieces forward;                 // over row_pos / row_col; target = row k
   SparsePieces backward;                // over li; target = column k (every column has a piece)
   int factor_slots = 0, solve_slots = 0;
+  // with a dense tail (tail > 0): the last `tail` columns are left out of the level schedule --
+  // their pivots, their update terms and their columns in the backward solve -- for a dense
+  // factorization and dense solves of that block; `levels` levels remain (pivot_ptr/pivot_col:
+  // their columns), and the forward solve has one more level, the tail rows' sums over the
+  // columns before the tail
+  int tail = 0, levels = 0;
+  std::vector<int> pivot_ptr, pivot_col;
 };
 
-SparseSchedule sparse_schedule(const SparseSymbolic& s);
+SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail = 0);
+
+// The trailing columns of L whose pattern is every later row (a dense trailing block: the root
+// clique of the elimination tree). Their L entries are stored column by column, rows ascending,
+// so the block is a column-packed lower triangle inside [D | L].
+int sparse_dense_tail(const SparseSymbolic& s);
 
 // The rows of a CSR pattern (ptr, rows + 1 entries) as pieces of one level: target = row; the
 // combine entries hold the rows that were cut, slots numbered from 0.

@@ -146,6 +146,31 @@ def solve_batch(models: list[Model], options: InteriorPointOptions | None = None
     return out
 
 
+def solve_family(models: list[Model], options: InteriorPointOptions | None = None, with_ipm: bool = False,
+                 warm_starts: list | None = None, with_diag: bool = False) -> list[Result]:
+    """LPs of one parametric family -- the same A, bounds and senses, their own b, c -- solved
+    together (sov_lp_solve_family): one symbolic analysis, up to 64 LPs per launch with their
+    vectors interleaved. Arguments as solve_batch."""
+    opt = (options or InteriorPointOptions()).to_abi()
+    bufs = []
+    for m in models:
+        n_ipm, m_ipm = _dims(m) if with_ipm else (0, 0)
+        bufs.append(ResultBuffers(m, with_ipm=with_ipm, with_diag=with_diag, n_ipm=n_ipm, m_ipm=m_ipm))
+    arr = (abi.SovModel * len(models))(*[m.to_abi() for m in models])
+    res = (abi.SovResult * len(models))(*[b.raw for b in bufs])
+    if warm_starts is None:
+        check(load().sov_lp_solve_family(len(models), arr, C.byref(opt), 0, res))
+    else:
+        opts, keep = _per_lp_options(opt, warm_starts)
+        check(load().sov_lp_solve_family(len(models), arr, opts, C.sizeof(abi.SovOptions), res))
+        del keep
+    out = []
+    for b, r in zip(bufs, res):
+        b.raw = r
+        out.append(b.to_result())
+    return out
+
+
 class DeviceBatch:
     """A prepared batch resident on the device (sov_batch_*): upload once, solve many times."""
 

@@ -54,15 +54,41 @@ static Sys make(int n, int m, bool quasi, unsigned seed) {
   return S;
 }
 
+// sparse graph plus a clique of c nodes joined to many others: ordered last, a dense tail
+static Sys clique(int n, int c, unsigned seed) {
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  Sys S{n, std::vector<std::vector<int>>(n), std::vector<std::vector<double>>(n, std::vector<double>(n, 0.0)),
+        std::vector<int>(n, 1)};
+  auto link = [&](int a, int b, double v) {
+    if (a == b || S.A[a][b] != 0.0) return;
+    S.A[a][b] = S.A[b][a] = v;
+    S.adj[a].push_back(b);
+    S.adj[b].push_back(a);
+  };
+  for (int j = 0; j + 1 < n - c; ++j) link(j, j + 1, 0.3 * u(rng));
+  for (int a = n - c; a < n; ++a) {
+    for (int b = a + 1; b < n; ++b) link(a, b, 0.05 * u(rng));
+    for (int t = 0; t < 12; ++t) link(a, static_cast<int>(rng() % (n - c)), 0.05 * u(rng));
+  }
+  for (int k = 0; k < n; ++k) {
+    double off = 0.0;
+    for (int j = 0; j < n; ++j) off += std::fabs(S.A[k][j]);
+    S.A[k][k] = off + 1.0;
+  }
+  return S;
+}
+
 // the kernels' walk of the schedule, sequential
-static long long run(const Sys& S, SparseOrder order, const char* name) {
+static long long run(const Sys& S, SparseOrder order, const char* name, bool use_tail = false) {
   SparseSymbolic s;
   if (!sparse_analyze_graph(S.adj, 0, s, order)) {
     std::printf("%s: analysis refused\n", name);
     return 1;
   }
   const int m = s.m;
-  const SparseSchedule P = sparse_schedule(s);
+  const int T = use_tail ? sparse_dense_tail(s) : 0, mt = m - T;
+  const SparseSchedule P = sparse_schedule(s, T);
   long long bad = 0;
   // every update term, row entry and column entry is covered exactly once by the pieces
   auto cover = [&](const SparsePieces& pc, size_t total, const char* what) {
@@ -90,12 +116,27 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
       }
     }
   };
-  split(P.factor, "factor");
-  split(P.forward, "forward");
-  split(P.backward, "backward");
+  auto split_levels = [&](const SparsePieces& pc, int levels, const char* what) {
+    for (int h = 0; h < levels; ++h) {
+      const int a = pc.piece_lvl[h], w = pc.warp_lvl[h], e = pc.piece_lvl[h + 1];
+      bool ok = a <= w && w <= e;
+      for (int q = a; ok && q < w; ++q) ok = pc.piece[q].end - pc.piece[q].first <= kSparseShort && pc.piece[q].slot < 0;
+      for (int q = w; ok && q < e; ++q) ok = pc.piece[q].end - pc.piece[q].first > kSparseShort || pc.piece[q].slot >= 0;
+      if (!ok) {
+        std::printf("%s: %s level %d mixes thread and warp pieces\n", name, what, h);
+        ++bad;
+        return;
+      }
+    }
+  };
+  split_levels(P.factor, P.levels, "factor");
+  split_levels(P.forward, P.levels + (T > 0), "forward");
+  split_levels(P.backward, P.levels, "backward");
   cover(P.factor, P.up_col.size(), "factor");
-  cover(P.forward, P.row_pos.size(), "forward");
-  cover(P.backward, s.li.size(), "backward");
+  if (T == 0) {
+    cover(P.forward, P.row_pos.size(), "forward");
+    cover(P.backward, s.li.size(), "backward");
+  }
   // values: [D | L] in elimination order
   std::vector<double> V(m + s.li.size(), 0.0), inv(m), part(std::max(1, std::max(P.factor_slots, P.solve_slots)));
   for (int i = 0; i < m; ++i) {
@@ -106,9 +147,9 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
   std::vector<int8_t> sg(m);
   for (int k = 0; k < m; ++k) sg[k] = static_cast<int8_t>(S.sign[s.perm[k]]);
   int drops = 0;
-  for (int h = 0; h < s.levels(); ++h) {
-    for (int q = s.lvl_ptr[h]; q < s.lvl_ptr[h + 1]; ++q) {
-      const int k = s.lvl_col[q];
+  for (int h = 0; h < P.levels; ++h) {
+    for (int q = P.pivot_ptr[h]; q < P.pivot_ptr[h + 1]; ++q) {
+      const int k = P.pivot_col[q];
       const double p = V[k];
       const bool drop = !(sg[k] * p > 0.0);
       drops += drop;
@@ -128,6 +169,15 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
       V[cb.target] -= t;
     }
   }
+  auto lt = [&](int a, int k) -> double& { return V[m + s.lp[k] + (a - k - 1)]; };  // L~_ak, k in the tail
+  for (int k = mt; k < m; ++k) {  // the dense tail, column by column
+    const double p = V[k];
+    const bool drop = !(sg[k] * p > 0.0);
+    drops += drop;
+    inv[k] = 1.0 / (drop ? sg[k] * 1e128 : p);
+    for (int a = k + 1; a < m; ++a)
+      for (int b = k + 1; b <= a; ++b) (a == b ? V[a] : lt(a, b)) -= lt(a, k) * lt(b, k) * inv[k];
+  }
   if (drops) {
     std::printf("%s: %d pivots with the wrong sign\n", name, drops);
     ++bad;
@@ -137,7 +187,7 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
   for (int i = 0; i < m; ++i)
     for (int j = 0; j < m; ++j) b[i] += S.A[i][j];
   for (int k = 0; k < m; ++k) w[k] = b[s.perm[k]];
-  for (int h = 0; h < s.levels(); ++h) {
+  for (int h = 0; h < P.levels + (T > 0); ++h) {
     for (int q = P.forward.piece_lvl[h]; q < P.forward.piece_lvl[h + 1]; ++q) {
       const SparsePiece& pc = P.forward.piece[q];
       double acc = 0.0;
@@ -152,7 +202,14 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
       w[cb.target] -= t;
     }
   }
-  for (int h = s.levels() - 1; h >= 0; --h) {
+  for (int k = mt; k < m; ++k)  // dense tail: forward, then backward
+    for (int i = k + 1; i < m; ++i) w[i] -= lt(i, k) * inv[k] * w[k];
+  for (int k = m - 1; k >= mt; --k) {
+    double acc = 0.0;
+    for (int i = k + 1; i < m; ++i) acc += lt(i, k) * w[i];
+    w[k] = (w[k] - acc) * inv[k];
+  }
+  for (int h = P.levels - 1; h >= 0; --h) {
     for (int q = P.backward.piece_lvl[h]; q < P.backward.piece_lvl[h + 1]; ++q) {
       const SparsePiece& pc = P.backward.piece[q];
       double acc = 0.0;
@@ -178,8 +235,8 @@ static long long run(const Sys& S, SparseOrder order, const char* name) {
   }
   err /= bmax;
   int cut = static_cast<int>(P.factor.comb.size() + P.forward.comb.size() + P.backward.comb.size());
-  std::printf("%s [%s]: N=%d levels=%d pieces %zu/%zu/%zu, cut items %d, |Kx - b| / |b| = %.2e\n", name,
-              s.ordering == SparseOrder::kNestedDissection ? "nested dissection" : "minimum degree", m, s.levels(),
+  std::printf("%s [%s, dense tail %d]: N=%d levels=%d pieces %zu/%zu/%zu, cut items %d, |Kx - b| / |b| = %.2e\n", name,
+              s.ordering == SparseOrder::kNestedDissection ? "nested dissection" : "minimum degree", T, m, P.levels,
               P.factor.piece.size(), P.forward.piece.size(), P.backward.piece.size(), cut, err);
   if (!(err < 1e-13)) ++bad;
   return bad;
@@ -192,6 +249,9 @@ int main() {
     failures += run(make(3000, 0, false, 1), o, "definite, dense row, N=3000");
     failures += run(make(2500, 150, true, 2), o, "quasi-definite, dense row, N=2650");
     failures += run(make(40, 10, true, 3), o, "quasi-definite, N=50");
+    failures += run(make(3000, 0, false, 1), o, "definite, dense row, N=3000", true);
+    failures += run(make(2500, 150, true, 2), o, "quasi-definite, dense row, N=2650", true);
+    failures += run(clique(600, 80, 5), o, "definite, 80-node clique, N=600", true);
   }
   std::printf("failures %lld\n", failures);
   return failures == 0 ? 0 : 1;
