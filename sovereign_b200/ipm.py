@@ -122,10 +122,113 @@ def _per_lp_options(opt: abi.SovOptions, warm_starts: list):
     return opts, keep
 
 
+def _struct_dtype(T) -> np.dtype:
+    """numpy view of a ctypes structure of the ABI, pointers as uint64 addresses."""
+    names, formats, offsets = [], [], []
+    for name, ctype in T._fields_:
+        names.append(name)
+        offsets.append(getattr(T, name).offset)
+        if isinstance(ctype, type) and issubclass(ctype, (C._Pointer, C.c_void_p)):
+            formats.append(np.uint64)
+        else:
+            formats.append(np.dtype(ctype))
+    return np.dtype(dict(names=names, formats=formats, offsets=offsets, itemsize=C.sizeof(T)))
+
+
+_MODEL_DT = None
+_RESULT_DT = None
+
+
+def _addr(a: np.ndarray) -> int:
+    return a.__array_interface__["data"][0]
+
+
+def _marshal(models: list[Model], with_ipm: bool):
+    """The models as one array of sov_model and one array of sov_result whose outputs are views
+    of one float64 buffer, built column-wise: no per-LP ctypes objects."""
+    global _MODEL_DT, _RESULT_DT
+    if _MODEL_DT is None:
+        _MODEL_DT, _RESULT_DT = _struct_dtype(abi.SovModel), _struct_dtype(abi.SovResult)
+    k = len(models)
+    M = np.zeros(k, dtype=_MODEL_DT)
+    for name, key in (("col_ptr", "col_ptr"), ("row_idx", "row_idx"), ("values", "values"), ("obj", "obj"),
+                      ("lb", "lb"), ("ub", "ub"), ("sense", "sense"), ("rhs", "rhs")):
+        arrs = [getattr(m, key) for m in models]
+        want = np.int8 if key == "sense" else np.int32 if key in ("col_ptr", "row_idx") else np.float64
+        for a in arrs:
+            if a.dtype != want or not a.flags["C_CONTIGUOUS"]:
+                raise TypeError(f"Model.{key} must be a contiguous {np.dtype(want)} array")
+        M[name] = [_addr(a) for a in arrs]
+    M["n"] = [m.n for m in models]
+    M["m"] = [m.m for m in models]
+    M["maximize"] = [int(m.maximize) for m in models]
+    M["obj_constant"] = [float(m.obj_constant) for m in models]
+    n = M["n"].astype(np.int64)
+    mm = M["m"].astype(np.int64)
+    dims = [_dims(m) for m in models] if with_ipm else None
+    ni = np.array([d[0] for d in dims], dtype=np.int64) if with_ipm else np.zeros(k, np.int64)
+    mi = np.array([d[1] for d in dims], dtype=np.int64) if with_ipm else np.zeros(k, np.int64)
+    sizes = 2 * n + mm + 2 * ni + mi
+    start = np.concatenate([[0], np.cumsum(sizes)])
+    buf = np.zeros(int(start[-1]) if k else 0)
+    base = _addr(buf) if buf.size else 0
+    R = np.zeros(k, dtype=_RESULT_DT)
+    off = start[:-1]
+    R["primal"] = base + 8 * off
+    R["dual_col"] = base + 8 * (off + n)
+    R["dual_row"] = base + 8 * (off + 2 * n)
+    if with_ipm:
+        R["ipm_x"] = base + 8 * (off + 2 * n + mm)
+        R["ipm_y"] = base + 8 * (off + 2 * n + mm + ni)
+        R["ipm_s"] = base + 8 * (off + 2 * n + mm + ni + mi)
+    return M, R, buf, (off, n, mm, ni, mi)
+
+
+def _unmarshal(R: np.ndarray, buf: np.ndarray, layout, with_ipm: bool) -> list[Result]:
+    off, n, mm, ni, mi = layout
+    out = []
+    status, its, has = R["status"], R["iterations"], R["has_objective_value"]
+    obj, gap, pres, dres = R["objective_value"], R["duality_gap"], R["primal_residual"], R["dual_residual"]
+    nip, mip, secs, msg = R["n_ipm"], R["m_ipm"], R["solve_seconds"], R["message"]
+    for k in range(len(R)):
+        o, a, b = int(off[k]), int(n[k]), int(mm[k])
+        r = Result(status=int(status[k]), iterations=int(its[k]), has_objective_value=bool(has[k]),
+                   objective_value=float(obj[k]), duality_gap=float(gap[k]), primal_residual=float(pres[k]),
+                   dual_residual=float(dres[k]), message=bytes(msg[k]).split(b"\0", 1)[0].decode(errors="replace"),
+                   primal=buf[o:o + a], dual_col=buf[o + a:o + 2 * a], dual_row=buf[o + 2 * a:o + 2 * a + b],
+                   n_ipm=int(nip[k]), m_ipm=int(mip[k]), solve_seconds=float(secs[k]))
+        if with_ipm:
+            p, x, y = o + 2 * a + b, int(ni[k]), int(mi[k])
+            r.ipm_x, r.ipm_y, r.ipm_s = buf[p:p + x], buf[p + x:p + x + y], buf[p + x + y:p + 2 * x + y]
+        out.append(r)
+    return out
+
+
+def _solve_many(entry, models: list[Model], options, with_ipm: bool, warm_starts, with_diag: bool) -> list[Result]:
+    """sov_lp_solve_batch / sov_lp_solve_family through the column-wise marshalling (results with
+    diagnostics take the per-LP buffers)."""
+    opt = (options or InteriorPointOptions()).to_abi()
+    if with_diag or any(m.is_qp for m in models):
+        return None
+    M, R, buf, layout = _marshal(models, with_ipm)
+    mp = C.cast(C.c_void_p(_addr(M)), C.POINTER(abi.SovModel)) if len(models) else None
+    rp = C.cast(C.c_void_p(_addr(R)), C.POINTER(abi.SovResult)) if len(models) else None
+    if warm_starts is None:
+        check(entry(len(models), mp, C.byref(opt), 0, rp))
+    else:
+        opts, keep = _per_lp_options(opt, warm_starts)
+        check(entry(len(models), mp, opts, C.sizeof(abi.SovOptions), rp))
+        del keep
+    return _unmarshal(R, buf, layout, with_ipm)
+
+
 def solve_batch(models: list[Model], options: InteriorPointOptions | None = None, with_ipm: bool = False,
                 warm_starts: list | None = None, with_diag: bool = False) -> list[Result]:
     """Independent LPs in one persistent batched launch (sov_lp_solve_batch). warm_starts: one
     (x, y, s) tuple (engine standard form) or None per LP; passed as per-LP option blocks."""
+    fast = _solve_many(load().sov_lp_solve_batch, models, options, with_ipm, warm_starts, with_diag)
+    if fast is not None:
+        return fast
     opt = (options or InteriorPointOptions()).to_abi()
     bufs = []
     for m in models:
@@ -151,6 +254,9 @@ def solve_family(models: list[Model], options: InteriorPointOptions | None = Non
     """LPs of one parametric family -- the same A, bounds and senses, their own b, c -- solved
     together (sov_lp_solve_family): one symbolic analysis, up to 64 LPs per launch with their
     vectors interleaved. Arguments as solve_batch."""
+    fast = _solve_many(load().sov_lp_solve_family, models, options, with_ipm, warm_starts, with_diag)
+    if fast is not None:
+        return fast
     opt = (options or InteriorPointOptions()).to_abi()
     bufs = []
     for m in models:
