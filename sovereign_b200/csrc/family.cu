@@ -24,9 +24,10 @@ namespace sov {
 namespace {
 
 constexpr int kFamThreads = 256;
-constexpr int kFamBlocks = 592;  // 4 CTAs per SM for the grid-stride passes with reductions
+constexpr int kFamBlocks = 296;  // 2 CTAs per SM for the grid-stride passes (the per-LP folds read one partial per CTA)
 constexpr int kWarmGiveUp = 40;  // iterations a supplied start gets before the default restart
 constexpr int kNv = 3;           // reduction slots per pass
+constexpr int kFamPiece = 32;    // terms per piece of the family's sparse schedule
 
 // Per-LP scalars of one iteration (the single engine's IpmScalars for an LP).
 struct FamScalars {
@@ -53,7 +54,10 @@ struct FamDev {
 struct FamSparse {
   int m, levels, W;
   int tail, mt;             // dense trailing block: columns mt .. m-1, factored and solved densely
-  const int* tail_off;      // tail: index into V of column mt + q's first L entry (row mt + q + 1)
+  double* Ld;               // its strict lower triangle, packed by columns (explicit zeros included)
+  const int* tail_off;      // tail column q's first entry (row q + 1) in Ld
+  const int *blk_src, *blk_dst;  // the block's pattern entries: index into V -> index into Ld
+  int blk_n;
   const int *pivot_ptr, *pivot_col;  // the columns before the tail, per level
   double *V, *diag, *inv_d, *work, *partial;  // (m + nnz(L)) x W, m x W, m x W, m x W, slots x W
   const int *perm, *lvl_ptr, *lvl_col, *li;
@@ -402,36 +406,66 @@ __global__ void __launch_bounds__(kFamThreads) k_fam_factor(FamSparse f) {
 // ---- the dense tail (the root clique of the elimination tree), factored per LP by panels of
 // kPanel columns: the panel's diagonal block, the rows below it, then the trailing block's
 // update -- the same operations per entry, in the same column order, as the level schedule ----
-constexpr int kPanel = 16;
+constexpr int kPanel = 16;       // columns per panel of the dense factorization
+constexpr int kSolvePanel = 32;  // rows per panel of the dense solves: a warp's lanes
 
-__device__ __forceinline__ size_t tail_at(const FamSparse& f, int a, int q, int lp) {  // L~_aq, a > q
+// the block's values after the level schedule, scattered from the pattern into the dense storage
+__global__ void k_tail_scatter(FamSparse f) {
+  const long long total = static_cast<long long>(f.blk_n) * f.W;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int q = static_cast<int>(t / f.W), lp = static_cast<int>(t % f.W);
+    f.Ld[static_cast<size_t>(f.blk_dst[q]) * f.W + lp] = f.V[static_cast<size_t>(f.blk_src[q]) * f.W + lp];
+  }
+}
+
+__device__ __forceinline__ size_t tail_at(const FamSparse& f, int a, int q, int lp) {  // L~_aq, a > q, in Ld
   return static_cast<size_t>(f.tail_off[q] + (a - q - 1)) * f.W + lp;
 }
 
-// one CTA of P x W threads (row r of the panel, LP)
+// one CTA of P x W threads (row r of the panel, LP): each thread holds its row of the panel's
+// diagonal block in registers; step j's column is exchanged through shared memory
 __global__ void k_tail_diag(FamSparse f, int j0, int j1) {
+  __shared__ double colv[kPanel][kFamilyWidth];
+  __shared__ double invs[kFamilyWidth];
   const int W = f.W, P = j1 - j0;
   const int r = static_cast<int>(threadIdx.x) / W, lp = static_cast<int>(threadIdx.x) % W;
   const bool on = r < P;
-  for (int j = 0; j < P; ++j) {
-    __syncthreads();
-    if (on && r == j) {
-      const size_t e = static_cast<size_t>(f.mt + j0 + j) * W + lp;
-      const double p = f.V[e];
-      const bool finite = fabs(p) <= 1.7976931348623157e308;
-      const bool drop = !(finite && p > f.drop_tol * fabs(f.diag[e]));
-      if (drop) atomicAdd(&f.sc[lp].drops, 1);
-      if (!finite) atomicExch(&f.sc[lp].fail, 1);
-      f.inv_d[e] = 1.0 / (drop ? 1e128 : p);
-    }
-    __syncthreads();
-    if (on && r > j) {
-      const double lrj = f.V[tail_at(f, j0 + r, j0 + j, lp)];
-      const double inv = f.inv_d[static_cast<size_t>(f.mt + j0 + j) * W + lp];
-      for (int c = j + 1; c <= r; ++c) {
-        const size_t dst = c == r ? static_cast<size_t>(f.mt + j0 + r) * W + lp : tail_at(f, j0 + r, j0 + c, lp);
-        f.V[dst] -= lrj * f.V[tail_at(f, j0 + c, j0 + j, lp)] * inv;
+  double a[kPanel];  // a[c] = L~_rc (c < r), a[r] = D_r
+#pragma unroll
+  for (int c = 0; c < kPanel; ++c)
+    a[c] = (on && c <= r) ? (c == r ? f.V[static_cast<size_t>(f.mt + j0 + r) * W + lp] : f.Ld[tail_at(f, j0 + r, j0 + c, lp)])
+                          : 0.0;
+#pragma unroll
+  for (int j = 0; j < kPanel; ++j) {
+    if (j < P) {  // uniform over the CTA
+      if (on && r == j) {
+        const size_t e = static_cast<size_t>(f.mt + j0 + j) * W + lp;
+        const double p = a[j];
+        const bool finite = fabs(p) <= 1.7976931348623157e308;
+        const bool drop = !(finite && p > f.drop_tol * fabs(f.diag[e]));
+        if (drop) atomicAdd(&f.sc[lp].drops, 1);
+        if (!finite) atomicExch(&f.sc[lp].fail, 1);
+        const double inv = 1.0 / (drop ? 1e128 : p);
+        f.inv_d[e] = inv;
+        invs[lp] = inv;
       }
+      if (on && r > j) colv[r][lp] = a[j];
+      __syncthreads();
+      if (on && r > j) {
+        const double lrj = a[j], inv = invs[lp];
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c)
+          if (c > j && c <= r) a[c] -= lrj * colv[c][lp] * inv;
+      }
+      __syncthreads();
+    }
+  }
+  if (on) {
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) {
+      if (c < r) f.Ld[tail_at(f, j0 + r, j0 + c, lp)] = a[c];
+      if (c == r) f.V[static_cast<size_t>(f.mt + j0 + r) * W + lp] = a[c];
     }
   }
 }
@@ -445,7 +479,7 @@ __global__ void k_tail_rows(FamSparse f, int j0, int j1) {
     const int a = j1 + static_cast<int>(t / W), lp = static_cast<int>(t % W);
     double l[kPanel];
 #pragma unroll
-    for (int c = 0; c < kPanel; ++c) l[c] = c < P ? f.V[tail_at(f, a, j0 + c, lp)] : 0.0;
+    for (int c = 0; c < kPanel; ++c) l[c] = c < P ? f.Ld[tail_at(f, a, j0 + c, lp)] : 0.0;
 #pragma unroll
     for (int j = 1; j < kPanel; ++j) {
       if (j >= P) break;
@@ -453,34 +487,57 @@ __global__ void k_tail_rows(FamSparse f, int j0, int j1) {
 #pragma unroll
       for (int c = 0; c < kPanel; ++c) {
         if (c >= j) break;
-        v -= l[c] * f.V[tail_at(f, j0 + j, j0 + c, lp)] * f.inv_d[static_cast<size_t>(f.mt + j0 + c) * W + lp];
+        v -= l[c] * f.Ld[tail_at(f, j0 + j, j0 + c, lp)] * f.inv_d[static_cast<size_t>(f.mt + j0 + c) * W + lp];
       }
       l[j] = v;
     }
 #pragma unroll
     for (int c = 0; c < kPanel; ++c)
-      if (c < P) f.V[tail_at(f, a, j0 + c, lp)] = l[c];
+      if (c < P) f.Ld[tail_at(f, a, j0 + c, lp)] = l[c];
   }
 }
 
-// the trailing block: entry (a, b), j1 <= b <= a, takes the panel's rank-P update
+// the trailing block: entry (a, b), j1 <= b <= a, takes the panel's rank-P update; a thread per
+// 4 x 4 tile of entries and LP (8 loads of L~ per column of the panel for 16 products)
 __global__ void k_tail_update(FamSparse f, int j0, int j1) {
   const int W = f.W, P = j1 - j0, n = f.tail - j1;
-  const long long pairs = static_cast<long long>(n) * (n + 1) / 2, total = pairs * W;
+  const long long nt = (n + 3) / 4, tiles = nt * (nt + 1) / 2, total = tiles * W;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long pr = t / W;
+    const long long tp = t / W;
     const int lp = static_cast<int>(t % W);
-    long long ai = static_cast<long long>((sqrt(8.0 * static_cast<double>(pr) + 1.0) - 1.0) * 0.5);
-    while (ai * (ai + 1) / 2 > pr) --ai;
-    while ((ai + 1) * (ai + 2) / 2 <= pr) ++ai;
-    const int a = j1 + static_cast<int>(ai), b = j1 + static_cast<int>(pr - ai * (ai + 1) / 2);
-    double acc = 0.0;
-    for (int c = 0; c < P; ++c)
-      acc += f.V[tail_at(f, a, j0 + c, lp)] * f.V[tail_at(f, b, j0 + c, lp)] *
-             f.inv_d[static_cast<size_t>(f.mt + j0 + c) * W + lp];
-    const size_t dst = a == b ? static_cast<size_t>(f.mt + a) * W + lp : tail_at(f, a, b, lp);
-    f.V[dst] -= acc;
+    long long ti = static_cast<long long>((sqrt(8.0 * static_cast<double>(tp) + 1.0) - 1.0) * 0.5);
+    while (ti * (ti + 1) / 2 > tp) --ti;
+    while ((ti + 1) * (ti + 2) / 2 <= tp) ++ti;
+    const int a0 = j1 + 4 * static_cast<int>(ti), b0 = j1 + 4 * static_cast<int>(tp - ti * (ti + 1) / 2);
+    double acc[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[q][r] = 0.0;
+    for (int c = 0; c < P; ++c) {
+      const int col = j0 + c;
+      const double inv = f.inv_d[static_cast<size_t>(f.mt + col) * W + lp];
+      double la[4], lb[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        la[q] = a0 + q < f.tail ? f.Ld[tail_at(f, a0 + q, col, lp)] * inv : 0.0;
+        lb[q] = b0 + q < f.tail ? f.Ld[tail_at(f, b0 + q, col, lp)] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[q][r] += la[q] * lb[r];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int a = a0 + q, b = b0 + r;
+        if (a >= f.tail || b > a) continue;
+        if (a == b) f.V[static_cast<size_t>(f.mt + a) * W + lp] -= acc[q][r];
+        else f.Ld[tail_at(f, a, b, lp)] -= acc[q][r];
+      }
   }
 }
 
@@ -521,35 +578,60 @@ __global__ void __launch_bounds__(kFamThreads) k_fam_solve(FamSparse f, double* 
     g.sync();
   }
   if (f.tail > 0) {
-    // the dense tail, forward then backward, column by column: CTA b takes LPs 32b .. 32b + 31
-    // (lane = LP), its 8 warps split the rows; the other CTAs go straight to the barrier
-    const int lanes = 32, groups = kFamThreads / 32;
-    const int lp = static_cast<int>(blockIdx.x) * lanes + (threadIdx.x & 31), grp = threadIdx.x >> 5;
-    if (static_cast<int>(blockIdx.x) * lanes < W) {
-      const bool on = lp < W;
-      const int T = f.tail, mt = f.mt;
-      auto tl = [&](int a, int q) { return static_cast<size_t>(f.tail_off[q] + (a - q - 1)) * W + lp; };
-      for (int q = 0; q < T; ++q) {  // forward: y_a -= L~_aq / D_q y_q for a > q
-        __syncthreads();
-        if (on) {
-          const size_t eq = static_cast<size_t>(mt + q) * W + lp;
-          const double coef = f.work[eq] * f.inv_d[eq];
-          for (int a = q + 1 + grp; a < T; a += groups) f.work[static_cast<size_t>(mt + a) * W + lp] -= f.V[tl(a, q)] * coef;
+    // The dense tail by panels of kSolvePanel (32) rows. Forward: the panel's triangle, a warp per LP with
+    // lane r holding row j0 + r (y_j / D_j broadcast by shuffle), then every row below the panel
+    // takes the panel's terms (a thread per row and LP). Backward, panels in reverse: the
+    // triangle the same way from its last row, then every row above takes the panel's x terms.
+    // Every barrier is reached by the whole grid.
+    const int T = f.tail, mt = f.mt, lane = threadIdx.x & 31;
+    const long long gwarp = rank >> 5, gwarps = size >> 5;
+    auto w_at = [&](int a, int lp) { return static_cast<size_t>(mt + a) * W + lp; };
+    for (int j0 = 0; j0 < T; j0 += kSolvePanel) {
+      const int P = min(T, j0 + kSolvePanel) - j0, j1 = j0 + P;
+      for (long long wl = gwarp; wl < W; wl += gwarps) {
+        const int lp = static_cast<int>(wl);
+        const bool on = lane < P;
+        double y = on ? f.work[w_at(j0 + lane, lp)] : 0.0;
+        const double inv = on ? f.inv_d[w_at(j0 + lane, lp)] : 0.0;
+        for (int j = 0; j < P; ++j) {
+          const double coef = __shfl_sync(0xffffffffu, y * inv, j);
+          if (on && lane > j) y -= f.Ld[tail_at(f, j0 + lane, j0 + j, lp)] * coef;
         }
+        if (on) f.work[w_at(j0 + lane, lp)] = y;
       }
-      // every thread of the CTA passes every barrier (LPs past W only skip the work between them)
-      for (int q = T - 1; q >= 0; --q) {  // backward: x_q = y'_q / D_q, then y'_a -= L~_qa x_q for a < q
-        __syncthreads();
-        const size_t eq = static_cast<size_t>(mt + q) * W + lp;
-        const double xq = on ? f.work[eq] * f.inv_d[eq] : 0.0;
-        __syncthreads();
-        if (on) {
-          if (grp == 0) f.work[eq] = xq;
-          for (int a = grp; a < q; a += groups) f.work[static_cast<size_t>(mt + a) * W + lp] -= f.V[tl(q, a)] * xq;
-        }
+      g.sync();
+      for (long long t = rank; t < static_cast<long long>(T - j1) * W; t += size) {
+        const int a = j1 + static_cast<int>(t / W), lp = static_cast<int>(t % W);
+        double acc = 0.0;
+        for (int j = j0; j < j1; ++j) acc += f.Ld[tail_at(f, a, j, lp)] * f.work[w_at(j, lp)] * f.inv_d[w_at(j, lp)];
+        f.work[w_at(a, lp)] -= acc;
       }
+      g.sync();
     }
-    g.sync();
+    const int last = (T - 1) / kSolvePanel * kSolvePanel;
+    for (int j0 = last; j0 >= 0; j0 -= kSolvePanel) {
+      const int P = min(T, j0 + kSolvePanel) - j0;
+      for (long long wl = gwarp; wl < W; wl += gwarps) {
+        const int lp = static_cast<int>(wl);
+        const bool on = lane < P;
+        double y = on ? f.work[w_at(j0 + lane, lp)] : 0.0;
+        const double inv = on ? f.inv_d[w_at(j0 + lane, lp)] : 0.0;
+        for (int i = P - 1; i >= 0; --i) {
+          const double xi = __shfl_sync(0xffffffffu, y * inv, i);
+          if (lane == i) y = xi;
+          if (on && lane < i) y -= f.Ld[tail_at(f, j0 + i, j0 + lane, lp)] * xi;
+        }
+        if (on) f.work[w_at(j0 + lane, lp)] = y;
+      }
+      g.sync();
+      for (long long t = rank; t < static_cast<long long>(j0) * W; t += size) {
+        const int k = static_cast<int>(t / W), lp = static_cast<int>(t % W);
+        double acc = 0.0;
+        for (int i = j0; i < j0 + P; ++i) acc += f.Ld[tail_at(f, i, k, lp)] * f.work[w_at(i, lp)];
+        f.work[w_at(k, lp)] -= acc;
+      }
+      g.sync();
+    }
   }
   for (int h = f.levels - 1; h >= 0; --h) {
     const long long pieces = static_cast<long long>(f.upiece_lvl[h + 1] - f.upiece_lvl[h]) * W;
@@ -675,9 +757,12 @@ class Family {
   Buf<int> row_ptr_, col_idx_, col_ptr_, row_idx_, asm_target_, asm_ptr_, asm_col_;
   Buf<double> rval_, cval_, asm_w_;
   Buf<int> perm_, lvl_ptr_, lvl_col_, li_, up_col_, up_a_, up_b_, row_pos_, row_col_;
-  Buf<int> fpl_, fcl_, lpl_, lcl_, upl_, ucl_, tail_off_, pivot_ptr_, pivot_col_;
-  int tail_ = 0;
-  static constexpr int kMinTail = 32;  // smaller root cliques stay in the level schedule
+  Buf<int> fpl_, fcl_, lpl_, lcl_, upl_, ucl_, tail_off_, pivot_ptr_, pivot_col_, blk_src_, blk_dst_;
+  Buf<double> Ld_;
+  int tail_ = 0, blk_n_ = 0;
+  size_t ld_size_ = 0;
+  static constexpr int kMinTail = 32;              // smaller blocks stay in the level schedule
+  static constexpr double kSparseTermCost = 10.0;  // a scheduled rank-1 term, in dense multiply-adds
   Buf<int4> fp_, fc_, lpc_, lc_, upc_, uc_;
   // per chunk (capacity kFamilyWidth LPs)
   Buf<double> b_, c_, bnorm_, cnorm_, x_, s_, y_, dx_, ds_, dxa_, dsa_, rd_, rp_, z_, t_;
@@ -763,14 +848,25 @@ void Family::setup_shared(const StdForm& f) {
     throw std::invalid_argument("sov_lp_solve_family: the sparse L D L' of the order-" + std::to_string(f.m) +
                                 " normal matrix needs more than " + std::to_string(kMaxUpdates) +
                                 " rank-1 update terms");
-  // the root clique of the elimination tree, when large, is factored and solved densely
-  tail_ = sparse_dense_tail(sym_);
-  if (tail_ < kMinTail) tail_ = 0;
-  const SparseSchedule S = sparse_schedule(sym_, tail_);
+  // the trailing block -- the root clique of the elimination tree and the nearly dense columns
+  // before it -- is factored and solved densely when that costs less than scheduling its terms;
+  // one thread per (piece, LP): long items are cut into short pieces
+  tail_ = sparse_dense_block(sym_, kSparseTermCost, kMinTail);
+  const SparseSchedule S = sparse_schedule(sym_, tail_, kFamPiece);
   {
-    std::vector<int> off(std::max(1, tail_));
-    for (int q = 0; q < tail_; ++q) off[q] = f.m + sym_.lp[f.m - tail_ + q];
+    const int T = tail_, mt = f.m - T;
+    std::vector<int> off(std::max(1, T)), src, dst;
+    for (int q = 0; q < T; ++q) off[q] = q * (T - 1) - q * (q - 1) / 2;
+    for (int q = 0; q < T; ++q)
+      for (int p = sym_.lp[mt + q]; p < sym_.lp[mt + q + 1]; ++p) {
+        src.push_back(f.m + p);
+        dst.push_back(off[q] + (sym_.li[p] - (mt + q) - 1));
+      }
     tail_off_.put(off, st_);
+    blk_src_.put(src, st_);
+    blk_dst_.put(dst, st_);
+    blk_n_ = static_cast<int>(src.size());
+    ld_size_ = static_cast<size_t>(T) * (T > 0 ? T - 1 : 0) / 2;
   }
   pivot_ptr_.put(S.pivot_ptr, st_);
   pivot_col_.put(S.pivot_col, st_);
@@ -823,6 +919,7 @@ void Family::setup_shared(const StdForm& f) {
   part_.alloc(static_cast<size_t>(kFamBlocks) * kNv * W);
   part_rows_.alloc(static_cast<size_t>(kFamBlocks) * kNv * W);
   V_.alloc((m + sym_.li.size()) * W);
+  Ld_.alloc(std::max<size_t>(1, ld_size_) * W);
   partial_.alloc(static_cast<size_t>(slots_) * W);
   sc_.alloc(W);
   step_.alloc(W);
@@ -841,6 +938,10 @@ void Family::setup_shared(const StdForm& f) {
   sp_.tail = tail_;
   sp_.mt = f.m - tail_;
   sp_.tail_off = tail_off_.p;
+  sp_.Ld = Ld_.p;
+  sp_.blk_src = blk_src_.p;
+  sp_.blk_dst = blk_dst_.p;
+  sp_.blk_n = blk_n_;
   sp_.pivot_ptr = pivot_ptr_.p;
   sp_.pivot_col = pivot_col_.p;
   sp_.V = V_.p;
@@ -924,12 +1025,17 @@ void Family::factor() {
   void* args[] = {&f};
   SOV_CUDA(cudaLaunchCooperativeKernel((const void*)k_fam_factor, dim3(sms_ * per_sm_factor_), dim3(kFamThreads), args,
                                        0, st_));
+  if (tail_ > 0) {
+    SOV_CUDA(cudaMemsetAsync(Ld_.p, 0, sizeof(double) * ld_size_ * sp_.W, st_));
+    const long long total = static_cast<long long>(blk_n_) * sp_.W;
+    k_tail_scatter<<<static_cast<int>(std::max(1LL, std::min(8LL * sms_, (total + 255) / 256))), 256, 0, st_>>>(sp_);
+  }
   for (int j0 = 0; j0 < tail_; j0 += kPanel) {
     const int j1 = std::min(tail_, j0 + kPanel), W = sp_.W;
     k_tail_diag<<<1, (j1 - j0) * W, 0, st_>>>(sp_, j0, j1);
     if (j1 < tail_) {
       const long long rows = static_cast<long long>(tail_ - j1) * W;
-      const long long n = tail_ - j1, pairs = n * (n + 1) / 2 * W;
+      const long long n = tail_ - j1, nt = (n + 3) / 4, pairs = nt * (nt + 1) / 2 * W;
       k_tail_rows<<<static_cast<int>(std::max(1LL, std::min(8LL * sms_, (rows + 255) / 256))), 256, 0, st_>>>(sp_, j0, j1);
       k_tail_update<<<static_cast<int>(std::max(1LL, std::min(16LL * sms_, (pairs + 255) / 256))), 256, 0, st_>>>(sp_, j0,
                                                                                                             j1);

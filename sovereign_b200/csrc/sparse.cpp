@@ -645,22 +645,21 @@ bool sparse_analyze_graph(const std::vector<std::vector<int>>& adj0, std::size_t
 
 namespace {
 
-void add_item(SparsePieces& P, int first, int end, int target, int* slots, bool keep_empty) {
+void add_item(SparsePieces& P, int first, int end, int target, int* slots, bool keep_empty, int piece = kSparsePiece) {
   const int len = end - first;
   if (len == 0 && !keep_empty) return;
   if (len <= kSparseShort) {
     P.piece.push_back({first, end, target, -1});
     return;
   }
-  if (len <= kSparsePiece) {
+  if (len <= piece) {
     P.pending_long.push_back({first, end, target, -1});
     return;
   }
-  const int n = (len + kSparsePiece - 1) / kSparsePiece;
+  const int n = (len + piece - 1) / piece;
   P.comb.push_back({target, *slots, n, 0});
   for (int q = 0; q < n; ++q)
-    P.pending_long.push_back(
-        {first + q * kSparsePiece, std::min(end, first + (q + 1) * kSparsePiece), target, *slots + q});
+    P.pending_long.push_back({first + q * piece, std::min(end, first + (q + 1) * piece), target, *slots + q});
   *slots += n;
 }
 
@@ -688,7 +687,27 @@ int sparse_dense_tail(const SparseSymbolic& s) {
   return t;
 }
 
-SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail) {
+int sparse_dense_block(const SparseSymbolic& s, double sparse_cost, int min_block) {
+  const int m = s.m, full = sparse_dense_tail(s);
+  // terms of the columns before k: prefix sums of colcount (colcount + 1) / 2
+  std::vector<double> before(m + 1, 0.0);
+  for (int k = 0; k < m; ++k) {
+    const double c = s.lp[k + 1] - s.lp[k];
+    before[k + 1] = before[k] + 0.5 * c * (c + 1.0);
+  }
+  int best = 0;
+  double best_cost = sparse_cost * before[m];
+  for (int T = std::max(full, 1); T <= m; T += (T < full + 16 ? 1 : 16)) {
+    const double cost = sparse_cost * before[m - T] + static_cast<double>(T) * T * T / 6.0;
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = T;
+    }
+  }
+  return best >= min_block ? best : 0;
+}
+
+SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail, int piece) {
   SparseSchedule S;
   const int m = s.m, levels = s.levels(), mt = m - tail;
   S.tail = tail;
@@ -748,7 +767,7 @@ SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail) {
       const int dst = s.pairs[4 * order[q] + 3];
       size_t e = q + 1;
       while (e < n_up && level_of[order[e]] == h && s.pairs[4 * order[e] + 3] == dst) ++e;
-      add_item(S.factor, static_cast<int>(q), static_cast<int>(e), dst, &S.factor_slots, false);
+      add_item(S.factor, static_cast<int>(q), static_cast<int>(e), dst, &S.factor_slots, false, piece);
       q = e;
     }
     close_level(S.factor);
@@ -771,7 +790,7 @@ SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail) {
   for (int h = 0; h < hn; ++h) {
     for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) {
       const int k = s.lvl_col[c];
-      if (k < mt) add_item(S.forward, row_ptr[k], row_ptr[k + 1], k, &S.solve_slots, false);
+      if (k < mt) add_item(S.forward, row_ptr[k], row_ptr[k + 1], k, &S.solve_slots, false, piece);
     }
     close_level(S.forward);
   }
@@ -779,14 +798,14 @@ SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail) {
     for (int k = mt; k < m; ++k) {
       int e = row_ptr[k];
       while (e < row_ptr[k + 1] && S.row_col[e] < mt) ++e;
-      add_item(S.forward, row_ptr[k], e, k, &S.solve_slots, false);
+      add_item(S.forward, row_ptr[k], e, k, &S.solve_slots, false, piece);
     }
     close_level(S.forward);
   }
   for (int h = 0; h < hn; ++h) {  // every column, empty ones too (x_k = y_k / D_k)
     for (int c = s.lvl_ptr[h]; c < s.lvl_ptr[h + 1]; ++c) {
       const int k = s.lvl_col[c];
-      if (k < mt) add_item(S.backward, s.lp[k], s.lp[k + 1], k, &S.solve_slots, true);
+      if (k < mt) add_item(S.backward, s.lp[k], s.lp[k + 1], k, &S.solve_slots, true, piece);
     }
     close_level(S.backward);
   }

@@ -100,12 +100,20 @@ struct SparseSchedule {
   std::vector<int> pivot_ptr, pivot_col;
 };
 
-SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail = 0);
+// piece: the longest piece (items beyond it are cut); a schedule walked by one thread per piece
+// takes short pieces
+SparseSchedule sparse_schedule(const SparseSymbolic& s, int tail = 0, int piece = kSparsePiece);
 
 // The trailing columns of L whose pattern is every later row (a dense trailing block: the root
 // clique of the elimination tree). Their L entries are stored column by column, rows ascending,
 // so the block is a column-packed lower triangle inside [D | L].
 int sparse_dense_tail(const SparseSymbolic& s);
+
+// The trailing block worth factoring densely: the T (at least the dense tail) minimizing
+// sparse_cost * (rank-1 terms left to the level schedule) + (T^3 / 6 dense multiply-adds), the
+// explicit zeros of a nearly dense block included. sparse_cost: a scheduled term's cost in dense
+// multiply-adds. 0 when no block of at least min_block columns pays.
+int sparse_dense_block(const SparseSymbolic& s, double sparse_cost, int min_block);
 
 // The rows of a CSR pattern (ptr, rows + 1 entries) as pieces of one level: target = row; the
 // combine entries hold the rows that were cut, slots numbered from 0.

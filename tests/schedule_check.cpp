@@ -80,15 +80,17 @@ static Sys clique(int n, int c, unsigned seed) {
 }
 
 // the kernels' walk of the schedule, sequential
-static long long run(const Sys& S, SparseOrder order, const char* name, bool use_tail = false) {
+static long long run(const Sys& S, SparseOrder order, const char* name, bool use_tail = false, int piece = kSparsePiece,
+                     int extra = 0) {
   SparseSymbolic s;
   if (!sparse_analyze_graph(S.adj, 0, s, order)) {
     std::printf("%s: analysis refused\n", name);
     return 1;
   }
   const int m = s.m;
-  const int T = use_tail ? sparse_dense_tail(s) : 0, mt = m - T;
-  const SparseSchedule P = sparse_schedule(s, T);
+  // the dense trailing block: the full-pattern tail, or more columns (explicit zeros included)
+  const int T = use_tail ? std::min(m, sparse_dense_tail(s) + extra) : 0, mt = m - T;
+  const SparseSchedule P = sparse_schedule(s, T, piece);
   long long bad = 0;
   // every update term, row entry and column entry is covered exactly once by the pieces
   auto cover = [&](const SparsePieces& pc, size_t total, const char* what) {
@@ -169,7 +171,11 @@ static long long run(const Sys& S, SparseOrder order, const char* name, bool use
       V[cb.target] -= t;
     }
   }
-  auto lt = [&](int a, int k) -> double& { return V[m + s.lp[k] + (a - k - 1)]; };  // L~_ak, k in the tail
+  // the block's strict lower triangle, dense (rows and columns relative to mt), from the pattern
+  std::vector<double> Ld(static_cast<size_t>(T) * T, 0.0);
+  for (int k = mt; k < m; ++k)
+    for (int p = s.lp[k]; p < s.lp[k + 1]; ++p) Ld[static_cast<size_t>(s.li[p] - mt) * T + (k - mt)] = V[m + p];
+  auto lt = [&](int a, int k) -> double& { return Ld[static_cast<size_t>(a - mt) * T + (k - mt)]; };  // L~_ak
   for (int k = mt; k < m; ++k) {  // the dense tail, column by column
     const double p = V[k];
     const bool drop = !(sg[k] * p > 0.0);
@@ -252,6 +258,10 @@ int main() {
     failures += run(make(3000, 0, false, 1), o, "definite, dense row, N=3000", true);
     failures += run(make(2500, 150, true, 2), o, "quasi-definite, dense row, N=2650", true);
     failures += run(clique(600, 80, 5), o, "definite, 80-node clique, N=600", true);
+    failures += run(clique(600, 80, 5), o, "definite, 80-node clique, N=600, 32-term pieces", true, 32);
+    failures += run(make(2500, 150, true, 2), o, "quasi-definite, dense row, N=2650, 32-term pieces", true, 32);
+    failures += run(clique(600, 80, 5), o, "definite, 80-node clique + 60 sparse columns densely", true, 32, 60);
+    failures += run(make(2500, 150, true, 2), o, "quasi-definite, dense row + 300 columns densely", true, 32, 300);
   }
   std::printf("failures %lld\n", failures);
   return failures == 0 ? 0 : 1;
