@@ -336,6 +336,33 @@ __global__ void k_fam_copy(int count, int W, const int* mask, double* dst, const
     if (mask[t % W]) dst[t] = src[t];
 }
 
+// ---- moving one LP's vector between its slot of the interleaved arrays and contiguous storage ----
+// slot column slot[i] of dst <- src + i * len, for i < count
+__global__ void k_slot_put(double* dst, int len, int W, const int* slot, const double* src, int count) {
+  const long long total = static_cast<long long>(count) * len;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(t / len), e = static_cast<int>(t % len);
+    dst[static_cast<size_t>(e) * W + slot[i]] = src[t];
+  }
+}
+
+// dst + i * len <- slot column slot[i] of src, for i < count
+__global__ void k_slot_get(double* dst, int len, int W, const int* slot, const double* src, int count) {
+  const long long total = static_cast<long long>(count) * len;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(t / len), e = static_cast<int>(t % len);
+    dst[t] = src[static_cast<size_t>(e) * W + slot[i]];
+  }
+}
+
+__global__ void k_fill(double* v, long long count, double value) {
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < count;
+       t += static_cast<long long>(gridDim.x) * blockDim.x)
+    v[t] = value;
+}
+
 // ---- normal matrices A D_k A' + 1e-12 I into the shared pattern (LP weights x/s, or 1) ----
 __global__ void k_fam_assemble(FamAssembly am, FamDev d, FamSparse f, int ones) {
   const long long total = static_cast<long long>(am.ntargets) * d.W;
@@ -732,10 +759,12 @@ class Family {
 
  private:
   void setup_shared(const StdForm& f);
-  void solve_chunk(const std::vector<int>& lps);
-  void publish(LpState& L, const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& s,
-               const std::vector<double>& cx, const std::vector<double>& cy, const std::vector<double>& cs, int k,
-               int W, double seconds);
+  void solve_wave(const std::vector<int>& lps);
+  // one LP's result from its vectors (contiguous; cx/cy/cs null unless captured)
+  void publish(LpState& l, const double* x, const double* y, const double* s, const double* cx, const double* cy,
+               const double* cs, double seconds);
+  void put_slots(double* dst, int len, const int* slots, const double* src, int count);
+  void get_slots(double* dst, int len, const int* slots, const double* src, int count);
   std::string describe() const;
   // launches over (entries, LPs)
   int grid_for(int items) const { return std::max(1, std::min(kFamBlocks, (items + dev_.G - 1) / dev_.G)); }
@@ -762,6 +791,7 @@ class Family {
   int tail_ = 0, blk_n_ = 0;
   size_t ld_size_ = 0;
   static constexpr int kMinTail = 32;              // smaller blocks stay in the level schedule
+  static constexpr size_t kWave = 2048;            // LPs whose data and start points sit on the device
   static constexpr double kSparseTermCost = 10.0;  // a scheduled rank-1 term, in dense multiply-adds
   Buf<int4> fp_, fc_, lpc_, lc_, upc_, uc_;
   // per chunk (capacity kFamilyWidth LPs)
@@ -835,9 +865,11 @@ int Family::run() {
   }
   if (members.empty()) return SOV_OK;
   setup_shared(forms_[members[0]]);
-  for (size_t c0 = 0; c0 < members.size(); c0 += kFamilyWidth) {
-    const size_t c1 = std::min(members.size(), c0 + kFamilyWidth);
-    solve_chunk(std::vector<int>(members.begin() + c0, members.begin() + c1));
+  // waves of at most kWave LPs (their data and start points sit on the device); inside a wave
+  // the W slots are refilled as LPs finish
+  for (size_t c0 = 0; c0 < members.size(); c0 += kWave) {
+    const size_t c1 = std::min(members.size(), c0 + kWave);
+    solve_wave(std::vector<int>(members.begin() + c0, members.begin() + c1));
   }
   return SOV_OK;
 }
@@ -1068,13 +1100,18 @@ std::string Family::describe() const {
   return buf;
 }
 
+// a slot's failure flags cleared (a restart, or the next LP taking the slot)
 __global__ void k_fam_clear_fail(FamScalars* sc, const int* mask, int W) {
   const int k = threadIdx.x;
-  if (k < W && (!mask || mask[k])) sc[k].fail = 0;
+  if (k < W && (!mask || mask[k])) {
+    sc[k].fail = 0;
+    sc[k].skipped = 0;
+  }
 }
 
-void Family::solve_chunk(const std::vector<int>& lps) {
-  const int W = static_cast<int>(lps.size());
+void Family::solve_wave(const std::vector<int>& lps) {
+  const int count = static_cast<int>(lps.size());
+  const int W = std::min(kFamilyWidth, count);
   const StdForm& f0 = forms_[lps[0]];
   const int n = f0.n, m = f0.m;
   dev_.W = W;
@@ -1082,148 +1119,269 @@ void Family::solve_chunk(const std::vector<int>& lps) {
   dev_.tau = opts_[lps[0]].fraction_to_boundary;
   sp_.W = W;
   const auto t_start = std::chrono::steady_clock::now();
-  // right-hand sides and costs, interleaved; their norms (max(1, max |.|) of the scaled problem)
+  const int bd = W * dev_.G, gn = grid_for(n);
+  const size_t smem = sizeof(double) * kNv * bd;
+  // ---- the wave's data on the device, one LP after another: b, c and the default starts ----
+  Buf<double> bpool, cpool, x0p, y0p, s0p, stage;
+  Buf<int> slot_dev, iota_dev;
+  std::vector<double> bn(count), cn(count);
   {
-    std::vector<double> bI(static_cast<size_t>(m) * W), cI(static_cast<size_t>(n) * W), bn(W), cn(W);
-    for (int k = 0; k < W; ++k) {
-      const StdForm& f = forms_[lps[k]];
+    std::vector<double> hb(static_cast<size_t>(count) * m), hc(static_cast<size_t>(count) * n);
+    for (int i = 0; i < count; ++i) {
+      const StdForm& f = forms_[lps[i]];
+      std::copy(f.b.begin(), f.b.end(), hb.begin() + static_cast<size_t>(i) * m);
+      std::copy(f.c.begin(), f.c.end(), hc.begin() + static_cast<size_t>(i) * n);
       double bm = 0.0, cm = 0.0;
-      for (int i = 0; i < m; ++i) {
-        bI[static_cast<size_t>(i) * W + k] = f.b[i];
-        bm = std::max(bm, std::abs(f.b[i]));
-      }
-      for (int j = 0; j < n; ++j) {
-        cI[static_cast<size_t>(j) * W + k] = f.c[j];
-        cm = std::max(cm, std::abs(f.c[j]));
-      }
-      bn[k] = std::max(1.0, bm);
-      cn[k] = std::max(1.0, cm);
+      for (double v : f.b) bm = std::max(bm, std::abs(v));
+      for (double v : f.c) cm = std::max(cm, std::abs(v));
+      bn[i] = std::max(1.0, bm);  // max(1, max |.|) of the scaled problem
+      cn[i] = std::max(1.0, cm);
     }
-    SOV_CUDA(cudaMemcpyAsync(b_.p, bI.data(), sizeof(double) * bI.size(), cudaMemcpyHostToDevice, st_));
-    SOV_CUDA(cudaMemcpyAsync(c_.p, cI.data(), sizeof(double) * cI.size(), cudaMemcpyHostToDevice, st_));
-    SOV_CUDA(cudaMemcpyAsync(bnorm_.p, bn.data(), sizeof(double) * W, cudaMemcpyHostToDevice, st_));
-    SOV_CUDA(cudaMemcpyAsync(cnorm_.p, cn.data(), sizeof(double) * W, cudaMemcpyHostToDevice, st_));
-    SOV_CUDA(cudaMemsetAsync(sc_.p, 0, sizeof(FamScalars) * W, st_));
+    bpool.put(hb, st_);
+    cpool.put(hc, st_);
     SOV_CUDA(cudaStreamSynchronize(st_));
   }
-  std::vector<LpState> L(W);
-  for (int k = 0; k < W; ++k) {
-    const StdForm& f = forms_[lps[k]];
-    L[k].idx = lps[k];
-    L[k].o = opts_[lps[k]];
-    sov_diagnostics& dg = L[k].dg;
-    dg.scaling_applied = f.scaling_applied;
-    dg.coefficient_min_abs_before = f.coef_min_before;
-    dg.coefficient_max_abs_before = f.coef_max_before;
-    dg.coefficient_min_abs_after = f.coef_min_after;
-    dg.coefficient_max_abs_after = f.coef_max_after;
-    dg.stall_iteration = -1;
+  x0p.alloc(static_cast<size_t>(count) * n);
+  s0p.alloc(static_cast<size_t>(count) * n);
+  y0p.alloc(static_cast<size_t>(count) * m);
+  stage.alloc(static_cast<size_t>(W) * (2 * n + m));
+  slot_dev.alloc(W);
+  {
+    std::vector<int> iota(W);
+    for (int k = 0; k < W; ++k) iota[k] = k;
+    iota_dev.put(iota, st_);
   }
-  const int gn = grid_for(n), bd = W * dev_.G;
-  const size_t smem = sizeof(double) * kNv * bd;
+  // slot norms, held on the host and uploaded whole when they change
+  std::vector<double> bnorm_h(W, 1.0), cnorm_h(W, 1.0);
+  auto put_norms = [&]() {
+    SOV_CUDA(cudaMemcpyAsync(bnorm_.p, bnorm_h.data(), sizeof(double) * W, cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(cnorm_.p, cnorm_h.data(), sizeof(double) * W, cudaMemcpyHostToDevice, st_));
+  };
   std::vector<int> hmask(W);
-  auto put_mask = [&](Buf<int>& b) {
-    SOV_CUDA(cudaMemcpyAsync(b.p, hmask.data(), sizeof(int) * W, cudaMemcpyHostToDevice, st_));
+  auto put_mask = [&]() {
+    SOV_CUDA(cudaMemcpyAsync(mask_.p, hmask.data(), sizeof(int) * W, cudaMemcpyHostToDevice, st_));
   };
   auto read_scalars = [&]() {
     SOV_CUDA(cudaMemcpyAsync(hsc_, sc_.p, sizeof(FamScalars) * W, cudaMemcpyDeviceToHost, st_));
     SOV_CUDA(cudaStreamSynchronize(st_));
   };
-  // ---- default start, kept in (x0, y0, s0) for restarts: A A' dy = b - A 1 ----
-  assemble(true);
-  factor();
-  k_fam_start_rhs<<<grid_for(m), bd, 0, st_>>>(dev_);
-  solve(z_.p);
-  k_fam_start_point<<<grid_for(std::max(n, m)), bd, 0, st_>>>(dev_, x0_.p, y0_.p, s0_.p);
-  SOV_LAUNCH_CHECK();
-  SOV_CUDA(cudaMemcpyAsync(x_.p, x0_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
-  SOV_CUDA(cudaMemcpyAsync(s_.p, s0_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
-  SOV_CUDA(cudaMemcpyAsync(y_.p, y0_.p, sizeof(double) * m * W, cudaMemcpyDeviceToDevice, st_));
-  for (auto& l : L) l.factorizations = 1;
-  // ---- supplied starts, kept only when their residual metric is within 10x the default start's
-  // and their mu is not larger (the single engine's safeguard) ----
-  bool any_warm = false;
-  for (auto& l : L) any_warm |= l.o.warm_x && l.o.warm_y && l.o.warm_s;
-  if (any_warm) {
+  // slots of unused width hold finite values: every per-LP pass reads its own slot only
+  k_fill<<<sms_, 256, 0, st_>>>(x_.p, static_cast<long long>(n) * W, 1.0);
+  k_fill<<<sms_, 256, 0, st_>>>(s_.p, static_cast<long long>(n) * W, 1.0);
+  k_fill<<<sms_, 256, 0, st_>>>(y_.p, static_cast<long long>(m) * W, 0.0);
+  SOV_CUDA(cudaMemsetAsync(sc_.p, 0, sizeof(FamScalars) * W, st_));
+  // supplied starts: a host copy of those that are kept, uploaded when the LP takes a slot
+  std::vector<char> warm_used(count, 0);
+  auto warm_of = [&](int i) {
+    const sov_options& o = opts_[lps[i]];
+    return o.warm_x && o.warm_y && o.warm_s;
+  };
+  // ---- default starts (Engine::run's default_start): A A' dy = b - A 1 for W LPs at a time; the
+  // supplied starts judged against them by the single engine's safeguard ----
+  for (int g0 = 0; g0 < count; g0 += W) {
+    const int G = std::min(W, count - g0);
+    put_slots(b_.p, m, iota_dev.p, bpool.p + static_cast<size_t>(g0) * m, G);
+    put_slots(c_.p, n, iota_dev.p, cpool.p + static_cast<size_t>(g0) * n, G);
+    for (int k = 0; k < G; ++k) {
+      bnorm_h[k] = bn[g0 + k];
+      cnorm_h[k] = cn[g0 + k];
+    }
+    put_norms();
+    SOV_CUDA(cudaMemsetAsync(sc_.p, 0, sizeof(FamScalars) * W, st_));
+    assemble(true);
+    factor();
+    k_fam_start_rhs<<<grid_for(m), bd, 0, st_>>>(dev_);
+    solve(z_.p);
+    k_fam_start_point<<<grid_for(std::max(n, m)), bd, 0, st_>>>(dev_, x0_.p, y0_.p, s0_.p);
+    SOV_LAUNCH_CHECK();
+    get_slots(x0p.p + static_cast<size_t>(g0) * n, n, iota_dev.p, x0_.p, G);
+    get_slots(s0p.p + static_cast<size_t>(g0) * n, n, iota_dev.p, s0_.p, G);
+    get_slots(y0p.p + static_cast<size_t>(g0) * m, m, iota_dev.p, y0_.p, G);
+    bool any_warm = false;
+    for (int k = 0; k < G; ++k) any_warm |= warm_of(g0 + k);
+    if (!any_warm) continue;
+    SOV_CUDA(cudaMemcpyAsync(x_.p, x0_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(s_.p, s0_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(y_.p, y0_.p, sizeof(double) * m * W, cudaMemcpyDeviceToDevice, st_));
     residuals();
     read_scalars();
-    std::vector<double> dmetric(W), dmu(W);
-    for (int k = 0; k < W; ++k) {
+    std::vector<double> dmetric(G), dmu(G);
+    for (int k = 0; k < G; ++k) {
       dmetric[k] = hsc_[k].metric;
       dmu[k] = hsc_[k].mu;
     }
-    std::vector<double> hx(static_cast<size_t>(n) * W), hs(hx.size()), hy(static_cast<size_t>(m) * W);
-    SOV_CUDA(cudaMemcpyAsync(hx.data(), x_.p, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st_));
-    SOV_CUDA(cudaMemcpyAsync(hs.data(), s_.p, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st_));
-    SOV_CUDA(cudaMemcpyAsync(hy.data(), y_.p, sizeof(double) * hy.size(), cudaMemcpyDeviceToHost, st_));
-    SOV_CUDA(cudaStreamSynchronize(st_));
-    for (int k = 0; k < W; ++k) {
-      const sov_options& o = L[k].o;
-      if (!(o.warm_x && o.warm_y && o.warm_s)) continue;
-      for (int j = 0; j < n; ++j) {
-        hx[static_cast<size_t>(j) * W + k] = o.warm_x[j];
-        hs[static_cast<size_t>(j) * W + k] = o.warm_s[j];
-      }
-      for (int i = 0; i < m; ++i) hy[static_cast<size_t>(i) * W + k] = o.warm_y[i];
+    // the supplied starts into their slots: x | s | y of each, staged contiguously
+    std::vector<int> ws;
+    std::vector<double> hx, hs, hy;
+    for (int k = 0; k < G; ++k) {
+      if (!warm_of(g0 + k)) continue;
+      const sov_options& o = opts_[lps[g0 + k]];
+      ws.push_back(k);
+      hx.insert(hx.end(), o.warm_x, o.warm_x + n);
+      hs.insert(hs.end(), o.warm_s, o.warm_s + n);
+      hy.insert(hy.end(), o.warm_y, o.warm_y + m);
     }
-    SOV_CUDA(cudaMemcpyAsync(x_.p, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, st_));
-    SOV_CUDA(cudaMemcpyAsync(s_.p, hs.data(), sizeof(double) * hs.size(), cudaMemcpyHostToDevice, st_));
-    SOV_CUDA(cudaMemcpyAsync(y_.p, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice, st_));
+    const int nw = static_cast<int>(ws.size());
+    SOV_CUDA(cudaMemcpyAsync(slot_dev.p, ws.data(), sizeof(int) * nw, cudaMemcpyHostToDevice, st_));
+    double* sx = stage.p;
+    double* ss = sx + static_cast<size_t>(nw) * n;
+    double* sy = ss + static_cast<size_t>(nw) * n;
+    SOV_CUDA(cudaMemcpyAsync(sx, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(ss, hs.data(), sizeof(double) * hs.size(), cudaMemcpyHostToDevice, st_));
+    SOV_CUDA(cudaMemcpyAsync(sy, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice, st_));
+    put_slots(x_.p, n, slot_dev.p, sx, nw);
+    put_slots(s_.p, n, slot_dev.p, ss, nw);
+    put_slots(y_.p, m, slot_dev.p, sy, nw);
     residuals();
     read_scalars();
-    for (int k = 0; k < W; ++k) {
-      const sov_options& o = L[k].o;
-      const bool supplied = o.warm_x && o.warm_y && o.warm_s;
+    for (int k : ws) {
       const FamScalars& sc = hsc_[k];
-      L[k].warm_used = supplied && std::isfinite(sc.metric) && std::isfinite(sc.mu) && sc.metric <= 10.0 * dmetric[k] &&
-                       sc.mu <= dmu[k];
-      hmask[k] = supplied && !L[k].warm_used;  // rejected: back to the default start
+      warm_used[g0 + k] = std::isfinite(sc.metric) && std::isfinite(sc.mu) && sc.metric <= 10.0 * dmetric[k] &&
+                          sc.mu <= dmu[k];
     }
-    put_mask(mask_);
-    copy(n, mask_.p, x_.p, x0_.p);
-    copy(n, mask_.p, s_.p, s0_.p);
-    copy(m, mask_.p, y_.p, y0_.p);
   }
-  for (auto& l : L) l.dg.warm_start_used = l.warm_used ? 1 : 0;
-  k_fam_clear_fail<<<1, kFamilyWidth, 0, st_>>>(sc_.p, nullptr, W);
-  SOV_CUDA(cudaMemcpyAsync(bx_.p, x_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
-  SOV_CUDA(cudaMemcpyAsync(bs_.p, s_.p, sizeof(double) * n * W, cudaMemcpyDeviceToDevice, st_));
-  SOV_CUDA(cudaMemcpyAsync(by_.p, y_.p, sizeof(double) * m * W, cudaMemcpyDeviceToDevice, st_));
-  // ---- the iteration loop (Engine::run's decisions, per LP; stepping LPs move together) ----
-  enum Source { kCurrent, kBest };
-  std::vector<int> source(W, kCurrent);
+  // ---- the iteration loop: W slots, each running one LP through Engine::run's decisions; a slot
+  // whose LP has finished takes the next LP of the wave ----
+  std::vector<int> slot_lp(W, -1), it_of(W, 0);
+  std::vector<LpState> L(W);
+  int next = 0;
   std::vector<int> hstep(W), hbest(W), hrestart(W), hcap(W);
   const char* fail_text =
       "IPM stopped because the affine predictor factorization failed; the best iterate is returned with optimality "
       "unproven.";
-  auto finish_best = [&](LpState& l, int k, const std::string& msg) {
-    l.active = false;
-    source[k] = kBest;
-    l.msg = msg;
+  // results of finished LPs: their vectors gathered from the slots, then published on the host
+  std::vector<double> hres;
+  Buf<double> out;
+  out.alloc(static_cast<size_t>(W) * 3 * (2 * n + m));
+  auto retire = [&](const std::vector<int>& done, const std::vector<char>& from_best) {
+    const int F = static_cast<int>(done.size());
+    if (!F) return;
+    bool any_cap = false;
+    for (int k : done) any_cap |= L[k].captured;
+    const size_t per = static_cast<size_t>(2 * n + m) * (any_cap ? 3 : 2);
+    SOV_CUDA(cudaMemcpyAsync(slot_dev.p, done.data(), sizeof(int) * F, cudaMemcpyHostToDevice, st_));
+    // layout per block: current x (F n) | s (F n) | y (F m), then the best ones, then captured
+    const double* src[3][3] = {{x_.p, s_.p, y_.p}, {bx_.p, bs_.p, by_.p}, {cx_.p, cs_.p, cy_.p}};
+    const size_t blk = static_cast<size_t>(2 * n + m) * F;
+    for (int b = 0; b < (any_cap ? 3 : 2); ++b) {
+      double* o = out.p + b * blk;
+      get_slots(o, n, slot_dev.p, src[b][0], F);
+      get_slots(o + static_cast<size_t>(F) * n, n, slot_dev.p, src[b][1], F);
+      get_slots(o + static_cast<size_t>(2 * F) * n, m, slot_dev.p, src[b][2], F);
+    }
+    hres.resize(per * F);
+    SOV_CUDA(cudaMemcpyAsync(hres.data(), out.p, sizeof(double) * hres.size(), cudaMemcpyDeviceToHost, st_));
+    SOV_CUDA(cudaStreamSynchronize(st_));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    for (int i = 0; i < F; ++i) {
+      const int k = done[i];
+      const double* o = hres.data() + (from_best[i] ? blk : 0);
+      const double* c = any_cap && L[k].captured ? hres.data() + 2 * blk : nullptr;
+      publish(L[k], o + static_cast<size_t>(i) * n, o + static_cast<size_t>(2 * F) * n + static_cast<size_t>(i) * m,
+              o + static_cast<size_t>(F) * n + static_cast<size_t>(i) * n,
+              c ? c + static_cast<size_t>(i) * n : nullptr,
+              c ? c + static_cast<size_t>(2 * F) * n + static_cast<size_t>(i) * m : nullptr,
+              c ? c + static_cast<size_t>(F) * n + static_cast<size_t>(i) * n : nullptr, secs);
+      slot_lp[k] = -1;
+    }
   };
-  for (int it = 0;; ++it) {
+  // free slots take the next LPs: data, start (default or the kept supplied one), bookkeeping
+  auto refill = [&]() {
+    std::vector<int> fs;
+    for (int k = 0; k < W && next + static_cast<int>(fs.size()) < count; ++k)
+      if (slot_lp[k] < 0) fs.push_back(k);
+    const int F = static_cast<int>(fs.size());
+    if (!F) return;
+    const int c0 = next;
+    next += F;
+    SOV_CUDA(cudaMemcpyAsync(slot_dev.p, fs.data(), sizeof(int) * F, cudaMemcpyHostToDevice, st_));
+    put_slots(b_.p, m, slot_dev.p, bpool.p + static_cast<size_t>(c0) * m, F);
+    put_slots(c_.p, n, slot_dev.p, cpool.p + static_cast<size_t>(c0) * n, F);
+    put_slots(x_.p, n, slot_dev.p, x0p.p + static_cast<size_t>(c0) * n, F);
+    put_slots(s_.p, n, slot_dev.p, s0p.p + static_cast<size_t>(c0) * n, F);
+    put_slots(y_.p, m, slot_dev.p, y0p.p + static_cast<size_t>(c0) * m, F);
+    std::vector<int> ws;
+    std::vector<double> hx, hs, hy;
+    std::fill(hmask.begin(), hmask.end(), 0);
+    for (int i = 0; i < F; ++i) {
+      const int k = fs[i], w = c0 + i;
+      hmask[k] = 1;
+      slot_lp[k] = w;
+      it_of[k] = 0;
+      bnorm_h[k] = bn[w];
+      cnorm_h[k] = cn[w];
+      LpState& l = L[k];
+      l = LpState{};
+      l.idx = lps[w];
+      l.o = opts_[lps[w]];
+      l.factorizations = 1;  // the start system's
+      l.warm_used = warm_used[w] != 0;
+      const StdForm& f = forms_[lps[w]];
+      sov_diagnostics& dg = l.dg;
+      dg.scaling_applied = f.scaling_applied;
+      dg.coefficient_min_abs_before = f.coef_min_before;
+      dg.coefficient_max_abs_before = f.coef_max_before;
+      dg.coefficient_min_abs_after = f.coef_min_after;
+      dg.coefficient_max_abs_after = f.coef_max_after;
+      dg.stall_iteration = -1;
+      dg.warm_start_used = l.warm_used ? 1 : 0;
+      if (l.warm_used) {
+        ws.push_back(k);
+        hx.insert(hx.end(), l.o.warm_x, l.o.warm_x + n);
+        hs.insert(hs.end(), l.o.warm_s, l.o.warm_s + n);
+        hy.insert(hy.end(), l.o.warm_y, l.o.warm_y + m);
+      }
+    }
+    if (!ws.empty()) {
+      const int nw = static_cast<int>(ws.size());
+      Buf<int> wslots;
+      wslots.put(ws, st_);
+      double* sx = stage.p;
+      double* ss = sx + static_cast<size_t>(nw) * n;
+      double* sy = ss + static_cast<size_t>(nw) * n;
+      SOV_CUDA(cudaMemcpyAsync(sx, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(ss, hs.data(), sizeof(double) * hs.size(), cudaMemcpyHostToDevice, st_));
+      SOV_CUDA(cudaMemcpyAsync(sy, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice, st_));
+      put_slots(x_.p, n, wslots.p, sx, nw);
+      put_slots(s_.p, n, wslots.p, ss, nw);
+      put_slots(y_.p, m, wslots.p, sy, nw);
+      SOV_CUDA(cudaStreamSynchronize(st_));  // wslots goes out of scope
+    }
+    put_norms();
+    put_mask();
+    copy(n, mask_.p, bx_.p, x_.p);
+    copy(n, mask_.p, bs_.p, s_.p);
+    copy(m, mask_.p, by_.p, y_.p);
+    k_fam_clear_fail<<<1, kFamilyWidth, 0, st_>>>(sc_.p, mask_.p, W);
+  };
+  for (;;) {
+    refill();
     bool any_active = false, any_cap = false;
     for (int k = 0; k < W; ++k) {
-      hcap[k] = L[k].active && L[k].o.ipm_iterate_at == it + 1;
+      const bool act = slot_lp[k] >= 0;
+      hcap[k] = act && L[k].o.ipm_iterate_at == it_of[k] + 1;
       any_cap |= hcap[k] != 0;
       if (hcap[k]) L[k].captured = true;
-      any_active |= L[k].active;
+      any_active |= act;
     }
     if (!any_active) break;
     if (any_cap) {
       hmask = hcap;
-      put_mask(mask_);
+      put_mask();
       copy(n, mask_.p, cx_.p, x_.p);
       copy(n, mask_.p, cs_.p, s_.p);
       copy(m, mask_.p, cy_.p, y_.p);
     }
     residuals();
     read_scalars();
-    bool any_step = false, any_best = false, any_restart = false;
+    bool any_step = false, any_best = false;
+    std::vector<int> done, restarts;
+    std::vector<char> from_best;
     for (int k = 0; k < W; ++k) {
       hstep[k] = hbest[k] = hrestart[k] = 0;
+      if (slot_lp[k] < 0) continue;
       LpState& l = L[k];
-      if (!l.active) continue;
+      const int it = it_of[k]++;  // Engine::run's iteration counter for this LP
       const FamScalars s = hsc_[k];
       sov_diagnostics& dg = l.dg;
       if (it >= l.o.max_iterations) {  // the loop of this LP has ended without convergence
@@ -1233,7 +1391,9 @@ void Family::solve_chunk(const std::vector<int>& lps) {
                       "lower-accuracy candidate. Relative duality gap = %g (tolerance %g), primal residual = %g, dual "
                       "residual = %g. Optimality is not proven.",
                       l.o.max_iterations, l.best_it, l.best_gap, l.o.optimality_tol, l.best_p, l.best_d);
-        finish_best(l, k, buf);
+        l.msg = buf;
+        done.push_back(k);
+        from_best.push_back(1);
         continue;
       }
       if (it > 0) {
@@ -1250,7 +1410,9 @@ void Family::solve_chunk(const std::vector<int>& lps) {
         }
       }
       if (s.fail || s.skipped) {
-        finish_best(l, k, fail_text);
+        l.msg = fail_text;
+        done.push_back(k);
+        from_best.push_back(1);
         continue;
       }
       if (s.metric < l.best_metric) {
@@ -1282,20 +1444,19 @@ void Family::solve_chunk(const std::vector<int>& lps) {
         dg.stall_mu = s.mu;
       }
       if (s.p_res < l.o.feasibility_tol && s.d_res < l.o.feasibility_tol && s.gap < l.o.optimality_tol) {
-        l.active = false;
         l.optimal = true;
         l.its = it + 1;
         l.gap = s.gap;
         l.p_res = s.p_res;
         l.d_res = s.d_res;
-        source[k] = kCurrent;
+        done.push_back(k);
+        from_best.push_back(0);
         continue;
       }
       if (l.warm_used && it + 1 == kWarmGiveUp) {  // the supplied start is abandoned once
         l.warm_used = false;
         dg.warm_start_used = 0;
-        hrestart[k] = 1;
-        any_restart = true;
+        restarts.push_back(k);
         l.best_metric = l.best_gap = l.best_p = l.best_d = INFINITY;
         l.best_it = 0;
         l.stale = 0;
@@ -1307,19 +1468,23 @@ void Family::solve_chunk(const std::vector<int>& lps) {
     }
     if (any_best) {
       hmask = hbest;
-      put_mask(mask_);
+      put_mask();
       copy(n, mask_.p, bx_.p, x_.p);
       copy(n, mask_.p, bs_.p, s_.p);
       copy(m, mask_.p, by_.p, y_.p);
     }
-    if (any_restart) {
-      hmask = hrestart;
-      put_mask(mask_);
-      copy(n, mask_.p, x_.p, x0_.p);
-      copy(n, mask_.p, s_.p, s0_.p);
-      copy(m, mask_.p, y_.p, y0_.p);
+    for (int k : restarts) {  // back to this LP's default start
+      const int w = slot_lp[k];
+      SOV_CUDA(cudaMemcpyAsync(slot_dev.p, &k, sizeof(int), cudaMemcpyHostToDevice, st_));
+      put_slots(x_.p, n, slot_dev.p, x0p.p + static_cast<size_t>(w) * n, 1);
+      put_slots(s_.p, n, slot_dev.p, s0p.p + static_cast<size_t>(w) * n, 1);
+      put_slots(y_.p, m, slot_dev.p, y0p.p + static_cast<size_t>(w) * m, 1);
+      std::fill(hmask.begin(), hmask.end(), 0);
+      hmask[k] = 1;
+      put_mask();
       k_fam_clear_fail<<<1, kFamilyWidth, 0, st_>>>(sc_.p, mask_.p, W);
     }
+    retire(done, from_best);
     if (!any_step) continue;
     SOV_CUDA(cudaMemcpyAsync(step_.p, hstep.data(), sizeof(int) * W, cudaMemcpyHostToDevice, st_));
     assemble(false);
@@ -1340,47 +1505,14 @@ void Family::solve_chunk(const std::vector<int>& lps) {
     for (int k = 0; k < W; ++k) L[k].factorizations += hstep[k];
   }
   SOV_CUDA(cudaStreamSynchronize(st_));
-  const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-  // ---- results ----
-  std::vector<double> hx(static_cast<size_t>(n) * W), hs(hx.size()), hy(static_cast<size_t>(m) * W);
-  std::vector<double> bxh(hx.size()), bsh(hx.size()), byh(hy.size()), cxh, csh, cyh;
-  auto get = [&](std::vector<double>& h, const Buf<double>& b) {
-    SOV_CUDA(cudaMemcpyAsync(h.data(), b.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st_));
-  };
-  get(hx, x_);
-  get(hs, s_);
-  get(hy, y_);
-  get(bxh, bx_);
-  get(bsh, bs_);
-  get(byh, by_);
-  bool any_captured = false;
-  for (auto& l : L) any_captured |= l.captured;
-  if (any_captured) {
-    cxh.resize(hx.size());
-    csh.resize(hx.size());
-    cyh.resize(hy.size());
-    get(cxh, cx_);
-    get(csh, cs_);
-    get(cyh, cy_);
-  }
-  SOV_CUDA(cudaStreamSynchronize(st_));
-  for (int k = 0; k < W; ++k) {
-    LpState& l = L[k];
-    if (source[k] == kBest) publish(l, bxh, byh, bsh, cxh, cyh, csh, k, W, seconds);
-    else publish(l, hx, hy, hs, cxh, cyh, csh, k, W, seconds);
-  }
 }
 
-// Engine::publish for an LP (publish_iterate, interior_point.cpp:541-563), from the chunk's
-// interleaved arrays
-void Family::publish(LpState& l, const std::vector<double>& x, const std::vector<double>& y,
-                     const std::vector<double>& s, const std::vector<double>& cx, const std::vector<double>& cy,
-                     const std::vector<double>& cs, int k, int W, double seconds) {
+void Family::publish(LpState& l, const double* x, const double* y, const double* s, const double* cx,
+                     const double* cy, const double* cs, double seconds) {
   const StdForm& f = forms_[l.idx];
   const sov_model& model = models_[l.idx];
   sov_result* r = &results_[l.idx];
   const int n = f.n, m = f.m;
-  auto at = [&](const std::vector<double>& v, int i) { return v[static_cast<size_t>(i) * W + k]; };
   r->n_ipm = n;
   r->m_ipm = m;
   if (l.optimal) {
@@ -1400,20 +1532,17 @@ void Family::publish(LpState& l, const std::vector<double>& x, const std::vector
   r->has_objective_value = 1;
   double obj = model.obj_constant;
   for (int j = 0; j < f.n_struct; ++j) {
-    const double v = f.shift[j] + f.col_scale[j] * at(x, j);
+    const double v = f.shift[j] + f.col_scale[j] * x[j];
     if (r->primal) r->primal[j] = v;
-    if (r->dual_col) r->dual_col[j] = at(s, j) / f.col_scale[j];
+    if (r->dual_col) r->dual_col[j] = s[j] / f.col_scale[j];
     obj += (model.obj ? model.obj[j] : 0.0) * v;
   }
   if (r->dual_row)
-    for (int i = 0; i < f.m0; ++i) r->dual_row[i] = f.row_scale[i] * at(y, i);
-  const bool cap = l.captured && !cx.empty();
-  for (int j = 0; j < n; ++j) {
-    if (r->ipm_x) r->ipm_x[j] = cap ? at(cx, j) : at(x, j);
-    if (r->ipm_s) r->ipm_s[j] = cap ? at(cs, j) : at(s, j);
-  }
-  if (r->ipm_y)
-    for (int i = 0; i < m; ++i) r->ipm_y[i] = cap ? at(cy, i) : at(y, i);
+    for (int i = 0; i < f.m0; ++i) r->dual_row[i] = f.row_scale[i] * y[i];
+  const bool cap = l.captured && cx;
+  if (r->ipm_x) std::copy(cap ? cx : x, (cap ? cx : x) + n, r->ipm_x);
+  if (r->ipm_s) std::copy(cap ? cs : s, (cap ? cs : s) + n, r->ipm_s);
+  if (r->ipm_y) std::copy(cap ? cy : y, (cap ? cy : y) + m, r->ipm_y);
   r->objective_value = obj;
   r->solve_seconds = seconds;
   std::snprintf(r->message, sizeof(r->message), "%s", l.msg.c_str());
@@ -1421,6 +1550,22 @@ void Family::publish(LpState& l, const std::vector<double>& x, const std::vector
     l.dg.refactorizations = l.factorizations;
     *r->diagnostics = l.dg;
   }
+}
+
+void Family::put_slots(double* dst, int len, const int* slots, const double* src, int count) {
+  const long long total = static_cast<long long>(count) * len;
+  if (total <= 0) return;
+  k_slot_put<<<static_cast<int>(std::max(1LL, std::min(8LL * sms_, (total + 255) / 256))), 256, 0, st_>>>(
+      dst, len, dev_.W, slots, src, count);
+  SOV_LAUNCH_CHECK();
+}
+
+void Family::get_slots(double* dst, int len, const int* slots, const double* src, int count) {
+  const long long total = static_cast<long long>(count) * len;
+  if (total <= 0) return;
+  k_slot_get<<<static_cast<int>(std::max(1LL, std::min(8LL * sms_, (total + 255) / 256))), 256, 0, st_>>>(
+      dst, len, dev_.W, slots, src, count);
+  SOV_LAUNCH_CHECK();
 }
 
 }  // namespace

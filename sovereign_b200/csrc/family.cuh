@@ -12,8 +12,9 @@
 // level by level in one cooperative launch for the chunk, each level's work W times wider than a
 // single LP's. Per-LP decisions (stopping test, best iterate, warm-start safeguard, iteration
 // limits) are the single engine's, taken on the host from one read of the chunk's scalars per
-// iteration; an LP that has finished is frozen (its iterate no longer updated) while the rest
-// of its chunk goes on.
+// iteration. An LP that has finished leaves its slot, which the next LP of the family takes with
+// its precomputed default start (or its kept supplied one), so the launch width stays full and a
+// family's time follows its LPs' mean iteration count rather than each chunk's slowest LP.
 #pragma once
 
 #include "sov_ipm.h"
