@@ -281,6 +281,7 @@ def run_single_workload(args):
         run_batched_warm_start(args)
         return
     # c4: learned warm start on the multicommodity family
+    from sovereign_b200.ipm import solve_family
     from sovereign_b200.warmstart import WarmStart, solve_many
     fam = P.MulticommodityFamily()
     train = [fam.instance_from_seed(100000 + k) for k in range(args.train)]
@@ -292,7 +293,8 @@ def run_single_workload(args):
     xs, ts, ws = [], [], None
     for c0 in range(0, len(train), 2048):
         chunk = train[c0:c0 + 2048]
-        res, _ = solve_many([m for m, _ in chunk], InteriorPointOptions(ipm_iterate_at=6), workers=args.workers)
+        # the family path: the instances share A (one symbolic analysis, 64 per launch)
+        res = solve_family([m for m, _ in chunk], InteriorPointOptions(ipm_iterate_at=6), with_ipm=True)
         if ws is None:
             ws = WarmStart(fam.param_dim, res[0].n_ipm, res[0].m_ipm, hidden=512, layers=3, seed=0)
         ok, t = ws.targets(res)
@@ -314,7 +316,6 @@ def run_single_workload(args):
               for k in ok) if ok else None
     # the family path: every eval instance shares A, so they are solved 64 per launch with one
     # symbolic analysis (sov_lp_solve_family), cold and from the same predicted starts
-    from sovereign_b200.ipm import solve_family
     test_models = [m for m, _ in test]
     solve_family(test_models[:64])  # module load, device pools
     t0 = time.perf_counter()
