@@ -256,10 +256,11 @@ inline SolverResult error_result(const std::string& what) {
   return r;
 }
 
-// One sov_lp_solve_batch call over `views` (model k of the caller is views[k]'s source); a failed
-// call marks every LP of it with the recorded error.
+// One sov_lp_solve_batch (or, with `family`, sov_lp_solve_family) call over `views` (model k of
+// the caller is views[k]'s source); a failed call marks every LP of it with the recorded error.
 inline std::vector<SolverResult> run_batch(const std::vector<const OptimizationModel*>& sources,
-                                           std::vector<sov_model>& views, const sov_options* opt) {
+                                           std::vector<sov_model>& views, const sov_options* opt,
+                                           bool family = false) {
   const int count = static_cast<int>(views.size());
   std::vector<BatchSlot> slots(count);
   std::vector<sov_result> res(count);
@@ -269,7 +270,10 @@ inline std::vector<SolverResult> run_batch(const std::vector<const OptimizationM
   }
   std::vector<SolverResult> out;
   out.reserve(count);
-  const int rc = count > 0 ? sov_lp_solve_batch(count, views.data(), opt, 0, res.data()) : SOV_OK;
+  int rc = SOV_OK;
+  if (count > 0)
+    rc = family ? sov_lp_solve_family(count, views.data(), opt, 0, res.data())
+                : sov_lp_solve_batch(count, views.data(), opt, 0, res.data());
   for (int k = 0; k < count; ++k) {
     if (rc != SOV_OK) {
       out.push_back(error_result(sov_last_error()));
@@ -280,13 +284,10 @@ inline std::vector<SolverResult> run_batch(const std::vector<const OptimizationM
   return out;
 }
 
-}  // namespace detail
-
-// N independent LPs in one batched GPU call. Results in input order; a model that cannot be
-// converted (unknown variable, ...) gets SolverStatus::Error with the reference's "IPM error: ..."
-// message and does not stop the others.
-inline std::vector<SolverResult> solve_lp_batch(const std::vector<OptimizationModel>& models,
-                                                const sov_options* opt = nullptr) {
+// Converts every model, solves those that converted in one batch or family call and puts each
+// result at its model's index.
+inline std::vector<SolverResult> solve_many(const std::vector<OptimizationModel>& models, const sov_options* opt,
+                                            bool family) {
   std::vector<SolverResult> out(models.size());
   std::vector<detail::IndexModel> ims;
   std::vector<std::size_t> at;
@@ -305,9 +306,30 @@ inline std::vector<SolverResult> solve_lp_batch(const std::vector<OptimizationMo
     views.push_back(ims[q].view);
     sources.push_back(&models[at[q]]);
   }
-  std::vector<SolverResult> solved = detail::run_batch(sources, views, opt);
+  std::vector<SolverResult> solved = detail::run_batch(sources, views, opt, family);
   for (std::size_t q = 0; q < at.size(); ++q) out[at[q]] = std::move(solved[q]);
   return out;
+}
+
+}  // namespace detail
+
+// N independent LPs in one batched GPU call. Results in input order; a model that cannot be
+// converted (unknown variable, ...) gets SolverStatus::Error with the reference's "IPM error: ..."
+// message and does not stop the others.
+inline std::vector<SolverResult> solve_lp_batch(const std::vector<OptimizationModel>& models,
+                                                const sov_options* opt = nullptr) {
+  return detail::solve_many(models, opt, false);
+}
+
+// The LPs of one parametric family -- the same variables, constraint matrix, variable bounds and
+// row senses; their own objectives and right-hand sides -- in one family call
+// (sov_lp_solve_family): the shared normal matrix is analysed once and 64 LPs advance together
+// per launch. Each result agrees with solve_lp's for that model within the stopping tolerance.
+// A model that cannot be converted gets SolverStatus::Error as in solve_lp_batch; when the
+// converted models do not share their structure, every result carries the library's error.
+inline std::vector<SolverResult> solve_lp_family(const std::vector<OptimizationModel>& models,
+                                                 const sov_options* opt = nullptr) {
+  return detail::solve_many(models, opt, true);
 }
 
 // The two children of branching on variable `var` at LP value `value`.

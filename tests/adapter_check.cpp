@@ -1,6 +1,6 @@
 // The reference-side adapter (include/sov_ipm_adapter.hpp) on a GPU, against the reference's own
 // solvers in the same process: sovereign::b200::solve_lp / solve_qp / solve_lp_batch /
-// solve_branch_children on name-keyed OptimizationModels, compared with InteriorPointSolver and
+// solve_lp_family / solve_branch_children on name-keyed OptimizationModels, compared with InteriorPointSolver and
 // QpInteriorPointSolver (solver/lp/src/interior_point.cpp:747-757,
 // solver/qp/src/qp_interior_point.cpp:3123-3186) on the same models: status, objective (1e-8
 // relative), the key sets and values of the name-keyed primal and dual maps ("row_<i>" for rows),
@@ -205,6 +205,8 @@ int main(int argc, char** argv) {
       const OptimizationModel m = k % 2 ? random_lp(40 + k, 90, 10 + k, false) : transport(5 + k, 6, 20 + k);
       if (ref_lp.solve(m).status != SolverStatus::Optimal) fail("reference node LP not optimal");
     }
+    for (int k = 0; k < 8; ++k)
+      if (ref_lp.solve(transport(12, 15, 40 + k)).status != SolverStatus::Optimal) fail("reference family LP not optimal");
     if (QpInteriorPointSolver(QpInteriorPointOptions{}).solve(portfolio(30, 4)).status != SolverStatus::Optimal)
       fail("reference QP not optimal");
     std::printf("failures %d\n", failures);
@@ -247,6 +249,19 @@ int main(int argc, char** argv) {
     const SolverResult want_bad = ref_lp.solve(bad);
     if (got.back().status != SolverStatus::Error || got.back().message != want_bad.message)
       fail("batch error model: " + got.back().message + " vs " + want_bad.message);
+  }
+  // one parametric family: transport LPs of one shape with their own costs and supplies, in one
+  // family call; then a set whose shapes differ, which the family call refuses for every LP
+  {
+    std::vector<OptimizationModel> fam;
+    for (int k = 0; k < 8; ++k) fam.push_back(transport(12, 15, 40 + k));
+    const auto got = b200::solve_lp_family(fam);
+    for (std::size_t k = 0; k < fam.size(); ++k)
+      compare("family member " + std::to_string(k), fam[k], got[k], ref_lp.solve(fam[k]), 1e-5);
+    const auto mixed = b200::solve_lp_family({transport(5, 6, 1), transport(6, 6, 2)});
+    for (const auto& r : mixed)
+      if (r.status != SolverStatus::Error || r.message.find("does not share") == std::string::npos)
+        fail("mixed family: " + r.message);
   }
   // strong-branching children of a relaxation at a fractional point
   {
