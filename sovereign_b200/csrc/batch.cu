@@ -71,6 +71,11 @@ struct BatchDev {
   const int* row_ptr;
   const int* col_idx;
   const double* rval;
+  // per IPM column j (at nv_off + j): its first two entries inline -- rows (r0, r1), the column's
+  // entry range [pb, pe) -- and their values (a0, a1), missing entries as row 0 with value 0; so
+  // a column pass reads a column with two independent 16-byte loads instead of col_ptr first
+  const int4* crec;
+  const double2* cval2;
   const double* b;
   const double* c;
   const double* warm;
@@ -110,13 +115,15 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
   double* vacc = vz + mmax;
   double* vdiag = vacc + mmax;
   double* vinv = vdiag + mmax;
+  int* srp = reinterpret_cast<int*>(vinv + mmax);  // the row pointers (m + 1), read by every row pass
 
-  const int* cp = bd.col_ptr + mt.cp_off;
   const int* ri = bd.row_idx + mt.a_off;
   const double* cv = bd.cval + mt.a_off;
   const int* rpp = bd.row_ptr + mt.rp_off;
   const int* ci = bd.col_idx + mt.a_off;
   const double* rv = bd.rval + mt.a_off;
+  const int4* crc = bd.crec + mt.nv_off;
+  const double2* cv2 = bd.cval2 + mt.nv_off;
   const double* b = bd.b + mt.mv_off;
   const double* c = bd.c + mt.nv_off;
   double* x = bd.x + mt.nv_off;
@@ -149,26 +156,41 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     }
   };
 
-  // Row pass, two rows per warp (both rows' gathers in flight), lanes over the row's entries:
+  // the same from a column record: a column of two entries adds its one term straight from the
+  // record (the product and the target of the loop above), longer columns take the loop
+  auto offdiag_rec = [&](const int4 rc, const double2 av, double dj) {
+    const int len = rc.w - rc.z;
+    if (len == 2) {
+      if (rc.y > rc.x) atomicAdd(M + tri(rc.y) + rc.x, (av.y * dj) * av.x);
+      else if (rc.x > rc.y) atomicAdd(M + tri(rc.x) + rc.y, (av.x * dj) * av.y);
+    } else if (len > 2) {
+      offdiag(rc.z, rc.w, dj);
+    }
+  };
+
+  // Row pass, RW rows per warp (all their gathers in flight), lanes over the row's entries:
   //  mode 0 (start):     z = b - A 1,                diag M_ii = sum a_ik^2 + 1e-12
   //  mode 1 (iteration): rp = b - A x, z = rp + A t,  diag M_ii = sum a_ik^2 d_k + 1e-12
-  //  mode 2 (corrector): z = rp + A t
+  //  mode 2 (corrector): z = rp + A t with t = tv - smu dv (tv = t0, dv = w of the predictor pass)
   // Returns this thread's share of max |rp_i| (mode 1).
-  auto row_pass = [&](const int mode, const double* dv, const double* tv) {
+  constexpr int RW = 3;
+  auto row_pass = [&](const int mode, const double* dv, const double* tv, double smu = 0.0) {
     double rpm = 0.0;
-    for (int i0 = warp; i0 < m; i0 += 2 * NW) {
-      const int rows[2] = {i0, i0 + NW};
-      int pb[2], pe[2];
+    for (int i0 = warp; i0 < m; i0 += RW * NW) {
+      int rows[RW], pb[RW], pe[RW];
+      double g0[RW], g1[RW], g2[RW];
+      int len = 0;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        pb[h] = rows[h] < m ? rpp[rows[h]] : 0;
-        pe[h] = rows[h] < m ? rpp[rows[h] + 1] : 0;
+      for (int h = 0; h < RW; ++h) {
+        rows[h] = i0 + h * NW;
+        pb[h] = rows[h] < m ? srp[rows[h]] : 0;
+        pe[h] = rows[h] < m ? srp[rows[h] + 1] : 0;
+        len = max(len, pe[h] - pb[h]);
+        g0[h] = g1[h] = g2[h] = 0.0;
       }
-      double g0[2] = {0.0, 0.0}, g1[2] = {0.0, 0.0}, g2[2] = {0.0, 0.0};
-      const int len = max(pe[0] - pb[0], pe[1] - pb[1]);
       for (int o = lane; o < len; o += 32) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < RW; ++h) {
           const int p = pb[h] + o;
           if (p < pe[h]) {
             const double a = rv[p];
@@ -180,14 +202,16 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
               if (mode == 1) {
                 g0[h] += a * x[k];
                 g1[h] += a * a * dv[k];
+                g2[h] += a * tv[k];
+              } else {
+                g2[h] += a * (tv[k] - smu * dv[k]);
               }
-              g2[h] += a * tv[k];
             }
           }
         }
       }
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < RW; ++h) {
         const double s0 = mode != 2 ? warp_sum(g0[h]) : 0.0;
         const double s1 = mode != 2 ? warp_sum(g1[h]) : 0.0;
         const double s2 = mode != 0 ? warp_sum(g2[h]) : 0.0;
@@ -379,27 +403,25 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     __syncthreads();
   };
 
-  // sum_p a_pj v[row_p] over column j, the first two entries loaded unconditionally-predicated so
-  // the loads of several columns can be in flight together
-  auto col_dot = [&](int pb, int pe, const double* v) {
-    const bool h0 = pb < pe, h1 = pb + 1 < pe;
-    const int r0 = h0 ? ri[pb] : 0, r1 = h1 ? ri[pb + 1] : 0;
-    const double a0 = h0 ? cv[pb] : 0.0, a1 = h1 ? cv[pb + 1] : 0.0;
-    double acc = a0 * v[r0] + a1 * v[r1];
-    for (int p = pb + 2; p < pe; ++p) acc += cv[p] * v[ri[p]];
+  // sum_p a_pj v[row_p] over column j from its record: the first two entries (missing ones as
+  // 0 * v[0]) need no load that waits on another, the rest of a longer column follows from col_ptr
+  auto col_dot = [&](const int4 rc, const double2 av, const double* v) {
+    double acc = av.x * v[rc.x] + av.y * v[rc.y];
+    for (int p = rc.z + 2; p < rc.w; ++p) acc += cv[p] * v[ri[p]];
     return acc;
   };
-  constexpr int U = 4;  // columns per thread per pass, loads issued before use
+  constexpr int U = 3;  // columns per thread per pass, loads issued before use
 
   // ---- Mehrotra-like start (interior_point.cpp:488-506) ----
-  // per-column scratch of an iteration: d = x/s in ds, t = d rd - rxs/s in dx (both free between
-  // the update of one iteration and the direction pass that overwrites them)
+  // per-column scratch of an iteration: d = x/s in ds and t = d rd - rxs/s in dx for the
+  // predictor's row pass, then w = 1/s in ds and t0 in dx for the corrector's (both free between
+  // the update of one iteration and the corrector's direction pass that overwrites them)
   double* dvec = ds;
   double* tvec = dx;
   auto mehrotra_start = [&]() {
     for (int i = tid; i < tri(m + 1); i += NT) M[i] = 0.0;
     __syncthreads();
-    for (int j = tid; j < n; j += NT) offdiag(cp[j], cp[j + 1], 1.0);
+    for (int j = tid; j < n; j += NT) offdiag_rec(crc[j], cv2[j], 1.0);
     __syncthreads();
     row_pass(0, nullptr, nullptr);
     __syncthreads();
@@ -410,7 +432,8 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       double xs = 1.0, ss = 1.0;
       if (start_ok) {
         double atdy = 0.0;
-        for (int p = cp[j]; p < cp[j + 1]; ++p) atdy += cv[p] * vz[ri[p]];
+        const int4 rc = crc[j];
+        for (int p = rc.z; p < rc.w; ++p) atdy += cv[p] * vz[ri[p]];
         xs = fmax(1.0, fabs(atdy));
         ss = fmax(1.0, fabs(c[j] - atdy));
       }
@@ -427,6 +450,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     fail = 0;
     __syncthreads();
   };
+  for (int i = tid; i <= m; i += NT) srp[i] = rpp[i];  // visible after mehrotra_start's first barrier
   mehrotra_start();
 
   const int ops_res[4] = {1, 1, 0, 0};
@@ -440,13 +464,13 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       double rpm = 0.0;
       for (int i = warp; i < m; i += NW) {
         double acc = 0.0;
-        for (int p = rpp[i] + lane; p < rpp[i + 1]; p += 32) acc += rv[p] * x[ci[p]];
+        for (int p = srp[i] + lane; p < srp[i + 1]; p += 32) acc += rv[p] * x[ci[p]];
         acc = warp_sum(acc);
         rpm = fmax(rpm, fabs(b[i] - acc));
       }
       double rdm = 0.0, xs = 0.0, cx = 0.0;
       for (int j = tid; j < n; j += NT) {
-        const double r = c[j] - (col_dot(cp[j], cp[j + 1], vy) + s[j]);
+        const double r = c[j] - (col_dot(crc[j], cv2[j], vy) + s[j]);
         rdm = fmax(rdm, fabs(r));
         xs += x[j] * s[j];
         cx += c[j] * x[j];
@@ -493,19 +517,20 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
     // passes (interior_point.cpp:572-582, :418-432, :74-101)
     double rdm = 0.0, xs = 0.0, cx = 0.0;
     for (int j0 = tid; j0 < n; j0 += U * NT) {
-      int pb[U], pe[U];
+      int4 rc[U];
+      double2 av[U];
       double xv[U], sv[U], cvv[U], aty[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int j = min(j0 + u * NT, n - 1);
-        pb[u] = cp[j];
-        pe[u] = cp[j + 1];
+        rc[u] = crc[j];
+        av[u] = cv2[j];
         xv[u] = x[j];
         sv[u] = s[j];
         cvv[u] = c[j];
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) aty[u] = col_dot(pb[u], pe[u], vy);
+      for (int u = 0; u < U; ++u) aty[u] = col_dot(rc[u], av[u], vy);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int j = j0 + u * NT;
@@ -520,7 +545,7 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
         const double rxs = -xv[u] * sv[u];
         dvec[j] = dj;
         tvec[j] = dj * r - rxs / sj;
-        offdiag(pb[u], pe[u], dj);
+        offdiag_rec(rc[u], av[u], dj);
       }
     }
     __syncthreads();
@@ -581,47 +606,32 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
       break;
     }
     // predictor and corrector
+    //  predictor: solve, then one column pass for the affine direction, its step-length ratios and
+    //    the four sums that give mu_aff = (1/n) sum (x + a_p dx)(s + a_d ds) once the steps are
+    //    known (sum xs + a_p sum dx s + a_d sum x ds + a_p a_d sum dx ds); the same pass leaves the
+    //    corrector's right-hand side as t0 = d rd + (x s + dx_aff ds_aff)/s and w = 1/s, so that
+    //    t = d rd - rxs/s with rxs = -x s - dx_aff ds_aff + sigma mu (interior_point.cpp:676-681)
+    //    is t0 - sigma mu w, formed inside the row pass z = rp + A t;
+    //  corrector: that row pass, solve, one column pass for the direction and the step lengths.
     for (int pass = 0; pass < 2; ++pass) {
       const double sigma_mu = pass ? cs.v[S_SIGMA] * mu : 0.0;
       if (pass == 1) {
-        // corrector right-hand side: t = d rd - rxs/s with rxs = -x s - dx_aff ds_aff + sigma mu
-        // (interior_point.cpp:676-681), then z = rp + A t; the predictor's was built with the residuals
-        for (int j0 = tid; j0 < n; j0 += U * NT) {
-          double xv[U], sv[U], rdv[U], av[U], bv[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int j = min(j0 + u * NT, n - 1);
-            xv[u] = x[j];
-            sv[u] = s[j];
-            rdv[u] = rd[j];
-            av[u] = dxa[j];
-            bv[u] = dsa[j];
-          }
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int j = j0 + u * NT;
-            if (j >= n) continue;
-            const double xj = fmax(xv[u], 1e-16), sj = fmax(sv[u], 1e-16);
-            const double rxs = -xv[u] * sv[u] - av[u] * bv[u] + sigma_mu;
-            tvec[j] = (xj / sj) * rdv[u] - rxs / sj;
-          }
-        }
-        __syncthreads();
-        row_pass(2, nullptr, tvec);
+        row_pass(2, dvec, tvec, sigma_mu);
         __syncthreads();
       }
       solve(pass == 0);
       double* ddx = pass ? dx : dxa;
       double* dds = pass ? ds : dsa;
-      double rpmin = 1.0, rdmin = 1.0;
+      double rpmin = 1.0, rdmin = 1.0, sxs = 0.0, sdxs = 0.0, sxds = 0.0, sdd = 0.0;
       for (int j0 = tid; j0 < n; j0 += U * NT) {
-        int pb[U], pe[U];
+        int4 rc[U];
+        double2 cav[U];
         double xv[U], sv[U], rdv[U], av[U], bv[U], atdy[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int j = min(j0 + u * NT, n - 1);
-          pb[u] = cp[j];
-          pe[u] = cp[j + 1];
+          rc[u] = crc[j];
+          cav[u] = cv2[j];
           xv[u] = x[j];
           sv[u] = s[j];
           rdv[u] = rd[j];
@@ -629,62 +639,53 @@ __device__ void solve_lp(const BatchDev& bd, const LpMeta& mt, int lp, double* s
           bv[u] = pass ? dsa[j] : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u) atdy[u] = col_dot(pb[u], pe[u], vz);
+        for (int u = 0; u < U; ++u) atdy[u] = col_dot(rc[u], cav[u], vz);
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int j = j0 + u * NT;
           if (j >= n) continue;
           const double xj = xv[u], sj = sv[u];
           const double rxs = pass ? -xj * sj - av[u] * bv[u] + sigma_mu : -xj * sj;
-          const double dj = fmax(xj, 1e-16) / fmax(sj, 1e-16);
-          const double dxj = dj * (atdy[u] - rdv[u]) + rxs / fmax(sj, 1e-16);
+          const double sg = fmax(sj, 1e-16);
+          const double dj = fmax(xj, 1e-16) / sg;
+          const double dxj = dj * (atdy[u] - rdv[u]) + rxs / sg;
           const double dsj = rdv[u] - atdy[u];
           ddx[j] = dxj;
           dds[j] = dsj;
           if (dxj < 0.0) rpmin = fmin(rpmin, -xj / dxj);
           if (dsj < 0.0) rdmin = fmin(rdmin, -sj / dsj);
+          if (pass == 0) {
+            sxs += xj * sj;
+            sdxs += dxj * sj;
+            sxds += xj * dsj;
+            sdd += dxj * dsj;
+            tvec[j] = dj * rdv[u] + (xj * sj + dxj * dsj) / sg;
+            dvec[j] = 1.0 / sg;
+          }
         }
       }
-      double u[4] = {rpmin, rdmin, 0.0, 0.0};
-      const int ops_min[4] = {2, 2, 0, 0};
-      cta_reduce4<NT>(u, ops_min, red);
-      if (tid == 0) {
-        if (pass == 0) {
-          cs.v[S_APAFF] = u[0];
-          cs.v[S_ADAFF] = u[1];
-        } else {
+      if (pass == 0) {
+        double u[6] = {rpmin, rdmin, sxs, sdxs, sxds, sdd};
+        const int ops[6] = {2, 2, 0, 0, 0, 0};
+        block_reduce<6>(u, ops, red);
+        if (tid == 0) {
+          const double apa = u[0], ada = u[1];
+          cs.v[S_APAFF] = apa;
+          cs.v[S_ADAFF] = ada;
+          const double mu_aff = fmax(0.0, u[2] + apa * u[3] + ada * u[4] + apa * ada * u[5]) / n;
+          const double r = mu_aff / mu;
+          cs.v[S_SIGMA] = mu > 0.0 ? fmin(1.0, r * r * r) : 0.0;
+        }
+      } else {
+        double u[4] = {rpmin, rdmin, 0.0, 0.0};
+        const int ops_min[4] = {2, 2, 0, 0};
+        cta_reduce4<NT>(u, ops_min, red);
+        if (tid == 0) {
           cs.v[S_AP] = fmin(1.0, mt.tau * u[0]);
           cs.v[S_AD] = fmin(1.0, mt.tau * u[1]);
         }
       }
       __syncthreads();
-      if (pass == 0) {
-        const double apa = cs.v[S_APAFF], ada = cs.v[S_ADAFF];
-        double acc = 0.0;
-        for (int j0 = tid; j0 < n; j0 += U * NT) {
-          double xv[U], sv[U], av[U], bv[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int j = min(j0 + u * NT, n - 1);
-            xv[u] = x[j];
-            sv[u] = s[j];
-            av[u] = dxa[j];
-            bv[u] = dsa[j];
-          }
-#pragma unroll
-          for (int u = 0; u < U; ++u)
-            if (j0 + u * NT < n) acc += (xv[u] + apa * av[u]) * (sv[u] + ada * bv[u]);
-        }
-        double w4[4] = {acc, 0.0, 0.0, 0.0};
-        const int ops_sum[4] = {0, 0, 0, 0};
-        cta_reduce4<NT>(w4, ops_sum, red);
-        if (tid == 0) {
-          const double mu_aff = w4[0] / n;
-          const double r = mu_aff / mu;
-          cs.v[S_SIGMA] = mu > 0.0 ? fmin(1.0, r * r * r) : 0.0;
-        }
-        __syncthreads();
-      }
     }
     // update (interior_point.cpp:709-718)
     const double ap = cs.v[S_AP], ad = cs.v[S_AD];
@@ -749,7 +750,7 @@ constexpr int kShapes[] = {128, 129, 256, 257, 512};
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_batch_ipm(BatchDev bd, int mmax) {
   extern __shared__ double sm[];
-  __shared__ double red[4 * 32];
+  __shared__ double red[6 * 32];
   __shared__ CtaScalars cs;
   __shared__ int slot_s;
   for (;;) {
@@ -763,7 +764,10 @@ __global__ void __launch_bounds__(NT, MINB) k_batch_ipm(BatchDev bd, int mmax) {
   }
 }
 
-size_t batch_smem(int mmax) { return sizeof(double) * (static_cast<size_t>(tri(mmax + 1)) + 6 * mmax); }
+// packed triangle (with the augmented row) | six m-vectors | m + 1 row pointers
+size_t batch_smem(int mmax) {
+  return sizeof(double) * (static_cast<size_t>(tri(mmax + 1)) + 6 * mmax) + sizeof(int) * (mmax + 2);
+}
 
 // The dynamic shared-memory limit of every instantiation is raised once to the largest bucket's
 // footprint, so launches (and launches captured in a graph) need no per-launch attribute call.
@@ -1131,6 +1135,8 @@ struct Batch {
   // one device arena for all packed inputs: [meta | ints | doubles | bucket orders]
   DBuf<unsigned char> in;
   DBuf<double> work;  // 9 n-vectors + 2 m-vectors
+  DBuf<int4> crec;     // column records (BatchDev::crec), built by k_batch_rows
+  DBuf<double2> cval2;
   DBuf<LpOut> out;
   DBuf<int> nexts;
   // published scale products of every LP (k_batch_publish), then per LP the coefficient range
@@ -1170,7 +1176,8 @@ struct Batch {
 
 namespace {
 
-// The row-wise copy (col_idx, rval) of every batched LP from its columns, one CTA per LP, on the
+// The row-wise copy (col_idx, rval) of every batched LP from its columns, and the column records
+// (BatchDev::crec, cval2), one CTA per LP, on the
 // device: the host sends the columns and the row starts only. Columns are taken in chunks of
 // 256 in ascending order; in a chunk, thread t (column c0 + t) sets bit t of each of its rows'
 // masks, and an entry's place in its row is the row's running count plus the bits below t, so
@@ -1180,7 +1187,8 @@ constexpr int kRowsThreads = 256;
 __global__ void __launch_bounds__(kRowsThreads) k_batch_rows(const LpMeta* __restrict__ meta, const int* __restrict__ cpa,
                                                              const int* __restrict__ ria, const double* __restrict__ cva,
                                                              const int* __restrict__ rpa, int* __restrict__ cia,
-                                                             double* __restrict__ rva) {
+                                                             double* __restrict__ rva, int4* __restrict__ crec,
+                                                             double2* __restrict__ cval2) {
   __shared__ unsigned mask[kBatchMaxRows][kRowsThreads / 32];
   __shared__ int base[kBatchMaxRows];
   const LpMeta mt = meta[blockIdx.x];
@@ -1198,6 +1206,11 @@ __global__ void __launch_bounds__(kRowsThreads) k_batch_rows(const LpMeta* __res
     __syncthreads();
     const int j = c0 + tid;
     const int pb = j < mt.n ? cp[j] : 0, pe = j < mt.n ? cp[j + 1] : 0;
+    if (j < mt.n) {
+      const bool h0 = pb < pe, h1 = pb + 1 < pe;
+      crec[mt.nv_off + j] = make_int4(h0 ? ri[pb] : 0, h1 ? ri[pb + 1] : 0, pb, pe);
+      cval2[mt.nv_off + j] = make_double2(h0 ? cv[pb] : 0.0, h1 ? cv[pb + 1] : 0.0);
+    }
     for (int p = pb; p < pe; ++p) atomicOr(&mask[ri[p]][w], 1u << lane);
     __syncthreads();
     for (int p = pb; p < pe; ++p) {
@@ -1565,6 +1578,8 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   if (starts) B->h2d_bytes -= static_cast<double>(sizeof(double) * wv);  // gathered on the device
   B->in.alloc(total);
   B->work.alloc(static_cast<size_t>(std::max(1LL, 9 * nv + 2 * mv)));
+  B->crec.alloc(static_cast<size_t>(std::max(1LL, nv)));
+  B->cval2.alloc(static_cast<size_t>(std::max(1LL, nv)));
   B->out.alloc(count);
   B->nexts.alloc(std::max<size_t>(1, B->buckets.size()));
   B->pout.alloc(static_cast<size_t>(pv + 2LL * count));
@@ -1675,7 +1690,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
         reinterpret_cast<const LpMeta*>(din + o_meta), reinterpret_cast<const int*>(din + o_cp),
         reinterpret_cast<const int*>(din + o_ri), reinterpret_cast<const double*>(din + o_cv),
         reinterpret_cast<const int*>(din + o_rp), reinterpret_cast<int*>(din + o_ci),
-        reinterpret_cast<double*>(din + o_rv));
+        reinterpret_cast<double*>(din + o_rv), B->crec.p, B->cval2.p);
     SOV_CUDA(cudaGetLastError());
     B->ready = pool.event(false);
     SOV_CUDA(cudaEventRecord(B->ready, cs));
@@ -1701,6 +1716,8 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   d.col_idx = reinterpret_cast<const int*>(base + o_ci);
   d.cval = reinterpret_cast<const double*>(base + o_cv);
   d.rval = reinterpret_cast<const double*>(base + o_rv);
+  d.crec = B->crec.p;
+  d.cval2 = B->cval2.p;
   d.b = reinterpret_cast<const double*>(base + o_b);
   d.c = reinterpret_cast<const double*>(base + o_c);
   d.warm = reinterpret_cast<const double*>(base + o_w);

@@ -45,8 +45,8 @@ __device__ __forceinline__ double warp_min(double v) {
   return v;
 }
 
-// Block-wide reduction of up to 4 values at once (sum / max / min chosen per slot by `ops`,
-// 0 = sum, 1 = max, 2 = min). `scratch` needs 4 * 32 doubles. Result valid in thread 0.
+// Block-wide reduction of NV values at once (sum / max / min chosen per slot by `ops`,
+// 0 = sum, 1 = max, 2 = min). `scratch` needs NV * 32 doubles. Result valid in thread 0.
 template <int NV>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], const int (&ops)[NV], double* scratch) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
