@@ -40,6 +40,30 @@ COUNT = 4096
 PLAIN_WORKERS = 16  # concurrent single-problem solves of the plain FP64 baseline
 
 
+def traffic_per_step(count: int, chosen: dict):
+    """DRAM bytes (read + write) of one step of the default batch workload, summed over its bucket
+    launches, from the ncu capture in profiles/traffic.json (taken with the bucket widths pinned to an
+    autotuned run's choice). Buckets that ran another width in this run may differ; if they carry less
+    than 1 % of the captured bytes the sum is kept with a note, otherwise the traffic is unknown."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            t = json.load(fh)["k_batch_ipm"]
+        per = t["dram_bytes_per_bucket"]
+        widths = t["threads_per_bucket"]
+    except (OSError, KeyError, ValueError):
+        return None, "no capture"
+    if count != t.get("lps", COUNT) or set(per) != set(chosen):
+        return None, "capture of another workload"
+    total = float(sum(per.values()))
+    other = [k for k in per if widths.get(k) != chosen.get(k)]
+    if sum(per[k] for k in other) > 0.01 * total:
+        return None, f"buckets {other} ran other widths than the capture"
+    note = "capture with this run's widths"
+    if other:
+        note += f"; {other} ran another width (under 1 % of the captured bytes)"
+    return total, note
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -478,6 +502,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sovereign_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain FP64 single-engine arm (profiler captures of the batched kernel)")
     ap.add_argument("--count", type=int, default=COUNT, help="LPs per step (profiling runs use fewer)")
     ap.add_argument("--workload", default="batch", choices=["batch", "c0", "c1", "c2", "c3w", "c4", "kkt", "wide"],
                     help="batch (default, headline): 4096 uneven transportation LPs; c0: one 50x50 transportation "
@@ -514,7 +540,8 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    if rank == 0:
+    plain = single = None
+    if rank == 0 and not args.no_plain:
         # the plain FP64 GPU IPM: the same LPs through the single-problem engine (sov_lp_solve, FP64),
         # PLAIN_WORKERS solves in flight at a time, each on its own CUDA stream, measured first
         # (after an untimed pass over a slice) so that it runs in a clean process state
@@ -561,23 +588,14 @@ def main():
     pk = peaks()
     achieved = alg_bytes / step_s / 1e9
     chosen = {k: v["chosen"] for k, v in tuning.items()}
-    traffic_ncu = None
-    try:  # DRAM bytes of one full-size step from an ncu capture, used only if its widths are this run's
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
-            t = json.load(fh)["k_batch_ipm"]
-        if count == COUNT and t.get("threads_per_bucket") == chosen:
-            traffic_ncu = dict(bytes_per_step=t["dram_bytes_per_step"], source="profiles/traffic.json",
-                               widths="same threads per bucket as this run")
-    except (OSError, KeyError, ValueError):
-        pass
+    traffic, traffic_note = traffic_per_step(count, chosen)
     roofline = dict(bound="hbm", achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
-                    frac=achieved / pk["hbm_gbs"], traffic=None,
+                    frac=achieved / pk["hbm_gbs"], traffic=traffic, traffic_note=traffic_note,
                     algorithmic_bytes_per_step=alg_bytes, kernel="k_batch_ipm", peak_source=pk["source"],
-                    traffic_ncu=traffic_ncu,
                     note="algorithmic bytes = sum over LPs of (iterations + 1) x [6 SpMV x (12 nnz + 8(m+n)) + "
-                         "15 x 8n + 10 x 8m] / device time per step. traffic is null: DRAM counters need an ncu "
-                         "capture, which a timed run cannot take; traffic_ncu holds a capture's figure when its "
-                         "widths match this run's",
+                         "15 x 8n + 10 x 8m] / device time per step. traffic = DRAM bytes of one step's bucket "
+                         "launches from an ncu capture run with this run's threads per bucket "
+                         "(profiles/traffic.json), null when a bucket that carries traffic ran another width",
                     binding=dict(limit="latency: shared-memory dependency chains of the per-LP L D L' and "
                                        "triangular solves, CTA barriers; the per-LP data stays in L2",
                                  fp64_tflops=alg_flops / step_s / 1e12,
@@ -629,11 +647,12 @@ def main():
                 optimal=f"{status_ok}/{count}", mean_iterations=float(iters.mean()))
     if rank == 0:
         line["clocks"] = clk.summary()
-        line["plain_fp64_gpu"] = plain
-        line["speedup_vs_plain_fp64"] = value / plain["value"]
-        err = max(abs(a.objective_value - b.objective_value) / max(1.0, abs(b.objective_value))
-                  for a, b in zip(res, single) if b.status_name == "OPTIMAL")
-        line["max_rel_obj_diff_batched_vs_plain"] = err
+        if plain is not None:
+            line["plain_fp64_gpu"] = plain
+            line["speedup_vs_plain_fp64"] = value / plain["value"]
+            err = max(abs(a.objective_value - b.objective_value) / max(1.0, abs(b.objective_value))
+                      for a, b in zip(res, single) if b.status_name == "OPTIMAL")
+            line["max_rel_obj_diff_batched_vs_plain"] = err
         if not args.no_cpu_baseline and world == 1:
             try:
                 cb = cpu_reference_sample(models)

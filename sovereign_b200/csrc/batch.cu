@@ -1372,6 +1372,24 @@ __global__ void __launch_bounds__(kScaleThreads) k_batch_publish(const LpMeta* _
   for (int k = threadIdx.x; k < mt.m0; k += kScaleThreads) P[2 * ns + k] = __dmul_rn(rs[k], y[k]);
 }
 
+// SOVEREIGN_BATCH_WIDTHS="128:256,96:128,..." pins the shape of each listed bucket (by its row
+// bound), so a profiler capture can run the widths an autotuned run chose; 0 when `mmax` is not
+// listed or the code is not a shape
+int pinned_threads(int mmax) {
+  const char* e = std::getenv("SOVEREIGN_BATCH_WIDTHS");
+  if (!e) return 0;
+  std::istringstream in(e);
+  std::string item;
+  while (std::getline(in, item, ',')) {
+    const size_t colon = item.find(':');
+    if (colon == std::string::npos || std::atoi(item.c_str()) != mmax) continue;
+    const int t = std::atoi(item.c_str() + colon + 1);
+    for (int code : kShapes)
+      if (t == code) return t;
+  }
+  return 0;
+}
+
 int threads_for(int mmax) {
   // SOVEREIGN_BATCH_THREADS=128|129|256|257|512 pins every bucket to a shape (tests run each one
   // this way; odd codes are the lean shapes)
@@ -1380,6 +1398,7 @@ int threads_for(int mmax) {
     for (int code : kShapes)
       if (t == code) return t;
   }
+  if (const int t = pinned_threads(mmax)) return t;
   std::lock_guard<std::mutex> g(g_tune_mu);
   auto it = g_tuned_threads.find(mmax);
   if (it != g_tuned_threads.end()) return it->second;
@@ -2056,8 +2075,15 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
   SOV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   std::vector<std::string> alone(B->buckets.size());
   std::vector<int> alone_t(B->buckets.size());
+  bool any_free = false;
   for (size_t k = 0; k < B->buckets.size(); ++k) {
     auto& bk = B->buckets[k];
+    if (pinned_threads(bk->mmax)) {  // threads_for gave the pinned shape: nothing to time
+      alone[k] = "\"pinned\": 1";
+      alone_t[k] = bk->threads;
+      continue;
+    }
+    any_free = true;
     float best_ms = 1e30f;
     int best_t = bk->threads;
     std::ostringstream part;
@@ -2108,8 +2134,9 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
     }
     return best;
   };
-  float cur = step_ms();
+  float cur = any_free ? step_ms() : 0.0f;
   for (auto& bk : B->buckets) {
+    if (pinned_threads(bk->mmax)) continue;
     const int first_t = bk->threads;
     for (int threads : kShapes) {
       if (threads == first_t) continue;
