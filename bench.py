@@ -596,8 +596,10 @@ def main():
                          "15 x 8n + 10 x 8m] / device time per step. traffic = DRAM bytes of one step's bucket "
                          "launches from an ncu capture run with this run's threads per bucket "
                          "(profiles/traffic.json), null when a bucket that carries traffic ran another width",
-                    binding=dict(limit="latency: shared-memory dependency chains of the per-LP L D L' and "
-                                       "triangular solves, CTA barriers; the per-LP data stays in L2",
+                    binding=dict(limit="latency: global-load chains of the row and column passes through L2 "
+                                       "(66-75 % sector hit rate) and CTA barriers behind the one-warp phases "
+                                       "(panel diagonal blocks, triangular solves); issue active 24-28 %, FP64 "
+                                       "pipe 9-11 % (ncu, profiles/k_batch_ipm_transport4096.md)",
                                  fp64_tflops=alg_flops / step_s / 1e12,
                                  fp64_flops_per_step=alg_flops,
                                  note="FP64 flops = sum over LPs of (iterations + 1) x [(2/3) m^3 + 8 m^2 + "
