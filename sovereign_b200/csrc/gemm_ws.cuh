@@ -84,37 +84,50 @@ __device__ __forceinline__ void stage_operand(const float* X, long long rs, long
   constexpr int kGroupsPerRow = C::kK / C::kGroup;  // 8
   constexpr int kPer = kTile * kGroupsPerRow / 128;  // groups per producer thread: 8
   const bool k_contig = ks == 1;
+  // The loads of a batch of groups are all issued before the first shared-memory store: the stores
+  // go through generic pointers the compiler cannot tell apart from X, so a load placed after a
+  // store would wait for it, and the chunk would cost one global round trip per group.
+  constexpr int kBatch = KIND == 1 ? 4 : 8;  // groups in flight: 32 floats either way
 #pragma unroll
-  for (int it = 0; it < kPer; ++it) {
-    const int g = it * 128 + p;
-    const int row = k_contig ? g / kGroupsPerRow : g % kTile;
-    const int kg = k_contig ? g % kGroupsPerRow : g / kTile;
-    const int gr = row0 + row;
-    float v[C::kGroup];
+  for (int b0 = 0; b0 < kPer; b0 += kBatch) {
+    float v[kBatch][C::kGroup];
 #pragma unroll
-    for (int e = 0; e < C::kGroup; ++e) {
-      const int gk = k0 + kg * C::kGroup + e;
-      v[e] = (gr < rows && gk < K) ? X[gr * rs + gk * ks] : 0.0f;
-    }
-    const uint32_t off = tc::kmajor_offset(row, kg * C::kGroup, C::kK, KIND == 1 ? 2 : 4);
-    if constexpr (KIND == 1) {
-      uint4 w;
-      __nv_bfloat162 b0 = __floats2bfloat162_rn(v[0], v[1]), b1 = __floats2bfloat162_rn(v[2], v[3]);
-      __nv_bfloat162 b2 = __floats2bfloat162_rn(v[4], v[5]), b3 = __floats2bfloat162_rn(v[6], v[7]);
-      w.x = *reinterpret_cast<uint32_t*>(&b0);
-      w.y = *reinterpret_cast<uint32_t*>(&b1);
-      w.z = *reinterpret_cast<uint32_t*>(&b2);
-      w.w = *reinterpret_cast<uint32_t*>(&b3);
-      *reinterpret_cast<uint4*>(hi + off) = w;
-    } else {
-      float h[4], l[4];
+    for (int ib = 0; ib < kBatch; ++ib) {
+      const int g = (b0 + ib) * 128 + p;
+      const int row = k_contig ? g / kGroupsPerRow : g % kTile;
+      const int kg = k_contig ? g % kGroupsPerRow : g / kTile;
+      const int gr = row0 + row;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        h[e] = to_tf32(v[e]);
-        l[e] = to_tf32(v[e] - h[e]);
+      for (int e = 0; e < C::kGroup; ++e) {
+        const int gk = k0 + kg * C::kGroup + e;
+        v[ib][e] = (gr < rows && gk < K) ? X[gr * rs + gk * ks] : 0.0f;
       }
-      *reinterpret_cast<float4*>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<float4*>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+    }
+#pragma unroll
+    for (int ib = 0; ib < kBatch; ++ib) {
+      const int g = (b0 + ib) * 128 + p;
+      const int row = k_contig ? g / kGroupsPerRow : g % kTile;
+      const int kg = k_contig ? g % kGroupsPerRow : g / kTile;
+      const uint32_t off = tc::kmajor_offset(row, kg * C::kGroup, C::kK, KIND == 1 ? 2 : 4);
+      if constexpr (KIND == 1) {
+        uint4 w;
+        __nv_bfloat162 q0 = __floats2bfloat162_rn(v[ib][0], v[ib][1]), q1 = __floats2bfloat162_rn(v[ib][2], v[ib][3]);
+        __nv_bfloat162 q2 = __floats2bfloat162_rn(v[ib][4], v[ib][5]), q3 = __floats2bfloat162_rn(v[ib][6], v[ib][7]);
+        w.x = *reinterpret_cast<uint32_t*>(&q0);
+        w.y = *reinterpret_cast<uint32_t*>(&q1);
+        w.z = *reinterpret_cast<uint32_t*>(&q2);
+        w.w = *reinterpret_cast<uint32_t*>(&q3);
+        *reinterpret_cast<uint4*>(hi + off) = w;
+      } else {
+        float h[4], l[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          h[e] = to_tf32(v[ib][e]);
+          l[e] = to_tf32(v[ib][e] - h[e]);
+        }
+        *reinterpret_cast<float4*>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+      }
     }
   }
 }
@@ -225,16 +238,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_ws(WsGemmArgs g) {
         float v[32];
         tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + cc * 32, v);
         if (r < g.M) {
+          // the 32 old values of C are read before the first store (a read after a store to
+          // a possibly aliasing address would wait for it: one round trip per column)
+          float old[32];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            const int n = n0 + cc * 32 + c;
+            old[c] = (g.beta != 0.0f && n < g.N) ? g.C[r * g.c_rs + n * g.c_cs] : 0.0f;
+          }
 #pragma unroll
           for (int c = 0; c < 32; ++c) {
             const int n = n0 + cc * 32 + c;
             if (n >= g.N) continue;
-            float* dst = g.C + r * g.c_rs + n * g.c_cs;
             float out = g.alpha * (nk > 0 ? v[c] : 0.0f);
-            if (g.beta != 0.0f) out += g.beta * *dst;
+            if (g.beta != 0.0f) out += g.beta * old[c];
             if (g.bias) out += g.bias[n];
             if (g.relu) out = fmaxf(out, 0.0f);
-            *dst = out;
+            g.C[r * g.c_rs + n * g.c_cs] = out;
           }
         }
       }
