@@ -73,33 +73,88 @@ def peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock, its maximum and the throttle reasons sampled during the timed region: NVML polled
+    every 10 ms from a thread (read-only queries), or nvidia-smi every 200 ms where NVML cannot be
+    loaded (then the region starts only once its first sample has arrived)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
-        self.rows: list[list[str]] = []
+        self.rows: list[tuple[float, float, list[str]]] = []  # (sm MHz, max sm MHz, active reasons)
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:  # the CUDA device's own GPU (CUDA_VISIBLE_DEVICES may renumber), by its PCI address
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            N, h = self._nvml_handle()
+            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
+            mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+
+            def sample():
+                sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((sm, mx, [nm for nm, b in zip(self.NAMES, bits) if r & b]))
+
+            sample()
+            self.nvml = N
+
+            def loop():
+                while not self.stop.wait(0.01):
+                    try:
+                        sample()
+                    except Exception:
+                        return
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
+            self.rows = []
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([v.strip() for v in line.split(",")])
+            r = [v.strip() for v in line.split(",")]
+            if len(r) > 8 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                self.rows.append((float(r[1]), float(r[2]),
+                                  [self.NAMES[k] for k in range(4) if r[5 + k] == "Active"]))
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=1.0)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -110,12 +165,9 @@ class ClockSampler:
     def summary(self) -> dict:
         if not self.rows:
             return dict(sm_mhz=None, sm_max_mhz=None, reasons=["unsampled"], samples=0)
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows if len(r) > 8 for k in range(4) if r[5 + k] == "Active"})
-        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
-                    reasons=reasons, samples=len(self.rows))
+        reasons = sorted({nm for _, _, rs in self.rows for nm in rs})
+        return dict(sm_mhz=statistics.median(r[0] for r in self.rows), sm_max_mhz=max(r[1] for r in self.rows),
+                    reasons=reasons, samples=len(self.rows), source="nvml" if self.nvml is not None else "nvidia-smi")
 
 
 def dist_setup(n_gpus: int):

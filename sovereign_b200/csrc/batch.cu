@@ -929,13 +929,73 @@ struct HBuf {
   }
 };
 
-// Grow-only pinned host staging shared by all batches of the process (H2D of the packed inputs,
-// D2H of the iterates), so repeated end-to-end calls do not re-pin memory.
+// Pinned host blocks for per-batch results (the statuses and published values of every LP, copied
+// behind the publish kernel on the solve's stream): released blocks stay pinned and are reused, so
+// a call pins no memory after the first few.
+class PinnedPool {
+ public:
+  void* acquire(size_t bytes, size_t* got) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      auto it = free_.lower_bound(bytes);
+      if (it != free_.end() && it->first <= 2 * bytes + (1u << 20)) {
+        void* p = it->second;
+        *got = it->first;
+        cached_ -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    void* p = nullptr;
+    SOV_CUDA(cudaMallocHost(&p, bytes));
+    *got = bytes;
+    return p;
+  }
+  void release(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    free_.emplace(bytes, p);
+    cached_ += bytes;
+    while (cached_ > kMaxCached && !free_.empty()) {
+      auto it = std::prev(free_.end());
+      cudaFreeHost(it->second);
+      cached_ -= it->first;
+      free_.erase(it);
+    }
+  }
+
+ private:
+  static constexpr size_t kMaxCached = size_t(1) << 30;
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  size_t cached_ = 0;
+};
+PinnedPool g_ppool;
+
+template <class T>
+struct PBuf {
+  T* p = nullptr;
+  size_t cap_bytes = 0;
+  void alloc(size_t count) {
+    if (count && !p) p = static_cast<T*>(g_ppool.acquire(sizeof(T) * count, &cap_bytes));
+  }
+  ~PBuf() {
+    if (p) g_ppool.release(p, cap_bytes);
+  }
+};
+
+// Grow-only pinned host stagings shared by all batches of the process (H2D of the packed inputs,
+// D2H of the iterates), so repeated end-to-end calls do not re-pin memory. Two of them, taken in
+// turn: a batch leaves its input copies in flight (`pending`) and the next batch builds into the
+// other staging, so the building of one part of a pipelined call overlaps the copies of the one
+// before. Whoever takes a staging next waits for its pending copies first.
 struct PinnedArena {
   std::mutex mu;
   unsigned char* p = nullptr;
   size_t cap = 0;
+  cudaEvent_t pending = nullptr;  // recorded behind the last async copies out of `p`
+  int pending_dev = -1;
   unsigned char* get(size_t bytes) {
+    if (pending) SOV_CUDA(cudaEventSynchronize(pending));
     if (bytes > cap) {
       if (p) cudaFreeHost(p);
       p = nullptr;
@@ -945,8 +1005,23 @@ struct PinnedArena {
     }
     return p;
   }
+  // mark the copies enqueued on `st` so far as readers of the staging
+  void record(cudaStream_t st) {
+    int dev = 0;
+    SOV_CUDA(cudaGetDevice(&dev));
+    if (pending && pending_dev != dev) {
+      cudaEventDestroy(pending);
+      pending = nullptr;
+    }
+    if (!pending) {
+      SOV_CUDA(cudaEventCreateWithFlags(&pending, cudaEventDisableTiming));
+      pending_dev = dev;
+    }
+    SOV_CUDA(cudaEventRecord(pending, st));
+  }
 };
-PinnedArena g_arena;
+PinnedArena g_arenas[2];
+std::atomic<unsigned> g_arena_turn{0};
 
 std::mutex g_tune_mu;
 std::map<int, int> g_tuned_threads;  // bucket mmax -> kernel shape code
@@ -1142,6 +1217,10 @@ struct Batch {
   // published scale products of every LP (k_batch_publish), then per LP the coefficient range
   // after scaling (k_batch_scale)
   DBuf<double> pout;
+  // host copies of `out` and `pout`, made on the solve's stream behind k_batch_publish (the
+  // `published` event covers them), so reading results waits for no copy of its own
+  PBuf<LpOut> h_out;
+  PBuf<double> h_pout;
   double* scl = nullptr;  // device: column scales (total_n) | row scales (total_m), inside `in`
   long long total_n = 0, total_m = 0, total_nnz = 0, total_cols = 0, total_rows = 0, total_pub = 0;
   BatchDev dev{};
@@ -1161,6 +1240,8 @@ struct Batch {
     if (graph) cudaGraphExecDestroy(graph);
     // the input kernels write the device buffers released below (a batch destroyed unsolved)
     if (ready) cudaEventSynchronize(ready);
+    // the result copies into h_out / h_pout (released below) follow the publish kernel
+    if (published) cudaEventSynchronize(published);
     if (cap) cudaStreamDestroy(cap);
     CudaObjectPool& pool = CudaObjectPool::get();
     for (auto st : streams) pool.give_stream(st, false);
@@ -1605,15 +1686,15 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   // 3. every LP's standard form written into its slots of the pinned staging, chunk by chunk in
   //    LP order; each finished chunk's slots are copied to the device (async) while the next
   //    chunk is built
-  std::lock_guard<std::mutex> lock(g_arena.mu);
-  unsigned char* h = g_arena.get(total);
+  PinnedArena& arena = g_arenas[g_arena_turn.fetch_add(1) % 2];
+  std::lock_guard<std::mutex> lock(arena.mu);
+  unsigned char* h = arena.get(total);
   double* pubd = B->pubdata.p;
   // the copies and the input kernels on a high-priority stream: while an earlier batch's persistent
   // kernels hold the SMs, this batch's short kernels take the first slots that free up
   CudaObjectPool& pool = CudaObjectPool::get();
   cudaStream_t cs = pool.stream(true);
   B->input_stream = cs;
-  cudaEvent_t copied = nullptr;
   auto copy_range = [&](size_t off, size_t bytes) {
     if (bytes) SOV_CUDA(cudaMemcpyAsync(B->in.p + off, h + off, bytes, cudaMemcpyHostToDevice, cs));
   };
@@ -1681,7 +1762,6 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     if (!all_orders.empty()) std::memcpy(h + o_ord, all_orders.data(), sizeof(int) * all_orders.size());
     copy_range(o_meta, sizeof(LpMeta) * count);
     copy_range(o_ord, sizeof(int) * all_orders.size());
-    copied = pool.event(false);
     if (from_form > 0)  // the scales of the LPs the host scaled
       for (int i = 0; i < count; ++i) {
         const LpMeta& mt = B->meta[i];
@@ -1690,7 +1770,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
         copy_range(o_scl + sizeof(double) * (nv + mt.mv_off), sizeof(double) * mt.m);
         B->h2d_bytes += sizeof(double) * (mt.n + mt.m);
       }
-    SOV_CUDA(cudaEventRecord(copied, cs));
+    arena.record(cs);  // the next user of this staging waits for these copies
     // the scaling, then the row-wise copies built on the device from the (scaled) columns
     unsigned char* din = B->in.p;
     B->scl = reinterpret_cast<double*>(din + o_scl);
@@ -1713,15 +1793,11 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     SOV_CUDA(cudaGetLastError());
     B->ready = pool.event(false);
     SOV_CUDA(cudaEventRecord(B->ready, cs));
-    // the staging is reused by the next batch: wait for the copies (the kernels run on; every
-    // launch of this batch waits for `ready`)
-    SOV_CUDA(cudaEventSynchronize(copied));
+    // the copies and the input kernels run on; every launch of this batch waits for `ready`
   } catch (...) {
     cudaStreamSynchronize(cs);  // `cs` goes back to the pool with the batch
-    pool.give_event(copied, false);
     throw;
   }
-  pool.give_event(copied, false);  // the input kernels still run on `cs`
   for (size_t k = 0; k < B->buckets.size(); ++k) {
     B->buckets[k]->order = reinterpret_cast<const int*>(B->in.p + o_ord) + order_at[k];
     B->buckets[k]->next = B->nexts.p + k;
@@ -1795,6 +1871,11 @@ void enqueue_publish(Batch* B, cudaStream_t st) {
   const BatchDev& d = B->dev;
   k_batch_publish<<<B->count, kScaleThreads, 0, st>>>(d.meta, d.out, d, B->scl, B->total_n, B->pout.p);
   SOV_CUDA(cudaGetLastError());
+  const size_t pn = static_cast<size_t>(B->total_pub + 2LL * B->count);
+  B->h_out.alloc(B->count);
+  B->h_pout.alloc(pn);
+  SOV_CUDA(cudaMemcpyAsync(B->h_out.p, B->out.p, sizeof(LpOut) * B->count, cudaMemcpyDeviceToHost, st));
+  SOV_CUDA(cudaMemcpyAsync(B->h_pout.p, B->pout.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, st));
   SOV_CUDA(cudaEventRecord(B->published, st));
   B->publish_queued = true;
 }
@@ -1866,19 +1947,21 @@ void batch_results(Batch* B, sov_result* results) {
     }
     pool.give_stream(ps, true);
   }
-  SOV_CUDA(cudaEventSynchronize(B->published));
+  SOV_CUDA(cudaEventSynchronize(B->published));  // the publish kernel and the copies of out / pout behind it
   B->publish_queued = false;
-  std::vector<LpOut> out(B->count);
-  SOV_CUDA(cudaMemcpy(out.data(), B->out.p, sizeof(LpOut) * B->count, cudaMemcpyDeviceToHost));
+  const LpOut* out = B->h_out.p;
+  const double* hp = B->h_pout.p;
   bool want_ipm = false;
   for (int i = 0; i < B->count && !want_ipm; ++i)
     want_ipm = B->meta[i].m >= 0 && (results[i].ipm_x || results[i].ipm_s || results[i].ipm_y);
   const size_t pbytes = sizeof(double) * (pv + 2LL * B->count);
   const size_t bytes = want_ipm ? sizeof(double) * (2 * nv + mv) : 0;
-  std::lock_guard<std::mutex> lock(g_arena.mu);
-  double* hp = reinterpret_cast<double*>(g_arena.get(std::max<size_t>(pbytes + bytes, 8)));
-  double* h = hp + pv + 2LL * B->count;
-  SOV_CUDA(cudaMemcpy(hp, B->pout.p, pbytes, cudaMemcpyDeviceToHost));
+  std::unique_lock<std::mutex> lock(g_arenas[0].mu, std::defer_lock);  // the iterates, when asked for
+  double* h = nullptr;
+  if (want_ipm) {
+    lock.lock();
+    h = reinterpret_cast<double*>(g_arenas[0].get(std::max<size_t>(bytes, 8)));
+  }
   const double* crange = hp + pv;
   if (want_ipm && nv) SOV_CUDA(cudaMemcpy(h, d.x, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost));  // x, s adjacent
   if (want_ipm && mv) SOV_CUDA(cudaMemcpy(h + 2 * nv, d.y, sizeof(double) * mv, cudaMemcpyDeviceToHost));
@@ -2036,12 +2119,29 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
   // 12 32.4
   int parts = count >= 3072 ? 6 : count >= 2048 ? 4 : 1;
   if (const char* e = std::getenv("SOVEREIGN_BATCH_PARTS")) parts = std::max(1, std::min(count, std::atoi(e)));
+  // Part sizes: equal, or (SOVEREIGN_BATCH_TAPER=1) falling linearly, part k weighted parts - k,
+  // so that the last parts, whose solves nothing overlaps, are the short ones.
+  bool taper = false;
+  if (const char* e = std::getenv("SOVEREIGN_BATCH_TAPER")) taper = std::atoi(e) != 0;
+  std::vector<int> lo_of(parts + 1);
+  {
+    const long long wsum = taper ? static_cast<long long>(parts) * (parts + 1) / 2 : parts;
+    long long acc = 0;
+    for (int k = 0; k <= parts; ++k) {
+      lo_of[k] = static_cast<int>(static_cast<long long>(count) * acc / wsum);
+      if (k < parts) acc += taper ? parts - k : 1;
+    }
+  }
   std::vector<std::unique_ptr<Batch>> batches;
   std::vector<cudaStream_t> streams;
-  auto part_lo = [&](int k) { return static_cast<int>(static_cast<long long>(count) * k / parts); };
+  auto part_lo = [&](int k) { return lo_of[k]; };
   try {
     for (int k = 0; k < parts; ++k) {
       const int lo = part_lo(k), hi = part_lo(k + 1);
+      if (hi == lo) {  // a tapered schedule over few LPs can leave a part empty
+        batches.emplace_back(nullptr);
+        continue;
+      }
       const sov_options* o = (opt && opt_stride > 0)
                                  ? reinterpret_cast<const sov_options*>(reinterpret_cast<const char*>(opt) +
                                                                         static_cast<size_t>(lo) * opt_stride)
@@ -2052,6 +2152,7 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
       batch_launch(batches.back().get(), st, true);
     }
     for (int k = 0; k < parts; ++k) {
+      if (!batches[k]) continue;
       batch_finish(batches[k].get());
       batch_results(batches[k].get(), results + part_lo(k));
     }

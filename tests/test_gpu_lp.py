@@ -208,7 +208,16 @@ def test_batch_device_scaling_matches_host_builder():
             # duals can shift by opposite constants): compare A' y
             A = mdl.dense_A()
             np.testing.assert_allclose(A.T @ r.dual_row, A.T @ s.dual_row, rtol=1e-5, atol=1e-5)
-            np.testing.assert_array_equal(ri.primal, r.primal)
+            # the with-iterates solve publishes the same values: bit for bit where every normal-matrix
+            # entry gets one term (no two rows share more than one column); otherwise an entry sums
+            # several terms by shared-memory atomics in arrival order, and two solves agree to rounding
+            nz = (A != 0).astype(int)
+            shared = nz @ nz.T
+            np.fill_diagonal(shared, 0)
+            if shared.max() > 1:
+                np.testing.assert_allclose(ri.primal, r.primal, rtol=1e-9, atol=1e-12)
+            else:
+                np.testing.assert_array_equal(ri.primal, r.primal)
             assert np.all(np.isfinite(ri.ipm_x)) and np.any(ri.ipm_x != 0.0)
 
 
