@@ -704,7 +704,8 @@ def main():
                             lps_per_gpu=count, precision="fp64 batched",
                             l2="per-step working set ~0.6 GB > 126 MB L2 (no flush needed)",
                             parallelism=f"independent LPs sharded per rank (dp{world})",
-                            threads_per_bucket={k: v["chosen"] for k, v in tuning.items()}),
+                            threads_per_bucket={k: v["chosen"] for k, v in tuning.items()},
+                            grid_per_bucket={k: v.get("grid") for k, v in tuning.items()}),
                 gpu_launches=int(stats["launches"] * args.steps), roofline=roofline, e2e=e2e,
                 optimal=f"{status_ok}/{count}", mean_iterations=float(iters.mean()))
     if rank == 0:

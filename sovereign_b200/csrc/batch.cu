@@ -1025,6 +1025,7 @@ std::atomic<unsigned> g_arena_turn{0};
 
 std::mutex g_tune_mu;
 std::map<int, int> g_tuned_threads;  // bucket mmax -> kernel shape code
+std::map<int, int> g_tuned_per_sm;   // bucket mmax -> resident CTAs per SM it launches (absent: all that fit)
 
 int bucket_of(int m) { return std::max(32, ((m + 31) / 32) * 32); }
 
@@ -1497,7 +1498,23 @@ void launch_any(const BatchDev& bd, int mmax, int code, int grid, cudaStream_t s
   }
 }
 
-int grid_for(int mmax, int code, int count) {
+// The grid of a bucket launch: every CTA that fits at once, or at most per_sm of them per SM
+// (fewer resident LPs keep a bucket's per-LP vectors inside L2; the autotuner decides).
+int tuned_per_sm(int mmax) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tuned_per_sm.find(mmax);
+  return it != g_tuned_per_sm.end() ? it->second : 0;
+}
+
+int sm_count() {
+  int dev = 0, sms = 0;
+  SOV_CUDA(cudaGetDevice(&dev));
+  SOV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return sms;
+}
+
+int grid_for(int mmax, int code, int count, int per_sm = -1) {
+  if (per_sm < 0) per_sm = tuned_per_sm(mmax);
   int cap;
   switch (code) {
     case 128: cap = max_ctas<128, false>(mmax); break;
@@ -1506,6 +1523,7 @@ int grid_for(int mmax, int code, int count) {
     case 512: cap = max_ctas<512, false>(mmax); break;
     default: cap = max_ctas<256, false>(mmax); break;
   }
+  if (per_sm > 0) cap = std::min(cap, per_sm * sm_count());
   return std::max(1, std::min(cap, count));
 }
 
@@ -2190,7 +2208,7 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
     std::ostringstream part;
     bool f2 = true;
     for (int threads : kShapes) {
-      const int grid = grid_for(bk->mmax, threads, bk->count);
+      const int grid = grid_for(bk->mmax, threads, bk->count, 0);
       BatchDev d = B->dev;
       d.order = bk->order;
       d.count = bk->count;
@@ -2221,7 +2239,7 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
     alone[k] = part.str();
     alone_t[k] = best_t;
     bk->threads = best_t;
-    bk->grid = grid_for(bk->mmax, best_t, bk->count);
+    bk->grid = grid_for(bk->mmax, best_t, bk->count, 0);
   }
   // Then the buckets together, as a solve runs them (concurrently, on forked streams): one pass
   // over the buckets trying each other width with the rest fixed, timing the whole step (best of
@@ -2243,7 +2261,7 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
       if (threads == first_t) continue;
       const int old_t = bk->threads, old_g = bk->grid;
       bk->threads = threads;
-      bk->grid = grid_for(bk->mmax, threads, bk->count);
+      bk->grid = grid_for(bk->mmax, threads, bk->count, 0);
       const float ms = step_ms();
       if (ms < 0.99f * cur) {
         cur = ms;
@@ -2251,6 +2269,25 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
         bk->threads = old_t;
         bk->grid = old_g;
       }
+    }
+  }
+  // Then, per bucket with its width fixed, one resident CTA per SM fewer than fit (a smaller
+  // working set of per-LP vectors for L2, the SMs' other slots left to the other buckets), kept
+  // only if the whole step gets at least 1 % faster.
+  std::vector<int> per_sm_kept(B->buckets.size(), 0);
+  const int sms = sm_count();
+  for (size_t k = 0; k < B->buckets.size(); ++k) {
+    auto& bk = B->buckets[k];
+    const int full = grid_for(bk->mmax, bk->threads, 1 << 30, 0) / sms;  // CTAs per SM that fit
+    if (full < 2 || bk->count <= (full - 1) * sms) continue;             // nothing to trim
+    const int old_g = bk->grid;
+    bk->grid = grid_for(bk->mmax, bk->threads, bk->count, full - 1);
+    const float ms = step_ms();
+    if (ms < 0.99f * cur) {
+      cur = ms;
+      per_sm_kept[k] = full - 1;
+    } else {
+      bk->grid = old_g;
     }
   }
   SOV_CUDA(cudaStreamSynchronize(st));
@@ -2264,8 +2301,11 @@ std::string autotune(int count, const sov_model* models, const sov_options* opt,
     for (size_t k = 0; k < B->buckets.size(); ++k) {
       const auto& bk = B->buckets[k];
       g_tuned_threads[bk->mmax] = bk->threads;
+      if (per_sm_kept[k] > 0) g_tuned_per_sm[bk->mmax] = per_sm_kept[k];
+      else g_tuned_per_sm.erase(bk->mmax);
       rep << (k ? ", " : "") << "\"m<=" << bk->mmax << "\": {" << alone[k] << ", \"alone\": " << alone_t[k]
-          << ", \"chosen\": " << bk->threads << ", \"count\": " << bk->count << "}";
+          << ", \"chosen\": " << bk->threads << ", \"per_sm\": " << per_sm_kept[k] << ", \"count\": " << bk->count
+          << ", \"grid\": " << bk->grid << "}";
     }
   }
   rep << "}";
