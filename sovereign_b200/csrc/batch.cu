@@ -1716,7 +1716,10 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
   auto copy_range = [&](size_t off, size_t bytes) {
     if (bytes) SOV_CUDA(cudaMemcpyAsync(B->in.p + off, h + off, bytes, cudaMemcpyHostToDevice, cs));
   };
-  const int chunks = count >= 512 ? 8 : 1;
+  // chunks of the staging whose copies overlap the building of the next one (each chunk is one
+  // parallel_for over the worker pool; SOVEREIGN_BATCH_CHUNKS overrides)
+  int chunks = count >= 512 ? 8 : 1;
+  if (const char* e = std::getenv("SOVEREIGN_BATCH_CHUNKS")) chunks = std::max(1, std::min(count, std::atoi(e)));
   try {
     for (int ch = 0; ch < chunks; ++ch) {
       const int lo = static_cast<int>(static_cast<long long>(count) * ch / chunks);
@@ -2133,9 +2136,9 @@ int solve_batch(int count, const sov_model* models, const sov_options* opt, int 
   // the device, so the host standard form and the copies of the next part overlap the solves of the
   // ones before; the results are read back in order once all parts are launched. A part's LPs are
   // solved exactly as in one batch (per-LP work, bucket widths by m).
-  // 4096 LPs per call (median of 6 calls): 1 part 29.5 ms, 2 25.9, 3 24.2, 4 24.4, 6 23.7, 8 24.0,
-  // 12 32.4
-  int parts = count >= 3072 ? 6 : count >= 2048 ? 4 : 1;
+  // 4096 LPs per call (medians of 5-7 calls, results read back behind the solves, two stagings):
+  // 4 parts 18.8-19.9 ms, 6 parts 18.4-19.2, 8 parts 18.2-18.3, 10 parts 19.5
+  int parts = count >= 3072 ? 8 : count >= 2048 ? 4 : 1;
   if (const char* e = std::getenv("SOVEREIGN_BATCH_PARTS")) parts = std::max(1, std::min(count, std::atoi(e)));
   // Part sizes: equal, or (SOVEREIGN_BATCH_TAPER=1) falling linearly, part k weighted parts - k,
   // so that the last parts, whose solves nothing overlaps, are the short ones.
