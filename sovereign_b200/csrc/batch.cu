@@ -1533,6 +1533,7 @@ size_t align8(size_t v) { return (v + 7) & ~size_t(7); }
 
 Batch* batch_create(int count, const sov_model* models, const sov_options* opt_in, int opt_stride,
                     const DeviceStarts* starts, int first_lp) {
+  auto model_no = [&](int i) { return std::to_string(first_lp + i); };  // the caller's numbering
   auto B = std::make_unique<Batch>();
   B->count = count;
   B->models.assign(models, models + count);
@@ -1569,7 +1570,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     try {
       B->forms[i] = build_std_form(models[i], false, opt_of(i).enable_scaling != 0);
     } catch (const std::exception& e) {
-      throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
+      throw std::runtime_error("model " + model_no(i) + ": " + e.what());
     }
     const StdForm& f = B->forms[i];
     shape[i] = LpShape{f.n_struct, f.m0, f.m, f.n, f.nnz(), 0};
@@ -1591,7 +1592,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
     LpMeta& mt = B->meta[i];
     std::memset(&mt, 0, sizeof(mt));
     if (starts && (sh.n != starts->n || sh.m != starts->m))
-      throw std::runtime_error("model " + std::to_string(first_lp + i) + ": IPM form " + std::to_string(sh.m) +
+      throw std::runtime_error("model " + model_no(i) + ": IPM form " + std::to_string(sh.m) +
                                " x " + std::to_string(sh.n) + " does not match the starts' " +
                                std::to_string(starts->m) + " x " + std::to_string(starts->n));
     if (kind[i] == kSingle) {
@@ -1750,7 +1751,7 @@ Batch* batch_create(int count, const sov_model* models, const sov_options* opt_i
           try {
             build_plain_lp_into(models[i], shape[i], false, out, &pb.info, false);
           } catch (const std::exception& e) {
-            throw std::runtime_error("model " + std::to_string(i) + ": " + e.what());
+            throw std::runtime_error("model " + model_no(i) + ": " + e.what());
           }
           pb.info.scaling_applied = mt.scale_mode == 1;
         } else {

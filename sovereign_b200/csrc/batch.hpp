@@ -21,6 +21,8 @@ struct DeviceStarts {
 
 int solve_batch(int count, const sov_model* models, const sov_options* opt, int opt_stride, sov_result* results,
                 const DeviceStarts* starts = nullptr);
+// first_lp: the caller's position of models[0] (a part of a larger call), for the device starts
+// and the model numbers in errors
 Batch* batch_create(int count, const sov_model* models, const sov_options* opt, int opt_stride = 0,
                     const DeviceStarts* starts = nullptr, int first_lp = 0);
 void batch_solve(Batch* b, cudaStream_t st);
