@@ -117,6 +117,19 @@ def test_batch_random_lps_match_reference():
         assert r.iterations <= ref.iterations + 2, k
 
 
+def test_batch_error_names_the_callers_model():
+    # a call of 3072 LPs runs in pipelined parts; a model that cannot be built is named by its
+    # position in the caller's list, not within its part
+    import dataclasses
+    models = P.transport_batch(3072, seed=41)
+    bad = models[2900]
+    ub = bad.ub.copy()
+    ub[0] = -1.0  # below its lower bound 0
+    models[2900] = dataclasses.replace(bad, ub=ub, _keep=[])
+    with pytest.raises(Exception, match=r"model 2900: Inconsistent bounds"):
+        solve_batch(models)
+
+
 def test_batch_run_to_run():
     # transportation LPs: every normal-matrix entry receives one term, so two runs agree bit for bit;
     # random LPs (several terms per entry, summed by shared-memory atomics in arrival order) agree to
