@@ -198,19 +198,26 @@ def _marshal(models: list[Model], with_ipm: bool):
 
 def _unmarshal(R: np.ndarray, buf: np.ndarray, layout, with_ipm: bool) -> list[Result]:
     off, n, mm, ni, mi = layout
+    k = len(R)
+    # the record fields as Python lists in one pass each (per-LP numpy scalar access costs more)
+    status, its, has = R["status"].tolist(), R["iterations"].tolist(), R["has_objective_value"].tolist()
+    obj, gap = R["objective_value"].tolist(), R["duality_gap"].tolist()
+    pres, dres = R["primal_residual"].tolist(), R["dual_residual"].tolist()
+    nip, mip, secs = R["n_ipm"].tolist(), R["m_ipm"].tolist(), R["solve_seconds"].tolist()
+    width = R.dtype["message"].itemsize  # the whole char array of a record
+    msgs = np.ascontiguousarray(R["message"]).view(f"S{width}").reshape(k).tolist() if k else []
+    offl, nl, ml = off.tolist(), n.tolist(), mm.tolist()
+    nil, mil = (ni.tolist(), mi.tolist()) if with_ipm else (None, None)
     out = []
-    status, its, has = R["status"], R["iterations"], R["has_objective_value"]
-    obj, gap, pres, dres = R["objective_value"], R["duality_gap"], R["primal_residual"], R["dual_residual"]
-    nip, mip, secs, msg = R["n_ipm"], R["m_ipm"], R["solve_seconds"], R["message"]
-    for k in range(len(R)):
-        o, a, b = int(off[k]), int(n[k]), int(mm[k])
-        r = Result(status=int(status[k]), iterations=int(its[k]), has_objective_value=bool(has[k]),
-                   objective_value=float(obj[k]), duality_gap=float(gap[k]), primal_residual=float(pres[k]),
-                   dual_residual=float(dres[k]), message=bytes(msg[k]).split(b"\0", 1)[0].decode(errors="replace"),
+    for q in range(k):
+        o, a, b = offl[q], nl[q], ml[q]
+        r = Result(status=status[q], iterations=its[q], has_objective_value=bool(has[q]),
+                   objective_value=obj[q], duality_gap=gap[q], primal_residual=pres[q],
+                   dual_residual=dres[q], message=msgs[q].split(b"\0", 1)[0].decode(errors="replace"),
                    primal=buf[o:o + a], dual_col=buf[o + a:o + 2 * a], dual_row=buf[o + 2 * a:o + 2 * a + b],
-                   n_ipm=int(nip[k]), m_ipm=int(mip[k]), solve_seconds=float(secs[k]))
+                   n_ipm=nip[q], m_ipm=mip[q], solve_seconds=secs[q])
         if with_ipm:
-            p, x, y = o + 2 * a + b, int(ni[k]), int(mi[k])
+            p, x, y = o + 2 * a + b, nil[q], mil[q]
             r.ipm_x, r.ipm_y, r.ipm_s = buf[p:p + x], buf[p + x:p + x + y], buf[p + x + y:p + 2 * x + y]
         out.append(r)
     return out
