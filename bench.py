@@ -675,7 +675,7 @@ def main():
     bufs = [ResultBuffers(m) for m in models]
     res_arr = (A.SovResult * count)(*[b.raw for b in bufs])
     opt = A.default_options()
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(1, min(args.steps, 20))  # as many calls as device steps (at most 20)
     for _ in range(max(1, min(args.warmup, 2))):  # untimed, like the device steps' warm-up
         _lib.check(lib.sov_lp_solve_batch(count, arr, C.byref(opt), 0, res_arr))
     barrier(dist, local)
